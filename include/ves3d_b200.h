@@ -1,0 +1,139 @@
+/* ves3d_b200 -- B200-native StokesVelocity path for Ves3D, C ABI.
+ *
+ * Every entry point returns an int status (0 = VES3D_OK) and never aborts; the
+ * message of the last failure on the calling thread is ves3d_last_error().
+ * Plain pointers and sizes only. Pointers documented as "device" are CUDA device
+ * pointers on the context's device; "host" pointers are ordinary host memory
+ * (pageable or pinned; the library stages through its own pinned buffers).
+ *
+ * Layouts follow the reference's containers (AxisMajor, src/Scalars.cc:36-44):
+ *   surface field   [n_ves][3][(p+1)*2p]   latitude-major Gauss-Legendre x uniform grid
+ *   SH coefficients [n_fun][p*(p+2)]        blocks by Fourier index, degrees m..p
+ *                                            (src/SphericalHarmonics.cc:32-38)
+ *   self matrix     [n_ves][3*Ncoef][3*Ncoef] row = input density coefficient,
+ *                                            column = output velocity coefficient
+ */
+#ifndef VES3D_B200_H
+#define VES3D_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum ves3d_status {
+  VES3D_OK = 0,
+  VES3D_ERR_ARG = 1,      /* invalid argument (sizes, orders, null pointers) */
+  VES3D_ERR_CUDA = 2,     /* a CUDA runtime call failed */
+  VES3D_ERR_NOMEM = 3,    /* device or pinned host allocation failed */
+  VES3D_ERR_STATE = 4,    /* call out of order (e.g. eval before set_src_coord) */
+  VES3D_ERR_NODEV = 5,    /* no CUDA device / not an sm_100 device */
+  VES3D_ERR_NUMERIC = 6   /* non-finite input or result detected */
+};
+
+enum ves3d_precision {
+  VES3D_PREC_FP64 = 0,    /* plain form: FP64 throughout */
+  VES3D_PREC_MIXED = 1    /* FP32 far field with compensated sums; FP64 pole quadrature */
+};
+
+int ves3d_version(void);
+const char* ves3d_last_error(void);
+/* Number of kernels this library launched since load (all entry points). */
+long long ves3d_kernel_launches(void);
+
+/* ---------------------------------------------------------------------------
+ * StokesVelocity operator context.
+ * Replaces StokesVelocity<Real> (include/StokesVelocity.h:16-44,
+ * src/StokesVelocity.cc:11-539) for surface targets, single layer:
+ *   StokesVelocity(sh_order, sh_order_up)      -> ves3d_sv_create
+ *   SetSrcCoord(S, up_self, up)                -> ves3d_sv_set_src_coord
+ *   SetDensitySL(f)                            -> ves3d_sv_set_density_sl
+ *   operator()(vel)                            -> ves3d_sv_eval
+ * The far field is the exact all-pairs sum over other vesicles' grid points
+ * (StokesAlltoAll - DirectStokesKernel, src/InterfacialVelocity.cc:1261-1291) in
+ * place of the reference's PVFMM call (src/StokesVelocity.cc:477-490).
+ * ------------------------------------------------------------------------- */
+typedef struct ves3d_sv ves3d_sv;
+
+/* sh_order_up <= 0 selects 2*sh_order (src/Parameters.cc:140). device < 0 uses the
+ * current device. */
+int ves3d_sv_create(int sh_order, int sh_order_up, int precision, int device, ves3d_sv** out);
+int ves3d_sv_destroy(ves3d_sv* sv);
+/* Bind a CUDA stream (cudaStream_t cast to void*) for all later work; NULL = the
+ * context's own stream. */
+int ves3d_sv_set_stream(ves3d_sv* sv, void* stream);
+
+/* Source surfaces, AxisMajor [n_ves][3][Ngrid]. Invalidates the cached self matrices
+ * (src/StokesVelocity.cc:26-57). is_device: 0 host pointer, 1 device pointer. */
+int ves3d_sv_set_src_coord(ves3d_sv* sv, const double* S, long n_ves, int is_device);
+/* Single-layer density, same layout as the surfaces (src/StokesVelocity.cc:66-97). */
+int ves3d_sv_set_density_sl(ves3d_sv* sv, const double* f, int is_device);
+/* Velocity at the surface points, same layout (src/StokesVelocity.cc:164-539).
+ * Builds the self matrices first if the surfaces changed. */
+int ves3d_sv_eval(ves3d_sv* sv, double* vel, int is_device);
+/* Build the self matrices now (the reference builds them lazily inside operator()). */
+int ves3d_sv_setup(ves3d_sv* sv);
+/* Copy the self matrices out, [n_ves][3Ncoef][3Ncoef]. */
+int ves3d_sv_get_self_matrix(ves3d_sv* sv, double* SL, int is_device);
+/* Split of the last eval into its parts: self (singular) and far (other vesicles),
+ * each AxisMajor like vel. Either pointer may be NULL. */
+int ves3d_sv_get_parts(ves3d_sv* sv, double* vel_self, double* vel_far, int is_device);
+/* Device time in ms of the last setup / eval stages:
+ * ms[0] self-matrix build, ms[1] self apply, ms[2] far field, ms[3] whole eval. */
+int ves3d_sv_stage_times(ves3d_sv* sv, float* ms);
+/* Device pointers of the context's resident buffers (for zero-copy callers):
+ * which = 0 surfaces, 1 density, 2 velocity. Valid until the next set_src_coord. */
+int ves3d_sv_device_buffer(ves3d_sv* sv, int which, double** ptr, size_t* n_elems);
+/* Evaluate using the resident density buffer (which=1) and write the resident
+ * velocity buffer (which=2); no host transfer. */
+int ves3d_sv_eval_resident(ves3d_sv* sv);
+
+/* ---------------------------------------------------------------------------
+ * Spherical-harmonic transforms on device pointers (SHTrans, include/SHTrans.h:21-63;
+ * math of SphericalHarmonics::Grid2SHC / SHC2Grid, src/SphericalHarmonics.cc:4-235).
+ * ------------------------------------------------------------------------- */
+/* grid at order p0 -> coefficients at order p1 (Grid2SHC). */
+int ves3d_sht_forward(const double* X, long n_fun, int p0, int p1, double* S, void* stream);
+/* coefficients at order p0 -> grid at order p1 (SHC2Grid), with optional longitude
+ * (X_theta) and latitude (X_phi) derivatives as named by the reference; NULL skips. */
+int ves3d_sht_backward(const double* S, long n_fun, int p0, int p1, double* X, double* X_theta,
+                       double* X_phi, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Direct Stokes sums on device pointers.
+ * ves3d_cuda_stokes: same arguments and meaning as the reference's
+ *   cuda_stokes(int src_m, int trg_m, int n, int t_head, int t_tail, const T* T,
+ *               const T* S, const T* D, T* U, const T* Q)   (include/CudaKernels.h,
+ *   src/CudaKernels.cu:1996-2006) i.e. Device<GPU>::DirectStokes
+ *   (include/Device.h:205-209): per-surface single layer with weights Q, targets
+ *   [t_head, t_tail) of each surface, AxisMajor strides src_m / trg_m, n surfaces.
+ * ------------------------------------------------------------------------- */
+int ves3d_cuda_stokes_f64(int src_m, int trg_m, int n, int t_head, int t_tail, const double* T,
+                          const double* S, const double* D, double* U, const double* Q, void* stream);
+
+/* All-pairs interaction with the reference's VesInteraction handle signature
+ * (include/VesInteraction.h:21, matched by StokesAlltoAll, include/CPUKernels.h:46-49):
+ * HOST pointers, point-major xyz, np points; pot[t] = sum over all s of the Stokeslet
+ * of den[s] (coincident points contribute nothing). *ctx may hold a library-owned
+ * workspace between calls; free it with ves3d_interaction_free(ctx). Errors are
+ * reported through ves3d_last_error() and leave pot filled with NaN. */
+void ves3d_stokes_alltoall_f64(const double* src, const double* den, size_t np, double* pot, void** ctx);
+void ves3d_interaction_free(void** ctx);
+/* Same on device pointers, with an int status. */
+int ves3d_stokes_alltoall_device_f64(const double* src, const double* den, size_t np, double* pot,
+                                     void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Diagnostics (host only, no GPU needed): copy one of the FP64 operator tables the
+ * library builds for (p0, p1) into out (capacity cap doubles); *n receives its length.
+ * Names: "nodes0", "weights0", "nodes1", "smooth_w0", "sing_w", "mr", "ana_leg",
+ * "ana_four", "syn1_leg", "syn1_dleg", "syn1_four", "syn1_dfour", "qp".
+ * ------------------------------------------------------------------------- */
+int ves3d_tables_export(int p0, int p1, const char* name, double* out, size_t cap, size_t* n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VES3D_B200_H */

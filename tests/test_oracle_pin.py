@@ -1,0 +1,142 @@
+"""Pin the CPU oracle (oracle/sh.py, oracle/direct.c) against the reference's own code
+compiled in place (oracle/_ref) and against analytic identities. CPU only."""
+import numpy as np
+import pytest
+
+from oracle import sh, stokes
+from tests.helpers import ellipsoid_pair, rel_err, unit_sphere
+
+# The reference's self part is reproducible only to ~1e-9 relative even against itself
+# (OpenBLAS vs plain-loop GEMM builds of the same source, test below): its MatRotate
+# forms sin(theta) = sqrt(1 - x^2) at rotated grid points that lie on a pole.
+REF_SELF_NOISE = 5e-9
+FAR_TOL = 1e-13
+PRIM_TOL = 1e-13
+
+
+@pytest.mark.parametrize("p", [6, 12, 16])
+def test_quadrature_rules(ref, p):
+    assert rel_err(sh.legendre_nodes(p), ref.legendre_nodes(p)) < PRIM_TOL
+    assert rel_err(sh.legendre_weights(p), ref.legendre_weights(p)) < PRIM_TOL
+    assert rel_err(sh.singular_weights(2 * p), ref.singular_weights(2 * p)) < PRIM_TOL
+
+
+@pytest.mark.parametrize("p,p1", [(6, 6), (6, 12), (12, 12), (12, 24), (16, 32), (12, 9)])
+def test_transforms(ref, p, p1):
+    rng = np.random.default_rng(p * 100 + p1)
+    X = rng.standard_normal(5 * sh.ngrid(p))
+    assert rel_err(sh.grid2shc(X, p, p1), ref.grid2shc(X, p, p1)) < PRIM_TOL
+    S = rng.standard_normal(5 * sh.ncoef(p))
+    if p1 >= p:
+        A = sh.shc2grid(S, p, p1, grads=True)
+        B = ref.shc2grid(S, p, p1, grads=True)
+        for a, b in zip(A, B):
+            assert rel_err(a, b) < PRIM_TOL
+    assert rel_err(sh.shc2pole(S, p), ref.shc2pole(S, p)) < PRIM_TOL
+
+
+def _poly(Q):
+    a, b, c = Q
+    return a * b * c + 0.3 * a ** 4 - b ** 3 * c + 0.7 * c ** 2 - a + 0.2 * b * c * c * a
+
+
+@pytest.mark.parametrize("p", [6, 12])
+def test_rotation_exact_on_polynomials(ref, p):
+    """Rotating a degree-4 polynomial restricted to the sphere must equal sampling it at
+    rotated points. The oracle's rotation (stable sin(theta)) is exact to rounding; the
+    reference's carries the pole noise."""
+    x = sh.legendre_nodes(p)
+    i = np.repeat(np.arange(p + 1), 2 * p)
+    j = np.tile(np.arange(2 * p), p + 1)
+    s = np.sqrt(1 - x[i] ** 2)
+    P = np.stack([x[i], s * np.sin(np.pi * j / p), s * np.cos(np.pi * j / p)])
+    S = sh.grid2shc(_poly(P), p, p)
+    ours = sh.rotate_all(S, p, 1).reshape(p + 1, p, -1)
+    theirs = ref.rotate_all(S, p, 1).reshape(p + 1, p, -1)
+    e_ours = e_ref = 0.0
+    for t in range(p + 1):
+        c_, s_ = -x[t], -np.sqrt(1 - x[t] ** 2)
+        Rm = np.array([[c_, 0, -s_], [0, 1, 0], [s_, 0, c_]])
+        for jj in range(p):
+            ph = np.pi * jj / p
+            Rz = np.array([[1, 0, 0], [0, np.cos(ph), np.sin(ph)], [0, -np.sin(ph), np.cos(ph)]])
+            truth = _poly(Rz @ Rm @ P)
+            e_ours = max(e_ours, np.abs(sh.shc2grid(ours[t, jj], p, p) - truth).max())
+            e_ref = max(e_ref, np.abs(sh.shc2grid(theirs[t, jj], p, p) - truth).max())
+    assert e_ours < 1e-13
+    assert e_ref < 1e-9  # reference: exact up to its pole noise
+
+
+@pytest.mark.parametrize("p", [6, 12])
+def test_reference_self_noise_floor(ref, p):
+    """Two builds of the reference that differ only in GEMM loop order disagree on the
+    self velocity by ~1e-10..1e-9; the oracle agrees with both within that floor."""
+    X = ellipsoid_pair(p)
+    f = np.random.default_rng(p).standard_normal(X.size)
+    A, _ = ref.singular_matrices(X, p, 2 * p)
+    B = ref.naive_singular_matrices(X, p, 2 * p)
+    va = ref.self_apply(A, f, p)
+    vb = ref.self_apply(B, f, p)
+    ours = sh.self_apply(sh.stokes_singular_matrix(X, p, 2 * p), f, p)
+    floor = rel_err(va, vb)
+    assert 1e-13 < floor < REF_SELF_NOISE
+    assert rel_err(ours, va) < REF_SELF_NOISE
+    assert rel_err(ours, vb) < REF_SELF_NOISE
+    # with the reference's own sin(theta) formula the oracle sits at the same floor
+    ours_u = sh.self_apply(sh.stokes_singular_matrix(X, p, 2 * p, stable=False), f, p)
+    assert rel_err(ours_u, va) < REF_SELF_NOISE
+
+
+@pytest.mark.parametrize("p", [6, 12])
+def test_sphere_identity(ref, p):
+    """Single layer on the unit sphere of f = (1,0,0) is (2/3) f (MonitorError-style
+    identity used by test/StokesDoubleLayerTest.cc:120-128)."""
+    X = unit_sphere(p)
+    f = np.zeros((3, sh.ngrid(p)))
+    f[0] = 1.0
+    v = sh.self_apply(sh.stokes_singular_matrix(X, p, 2 * p), f.reshape(-1), p).reshape(3, -1)
+    assert np.abs(v[0] - 2.0 / 3.0).max() < 1e-10
+    assert np.abs(v[1:]).max() < 1e-10
+    SL, _ = ref.singular_matrices(X, p, 2 * p)
+    vr = ref.self_apply(SL, f.reshape(-1), p).reshape(3, -1)
+    assert np.abs(vr[0] - 2.0 / 3.0).max() < 1e-10
+
+
+def test_far_field_vs_reference(ref):
+    from tests.helpers import small_suspension
+    X, f = small_suspension(2, 6, seed=5)
+    p = 6
+    ours = stokes.far_velocity(X, f, p)
+    theirs, _ = ref.far_sl(X, f, p)
+    assert rel_err(ours, theirs) < FAR_TOL
+    a1, qw1 = ref.area_weights(X, p)
+    assert rel_err(sh.area_element(X, p).reshape(-1), a1) < PRIM_TOL
+    assert rel_err(sh.smooth_weights_grid(p), qw1) < PRIM_TOL
+
+
+def test_direct_kernels_vs_reference(ref):
+    rng = np.random.default_rng(7)
+    np_ = 300
+    src = rng.standard_normal(3 * np_)
+    den = rng.standard_normal(3 * np_)
+    assert rel_err(stokes.alltoall(src, den), ref.alltoall(src, den)) < FAR_TOL
+    src[3:6] = src[0:3]  # a coincident pair contributes nothing in both
+    assert rel_err(stokes.alltoall(src, den), ref.alltoall(src, den)) < FAR_TOL
+    ns, stride = 3, 40
+    S = rng.standard_normal(3 * ns * stride)
+    T = rng.standard_normal(3 * ns * stride)
+    D = rng.standard_normal(3 * ns * stride)
+    Q = rng.uniform(0.5, 1.5, stride)
+    a = stokes.direct_stokes(stride, stride, ns, 5, 33, Q, T, S, D)
+    b = ref.direct_stokes(stride, stride, ns, 5, 33, Q, T, S, D)
+    assert rel_err(a, b) < FAR_TOL
+
+
+@pytest.mark.slow
+def test_full_composition_c1(ref):
+    """The FP64 StokesVelocity composition on the 8-vesicle p=12 suspension."""
+    from ves3d_b200 import workloads
+    X, f, p = workloads.make("c1_8ves_p12")
+    ours = stokes.stokes_velocity_sl(X, f, p)
+    theirs, _ = ref.stokes_velocity_sl(X, f, p, 2 * p)
+    assert rel_err(ours, theirs) < REF_SELF_NOISE

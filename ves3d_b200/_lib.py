@@ -1,0 +1,88 @@
+"""ctypes binding of the in-tree CUDA library ves3d_b200/libves3d_b200.so (C ABI of
+include/ves3d_b200.h). There is no CPU fallback: if the library is missing, or a call
+needs a GPU that is not there, the call raises."""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libves3d_b200.so")
+
+VES3D_OK = 0
+STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_NOMEM", 4: "ERR_STATE", 5: "ERR_NODEV", 6: "ERR_NUMERIC"}
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+_lib = None
+
+_d = ctypes.c_double
+_dp = ctypes.POINTER(ctypes.c_double)
+_vp = ctypes.c_void_p
+_i = ctypes.c_int
+_l = ctypes.c_long
+_sz = ctypes.c_size_t
+
+# (name, restype, argtypes) for every symbol declared in include/ves3d_b200.h
+SIGNATURES = [
+    ("ves3d_version", _i, []),
+    ("ves3d_last_error", ctypes.c_char_p, []),
+    ("ves3d_kernel_launches", ctypes.c_longlong, []),
+    ("ves3d_sv_create", _i, [_i, _i, _i, _i, ctypes.POINTER(_vp)]),
+    ("ves3d_sv_destroy", _i, [_vp]),
+    ("ves3d_sv_set_stream", _i, [_vp, _vp]),
+    ("ves3d_sv_set_src_coord", _i, [_vp, _vp, _l, _i]),
+    ("ves3d_sv_set_density_sl", _i, [_vp, _vp, _i]),
+    ("ves3d_sv_eval", _i, [_vp, _vp, _i]),
+    ("ves3d_sv_setup", _i, [_vp]),
+    ("ves3d_sv_get_self_matrix", _i, [_vp, _vp, _i]),
+    ("ves3d_sv_get_parts", _i, [_vp, _vp, _vp, _i]),
+    ("ves3d_sv_stage_times", _i, [_vp, ctypes.POINTER(ctypes.c_float)]),
+    ("ves3d_sv_device_buffer", _i, [_vp, _i, ctypes.POINTER(_vp), ctypes.POINTER(_sz)]),
+    ("ves3d_sv_eval_resident", _i, [_vp]),
+    ("ves3d_sht_forward", _i, [_vp, _l, _i, _i, _vp, _vp]),
+    ("ves3d_sht_backward", _i, [_vp, _l, _i, _i, _vp, _vp, _vp, _vp]),
+    ("ves3d_cuda_stokes_f64", _i, [_i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
+    ("ves3d_stokes_alltoall_f64", None, [_vp, _vp, _sz, _vp, ctypes.POINTER(_vp)]),
+    ("ves3d_interaction_free", None, [ctypes.POINTER(_vp)]),
+    ("ves3d_stokes_alltoall_device_f64", _i, [_vp, _vp, _sz, _vp, _vp]),
+    ("ves3d_tables_export", _i, [_i, _i, ctypes.c_char_p, _vp, _sz, ctypes.POINTER(_sz)]),
+]
+
+
+class Ves3dError(RuntimeError):
+    pass
+
+
+def lib():
+    """Load the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise Ves3dError(f"{LIB_PATH} is missing: build it with `python -m ves3d_b200.build` "
+                             "(there is no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status, what=""):
+    if status != VES3D_OK:
+        msg = lib().ves3d_last_error().decode(errors="replace")
+        raise Ves3dError(f"{what}: {STATUS.get(status, status)}: {msg}")
+    return status
+
+
+def kernel_launches():
+    return int(lib().ves3d_kernel_launches())
+
+
+def tables_export(p0, p1, name):
+    import numpy as np
+    n = _sz(0)
+    check(lib().ves3d_tables_export(p0, p1, name.encode(), None, 0, ctypes.byref(n)), "tables_export")
+    out = np.empty(n.value)
+    check(lib().ves3d_tables_export(p0, p1, name.encode(), out.ctypes.data, out.size, ctypes.byref(n)), "tables_export")
+    return out

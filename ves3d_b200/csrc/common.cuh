@@ -1,0 +1,59 @@
+// Shared helpers for the ves3d_b200 CUDA library: status codes, thread-local error
+// text, a global launch counter, and device helpers.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdio>
+#include <string>
+
+#include "../../include/ves3d_b200.h"
+
+namespace ves3d {
+
+void set_error(const char* fmt, ...);
+std::atomic<long long>& launch_counter();
+
+inline int cuda_status(cudaError_t e, const char* what, const char* file, int line) {
+  if (e == cudaSuccess) return VES3D_OK;
+  set_error("%s failed at %s:%d: %s", what, file, line, cudaGetErrorString(e));
+  return e == cudaErrorMemoryAllocation ? VES3D_ERR_NOMEM : VES3D_ERR_CUDA;
+}
+
+#define VES3D_CK(call)                                                          \
+  do {                                                                          \
+    int _st = ::ves3d::cuda_status((call), #call, __FILE__, __LINE__);          \
+    if (_st != VES3D_OK) return _st;                                            \
+  } while (0)
+
+// Check the launch that was just issued and count it.
+#define VES3D_LAUNCHED()                                                        \
+  do {                                                                          \
+    ::ves3d::launch_counter().fetch_add(1, std::memory_order_relaxed);          \
+    int _st = ::ves3d::cuda_status(cudaGetLastError(), "kernel launch", __FILE__, __LINE__); \
+    if (_st != VES3D_OK) return _st;                                            \
+  } while (0)
+
+#define VES3D_ARG(cond, msg)                                                    \
+  do {                                                                          \
+    if (!(cond)) {                                                              \
+      ::ves3d::set_error("invalid argument: %s", msg);                          \
+      return VES3D_ERR_ARG;                                                     \
+    }                                                                           \
+  } while (0)
+
+constexpr double kInv8Pi = 0.039788735772973836;  // 1/(8 pi)
+
+// 1/sqrt(r2) in FP64 for r2 > 0: single-precision hardware seed (rsqrtf) refined by one
+// third-order Newton/Householder step y <- y (1 + e/2 + 3e^2/8), e = 1 - r2 y^2
+// (Householder's method of order 3 applied to f(y) = y^-2 - r2). The seed's relative
+// error (~2^-23) becomes O(2^-66), i.e. the result is within rounding of 1/sqrt(r2).
+// Valid for FLT_MIN < r2 < FLT_MAX.
+__device__ __forceinline__ double rsqrt_f64(double r2) {
+  double y = (double)rsqrtf((float)r2);
+  double e = fma(-r2 * y, y, 1.0);
+  double c = fma(e, 0.375, 0.5);
+  return fma(y * e, c, y);
+}
+
+}  // namespace ves3d

@@ -1,0 +1,257 @@
+// FP64 direct Stokes single-layer sums (plain form) and the far-field source packing.
+//
+// Pair kernel (StokesAlltoAll, src/CPUKernels.cc:1011-1057; DirectStokesKernel, :123-178):
+//   r = x_s - x_t,  u_t += [ d_s / |r| + (r . d_s) r / |r|^3 ] / (8 pi),
+// and a coincident pair (|r| = 0) contributes nothing.
+//
+// Far field: targets are all N surface points, sources are the points of all OTHER
+// vesicles (the reference forms AllPairs - SameVesicle, src/InterfacialVelocity.cc:
+// 1261-1291; here same-vesicle pairs are masked pair by pair, which is the same sum
+// without the cancellation). One thread per target, source tiles staged in shared
+// memory, FP64 accumulation in registers.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace ves3d {
+
+constexpr int kFarBS = 128;
+
+struct PairAcc {
+  double x = 0.0, y = 0.0, z = 0.0;
+};
+
+__device__ __forceinline__ void pair_f64(double tx, double ty, double tz, double sx, double sy, double sz, double dx_,
+                                         double dy_, double dz_, bool skip, PairAcc& a) {
+  const double dx = sx - tx, dy = sy - ty, dz = sz - tz;
+  const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
+  double rinv = rsqrt_f64(r2);
+  rinv = (skip || r2 == 0.0) ? 0.0 : rinv;
+  const double cc = fma(dz, dz_, fma(dy, dy_, dx * dx_)) * rinv * rinv;
+  a.x = fma(fma(cc, dx, dx_), rinv, a.x);
+  a.y = fma(fma(cc, dy, dy_), rinv, a.y);
+  a.z = fma(fma(cc, dz, dz_), rinv, a.z);
+}
+
+// pos/den point-major [N][3]; out/add AxisMajor [nv][3][ng].
+__global__ void __launch_bounds__(kFarBS) k_far_f64(const double* __restrict__ pos, const double* __restrict__ den,
+                                                    long N, int ng, const double* __restrict__ add,
+                                                    double* __restrict__ out) {
+  __shared__ double sp[kFarBS * 3];
+  __shared__ double sd[kFarBS * 3];
+  const long g = (long)blockIdx.x * kFarBS + threadIdx.x;
+  const bool active = g < N;
+  double tx = 0, ty = 0, tz = 0;
+  long lo = 0;
+  if (active) {
+    tx = pos[3 * g];
+    ty = pos[3 * g + 1];
+    tz = pos[3 * g + 2];
+    lo = (g / ng) * ng;
+  }
+  PairAcc acc;
+  for (long s0 = 0; s0 < N; s0 += kFarBS) {
+    const int ns = (int)min((long)kFarBS, N - s0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < 3 * ns; i += kFarBS) {
+      sp[i] = pos[3 * s0 + i];
+      sd[i] = den[3 * s0 + i];
+    }
+    __syncthreads();
+    if (!active) continue;
+    const long rel = s0 - lo;  // source index relative to the target's vesicle start
+#pragma unroll 4
+    for (int k = 0; k < ns; k++) {
+      const bool same = (unsigned long)(rel + k) < (unsigned long)ng;
+      pair_f64(tx, ty, tz, sp[3 * k], sp[3 * k + 1], sp[3 * k + 2], sd[3 * k], sd[3 * k + 1], sd[3 * k + 2], same,
+               acc);
+    }
+  }
+  if (!active) return;
+  const long v = g / ng, k = g - v * ng;
+  const long o = v * 3 * ng + k;
+  const double b0 = add ? add[o] : 0.0, b1 = add ? add[o + ng] : 0.0, b2 = add ? add[o + 2 * ng] : 0.0;
+  out[o] = b0 + acc.x * kInv8Pi;
+  out[o + ng] = b1 + acc.y * kInv8Pi;
+  out[o + 2 * ng] = b2 + acc.z * kInv8Pi;
+}
+
+int launch_far_f64(const double* pos, const double* den, long nv, int ng, const double* add, double* out,
+                   cudaStream_t st) {
+  const long N = nv * ng;
+  if (N <= 0) return VES3D_OK;
+  k_far_f64<<<(unsigned)((N + kFarBS - 1) / kFarBS), kFarBS, 0, st>>>(pos, den, N, ng, add, out);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
+// All pairs, point-major in and out.
+__global__ void __launch_bounds__(kFarBS) k_alltoall_f64(const double* __restrict__ pos, const double* __restrict__ den,
+                                                         long N, double* __restrict__ pot) {
+  __shared__ double sp[kFarBS * 3];
+  __shared__ double sd[kFarBS * 3];
+  const long g = (long)blockIdx.x * kFarBS + threadIdx.x;
+  const bool active = g < N;
+  double tx = 0, ty = 0, tz = 0;
+  if (active) {
+    tx = pos[3 * g];
+    ty = pos[3 * g + 1];
+    tz = pos[3 * g + 2];
+  }
+  PairAcc acc;
+  for (long s0 = 0; s0 < N; s0 += kFarBS) {
+    const int ns = (int)min((long)kFarBS, N - s0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < 3 * ns; i += kFarBS) {
+      sp[i] = pos[3 * s0 + i];
+      sd[i] = den[3 * s0 + i];
+    }
+    __syncthreads();
+    if (!active) continue;
+#pragma unroll 4
+    for (int k = 0; k < ns; k++)
+      pair_f64(tx, ty, tz, sp[3 * k], sp[3 * k + 1], sp[3 * k + 2], sd[3 * k], sd[3 * k + 1], sd[3 * k + 2], false,
+               acc);
+  }
+  if (!active) return;
+  pot[3 * g] = acc.x * kInv8Pi;
+  pot[3 * g + 1] = acc.y * kInv8Pi;
+  pot[3 * g + 2] = acc.z * kInv8Pi;
+}
+
+int launch_alltoall_f64(const double* pos, const double* den, long np, double* pot, cudaStream_t st) {
+  if (np <= 0) return VES3D_OK;
+  k_alltoall_f64<<<(unsigned)((np + kFarBS - 1) / kFarBS), kFarBS, 0, st>>>(pos, den, np, pot);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
+// Device<GPU>::DirectStokes / cuda_stokes (src/CudaKernels.cu:1840-1916, 1996-2006):
+// per surface v, targets t in [t_head, t_tail) of T[v] (stride trg_m), sources all
+// src_m points of S[v] with density D * Q. grid = (target chunks, n surfaces).
+__global__ void __launch_bounds__(kFarBS) k_direct_stokes_f64(int src_m, int trg_m, int t_head, int t_tail,
+                                                              const double* __restrict__ T,
+                                                              const double* __restrict__ S,
+                                                              const double* __restrict__ D, double* __restrict__ U,
+                                                              const double* __restrict__ Q) {
+  __shared__ double sp[kFarBS * 3];
+  __shared__ double sd[kFarBS * 3];
+  const long v = blockIdx.y;
+  const int t = t_head + blockIdx.x * kFarBS + threadIdx.x;
+  const bool active = t < t_tail;
+  const double* Tv = T + v * 3 * (long)trg_m;
+  const double* Sv = S + v * 3 * (long)src_m;
+  const double* Dv = D + v * 3 * (long)src_m;
+  double tx = 0, ty = 0, tz = 0;
+  if (active) {
+    tx = Tv[t];
+    ty = Tv[trg_m + t];
+    tz = Tv[2 * trg_m + t];
+  }
+  PairAcc acc;
+  for (int s0 = 0; s0 < src_m; s0 += kFarBS) {
+    const int ns = min(kFarBS, src_m - s0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < ns; i += kFarBS) {
+      const int s = s0 + i;
+      const double q = Q[s];
+      sp[3 * i] = Sv[s];
+      sp[3 * i + 1] = Sv[src_m + s];
+      sp[3 * i + 2] = Sv[2 * src_m + s];
+      sd[3 * i] = Dv[s] * q;
+      sd[3 * i + 1] = Dv[src_m + s] * q;
+      sd[3 * i + 2] = Dv[2 * src_m + s] * q;
+    }
+    __syncthreads();
+    if (!active) continue;
+    for (int k = 0; k < ns; k++)
+      pair_f64(tx, ty, tz, sp[3 * k], sp[3 * k + 1], sp[3 * k + 2], sd[3 * k], sd[3 * k + 1], sd[3 * k + 2], false,
+               acc);
+  }
+  if (!active) return;
+  double* Uv = U + v * 3 * (long)trg_m;
+  Uv[t] = acc.x * kInv8Pi;
+  Uv[trg_m + t] = acc.y * kInv8Pi;
+  Uv[2 * trg_m + t] = acc.z * kInv8Pi;
+}
+
+int launch_direct_stokes_f64(int src_m, int trg_m, int n, int t_head, int t_tail, const double* T,
+                             const double* S, const double* D, double* U, const double* Q, cudaStream_t st) {
+  if (n <= 0 || t_tail <= t_head) return VES3D_OK;
+  dim3 grid((t_tail - t_head + kFarBS - 1) / kFarBS, n);
+  k_direct_stokes_f64<<<grid, kFarBS, 0, st>>>(src_m, trg_m, t_head, t_tail, T, S, D, U, Q);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
+// area = |X_theta x X_phi|; pos point-major; den = f * area * w[lat].
+__global__ void k_far_sources(const double* __restrict__ X, const double* __restrict__ f,
+                              const double* __restrict__ Xt, const double* __restrict__ Xp, long nv, int p0,
+                              const double* __restrict__ w, double* __restrict__ area, double* __restrict__ pos,
+                              double* __restrict__ den) {
+  const int ng = 2 * p0 * (p0 + 1);
+  const long g = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= nv * ng) return;
+  const long v = g / ng;
+  const int k = (int)(g - v * ng);
+  const long b = v * 3 * ng + k;
+  const double ax = Xt[b], ay = Xt[b + ng], az = Xt[b + 2 * ng];
+  const double bx = Xp[b], by = Xp[b + ng], bz = Xp[b + 2 * ng];
+  const double nx = ay * bz - az * by, ny = az * bx - ax * bz, nz = ax * by - ay * bx;
+  const double a = sqrt(nx * nx + ny * ny + nz * nz);
+  area[g] = a;
+  const double q = a * w[k / (2 * p0)];
+  pos[3 * g] = X[b];
+  pos[3 * g + 1] = X[b + ng];
+  pos[3 * g + 2] = X[b + 2 * ng];
+  if (f) {
+    den[3 * g] = f[b] * q;
+    den[3 * g + 1] = f[b + ng] * q;
+    den[3 * g + 2] = f[b + 2 * ng] * q;
+  }
+}
+
+int launch_far_sources(const double* X, const double* f, const double* Xt, const double* Xp, long nv, int p0,
+                       const double* smooth_w, double* area, double* pos, double* den, cudaStream_t st) {
+  const long N = nv * ngrid_(p0);
+  if (N <= 0) return VES3D_OK;
+  k_far_sources<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(X, f, Xt, Xp, nv, p0, smooth_w, area, pos, den);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
+__global__ void k_far_density(const double* __restrict__ f, const double* __restrict__ area, long nv, int p0,
+                              const double* __restrict__ w, double* __restrict__ den) {
+  const int ng = 2 * p0 * (p0 + 1);
+  const long g = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= nv * ng) return;
+  const long v = g / ng;
+  const int k = (int)(g - v * ng);
+  const long b = v * 3 * ng + k;
+  const double q = area[g] * w[k / (2 * p0)];
+  den[3 * g] = f[b] * q;
+  den[3 * g + 1] = f[b + ng] * q;
+  den[3 * g + 2] = f[b + 2 * ng] * q;
+}
+
+int launch_far_density(const double* f, const double* area, long nv, int p0, const double* smooth_w, double* den,
+                       cudaStream_t st) {
+  const long N = nv * ngrid_(p0);
+  if (N <= 0) return VES3D_OK;
+  k_far_density<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(f, area, nv, p0, smooth_w, den);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
+__global__ void k_add(const double* __restrict__ a, const double* __restrict__ b, long n, double* __restrict__ out) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = a[i] + b[i];
+}
+
+int launch_add(const double* a, const double* b, long n, double* out, cudaStream_t st) {
+  if (n <= 0) return VES3D_OK;
+  k_add<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a, b, n, out);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
+}  // namespace ves3d

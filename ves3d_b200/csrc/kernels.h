@@ -1,0 +1,60 @@
+// Kernel launchers of the ves3d_b200 CUDA library (device pointers, one stream).
+#pragma once
+#include <cuda_runtime.h>
+
+namespace ves3d {
+
+inline int ncoef_(int p) { return p * (p + 2); }
+inline int ngrid_(int p) { return 2 * p * (p + 1); }
+
+// Device copies of the tables of one (p0, p1) pair (layouts as in sh_tables.h).
+struct DevTables {
+  int p0 = 0, p1 = 0;
+  double *ana_four = nullptr, *ana_leg = nullptr;                   // Grid2SHC(p0, p0)
+  double *syn0_leg = nullptr, *syn0_dleg = nullptr, *syn0_four = nullptr, *syn0_dfour = nullptr;
+  double *syn1_leg = nullptr, *syn1_dleg = nullptr, *syn1_four = nullptr, *syn1_dfour = nullptr;
+  double *synT_four = nullptr;                                      // [2p1][2p0]
+  int *jf_of_coef = nullptr, *blk_off = nullptr, *m_of_coef = nullptr, *n_of_coef = nullptr;
+  int *partner = nullptr, *is_sin = nullptr;
+  double* mr = nullptr;
+  int *mr_off = nullptr, *perm = nullptr, *perm_off = nullptr, *pos_in_block = nullptr;
+  double *sing_w = nullptr, *smooth_w0 = nullptr, *qp = nullptr, *cos_tab = nullptr, *sin_tab = nullptr;
+};
+
+int launch_analysis(const double* in, long nfun, int pin, int pout, const double* four, const double* leg,
+                    const int* jf, double* out, cudaStream_t st);
+int launch_synthesis(const double* S, long nfun, int p0, int q, const double* leg, const double* dleg,
+                     const double* four, const double* dfour, const int* blk_off, double* X, double* Xt,
+                     double* Xp, cudaStream_t st);
+
+// RotateAll with dof = 3 (src/SphericalHarmonics.cc:363-449):
+// S [nv][3][Ncoef] -> R [nv][p0+1][p0][3][Ncoef].
+int launch_rotate_all(const double* S, long nv, const DevTables& T, double* R, cudaStream_t st);
+// Singular kernel (src/SphericalHarmonics.cc:971-1068) for nrot rotated surfaces:
+// X, Xt, Xp [nrot][3][M1], R [nrot][3][Ncoef] -> K [nrot][2][6][M1].
+int launch_singular_sl(const double* X, const double* Xt, const double* Xp, const double* R, long nrot,
+                       const DevTables& T, double* K, cudaStream_t st);
+// RotateTranspose with dof = 12 (:452-541) fused with the Rearrange (:1090-1172):
+// C [nv][p0+1][p0][2][6][Ncoef] -> SL3 [nv][3][Ncoef][3][Ngrid].
+int launch_rotate_transpose_scatter(const double* C, long nv, const DevTables& T, double* SL3, cudaStream_t st);
+// V[v] = F[v] . SL[v] (src/StokesVelocity.cc:397-416), n = 3 Ncoef.
+int launch_self_gemv(const double* F, const double* SL, long nv, int n, double* V, cudaStream_t st);
+// area element |X_theta x X_phi| and far-field sources: pos/den point-major [N][3],
+// den = f * area * smooth_w[lat]; X, f, Xt, Xp AxisMajor [nv][3][ng].
+int launch_far_sources(const double* X, const double* f, const double* Xt, const double* Xp, long nv, int p0,
+                       const double* smooth_w, double* area, double* pos, double* den, cudaStream_t st);
+// den only, from a stored area element.
+int launch_far_density(const double* f, const double* area, long nv, int p0, const double* smooth_w, double* den,
+                       cudaStream_t st);
+// out (AxisMajor) = add (AxisMajor, may be null) + sum over other vesicles' sources.
+int launch_far_f64(const double* pos, const double* den, long nv, int ng, const double* add, double* out,
+                   cudaStream_t st);
+// out = a + b elementwise.
+int launch_add(const double* a, const double* b, long n, double* out, cudaStream_t st);
+// All pairs, point-major in/out (StokesAlltoAll semantics).
+int launch_alltoall_f64(const double* pos, const double* den, long np, double* pot, cudaStream_t st);
+// Per-surface DirectStokes with weights (cuda_stokes semantics).
+int launch_direct_stokes_f64(int src_m, int trg_m, int n, int t_head, int t_tail, const double* T,
+                             const double* S, const double* D, double* U, const double* Q, cudaStream_t st);
+
+}  // namespace ves3d

@@ -1,0 +1,235 @@
+// FP64 kernels of the singular self-interaction build (plain form): coefficient
+// rotation to every target, the pole-singular Stokes kernel, and the adjoint rotation
+// that scatters the result into the per-vesicle self-matrix layout.
+// Math: SphericalHarmonics<Real>::RotateAll / StokesSingularInteg_ / RotateTranspose
+// (src/SphericalHarmonics.cc:363-541, 954-1180).
+#include "common.cuh"
+#include "kernels.h"
+
+namespace ves3d {
+
+// One CTA per (vesicle v, latitude rotation t); loops over the p0 longitude phases j.
+// out[c'] = sum_b (P_j s)[perm_n[b]] * Mr[t][n][b][pos(c')],   n = degree(c').
+__global__ void __launch_bounds__(256) k_rotate_all(const double* __restrict__ S, int p0, DevTables T,
+                                                    double* __restrict__ R) {
+  extern __shared__ double sm[];
+  const int nc = p0 * (p0 + 2);
+  double* sS = sm;
+  double* sB = sm + 3 * nc;
+  const int t = blockIdx.x;
+  const long v = blockIdx.y;
+  for (int i = threadIdx.x; i < 3 * nc; i += blockDim.x) sS[i] = S[v * 3 * nc + i];
+  __syncthreads();
+  for (int j = 0; j < p0; j++) {
+    for (int i = threadIdx.x; i < 3 * nc; i += blockDim.x) {
+      const int d = i / nc, c = i % nc;
+      const int pc = __ldg(T.partner + c);
+      if (pc < 0) {
+        sB[i] = sS[i];
+      } else {
+        const int q = (__ldg(T.m_of_coef + c) * j) % (2 * p0);
+        const double cs = __ldg(T.cos_tab + q), sn = __ldg(T.sin_tab + q);
+        if (!__ldg(T.is_sin + c)) {
+          sB[i] = sS[i] * cs + sS[d * nc + pc] * sn;
+        } else {
+          sB[i] = -sS[d * nc + pc] * sn + sS[i] * cs;
+        }
+      }
+    }
+    __syncthreads();
+    double* out = R + (((v * (p0 + 1) + t) * p0 + j) * 3) * (long)nc;
+    for (int i = threadIdx.x; i < 3 * nc; i += blockDim.x) {
+      const int d = i / nc, c = i % nc;
+      const int n = __ldg(T.n_of_coef + c), bp = __ldg(T.pos_in_block + c);
+      const int po = __ldg(T.perm_off + n), bn = __ldg(T.perm_off + n + 1) - po;
+      const double* M = T.mr + __ldg(T.mr_off + t * (p0 + 1) + n);
+      const double* b = sB + d * nc;
+      double s = 0.0;
+      for (int k = 0; k < bn; k++) s = fma(b[__ldg(T.perm + po + k)], __ldg(M + k * bn + bp), s);
+      out[i] = s;
+    }
+    __syncthreads();
+  }
+}
+
+int launch_rotate_all(const double* S, long nv, const DevTables& T, double* R, cudaStream_t st) {
+  if (nv <= 0) return VES3D_OK;
+  const int p0 = T.p0;
+  size_t smem = (size_t)6 * ncoef_(p0) * sizeof(double);
+  if (smem > 48 * 1024) VES3D_CK(cudaFuncSetAttribute(k_rotate_all, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 grid(p0 + 1, (unsigned)nv);
+  k_rotate_all<<<grid, 256, smem, st>>>(S, p0, T, R);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
+// One CTA per rotated surface. Pole targets from the m = 0 block (SHC2Pole, :325-360),
+// then for every upsampled source point s (latitude j0) and pole t:
+//   SL components  a1 + r_a r_b a2 with a1 = qs * area / (8 pi |r|), a2 = a1 / |r|^2,
+//   qs = SingularWeights(p1)[t ? j0 : p1 - j0], |r|^-1 := 0 when |r|^2 <= 2^-52.
+__global__ void __launch_bounds__(256) k_singular_sl(const double* __restrict__ X, const double* __restrict__ Xt,
+                                                     const double* __restrict__ Xp, const double* __restrict__ R,
+                                                     int p0, int p1, const double* __restrict__ qp,
+                                                     const double* __restrict__ sw, double* __restrict__ K) {
+  __shared__ double trg[6];
+  const long rot = blockIdx.x;
+  const int nc = p0 * (p0 + 2), M1 = 2 * p1 * (p1 + 1);
+  if (threadIdx.x < 6) {
+    const int c = threadIdx.x >> 1, t = threadIdx.x & 1;
+    const double* r = R + (rot * 3 + c) * nc;
+    double s = 0.0;
+    for (int n = 0; n <= p0; n++) s += r[n] * __ldg(qp + t * (p0 + 1) + n);
+    trg[c * 2 + t] = s;
+  }
+  __syncthreads();
+  const double eps = 2.220446049250313e-16;
+  const double* x = X + rot * 3 * M1;
+  const double* xt = Xt + rot * 3 * M1;
+  const double* xp = Xp + rot * 3 * M1;
+  double* k = K + rot * 12 * (long)M1;
+  for (int s = threadIdx.x; s < M1; s += blockDim.x) {
+    const int j0 = s / (2 * p1);
+    const double px = x[s], py = x[M1 + s], pz = x[2 * M1 + s];
+    const double ax = xt[s], ay = xt[M1 + s], az = xt[2 * M1 + s];
+    const double bx = xp[s], by = xp[M1 + s], bz = xp[2 * M1 + s];
+    const double nx = ay * bz - az * by, ny = az * bx - ax * bz, nz = ax * by - ay * bx;
+    const double area = sqrt(nx * nx + ny * ny + nz * nz);
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+      const double dx = trg[t] - px, dy = trg[2 + t] - py, dz = trg[4 + t] - pz;
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      double rinv = 1.0 / sqrt(r2);
+      if (r2 <= eps) rinv = 0.0;
+      const double rinv2 = rinv * rinv;
+      const double a1 = kInv8Pi * __ldg(sw + (t ? j0 : p1 - j0)) * area * rinv;
+      const double a2 = a1 * rinv2;
+      double* kt = k + (long)t * 6 * M1;
+      kt[s] = a1 + dx * dx * a2;
+      kt[M1 + s] = dx * dy * a2;
+      kt[2 * M1 + s] = dx * dz * a2;
+      kt[3 * M1 + s] = a1 + dy * dy * a2;
+      kt[4 * M1 + s] = dy * dz * a2;
+      kt[5 * M1 + s] = a1 + dz * dz * a2;
+    }
+  }
+}
+
+int launch_singular_sl(const double* X, const double* Xt, const double* Xp, const double* R, long nrot,
+                       const DevTables& T, double* K, cudaStream_t st) {
+  if (nrot <= 0) return VES3D_OK;
+  k_singular_sl<<<(unsigned)nrot, 256, 0, st>>>(X, Xt, Xp, R, T.p0, T.p1, T.qp, T.sing_w, K);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
+// One CTA per (vesicle, latitude rotation t), looping over (pole, component) and over
+// chunks of jb longitude rotations. For each input vector a (coefficients of one
+// (t, j, pole, comp) function): b = Mr_t^T a per degree block, then the inverse phase
+// P_j^T, then scatter into SL3[v][c_in][k][c_out][grid] at grid (t, j) for pole 0 and
+// (p0 - t, p0 + j) for pole 1, for both (c_in, c_out) orders of the symmetric component.
+__global__ void __launch_bounds__(256) k_rotate_transpose_scatter(const double* __restrict__ C, int p0, int jb,
+                                                                  DevTables T, double* __restrict__ SL3) {
+  extern __shared__ double sm[];
+  const int nc = p0 * (p0 + 2), ng = 2 * p0 * (p0 + 1);
+  double* sA = sm;             // jb * nc
+  double* sB = sm + jb * nc;   // jb * nc
+  const int t = blockIdx.x;
+  const long v = blockIdx.y;
+  // symmetric component -> (c_in, c_out) pairs
+  const int ci0[6] = {0, 0, 0, 1, 1, 2}, co0[6] = {0, 1, 2, 1, 2, 2};
+  for (int pole = 0; pole < 2; pole++) {
+    for (int comp = 0; comp < 6; comp++) {
+      for (int j0 = 0; j0 < p0; j0 += jb) {
+        const int nj = min(jb, p0 - j0);
+        for (int i = threadIdx.x; i < nj * nc; i += blockDim.x) {
+          const int jj = i / nc, c = i % nc;
+          sA[i] = C[((((v * (p0 + 1) + t) * p0 + j0 + jj) * 2 + pole) * 6 + comp) * (long)nc + c];
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < nj * nc; i += blockDim.x) {
+          const int jj = i / nc, c = i % nc;
+          const int n = __ldg(T.n_of_coef + c), b = __ldg(T.pos_in_block + c);
+          const int po = __ldg(T.perm_off + n), bn = __ldg(T.perm_off + n + 1) - po;
+          const double* M = T.mr + __ldg(T.mr_off + t * (p0 + 1) + n);
+          const double* a = sA + jj * nc;
+          double s = 0.0;
+          for (int k = 0; k < bn; k++) s = fma(a[__ldg(T.perm + po + k)], __ldg(M + b * bn + k), s);
+          sB[i] = s;
+        }
+        __syncthreads();
+        // inverse phase and scatter; consecutive threads take consecutive j for coalescing
+        for (int i = threadIdx.x; i < nj * nc; i += blockDim.x) {
+          const int jj = i % nj, c = i / nj;
+          const int j = j0 + jj;
+          const int pc = __ldg(T.partner + c);
+          double val;
+          if (pc < 0) {
+            val = sB[jj * nc + c];
+          } else {
+            const int q = (__ldg(T.m_of_coef + c) * j) % (2 * p0);
+            const double cs = __ldg(T.cos_tab + q), sn = __ldg(T.sin_tab + q);
+            if (!__ldg(T.is_sin + c)) {
+              val = sB[jj * nc + c] * cs - sB[jj * nc + pc] * sn;
+            } else {
+              val = sB[jj * nc + pc] * sn + sB[jj * nc + c] * cs;
+            }
+          }
+          const int grid = pole == 0 ? t * 2 * p0 + j : (p0 - t) * 2 * p0 + p0 + j;
+          const int cin = ci0[comp], cout = co0[comp];
+          SL3[(((v * 3 + cin) * nc + c) * 3 + cout) * (long)ng + grid] = val;
+          if (cin != cout) SL3[(((v * 3 + cout) * nc + c) * 3 + cin) * (long)ng + grid] = val;
+        }
+        __syncthreads();
+      }
+    }
+  }
+}
+
+int launch_rotate_transpose_scatter(const double* C, long nv, const DevTables& T, double* SL3, cudaStream_t st) {
+  if (nv <= 0) return VES3D_OK;
+  const int p0 = T.p0, nc = ncoef_(p0);
+  int jb = (int)((96 * 1024 / sizeof(double)) / (2 * (size_t)nc));
+  if (jb > p0) jb = p0;
+  if (jb < 1) jb = 1;
+  size_t smem = (size_t)2 * jb * nc * sizeof(double);
+  if (smem > 48 * 1024)
+    VES3D_CK(cudaFuncSetAttribute(k_rotate_transpose_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 grid(p0 + 1, (unsigned)nv);
+  k_rotate_transpose_scatter<<<grid, 256, smem, st>>>(C, p0, jb, T, SL3);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
+// V[v][col] = sum_row F[v][row] * SL[v][row][col]; one thread per output column.
+__global__ void __launch_bounds__(128) k_self_gemv(const double* __restrict__ F, const double* __restrict__ SL,
+                                                   int n, double* __restrict__ V) {
+  extern __shared__ double sF[];
+  const long v = blockIdx.y;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) sF[i] = F[v * n + i];
+  __syncthreads();
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= n) return;
+  const double* M = SL + v * (long)n * n + col;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  int r = 0;
+  for (; r + 4 <= n; r += 4) {
+    s0 = fma(sF[r], __ldg(M + (long)r * n), s0);
+    s1 = fma(sF[r + 1], __ldg(M + (long)(r + 1) * n), s1);
+    s2 = fma(sF[r + 2], __ldg(M + (long)(r + 2) * n), s2);
+    s3 = fma(sF[r + 3], __ldg(M + (long)(r + 3) * n), s3);
+  }
+  for (; r < n; r++) s0 = fma(sF[r], __ldg(M + (long)r * n), s0);
+  V[v * n + col] = (s0 + s1) + (s2 + s3);
+}
+
+int launch_self_gemv(const double* F, const double* SL, long nv, int n, double* V, cudaStream_t st) {
+  if (nv <= 0) return VES3D_OK;
+  dim3 grid((n + 127) / 128, (unsigned)nv);
+  size_t smem = (size_t)n * sizeof(double);
+  if (smem > 48 * 1024) VES3D_CK(cudaFuncSetAttribute(k_self_gemv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_self_gemv<<<grid, 128, smem, st>>>(F, SL, n, V);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
+}  // namespace ves3d

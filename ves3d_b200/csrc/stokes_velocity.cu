@@ -1,0 +1,636 @@
+// StokesVelocity operator context and the C ABI (include/ves3d_b200.h).
+//
+// Pipeline (plain FP64 form), all on one stream:
+//   set_src_coord: X -> Sx = Grid2SHC(X); (X_theta, X_phi) = SHC2Grid(Sx) at p;
+//                  area = |X_theta x X_phi|; far-field source positions.
+//   setup        : per chunk of vesicles: RotateAll(Sx) -> SHC2Grid(p -> p_up, +grads)
+//                  -> singular kernel -> SHC2GridTranspose(p_up -> p) -> RotateTranspose
+//                  + Rearrange -> Grid2SHC -> SL [v][3Nc][3Nc]
+//                  (SphericalHarmonics::StokesSingularInteg_, src/SphericalHarmonics.cc:954-1180)
+//   eval         : Fc = Grid2SHC(f); Vc = Fc . SL; Vself = SHC2Grid(Vc)
+//                  (src/StokesVelocity.cc:385-473); den = f * area * qw;
+//                  vel = Vself + sum over other vesicles (exact all-pairs far field).
+#include <cstdarg>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.h"
+#include "sh_tables.h"
+
+namespace ves3d {
+
+static thread_local char g_err[1024] = {0};
+
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+std::atomic<long long>& launch_counter() {
+  static std::atomic<long long> c{0};
+  return c;
+}
+
+template <class T>
+static int dalloc(T** p, size_t n) {
+  *p = nullptr;
+  if (n == 0) return VES3D_OK;
+  VES3D_CK(cudaMalloc((void**)p, n * sizeof(T)));
+  return VES3D_OK;
+}
+
+template <class T>
+static int dupload(T** p, const std::vector<T>& v, cudaStream_t st) {
+  int s = dalloc(p, v.size());
+  if (s) return s;
+  if (!v.empty()) VES3D_CK(cudaMemcpyAsync(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+  return VES3D_OK;
+}
+
+static void dfree(void* p) {
+  if (p) cudaFree(p);
+}
+
+struct TablesOwner {
+  ShTables h;
+  DevTables d;
+  ~TablesOwner() {
+    void* ptrs[] = {d.ana_four, d.ana_leg, d.syn0_leg, d.syn0_dleg, d.syn0_four, d.syn0_dfour, d.syn1_leg,
+                    d.syn1_dleg, d.syn1_four, d.syn1_dfour, d.synT_four, d.jf_of_coef, d.blk_off, d.m_of_coef,
+                    d.n_of_coef, d.partner, d.is_sin, d.mr, d.mr_off, d.perm, d.perm_off, d.pos_in_block,
+                    d.sing_w, d.smooth_w0, d.qp, d.cos_tab, d.sin_tab};
+    for (void* p : ptrs) dfree(p);
+  }
+  int upload(cudaStream_t st) {
+    d.p0 = h.p0;
+    d.p1 = h.p1;
+    int s = 0;
+    s |= dupload(&d.ana_four, h.ana.four, st);
+    s |= dupload(&d.ana_leg, h.ana.leg, st);
+    s |= dupload(&d.syn0_leg, h.syn0.leg, st);
+    s |= dupload(&d.syn0_dleg, h.syn0.dleg, st);
+    s |= dupload(&d.syn0_four, h.syn0.four, st);
+    s |= dupload(&d.syn0_dfour, h.syn0.dfour, st);
+    s |= dupload(&d.syn1_leg, h.syn1.leg, st);
+    s |= dupload(&d.syn1_dleg, h.syn1.dleg, st);
+    s |= dupload(&d.syn1_four, h.syn1.four, st);
+    s |= dupload(&d.syn1_dfour, h.syn1.dfour, st);
+    s |= dupload(&d.synT_four, h.synT.four, st);
+    s |= dupload(&d.jf_of_coef, h.jf_of_coef, st);
+    s |= dupload(&d.blk_off, h.blk_off, st);
+    s |= dupload(&d.m_of_coef, h.m_of_coef, st);
+    s |= dupload(&d.n_of_coef, h.n_of_coef, st);
+    s |= dupload(&d.partner, h.partner, st);
+    s |= dupload(&d.is_sin, h.is_sin, st);
+    s |= dupload(&d.mr, h.mr, st);
+    s |= dupload(&d.mr_off, h.mr_off, st);
+    s |= dupload(&d.perm, h.perm, st);
+    s |= dupload(&d.perm_off, h.perm_off, st);
+    s |= dupload(&d.pos_in_block, h.pos_in_block, st);
+    s |= dupload(&d.sing_w, h.sing_w, st);
+    s |= dupload(&d.smooth_w0, h.smooth_w0, st);
+    s |= dupload(&d.qp, h.qp, st);
+    s |= dupload(&d.cos_tab, h.cos_tab, st);
+    s |= dupload(&d.sin_tab, h.sin_tab, st);
+    if (s) return VES3D_ERR_NOMEM;
+    VES3D_CK(cudaStreamSynchronize(st));
+    return VES3D_OK;
+  }
+};
+
+}  // namespace ves3d
+
+using namespace ves3d;
+
+struct ves3d_sv {
+  int p = 0, pup = 0, prec = 0, device = 0;
+  cudaStream_t stream = nullptr, own_stream = nullptr;
+  std::unique_ptr<TablesOwner> tab;
+  long nves = 0, cap_ves = 0;
+  // resident buffers
+  double *X = nullptr, *F = nullptr, *V = nullptr, *Vself = nullptr, *Vfar = nullptr;
+  double *Sx = nullptr, *Xt = nullptr, *Xp = nullptr, *area = nullptr, *pos = nullptr, *den = nullptr;
+  double *SL = nullptr, *Fc = nullptr, *Vc = nullptr;
+  // setup scratch (one chunk of vesicles)
+  long chunk = 0;
+  double *R = nullptr, *Xu = nullptr, *Xut = nullptr, *Xup = nullptr, *K = nullptr, *C = nullptr, *SL3 = nullptr;
+  bool have_src = false, have_den = false, sl_valid = false, parts_valid = false;
+  cudaEvent_t ev[6] = {};
+  float ms[4] = {0, 0, 0, 0};
+
+  ~ves3d_sv() {
+    free_buffers();
+    free_scratch();
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    tab.reset();
+    if (own_stream) cudaStreamDestroy(own_stream);
+  }
+  void free_buffers() {
+    double* ps[] = {X, F, V, Vself, Vfar, Sx, Xt, Xp, area, pos, den, SL, Fc, Vc};
+    for (double* q : ps) dfree(q);
+    X = F = V = Vself = Vfar = Sx = Xt = Xp = area = pos = den = SL = Fc = Vc = nullptr;
+    cap_ves = 0;
+  }
+  void free_scratch() {
+    double* ps[] = {R, Xu, Xut, Xup, K, C, SL3};
+    for (double* q : ps) dfree(q);
+    R = Xu = Xut = Xup = K = C = SL3 = nullptr;
+    chunk = 0;
+  }
+  long npts() const { return nves * ngrid_(p); }
+};
+
+namespace {
+
+int check_sv(ves3d_sv* sv) {
+  if (!sv) {
+    set_error("invalid argument: null context");
+    return VES3D_ERR_ARG;
+  }
+  VES3D_CK(cudaSetDevice(sv->device));
+  return VES3D_OK;
+}
+
+int alloc_resident(ves3d_sv* sv, long nves) {
+  if (nves <= sv->cap_ves) return VES3D_OK;
+  sv->free_buffers();
+  const size_t ng = ngrid_(sv->p), nc = ncoef_(sv->p), n = 3 * nc, fld = (size_t)nves * 3 * ng;
+  int s = 0;
+  s |= dalloc(&sv->X, fld);
+  s |= dalloc(&sv->F, fld);
+  s |= dalloc(&sv->V, fld);
+  s |= dalloc(&sv->Vself, fld);
+  s |= dalloc(&sv->Vfar, fld);
+  s |= dalloc(&sv->Sx, (size_t)nves * 3 * nc);
+  s |= dalloc(&sv->Xt, fld);
+  s |= dalloc(&sv->Xp, fld);
+  s |= dalloc(&sv->area, (size_t)nves * ng);
+  s |= dalloc(&sv->pos, fld);
+  s |= dalloc(&sv->den, fld);
+  s |= dalloc(&sv->SL, (size_t)nves * n * n);
+  s |= dalloc(&sv->Fc, (size_t)nves * n);
+  s |= dalloc(&sv->Vc, (size_t)nves * n);
+  if (s) {
+    sv->free_buffers();
+    return s;
+  }
+  sv->cap_ves = nves;
+  return VES3D_OK;
+}
+
+// Doubles of setup scratch per vesicle.
+size_t scratch_per_vesicle(int p0, int p1) {
+  const size_t npr = (size_t)p0 * (p0 + 1), nc = ncoef_(p0), M1 = ngrid_(p1), ng = ngrid_(p0);
+  return npr * 3 * nc            // R
+         + 3 * npr * 3 * M1      // Xu, Xut, Xup
+         + npr * 12 * M1         // K
+         + npr * 12 * nc         // C
+         + 3 * nc * 3 * ng;      // SL3
+}
+
+int alloc_scratch(ves3d_sv* sv) {
+  const long want = sv->nves;
+  size_t per = scratch_per_vesicle(sv->p, sv->pup) * sizeof(double);
+  size_t free_b = 0, total_b = 0;
+  VES3D_CK(cudaMemGetInfo(&free_b, &total_b));
+  size_t budget = (size_t)8 << 30;
+  if (budget > free_b / 3) budget = free_b / 3;
+  long chunk = (long)(budget / per);
+  if (chunk < 1) chunk = 1;
+  if (chunk > want) chunk = want;
+  if (chunk <= sv->chunk) return VES3D_OK;
+  sv->free_scratch();
+  const size_t npr = (size_t)sv->p * (sv->p + 1), nc = ncoef_(sv->p), M1 = ngrid_(sv->pup), ng = ngrid_(sv->p);
+  int s = 0;
+  s |= dalloc(&sv->R, chunk * npr * 3 * nc);
+  s |= dalloc(&sv->Xu, chunk * npr * 3 * M1);
+  s |= dalloc(&sv->Xut, chunk * npr * 3 * M1);
+  s |= dalloc(&sv->Xup, chunk * npr * 3 * M1);
+  s |= dalloc(&sv->K, chunk * npr * 12 * M1);
+  s |= dalloc(&sv->C, chunk * npr * 12 * nc);
+  s |= dalloc(&sv->SL3, chunk * 3 * nc * 3 * ng);
+  if (s) {
+    sv->free_scratch();
+    return s;
+  }
+  sv->chunk = chunk;
+  return VES3D_OK;
+}
+
+int copy_in(double* dst, const double* src, size_t n, int is_device, cudaStream_t st) {
+  VES3D_CK(cudaMemcpyAsync(dst, src, n * sizeof(double), is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                           st));
+  return VES3D_OK;
+}
+
+int copy_out(double* dst, const double* src, size_t n, int is_device, cudaStream_t st) {
+  VES3D_CK(cudaMemcpyAsync(dst, src, n * sizeof(double), is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                           st));
+  if (!is_device) VES3D_CK(cudaStreamSynchronize(st));
+  return VES3D_OK;
+}
+
+int run_setup(ves3d_sv* sv) {
+  const DevTables& T = sv->tab->d;
+  const int p0 = sv->p, p1 = sv->pup, nc = ncoef_(p0), ng = ngrid_(p0), M1 = ngrid_(p1);
+  const long npr = (long)p0 * (p0 + 1);
+  cudaStream_t st = sv->stream;
+  int s = alloc_scratch(sv);
+  if (s) return s;
+  VES3D_CK(cudaEventRecord(sv->ev[0], st));
+  for (long v0 = 0; v0 < sv->nves; v0 += sv->chunk) {
+    const long nb = std::min(sv->chunk, sv->nves - v0);
+    const long nrot = nb * npr;
+    if ((s = launch_rotate_all(sv->Sx + v0 * 3 * nc, nb, T, sv->R, st))) return s;
+    if ((s = launch_synthesis(sv->R, nrot * 3, p0, p1, T.syn1_leg, T.syn1_dleg, T.syn1_four, T.syn1_dfour, T.blk_off,
+                              sv->Xu, sv->Xut, sv->Xup, st)))
+      return s;
+    if ((s = launch_singular_sl(sv->Xu, sv->Xut, sv->Xup, sv->R, nrot, T, sv->K, st))) return s;
+    if ((s = launch_analysis(sv->K, nrot * 12, p1, p0, T.synT_four, T.syn1_leg, T.jf_of_coef, sv->C, st))) return s;
+    if ((s = launch_rotate_transpose_scatter(sv->C, nb, T, sv->SL3, st))) return s;
+    if ((s = launch_analysis(sv->SL3, nb * 3 * nc * 3, p0, p0, T.ana_four, T.ana_leg, T.jf_of_coef,
+                             sv->SL + v0 * (long)(3 * nc) * (3 * nc), st)))
+      return s;
+    (void)ng;
+    (void)M1;
+  }
+  VES3D_CK(cudaEventRecord(sv->ev[1], st));
+  VES3D_CK(cudaEventSynchronize(sv->ev[1]));
+  VES3D_CK(cudaEventElapsedTime(&sv->ms[0], sv->ev[0], sv->ev[1]));
+  sv->sl_valid = true;
+  return VES3D_OK;
+}
+
+int run_eval(ves3d_sv* sv) {
+  const DevTables& T = sv->tab->d;
+  const int p0 = sv->p, nc = ncoef_(p0), n = 3 * nc;
+  cudaStream_t st = sv->stream;
+  int s;
+  if (!sv->have_src || !sv->have_den) {
+    set_error("eval before set_src_coord / set_density_sl");
+    return VES3D_ERR_STATE;
+  }
+  if (!sv->sl_valid && (s = run_setup(sv))) return s;
+  VES3D_CK(cudaEventRecord(sv->ev[2], st));
+  if ((s = launch_analysis(sv->F, sv->nves * 3, p0, p0, T.ana_four, T.ana_leg, T.jf_of_coef, sv->Fc, st))) return s;
+  if ((s = launch_self_gemv(sv->Fc, sv->SL, sv->nves, n, sv->Vc, st))) return s;
+  if ((s = launch_synthesis(sv->Vc, sv->nves * 3, p0, p0, T.syn0_leg, T.syn0_dleg, T.syn0_four, T.syn0_dfour,
+                            T.blk_off, sv->Vself, nullptr, nullptr, st)))
+    return s;
+  VES3D_CK(cudaEventRecord(sv->ev[3], st));
+  if ((s = launch_far_density(sv->F, sv->area, sv->nves, p0, T.smooth_w0, sv->den, st))) return s;
+  if ((s = launch_far_f64(sv->pos, sv->den, sv->nves, ngrid_(p0), nullptr, sv->Vfar, st))) return s;
+  if ((s = launch_add(sv->Vself, sv->Vfar, (long)sv->nves * 3 * ngrid_(p0), sv->V, st))) return s;
+  VES3D_CK(cudaEventRecord(sv->ev[4], st));
+  VES3D_CK(cudaEventSynchronize(sv->ev[4]));
+  VES3D_CK(cudaEventElapsedTime(&sv->ms[1], sv->ev[2], sv->ev[3]));
+  VES3D_CK(cudaEventElapsedTime(&sv->ms[2], sv->ev[3], sv->ev[4]));
+  VES3D_CK(cudaEventElapsedTime(&sv->ms[3], sv->ev[2], sv->ev[4]));
+  sv->parts_valid = true;
+  return VES3D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ves3d_version(void) { return 100; }
+
+const char* ves3d_last_error(void) { return g_err; }
+
+long long ves3d_kernel_launches(void) { return launch_counter().load(); }
+
+int ves3d_sv_create(int sh_order, int sh_order_up, int precision, int device, ves3d_sv** out) {
+  VES3D_ARG(out != nullptr, "out is null");
+  *out = nullptr;
+  VES3D_ARG(sh_order >= 2 && sh_order <= 64, "sh_order must be in [2, 64]");
+  if (sh_order_up <= 0) sh_order_up = 2 * sh_order;
+  VES3D_ARG(sh_order_up >= sh_order && sh_order_up <= 128, "sh_order_up must be in [sh_order, 128]");
+  VES3D_ARG(precision == VES3D_PREC_FP64 || precision == VES3D_PREC_MIXED, "unknown precision");
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    set_error("no CUDA device: %s", cudaGetErrorString(e));
+    return VES3D_ERR_NODEV;
+  }
+  if (device < 0) VES3D_CK(cudaGetDevice(&device));
+  VES3D_ARG(device < ndev, "device index out of range");
+  VES3D_CK(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  VES3D_CK(cudaGetDeviceProperties(&prop, device));
+  if (prop.major != 10) {
+    set_error("device %d is sm_%d%d; this library is built for sm_100a", device, prop.major, prop.minor);
+    return VES3D_ERR_NODEV;
+  }
+  std::unique_ptr<ves3d_sv> sv(new ves3d_sv());
+  sv->p = sh_order;
+  sv->pup = sh_order_up;
+  sv->prec = precision;
+  sv->device = device;
+  VES3D_CK(cudaStreamCreateWithFlags(&sv->own_stream, cudaStreamNonBlocking));
+  sv->stream = sv->own_stream;
+  for (auto& ev : sv->ev) VES3D_CK(cudaEventCreate(&ev));
+  sv->tab.reset(new TablesOwner());
+  build_tables(sh_order, sh_order_up, sv->tab->h);
+  int s = sv->tab->upload(sv->stream);
+  if (s) return s;
+  *out = sv.release();
+  return VES3D_OK;
+}
+
+int ves3d_sv_destroy(ves3d_sv* sv) {
+  if (!sv) return VES3D_OK;
+  cudaSetDevice(sv->device);
+  if (sv->stream) cudaStreamSynchronize(sv->stream);
+  delete sv;
+  return VES3D_OK;
+}
+
+int ves3d_sv_set_stream(ves3d_sv* sv, void* stream) {
+  int s = check_sv(sv);
+  if (s) return s;
+  sv->stream = stream ? (cudaStream_t)stream : sv->own_stream;
+  return VES3D_OK;
+}
+
+int ves3d_sv_set_src_coord(ves3d_sv* sv, const double* S, long n_ves, int is_device) {
+  int s = check_sv(sv);
+  if (s) return s;
+  VES3D_ARG(S != nullptr, "S is null");
+  VES3D_ARG(n_ves >= 1, "n_ves must be >= 1");
+  if ((s = alloc_resident(sv, n_ves))) return s;
+  sv->nves = n_ves;
+  const int p0 = sv->p, ng = ngrid_(p0);
+  const DevTables& T = sv->tab->d;
+  if ((s = copy_in(sv->X, S, (size_t)n_ves * 3 * ng, is_device, sv->stream))) return s;
+  if ((s = launch_analysis(sv->X, n_ves * 3, p0, p0, T.ana_four, T.ana_leg, T.jf_of_coef, sv->Sx, sv->stream))) return s;
+  if ((s = launch_synthesis(sv->Sx, n_ves * 3, p0, p0, T.syn0_leg, T.syn0_dleg, T.syn0_four, T.syn0_dfour, T.blk_off,
+                            sv->Vself /* scratch: filtered grid, unused */, sv->Xt, sv->Xp, sv->stream)))
+    return s;
+  if ((s = launch_far_sources(sv->X, nullptr, sv->Xt, sv->Xp, n_ves, p0, T.smooth_w0, sv->area, sv->pos, nullptr,
+                              sv->stream)))
+    return s;
+  VES3D_CK(cudaStreamSynchronize(sv->stream));
+  sv->have_src = true;
+  sv->have_den = false;
+  sv->sl_valid = false;
+  sv->parts_valid = false;
+  return VES3D_OK;
+}
+
+int ves3d_sv_set_density_sl(ves3d_sv* sv, const double* f, int is_device) {
+  int s = check_sv(sv);
+  if (s) return s;
+  VES3D_ARG(f != nullptr, "f is null");
+  if (!sv->have_src) {
+    set_error("set_density_sl before set_src_coord");
+    return VES3D_ERR_STATE;
+  }
+  if ((s = copy_in(sv->F, f, (size_t)sv->npts() * 3, is_device, sv->stream))) return s;
+  sv->have_den = true;
+  sv->parts_valid = false;
+  return VES3D_OK;
+}
+
+int ves3d_sv_setup(ves3d_sv* sv) {
+  int s = check_sv(sv);
+  if (s) return s;
+  if (!sv->have_src) {
+    set_error("setup before set_src_coord");
+    return VES3D_ERR_STATE;
+  }
+  return run_setup(sv);
+}
+
+int ves3d_sv_eval(ves3d_sv* sv, double* vel, int is_device) {
+  int s = check_sv(sv);
+  if (s) return s;
+  VES3D_ARG(vel != nullptr, "vel is null");
+  if ((s = run_eval(sv))) return s;
+  return copy_out(vel, sv->V, (size_t)sv->npts() * 3, is_device, sv->stream);
+}
+
+int ves3d_sv_eval_resident(ves3d_sv* sv) {
+  int s = check_sv(sv);
+  if (s) return s;
+  return run_eval(sv);
+}
+
+int ves3d_sv_get_self_matrix(ves3d_sv* sv, double* SL, int is_device) {
+  int s = check_sv(sv);
+  if (s) return s;
+  VES3D_ARG(SL != nullptr, "SL is null");
+  if (!sv->have_src) {
+    set_error("no surfaces set");
+    return VES3D_ERR_STATE;
+  }
+  if (!sv->sl_valid && (s = run_setup(sv))) return s;
+  const size_t n = 3 * (size_t)ncoef_(sv->p);
+  return copy_out(SL, sv->SL, (size_t)sv->nves * n * n, is_device, sv->stream);
+}
+
+int ves3d_sv_get_parts(ves3d_sv* sv, double* vel_self, double* vel_far, int is_device) {
+  int s = check_sv(sv);
+  if (s) return s;
+  if (!sv->parts_valid) {
+    set_error("no evaluation since the last input change");
+    return VES3D_ERR_STATE;
+  }
+  const size_t n = (size_t)sv->npts() * 3;
+  if (vel_self && (s = copy_out(vel_self, sv->Vself, n, is_device, sv->stream))) return s;
+  if (vel_far && (s = copy_out(vel_far, sv->Vfar, n, is_device, sv->stream))) return s;
+  return VES3D_OK;
+}
+
+int ves3d_sv_stage_times(ves3d_sv* sv, float* ms) {
+  VES3D_ARG(sv != nullptr && ms != nullptr, "null argument");
+  for (int i = 0; i < 4; i++) ms[i] = sv->ms[i];
+  return VES3D_OK;
+}
+
+int ves3d_sv_device_buffer(ves3d_sv* sv, int which, double** ptr, size_t* n_elems) {
+  VES3D_ARG(sv != nullptr && ptr != nullptr, "null argument");
+  if (!sv->have_src) {
+    set_error("no surfaces set");
+    return VES3D_ERR_STATE;
+  }
+  double* p = which == 0 ? sv->X : which == 1 ? sv->F : which == 2 ? sv->V : nullptr;
+  VES3D_ARG(p != nullptr, "which must be 0, 1 or 2");
+  *ptr = p;
+  if (n_elems) *n_elems = (size_t)sv->npts() * 3;
+  if (which == 1) {
+    sv->have_den = true;  // caller writes the density in place
+    sv->parts_valid = false;
+  }
+  return VES3D_OK;
+}
+
+int ves3d_sht_forward(const double* X, long n_fun, int p0, int p1, double* S, void* stream) {
+  VES3D_ARG(X && S, "null pointer");
+  VES3D_ARG(p0 >= 1 && p1 >= 1 && p0 <= 128 && p1 <= 128, "orders must be in [1, 128]");
+  VES3D_ARG(n_fun >= 0, "n_fun < 0");
+  cudaStream_t st = (cudaStream_t)stream;
+  AnalysisTables A;
+  build_analysis_tables(p0, p1, A);
+  std::vector<int> blk, jf;
+  coef_blocks(p1, blk, jf);
+  double *dfour = nullptr, *dleg = nullptr;
+  int* djf = nullptr;
+  int s = 0;
+  s |= dupload(&dfour, A.four, st);
+  s |= dupload(&dleg, A.leg, st);
+  s |= dupload(&djf, jf, st);
+  if (!s) s = launch_analysis(X, n_fun, p0, p1, dfour, dleg, djf, S, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  dfree(dfour);
+  dfree(dleg);
+  dfree(djf);
+  if (s) return s;
+  VES3D_CK(e);
+  return VES3D_OK;
+}
+
+int ves3d_sht_backward(const double* S, long n_fun, int p0, int p1, double* X, double* X_theta, double* X_phi,
+                       void* stream) {
+  VES3D_ARG(S && X, "null pointer");
+  VES3D_ARG(p0 >= 1 && p1 >= 1 && p0 <= 128 && p1 <= 128, "orders must be in [1, 128]");
+  VES3D_ARG(n_fun >= 0, "n_fun < 0");
+  cudaStream_t st = (cudaStream_t)stream;
+  SynthTables syn;
+  build_synth_tables(p0, p1, syn);
+  std::vector<int> blk, jf;
+  coef_blocks(p0, blk, jf);
+  double *dl = nullptr, *ddl = nullptr, *df = nullptr, *ddf = nullptr;
+  int* db = nullptr;
+  int s = 0;
+  s |= dupload(&dl, syn.leg, st);
+  s |= dupload(&ddl, syn.dleg, st);
+  s |= dupload(&df, syn.four, st);
+  s |= dupload(&ddf, syn.dfour, st);
+  s |= dupload(&db, blk, st);
+  if (!s) s = launch_synthesis(S, n_fun, p0, p1, dl, ddl, df, ddf, db, X, X_theta, X_phi, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  dfree(dl);
+  dfree(ddl);
+  dfree(df);
+  dfree(ddf);
+  dfree(db);
+  if (s) return s;
+  VES3D_CK(e);
+  return VES3D_OK;
+}
+
+int ves3d_tables_export(int p0, int p1, const char* name, double* out, size_t cap, size_t* n) {
+  VES3D_ARG(name != nullptr && n != nullptr, "null argument");
+  VES3D_ARG(p0 >= 2 && p0 <= 64 && p1 >= p0 && p1 <= 128, "orders out of range");
+  ShTables T;
+  build_tables(p0, p1, T);
+  const std::vector<double>* v = nullptr;
+  std::string nm(name);
+  if (nm == "nodes0") v = &T.x0;
+  else if (nm == "weights0") v = &T.w0;
+  else if (nm == "nodes1") v = &T.x1;
+  else if (nm == "smooth_w0") v = &T.smooth_w0;
+  else if (nm == "sing_w") v = &T.sing_w;
+  else if (nm == "mr") v = &T.mr;
+  else if (nm == "ana_leg") v = &T.ana.leg;
+  else if (nm == "ana_four") v = &T.ana.four;
+  else if (nm == "syn1_leg") v = &T.syn1.leg;
+  else if (nm == "syn1_dleg") v = &T.syn1.dleg;
+  else if (nm == "syn1_four") v = &T.syn1.four;
+  else if (nm == "syn1_dfour") v = &T.syn1.dfour;
+  else if (nm == "qp") v = &T.qp;
+  VES3D_ARG(v != nullptr, "unknown table name");
+  *n = v->size();
+  if (out) {
+    VES3D_ARG(cap >= v->size(), "output capacity too small");
+    std::memcpy(out, v->data(), v->size() * sizeof(double));
+  }
+  return VES3D_OK;
+}
+
+int ves3d_cuda_stokes_f64(int src_m, int trg_m, int n, int t_head, int t_tail, const double* T, const double* S,
+                          const double* D, double* U, const double* Q, void* stream) {
+  VES3D_ARG(T && S && D && U && Q, "null pointer");
+  VES3D_ARG(src_m >= 0 && trg_m >= 0 && n >= 0, "negative size");
+  VES3D_ARG(t_head >= 0 && t_tail <= trg_m && t_head <= t_tail, "target range outside [0, trg_m]");
+  return launch_direct_stokes_f64(src_m, trg_m, n, t_head, t_tail, T, S, D, U, Q, (cudaStream_t)stream);
+}
+
+int ves3d_stokes_alltoall_device_f64(const double* src, const double* den, size_t np, double* pot, void* stream) {
+  VES3D_ARG(src && den && pot, "null pointer");
+  return launch_alltoall_f64(src, den, (long)np, pot, (cudaStream_t)stream);
+}
+
+struct InteractionWorkspace {
+  double* buf = nullptr;
+  size_t cap = 0;
+  cudaStream_t st = nullptr;
+};
+
+void ves3d_stokes_alltoall_f64(const double* src, const double* den, size_t np, double* pot, void** ctx) {
+  auto fail = [&](void) {
+    for (size_t i = 0; i < 3 * np; i++) pot[i] = __builtin_nan("");
+  };
+  if (!src || !den || !pot) {
+    set_error("invalid argument: null pointer");
+    if (pot) fail();
+    return;
+  }
+  InteractionWorkspace local;
+  InteractionWorkspace* ws = &local;
+  if (ctx) {
+    if (!*ctx) *ctx = new InteractionWorkspace();
+    ws = (InteractionWorkspace*)*ctx;
+  }
+  const size_t need = 9 * np;
+  if (ws->cap < need) {
+    if (ws->buf) cudaFree(ws->buf);
+    ws->buf = nullptr;
+    ws->cap = 0;
+    if (cudaMalloc((void**)&ws->buf, need * sizeof(double)) != cudaSuccess) {
+      set_error("cudaMalloc of %zu bytes failed", need * sizeof(double));
+      fail();
+      return;
+    }
+    ws->cap = need;
+  }
+  if (!ws->st && cudaStreamCreateWithFlags(&ws->st, cudaStreamNonBlocking) != cudaSuccess) {
+    set_error("cudaStreamCreate failed");
+    fail();
+    return;
+  }
+  double *dsrc = ws->buf, *dden = ws->buf + 3 * np, *dpot = ws->buf + 6 * np;
+  int s = VES3D_OK;
+  if (cudaMemcpyAsync(dsrc, src, 3 * np * sizeof(double), cudaMemcpyHostToDevice, ws->st) != cudaSuccess ||
+      cudaMemcpyAsync(dden, den, 3 * np * sizeof(double), cudaMemcpyHostToDevice, ws->st) != cudaSuccess)
+    s = VES3D_ERR_CUDA;
+  if (!s) s = launch_alltoall_f64(dsrc, dden, (long)np, dpot, ws->st);
+  if (!s && cudaMemcpyAsync(pot, dpot, 3 * np * sizeof(double), cudaMemcpyDeviceToHost, ws->st) != cudaSuccess)
+    s = VES3D_ERR_CUDA;
+  if (cudaStreamSynchronize(ws->st) != cudaSuccess) s = VES3D_ERR_CUDA;
+  if (s) {
+    if (!g_err[0]) set_error("all-to-all interaction failed");
+    fail();
+  }
+  if (!ctx) {
+    cudaFree(ws->buf);
+    cudaStreamDestroy(ws->st);
+  }
+}
+
+void ves3d_interaction_free(void** ctx) {
+  if (!ctx || !*ctx) return;
+  InteractionWorkspace* ws = (InteractionWorkspace*)*ctx;
+  if (ws->buf) cudaFree(ws->buf);
+  if (ws->st) cudaStreamDestroy(ws->st);
+  delete ws;
+  *ctx = nullptr;
+}
+
+}  // extern "C"

@@ -1,0 +1,136 @@
+"""Host-side mirror of the reference's StokesVelocity operator contract
+(include/StokesVelocity.h:16-44, src/StokesVelocity.cc:11-539), backed by the CUDA
+library through its C ABI.
+
+    sv = StokesVelocity(sh_order, sh_order_up)          # StokesVelocity(p, p_up)
+    sv.SetSrcCoord(S)                                    # AxisMajor [n_ves][3][(p+1)2p]
+    sv.SetDensitySL(f)                                   # same layout
+    vel = sv()                                           # operator()()
+
+Arrays are numpy float64 (host) or torch float64 CUDA tensors (device, passed by
+pointer without a copy). Errors raise Ves3dError with the library's message.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib
+
+
+def _ptr(a):
+    """(pointer, is_device, n_elems) of a contiguous float64 numpy array or CUDA tensor."""
+    if isinstance(a, np.ndarray):
+        if a.dtype != np.float64 or not a.flags.c_contiguous:
+            raise ValueError("expected a C-contiguous float64 array")
+        return a.ctypes.data, 0, a.size
+    try:
+        import torch
+    except ImportError:  # pragma: no cover
+        torch = None
+    if torch is not None and isinstance(a, torch.Tensor):
+        if a.dtype != torch.float64 or not a.is_contiguous():
+            raise ValueError("expected a contiguous float64 tensor")
+        return a.data_ptr(), 1 if a.is_cuda else 0, a.numel()
+    raise TypeError(f"unsupported array type {type(a)}")
+
+
+def ngrid(p):
+    return 2 * p * (p + 1)
+
+
+def ncoef(p):
+    return p * (p + 2)
+
+
+class StokesVelocity:
+    """Single-layer Stokes velocity of a suspension of vesicles at their own surface points."""
+
+    def __init__(self, sh_order, sh_order_up=-1, precision="fp64", device=-1):
+        prec = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}[precision]
+        h = ctypes.c_void_p()
+        check(lib().ves3d_sv_create(int(sh_order), int(sh_order_up), prec, int(device), ctypes.byref(h)),
+              "StokesVelocity")
+        self._h = h
+        self.sh_order = int(sh_order)
+        self.sh_order_up = int(sh_order_up) if sh_order_up > 0 else 2 * int(sh_order)
+        self.n_ves = 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ves3d_sv_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # --- reference API names -------------------------------------------------
+    def SetSrcCoord(self, S, sh_order_up_self=-1, sh_order_up=-1):
+        if (sh_order_up_self > 0 and sh_order_up_self != self.sh_order_up) or \
+                (sh_order_up > 0 and sh_order_up != self.sh_order_up):
+            raise ValueError("changing the upsample order needs a new operator")
+        p, dev, n = _ptr(S)
+        ng = ngrid(self.sh_order)
+        if n % (3 * ng):
+            raise ValueError(f"surface size {n} is not a multiple of 3*{ng}")
+        self.n_ves = n // (3 * ng)
+        check(lib().ves3d_sv_set_src_coord(self._h, p, self.n_ves, dev), "SetSrcCoord")
+
+    def SetDensitySL(self, f, add_repul=False):
+        if add_repul:
+            raise NotImplementedError("repulsion needs the near-singular module, which is not on this path")
+        p, dev, n = _ptr(f)
+        if n != self.n_ves * 3 * ngrid(self.sh_order):
+            raise ValueError("density size does not match the surfaces")
+        check(lib().ves3d_sv_set_density_sl(self._h, p, dev), "SetDensitySL")
+
+    def __call__(self, out=None):
+        if out is None:
+            out = np.empty(self.n_ves * 3 * ngrid(self.sh_order))
+        p, dev, n = _ptr(out)
+        if n != self.n_ves * 3 * ngrid(self.sh_order):
+            raise ValueError("output size does not match the surfaces")
+        check(lib().ves3d_sv_eval(self._h, p, dev), "StokesVelocity()")
+        return out
+
+    # --- extras ----------------------------------------------------------------
+    def setup(self):
+        check(lib().ves3d_sv_setup(self._h), "setup")
+
+    def self_matrix(self):
+        n = 3 * ncoef(self.sh_order)
+        out = np.empty((self.n_ves, n, n))
+        check(lib().ves3d_sv_get_self_matrix(self._h, out.ctypes.data, 0), "self_matrix")
+        return out
+
+    def parts(self):
+        n = self.n_ves * 3 * ngrid(self.sh_order)
+        a, b = np.empty(n), np.empty(n)
+        check(lib().ves3d_sv_get_parts(self._h, a.ctypes.data, b.ctypes.data, 0), "parts")
+        return a, b
+
+    def stage_times(self):
+        ms = (ctypes.c_float * 4)()
+        check(lib().ves3d_sv_stage_times(self._h, ms), "stage_times")
+        return {"setup_ms": ms[0], "self_apply_ms": ms[1], "far_ms": ms[2], "eval_ms": ms[3]}
+
+    def device_buffer(self, which):
+        ptr = ctypes.c_void_p()
+        n = ctypes.c_size_t()
+        check(lib().ves3d_sv_device_buffer(self._h, int(which), ctypes.byref(ptr), ctypes.byref(n)), "device_buffer")
+        return ptr.value, n.value
+
+    def eval_resident(self):
+        check(lib().ves3d_sv_eval_resident(self._h), "eval_resident")
+
+    def set_stream(self, stream_ptr):
+        check(lib().ves3d_sv_set_stream(self._h, stream_ptr), "set_stream")
