@@ -1,0 +1,429 @@
+"""Benchmark: vesicle-point velocity evaluations per second of the Ves3D StokesVelocity
+path (single layer, surface targets) on the 512-vesicle p=16 suspension
+(278,528 points), one full evaluation per step:
+    SetSrcCoord(X) -> self-matrix build (singular quadrature)
+    SetDensitySL(f) -> self apply + exact all-pairs far field -> velocity.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+                    [--impl ours|reference]
+
+Prints one JSON line (rank 0). With N > 1 (torchrun) every rank evaluates its own
+independent suspension (weak scaling, no data-path collective); the time is the max
+over ranks. `--impl reference` times the reference's own CPU code (oracle/_ref, built
+from the reference sources) on a bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "c2_512ves_p16"
+FLOPS_PER_PAIR = 28  # the reference's own count for the Stokeslet pair (src/CPUKernels.cc:1007)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    return ap.parse_args()
+
+
+def dist_setup():
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 8:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[4 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def far_pairs(nves, ng):
+    n = nves * ng
+    return n * n - nves * ng * ng
+
+
+def load_traffic(kernel_key):
+    """dram read+write bytes per launch recorded from an ncu capture (profiles/traffic.json)."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as fh:
+            return json.load(fh).get(kernel_key)
+    except (OSError, ValueError):
+        return None
+
+
+# --------------------------------------------------------------------------------------
+# CPU baseline: the reference's own code (oracle/_ref) on a bounded sample of the workload
+# --------------------------------------------------------------------------------------
+def cpu_reference_rate(X, f, p, budget_s=20.0):
+    """Points/s of one full StokesVelocity evaluation by the reference's CPU code,
+    extrapolated from a bounded sample: the self part on a subset of vesicles and the
+    all-pairs far field on a subset of targets (linear in each)."""
+    from oracle import reflib
+    ng = 2 * p * (p + 1)
+    nves = X.size // (3 * ng)
+    N = nves * ng
+    cores = os.cpu_count() or 1
+    kind = "reference" if reflib.available() else "port"
+    if kind == "reference":
+        reflib.set_threads(cores)
+    else:
+        from oracle import sh, stokes  # noqa: F401
+    Xv = X.reshape(nves, 3 * ng)
+    fv = f.reshape(nves, 3 * ng)
+    # self part: build + apply on ns vesicles (>= one per thread)
+    ns = min(nves, max(4 * cores, 16))
+    Xs = np.ascontiguousarray(Xv[:ns].reshape(-1))
+    fs = np.ascontiguousarray(fv[:ns].reshape(-1))
+    t0 = time.perf_counter()
+    if kind == "reference":
+        SL, _ = reflib.singular_matrices(Xs, p, 2 * p)
+        t1 = time.perf_counter()
+        reflib.self_apply(SL, fs, p)
+    else:
+        from oracle import sh
+        SL = sh.stokes_singular_matrix(Xs, p, 2 * p)
+        t1 = time.perf_counter()
+        sh.self_apply(SL, fs, p)
+    t2 = time.perf_counter()
+    t_build = (t1 - t0) * nves / ns
+    t_apply = (t2 - t1) * nves / ns
+    # far part: the all-pairs Stokeslet sum for a sample of targets against all N sources
+    # (DirectStokesKernel's pair arithmetic, one "surface" per thread so that the
+    # reference's OpenMP loop over surfaces uses every core), plus the same-vesicle
+    # subtraction, which is 1/nves of the all-pairs work.
+    rng = np.random.default_rng(7)
+    pos = X.reshape(nves, 3, ng).transpose(1, 0, 2).reshape(3, N)
+    den = f.reshape(nves, 3, ng).transpose(1, 0, 2).reshape(3, N)
+    per_thread = 64
+    t_far = None
+    while True:
+        nt = per_thread * cores
+        idx = rng.choice(N, size=nt, replace=False)
+        trg = pos[:, idx]
+        if kind == "reference":
+            src_rep = np.ascontiguousarray(np.broadcast_to(pos[None], (cores, 3, N)).reshape(-1))
+            den_rep = np.ascontiguousarray(np.broadcast_to(den[None], (cores, 3, N)).reshape(-1))
+            trg_rep = np.ascontiguousarray(trg.reshape(3, cores, per_thread).transpose(1, 0, 2).reshape(-1))
+            qw = np.ones(N)
+            t3 = time.perf_counter()
+            reflib.direct_stokes(N, per_thread, cores, 0, per_thread, qw, trg_rep, src_rep, den_rep)
+            t4 = time.perf_counter()
+        else:
+            from oracle import stokes
+            t3 = time.perf_counter()
+            stokes.far(X, f, np.arange(nves + 1) * ng, idx)
+            t4 = time.perf_counter()
+        t_far = (t4 - t3) * N / nt * (1.0 + 1.0 / nves)
+        if (t4 - t3) > 6.0 or per_thread >= 16384:
+            break
+        per_thread = int(per_thread * min(16.0, max(2.0, 8.0 / max(t4 - t3, 1e-3))))
+    total = t_build + t_apply + t_far
+    sample = (f"self part on {ns} of {nves} vesicles (build {t1 - t0:.2f}s, apply {t2 - t1:.3f}s), all-pairs far "
+              f"field on {nt} of {N} targets ({t4 - t3:.2f}s); each extrapolated linearly to the full evaluation")
+    return {"value": N / total, "unit": "points/s", "cores": cores, "kind": kind, "sample": sample,
+            "seconds_per_eval": total, "parts_s": {"self_build": t_build, "self_apply": t_apply, "far": t_far}}
+
+
+def run_reference(args, world, rank):
+    from ves3d_b200 import workloads
+    if rank != 0:
+        return
+    X, f, p = workloads.make(args.workload)
+    ng = 2 * p * (p + 1)
+    N = X.size // 3
+    vals = []
+    res = None
+    for i in range(args.warmup + args.steps):
+        res = cpu_reference_rate(X, f, p)
+        if i >= args.warmup:
+            vals.append(res["value"])
+    value = statistics.median(vals) if vals else res["value"]
+    line = {
+        "impl": "reference", "metric": "vesicle-point velocity evaluations/s", "value": value, "unit": "points/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * N / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.workload}: {N // ng} vesicles p={p} ({N} points), full StokesVelocity "
+                               f"evaluation (self-matrix build + self apply + all-pairs far field)",
+                   "precision": "fp64", "seed": workloads.CONFIGS[args.workload]["seed"]},
+        "cpu_baseline": {"value": value, "unit": "points/s", "cores": res["cores"], "kind": res["kind"],
+                         "sample": res["sample"]},
+        "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "parts_s": res["parts_s"],
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------------------
+# our arm
+# --------------------------------------------------------------------------------------
+def sampled_error_vs_oracle(X, f, p, vel, nves_check=2, n_targets=256, seed=11):
+    """Max relative error of vel against the FP64 oracle on a sample: the full velocity
+    (self + far) at points of nves_check vesicles, far part at those points only."""
+    from oracle import sh, stokes
+    ng = 2 * p * (p + 1)
+    nves = X.size // (3 * ng)
+    rng = np.random.default_rng(seed)
+    vs = rng.choice(nves, size=min(nves_check, nves), replace=False)
+    Xv = X.reshape(nves, 3 * ng)
+    fv = f.reshape(nves, 3 * ng)
+    worst = 0.0
+    scale = np.abs(vel).max()
+    for v in vs:
+        SL = sh.stokes_singular_matrix(Xv[v], p, 2 * p)
+        self_v = sh.self_apply(SL, fv[v], p).reshape(3, ng)
+        k = rng.choice(ng, size=min(n_targets // len(vs), ng), replace=False)
+        idx = v * ng + k
+        far = stokes.far(X, stokes.far_density(X, f, p), np.arange(nves + 1) * ng, idx)
+        ref = self_v[:, k].T + far
+        got = vel.reshape(nves, 3, ng)[v][:, k].T
+        worst = max(worst, float(np.abs(got - ref).max() / scale))
+    return worst
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    from ves3d_b200 import _lib, workloads
+    from ves3d_b200.stokes_velocity import StokesVelocity
+
+    cfg = dict(workloads.CONFIGS[args.workload])
+    cfg["seed"] = cfg["seed"] + 100 * rank  # every rank owns an independent suspension
+    p = cfg["p"]
+    X, f = workloads.suspension(**cfg)
+    ng = 2 * p * (p + 1)
+    nves = X.size // (3 * ng)
+    N = nves * ng
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    sv = StokesVelocity(p, 2 * p, precision=args.precision, device=local)
+    sv.set_stream(stream.cuda_stream)
+    dX = torch.from_numpy(X).to(dev)
+    dF = torch.from_numpy(f).to(dev)
+    out = torch.empty_like(dX)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
+
+    def step():
+        sv.SetSrcCoord(dX)
+        sv.SetDensitySL(dF)
+        sv(out)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    peak64 = _lib.measure_fma_peak(True)
+    peak32 = _lib.measure_fma_peak(False)
+    times, setup_ms, far_ms, apply_ms = [], [], [], []
+    launches0 = _lib.kernel_launches()
+    flush_launches = 0
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            flush_launches += 0  # torch's fill kernel is not ours
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+            st = sv.stage_times()
+            setup_ms.append(st["setup_ms"])
+            far_ms.append(st["far_ms"])
+            apply_ms.append(st["self_apply_ms"])
+    torch.cuda.synchronize()
+    barrier(world)
+    launches = _lib.kernel_launches() - launches0
+    total_ms = sum(times)
+    total_ms_max = max_over_ranks(total_ms, world)
+    ms_per_step = total_ms_max / args.steps
+    value = N * world * args.steps / (total_ms_max * 1e-3)
+
+    # end to end through the public API with pinned host buffers: H2D of X and f,
+    # evaluation, D2H of the velocity, every step
+    hX = torch.from_numpy(X).pin_memory().numpy()
+    hF = torch.from_numpy(f).pin_memory().numpy()
+    hV = torch.empty(X.size, dtype=torch.float64).pin_memory().numpy()
+    e2e_ms = []
+    for _ in range(args.e2e_steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sv.SetSrcCoord(hX)
+        sv.SetDensitySL(hF)
+        sv(hV)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms.append(e0.elapsed_time(e1))
+    e2e_max = max_over_ranks(sum(e2e_ms), world) if e2e_ms else None
+    e2e_value = N * world * len(e2e_ms) / (e2e_max * 1e-3) if e2e_ms else None
+
+    result = None
+    if rank == 0:
+        far_avg_ms = statistics.mean(far_ms)
+        pairs = far_pairs(nves, ng)
+        achieved = FLOPS_PER_PAIR * pairs / (far_avg_ms * 1e-3) / 1e12
+        peak = peak64 if args.precision == "fp64" else peak32
+        if not e2e_ms:
+            sv(hV)
+        err = sampled_error_vs_oracle(X, f, p, hV)
+        clocks = clk.summary()
+        result = {
+            "metric": "vesicle-point velocity evaluations/s",
+            "value": value,
+            "unit": "points/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_per_step,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "data": "synthetic",
+            "config": {
+                "workload": f"{args.workload}: {nves} vesicles p={p} ({N} points), full StokesVelocity evaluation "
+                            f"(self-matrix build + self apply + all-pairs far field) per step",
+                "precision": args.precision,
+                "sh_order_up": 2 * p,
+                "l2": "flushed between steps (256 MB write, untimed)",
+                "seed": cfg["seed"],
+            },
+            "e2e": {"value": e2e_value, "unit": "points/s", "h2d_bytes_per_step": int(2 * X.nbytes),
+                    "d2h_bytes_per_step": int(X.nbytes)},
+            "gpu_launches": int(launches),
+            "stages_ms": {"self_build": statistics.mean(setup_ms), "self_apply": statistics.mean(apply_ms),
+                          "far_field": far_avg_ms},
+            "roofline": {
+                "kernel": "k_far_f64" if args.precision == "fp64" else "k_far_f32",
+                "bound": "fp64_pipe" if args.precision == "fp64" else "fp32_pipe",
+                "achieved": achieved,
+                "peak": peak,
+                "unit": "TFLOP/s",
+                "frac": achieved / peak,
+                "peak_source": "measured on this GPU by ves3d_measure_fma_peak (FMA throughput probe)",
+                "work": f"{FLOPS_PER_PAIR} flops per (target, source) pair x {pairs} pairs per launch",
+                "traffic": load_traffic(f"far_{args.precision}_{args.workload}"),
+            },
+            "error_vs_fp64_oracle": {"max_rel": err, "sample": "2 vesicles: full velocity at 256 of their points"},
+            "clocks": clocks,
+            "peaks_tflops": {"fp64_fma": peak64, "fp32_fma": peak32},
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            cb = cpu_reference_rate(X, f, p)
+            result["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        print(json.dumps(result), flush=True)
+    sv.close()
+    return result
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        run_reference(args, world, rank)
+        return
+    world, rank, local = dist_setup()
+    try:
+        run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -80,7 +80,8 @@ int ves3d_sv_get_self_matrix(ves3d_sv* sv, double* SL, int is_device);
  * each AxisMajor like vel. Either pointer may be NULL. */
 int ves3d_sv_get_parts(ves3d_sv* sv, double* vel_self, double* vel_far, int is_device);
 /* Device time in ms of the last setup / eval stages:
- * ms[0] self-matrix build, ms[1] self apply, ms[2] far field, ms[3] whole eval. */
+ * ms[0] self-matrix build, ms[1] self apply, ms[2] far-field kernel, ms[3] whole eval
+ * (everything after the build). */
 int ves3d_sv_stage_times(ves3d_sv* sv, float* ms);
 /* Device pointers of the context's resident buffers (for zero-copy callers):
  * which = 0 surfaces, 1 density, 2 velocity. Valid until the next set_src_coord. */
@@ -131,6 +132,9 @@ int ves3d_stokes_alltoall_device_f64(const double* src, const double* den, size_
  * "ana_four", "syn1_leg", "syn1_dleg", "syn1_four", "syn1_dfour", "qp".
  * ------------------------------------------------------------------------- */
 int ves3d_tables_export(int p0, int p1, const char* name, double* out, size_t cap, size_t* n);
+/* Measured FMA throughput of the current device's CUDA cores in TFLOP/s (2 flops per
+ * FMA): fp64 != 0 for FP64, else FP32. The roofline denominator of the direct sums. */
+int ves3d_measure_fma_peak(int fp64, double* tflops);
 
 #ifdef __cplusplus
 }

@@ -45,6 +45,7 @@ SIGNATURES = [
     ("ves3d_interaction_free", None, [ctypes.POINTER(_vp)]),
     ("ves3d_stokes_alltoall_device_f64", _i, [_vp, _vp, _sz, _vp, _vp]),
     ("ves3d_tables_export", _i, [_i, _i, ctypes.c_char_p, _vp, _sz, ctypes.POINTER(_sz)]),
+    ("ves3d_measure_fma_peak", _i, [_i, ctypes.POINTER(_d)]),
 ]
 
 
@@ -77,6 +78,12 @@ def check(status, what=""):
 
 def kernel_launches():
     return int(lib().ves3d_kernel_launches())
+
+
+def measure_fma_peak(fp64=True):
+    t = _d(0)
+    check(lib().ves3d_measure_fma_peak(1 if fp64 else 0, ctypes.byref(t)), "measure_fma_peak")
+    return t.value
 
 
 def tables_export(p0, p1, name):

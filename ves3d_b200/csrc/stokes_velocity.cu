@@ -11,6 +11,7 @@
 //                  (src/StokesVelocity.cc:385-473); den = f * area * qw;
 //                  vel = Vself + sum over other vesicles (exact all-pairs far field).
 #include <cstdarg>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -119,7 +120,7 @@ struct ves3d_sv {
   long chunk = 0;
   double *R = nullptr, *Xu = nullptr, *Xut = nullptr, *Xup = nullptr, *K = nullptr, *C = nullptr, *SL3 = nullptr;
   bool have_src = false, have_den = false, sl_valid = false, parts_valid = false;
-  cudaEvent_t ev[6] = {};
+  cudaEvent_t ev[8] = {};
   float ms[4] = {0, 0, 0, 0};
 
   ~ves3d_sv() {
@@ -198,7 +199,13 @@ int alloc_scratch(ves3d_sv* sv) {
   size_t per = scratch_per_vesicle(sv->p, sv->pup) * sizeof(double);
   size_t free_b = 0, total_b = 0;
   VES3D_CK(cudaMemGetInfo(&free_b, &total_b));
+  // Scratch budget for one chunk of the self-matrix build: 8 GiB by default, capped at a
+  // third of free memory; VES3D_SCRATCH_MB overrides (e.g. to keep profiler captures small).
   size_t budget = (size_t)8 << 30;
+  if (const char* env = getenv("VES3D_SCRATCH_MB")) {
+    long mb = atol(env);
+    if (mb > 0) budget = (size_t)mb << 20;
+  }
   if (budget > free_b / 3) budget = free_b / 3;
   long chunk = (long)(budget / per);
   if (chunk < 1) chunk = 1;
@@ -284,13 +291,16 @@ int run_eval(ves3d_sv* sv) {
     return s;
   VES3D_CK(cudaEventRecord(sv->ev[3], st));
   if ((s = launch_far_density(sv->F, sv->area, sv->nves, p0, T.smooth_w0, sv->den, st))) return s;
-  if ((s = launch_far_f64(sv->pos, sv->den, sv->nves, ngrid_(p0), nullptr, sv->Vfar, st))) return s;
-  if ((s = launch_add(sv->Vself, sv->Vfar, (long)sv->nves * 3 * ngrid_(p0), sv->V, st))) return s;
+  // events bracket the far-field kernel alone: its duration is the roofline denominator
   VES3D_CK(cudaEventRecord(sv->ev[4], st));
-  VES3D_CK(cudaEventSynchronize(sv->ev[4]));
+  if ((s = launch_far_f64(sv->pos, sv->den, sv->nves, ngrid_(p0), nullptr, sv->Vfar, st))) return s;
+  VES3D_CK(cudaEventRecord(sv->ev[5], st));
+  if ((s = launch_add(sv->Vself, sv->Vfar, (long)sv->nves * 3 * ngrid_(p0), sv->V, st))) return s;
+  VES3D_CK(cudaEventRecord(sv->ev[6], st));
+  VES3D_CK(cudaEventSynchronize(sv->ev[6]));
   VES3D_CK(cudaEventElapsedTime(&sv->ms[1], sv->ev[2], sv->ev[3]));
-  VES3D_CK(cudaEventElapsedTime(&sv->ms[2], sv->ev[3], sv->ev[4]));
-  VES3D_CK(cudaEventElapsedTime(&sv->ms[3], sv->ev[2], sv->ev[4]));
+  VES3D_CK(cudaEventElapsedTime(&sv->ms[2], sv->ev[4], sv->ev[5]));
+  VES3D_CK(cudaEventElapsedTime(&sv->ms[3], sv->ev[2], sv->ev[6]));
   sv->parts_valid = true;
   return VES3D_OK;
 }

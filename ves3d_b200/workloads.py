@@ -95,6 +95,9 @@ CONFIGS = {
     # 512 vesicles, p=16, unit spheres + deg<=6 amp 0.1, jittered 8x8x8 lattice spacing 2.5, min sep 0.2.
     "c2_512ves_p16": dict(nves_side=8, p=16, spacing=2.5, semi_axes=(1.0, 1.0, 1.0), deg=6, amp=0.1, jitter=0.15,
                           min_sep=0.2, seed=1001),
+    # 64-vesicle cut of the above (4x4x4 lattice): the small case for profiler captures.
+    "c2s_64ves_p16": dict(nves_side=4, p=16, spacing=2.5, semi_axes=(1.0, 1.0, 1.0), deg=6, amp=0.1, jitter=0.15,
+                          min_sep=0.2, seed=1001),
 }
 
 
