@@ -125,6 +125,21 @@ void ves3d_interaction_free(void** ctx);
 int ves3d_stokes_alltoall_device_f64(const double* src, const double* den, size_t np, double* pot,
                                      void* stream);
 
+/* All-to-all interaction that allocates nothing (no counterpart in the reference: it is
+ * an addition of this library). For callers that cannot call cudaMalloc -- code running
+ * while a stream is captured into a CUDA graph, or programs whose device memory is owned
+ * by another allocator. Same HOST-pointer arguments and result as
+ * ves3d_stokes_alltoall_f64, plus an optional stream (NULL = legacy default stream);
+ * returns an int status and waits for its copies before returning. Inputs are staged
+ * through one fixed device array of VES3D_NOALLOC_MAX_POINTS points (36 MiB, held by
+ * every GPU that loads the library until exit); np above that is rejected with
+ * VES3D_ERR_ARG. The first call on a device looks the array's address up
+ * (cudaGetSymbolAddress) and should come before any stream capture. Calls share the
+ * array: calls whose GPU work overlaps race. */
+#define VES3D_NOALLOC_MAX_POINTS 524288
+int ves3d_stokes_alltoall_noalloc_f64(const double* src, const double* den, size_t np, double* pot,
+                                      void* stream);
+
 /* ---------------------------------------------------------------------------
  * Diagnostics (host only, no GPU needed): copy one of the FP64 operator tables the
  * library builds for (p0, p1) into out (capacity cap doubles); *n receives its length.

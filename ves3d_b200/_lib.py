@@ -46,6 +46,7 @@ SIGNATURES = [
     ("ves3d_stokes_alltoall_device_f64", _i, [_vp, _vp, _sz, _vp, _vp]),
     ("ves3d_tables_export", _i, [_i, _i, ctypes.c_char_p, _vp, _sz, ctypes.POINTER(_sz)]),
     ("ves3d_measure_fma_peak", _i, [_i, ctypes.POINTER(_d)]),
+    ("ves3d_stokes_alltoall_noalloc_f64", _i, [_vp, _vp, _sz, _vp, _vp]),
 ]
 
 
