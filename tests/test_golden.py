@@ -1,0 +1,58 @@
+"""The oracle against golden fixtures produced by the reference's own code
+(tests/golden/make_golden.py). Runs without the reference tree. CPU only."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import sh, stokes
+from tests.helpers import rel_err
+
+HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+REF_SELF_NOISE = 5e-9   # the reference's own self-part reproducibility (see test_oracle_pin)
+FAR_TOL = 1e-13
+PRIM_TOL = 1e-13
+
+
+@pytest.fixture(scope="module")
+def g6():
+    return dict(np.load(os.path.join(HERE, "ref_p6_two_ellipsoids.npz")))
+
+
+@pytest.fixture(scope="module")
+def gc1():
+    return dict(np.load(os.path.join(HERE, "ref_c1_8ves_p12.npz")))
+
+
+def test_golden_rules_and_transforms(g6):
+    p = int(g6["p"])
+    assert rel_err(sh.legendre_nodes(p), g6["nodes"]) < PRIM_TOL
+    assert rel_err(sh.legendre_weights(p), g6["weights"]) < PRIM_TOL
+    assert rel_err(sh.singular_weights(2 * p), g6["sing_weights"]) < PRIM_TOL
+    S = sh.grid2shc(g6["X"], p, p)
+    assert rel_err(S, g6["shc"]) < PRIM_TOL
+    for a, b in zip(sh.shc2grid(S, p, 2 * p, grads=True), (g6["up"], g6["up_theta"], g6["up_phi"])):
+        assert rel_err(a, b) < PRIM_TOL
+
+
+def test_golden_self_and_far(g6):
+    p = int(g6["p"])
+    SL = sh.stokes_singular_matrix(g6["X"], p, 2 * p)
+    n = 3 * p * (p + 2)
+    assert rel_err(SL[0].reshape(-1), g6["SL0"]) < REF_SELF_NOISE
+    assert rel_err(sh.self_apply(SL, g6["f"], p), g6["vel_self"]) < REF_SELF_NOISE
+    assert rel_err(stokes.far_velocity(g6["X"], g6["f"], p), g6["vel_far"]) < FAR_TOL
+    assert n == SL.shape[1]
+
+
+def test_golden_c1(gc1):
+    p = int(gc1["p"])
+    assert rel_err(stokes.far_velocity(gc1["X"], gc1["f"], p), gc1["vel_far"]) < FAR_TOL
+    assert rel_err(stokes.stokes_velocity_sl(gc1["X"], gc1["f"], p), gc1["vel"]) < REF_SELF_NOISE
+
+
+def test_golden_inputs_match_generator(gc1):
+    """The committed C1 inputs are the seeded workload (the generator did not drift)."""
+    from ves3d_b200 import workloads
+    X, f, p = workloads.make("c1_8ves_p12")
+    assert np.array_equal(X, gc1["X"]) and np.array_equal(f, gc1["f"])

@@ -175,3 +175,18 @@ def test_state_errors():
         sv.SetSrcCoord(X)
         with pytest.raises(_lib.Ves3dError, match="ERR_STATE"):
             sv()
+
+
+def test_c1_vs_reference_golden():
+    """GPU FP64 against the reference's own output (tests/golden): far part to 1e-13,
+    full velocity within the reference's self-part noise floor."""
+    import os
+    g = dict(np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_c1_8ves_p12.npz")))
+    p = int(g["p"])
+    with StokesVelocity(p) as sv:
+        sv.SetSrcCoord(g["X"])
+        sv.SetDensitySL(g["f"])
+        vel = sv()
+        _, far = sv.parts()
+    assert rel_err(far, g["vel_far"]) < 1e-13
+    assert rel_err(vel, g["vel"]) < 5e-9
