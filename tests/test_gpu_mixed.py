@@ -1,0 +1,67 @@
+"""Mixed-precision form (packed-FP32 far field with FP64 accumulation) against the FP64
+oracle; tolerance 1e-6 relative, max-norm (the accuracy target of the mixed form)."""
+import numpy as np
+import pytest
+
+from oracle import sh, stokes
+from tests.helpers import rel_err, small_suspension
+from ves3d_b200.stokes_velocity import StokesVelocity
+
+pytestmark = pytest.mark.gpu
+MIXED_TOL = 1e-6
+
+
+@pytest.mark.parametrize("nside,p,seed", [(2, 6, 21), (2, 12, 22)])
+def test_mixed_vs_oracle(nside, p, seed):
+    X, f = small_suspension(nside, p, seed)
+    with StokesVelocity(p, precision="mixed") as sv:
+        sv.SetSrcCoord(X)
+        sv.SetDensitySL(f)
+        vel = sv()
+        _, far = sv.parts()
+    ref_far = stokes.far_velocity(X, f, p)
+    ref = sh.self_apply(sh.stokes_singular_matrix(X, p, 2 * p), f, p) + ref_far
+    assert rel_err(far, ref_far) < MIXED_TOL
+    assert rel_err(vel, ref) < MIXED_TOL
+
+
+def test_mixed_vs_fp64_full_c2():
+    """Full 512-vesicle p=16 suspension: mixed against the FP64 GPU path (itself checked
+    against the oracle to 1e-12), far part and total."""
+    from ves3d_b200 import workloads
+    X, f, p = workloads.make("c2_512ves_p16")
+    out = {}
+    for prec in ("fp64", "mixed"):
+        with StokesVelocity(p, precision=prec) as sv:
+            sv.SetSrcCoord(X)
+            sv.SetDensitySL(f)
+            v = sv()
+            out[prec] = (v, sv.parts()[1])
+    assert rel_err(out["mixed"][1], out["fp64"][1]) < MIXED_TOL
+    assert rel_err(out["mixed"][0], out["fp64"][0]) < MIXED_TOL
+
+
+def test_far_targets_in_chunks_p24():
+    """p=24 vesicles (1,200 points) run as two target chunks per vesicle."""
+    X, f = small_suspension(1, 24, 23)
+    X2 = np.concatenate([X, X.reshape(3, -1).__add__(np.array([[2.7], [0.2], [0.1]])).reshape(-1)])
+    f2 = np.concatenate([f, -0.5 * f])
+    p = 24
+    ref_far = stokes.far_velocity(X2, f2, p)
+    for prec, tol in (("fp64", 1e-12), ("mixed", MIXED_TOL)):
+        with StokesVelocity(p, precision=prec) as sv:
+            sv.SetSrcCoord(X2)
+            sv.SetDensitySL(f2)
+            sv()
+            _, far = sv.parts()
+        assert rel_err(far, ref_far) < tol, prec
+
+
+def test_mixed_deterministic():
+    X, f = small_suspension(2, 6, 24)
+    with StokesVelocity(6, precision="mixed") as sv:
+        sv.SetSrcCoord(X)
+        sv.SetDensitySL(f)
+        a = sv()
+        b = sv()
+    assert np.array_equal(a, b)

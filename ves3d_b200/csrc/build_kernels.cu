@@ -1,0 +1,264 @@
+// Fused singular-quadrature kernel of the self-matrix build (FP64), one CTA per rotated
+// surface (vesicle v, rotation (t, j)):
+//
+//   R (rotated coefficients, 3 x Nc)
+//     -> Legendre synthesis at the p1 = 2 p0 nodes, values and theta-derivatives
+//     -> DFT synthesis: X, X_theta, X_phi on the upsampled grid          [GEMM, K = 2p0]
+//     -> pole targets and the singular Stokes kernel, 2 poles x 6 components
+//     -> transposed DFT                                                  [GEMM, K = 2p1]
+//     -> transposed Legendre sums, accumulated over latitude groups
+//     -> C (2 x 6 x Nc): the kernel contracted back to order-p0 coefficients.
+//
+// This is SHC2Grid(p0 -> p1, grads) + the kernel loop + SHC2GridTranspose(p1 -> p0) of
+// SphericalHarmonics<Real>::StokesSingularInteg_ (src/SphericalHarmonics.cc:963-1082)
+// with every intermediate in shared memory (the unfused form writes 150 KB of upsampled
+// surface and 200 KB of kernel values per rotation to HBM and reads them back).
+//
+// Both DFT GEMMs run on the FP64 tensor cores with mma.sync m8n8k4 (sm_100 has no FP64
+// kind in tcgen05). Fragment layout (PTX ISA, m8n8k4 .f64): A: a0 = A[lane/4][lane%4];
+// B: b0 = B[lane%4][lane/4]; C: {c0, c1} = C[lane/4][2(lane%4) + {0, 1}]. Shared-memory
+// row strides are padded to 4 mod 16 doubles so those loads are bank-conflict free.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace ves3d {
+
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+// Row stride >= n with stride = 4 (mod 16) doubles.
+__host__ __device__ constexpr int pad16_4(int n) { return ((n + 11) / 16) * 16 + 4; }
+
+template <int P0>
+struct RingCfg {
+  static constexpr int P1 = 2 * P0;
+  static constexpr int NC = P0 * (P0 + 2);
+  static constexpr int L1 = P1 + 1;           // latitudes of the upsampled grid
+  static constexpr int F0 = 2 * P0;           // Fourier coefficients at order p0
+  static constexpr int N1 = 2 * P1;           // longitudes of the upsampled grid
+  static constexpr int LG = 4;                // latitudes per group
+  static constexpr int NGRP = (L1 + LG - 1) / LG;
+  static constexpr int ROWS1 = ((3 * LG + 7) / 8) * 8;   // (lat, d) rows of a group, m-tile padded
+  static constexpr int LDA = pad16_4(F0);
+  static constexpr int LDM = pad16_4(N1);
+  static constexpr int LDX = pad16_4(N1);
+  static constexpr int LDK = pad16_4(N1);
+  static constexpr int LDC = pad16_4(F0);
+  // Shared memory, with buffers of disjoint lifetimes aliased:
+  //   region Q: A/dA (Legendre synthesis -> G1)  then  K (kernel -> G2)
+  //   region P: X/X_theta/X_phi (G1 -> kernel)   then  C (G2 -> Legendre sums)
+  static constexpr int SZ_A = 2 * ROWS1 * LDA;
+  static constexpr int SZ_K = (LG * 12) * LDK;
+  static constexpr int SZ_X = 3 * ROWS1 * LDX;
+  static constexpr int SZ_C = (LG * 12) * LDC;
+  static constexpr int OFF_R = 0;
+  static constexpr int OFF_MF = OFF_R + 3 * NC;
+  static constexpr int OFF_DMF = OFF_MF + F0 * LDM;
+  static constexpr int OFF_LEG = OFF_DMF + F0 * LDM;       // [LG][NC] slice of the latitude group
+  static constexpr int OFF_DLEG = OFF_LEG + NC * LG;
+  static constexpr int OFF_Q = OFF_DLEG + NC * LG;
+  static constexpr int OFF_P = OFF_Q + (SZ_A > SZ_K ? SZ_A : SZ_K);
+  static constexpr int OFF_TRG = OFF_P + (SZ_X > SZ_C ? SZ_X : SZ_C);
+  static constexpr int TOTAL = OFF_TRG + 8;
+  static constexpr size_t SMEM = (size_t)TOTAL * sizeof(double);
+  static constexpr int NOUT = 12 * NC;
+  static constexpr int OUT_PER_THREAD = (NOUT + 255) / 256;
+};
+
+template <int P0>
+__global__ void __launch_bounds__(256, 2) k_build_ring(const double* __restrict__ R, DevTables T,
+                                                       double* __restrict__ C) {
+  using G = RingCfg<P0>;
+  extern __shared__ __align__(16) double sm[];
+  double* sR = sm + G::OFF_R;
+  double* sMf = sm + G::OFF_MF;
+  double* sdMf = sm + G::OFF_DMF;
+  double* sLeg = sm + G::OFF_LEG;
+  double* sdLeg = sm + G::OFF_DLEG;
+  double* sA = sm + G::OFF_Q;
+  double* sdA = sA + G::ROWS1 * G::LDA;
+  double* sK = sm + G::OFF_Q;
+  double* sX = sm + G::OFF_P;
+  double* sC = sm + G::OFF_P;
+  double* trg = sm + G::OFF_TRG;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const long rot = blockIdx.x;
+
+  // ---- rotated coefficients, DFT tables, pole targets ----------------------------------
+  for (int i = tid; i < 3 * G::NC; i += 256) sR[i] = R[rot * 3 * G::NC + i];
+  for (int i = tid; i < G::F0 * G::N1; i += 256) {
+    const int k = i / G::N1, j = i - k * G::N1;
+    sMf[k * G::LDM + j] = __ldg(T.syn1_four + i);
+    sdMf[k * G::LDM + j] = __ldg(T.syn1_dfour + i);
+  }
+  __syncthreads();
+  if (tid < 6) {
+    const int c = tid >> 1, t = tid & 1;
+    double s = 0.0;
+    for (int n = 0; n <= P0; n++) s += sR[c * G::NC + n] * __ldg(T.qp + t * (P0 + 1) + n);
+    trg[c * 2 + t] = s;
+  }
+  double acc[G::OUT_PER_THREAD];
+#pragma unroll
+  for (int q = 0; q < G::OUT_PER_THREAD; q++) acc[q] = 0.0;
+
+  const int grow = lane >> 2, gcol = lane & 3;
+  for (int g = 0; g < G::NGRP; g++) {
+    const int lat0 = g * G::LG;
+    const int nlat = min(G::LG, G::L1 - lat0);
+    // ---- the group's slice of the Legendre tables -------------------------------------
+    for (int i = tid; i < G::NC * G::LG; i += 256) {
+      const int l = i / G::NC, c = i - l * G::NC;
+      const bool ok = l < nlat;
+      sLeg[i] = ok ? __ldg(T.syn1_leg + c * G::L1 + lat0 + l) : 0.0;
+      sdLeg[i] = ok ? __ldg(T.syn1_dleg + c * G::L1 + lat0 + l) : 0.0;
+    }
+    __syncthreads();
+    // ---- Legendre synthesis of the group's latitudes: A[(l,d)][k], dA -----------------
+    for (int i = tid; i < G::ROWS1 * G::F0; i += 256) {
+      const int k = i % G::F0, row = i / G::F0;
+      double s = 0.0, d = 0.0;
+      if (row < 3 * nlat) {
+        const int l = row / 3, dd = row - 3 * l;
+        const int c0 = __ldg(T.blk_off + k), c1 = __ldg(T.blk_off + k + 1);
+        const double* r = sR + dd * G::NC;
+        for (int c = c0; c < c1; c++) {
+          s = fma(r[c], sLeg[l * G::NC + c], s);
+          d = fma(r[c], sdLeg[l * G::NC + c], d);
+        }
+      }
+      sA[row * G::LDA + k] = s;
+      sdA[row * G::LDA + k] = d;
+    }
+    __syncthreads();
+    // ---- DFT synthesis on tensor cores: X, X_theta (from A), X_phi (from dA) ------------
+    {
+      const int mt_n = (3 * nlat + 7) / 8;
+      const int nitems = mt_n * 3 * (G::N1 / 16);    // (m-tile, variant, pair of n-tiles)
+      for (int it = warp; it < nitems; it += 8) {
+        const int np2 = it % (G::N1 / 16);
+        const int var = (it / (G::N1 / 16)) % 3;
+        const int mt = it / (3 * (G::N1 / 16));
+        const double* Asrc = (var == 2 ? sdA : sA) + (mt * 8 + grow) * G::LDA + gcol;
+        const double* Bsrc = (var == 1 ? sdMf : sMf) + gcol * G::LDM + np2 * 16 + grow;
+        double c00 = 0, c01 = 0, c10 = 0, c11 = 0;
+#pragma unroll
+        for (int ks = 0; ks < G::F0 / 4; ks++) {
+          const double a = Asrc[ks * 4];
+          dmma(c00, c01, a, Bsrc[ks * 4 * G::LDM]);
+          dmma(c10, c11, a, Bsrc[ks * 4 * G::LDM + 8]);
+        }
+        double* out = sX + var * G::ROWS1 * G::LDX + (mt * 8 + grow) * G::LDX + np2 * 16 + 2 * gcol;
+        out[0] = c00;
+        out[1] = c01;
+        out[8] = c10;
+        out[9] = c11;
+      }
+    }
+    __syncthreads();
+    // ---- singular kernel at the group's upsampled points (K aliases A/dA) ---------------
+    for (int pnt = tid; pnt < nlat * G::N1; pnt += 256) {
+      const int l = pnt / G::N1, j = pnt - l * G::N1;
+      const int lat = lat0 + l;
+      const double* x = sX + (l * 3) * G::LDX + j;
+      const double* xt = x + G::ROWS1 * G::LDX;
+      const double* xp = xt + G::ROWS1 * G::LDX;
+      const double px = x[0], py = x[G::LDX], pz = x[2 * G::LDX];
+      const double ax = xt[0], ay = xt[G::LDX], az = xt[2 * G::LDX];
+      const double bx = xp[0], by = xp[G::LDX], bz = xp[2 * G::LDX];
+      const double nx = ay * bz - az * by, ny = az * bx - ax * bz, nz = ax * by - ay * bx;
+      const double area = sqrt(nx * nx + ny * ny + nz * nz);
+#pragma unroll
+      for (int t = 0; t < 2; t++) {
+        const double dx = trg[t] - px, dy = trg[2 + t] - py, dz = trg[4 + t] - pz;
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        double rinv = 1.0 / sqrt(r2);
+        if (r2 <= 2.220446049250313e-16) rinv = 0.0;
+        const double a1 = kInv8Pi * __ldg(T.sing_w + (t ? lat : G::P1 - lat)) * area * rinv;
+        const double a2 = a1 * rinv * rinv;
+        double* k = sK + (l * 12 + t * 6) * G::LDK + j;
+        k[0] = a1 + dx * dx * a2;
+        k[G::LDK] = dx * dy * a2;
+        k[2 * G::LDK] = dx * dz * a2;
+        k[3 * G::LDK] = a1 + dy * dy * a2;
+        k[4 * G::LDK] = dy * dz * a2;
+        k[5 * G::LDK] = a1 + dz * dz * a2;
+      }
+    }
+    __syncthreads();
+    // ---- transposed DFT on tensor cores: Cg[(l,q)][jf] = sum_j K[(l,q)][j] Mf[jf][j] -----
+    {
+      const int mt_n = (12 * nlat + 7) / 8;
+      const int nitems = mt_n * (G::F0 / 8);
+      for (int it = warp; it < nitems; it += 8) {
+        const int nt = it % (G::F0 / 8), mt = it / (G::F0 / 8);
+        const double* Asrc = sK + (mt * 8 + grow) * G::LDK + gcol;
+        const double* Bsrc = sMf + (nt * 8 + grow) * G::LDM + gcol;  // B[j][jf] = Mf[jf][j]
+        double c0 = 0, c1 = 0, d0 = 0, d1 = 0;
+#pragma unroll
+        for (int ks = 0; ks < G::N1 / 4; ks += 2) {
+          dmma(c0, c1, Asrc[ks * 4], Bsrc[ks * 4]);
+          dmma(d0, d1, Asrc[ks * 4 + 4], Bsrc[ks * 4 + 4]);
+        }
+        double* out = sC + (mt * 8 + grow) * G::LDC + nt * 8 + 2 * gcol;
+        out[0] = c0 + d0;
+        out[1] = c1 + d1;
+      }
+    }
+    __syncthreads();
+    // ---- transposed Legendre sums, accumulated in registers -----------------------------
+#pragma unroll
+    for (int q = 0; q < G::OUT_PER_THREAD; q++) {
+      const int o = tid + q * 256;
+      if (o < G::NOUT) {
+        const int comp = o / G::NC, c = o - comp * G::NC;
+        const int jf = __ldg(T.jf_of_coef + c);
+        double s = acc[q];
+        for (int l = 0; l < nlat; l++) s = fma(sC[(l * 12 + comp) * G::LDC + jf], sLeg[l * G::NC + c], s);
+        acc[q] = s;
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < G::OUT_PER_THREAD; q++) {
+    const int o = tid + q * 256;
+    if (o < G::NOUT) C[rot * G::NOUT + o] = acc[q];
+  }
+}
+
+template <int P0>
+static int launch_ring(const double* R, long nrot, const DevTables& T, double* C, cudaStream_t st) {
+  using G = RingCfg<P0>;
+  VES3D_CK(cudaFuncSetAttribute(k_build_ring<P0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM));
+  k_build_ring<P0><<<(unsigned)nrot, 256, G::SMEM, st>>>(R, T, C);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
+bool fused_build_supported(int p0, int p1) {
+  if (p1 != 2 * p0) return false;
+  // the tensor-core tiling needs 2 p0 % 8 == 0 and 4 p0 % 16 == 0
+  switch (p0) {
+    case 4: case 8: case 12: case 16: return true;
+    default: return false;
+  }
+}
+
+int launch_build_ring(const double* R, long nrot, const DevTables& T, double* C, cudaStream_t st) {
+  if (nrot <= 0) return VES3D_OK;
+  switch (T.p0) {
+    case 4: return launch_ring<4>(R, nrot, T, C, st);
+    case 8: return launch_ring<8>(R, nrot, T, C, st);
+    case 12: return launch_ring<12>(R, nrot, T, C, st);
+    case 16: return launch_ring<16>(R, nrot, T, C, st);
+    default:
+      set_error("fused build not instantiated for p = %d", T.p0);
+      return VES3D_ERR_ARG;
+  }
+}
+
+}  // namespace ves3d

@@ -4,11 +4,7 @@
 //   r = x_s - x_t,  u_t += [ d_s / |r| + (r . d_s) r / |r|^3 ] / (8 pi),
 // and a coincident pair (|r| = 0) contributes nothing.
 //
-// Far field: targets are all N surface points, sources are the points of all OTHER
-// vesicles (the reference forms AllPairs - SameVesicle, src/InterfacialVelocity.cc:
-// 1261-1291; here same-vesicle pairs are masked pair by pair, which is the same sum
-// without the cancellation). One thread per target, source tiles staged in shared
-// memory, FP64 accumulation in registers.
+// (The far field with same-vesicle exclusion is in far_kernels.cu.)
 #include "common.cuh"
 #include "kernels.h"
 
@@ -30,58 +26,6 @@ __device__ __forceinline__ void pair_f64(double tx, double ty, double tz, double
   a.x = fma(fma(cc, dx, dx_), rinv, a.x);
   a.y = fma(fma(cc, dy, dy_), rinv, a.y);
   a.z = fma(fma(cc, dz, dz_), rinv, a.z);
-}
-
-// pos/den point-major [N][3]; out/add AxisMajor [nv][3][ng].
-__global__ void __launch_bounds__(kFarBS) k_far_f64(const double* __restrict__ pos, const double* __restrict__ den,
-                                                    long N, int ng, const double* __restrict__ add,
-                                                    double* __restrict__ out) {
-  __shared__ double sp[kFarBS * 3];
-  __shared__ double sd[kFarBS * 3];
-  const long g = (long)blockIdx.x * kFarBS + threadIdx.x;
-  const bool active = g < N;
-  double tx = 0, ty = 0, tz = 0;
-  long lo = 0;
-  if (active) {
-    tx = pos[3 * g];
-    ty = pos[3 * g + 1];
-    tz = pos[3 * g + 2];
-    lo = (g / ng) * ng;
-  }
-  PairAcc acc;
-  for (long s0 = 0; s0 < N; s0 += kFarBS) {
-    const int ns = (int)min((long)kFarBS, N - s0);
-    __syncthreads();
-    for (int i = threadIdx.x; i < 3 * ns; i += kFarBS) {
-      sp[i] = pos[3 * s0 + i];
-      sd[i] = den[3 * s0 + i];
-    }
-    __syncthreads();
-    if (!active) continue;
-    const long rel = s0 - lo;  // source index relative to the target's vesicle start
-#pragma unroll 4
-    for (int k = 0; k < ns; k++) {
-      const bool same = (unsigned long)(rel + k) < (unsigned long)ng;
-      pair_f64(tx, ty, tz, sp[3 * k], sp[3 * k + 1], sp[3 * k + 2], sd[3 * k], sd[3 * k + 1], sd[3 * k + 2], same,
-               acc);
-    }
-  }
-  if (!active) return;
-  const long v = g / ng, k = g - v * ng;
-  const long o = v * 3 * ng + k;
-  const double b0 = add ? add[o] : 0.0, b1 = add ? add[o + ng] : 0.0, b2 = add ? add[o + 2 * ng] : 0.0;
-  out[o] = b0 + acc.x * kInv8Pi;
-  out[o + ng] = b1 + acc.y * kInv8Pi;
-  out[o + 2 * ng] = b2 + acc.z * kInv8Pi;
-}
-
-int launch_far_f64(const double* pos, const double* den, long nv, int ng, const double* add, double* out,
-                   cudaStream_t st) {
-  const long N = nv * ng;
-  if (N <= 0) return VES3D_OK;
-  k_far_f64<<<(unsigned)((N + kFarBS - 1) / kFarBS), kFarBS, 0, st>>>(pos, den, N, ng, add, out);
-  VES3D_LAUNCHED();
-  return VES3D_OK;
 }
 
 // All pairs, point-major in and out.

@@ -1,0 +1,296 @@
+// Far field of the StokesVelocity path: for every surface point t, the Stokeslet sum
+// over the points s of all OTHER vesicles,
+//     u_t = 1/(8 pi) sum_s [ d_s / |r| + (r . d_s) r / |r|^3 ],   r = x_s - x_t,
+// d_s = f_s * area_s * qw_s (StokesAlltoAll - DirectStokesKernel, src/CPUKernels.cc:
+// 123-178, 1011-1057, composed in src/InterfacialVelocity.cc:1261-1291).
+//
+// Work decomposition: one CTA per (source segment, target vesicle). All targets of a
+// CTA belong to one vesicle, so the excluded same-vesicle sources form one contiguous
+// index range and every source tile is swept as at most two unmasked sub-ranges.
+// Sources are staged in shared memory, two targets per thread. Each CTA writes FP64
+// partial sums for its segment; k_far_reduce adds the segments in a fixed order (the
+// result is deterministic) and fuses the addition of the self part.
+//
+// FP64 form: two independent FP64 chains per thread; 1/sqrt from an FP32 hardware seed
+// refined in FP64; a coincident pair (|r| = 0) contributes nothing, as in the reference.
+// Mixed form: coordinates relative to the target vesicle's centroid (differences taken
+// in FP64, rounded to FP32 once per source per CTA), the pair arithmetic in packed FP32
+// (Blackwell f32x2 FMA: both targets of a thread in one instruction), one Newton step on
+// the hardware reciprocal square root, and the FP32 partial of every source tile added
+// into FP64 accumulators. Distinct vesicles must not share points in the mixed form.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace ves3d {
+
+constexpr int kTileF64 = 128;
+constexpr int kTileF32 = 256;
+
+// Source sub-ranges of tile [s0, s0 + ns) that lie outside the excluded range [e0, e1).
+__device__ __forceinline__ void split_tile(long s0, int ns, long e0, long e1, int& a0, int& a1, int& b0, int& b1) {
+  const long lo = max(e0 - s0, 0L), hi = min(e1 - s0, (long)ns);
+  if (hi <= lo) {  // no overlap
+    a0 = 0; a1 = ns; b0 = b1 = 0;
+  } else {
+    a0 = 0; a1 = (int)lo; b0 = (int)hi; b1 = ns;
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// FP64
+// ------------------------------------------------------------------------------------
+struct Acc64 {
+  double x = 0.0, y = 0.0, z = 0.0;
+};
+
+__device__ __forceinline__ void pair64(const double* s, double tx, double ty, double tz, Acc64& a) {
+  const double dx = s[0] - tx, dy = s[1] - ty, dz = s[2] - tz;
+  const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
+  double rinv = rsqrt_f64(r2);
+  rinv = r2 > 0.0 ? rinv : 0.0;
+  const double cc = fma(dz, s[5], fma(dy, s[4], dx * s[3])) * rinv * rinv;
+  a.x = fma(fma(cc, dx, s[3]), rinv, a.x);
+  a.y = fma(fma(cc, dy, s[4]), rinv, a.y);
+  a.z = fma(fma(cc, dz, s[5]), rinv, a.z);
+}
+
+// grid (segments, vesicles, target chunks of 2*blockDim targets); pos/den point-major
+// [N][3]; part [seg][N][3].
+__global__ void __launch_bounds__(512) k_far_f64_seg(const double* __restrict__ pos, const double* __restrict__ den,
+                                                     const long* __restrict__ off, long N, int seg_tiles,
+                                                     double* __restrict__ part) {
+  __shared__ __align__(16) double sm[kTileF64 * 6];
+  const int v = blockIdx.y, seg = blockIdx.x;
+  const long t0 = off[v], nt = off[v + 1] - t0;
+  const int nthr = blockDim.x;
+  const long c0 = (long)blockIdx.z * 2 * nthr;
+  const long ia = t0 + c0 + threadIdx.x, ib = ia + nthr;
+  const bool va = c0 + threadIdx.x < nt, vb = c0 + threadIdx.x + nthr < nt;
+  const long la = va ? ia : t0, lb = vb ? ib : t0;
+  const double ax_ = pos[3 * la], ay_ = pos[3 * la + 1], az_ = pos[3 * la + 2];
+  const double bx_ = pos[3 * lb], by_ = pos[3 * lb + 1], bz_ = pos[3 * lb + 2];
+  Acc64 A, B;
+  const long ntiles = (N + kTileF64 - 1) / kTileF64;
+  const long tb = (long)seg * seg_tiles, te = min(tb + seg_tiles, ntiles);
+  for (long tile = tb; tile < te; tile++) {
+    const long s0 = tile * kTileF64;
+    const int ns = (int)min((long)kTileF64, N - s0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < ns; i += nthr) {
+      const long s = s0 + i;
+      double* d = sm + 6 * i;
+      d[0] = pos[3 * s];
+      d[1] = pos[3 * s + 1];
+      d[2] = pos[3 * s + 2];
+      d[3] = den[3 * s];
+      d[4] = den[3 * s + 1];
+      d[5] = den[3 * s + 2];
+    }
+    __syncthreads();
+    int a0, a1, b0, b1;
+    split_tile(s0, ns, t0, t0 + nt, a0, a1, b0, b1);
+#pragma unroll 2
+    for (int k = a0; k < a1; k++) {
+      pair64(sm + 6 * k, ax_, ay_, az_, A);
+      pair64(sm + 6 * k, bx_, by_, bz_, B);
+    }
+#pragma unroll 2
+    for (int k = b0; k < b1; k++) {
+      pair64(sm + 6 * k, ax_, ay_, az_, A);
+      pair64(sm + 6 * k, bx_, by_, bz_, B);
+    }
+  }
+  double* P = part + (long)seg * 3 * N;
+  if (va) {
+    P[3 * ia] = A.x;
+    P[3 * ia + 1] = A.y;
+    P[3 * ia + 2] = A.z;
+  }
+  if (vb) {
+    P[3 * ib] = B.x;
+    P[3 * ib + 1] = B.y;
+    P[3 * ib + 2] = B.z;
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// Mixed (packed FP32 pairs, FP64 accumulation)
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+
+__global__ void __launch_bounds__(512) k_far_f32_seg(const double* __restrict__ pos, const double* __restrict__ den,
+                                                     const long* __restrict__ off, long N, int seg_tiles,
+                                                     double* __restrict__ part) {
+  // one source = 6 broadcast float2: (x,x) (y,y) (z,z) (dx,dx) (dy,dy) (dz,dz)
+  __shared__ __align__(16) float2 sm[kTileF32 * 6];
+  __shared__ double cen[3];
+  __shared__ double red[3][32];
+  const int v = blockIdx.y, seg = blockIdx.x;
+  const long t0 = off[v], nt = off[v + 1] - t0;
+  const int nthr = blockDim.x;
+  // centroid of the target vesicle (FP64), the origin of this CTA's FP32 coordinates
+  {
+    double cx = 0, cy = 0, cz = 0;
+    for (long i = threadIdx.x; i < nt; i += nthr) {
+      cx += pos[3 * (t0 + i)];
+      cy += pos[3 * (t0 + i) + 1];
+      cz += pos[3 * (t0 + i) + 2];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      cx += __shfl_down_sync(0xffffffffu, cx, o);
+      cy += __shfl_down_sync(0xffffffffu, cy, o);
+      cz += __shfl_down_sync(0xffffffffu, cz, o);
+    }
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+      red[0][w] = cx;
+      red[1][w] = cy;
+      red[2][w] = cz;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+      double s = 0;
+      for (int i = 0; i < (nthr + 31) / 32; i++) s += red[threadIdx.x][i];
+      cen[threadIdx.x] = s / (double)nt;
+    }
+    __syncthreads();
+  }
+  const double cx = cen[0], cy = cen[1], cz = cen[2];
+  const long c0 = (long)blockIdx.z * 2 * nthr;
+  const long ia = t0 + c0 + threadIdx.x, ib = ia + nthr;
+  const bool va = c0 + threadIdx.x < nt, vb = c0 + threadIdx.x + nthr < nt;
+  const long la = va ? ia : t0, lb = vb ? ib : t0;
+  // negated targets, packed (lane x = target a, lane y = target b)
+  const float2 ntx = make_float2((float)(cx - pos[3 * la]), (float)(cx - pos[3 * lb]));
+  const float2 nty = make_float2((float)(cy - pos[3 * la + 1]), (float)(cy - pos[3 * lb + 1]));
+  const float2 ntz = make_float2((float)(cz - pos[3 * la + 2]), (float)(cz - pos[3 * lb + 2]));
+  double Ax = 0, Ay = 0, Az = 0, Bx = 0, By = 0, Bz = 0;
+  const long ntiles = (N + kTileF32 - 1) / kTileF32;
+  const long tb = (long)seg * seg_tiles, te = min(tb + seg_tiles, ntiles);
+  const float2 c15 = f2(1.5f), cm05 = f2(-0.5f);
+  for (long tile = tb; tile < te; tile++) {
+    const long s0 = tile * kTileF32;
+    const int ns = (int)min((long)kTileF32, N - s0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < ns; i += nthr) {
+      const long s = s0 + i;
+      float2* d = sm + 6 * i;
+      d[0] = f2((float)(pos[3 * s] - cx));
+      d[1] = f2((float)(pos[3 * s + 1] - cy));
+      d[2] = f2((float)(pos[3 * s + 2] - cz));
+      d[3] = f2((float)den[3 * s]);
+      d[4] = f2((float)den[3 * s + 1]);
+      d[5] = f2((float)den[3 * s + 2]);
+    }
+    __syncthreads();
+    int r0[2], r1[2];
+    split_tile(s0, ns, t0, t0 + nt, r0[0], r1[0], r0[1], r1[1]);
+    float2 ux = f2(0.f), uy = f2(0.f), uz = f2(0.f);
+#pragma unroll
+    for (int part_i = 0; part_i < 2; part_i++) {
+#pragma unroll 4
+      for (int k = r0[part_i]; k < r1[part_i]; k++) {
+        const float4* q = reinterpret_cast<const float4*>(sm + 6 * k);
+        const float4 q0 = q[0], q1 = q[1], q2 = q[2];
+        const float2 sx = make_float2(q0.x, q0.y), sy = make_float2(q0.z, q0.w);
+        const float2 sz = make_float2(q1.x, q1.y), dx_ = make_float2(q1.z, q1.w);
+        const float2 dy_ = make_float2(q2.x, q2.y), dz_ = make_float2(q2.z, q2.w);
+        const float2 rx = __fadd2_rn(sx, ntx), ry = __fadd2_rn(sy, nty), rz = __fadd2_rn(sz, ntz);
+        float2 r2 = __fmul2_rn(rx, rx);
+        r2 = __ffma2_rn(ry, ry, r2);
+        r2 = __ffma2_rn(rz, rz, r2);
+        float2 y = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+        // one Newton step: y <- y (1.5 - 0.5 r2 y^2)
+        const float2 h = __fmul2_rn(__fmul2_rn(r2, y), y);
+        y = __fmul2_rn(y, __ffma2_rn(h, cm05, c15));
+        float2 dot = __fmul2_rn(rx, dx_);
+        dot = __ffma2_rn(ry, dy_, dot);
+        dot = __ffma2_rn(rz, dz_, dot);
+        const float2 cc = __fmul2_rn(dot, __fmul2_rn(y, y));
+        ux = __ffma2_rn(__ffma2_rn(cc, rx, dx_), y, ux);
+        uy = __ffma2_rn(__ffma2_rn(cc, ry, dy_), y, uy);
+        uz = __ffma2_rn(__ffma2_rn(cc, rz, dz_), y, uz);
+      }
+    }
+    Ax += ux.x;
+    Ay += uy.x;
+    Az += uz.x;
+    Bx += ux.y;
+    By += uy.y;
+    Bz += uz.y;
+  }
+  double* P = part + (long)seg * 3 * N;
+  if (va) {
+    P[3 * ia] = Ax;
+    P[3 * ia + 1] = Ay;
+    P[3 * ia + 2] = Az;
+  }
+  if (vb) {
+    P[3 * ib] = Bx;
+    P[3 * ib + 1] = By;
+    P[3 * ib + 2] = Bz;
+  }
+}
+
+// out (AxisMajor per vesicle) = add + (1/8pi) sum over segments in order. One CTA per
+// vesicle; vesicle v holds points [off[v], off[v+1]) as [3][n_v] from 3*off[v].
+__global__ void k_far_reduce(const double* __restrict__ part, int nseg, const long* __restrict__ off, long N,
+                             const double* __restrict__ add, double* __restrict__ out, double* __restrict__ far_out) {
+  const int v = blockIdx.x;
+  const long t0 = off[v], nt = off[v + 1] - t0;
+  for (long i = threadIdx.x; i < 3 * nt; i += blockDim.x) {
+    const long k = i / 3;
+    const int c = (int)(i - 3 * k);
+    const long g = t0 + k;
+    double s = 0.0;
+    for (int q = 0; q < nseg; q++) s += part[(long)q * 3 * N + 3 * g + c];
+    s *= kInv8Pi;
+    const long o = 3 * t0 + c * nt + k;
+    if (far_out) far_out[o] = s;
+    out[o] = (add ? add[o] : 0.0) + s;
+  }
+}
+
+int far_segments(long nves, long N, int tile, int nthr, int* seg_tiles) {
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const long ntiles = (N + tile - 1) / tile;
+  const int per_sm = max(1, 2048 / max(nthr, 32));  // resident CTAs per SM if threads limit
+  const long want = (long)nsm * per_sm * 8;         // about eight waves
+  long nseg = (want + nves - 1) / nves;
+  if (nseg < 1) nseg = 1;
+  if (nseg > ntiles) nseg = ntiles;
+  *seg_tiles = (int)((ntiles + nseg - 1) / nseg);
+  return (int)((ntiles + *seg_tiles - 1) / *seg_tiles);
+}
+
+int launch_far(bool mixed, const double* pos, const double* den, const long* off, long nves, long N, int max_nt,
+               const double* add, double* out, double* far_out, double* part, long part_cap_segments,
+               cudaStream_t st) {
+  if (N <= 0) return VES3D_OK;
+  // targets of a vesicle in chunks of at most 1024 (two per thread, <= 512 threads)
+  const int nchunk = (max_nt + 1023) / 1024;
+  const int per_chunk = (max_nt + nchunk - 1) / nchunk;
+  const int nthr = 32 * ((((per_chunk + 1) / 2) + 31) / 32);
+  const int tile = mixed ? kTileF32 : kTileF64;
+  int seg_tiles = 1;
+  int nseg = far_segments(nves * nchunk, N, tile, nthr, &seg_tiles);
+  if (nseg > part_cap_segments) {
+    // fewer, longer segments if the partial-sum buffer is smaller than the choice
+    const long ntiles = (N + tile - 1) / tile;
+    seg_tiles = (int)((ntiles + part_cap_segments - 1) / part_cap_segments);
+    nseg = (int)((ntiles + seg_tiles - 1) / seg_tiles);
+  }
+  dim3 grid(nseg, (unsigned)nves, nchunk);
+  if (mixed)
+    k_far_f32_seg<<<grid, nthr, 0, st>>>(pos, den, off, N, seg_tiles, part);
+  else
+    k_far_f64_seg<<<grid, nthr, 0, st>>>(pos, den, off, N, seg_tiles, part);
+  VES3D_LAUNCHED();
+  k_far_reduce<<<(unsigned)nves, 256, 0, st>>>(part, nseg, off, N, add, out, far_out);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
+}  // namespace ves3d

@@ -17,12 +17,17 @@ struct DevTables {
   int *jf_of_coef = nullptr, *blk_off = nullptr, *m_of_coef = nullptr, *n_of_coef = nullptr;
   int *partner = nullptr, *is_sin = nullptr;
   double* mr = nullptr;
+  int mr_total = 0;  // doubles in mr; (p0+1) equal parts, one per latitude rotation t
   int *mr_off = nullptr, *perm = nullptr, *perm_off = nullptr, *pos_in_block = nullptr;
   double *sing_w = nullptr, *smooth_w0 = nullptr, *qp = nullptr, *cos_tab = nullptr, *sin_tab = nullptr;
 };
 
 int launch_analysis(const double* in, long nfun, int pin, int pout, const double* four, const double* leg,
                     const int* jf, double* out, cudaStream_t st);
+// Grid2SHC(p, p): tensor-core kernel where instantiated (2p % 8 == 0), generic otherwise;
+// VES3D_TC_ANALYSIS=0 forces the generic kernel.
+int launch_grid2shc(const double* in, long nfun, int p, const double* four, const double* leg, const int* jf,
+                    double* out, cudaStream_t st);
 int launch_synthesis(const double* S, long nfun, int p0, int q, const double* leg, const double* dleg,
                      const double* four, const double* dfour, const int* blk_off, double* X, double* Xt,
                      double* Xp, cudaStream_t st);
@@ -37,6 +42,10 @@ int launch_singular_sl(const double* X, const double* Xt, const double* Xp, cons
 // RotateTranspose with dof = 12 (:452-541) fused with the Rearrange (:1090-1172):
 // C [nv][p0+1][p0][2][6][Ncoef] -> SL3 [nv][3][Ncoef][3][Ngrid].
 int launch_rotate_transpose_scatter(const double* C, long nv, const DevTables& T, double* SL3, cudaStream_t st);
+// Fused per-rotation build (FP64 tensor cores): R [nrot][3][Nc] -> C [nrot][2][6][Nc],
+// i.e. upsampled synthesis + singular kernel + transposed synthesis in one kernel.
+bool fused_build_supported(int p0, int p1);
+int launch_build_ring(const double* R, long nrot, const DevTables& T, double* C, cudaStream_t st);
 // V[v] = F[v] . SL[v] (src/StokesVelocity.cc:397-416), n = 3 Ncoef.
 int launch_self_gemv(const double* F, const double* SL, long nv, int n, double* V, cudaStream_t st);
 // area element |X_theta x X_phi| and far-field sources: pos/den point-major [N][3],
@@ -46,9 +55,14 @@ int launch_far_sources(const double* X, const double* f, const double* Xt, const
 // den only, from a stored area element.
 int launch_far_density(const double* f, const double* area, long nv, int p0, const double* smooth_w, double* den,
                        cudaStream_t st);
-// out (AxisMajor) = add (AxisMajor, may be null) + sum over other vesicles' sources.
-int launch_far_f64(const double* pos, const double* den, long nv, int ng, const double* add, double* out,
-                   cudaStream_t st);
+// Far field: out (AxisMajor per vesicle) = add (may be null) + sum over other vesicles'
+// sources; far_out (may be null) receives the far part alone. off [nves+1] point offsets,
+// max_nt the largest vesicle; part is a [part_cap_segments][N][3] FP64 work buffer.
+// mixed selects the packed-FP32 pair arithmetic with FP64 accumulation.
+int launch_far(bool mixed, const double* pos, const double* den, const long* off, long nves, long N, int max_nt,
+               const double* add, double* out, double* far_out, double* part, long part_cap_segments,
+               cudaStream_t st);
+constexpr long kFarMaxSegments = 32;
 // out = a + b elementwise.
 int launch_add(const double* a, const double* b, long n, double* out, cudaStream_t st);
 // All pairs, point-major in/out (StokesAlltoAll semantics).

@@ -9,6 +9,8 @@
 //     X[lat][j]  = sum_jf B[lat][jf] * four[jf][j]   (X_theta with dfour, X_phi from dleg)
 // One CTA transforms FPB functions with every intermediate in shared memory; the
 // tables are small and read through the read-only cache.
+#include <cstdlib>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -136,6 +138,115 @@ int launch_synthesis(const double* S, long nfun, int p0, int q, const double* le
                                                   fpb, X, Xt, Xp);
   VES3D_LAUNCHED();
   return VES3D_OK;
+}
+
+}  // namespace ves3d
+
+namespace ves3d {
+
+__device__ __forceinline__ void dmma_a(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+constexpr int pad4m16(int n) { return ((n + 11) / 16) * 16 + 4; }
+
+// Grid2SHC(p, p) on FP64 tensor cores: 4 functions per CTA. The length-2p DFT of every
+// (function, latitude) row is one GEMM [rows x 2p] . MatFourierInv(p, p) with
+// mma.sync m8n8k4 (fragments as in build_kernels.cu); the per-frequency Legendre sums
+// run on the CUDA cores from shared memory. Needs 2p % 8 == 0.
+template <int P>
+struct AnaTcCfg {
+  static constexpr int FB = 4;
+  static constexpr int NLAT = P + 1, NLON = 2 * P, NC = P * (P + 2);
+  static constexpr int ROWS = ((FB * NLAT + 7) / 8) * 8;
+  static constexpr int LD = pad4m16(NLON);
+  static constexpr int OFF_A = 0, OFF_F = ROWS * LD, OFF_M = 2 * ROWS * LD, OFF_L = OFF_M + NLON * LD;
+  static constexpr int TOTAL = OFF_L + NC * NLAT;
+  static constexpr size_t SMEM = (size_t)TOTAL * sizeof(double);
+};
+
+template <int P>
+__global__ void __launch_bounds__(256, 2) k_analysis_tc(const double* __restrict__ in, long nfun,
+                                                        const double* __restrict__ four, const double* __restrict__ leg,
+                                                        const int* __restrict__ jf, double* __restrict__ out) {
+  using G = AnaTcCfg<P>;
+  extern __shared__ __align__(16) double sm[];
+  double* sA = sm + G::OFF_A;
+  double* sF = sm + G::OFF_F;
+  double* sM = sm + G::OFF_M;
+  double* sL = sm + G::OFF_L;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const long f0 = (long)blockIdx.x * G::FB;
+  const int nf = (int)min((long)G::FB, nfun - f0);
+  const double* src = in + f0 * G::NLAT * G::NLON;
+  for (int i = tid; i < G::ROWS * G::NLON; i += 256) {
+    const int r = i / G::NLON, j = i - r * G::NLON;
+    sA[r * G::LD + j] = r < nf * G::NLAT ? src[i] : 0.0;
+  }
+  for (int i = tid; i < G::NLON * G::NLON; i += 256) {
+    const int r = i / G::NLON, j = i - r * G::NLON;
+    sM[r * G::LD + j] = __ldg(four + i);
+  }
+  for (int i = tid; i < G::NC * G::NLAT; i += 256) sL[i] = __ldg(leg + i);
+  __syncthreads();
+  const int grow = lane >> 2, gcol = lane & 3;
+  constexpr int MT = G::ROWS / 8, NT = G::NLON / 8;
+  for (int it = warp; it < MT * NT; it += 8) {
+    const int nt = it % NT, mt = it / NT;
+    const double* a = sA + (mt * 8 + grow) * G::LD + gcol;
+    const double* b = sM + gcol * G::LD + nt * 8 + grow;  // B[k][n] = four[k][n]
+    double c0 = 0, c1 = 0, d0 = 0, d1 = 0;
+#pragma unroll
+    for (int ks = 0; ks < G::NLON / 4; ks += 2) {
+      dmma_a(c0, c1, a[ks * 4], b[ks * 4 * G::LD]);
+      if (ks + 1 < G::NLON / 4) dmma_a(d0, d1, a[ks * 4 + 4], b[(ks * 4 + 4) * G::LD]);
+    }
+    double* o = sF + (mt * 8 + grow) * G::LD + nt * 8 + 2 * gcol;
+    o[0] = c0 + d0;
+    o[1] = c1 + d1;
+  }
+  __syncthreads();
+  for (int i = tid; i < nf * G::NC; i += 256) {
+    const int f = i / G::NC, c = i - f * G::NC;
+    const int k = __ldg(jf + c);
+    const double* fr = sF + (f * G::NLAT) * G::LD + k;
+    const double* lr = sL + c * G::NLAT;
+    double s = 0.0;
+#pragma unroll
+    for (int lat = 0; lat < G::NLAT; lat++) s = fma(fr[lat * G::LD], lr[lat], s);
+    out[(f0 + f) * G::NC + c] = s;
+  }
+}
+
+template <int P>
+static int launch_ana_tc(const double* in, long nfun, const double* four, const double* leg, const int* jf,
+                         double* out, cudaStream_t st) {
+  using G = AnaTcCfg<P>;
+  VES3D_CK(cudaFuncSetAttribute(k_analysis_tc<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM));
+  const long nblk = (nfun + G::FB - 1) / G::FB;
+  k_analysis_tc<P><<<(unsigned)nblk, 256, G::SMEM, st>>>(in, nfun, four, leg, jf, out);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
+// Grid2SHC(p, p) with the tensor-core kernel where it is instantiated, else the generic one.
+int launch_grid2shc(const double* in, long nfun, int p, const double* four, const double* leg, const int* jf,
+                    double* out, cudaStream_t st) {
+  if (nfun <= 0) return VES3D_OK;
+  const char* env = getenv("VES3D_TC_ANALYSIS");
+  const bool tc = !(env && env[0] == '0');
+  if (tc) {
+    switch (p) {
+      case 4: return launch_ana_tc<4>(in, nfun, four, leg, jf, out, st);
+      case 8: return launch_ana_tc<8>(in, nfun, four, leg, jf, out, st);
+      case 12: return launch_ana_tc<12>(in, nfun, four, leg, jf, out, st);
+      case 16: return launch_ana_tc<16>(in, nfun, four, leg, jf, out, st);
+      default: break;
+    }
+  }
+  return launch_analysis(in, nfun, p, p, four, leg, jf, out, st);
 }
 
 }  // namespace ves3d

@@ -10,15 +10,19 @@ namespace ves3d {
 
 // One CTA per (vesicle v, latitude rotation t); loops over the p0 longitude phases j.
 // out[c'] = sum_b (P_j s)[perm_n[b]] * Mr[t][n][b][pos(c')],   n = degree(c').
-__global__ void __launch_bounds__(256) k_rotate_all(const double* __restrict__ S, int p0, DevTables T,
+// The blocks Mr[t][.] (mr_per_t doubles, contiguous for one t) are staged in shared memory.
+__global__ void __launch_bounds__(256) k_rotate_all(const double* __restrict__ S, int p0, int mr_per_t, DevTables T,
                                                     double* __restrict__ R) {
   extern __shared__ double sm[];
   const int nc = p0 * (p0 + 2);
   double* sS = sm;
   double* sB = sm + 3 * nc;
+  double* sM = sm + 6 * nc;
   const int t = blockIdx.x;
   const long v = blockIdx.y;
+  const int mbase = __ldg(T.mr_off + t * (p0 + 1));
   for (int i = threadIdx.x; i < 3 * nc; i += blockDim.x) sS[i] = S[v * 3 * nc + i];
+  for (int i = threadIdx.x; i < mr_per_t; i += blockDim.x) sM[i] = __ldg(T.mr + mbase + i);
   __syncthreads();
   for (int j = 0; j < p0; j++) {
     for (int i = threadIdx.x; i < 3 * nc; i += blockDim.x) {
@@ -42,23 +46,26 @@ __global__ void __launch_bounds__(256) k_rotate_all(const double* __restrict__ S
       const int d = i / nc, c = i % nc;
       const int n = __ldg(T.n_of_coef + c), bp = __ldg(T.pos_in_block + c);
       const int po = __ldg(T.perm_off + n), bn = __ldg(T.perm_off + n + 1) - po;
-      const double* M = T.mr + __ldg(T.mr_off + t * (p0 + 1) + n);
+      const double* M = sM + (__ldg(T.mr_off + t * (p0 + 1) + n) - mbase);
       const double* b = sB + d * nc;
       double s = 0.0;
-      for (int k = 0; k < bn; k++) s = fma(b[__ldg(T.perm + po + k)], __ldg(M + k * bn + bp), s);
+      for (int k = 0; k < bn; k++) s = fma(b[__ldg(T.perm + po + k)], M[k * bn + bp], s);
       out[i] = s;
     }
     __syncthreads();
   }
 }
 
+static int mr_per_t(const DevTables& T) { return T.mr_total / (T.p0 + 1); }
+
 int launch_rotate_all(const double* S, long nv, const DevTables& T, double* R, cudaStream_t st) {
   if (nv <= 0) return VES3D_OK;
   const int p0 = T.p0;
-  size_t smem = (size_t)6 * ncoef_(p0) * sizeof(double);
+  const int mpt = mr_per_t(T);
+  size_t smem = ((size_t)6 * ncoef_(p0) + mpt) * sizeof(double);
   if (smem > 48 * 1024) VES3D_CK(cudaFuncSetAttribute(k_rotate_all, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid(p0 + 1, (unsigned)nv);
-  k_rotate_all<<<grid, 256, smem, st>>>(S, p0, T, R);
+  k_rotate_all<<<grid, 256, smem, st>>>(S, p0, mpt, T, R);
   VES3D_LAUNCHED();
   return VES3D_OK;
 }
@@ -127,34 +134,56 @@ int launch_singular_sl(const double* X, const double* Xt, const double* Xp, cons
 // (t, j, pole, comp) function): b = Mr_t^T a per degree block, then the inverse phase
 // P_j^T, then scatter into SL3[v][c_in][k][c_out][grid] at grid (t, j) for pole 0 and
 // (p0 - t, p0 + j) for pole 1, for both (c_in, c_out) orders of the symmetric component.
+// The blocks Mr[t][.] are staged in shared memory; each input vector is stored in
+// degree-major order (coefficients of one degree contiguous) so the block products read
+// contiguous data, and every thread forms one coefficient for 4 rotations at a time.
+constexpr int kRtJ = 4;
+
 __global__ void __launch_bounds__(256) k_rotate_transpose_scatter(const double* __restrict__ C, int p0, int jb,
-                                                                  DevTables T, double* __restrict__ SL3) {
+                                                                  int mr_per_t, DevTables T,
+                                                                  double* __restrict__ SL3) {
   extern __shared__ double sm[];
   const int nc = p0 * (p0 + 2), ng = 2 * p0 * (p0 + 1);
-  double* sA = sm;             // jb * nc
-  double* sB = sm + jb * nc;   // jb * nc
+  const int lda = nc + 2;      // row padding against bank conflicts between rotations
+  double* sA = sm;             // jb * lda, degree-major
+  double* sB = sm + jb * lda;  // jb * lda, coefficient order
+  double* sM = sm + 2 * jb * lda;
   const int t = blockIdx.x;
   const long v = blockIdx.y;
+  const int mbase = __ldg(T.mr_off + t * (p0 + 1));
+  for (int i = threadIdx.x; i < mr_per_t; i += blockDim.x) sM[i] = __ldg(T.mr + mbase + i);
   // symmetric component -> (c_in, c_out) pairs
   const int ci0[6] = {0, 0, 0, 1, 1, 2}, co0[6] = {0, 1, 2, 1, 2, 2};
   for (int pole = 0; pole < 2; pole++) {
     for (int comp = 0; comp < 6; comp++) {
       for (int j0 = 0; j0 < p0; j0 += jb) {
         const int nj = min(jb, p0 - j0);
-        for (int i = threadIdx.x; i < nj * nc; i += blockDim.x) {
-          const int jj = i / nc, c = i % nc;
-          sA[i] = C[((((v * (p0 + 1) + t) * p0 + j0 + jj) * 2 + pole) * 6 + comp) * (long)nc + c];
-        }
         __syncthreads();
         for (int i = threadIdx.x; i < nj * nc; i += blockDim.x) {
           const int jj = i / nc, c = i % nc;
+          const int n = __ldg(T.n_of_coef + c);
+          const int dm = __ldg(T.perm_off + n) + __ldg(T.pos_in_block + c);
+          sA[jj * lda + dm] = C[((((v * (p0 + 1) + t) * p0 + j0 + jj) * 2 + pole) * 6 + comp) * (long)nc + c];
+        }
+        __syncthreads();
+        const int njq = (nj + kRtJ - 1) / kRtJ;
+        for (int i = threadIdx.x; i < njq * nc; i += blockDim.x) {
+          const int c = i % nc, jq = i / nc;
           const int n = __ldg(T.n_of_coef + c), b = __ldg(T.pos_in_block + c);
           const int po = __ldg(T.perm_off + n), bn = __ldg(T.perm_off + n + 1) - po;
-          const double* M = T.mr + __ldg(T.mr_off + t * (p0 + 1) + n);
-          const double* a = sA + jj * nc;
-          double s = 0.0;
-          for (int k = 0; k < bn; k++) s = fma(a[__ldg(T.perm + po + k)], __ldg(M + b * bn + k), s);
-          sB[i] = s;
+          const double* M = sM + (__ldg(T.mr_off + t * (p0 + 1) + n) - mbase) + b * bn;
+          const double* a = sA + jq * kRtJ * lda + po;
+          double acc[kRtJ];
+#pragma unroll
+          for (int q = 0; q < kRtJ; q++) acc[q] = 0.0;
+          for (int k = 0; k < bn; k++) {
+            const double m = M[k];
+#pragma unroll
+            for (int q = 0; q < kRtJ; q++) acc[q] = fma(a[q * lda + k], m, acc[q]);
+          }
+#pragma unroll
+          for (int q = 0; q < kRtJ; q++)
+            if (jq * kRtJ + q < nj) sB[(jq * kRtJ + q) * lda + c] = acc[q];
         }
         __syncthreads();
         // inverse phase and scatter; consecutive threads take consecutive j for coalescing
@@ -164,14 +193,14 @@ __global__ void __launch_bounds__(256) k_rotate_transpose_scatter(const double* 
           const int pc = __ldg(T.partner + c);
           double val;
           if (pc < 0) {
-            val = sB[jj * nc + c];
+            val = sB[jj * lda + c];
           } else {
             const int q = (__ldg(T.m_of_coef + c) * j) % (2 * p0);
             const double cs = __ldg(T.cos_tab + q), sn = __ldg(T.sin_tab + q);
             if (!__ldg(T.is_sin + c)) {
-              val = sB[jj * nc + c] * cs - sB[jj * nc + pc] * sn;
+              val = sB[jj * lda + c] * cs - sB[jj * lda + pc] * sn;
             } else {
-              val = sB[jj * nc + pc] * sn + sB[jj * nc + c] * cs;
+              val = sB[jj * lda + pc] * sn + sB[jj * lda + c] * cs;
             }
           }
           const int grid = pole == 0 ? t * 2 * p0 + j : (p0 - t) * 2 * p0 + p0 + j;
@@ -179,7 +208,6 @@ __global__ void __launch_bounds__(256) k_rotate_transpose_scatter(const double* 
           SL3[(((v * 3 + cin) * nc + c) * 3 + cout) * (long)ng + grid] = val;
           if (cin != cout) SL3[(((v * 3 + cout) * nc + c) * 3 + cin) * (long)ng + grid] = val;
         }
-        __syncthreads();
       }
     }
   }
@@ -188,14 +216,18 @@ __global__ void __launch_bounds__(256) k_rotate_transpose_scatter(const double* 
 int launch_rotate_transpose_scatter(const double* C, long nv, const DevTables& T, double* SL3, cudaStream_t st) {
   if (nv <= 0) return VES3D_OK;
   const int p0 = T.p0, nc = ncoef_(p0);
-  int jb = (int)((96 * 1024 / sizeof(double)) / (2 * (size_t)nc));
-  if (jb > p0) jb = p0;
-  if (jb < 1) jb = 1;
-  size_t smem = (size_t)2 * jb * nc * sizeof(double);
+  const int mpt = mr_per_t(T);
+  // two CTAs per SM: keep shared memory under ~110 KB; whole groups of kRtJ rotations
+  long budget = (110 * 1024) / (long)sizeof(double) - mpt;
+  int jb = (int)(budget / (2 * (long)(nc + 2)));
+  jb = (jb / kRtJ) * kRtJ;
+  if (jb > p0) jb = ((p0 + kRtJ - 1) / kRtJ) * kRtJ;
+  if (jb < kRtJ) jb = kRtJ;
+  size_t smem = ((size_t)2 * jb * (nc + 2) + mpt) * sizeof(double);
   if (smem > 48 * 1024)
     VES3D_CK(cudaFuncSetAttribute(k_rotate_transpose_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid(p0 + 1, (unsigned)nv);
-  k_rotate_transpose_scatter<<<grid, 256, smem, st>>>(C, p0, jb, T, SL3);
+  k_rotate_transpose_scatter<<<grid, 256, smem, st>>>(C, p0, jb, mpt, T, SL3);
   VES3D_LAUNCHED();
   return VES3D_OK;
 }

@@ -69,6 +69,7 @@ struct TablesOwner {
   int upload(cudaStream_t st) {
     d.p0 = h.p0;
     d.p1 = h.p1;
+    d.mr_total = (int)h.mr.size();
     int s = 0;
     s |= dupload(&d.ana_four, h.ana.four, st);
     s |= dupload(&d.ana_leg, h.ana.leg, st);
@@ -115,7 +116,8 @@ struct ves3d_sv {
   // resident buffers
   double *X = nullptr, *F = nullptr, *V = nullptr, *Vself = nullptr, *Vfar = nullptr;
   double *Sx = nullptr, *Xt = nullptr, *Xp = nullptr, *area = nullptr, *pos = nullptr, *den = nullptr;
-  double *SL = nullptr, *Fc = nullptr, *Vc = nullptr;
+  double *SL = nullptr, *Fc = nullptr, *Vc = nullptr, *part = nullptr;
+  long* off = nullptr;  // [nves+1] point offsets of the vesicles
   // setup scratch (one chunk of vesicles)
   long chunk = 0;
   double *R = nullptr, *Xu = nullptr, *Xut = nullptr, *Xup = nullptr, *K = nullptr, *C = nullptr, *SL3 = nullptr;
@@ -132,9 +134,11 @@ struct ves3d_sv {
     if (own_stream) cudaStreamDestroy(own_stream);
   }
   void free_buffers() {
-    double* ps[] = {X, F, V, Vself, Vfar, Sx, Xt, Xp, area, pos, den, SL, Fc, Vc};
+    double* ps[] = {X, F, V, Vself, Vfar, Sx, Xt, Xp, area, pos, den, SL, Fc, Vc, part};
     for (double* q : ps) dfree(q);
-    X = F = V = Vself = Vfar = Sx = Xt = Xp = area = pos = den = SL = Fc = Vc = nullptr;
+    dfree(off);
+    off = nullptr;
+    X = F = V = Vself = Vfar = Sx = Xt = Xp = area = pos = den = SL = Fc = Vc = part = nullptr;
     cap_ves = 0;
   }
   void free_scratch() {
@@ -176,6 +180,8 @@ int alloc_resident(ves3d_sv* sv, long nves) {
   s |= dalloc(&sv->SL, (size_t)nves * n * n);
   s |= dalloc(&sv->Fc, (size_t)nves * n);
   s |= dalloc(&sv->Vc, (size_t)nves * n);
+  s |= dalloc(&sv->part, (size_t)kFarMaxSegments * fld);
+  s |= dalloc(&sv->off, (size_t)nves + 1);
   if (s) {
     sv->free_buffers();
     return s;
@@ -184,19 +190,28 @@ int alloc_resident(ves3d_sv* sv, long nves) {
   return VES3D_OK;
 }
 
+// The fused per-rotation build is used when it is instantiated for (p, p_up);
+// VES3D_FUSED_BUILD=0 forces the unfused stage-by-stage pipeline (A/B checks).
+bool use_fused(const ves3d_sv* sv) {
+  const char* env = getenv("VES3D_FUSED_BUILD");
+  if (env && env[0] == '0') return false;
+  return fused_build_supported(sv->p, sv->pup);
+}
+
 // Doubles of setup scratch per vesicle.
-size_t scratch_per_vesicle(int p0, int p1) {
+size_t scratch_per_vesicle(int p0, int p1, bool fused) {
   const size_t npr = (size_t)p0 * (p0 + 1), nc = ncoef_(p0), M1 = ngrid_(p1), ng = ngrid_(p0);
-  return npr * 3 * nc            // R
-         + 3 * npr * 3 * M1      // Xu, Xut, Xup
-         + npr * 12 * M1         // K
-         + npr * 12 * nc         // C
-         + 3 * nc * 3 * ng;      // SL3
+  return npr * 3 * nc                            // R
+         + (fused ? 0 : 3 * npr * 3 * M1)        // Xu, Xut, Xup
+         + (fused ? 0 : npr * 12 * M1)           // K
+         + npr * 12 * nc                         // C
+         + 3 * nc * 3 * ng;                      // SL3
 }
 
 int alloc_scratch(ves3d_sv* sv) {
   const long want = sv->nves;
-  size_t per = scratch_per_vesicle(sv->p, sv->pup) * sizeof(double);
+  const bool fused = use_fused(sv);
+  size_t per = scratch_per_vesicle(sv->p, sv->pup, fused) * sizeof(double);
   size_t free_b = 0, total_b = 0;
   VES3D_CK(cudaMemGetInfo(&free_b, &total_b));
   // Scratch budget for one chunk of the self-matrix build: 8 GiB by default, capped at a
@@ -215,10 +230,12 @@ int alloc_scratch(ves3d_sv* sv) {
   const size_t npr = (size_t)sv->p * (sv->p + 1), nc = ncoef_(sv->p), M1 = ngrid_(sv->pup), ng = ngrid_(sv->p);
   int s = 0;
   s |= dalloc(&sv->R, chunk * npr * 3 * nc);
-  s |= dalloc(&sv->Xu, chunk * npr * 3 * M1);
-  s |= dalloc(&sv->Xut, chunk * npr * 3 * M1);
-  s |= dalloc(&sv->Xup, chunk * npr * 3 * M1);
-  s |= dalloc(&sv->K, chunk * npr * 12 * M1);
+  if (!fused) {
+    s |= dalloc(&sv->Xu, chunk * npr * 3 * M1);
+    s |= dalloc(&sv->Xut, chunk * npr * 3 * M1);
+    s |= dalloc(&sv->Xup, chunk * npr * 3 * M1);
+    s |= dalloc(&sv->K, chunk * npr * 12 * M1);
+  }
   s |= dalloc(&sv->C, chunk * npr * 12 * nc);
   s |= dalloc(&sv->SL3, chunk * 3 * nc * 3 * ng);
   if (s) {
@@ -242,6 +259,8 @@ int copy_out(double* dst, const double* src, size_t n, int is_device, cudaStream
   return VES3D_OK;
 }
 
+int alloc_scratch(ves3d_sv* sv);
+
 int run_setup(ves3d_sv* sv) {
   const DevTables& T = sv->tab->d;
   const int p0 = sv->p, p1 = sv->pup, nc = ncoef_(p0), ng = ngrid_(p0), M1 = ngrid_(p1);
@@ -249,18 +268,24 @@ int run_setup(ves3d_sv* sv) {
   cudaStream_t st = sv->stream;
   int s = alloc_scratch(sv);
   if (s) return s;
+  const bool fused = use_fused(sv);
   VES3D_CK(cudaEventRecord(sv->ev[0], st));
   for (long v0 = 0; v0 < sv->nves; v0 += sv->chunk) {
     const long nb = std::min(sv->chunk, sv->nves - v0);
     const long nrot = nb * npr;
     if ((s = launch_rotate_all(sv->Sx + v0 * 3 * nc, nb, T, sv->R, st))) return s;
-    if ((s = launch_synthesis(sv->R, nrot * 3, p0, p1, T.syn1_leg, T.syn1_dleg, T.syn1_four, T.syn1_dfour, T.blk_off,
-                              sv->Xu, sv->Xut, sv->Xup, st)))
-      return s;
-    if ((s = launch_singular_sl(sv->Xu, sv->Xut, sv->Xup, sv->R, nrot, T, sv->K, st))) return s;
-    if ((s = launch_analysis(sv->K, nrot * 12, p1, p0, T.synT_four, T.syn1_leg, T.jf_of_coef, sv->C, st))) return s;
+    if (fused) {
+      if ((s = launch_build_ring(sv->R, nrot, T, sv->C, st))) return s;
+    } else {
+      if ((s = launch_synthesis(sv->R, nrot * 3, p0, p1, T.syn1_leg, T.syn1_dleg, T.syn1_four, T.syn1_dfour,
+                                T.blk_off, sv->Xu, sv->Xut, sv->Xup, st)))
+        return s;
+      if ((s = launch_singular_sl(sv->Xu, sv->Xut, sv->Xup, sv->R, nrot, T, sv->K, st))) return s;
+      if ((s = launch_analysis(sv->K, nrot * 12, p1, p0, T.synT_four, T.syn1_leg, T.jf_of_coef, sv->C, st)))
+        return s;
+    }
     if ((s = launch_rotate_transpose_scatter(sv->C, nb, T, sv->SL3, st))) return s;
-    if ((s = launch_analysis(sv->SL3, nb * 3 * nc * 3, p0, p0, T.ana_four, T.ana_leg, T.jf_of_coef,
+    if ((s = launch_grid2shc(sv->SL3, nb * 3 * nc * 3, p0, T.ana_four, T.ana_leg, T.jf_of_coef,
                              sv->SL + v0 * (long)(3 * nc) * (3 * nc), st)))
       return s;
     (void)ng;
@@ -284,7 +309,7 @@ int run_eval(ves3d_sv* sv) {
   }
   if (!sv->sl_valid && (s = run_setup(sv))) return s;
   VES3D_CK(cudaEventRecord(sv->ev[2], st));
-  if ((s = launch_analysis(sv->F, sv->nves * 3, p0, p0, T.ana_four, T.ana_leg, T.jf_of_coef, sv->Fc, st))) return s;
+  if ((s = launch_grid2shc(sv->F, sv->nves * 3, p0, T.ana_four, T.ana_leg, T.jf_of_coef, sv->Fc, st))) return s;
   if ((s = launch_self_gemv(sv->Fc, sv->SL, sv->nves, n, sv->Vc, st))) return s;
   if ((s = launch_synthesis(sv->Vc, sv->nves * 3, p0, p0, T.syn0_leg, T.syn0_dleg, T.syn0_four, T.syn0_dfour,
                             T.blk_off, sv->Vself, nullptr, nullptr, st)))
@@ -293,9 +318,10 @@ int run_eval(ves3d_sv* sv) {
   if ((s = launch_far_density(sv->F, sv->area, sv->nves, p0, T.smooth_w0, sv->den, st))) return s;
   // events bracket the far-field kernel alone: its duration is the roofline denominator
   VES3D_CK(cudaEventRecord(sv->ev[4], st));
-  if ((s = launch_far_f64(sv->pos, sv->den, sv->nves, ngrid_(p0), nullptr, sv->Vfar, st))) return s;
+  if ((s = launch_far(sv->prec == VES3D_PREC_MIXED, sv->pos, sv->den, sv->off, sv->nves, sv->npts(), ngrid_(p0),
+                      sv->Vself, sv->V, sv->Vfar, sv->part, kFarMaxSegments, st)))
+    return s;
   VES3D_CK(cudaEventRecord(sv->ev[5], st));
-  if ((s = launch_add(sv->Vself, sv->Vfar, (long)sv->nves * 3 * ngrid_(p0), sv->V, st))) return s;
   VES3D_CK(cudaEventRecord(sv->ev[6], st));
   VES3D_CK(cudaEventSynchronize(sv->ev[6]));
   VES3D_CK(cudaEventElapsedTime(&sv->ms[1], sv->ev[2], sv->ev[3]));
@@ -378,7 +404,14 @@ int ves3d_sv_set_src_coord(ves3d_sv* sv, const double* S, long n_ves, int is_dev
   const int p0 = sv->p, ng = ngrid_(p0);
   const DevTables& T = sv->tab->d;
   if ((s = copy_in(sv->X, S, (size_t)n_ves * 3 * ng, is_device, sv->stream))) return s;
-  if ((s = launch_analysis(sv->X, n_ves * 3, p0, p0, T.ana_four, T.ana_leg, T.jf_of_coef, sv->Sx, sv->stream))) return s;
+  {
+    std::vector<long> off(n_ves + 1);
+    for (long v = 0; v <= n_ves; v++) off[v] = v * ng;
+    VES3D_CK(cudaMemcpyAsync(sv->off, off.data(), off.size() * sizeof(long), cudaMemcpyHostToDevice, sv->stream));
+    VES3D_CK(cudaStreamSynchronize(sv->stream));
+  }
+  if ((s = launch_grid2shc(sv->X, n_ves * 3, p0, T.ana_four, T.ana_leg, T.jf_of_coef, sv->Sx, sv->stream)))
+    return s;
   if ((s = launch_synthesis(sv->Sx, n_ves * 3, p0, p0, T.syn0_leg, T.syn0_dleg, T.syn0_four, T.syn0_dfour, T.blk_off,
                             sv->Vself /* scratch: filtered grid, unused */, sv->Xt, sv->Xp, sv->stream)))
     return s;
