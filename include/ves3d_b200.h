@@ -91,6 +91,43 @@ int ves3d_sv_device_buffer(ves3d_sv* sv, int which, double** ptr, size_t* n_elem
 int ves3d_sv_eval_resident(ves3d_sv* sv);
 
 /* ---------------------------------------------------------------------------
+ * Surface geometry, tractions and the globally implicit step on the context's surfaces
+ * (Surface, src/Surface.cc:212-569; InterfacialForce, src/InterfacialForce.cc:21-125;
+ * InterfacialVelocity::ImplicitMatvecPhysical / AssembleRhsVel, src/InterfacialVelocity.cc:
+ * 716-979). Fields are AxisMajor per vesicle; scalars [n_ves][Ngrid], vectors
+ * [n_ves][3][Ngrid]; the implicit unknown is [u (vector) ; sigma (scalar)].
+ * ------------------------------------------------------------------------- */
+enum ves3d_surface_op {
+  VES3D_OP_GEOMETRY = 0,     /* out [n_ves][15][Ngrid]: E,F,G (/W^2), W, n, cu, cv, H, K   */
+  VES3D_OP_GRAD = 1,         /* scalar -> vector: surface gradient                         */
+  VES3D_OP_DIV = 2,          /* vector -> scalar: surface divergence                       */
+  VES3D_OP_LIN_MEANCURV = 3, /* vector -> scalar: linearised mean curvature                */
+  VES3D_OP_LIN_BENDING = 4,  /* vector -> vector: linear bending traction (kappa)          */
+  VES3D_OP_BENDING = 5,      /* (in unused) -> vector: bending traction of the surfaces    */
+  VES3D_OP_TENSION = 6,      /* scalar -> vector: tension traction 2 sigma H n + grad sigma */
+  VES3D_OP_IMPLICIT_MATVEC = 7, /* [u;sigma] -> [u - S f ; -div S f], f = linbend(dt u) + tension(sigma) */
+  VES3D_OP_IMPLICIT_RHS = 8     /* (in unused) -> [u_inf + S f_b ; div(u_inf + S f_b)]       */
+};
+/* Parameters of the implicit step: time step, bending modulus, shear rate of the
+ * background flow u = (rate * y, 0, 0). */
+int ves3d_sv_set_implicit_params(ves3d_sv* sv, double dt, double kappa, double shear_rate);
+int ves3d_sv_surface_op(ves3d_sv* sv, int op, const double* in, double* out, int is_device);
+/* Solve the implicit system with BiCGStab in its Galerkin form (unknowns: SH coefficients
+ * of u and sigma, ImplicitApply src/InterfacialVelocity.cc:982-1052; the reference's
+ * default, params.pseudospectral = false). x0 (NULL = zero) and x are grid fields
+ * [u; sigma]; on return *tol is the relative residual of the coefficient system,
+ * *max_iter the iterations, *code the BiCGSReturn code (100 success, 101 max iterations,
+ * 102/103 breakdown, 104 NaN). */
+int ves3d_sv_implicit_solve(ves3d_sv* sv, const double* x0, double* x, double* tol, int* max_iter, int* code,
+                            int is_device);
+
+/* BiCGStab on device vectors of length n (BiCGStab::operator(), src/BiCGStab.cc:45-138,
+ * identity preconditioner); A computes y = A x on device pointers and returns 0 on success. */
+typedef int (*ves3d_matvec_fn)(void* ctx, const double* x, double* y);
+int ves3d_bicgstab_f64(ves3d_matvec_fn A, void* ctx, double* x, const double* b, size_t n, double* tol,
+                       int* max_iter, int* code, void* stream);
+
+/* ---------------------------------------------------------------------------
  * Spherical-harmonic transforms on device pointers (SHTrans, include/SHTrans.h:21-63;
  * math of SphericalHarmonics::Grid2SHC / SHC2Grid, src/SphericalHarmonics.cc:4-235).
  * ------------------------------------------------------------------------- */

@@ -12,6 +12,7 @@
 //   ref_singular_sl     SphericalHarmonics<double>::StokesSingularInteg  :863 (SL and/or DL)
 //   ref_alltoall        StokesAlltoAll (double)                    src/CPUKernels.cc:1011
 //   ref_direct_stokes   DirectStokesKernel (double)               src/CPUKernels.cc:123
+//   ref_bicgstab_dense  BiCGStab<Container, MatVec, Precond>  src/BiCGStab.cc:45-138
 //   ref_stokes_velocity_sl  the non-FMM StokesVelocity composition:
 //       u = SHC2Grid(Grid2SHC(f) . SLMatrix)                        (src/StokesVelocity.cc:385-473)
 //         + StokesAlltoAll(x, f.area.qw) - DirectStokesKernel(x, f.area, qw)
@@ -204,3 +205,50 @@ int ref_stokes_velocity_sl(const double* X, const double* f, long nves, long p, 
 }
 
 }  // extern "C"
+
+// ---- BiCGStab (include/BiCGStab.h, src/BiCGStab.cc) on a dense matrix -----------------
+#include <BiCGStab.h>
+
+namespace refbicg {
+struct RVec {
+  typedef double value_type;
+  std::vector<double> d;
+  void replicate(const RVec& o) { d.assign(o.d.size(), 0.0); }
+  size_t size() const { return d.size(); }
+};
+// out = a * x + y
+void axpy(double a, const RVec& x, const RVec& y, RVec& out) {
+  for (size_t i = 0; i < x.d.size(); i++) out.d[i] = a * x.d[i] + y.d[i];
+}
+double AlgebraicDot(const RVec& x, const RVec& y) {
+  double s = 0;
+  for (size_t i = 0; i < x.d.size(); i++) s += x.d[i] * y.d[i];
+  return s;
+}
+struct Dense {
+  const double* A;
+  long n;
+  void operator()(const RVec& x, RVec& y) const {
+    for (long i = 0; i < n; i++) {
+      double s = 0;
+      for (long j = 0; j < n; j++) s += A[i * n + j] * x.d[j];
+      y.d[i] = s;
+    }
+  }
+};
+struct Ident {
+  void operator()(const RVec& in, RVec& out) const { out.d = in.d; }
+};
+}  // namespace refbicg
+
+extern "C" int ref_bicgstab_dense(const double* A, const double* b, double* x, long n, double* tol, int* max_iter) {
+  using namespace refbicg;
+  RVec xv, bv;
+  xv.d.assign(x, x + n);
+  bv.d.assign(b, b + n);
+  Dense M = {A, n};
+  BiCGStab<RVec, Dense, Ident> solver;
+  BiCGSReturn r = solver(M, xv, bv, *max_iter, *tol, Ident());
+  std::memcpy(x, &xv.d[0], sizeof(double) * n);
+  return (int)r;
+}

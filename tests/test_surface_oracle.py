@@ -1,0 +1,67 @@
+"""CPU checks of the geometry / force / BiCGStab oracle (oracle/surface.py): analytic
+identities, and the reference's own BiCGStab class (oracle/_ref)."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle import sh, surface as su
+from tests.helpers import ellipsoid_pair, unit_sphere
+
+
+@pytest.mark.parametrize("p", [8, 12])
+def test_sphere_curvatures(p):
+    g = su.geometry(2.0 * unit_sphere(p), p)
+    assert np.abs(g["H"] - 0.5).max() < 1e-12
+    assert np.abs(g["K"] - 0.25).max() < 1e-12
+
+
+def test_surface_divergence_of_position_is_two():
+    p = 12
+    g = su.geometry(ellipsoid_pair(p), p)
+    assert np.abs(su.div(g["X"], g) - 2.0).max() < 1e-11
+
+
+def test_laplace_beltrami_eigenvalue_on_sphere():
+    p = 12
+    g = su.geometry(unit_sphere(p), p)
+    P = g["X"][0]
+    f = (P[0] * P[1] * P[2])[None]  # degree 3: eigenvalue -12
+    lap = su.div(su.grad(f, g), g)
+    assert np.abs(lap + 12.0 * f).max() < 1e-11
+    assert np.abs((su.grad(f, g) * g["n"]).sum(1)).max() < 1e-14
+
+
+def test_gauss_bonnet():
+    p = 16
+    g = su.geometry(ellipsoid_pair(p), p)
+    x = sh.legendre_nodes(p)
+    w = sh.gauss_legendre(p + 1)[1]
+    qw = np.repeat(w * np.pi / p / np.sqrt(1 - x * x), 2 * p)
+    gb = (g["K"] * g["W"] * qw).sum(axis=1) / (4 * np.pi)
+    assert np.abs(gb - 1.0).max() < 1e-5
+
+
+def test_sphere_has_no_bending_force():
+    p = 12
+    g = su.geometry(unit_sphere(p), p)
+    assert np.abs(su.bending_force(g, 0.1)).max() < 1e-10
+
+
+def test_bicgstab_matches_reference_class(ref):
+    L = ref.lib()
+    L.ref_bicgstab_dense.restype = ctypes.c_int
+    dp = ctypes.POINTER(ctypes.c_double)
+    rng = np.random.default_rng(0)
+    for n, tol in ((60, 1e-10), (120, 1e-8)):
+        A = np.eye(n) * 3 + rng.standard_normal((n, n)) * (2.0 / np.sqrt(n))
+        b = rng.standard_normal(n)
+        x = np.zeros(n)
+        t = ctypes.c_double(tol)
+        it = ctypes.c_int(300)
+        code = L.ref_bicgstab_dense(A.ctypes.data_as(dp), b.ctypes.data_as(dp), x.ctypes.data_as(dp),
+                                    ctypes.c_long(n), ctypes.byref(t), ctypes.byref(it))
+        xo, c2, i2, r2 = su.bicgstab(lambda v: A @ v, b, np.zeros(n), tol, 300)
+        assert code == c2 == 100 and it.value == i2
+        assert abs(r2 - t.value) <= 1e-3 * t.value  # residual of an iterate that rounds differently
+        assert np.abs(x - xo).max() < 1e-12

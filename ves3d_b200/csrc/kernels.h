@@ -20,7 +20,13 @@ struct DevTables {
   int mr_total = 0;  // doubles in mr; (p0+1) equal parts, one per latitude rotation t
   int *mr_off = nullptr, *perm = nullptr, *perm_off = nullptr, *pos_in_block = nullptr;
   double *sing_w = nullptr, *smooth_w0 = nullptr, *qp = nullptr, *cos_tab = nullptr, *sin_tab = nullptr;
+  double *syn0_d2leg = nullptr, *syn0_d2four = nullptr;
 };
+
+// Geometry record per point: E, F, G (divided by W^2), W, n[3], cu[3], cv[3], H, K.
+constexpr int kGeoComps = 15;
+
+typedef int (*MatVecFn)(void* ctx, const double* x, double* y);
 
 int launch_analysis(const double* in, long nfun, int pin, int pout, const double* four, const double* leg,
                     const int* jf, double* out, cudaStream_t st);
@@ -70,5 +76,28 @@ int launch_alltoall_f64(const double* pos, const double* den, long np, double* p
 // Per-surface DirectStokes with weights (cuda_stokes semantics).
 int launch_direct_stokes_f64(int src_m, int trg_m, int n, int t_head, int t_tail, const double* T,
                              const double* S, const double* D, double* U, const double* Q, cudaStream_t st);
+
+// surface geometry and tractions (geometry_kernels.cu); fields AxisMajor [nv][comp][ng]
+int launch_geometry(const double* xu, const double* xv, const double* xuu, const double* xuv, const double* xvv,
+                    long nv, int ng, double* geo, cudaStream_t st);
+int launch_grad_combine(const double* fu, const double* fv, const double* geo, long nv, int ng, double* out,
+                        cudaStream_t st);
+int launch_div_combine(const double* Fu, const double* Fv, const double* geo, long nv, int ng, double scale,
+                       double* out, cudaStream_t st);
+int launch_linH_combine(const double* duu, const double* duv, const double* dvv, const double* geo, long nv, int ng,
+                        double* out, cudaStream_t st);
+int launch_bend_combine(const double* h, const double* lap, const double* geo, long nv, int ng, double kappa,
+                        const double* add, double* out, cudaStream_t st);
+int launch_tension_combine(const double* sigma, const double* gsig, const double* geo, long nv, int ng,
+                           const double* add, double* out, cudaStream_t st);
+int launch_shear(const double* X, long nv, int ng, double rate, double* out, cudaStream_t st);
+
+// BiCGStab (bicgstab.cu)
+int dot_f64(const double* x, const double* y, long n, double* scratch, double* result, cudaStream_t st);
+int lincomb_f64(long n, double a, const double* x, double b, const double* y, double c, const double* z, double* out,
+                cudaStream_t st);
+size_t bicgstab_workspace_doubles(long n);
+int bicgstab_run(MatVecFn A, void* ctx, double* x, const double* b, long n, double* tol, int* max_iter, int* code,
+                 double* ws, cudaStream_t st);
 
 }  // namespace ves3d

@@ -263,7 +263,22 @@ void build_tables(int p0, int p1, ShTables& T) {
   }
 
   build_analysis(p0, p0, T.ana);
+  // (second-derivative Legendre table filled below, once degrees are known)
   build_synth(p0, p0, T.x0, T.syn0);
+  // P_uu = cot(theta) P_u - (n(n+1) - m^2 / sin^2 theta) P from the associated Legendre
+  // equation; P_u = syn0.dleg is the latitude derivative (-d/dtheta).
+  T.syn0_d2leg.assign((size_t)nc * (p0 + 1), 0.0);
+  T.syn0_d2four.assign((size_t)4 * p0 * p0, 0.0);
+  {
+    const double s2p = std::sqrt(2.0 * kPi);
+    for (int j = 0; j < 2 * p0; j++) {
+      for (int k = 1; k < p0; k++) {
+        T.syn0_d2four[(size_t)(2 * k - 1) * 2 * p0 + j] = -s2p * k * k * std::cos(j * k * kPi / p0);
+        T.syn0_d2four[(size_t)(2 * k) * 2 * p0 + j] = -s2p * k * k * std::sin(j * k * kPi / p0);
+      }
+      T.syn0_d2four[(size_t)(2 * p0 - 1) * 2 * p0 + j] = -s2p * p0 * p0 * std::cos(j * p0 * kPi / p0);
+    }
+  }
   build_synth(p0, p1, T.x1, T.syn1);
   // SHC2GridTranspose(., p1, p0): Fourier = MatFourier(p0,p1)^T, Legendre = MatLegendre(p0,p1)^T.
   T.synT.pin = p1;
@@ -272,6 +287,15 @@ void build_tables(int p0, int p1, ShTables& T) {
   for (int r = 0; r < 2 * p0; r++)
     for (int c = 0; c < 2 * p1; c++) T.synT.four[(size_t)c * 2 * p0 + r] = T.syn1.four[(size_t)r * 2 * p1 + c];
   T.synT.leg = T.syn1.leg;  // [Ncoef0][p1+1]
+
+  for (int c = 0; c < nc; c++) {
+    const int m = T.m_of_coef[c], n = T.n_of_coef[c];
+    for (int i = 0; i <= p0; i++) {
+      const double x = T.x0[i], sn = std::sqrt(1.0 - x * x);
+      const size_t o = (size_t)c * (p0 + 1) + i;
+      T.syn0_d2leg[o] = (x / sn) * T.syn0.dleg[o] - (n * (n + 1.0) - (double)(m * m) / (sn * sn)) * T.syn0.leg[o];
+    }
+  }
 
   // coeff_perm (:365-376)
   std::vector<std::vector<int>> perm(p0 + 1);

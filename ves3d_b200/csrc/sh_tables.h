@@ -52,6 +52,9 @@ struct ShTables {
   AnalysisTables ana;                  // Grid2SHC(p0, p0)
   SynthTables syn0;                    // SHC2Grid(p0, p0)
   SynthTables syn1;                    // SHC2Grid(p0, p1)
+  // Second derivatives at order p0 (Surface curvatures, src/Surface.cc:264-323):
+  std::vector<double> syn0_d2leg;      // [Ncoef0][p0+1] d^2/du^2 of P_n^m at the p0 nodes (u = latitude)
+  std::vector<double> syn0_d2four;     // [2p0][2p0]     d^2/dv^2 of MatFourier(p0, p0)
   // Transpose of SHC2Grid(p0, p1), used as an analysis-like map p1 grid -> p0 coefficients
   // (SHC2GridTranspose(., p1, p0), src/SphericalHarmonics.cc:238-322).
   AnalysisTables synT;

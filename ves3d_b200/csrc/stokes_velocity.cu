@@ -63,7 +63,7 @@ struct TablesOwner {
     void* ptrs[] = {d.ana_four, d.ana_leg, d.syn0_leg, d.syn0_dleg, d.syn0_four, d.syn0_dfour, d.syn1_leg,
                     d.syn1_dleg, d.syn1_four, d.syn1_dfour, d.synT_four, d.jf_of_coef, d.blk_off, d.m_of_coef,
                     d.n_of_coef, d.partner, d.is_sin, d.mr, d.mr_off, d.perm, d.perm_off, d.pos_in_block,
-                    d.sing_w, d.smooth_w0, d.qp, d.cos_tab, d.sin_tab};
+                    d.sing_w, d.smooth_w0, d.qp, d.cos_tab, d.sin_tab, d.syn0_d2leg, d.syn0_d2four};
     for (void* p : ptrs) dfree(p);
   }
   int upload(cudaStream_t st) {
@@ -98,6 +98,8 @@ struct TablesOwner {
     s |= dupload(&d.qp, h.qp, st);
     s |= dupload(&d.cos_tab, h.cos_tab, st);
     s |= dupload(&d.sin_tab, h.sin_tab, st);
+    s |= dupload(&d.syn0_d2leg, h.syn0_d2leg, st);
+    s |= dupload(&d.syn0_d2four, h.syn0_d2four, st);
     if (s) return VES3D_ERR_NOMEM;
     VES3D_CK(cudaStreamSynchronize(st));
     return VES3D_OK;
@@ -122,10 +124,16 @@ struct ves3d_sv {
   long chunk = 0;
   double *R = nullptr, *Xu = nullptr, *Xut = nullptr, *Xup = nullptr, *K = nullptr, *C = nullptr, *SL3 = nullptr;
   bool have_src = false, have_den = false, sl_valid = false, parts_valid = false;
+  // implicit step: geometry record and work fields (allocated on first use)
+  double *geo = nullptr, *wc = nullptr, *w[8] = {nullptr}, *bws = nullptr;
+  long geo_cap = 0, bws_cap = 0;
+  bool geo_valid = false;
+  double dt = 0.01, kappa = 0.05, shear = 1.0;
   cudaEvent_t ev[8] = {};
   float ms[4] = {0, 0, 0, 0};
 
   ~ves3d_sv() {
+    free_implicit();
     free_buffers();
     free_scratch();
     for (auto& e : ev)
@@ -140,6 +148,18 @@ struct ves3d_sv {
     off = nullptr;
     X = F = V = Vself = Vfar = Sx = Xt = Xp = area = pos = den = SL = Fc = Vc = part = nullptr;
     cap_ves = 0;
+  }
+  void free_implicit() {
+    dfree(geo);
+    dfree(wc);
+    for (auto& q : w) {
+      dfree(q);
+      q = nullptr;
+    }
+    dfree(bws);
+    geo = wc = bws = nullptr;
+    geo_cap = bws_cap = 0;
+    geo_valid = false;
   }
   void free_scratch() {
     double* ps[] = {R, Xu, Xut, Xup, K, C, SL3};
@@ -423,6 +443,7 @@ int ves3d_sv_set_src_coord(ves3d_sv* sv, const double* S, long n_ves, int is_dev
   sv->have_den = false;
   sv->sl_valid = false;
   sv->parts_valid = false;
+  sv->geo_valid = false;
   return VES3D_OK;
 }
 
@@ -674,6 +695,345 @@ void ves3d_interaction_free(void** ctx) {
   if (ws->st) cudaStreamDestroy(ws->st);
   delete ws;
   *ctx = nullptr;
+}
+
+}  // extern "C"
+
+// ======================================================================================
+// Surface geometry, tractions, implicit step
+// ======================================================================================
+namespace {
+
+int ensure_implicit_buffers(ves3d_sv* sv) {
+  if (sv->geo_cap >= sv->nves) return VES3D_OK;
+  sv->free_implicit();
+  const size_t ng = ngrid_(sv->p), nc = ncoef_(sv->p), nv = sv->nves;
+  int s = 0;
+  s |= dalloc(&sv->geo, nv * kGeoComps * ng);
+  s |= dalloc(&sv->wc, nv * 3 * nc);
+  for (auto& q : sv->w) s |= dalloc(&q, nv * 3 * ng);
+  if (s) {
+    sv->free_implicit();
+    return s;
+  }
+  sv->geo_cap = sv->nves;
+  return VES3D_OK;
+}
+
+// coefficient derivatives at order p: which = 0 -> (value, v, u); 1 -> (u, uv, uu); 2 -> vv
+int synth_d(ves3d_sv* sv, const double* coef, long nfun, int which, double* a, double* b, double* c) {
+  const DevTables& T = sv->tab->d;
+  const int p = sv->p;
+  if (which == 0)
+    return launch_synthesis(coef, nfun, p, p, T.syn0_leg, T.syn0_dleg, T.syn0_four, T.syn0_dfour, T.blk_off, a, b, c,
+                            sv->stream);
+  if (which == 1)
+    return launch_synthesis(coef, nfun, p, p, T.syn0_dleg, T.syn0_d2leg, T.syn0_four, T.syn0_dfour, T.blk_off, a, b,
+                            c, sv->stream);
+  return launch_synthesis(coef, nfun, p, p, T.syn0_leg, T.syn0_leg, T.syn0_d2four, T.syn0_d2four, T.blk_off, a,
+                          nullptr, nullptr, sv->stream);
+}
+
+int grid2shc_p(ves3d_sv* sv, const double* in, long nfun, double* out) {
+  const DevTables& T = sv->tab->d;
+  return launch_grid2shc(in, nfun, sv->p, T.ana_four, T.ana_leg, T.jf_of_coef, out, sv->stream);
+}
+
+int ensure_geometry(ves3d_sv* sv) {
+  int s;
+  if ((s = ensure_implicit_buffers(sv))) return s;
+  if (sv->geo_valid) return VES3D_OK;
+  const long nv = sv->nves, nf = 3 * nv;
+  const int ng = ngrid_(sv->p);
+  double** w = sv->w;
+  // w0 value, w1 v, w2 u, w3 (u again), w4 uv, w5 uu, w6 vv
+  if ((s = synth_d(sv, sv->Sx, nf, 0, w[0], w[1], w[2]))) return s;
+  if ((s = synth_d(sv, sv->Sx, nf, 1, w[3], w[4], w[5]))) return s;
+  if ((s = synth_d(sv, sv->Sx, nf, 2, w[6], nullptr, nullptr))) return s;
+  if ((s = launch_geometry(w[2], w[1], w[5], w[4], w[6], nv, ng, sv->geo, sv->stream))) return s;
+  sv->geo_valid = true;
+  return VES3D_OK;
+}
+
+// grad of a scalar field (in [nv][ng]) -> out [nv][3][ng]; uses w6, w7 and wc
+int op_grad(ves3d_sv* sv, const double* in, double* out) {
+  int s;
+  const long nv = sv->nves;
+  const int ng = ngrid_(sv->p);
+  double *a = sv->w[6], *b = sv->w[7];
+  if ((s = grid2shc_p(sv, in, nv, sv->wc))) return s;
+  // value into out (overwritten below), v-derivative into a, u-derivative into b
+  if ((s = synth_d(sv, sv->wc, nv, 0, out, a, b))) return s;
+  return launch_grad_combine(b, a, sv->geo, nv, ng, out, sv->stream);
+}
+
+// div of a vector field (in [nv][3][ng]) -> out [nv][ng] times scale; uses w5, w6, w7, wc
+int op_div(ves3d_sv* sv, const double* in, double* out, double scale) {
+  int s;
+  const long nv = sv->nves;
+  const int ng = ngrid_(sv->p);
+  if ((s = grid2shc_p(sv, in, 3 * nv, sv->wc))) return s;
+  if ((s = synth_d(sv, sv->wc, 3 * nv, 0, sv->w[5], sv->w[6], sv->w[7]))) return s;
+  return launch_div_combine(sv->w[7], sv->w[6], sv->geo, nv, ng, scale, out, sv->stream);
+}
+
+// linearised mean curvature of a displacement field; uses w4..w7, wc
+int op_linH(ves3d_sv* sv, const double* in, double* out) {
+  int s;
+  const long nv = sv->nves;
+  const int ng = ngrid_(sv->p);
+  if ((s = grid2shc_p(sv, in, 3 * nv, sv->wc))) return s;
+  if ((s = synth_d(sv, sv->wc, 3 * nv, 1, sv->w[4], sv->w[5], sv->w[6]))) return s;  // u, uv, uu
+  if ((s = synth_d(sv, sv->wc, 3 * nv, 2, sv->w[7], nullptr, nullptr))) return s;    // vv
+  return launch_linH_combine(sv->w[6], sv->w[5], sv->w[7], sv->geo, nv, ng, out, sv->stream);
+}
+
+// bending traction of a scalar h (the mean curvature or its linearisation), added to add.
+// scratch: w3 (gradient), w2 (Laplacian)
+int op_bend_of(ves3d_sv* sv, const double* h, const double* add, double* out) {
+  int s;
+  const long nv = sv->nves;
+  const int ng = ngrid_(sv->p);
+  if ((s = op_grad(sv, h, sv->w[3]))) return s;
+  if ((s = op_div(sv, sv->w[3], sv->w[2], 1.0))) return s;
+  return launch_bend_combine(h, sv->w[2], sv->geo, nv, ng, sv->kappa, add, out, sv->stream);
+}
+
+// tension traction of sigma added to add; scratch w3
+int op_tension(ves3d_sv* sv, const double* sigma, const double* add, double* out) {
+  int s;
+  const long nv = sv->nves;
+  const int ng = ngrid_(sv->p);
+  if ((s = op_grad(sv, sigma, sv->w[3]))) return s;
+  return launch_tension_combine(sigma, sv->w[3], sv->geo, nv, ng, add, out, sv->stream);
+}
+
+// Stokes single layer of a device density f (AxisMajor) -> out (device), through the
+// context's cached self matrices and far field.
+int stokes_apply(ves3d_sv* sv, const double* f, double* out) {
+  int s;
+  const size_t n = (size_t)sv->npts() * 3;
+  VES3D_CK(cudaMemcpyAsync(sv->F, f, n * sizeof(double), cudaMemcpyDeviceToDevice, sv->stream));
+  sv->have_den = true;
+  if ((s = run_eval(sv))) return s;
+  VES3D_CK(cudaMemcpyAsync(out, sv->V, n * sizeof(double), cudaMemcpyDeviceToDevice, sv->stream));
+  return VES3D_OK;
+}
+
+// work vectors of the implicit operator (beyond w[]): f, Sf [3N], h [N], y [3N], and two
+// grid-space [u; sigma] vectors g1, g2 [4N] for the Galerkin form.
+struct ImplicitWork {
+  double *f, *Sf, *h, *y, *g1, *g2;
+};
+
+long sh_unknowns(const ves3d_sv* sv) { return 4L * sv->nves * ncoef_(sv->p); }
+
+int implicit_work(ves3d_sv* sv, ImplicitWork& iw) {
+  const size_t N = sv->npts();
+  const size_t need = bicgstab_workspace_doubles(sh_unknowns(sv)) + 3 * N + 3 * N + N + 3 * N + 8 * N;
+  if (sv->bws_cap < (long)need) {
+    dfree(sv->bws);
+    sv->bws = nullptr;
+    sv->bws_cap = 0;
+    int s = dalloc(&sv->bws, need);
+    if (s) return s;
+    sv->bws_cap = (long)need;
+  }
+  double* base = sv->bws + bicgstab_workspace_doubles(sh_unknowns(sv));
+  iw.f = base;
+  iw.Sf = base + 3 * N;
+  iw.h = base + 6 * N;
+  iw.y = base + 7 * N;
+  iw.g1 = base + 10 * N;
+  iw.g2 = base + 14 * N;
+  return VES3D_OK;
+}
+
+// [u; sigma] -> [u - S f ; -div S f],  f = linbend(dt u) + tension(sigma)
+int implicit_matvec(ves3d_sv* sv, const double* x, double* y) {
+  int s;
+  ImplicitWork iw;
+  if ((s = implicit_work(sv, iw))) return s;
+  const long N = sv->npts();
+  const double* u = x;
+  const double* sig = x + 3 * N;
+  if ((s = lincomb_f64(3 * N, sv->dt, u, 0.0, u, 0.0, nullptr, iw.y, sv->stream))) return s;  // y = dt u
+  if ((s = op_linH(sv, iw.y, iw.h))) return s;
+  if ((s = op_bend_of(sv, iw.h, nullptr, iw.f))) return s;
+  if ((s = op_tension(sv, sig, iw.f, iw.f))) return s;
+  if ((s = stokes_apply(sv, iw.f, iw.Sf))) return s;
+  if ((s = lincomb_f64(3 * N, 1.0, u, -1.0, iw.Sf, 0.0, nullptr, y, sv->stream))) return s;
+  return op_div(sv, iw.Sf, y + 3 * N, -1.0);
+}
+
+// Galerkin maps: SH coefficients [u (3 nv fun); sigma (nv fun)] <-> grid [u; sigma]
+int coef_to_grid(ves3d_sv* sv, const double* c, double* g) {
+  const long nv = sv->nves, N = sv->npts();
+  const long nc = ncoef_(sv->p);
+  int s = synth_d(sv, c, 3 * nv, 0, g, nullptr, nullptr);
+  if (s) return s;
+  return synth_d(sv, c + 3 * nv * nc, nv, 0, g + 3 * N, nullptr, nullptr);
+}
+
+int grid_to_coef(ves3d_sv* sv, const double* g, double* c) {
+  const long nv = sv->nves, N = sv->npts();
+  const long nc = ncoef_(sv->p);
+  int s = grid2shc_p(sv, g, 3 * nv, c);
+  if (s) return s;
+  return grid2shc_p(sv, g + 3 * N, nv, c + 3 * nv * nc);
+}
+
+// ImplicitApply, Galerkin form (src/InterfacialVelocity.cc:982-1052)
+int implicit_matvec_sh(ves3d_sv* sv, const double* c, double* y) {
+  int s;
+  ImplicitWork iw;
+  if ((s = implicit_work(sv, iw))) return s;
+  if ((s = coef_to_grid(sv, c, iw.g1))) return s;
+  if ((s = implicit_matvec(sv, iw.g1, iw.g2))) return s;
+  return grid_to_coef(sv, iw.g2, y);
+}
+
+int implicit_rhs(ves3d_sv* sv, double* y) {
+  int s;
+  ImplicitWork iw;
+  if ((s = implicit_work(sv, iw))) return s;
+  const long N = sv->npts();
+  const int ng = ngrid_(sv->p);
+  // f_b = bending traction of the mean curvature H (geo component 13)
+  double* H = iw.h;
+  for (long v = 0; v < sv->nves; v++)
+    VES3D_CK(cudaMemcpyAsync(H + v * ng, sv->geo + (v * kGeoComps + 13) * (long)ng, ng * sizeof(double),
+                             cudaMemcpyDeviceToDevice, sv->stream));
+  if ((s = op_bend_of(sv, H, nullptr, iw.f))) return s;
+  if ((s = stokes_apply(sv, iw.f, iw.Sf))) return s;
+  if ((s = launch_shear(sv->X, sv->nves, ng, sv->shear, y, sv->stream))) return s;
+  if ((s = lincomb_f64(3 * N, 1.0, y, 1.0, iw.Sf, 0.0, nullptr, y, sv->stream))) return s;
+  return op_div(sv, y, y + 3 * N, 1.0);
+}
+
+int implicit_matvec_cb(void* ctx, const double* x, double* y) { return implicit_matvec_sh((ves3d_sv*)ctx, x, y); }
+
+}  // namespace
+
+extern "C" {
+
+int ves3d_sv_set_implicit_params(ves3d_sv* sv, double dt, double kappa, double shear_rate) {
+  int s = check_sv(sv);
+  if (s) return s;
+  VES3D_ARG(dt > 0 && kappa >= 0, "dt must be > 0 and kappa >= 0");
+  sv->dt = dt;
+  sv->kappa = kappa;
+  sv->shear = shear_rate;
+  return VES3D_OK;
+}
+
+int ves3d_sv_surface_op(ves3d_sv* sv, int op, const double* in, double* out, int is_device) {
+  int s = check_sv(sv);
+  if (s) return s;
+  VES3D_ARG(out != nullptr, "out is null");
+  if (!sv->have_src) {
+    set_error("no surfaces set");
+    return VES3D_ERR_STATE;
+  }
+  if ((s = ensure_geometry(sv))) return s;
+  const long N = sv->npts();
+  const int ng = ngrid_(sv->p);
+  size_t nin = 0, nout = 0;
+  switch (op) {
+    case VES3D_OP_GEOMETRY: nout = (size_t)sv->nves * kGeoComps * ng; break;
+    case VES3D_OP_GRAD: nin = N; nout = 3 * N; break;
+    case VES3D_OP_DIV: nin = 3 * N; nout = N; break;
+    case VES3D_OP_LIN_MEANCURV: nin = 3 * N; nout = N; break;
+    case VES3D_OP_LIN_BENDING: nin = 3 * N; nout = 3 * N; break;
+    case VES3D_OP_BENDING: nout = 3 * N; break;
+    case VES3D_OP_TENSION: nin = N; nout = 3 * N; break;
+    case VES3D_OP_IMPLICIT_MATVEC: nin = 4 * N; nout = 4 * N; break;
+    case VES3D_OP_IMPLICIT_RHS: nout = 4 * N; break;
+    default: VES3D_ARG(false, "unknown surface op");
+  }
+  VES3D_ARG(nin == 0 || in != nullptr, "in is null");
+  double *din = nullptr, *dout = nullptr;
+  int st = VES3D_OK;
+  if (nin && (st = dalloc(&din, nin))) return st;
+  if ((st = dalloc(&dout, nout))) {
+    dfree(din);
+    return st;
+  }
+  if (nin) st = copy_in(din, in, nin, is_device, sv->stream);
+  ImplicitWork iw;
+  if (!st) st = implicit_work(sv, iw);
+  if (!st) {
+    switch (op) {
+      case VES3D_OP_GEOMETRY:
+        st = cuda_status(cudaMemcpyAsync(dout, sv->geo, nout * sizeof(double), cudaMemcpyDeviceToDevice, sv->stream),
+                         "copy", __FILE__, __LINE__);
+        break;
+      case VES3D_OP_GRAD: st = op_grad(sv, din, dout); break;
+      case VES3D_OP_DIV: st = op_div(sv, din, dout, 1.0); break;
+      case VES3D_OP_LIN_MEANCURV: st = op_linH(sv, din, dout); break;
+      case VES3D_OP_LIN_BENDING:
+        st = op_linH(sv, din, iw.h);
+        if (!st) st = op_bend_of(sv, iw.h, nullptr, dout);
+        break;
+      case VES3D_OP_BENDING:
+        for (long v = 0; v < sv->nves && !st; v++)
+          st = cuda_status(cudaMemcpyAsync(iw.h + v * ng, sv->geo + (v * kGeoComps + 13) * (long)ng,
+                                           ng * sizeof(double), cudaMemcpyDeviceToDevice, sv->stream),
+                           "copy", __FILE__, __LINE__);
+        if (!st) st = op_bend_of(sv, iw.h, nullptr, dout);
+        break;
+      case VES3D_OP_TENSION: st = op_tension(sv, din, nullptr, dout); break;
+      case VES3D_OP_IMPLICIT_MATVEC: st = implicit_matvec(sv, din, dout); break;
+      case VES3D_OP_IMPLICIT_RHS: st = implicit_rhs(sv, dout); break;
+    }
+  }
+  if (!st) st = copy_out(out, dout, nout, is_device, sv->stream);
+  cudaStreamSynchronize(sv->stream);
+  dfree(din);
+  dfree(dout);
+  return st;
+}
+
+int ves3d_sv_implicit_solve(ves3d_sv* sv, const double* x0, double* x, double* tol, int* max_iter, int* code,
+                            int is_device) {
+  int s = check_sv(sv);
+  if (s) return s;
+  VES3D_ARG(x && tol && max_iter && code, "null argument");
+  if (!sv->have_src) {
+    set_error("no surfaces set");
+    return VES3D_ERR_STATE;
+  }
+  if ((s = ensure_geometry(sv))) return s;
+  ImplicitWork iw;
+  if ((s = implicit_work(sv, iw))) return s;
+  const long ng4 = 4 * sv->npts(), nsh = sh_unknowns(sv);
+  double *dc = nullptr, *db = nullptr, *dg = nullptr;
+  if ((s = dalloc(&dc, nsh))) return s;
+  if ((s = dalloc(&db, nsh))) {
+    dfree(dc);
+    return s;
+  }
+  if ((s = dalloc(&dg, ng4))) {
+    dfree(dc);
+    dfree(db);
+    return s;
+  }
+  if (x0) {
+    s = copy_in(dg, x0, ng4, is_device, sv->stream);
+    if (!s) s = grid_to_coef(sv, dg, dc);
+  } else {
+    s = cuda_status(cudaMemsetAsync(dc, 0, nsh * sizeof(double), sv->stream), "memset", __FILE__, __LINE__);
+  }
+  if (!s) s = implicit_rhs(sv, dg);
+  if (!s) s = grid_to_coef(sv, dg, db);
+  if (!s) s = bicgstab_run(implicit_matvec_cb, sv, dc, db, nsh, tol, max_iter, code, sv->bws, sv->stream);
+  if (!s) s = coef_to_grid(sv, dc, dg);
+  if (!s) s = copy_out(x, dg, ng4, is_device, sv->stream);
+  cudaStreamSynchronize(sv->stream);
+  dfree(dc);
+  dfree(db);
+  dfree(dg);
+  return s;
 }
 
 }  // extern "C"

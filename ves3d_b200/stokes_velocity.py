@@ -134,3 +134,40 @@ class StokesVelocity:
 
     def set_stream(self, stream_ptr):
         check(lib().ves3d_sv_set_stream(self._h, stream_ptr), "set_stream")
+
+    # --- surface geometry, tractions, implicit step ---------------------------------------
+    OPS = {"geometry": 0, "grad": 1, "div": 2, "lin_mean_curv": 3, "lin_bending": 4, "bending": 5,
+           "tension": 6, "implicit_matvec": 7, "implicit_rhs": 8}
+
+    def set_implicit_params(self, dt, kappa, shear_rate):
+        check(lib().ves3d_sv_set_implicit_params(self._h, float(dt), float(kappa), float(shear_rate)),
+              "set_implicit_params")
+
+    def surface_op(self, op, field=None):
+        ng = ngrid(self.sh_order)
+        N = self.n_ves * ng
+        sizes = {0: 15 * N, 1: 3 * N, 2: N, 3: N, 4: 3 * N, 5: 3 * N, 6: 3 * N, 7: 4 * N, 8: 4 * N}
+        code = self.OPS[op] if isinstance(op, str) else int(op)
+        out = np.empty(sizes[code])
+        if field is None:
+            ptr = None
+        else:
+            field = np.ascontiguousarray(field, dtype=np.float64).reshape(-1)
+            ptr = field.ctypes.data
+        check(lib().ves3d_sv_surface_op(self._h, code, ptr, out.ctypes.data, 0), f"surface_op({op})")
+        return out
+
+    def implicit_solve(self, x0=None, tol=1e-8, max_iter=200):
+        """Solve the implicit system for [u; sigma]; returns (x, iterations, relres, code)."""
+        N = self.n_ves * ngrid(self.sh_order)
+        x = np.empty(4 * N)
+        t = ctypes.c_double(tol)
+        it = ctypes.c_int(max_iter)
+        code = ctypes.c_int(0)
+        p0 = None
+        if x0 is not None:
+            x0 = np.ascontiguousarray(x0, dtype=np.float64).reshape(-1)
+            p0 = x0.ctypes.data
+        check(lib().ves3d_sv_implicit_solve(self._h, p0, x.ctypes.data, ctypes.byref(t), ctypes.byref(it),
+                                            ctypes.byref(code), 0), "implicit_solve")
+        return x, it.value, t.value, code.value
