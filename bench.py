@@ -40,6 +40,7 @@ def parse():
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-implicit", action="store_true", help="skip the implicit-step measurement")
     return ap.parse_args()
 
 
@@ -269,6 +270,48 @@ def sampled_error_vs_oracle(X, f, p, vel, nves_check=2, n_targets=256, seed=11):
     return worst
 
 
+IMPLICIT = dict(workload="c4_256ves_p16", dt=0.01, kappa=0.05, shear_rate=1.0, tol=1e-8, max_iter=500)
+
+
+def implicit_step_measurement(precision, local, stream):
+    """Two globally implicit steps of the 256-vesicle p=16 suspension in shear flow: the
+    first from a zero initial guess, the second (after x += dt u) from the previous
+    step's solution. Device time per step: geometry + self-matrix build + right-hand side
+    + BiCGStab (Galerkin form) to the tolerance."""
+    import torch
+    from ves3d_b200 import workloads
+    from ves3d_b200.stokes_velocity import StokesVelocity
+    X, _, p = workloads.make(IMPLICIT["workload"])
+    ng = 2 * p * (p + 1)
+    nves = X.size // (3 * ng)
+    N = nves * ng
+    sv = StokesVelocity(p, 2 * p, precision=precision, device=local)
+    sv.set_stream(stream.cuda_stream)
+    sv.set_implicit_params(IMPLICIT["dt"], IMPLICIT["kappa"], IMPLICIT["shear_rate"])
+    out = []
+    guess = None
+    for label in ("zero guess", "previous-step guess"):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sv.SetSrcCoord(X)
+        x, it, relres, code = sv.implicit_solve(x0=guess, tol=IMPLICIT["tol"], max_iter=IMPLICIT["max_iter"])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        rec = {"guess": label, "ms": e0.elapsed_time(e1), "bicgstab_iterations": it, "relres": relres, "code": code}
+        if precision == "mixed":
+            st = sv.solver_stats()
+            rec["fp64_residual_evaluations"] = st["outer"]
+        out.append(rec)
+        X = X + IMPLICIT["dt"] * x[:3 * N]
+        guess = x
+    sv.close()
+    return {"workload": f"{IMPLICIT['workload']}: {nves} vesicles p={p} ({N} points), shear u=(y,0,0), "
+                        f"kappa={IMPLICIT['kappa']}, dt={IMPLICIT['dt']}, BiCGStab tol {IMPLICIT['tol']}, "
+                        "Galerkin form", "steps": out}
+
+
 def run_ours(args, world, rank, local):
     import torch
     from ves3d_b200 import _lib, workloads
@@ -401,6 +444,8 @@ def run_ours(args, world, rank, local):
             "clocks": clocks,
             "peaks_tflops": {"fp64_fma": peak64, "fp32_fma": peak32},
         }
+        if not args.no_implicit:
+            result["implicit_step"] = implicit_step_measurement(args.precision, local, stream)
         if world == 1 and not args.no_cpu_baseline:
             cb = cpu_reference_rate(X, f, p)
             result["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}

@@ -121,6 +121,12 @@ int ves3d_sv_surface_op(ves3d_sv* sv, int op, const double* in, double* out, int
 int ves3d_sv_implicit_solve(ves3d_sv* sv, const double* x0, double* x, double* tol, int* max_iter, int* code,
                             int is_device);
 
+/* Iterations of the last implicit solve in the mixed form: FP64 residual evaluations of
+ * the outer refinement loop, and inner (mixed-operator) BiCGStab iterations. In the mixed
+ * form the solve is an iterative refinement: outer residuals with the FP64 operator,
+ * corrections by BiCGStab on the mixed operator. */
+int ves3d_sv_solver_stats(ves3d_sv* sv, int* outer, int* inner);
+
 /* BiCGStab on device vectors of length n (BiCGStab::operator(), src/BiCGStab.cc:45-138,
  * identity preconditioner); A computes y = A x on device pointers and returns 0 on success. */
 typedef int (*ves3d_matvec_fn)(void* ctx, const double* x, double* y);

@@ -90,3 +90,24 @@ def test_sphere_geometry_gpu():
         g = sv.surface_op("geometry").reshape(1, 15, -1)
     assert np.abs(g[0, 13] - 0.5).max() < 1e-12
     assert np.abs(g[0, 14] - 0.25).max() < 1e-12
+
+
+def test_mixed_implicit_solve_refines_to_fp64_residual():
+    """Mixed form: iterative refinement with FP64 residuals reaches the tolerance and
+    agrees with the FP64 solve on the velocity."""
+    X, _ = small_suspension(2, P, 43, spacing=2.8)
+    sols = {}
+    for prec in ("fp64", "mixed"):
+        with StokesVelocity(P, precision=prec) as sv:
+            sv.SetSrcCoord(X)
+            sv.set_implicit_params(DT, KAPPA, RATE)
+            x, it, relres, code = sv.implicit_solve(tol=1e-8, max_iter=600)
+            assert code == 100, (prec, it, relres)
+            assert relres < 1e-8
+            sols[prec] = x
+    step = su.ImplicitStep(X, P, KAPPA, DT, RATE)
+    b = step.to_coef(step.rhs())
+    r = b - step.matvec_sh(step.to_coef(sols["mixed"]))
+    assert np.linalg.norm(r) / np.linalg.norm(b) < 2e-8
+    nu = 3 * X.size // 3
+    assert rel_err(sols["mixed"][:nu], sols["fp64"][:nu]) < 1e-6

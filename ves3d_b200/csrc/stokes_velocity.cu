@@ -10,6 +10,8 @@
 //   eval         : Fc = Grid2SHC(f); Vc = Fc . SL; Vself = SHC2Grid(Vc)
 //                  (src/StokesVelocity.cc:385-473); den = f * area * qw;
 //                  vel = Vself + sum over other vesicles (exact all-pairs far field).
+#include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdlib>
 #include <cstring>
@@ -129,6 +131,8 @@ struct ves3d_sv {
   long geo_cap = 0, bws_cap = 0;
   bool geo_valid = false;
   double dt = 0.01, kappa = 0.05, shear = 1.0;
+  int far_force_fp64 = 0;      // 1: evaluate the far field in FP64 even in the mixed form
+  int ir_outer = 0, ir_inner = 0;  // last mixed solve: outer refinements, inner iterations
   cudaEvent_t ev[8] = {};
   float ms[4] = {0, 0, 0, 0};
 
@@ -338,7 +342,7 @@ int run_eval(ves3d_sv* sv) {
   if ((s = launch_far_density(sv->F, sv->area, sv->nves, p0, T.smooth_w0, sv->den, st))) return s;
   // events bracket the far-field kernel alone: its duration is the roofline denominator
   VES3D_CK(cudaEventRecord(sv->ev[4], st));
-  if ((s = launch_far(sv->prec == VES3D_PREC_MIXED, sv->pos, sv->den, sv->off, sv->nves, sv->npts(), ngrid_(p0),
+  if ((s = launch_far(sv->prec == VES3D_PREC_MIXED && !sv->far_force_fp64, sv->pos, sv->den, sv->off, sv->nves, sv->npts(), ngrid_(p0),
                       sv->Vself, sv->V, sv->Vfar, sv->part, kFarMaxSegments, st)))
     return s;
   VES3D_CK(cudaEventRecord(sv->ev[5], st));
@@ -913,9 +917,90 @@ int implicit_rhs(ves3d_sv* sv, double* y) {
 
 int implicit_matvec_cb(void* ctx, const double* x, double* y) { return implicit_matvec_sh((ves3d_sv*)ctx, x, y); }
 
+int implicit_matvec_fp64_cb(void* ctx, const double* x, double* y) {
+  ves3d_sv* sv = (ves3d_sv*)ctx;
+  sv->far_force_fp64 = 1;
+  int s = implicit_matvec_sh(sv, x, y);
+  sv->far_force_fp64 = 0;
+  return s;
+}
+
+// Mixed-precision iterative refinement: outer residuals r = b - A x with the FP64
+// operator; inner BiCGStab with the mixed operator on A d = r to a relative tolerance of
+// 1e-2 (at most 150 iterations per correction); x += d. A correction that does not reduce the FP64 residual is undone and
+// the remaining work falls back to FP64 inner solves. *tol in: target relative residual;
+// out: achieved. *max_iter in: bound on inner iterations in total; out: inner iterations
+// used (FP64 matvecs of the outer loop are reported through ves3d_sv::ir_outer).
+int mixed_refinement(ves3d_sv* sv, double* x, const double* b, long n, double* tol, int* max_iter, int* code) {
+  int s;
+  const double target = *tol;
+  const int budget = *max_iter;
+  double *r = nullptr, *d = nullptr, *ax = nullptr, *ws = nullptr;
+  if ((s = dalloc(&r, n))) return s;
+  if ((s = dalloc(&d, n)) || (s = dalloc(&ax, n)) || (s = dalloc(&ws, bicgstab_workspace_doubles(n)))) {
+    dfree(r); dfree(d); dfree(ax);
+    return s;
+  }
+  double nb2 = 0;
+  s = dot_f64(b, b, n, ws + 8 * n, &nb2, sv->stream);
+  const double normb = nb2 > 0 ? std::sqrt(nb2) : 1.0;
+  int used = 0, outer = 0;
+  bool fp64_inner = false;
+  double relres = 1e300;
+  *code = 101;
+  while (!s && outer < 30) {
+    // FP64 residual
+    if ((s = implicit_matvec_fp64_cb(sv, x, ax))) break;
+    if ((s = lincomb_f64(n, 1.0, b, -1.0, ax, 0.0, nullptr, r, sv->stream))) break;
+    double rr = 0;
+    if ((s = dot_f64(r, r, n, ws + 8 * n, &rr, sv->stream))) break;
+    const double cur = std::sqrt(rr) / normb;
+    outer++;
+    if (cur > relres) {
+      // the last correction made things worse: undo it, continue with FP64 inner solves
+      if ((s = lincomb_f64(n, 1.0, x, -1.0, d, 0.0, nullptr, x, sv->stream))) break;
+      fp64_inner = true;
+      continue;
+    }
+    relres = cur;
+    if (relres < target) {
+      *code = 100;
+      break;
+    }
+    if (used >= budget) break;
+    // inner solve for the correction, from zero, to 1e-2 of the current residual (or the
+    // target): the FP32 far field is accurate to ~1e-5 for dipole-dominated densities, so
+    // each correction only has to make a modest, reliable reduction
+    VES3D_CK(cudaMemsetAsync(d, 0, n * sizeof(double), sv->stream));
+    double itol = std::max(1e-2, 0.5 * target / relres);
+    int imax = std::min(budget - used, 150), icode = 0;
+    if ((s = bicgstab_run(fp64_inner ? implicit_matvec_fp64_cb : implicit_matvec_cb, sv, d, r, n, &itol, &imax,
+                          &icode, ws, sv->stream)))
+      break;
+    used += imax;
+    if ((s = lincomb_f64(n, 1.0, x, 1.0, d, 0.0, nullptr, x, sv->stream))) break;
+  }
+  *tol = relres;
+  *max_iter = used;
+  sv->ir_outer = outer;
+  sv->ir_inner = used;
+  dfree(r);
+  dfree(d);
+  dfree(ax);
+  dfree(ws);
+  return s;
+}
+
 }  // namespace
 
 extern "C" {
+
+int ves3d_sv_solver_stats(ves3d_sv* sv, int* outer, int* inner) {
+  VES3D_ARG(sv && outer && inner, "null argument");
+  *outer = sv->ir_outer;
+  *inner = sv->ir_inner;
+  return VES3D_OK;
+}
 
 int ves3d_sv_set_implicit_params(ves3d_sv* sv, double dt, double kappa, double shear_rate) {
   int s = check_sv(sv);
@@ -1024,9 +1109,17 @@ int ves3d_sv_implicit_solve(ves3d_sv* sv, const double* x0, double* x, double* t
   } else {
     s = cuda_status(cudaMemsetAsync(dc, 0, nsh * sizeof(double), sv->stream), "memset", __FILE__, __LINE__);
   }
+  // right-hand side always with the FP64 far field
+  sv->far_force_fp64 = 1;
   if (!s) s = implicit_rhs(sv, dg);
+  sv->far_force_fp64 = 0;
   if (!s) s = grid_to_coef(sv, dg, db);
-  if (!s) s = bicgstab_run(implicit_matvec_cb, sv, dc, db, nsh, tol, max_iter, code, sv->bws, sv->stream);
+  if (!s) {
+    if (sv->prec == VES3D_PREC_FP64)
+      s = bicgstab_run(implicit_matvec_cb, sv, dc, db, nsh, tol, max_iter, code, sv->bws, sv->stream);
+    else
+      s = mixed_refinement(sv, dc, db, nsh, tol, max_iter, code);
+  }
   if (!s) s = coef_to_grid(sv, dc, dg);
   if (!s) s = copy_out(x, dg, ng4, is_device, sv->stream);
   cudaStreamSynchronize(sv->stream);

@@ -157,6 +157,11 @@ class StokesVelocity:
         check(lib().ves3d_sv_surface_op(self._h, code, ptr, out.ctypes.data, 0), f"surface_op({op})")
         return out
 
+    def solver_stats(self):
+        o, i = ctypes.c_int(0), ctypes.c_int(0)
+        check(lib().ves3d_sv_solver_stats(self._h, ctypes.byref(o), ctypes.byref(i)), "solver_stats")
+        return {"outer": o.value, "inner": i.value}
+
     def implicit_solve(self, x0=None, tol=1e-8, max_iter=200):
         """Solve the implicit system for [u; sigma]; returns (x, iterations, relres, code)."""
         N = self.n_ves * ngrid(self.sh_order)

@@ -57,8 +57,10 @@ def shape(p, center, semi_axes=(1.0, 1.0, 1.0), scale=1.0, deg=4, amp=0.05, rng=
 
 
 def lattice_centers(n, spacing):
-    g = np.arange(n) * spacing
-    return np.stack(np.meshgrid(g, g, g, indexing="ij"), axis=-1).reshape(-1, 3)
+    """Centres of an n x n x n (or nx x ny x nz for a tuple n) lattice."""
+    nx, ny, nz = (n, n, n) if np.isscalar(n) else n
+    axes = [np.arange(k) * spacing for k in (nx, ny, nz)]
+    return np.stack(np.meshgrid(*axes, indexing="ij"), axis=-1).reshape(-1, 3)
 
 
 def suspension(nves_side, p, spacing, semi_axes=(1.0, 1.0, 1.0), deg=4, amp=0.05, jitter=0.0, min_sep=0.0,
@@ -95,7 +97,11 @@ CONFIGS = {
     # 512 vesicles, p=16, unit spheres + deg<=6 amp 0.1, jittered 8x8x8 lattice spacing 2.5, min sep 0.2.
     "c2_512ves_p16": dict(nves_side=8, p=16, spacing=2.5, semi_axes=(1.0, 1.0, 1.0), deg=6, amp=0.1, jitter=0.15,
                           min_sep=0.2, seed=1001),
-    # 64-vesicle cut of the above (4x4x4 lattice): the small case for profiler captures.
+    # 256 vesicles, p=16, spheres + deg<=4 amp 0.05 on a jittered 8x8x4 lattice: the
+    # implicit-step workload (shear u = (y, 0, 0), bending modulus 0.05, dt 0.01).
+    "c4_256ves_p16": dict(nves_side=(8, 8, 4), p=16, spacing=2.5, semi_axes=(1.0, 1.0, 1.0), deg=4, amp=0.05,
+                          jitter=0.15, min_sep=0.2, seed=1003),
+    # 64-vesicle cut of the C2 suspension (4x4x4 lattice): the small case for profiler captures.
     "c2s_64ves_p16": dict(nves_side=4, p=16, spacing=2.5, semi_axes=(1.0, 1.0, 1.0), deg=6, amp=0.1, jitter=0.15,
                           min_sep=0.2, seed=1001),
 }
