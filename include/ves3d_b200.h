@@ -91,6 +91,24 @@ int ves3d_sv_device_buffer(ves3d_sv* sv, int which, double** ptr, size_t* n_elem
 int ves3d_sv_eval_resident(ves3d_sv* sv);
 
 /* ---------------------------------------------------------------------------
+ * Polydisperse suspensions: vesicles of different SH orders p in one evaluation (the
+ * reference needs one StokesVelocity per order; here the self part runs per order group
+ * and the far field is one all-pairs launch over every point). Surfaces, densities and
+ * velocities are the per-vesicle AxisMajor blocks [3][(p_v+1) 2 p_v] concatenated in
+ * vesicle order; vesicles of equal order must be contiguous (runs of any order sequence).
+ * Upsample order 2 p_v per vesicle.
+ * ------------------------------------------------------------------------- */
+typedef struct ves3d_svp ves3d_svp;
+int ves3d_svp_create(int precision, int device, ves3d_svp** out);
+int ves3d_svp_destroy(ves3d_svp* g);
+int ves3d_svp_set_src_coord(ves3d_svp* g, const double* S, const int* orders, long n_ves, int is_device);
+int ves3d_svp_set_density_sl(ves3d_svp* g, const double* f, int is_device);
+int ves3d_svp_setup(ves3d_svp* g);
+int ves3d_svp_eval(ves3d_svp* g, double* vel, int is_device);
+/* ms[0] self-matrix builds, ms[1] self parts, ms[2] far field, ms[3] whole last eval. */
+int ves3d_svp_stage_times(ves3d_svp* g, float* ms);
+
+/* ---------------------------------------------------------------------------
  * Surface geometry, tractions and the globally implicit step on the context's surfaces
  * (Surface, src/Surface.cc:212-569; InterfacialForce, src/InterfacialForce.cc:21-125;
  * InterfacialVelocity::ImplicitMatvecPhysical / AssembleRhsVel, src/InterfacialVelocity.cc:

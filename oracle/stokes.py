@@ -122,3 +122,27 @@ def stokes_velocity_sl(X, f, p, p_up=None, SL=None):
     if SL is None:
         SL = sh.stokes_singular_matrix(X, p, p_up)
     return sh.self_apply(SL, f, p) + far_velocity(X, f, p)
+
+
+def stokes_velocity_poly(X, f, orders):
+    """FP64 velocity of a polydisperse suspension (per-vesicle AxisMajor blocks concatenated;
+    each vesicle's self part at its own order, p_up = 2p)."""
+    X = np.asarray(X, np.float64)
+    f = np.asarray(f, np.float64)
+    orders = np.asarray(orders)
+    ng = np.array([sh.ngrid(int(p)) for p in orders])
+    off = np.concatenate([[0], np.cumsum(ng)]).astype(np.int64)
+    D = np.empty_like(f)
+    vel = np.empty_like(f)
+    for v, p in enumerate(orders):
+        p = int(p)
+        a, b = 3 * off[v], 3 * off[v + 1]
+        D[a:b] = far_density(X[a:b], f[a:b], p)
+        SL = sh.stokes_singular_matrix(X[a:b], p, 2 * p)
+        vel[a:b] = sh.self_apply(SL, f[a:b], p)
+    farv = far(X, D, off)
+    for v in range(orders.size):
+        a = off[v]
+        n = ng[v]
+        vel[3 * a:3 * (a + n)] += farv[a:a + n].T.reshape(-1)
+    return vel

@@ -50,6 +50,13 @@ SIGNATURES = [
     ("ves3d_sv_set_implicit_params", _i, [_vp, _d, _d, _d]),
     ("ves3d_sv_surface_op", _i, [_vp, _i, _vp, _vp, _i]),
     ("ves3d_sv_implicit_solve", _i, [_vp, _vp, _vp, ctypes.POINTER(_d), ctypes.POINTER(_i), ctypes.POINTER(_i), _i]),
+    ("ves3d_svp_create", _i, [_i, _i, ctypes.POINTER(_vp)]),
+    ("ves3d_svp_destroy", _i, [_vp]),
+    ("ves3d_svp_set_src_coord", _i, [_vp, _vp, _vp, _l, _i]),
+    ("ves3d_svp_set_density_sl", _i, [_vp, _vp, _i]),
+    ("ves3d_svp_setup", _i, [_vp]),
+    ("ves3d_svp_eval", _i, [_vp, _vp, _i]),
+    ("ves3d_svp_stage_times", _i, [_vp, ctypes.POINTER(ctypes.c_float)]),
     ("ves3d_sv_solver_stats", _i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     ("ves3d_bicgstab_f64", _i, [_vp, _vp, _vp, _vp, _sz, ctypes.POINTER(_d), ctypes.POINTER(_i),
                                 ctypes.POINTER(_i), _vp]),

@@ -57,10 +57,10 @@ __device__ __forceinline__ void pair64(const double* s, double tx, double ty, do
 // grid (segments, vesicles, target chunks of 2*blockDim targets); pos/den point-major
 // [N][3]; part [seg][N][3].
 __global__ void __launch_bounds__(512) k_far_f64_seg(const double* __restrict__ pos, const double* __restrict__ den,
-                                                     const long* __restrict__ off, long N, int seg_tiles,
+                                                     const long* __restrict__ off, long N, int seg_tiles, int v0,
                                                      double* __restrict__ part) {
   __shared__ __align__(16) double sm[kTileF64 * 6];
-  const int v = blockIdx.y, seg = blockIdx.x;
+  const int v = v0 + blockIdx.y, seg = blockIdx.x;
   const long t0 = off[v], nt = off[v + 1] - t0;
   const int nthr = blockDim.x;
   const long c0 = (long)blockIdx.z * 2 * nthr;
@@ -119,13 +119,13 @@ __global__ void __launch_bounds__(512) k_far_f64_seg(const double* __restrict__ 
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 
 __global__ void __launch_bounds__(512) k_far_f32_seg(const double* __restrict__ pos, const double* __restrict__ den,
-                                                     const long* __restrict__ off, long N, int seg_tiles,
+                                                     const long* __restrict__ off, long N, int seg_tiles, int v0,
                                                      double* __restrict__ part) {
   // one source = 6 broadcast float2: (x,x) (y,y) (z,z) (dx,dx) (dy,dy) (dz,dz)
   __shared__ __align__(16) float2 sm[kTileF32 * 6];
   __shared__ double cen[3];
   __shared__ double red[3][32];
-  const int v = blockIdx.y, seg = blockIdx.x;
+  const int v = v0 + blockIdx.y, seg = blockIdx.x;
   const long t0 = off[v], nt = off[v + 1] - t0;
   const int nthr = blockDim.x;
   // centroid of the target vesicle (FP64), the origin of this CTA's FP32 coordinates
@@ -265,32 +265,55 @@ int far_segments(long nves, long N, int tile, int nthr, int* seg_tiles) {
   return (int)((ntiles + *seg_tiles - 1) / *seg_tiles);
 }
 
-int launch_far(bool mixed, const double* pos, const double* den, const long* off, long nves, long N, int max_nt,
-               const double* add, double* out, double* far_out, double* part, long part_cap_segments,
-               cudaStream_t st) {
-  if (N <= 0) return VES3D_OK;
+static void chunking(int nt, int* nchunk, int* nthr) {
   // targets of a vesicle in chunks of at most 1024 (two per thread, <= 512 threads)
-  const int nchunk = (max_nt + 1023) / 1024;
-  const int per_chunk = (max_nt + nchunk - 1) / nchunk;
-  const int nthr = 32 * ((((per_chunk + 1) / 2) + 31) / 32);
+  *nchunk = (nt + 1023) / 1024;
+  const int per_chunk = (nt + *nchunk - 1) / *nchunk;
+  *nthr = 32 * ((((per_chunk + 1) / 2) + 31) / 32);
+}
+
+int launch_far_groups(bool mixed, const double* pos, const double* den, const long* off, long nves, long N,
+                      const FarGroup* groups, int ngroups, const double* add, double* out, double* far_out,
+                      double* part, long part_cap_segments, cudaStream_t st) {
+  if (N <= 0) return VES3D_OK;
   const int tile = mixed ? kTileF32 : kTileF64;
+  // one segment layout for all groups, sized by the average vesicle
+  int nthr_avg = 0, nchunk_tot = 0;
+  for (int g = 0; g < ngroups; g++) {
+    int nc, nt;
+    chunking(groups[g].nt, &nc, &nt);
+    nthr_avg += nt * groups[g].nv;
+    nchunk_tot += nc * groups[g].nv;
+  }
+  nthr_avg = (int)(nthr_avg / nves);
   int seg_tiles = 1;
-  int nseg = far_segments(nves * nchunk, N, tile, nthr, &seg_tiles);
+  int nseg = far_segments(nchunk_tot, N, tile, nthr_avg, &seg_tiles);
   if (nseg > part_cap_segments) {
-    // fewer, longer segments if the partial-sum buffer is smaller than the choice
     const long ntiles = (N + tile - 1) / tile;
     seg_tiles = (int)((ntiles + part_cap_segments - 1) / part_cap_segments);
     nseg = (int)((ntiles + seg_tiles - 1) / seg_tiles);
   }
-  dim3 grid(nseg, (unsigned)nves, nchunk);
-  if (mixed)
-    k_far_f32_seg<<<grid, nthr, 0, st>>>(pos, den, off, N, seg_tiles, part);
-  else
-    k_far_f64_seg<<<grid, nthr, 0, st>>>(pos, den, off, N, seg_tiles, part);
-  VES3D_LAUNCHED();
+  for (int g = 0; g < ngroups; g++) {
+    if (groups[g].nv <= 0) continue;
+    int nchunk, nthr;
+    chunking(groups[g].nt, &nchunk, &nthr);
+    dim3 grid(nseg, (unsigned)groups[g].nv, nchunk);
+    if (mixed)
+      k_far_f32_seg<<<grid, nthr, 0, st>>>(pos, den, off, N, seg_tiles, (int)groups[g].v0, part);
+    else
+      k_far_f64_seg<<<grid, nthr, 0, st>>>(pos, den, off, N, seg_tiles, (int)groups[g].v0, part);
+    VES3D_LAUNCHED();
+  }
   k_far_reduce<<<(unsigned)nves, 256, 0, st>>>(part, nseg, off, N, add, out, far_out);
   VES3D_LAUNCHED();
   return VES3D_OK;
+}
+
+int launch_far(bool mixed, const double* pos, const double* den, const long* off, long nves, long N, int max_nt,
+               const double* add, double* out, double* far_out, double* part, long part_cap_segments,
+               cudaStream_t st) {
+  FarGroup g{0, nves, max_nt};
+  return launch_far_groups(mixed, pos, den, off, nves, N, &g, 1, add, out, far_out, part, part_cap_segments, st);
 }
 
 }  // namespace ves3d

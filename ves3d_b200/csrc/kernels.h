@@ -69,6 +69,14 @@ int launch_far(bool mixed, const double* pos, const double* den, const long* off
                const double* add, double* out, double* far_out, double* part, long part_cap_segments,
                cudaStream_t st);
 constexpr long kFarMaxSegments = 32;
+// Vesicles [v0, v0 + nv) all with nt points: one far-field launch each, sized for nt.
+struct FarGroup {
+  long v0, nv;
+  int nt;
+};
+int launch_far_groups(bool mixed, const double* pos, const double* den, const long* off, long nves, long N,
+                      const FarGroup* groups, int ngroups, const double* add, double* out, double* far_out,
+                      double* part, long part_cap_segments, cudaStream_t st);
 // out = a + b elementwise.
 int launch_add(const double* a, const double* b, long n, double* out, cudaStream_t st);
 // All pairs, point-major in/out (StokesAlltoAll semantics).

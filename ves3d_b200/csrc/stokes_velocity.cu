@@ -322,9 +322,24 @@ int run_setup(ves3d_sv* sv) {
   return VES3D_OK;
 }
 
-int run_eval(ves3d_sv* sv) {
+// Self part of an evaluation: Vself = SHC2Grid(Grid2SHC(F) . SL) and the weighted far-field
+// density den = F * area * qw, written to the given buffers (the context's own, or slices
+// of a polydisperse suspension's global arrays).
+int run_self(ves3d_sv* sv, double* vself, double* den) {
   const DevTables& T = sv->tab->d;
-  const int p0 = sv->p, nc = ncoef_(p0), n = 3 * nc;
+  const int p0 = sv->p, n = 3 * ncoef_(p0);
+  cudaStream_t st = sv->stream;
+  int s;
+  if ((s = launch_grid2shc(sv->F, sv->nves * 3, p0, T.ana_four, T.ana_leg, T.jf_of_coef, sv->Fc, st))) return s;
+  if ((s = launch_self_gemv(sv->Fc, sv->SL, sv->nves, n, sv->Vc, st))) return s;
+  if ((s = launch_synthesis(sv->Vc, sv->nves * 3, p0, p0, T.syn0_leg, T.syn0_dleg, T.syn0_four, T.syn0_dfour,
+                            T.blk_off, vself, nullptr, nullptr, st)))
+    return s;
+  return launch_far_density(sv->F, sv->area, sv->nves, p0, T.smooth_w0, den, st);
+}
+
+int run_eval(ves3d_sv* sv) {
+  const int p0 = sv->p;
   cudaStream_t st = sv->stream;
   int s;
   if (!sv->have_src || !sv->have_den) {
@@ -333,13 +348,8 @@ int run_eval(ves3d_sv* sv) {
   }
   if (!sv->sl_valid && (s = run_setup(sv))) return s;
   VES3D_CK(cudaEventRecord(sv->ev[2], st));
-  if ((s = launch_grid2shc(sv->F, sv->nves * 3, p0, T.ana_four, T.ana_leg, T.jf_of_coef, sv->Fc, st))) return s;
-  if ((s = launch_self_gemv(sv->Fc, sv->SL, sv->nves, n, sv->Vc, st))) return s;
-  if ((s = launch_synthesis(sv->Vc, sv->nves * 3, p0, p0, T.syn0_leg, T.syn0_dleg, T.syn0_four, T.syn0_dfour,
-                            T.blk_off, sv->Vself, nullptr, nullptr, st)))
-    return s;
+  if ((s = run_self(sv, sv->Vself, sv->den))) return s;
   VES3D_CK(cudaEventRecord(sv->ev[3], st));
-  if ((s = launch_far_density(sv->F, sv->area, sv->nves, p0, T.smooth_w0, sv->den, st))) return s;
   // events bracket the far-field kernel alone: its duration is the roofline denominator
   VES3D_CK(cudaEventRecord(sv->ev[4], st));
   if ((s = launch_far(sv->prec == VES3D_PREC_MIXED && !sv->far_force_fp64, sv->pos, sv->den, sv->off, sv->nves, sv->npts(), ngrid_(p0),
@@ -1130,3 +1140,210 @@ int ves3d_sv_implicit_solve(ves3d_sv* sv, const double* x0, double* x, double* t
 }
 
 }  // extern "C"
+
+// ======================================================================================
+// Polydisperse suspensions: vesicles of different SH orders in one evaluation
+// ======================================================================================
+struct ves3d_svp {
+  int prec = 0, device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<ves3d_sv*> grp;          // one operator per run of equal order
+  std::vector<int> gp;                 // order of each run
+  std::vector<long> gnv, gpt0;         // vesicles and first point of each run
+  long nves = 0, N = 0;
+  int max_nt = 0;
+  double *pos = nullptr, *den = nullptr, *vself = nullptr, *V = nullptr, *Vfar = nullptr, *part = nullptr;
+  long* off = nullptr;
+  long capN = 0, capV = 0;
+  bool have_den = false;
+  cudaEvent_t ev[4] = {};
+  float ms[4] = {0, 0, 0, 0};
+  void free_global() {
+    double* ps[] = {pos, den, vself, V, Vfar, part};
+    for (double* q : ps) dfree(q);
+    dfree(off);
+    pos = den = vself = V = Vfar = part = nullptr;
+    off = nullptr;
+    capN = capV = 0;
+  }
+  void free_groups() {
+    for (ves3d_sv* g : grp) ves3d_sv_destroy(g);
+    grp.clear();
+    gp.clear();
+  }
+  ~ves3d_svp() {
+    free_groups();
+    free_global();
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+extern "C" {
+
+int ves3d_svp_create(int precision, int device, ves3d_svp** out) {
+  VES3D_ARG(out != nullptr, "out is null");
+  *out = nullptr;
+  VES3D_ARG(precision == VES3D_PREC_FP64 || precision == VES3D_PREC_MIXED, "unknown precision");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    set_error("no CUDA device");
+    return VES3D_ERR_NODEV;
+  }
+  if (device < 0) VES3D_CK(cudaGetDevice(&device));
+  VES3D_ARG(device < ndev, "device index out of range");
+  VES3D_CK(cudaSetDevice(device));
+  std::unique_ptr<ves3d_svp> g(new ves3d_svp());
+  g->prec = precision;
+  g->device = device;
+  VES3D_CK(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+  for (auto& e : g->ev) VES3D_CK(cudaEventCreate(&e));
+  *out = g.release();
+  return VES3D_OK;
+}
+
+int ves3d_svp_destroy(ves3d_svp* g) {
+  if (!g) return VES3D_OK;
+  cudaSetDevice(g->device);
+  cudaStreamSynchronize(g->stream);
+  delete g;
+  return VES3D_OK;
+}
+
+int ves3d_svp_set_src_coord(ves3d_svp* g, const double* S, const int* orders, long n_ves, int is_device) {
+  VES3D_ARG(g && S && orders && n_ves >= 1, "bad arguments");
+  VES3D_CK(cudaSetDevice(g->device));
+  // runs of equal order
+  std::vector<int> rp;
+  std::vector<long> rnv;
+  for (long v = 0; v < n_ves; v++) {
+    VES3D_ARG(orders[v] >= 2 && orders[v] <= 64, "order out of range");
+    if (rp.empty() || rp.back() != orders[v]) {
+      rp.push_back(orders[v]);
+      rnv.push_back(0);
+    }
+    rnv.back()++;
+  }
+  if (rp != g->gp) {
+    g->free_groups();
+    for (int p : rp) {
+      ves3d_sv* sv = nullptr;
+      int s = ves3d_sv_create(p, 2 * p, g->prec, g->device, &sv);
+      if (s) return s;
+      ves3d_sv_set_stream(sv, g->stream);
+      g->grp.push_back(sv);
+    }
+    g->gp = rp;
+  }
+  g->gnv = rnv;
+  g->gpt0.assign(rp.size(), 0);
+  std::vector<long> off(n_ves + 1, 0);
+  long pt = 0, v = 0;
+  int max_nt = 0;
+  for (size_t r = 0; r < rp.size(); r++) {
+    g->gpt0[r] = pt;
+    const int ng = ngrid_(rp[r]);
+    max_nt = std::max(max_nt, ng);
+    for (long k = 0; k < rnv[r]; k++, v++) {
+      off[v] = pt;
+      pt += ng;
+    }
+  }
+  off[n_ves] = pt;
+  g->nves = n_ves;
+  g->N = pt;
+  g->max_nt = max_nt;
+  if (g->capN < pt || g->capV < n_ves) {
+    g->free_global();
+    int s = 0;
+    s |= dalloc(&g->pos, 3 * (size_t)pt);
+    s |= dalloc(&g->den, 3 * (size_t)pt);
+    s |= dalloc(&g->vself, 3 * (size_t)pt);
+    s |= dalloc(&g->V, 3 * (size_t)pt);
+    s |= dalloc(&g->Vfar, 3 * (size_t)pt);
+    s |= dalloc(&g->part, (size_t)kFarMaxSegments * 3 * pt);
+    s |= dalloc(&g->off, (size_t)n_ves + 1);
+    if (s) {
+      g->free_global();
+      return s;
+    }
+    g->capN = pt;
+    g->capV = n_ves;
+  }
+  VES3D_CK(cudaMemcpyAsync(g->off, off.data(), off.size() * sizeof(long), cudaMemcpyHostToDevice, g->stream));
+  for (size_t r = 0; r < rp.size(); r++) {
+    int s = ves3d_sv_set_src_coord(g->grp[r], S + 3 * g->gpt0[r], rnv[r], is_device);
+    if (s) return s;
+    VES3D_CK(cudaMemcpyAsync(g->pos + 3 * g->gpt0[r], g->grp[r]->pos, 3 * (size_t)g->grp[r]->npts() * sizeof(double),
+                             cudaMemcpyDeviceToDevice, g->stream));
+  }
+  VES3D_CK(cudaStreamSynchronize(g->stream));
+  g->have_den = false;
+  return VES3D_OK;
+}
+
+int ves3d_svp_set_density_sl(ves3d_svp* g, const double* f, int is_device) {
+  VES3D_ARG(g && f, "null argument");
+  VES3D_ARG(!g->grp.empty(), "set_src_coord first");
+  for (size_t r = 0; r < g->grp.size(); r++) {
+    int s = ves3d_sv_set_density_sl(g->grp[r], f + 3 * g->gpt0[r], is_device);
+    if (s) return s;
+  }
+  g->have_den = true;
+  return VES3D_OK;
+}
+
+int ves3d_svp_setup(ves3d_svp* g) {
+  VES3D_ARG(g != nullptr, "null context");
+  VES3D_ARG(!g->grp.empty(), "set_src_coord first");
+  for (ves3d_sv* sv : g->grp) {
+    if (!sv->sl_valid) {
+      int s = run_setup(sv);
+      if (s) return s;
+    }
+  }
+  return VES3D_OK;
+}
+
+int ves3d_svp_eval(ves3d_svp* g, double* vel, int is_device) {
+  VES3D_ARG(g && vel, "null argument");
+  if (g->grp.empty() || !g->have_den) {
+    set_error("eval before set_src_coord / set_density_sl");
+    return VES3D_ERR_STATE;
+  }
+  VES3D_CK(cudaSetDevice(g->device));
+  int s;
+  VES3D_CK(cudaEventRecord(g->ev[0], g->stream));
+  if ((s = ves3d_svp_setup(g))) return s;
+  VES3D_CK(cudaEventRecord(g->ev[1], g->stream));
+  for (size_t r = 0; r < g->grp.size(); r++)
+    if ((s = run_self(g->grp[r], g->vself + 3 * g->gpt0[r], g->den + 3 * g->gpt0[r]))) return s;
+  VES3D_CK(cudaEventRecord(g->ev[2], g->stream));
+  const bool mixed = g->prec == VES3D_PREC_MIXED;
+  std::vector<FarGroup> fg;
+  long v0 = 0;
+  for (size_t r = 0; r < g->grp.size(); r++) {
+    fg.push_back(FarGroup{v0, g->gnv[r], ngrid_(g->gp[r])});
+    v0 += g->gnv[r];
+  }
+  if ((s = launch_far_groups(mixed, g->pos, g->den, g->off, g->nves, g->N, fg.data(), (int)fg.size(), g->vself, g->V,
+                             g->Vfar, g->part, kFarMaxSegments, g->stream)))
+    return s;
+  VES3D_CK(cudaEventRecord(g->ev[3], g->stream));
+  VES3D_CK(cudaEventSynchronize(g->ev[3]));
+  VES3D_CK(cudaEventElapsedTime(&g->ms[0], g->ev[0], g->ev[1]));
+  VES3D_CK(cudaEventElapsedTime(&g->ms[1], g->ev[1], g->ev[2]));
+  VES3D_CK(cudaEventElapsedTime(&g->ms[2], g->ev[2], g->ev[3]));
+  VES3D_CK(cudaEventElapsedTime(&g->ms[3], g->ev[0], g->ev[3]));
+  return copy_out(vel, g->V, 3 * (size_t)g->N, is_device, g->stream);
+}
+
+int ves3d_svp_stage_times(ves3d_svp* g, float* ms) {
+  VES3D_ARG(g && ms, "null argument");
+  for (int i = 0; i < 4; i++) ms[i] = g->ms[i];
+  return VES3D_OK;
+}
+
+}  // extern "C"
+

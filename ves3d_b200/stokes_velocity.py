@@ -176,3 +176,65 @@ class StokesVelocity:
         check(lib().ves3d_sv_implicit_solve(self._h, p0, x.ctypes.data, ctypes.byref(t), ctypes.byref(it),
                                             ctypes.byref(code), 0), "implicit_solve")
         return x, it.value, t.value, code.value
+
+
+class PolydisperseStokesVelocity:
+    """Single-layer velocity of a suspension whose vesicles have different SH orders.
+    Arrays are the per-vesicle AxisMajor blocks concatenated in vesicle order; vesicles of
+    equal order must be contiguous."""
+
+    def __init__(self, precision="fp64", device=-1):
+        prec = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}[precision]
+        h = ctypes.c_void_p()
+        check(lib().ves3d_svp_create(prec, int(device), ctypes.byref(h)), "PolydisperseStokesVelocity")
+        self._h = h
+        self.orders = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ves3d_svp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def npoints(self):
+        return int(sum(ngrid(p) for p in self.orders))
+
+    def SetSrcCoord(self, S, orders):
+        self.orders = np.ascontiguousarray(orders, dtype=np.int32)
+        p, dev, n = _ptr(S)
+        if n != 3 * self.npoints():
+            raise ValueError("surface size does not match the orders")
+        check(lib().ves3d_svp_set_src_coord(self._h, p, self.orders.ctypes.data, self.orders.size, dev),
+              "SetSrcCoord")
+
+    def SetDensitySL(self, f):
+        p, dev, n = _ptr(f)
+        if n != 3 * self.npoints():
+            raise ValueError("density size does not match the surfaces")
+        check(lib().ves3d_svp_set_density_sl(self._h, p, dev), "SetDensitySL")
+
+    def setup(self):
+        check(lib().ves3d_svp_setup(self._h), "setup")
+
+    def __call__(self, out=None):
+        if out is None:
+            out = np.empty(3 * self.npoints())
+        p, dev, n = _ptr(out)
+        check(lib().ves3d_svp_eval(self._h, p, dev), "StokesVelocity()")
+        return out
+
+    def stage_times(self):
+        ms = (ctypes.c_float * 4)()
+        check(lib().ves3d_svp_stage_times(self._h, ms), "stage_times")
+        return {"setup_ms": ms[0], "self_ms": ms[1], "far_ms": ms[2], "eval_ms": ms[3]}

@@ -107,8 +107,71 @@ CONFIGS = {
 }
 
 
+POLYDISPERSE = {
+    # 4096 vesicles, p ~ U{8,12,16,24}, radii ~ U[0.7,1.3], SH-perturbed ellipsoids, 20% volume fraction
+    "c3_4096ves_poly": dict(n_ves=4096, seed=1002),
+}
+
+
 def make(name):
     cfg = dict(CONFIGS[name])
     p = cfg["p"]
     X, f = suspension(**cfg)
     return X, f, p
+
+
+def poisson_disk_centers(radii, volume_fraction, gap, rng, max_tries=200000):
+    """Random sequential addition of non-overlapping spheres (radius r_i + gap/2 each) in a
+    cube sized for the given volume fraction of the bare spheres."""
+    vol = (4.0 / 3.0) * np.pi * np.sum(np.asarray(radii) ** 3)
+    L = (vol / volume_fraction) ** (1.0 / 3.0)
+    cell = 2.0 * (np.max(radii) + gap)
+    nc = max(1, int(L / cell))
+    grid = {}
+    centers = np.zeros((len(radii), 3))
+    order = np.argsort(-np.asarray(radii))  # place large ones first
+    tries = 0
+    for i in order:
+        r = radii[i]
+        while True:
+            tries += 1
+            if tries > max_tries:
+                raise RuntimeError("could not place all spheres; lower the volume fraction")
+            c = rng.uniform(r, L - r, size=3)
+            key = tuple(np.minimum((c / cell).astype(int), nc - 1))
+            ok = True
+            for dx in (-1, 0, 1):
+                for dy in (-1, 0, 1):
+                    for dz in (-1, 0, 1):
+                        for j in grid.get((key[0] + dx, key[1] + dy, key[2] + dz), ()):
+                            if np.sum((centers[j] - c) ** 2) < (r + radii[j] + gap) ** 2:
+                                ok = False
+                                break
+                        if not ok:
+                            break
+                    if not ok:
+                        break
+                if not ok:
+                    break
+            if ok:
+                centers[i] = c
+                grid.setdefault(key, []).append(i)
+                break
+    return centers, L
+
+
+def polydisperse(n_ves, orders=(8, 12, 16, 24), radius=(0.7, 1.3), volume_fraction=0.2, deg=4, amp=0.05,
+                 semi_axes=(1.0, 1.0, 0.8), gap=0.2, seed=1002):
+    """Vesicles with p ~ U(orders) and radii ~ U(radius); SH-perturbed ellipsoids; centres
+    by random sequential addition at the given volume fraction. Returned sorted by order
+    (runs of equal p contiguous): (X, f, orders)."""
+    rng = np.random.default_rng(seed)
+    ps = np.sort(rng.choice(np.asarray(orders), size=n_ves))
+    radii = rng.uniform(radius[0], radius[1], size=n_ves)
+    ext = radii * (1.0 + amp) * max(semi_axes)
+    centers, _ = poisson_disk_centers(ext, volume_fraction * (np.mean(ext ** 3) / np.mean(radii ** 3)), gap, rng)
+    Xs, fs = [], []
+    for v in range(n_ves):
+        Xs.append(shape(int(ps[v]), centers[v], semi_axes, radii[v], deg, amp, rng).reshape(-1))
+        fs.append(rng.standard_normal(3 * 2 * ps[v] * (ps[v] + 1)))
+    return np.concatenate(Xs), np.concatenate(fs), ps.astype(np.int32)
