@@ -41,6 +41,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-implicit", action="store_true", help="skip the implicit-step measurement")
+    ap.add_argument("--no-poly", action="store_true", help="skip the polydisperse measurement")
     return ap.parse_args()
 
 
@@ -312,6 +313,53 @@ def implicit_step_measurement(precision, local, stream):
                         "Galerkin form", "steps": out}
 
 
+def polydisperse_measurement(precision, local, stream):
+    """One full evaluation (self-matrix builds for every order + self parts + far field)
+    of the 4096-vesicle polydisperse suspension (p in {8,12,16,24}), device time, and the
+    error against the FP64 oracle at points of two sampled vesicles of order <= 16."""
+    import torch
+    from oracle import sh, stokes
+    from ves3d_b200 import workloads
+    from ves3d_b200.stokes_velocity import PolydisperseStokesVelocity
+    cfg = workloads.POLYDISPERSE["c3_4096ves_poly"]
+    X, f, orders = workloads.polydisperse(**cfg)
+    N = X.size // 3
+    sv = PolydisperseStokesVelocity(precision, device=local)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sv.SetSrcCoord(X, orders)
+    sv.SetDensitySL(f)
+    vel = sv()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    st = sv.stage_times()
+    sv.close()
+    # sampled error: two vesicles of order <= 16, all their points
+    ng = np.array([2 * p * (p + 1) for p in orders])
+    off = np.concatenate([[0], np.cumsum(ng)])
+    rng = np.random.default_rng(5)
+    cand = np.nonzero(orders <= 16)[0]
+    D = np.empty_like(f)
+    for v, p in enumerate(orders):
+        a, b = 3 * off[v], 3 * off[v + 1]
+        D[a:b] = stokes.far_density(X[a:b], f[a:b], int(p))
+    worst = 0.0
+    scale = np.abs(vel).max()
+    for v in rng.choice(cand, size=2, replace=False):
+        p = int(orders[v])
+        a, b = 3 * off[v], 3 * off[v + 1]
+        SL = sh.stokes_singular_matrix(X[a:b], p, 2 * p)
+        ref = sh.self_apply(SL, f[a:b], p) + stokes.far(X, D, off, np.arange(off[v], off[v + 1])).T.reshape(-1)
+        worst = max(worst, float(np.abs(vel[a:b] - ref).max() / scale))
+    counts = {int(p): int((orders == p).sum()) for p in np.unique(orders)}
+    return {"workload": f"c3_4096ves_poly: 4096 vesicles, p counts {counts}, {N} points, 20% volume fraction",
+            "ms_per_eval": ms, "points_per_s": N / (ms * 1e-3), "stages_ms": st,
+            "error_vs_fp64_oracle": {"max_rel": worst, "sample": "all points of 2 vesicles with p <= 16"}}
+
+
 def run_ours(args, world, rank, local):
     import torch
     from ves3d_b200 import _lib, workloads
@@ -446,6 +494,8 @@ def run_ours(args, world, rank, local):
         }
         if not args.no_implicit:
             result["implicit_step"] = implicit_step_measurement(args.precision, local, stream)
+        if not args.no_poly:
+            result["polydisperse"] = polydisperse_measurement(args.precision, local, stream)
         if world == 1 and not args.no_cpu_baseline:
             cb = cpu_reference_rate(X, f, p)
             result["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}

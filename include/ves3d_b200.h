@@ -145,6 +145,72 @@ int ves3d_sv_implicit_solve(ves3d_sv* sv, const double* x0, double* x, double* t
  * corrections by BiCGStab on the mixed operator. */
 int ves3d_sv_solver_stats(ves3d_sv* sv, int* outer, int* inner);
 
+/* Preconditioner of the implicit solve (right preconditioning, BiCGStab::operator()
+ * src/BiCGStab.cc:45-138 with its Precond argument):
+ *   NONE           identity (default)
+ *   DIAG_SPECTRAL  the reference's diagonal spectral scaling (ConfigurePrecond /
+ *                  ImplicitPrecond, src/InterfacialVelocity.cc:665-713, 1055-1109)
+ *   SELF_BLOCK     per-vesicle inverse of the isolated-vesicle operator (the implicit
+ *                  operator with the self part of the single layer only); no counterpart in
+ *                  the reference. Rebuilt on the first solve after the surfaces or dt /
+ *                  kappa change: 4 nc operator applications plus one dense LU per vesicle
+ *                  (cuSOLVER), stored in FP32, (4 nc)^2 * 4 bytes per vesicle.
+ * The solution's accuracy is set by the tolerance on the true residual in every case. */
+enum ves3d_precond { VES3D_PRECOND_NONE = 0, VES3D_PRECOND_DIAG_SPECTRAL = 1, VES3D_PRECOND_SELF_BLOCK = 2 };
+int ves3d_sv_set_precond(ves3d_sv* sv, int scheme);
+/* Device time of the last preconditioner build, ms[3] = {total, operator assembly, LU
+ * factorisation and inversion} in ms, and the bytes the preconditioner holds. */
+int ves3d_sv_precond_info(ves3d_sv* sv, double* ms, size_t* bytes);
+
+/* ---------------------------------------------------------------------------
+ * Initial guess of the implicit solve. The reference starts each solve from the previous
+ * step's solution (InterfacialVelocity::AssembleInitial, src/InterfacialVelocity.cc:874-919);
+ * these entry points add a learned per-vesicle guess and a residual-based choice among
+ * candidates. They have no counterpart in the reference. nc = p (p + 2) SH coefficients
+ * per scalar function, in this library's coefficient order (index 0 = degree 0).
+ * ------------------------------------------------------------------------- */
+/* feat [n_ves][3 nc] (FP32): SH coefficients of each vesicle's x, y, z with the degree-0
+ * coefficients set to 0 (translation removed). */
+int ves3d_sv_guess_features(ves3d_sv* sv, float* feat, int is_device);
+/* tgt [n_ves][4 nc] (FP32): SH coefficients of [u - u_inf; sigma] of the grid field x
+ * (u_inf = (shear_rate * y, 0, 0), the background flow of the implicit step). */
+int ves3d_sv_guess_targets(ves3d_sv* sv, const double* x, float* tgt, int is_device);
+/* Inverse of ves3d_sv_guess_targets: grid [u; sigma] from coefficients tgt. */
+int ves3d_sv_guess_from_targets(ves3d_sv* sv, const float* tgt, double* x0, int is_device);
+/* Residual-minimising combination of n_cand (1..8) candidate guesses cand[i] (grid
+ * [u; sigma], 4 N doubles each): x0 = sum_i weights[i] cand[i] minimises the true
+ * residual |b - A x0| of the Galerkin system over the candidates' span (FP64 operator).
+ * relres[0..n_cand-1] are the candidates' own relative residuals, relres[n_cand] that of
+ * x0 (never above the smallest of them, up to rounding). Candidates with non-finite
+ * images get weight 0. Costs n_cand + 1 FP64 operator applications. */
+int ves3d_sv_implicit_combine(ves3d_sv* sv, int n_cand, const double* const* cand, double* x0, double* weights,
+                              double* relres, int is_device);
+
+/* Multilayer perceptron with hand-written BF16 tensor-core kernels (FP32 accumulation,
+ * FP32 master weights, Adam): x -> [Linear -> ReLU] x (n_layers - 1) -> Linear. Inputs
+ * are normalised by (x - in_shift) * in_scale; the network's output z maps to the
+ * prediction z * out_scale + out_shift, and the loss is the mean squared error in the
+ * normalised output space. Parameters are one flat FP32 vector: per layer W [in][out]
+ * (row-major) then b [out]. Host pointers unless is_device. */
+typedef struct ves3d_mlp ves3d_mlp;
+int ves3d_mlp_create(int n_in, int n_hidden, int n_layers, int n_out, unsigned long long seed, ves3d_mlp** out);
+int ves3d_mlp_destroy(ves3d_mlp* net);
+long ves3d_mlp_num_params(ves3d_mlp* net);
+int ves3d_mlp_get_params(ves3d_mlp* net, float* out);
+int ves3d_mlp_set_params(ves3d_mlp* net, const float* in);
+/* NULL arrays mean shift 0 / scale 1. */
+int ves3d_mlp_set_scaling(ves3d_mlp* net, const float* in_shift, const float* in_scale, const float* out_shift,
+                          const float* out_scale);
+/* Y [batch][n_out] = prediction for X [batch][n_in]. */
+int ves3d_mlp_forward(ves3d_mlp* net, const float* X, long batch, float* Y, int is_device);
+/* Loss and its gradient with respect to the parameters (grads: host, may be NULL). */
+int ves3d_mlp_gradients(ves3d_mlp* net, const float* X, const float* T, long batch, float* grads, double* loss,
+                        int is_device);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) at learning rate lr; *loss is the loss
+ * before the step. */
+int ves3d_mlp_train_step(ves3d_mlp* net, const float* X, const float* T, long batch, float lr, double* loss,
+                         int is_device);
+
 /* BiCGStab on device vectors of length n (BiCGStab::operator(), src/BiCGStab.cc:45-138,
  * identity preconditioner); A computes y = A x on device pointers and returns 0 on success. */
 typedef int (*ves3d_matvec_fn)(void* ctx, const double* x, double* y);

@@ -58,6 +58,21 @@ SIGNATURES = [
     ("ves3d_svp_eval", _i, [_vp, _vp, _i]),
     ("ves3d_svp_stage_times", _i, [_vp, ctypes.POINTER(ctypes.c_float)]),
     ("ves3d_sv_solver_stats", _i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
+    ("ves3d_sv_set_precond", _i, [_vp, _i]),
+    ("ves3d_sv_precond_info", _i, [_vp, _dp, ctypes.POINTER(_sz)]),
+    ("ves3d_sv_guess_features", _i, [_vp, _vp, _i]),
+    ("ves3d_sv_guess_targets", _i, [_vp, _vp, _vp, _i]),
+    ("ves3d_sv_guess_from_targets", _i, [_vp, _vp, _vp, _i]),
+    ("ves3d_sv_implicit_combine", _i, [_vp, _i, ctypes.POINTER(_vp), _vp, _dp, _dp, _i]),
+    ("ves3d_mlp_create", _i, [_i, _i, _i, _i, ctypes.c_ulonglong, ctypes.POINTER(_vp)]),
+    ("ves3d_mlp_destroy", _i, [_vp]),
+    ("ves3d_mlp_num_params", _l, [_vp]),
+    ("ves3d_mlp_get_params", _i, [_vp, _vp]),
+    ("ves3d_mlp_set_params", _i, [_vp, _vp]),
+    ("ves3d_mlp_set_scaling", _i, [_vp, _vp, _vp, _vp, _vp]),
+    ("ves3d_mlp_forward", _i, [_vp, _vp, _l, _vp, _i]),
+    ("ves3d_mlp_gradients", _i, [_vp, _vp, _vp, _l, _vp, ctypes.POINTER(_d), _i]),
+    ("ves3d_mlp_train_step", _i, [_vp, _vp, _vp, _l, ctypes.c_float, ctypes.POINTER(_d), _i]),
     ("ves3d_bicgstab_f64", _i, [_vp, _vp, _vp, _vp, _sz, ctypes.POINTER(_d), ctypes.POINTER(_i),
                                 ctypes.POINTER(_i), _vp]),
 ]

@@ -7,9 +7,13 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libves3d_b200.so")
 SOURCES = ["sh_tables.cc", "sht_kernels.cu", "singular_kernels.cu", "direct_kernels.cu", "far_kernels.cu", "build_kernels.cu", "stokes_velocity.cu",
-           "peak_probe.cu", "noalloc.cu", "geometry_kernels.cu", "bicgstab.cu"]
+           "peak_probe.cu", "noalloc.cu", "geometry_kernels.cu", "bicgstab.cu", "mlp.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared", "-Wno-deprecated-gpu-targets"]
+
+
+# cuSOLVER: dense LU of the self-block preconditioner of the implicit solve
+LIBS = ["-lcusolver", "-lcublas"]
 
 
 def _nvcc():
@@ -30,7 +34,7 @@ def build(force=False, verbose=False):
     srcs, deps = sources()
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(d) for d in deps):
         return LIB
-    cmd = [_nvcc()] + NVCC_FLAGS + ["-o", LIB] + srcs
+    cmd = [_nvcc()] + NVCC_FLAGS + ["-o", LIB] + srcs + LIBS
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.check_call(cmd, cwd=CSRC)

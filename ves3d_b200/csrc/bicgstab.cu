@@ -1,6 +1,7 @@
-// Preconditioner-free BiCGStab on device vectors (FP64), the reference's iteration
-// (BiCGStab<Container, MatVec, Precond>::operator(), src/BiCGStab.cc:45-138, with the
-// identity preconditioner): same update order, same tests (initial residual <= tol;
+// BiCGStab on device vectors (FP64), the reference's iteration
+// (BiCGStab<Container, MatVec, Precond>::operator(), src/BiCGStab.cc:45-138): right
+// preconditioning phat = P p, shat = P s (identity when no preconditioner is given), same
+// update order, same tests on the unpreconditioned residual (initial residual <= tol;
 // afterwards s- and r-residuals < tol), same breakdown codes (BiCGSReturn,
 // include/BiCGStab.h:19-23). Dot products are two-pass block reductions in a fixed
 // order, so a solve is deterministic run to run. Scalars come back to the host once per
@@ -85,10 +86,12 @@ int lincomb_f64(long n, double a, const double* x, double b, const double* y, do
   return VES3D_OK;
 }
 
-size_t bicgstab_workspace_doubles(long n) { return (size_t)8 * n + kDotBlocks + 8; }
+size_t bicgstab_workspace_doubles(long n) { return (size_t)9 * n + kDotBlocks + 8; }
+
+double* bicgstab_dot_scratch(double* ws, long n) { return ws + 9 * n; }
 
 int bicgstab_run(MatVecFn A, void* ctx, double* x, const double* b, long n, double* tol, int* max_iter, int* code,
-                 double* ws, cudaStream_t st) {
+                 double* ws, cudaStream_t st, MatVecFn P, void* pctx) {
   double* p = ws;
   double* s = ws + n;
   double* t = ws + 2 * n;
@@ -96,7 +99,9 @@ int bicgstab_run(MatVecFn A, void* ctx, double* x, const double* b, long n, doub
   double* r = ws + 4 * n;
   double* rt = ws + 5 * n;
   double* ax = ws + 6 * n;
-  double* dscr = ws + 8 * n;
+  double* phat = P ? ws + 7 * n : p;
+  double* shat = P ? ws + 8 * n : s;
+  double* dscr = bicgstab_dot_scratch(ws, n);
   int st_;
   const double tol_in = *tol;
   const int iter_max = *max_iter;
@@ -140,7 +145,8 @@ int bicgstab_run(MatVecFn A, void* ctx, double* x, const double* b, long n, doub
       k_p_update<<<grid_for(n), 256, 0, st>>>(n, r, beta, omega, v, p);
       VES3D_LAUNCHED();
     }
-    if ((st_ = A(ctx, p, v))) return st_;
+    if (P && (st_ = P(pctx, p, phat))) return st_;
+    if ((st_ = A(ctx, phat, v))) return st_;
     double rtv = 0;
     if ((st_ = dot_f64(rt, v, n, dscr, &rtv, st))) return st_;
     alpha = rho1 / rtv;
@@ -149,18 +155,19 @@ int bicgstab_run(MatVecFn A, void* ctx, double* x, const double* b, long n, doub
     if ((st_ = dot_f64(s, s, n, dscr, &ss, st))) return st_;
     resid = std::sqrt(ss) / normb;
     if (resid < tol_in) {
-      if ((st_ = lincomb_f64(n, 1.0, x, alpha, p, 0, nullptr, x, st))) return st_;
+      if ((st_ = lincomb_f64(n, 1.0, x, alpha, phat, 0, nullptr, x, st))) return st_;
       *tol = resid;
       *max_iter = i;
       *code = 100;
       return VES3D_OK;
     }
-    if ((st_ = A(ctx, s, t))) return st_;
+    if (P && (st_ = P(pctx, s, shat))) return st_;
+    if ((st_ = A(ctx, shat, t))) return st_;
     double ts = 0, tt = 0;
     if ((st_ = dot_f64(t, s, n, dscr, &ts, st))) return st_;
     if ((st_ = dot_f64(t, t, n, dscr, &tt, st))) return st_;
     omega = ts / tt;
-    if ((st_ = lincomb_f64(n, 1.0, x, alpha, p, omega, s, x, st))) return st_;
+    if ((st_ = lincomb_f64(n, 1.0, x, alpha, phat, omega, shat, x, st))) return st_;
     if ((st_ = lincomb_f64(n, 1.0, s, -omega, t, 0, nullptr, r, st))) return st_;
     rho2 = rho1;
     if ((st_ = dot_f64(r, r, n, dscr, &rr, st))) return st_;
@@ -195,7 +202,7 @@ extern "C" int ves3d_bicgstab_f64(ves3d_matvec_fn A, void* ctx, double* x, const
   cudaStream_t st = (cudaStream_t)stream;
   double* ws = nullptr;
   VES3D_CK(cudaMalloc((void**)&ws, bicgstab_workspace_doubles((long)n) * sizeof(double)));
-  int s = bicgstab_run(A, ctx, x, b, (long)n, tol, max_iter, code, ws, st);
+  int s = bicgstab_run(A, ctx, x, b, (long)n, tol, max_iter, code, ws, st, nullptr, nullptr);
   cudaStreamSynchronize(st);
   cudaFree(ws);
   return s;

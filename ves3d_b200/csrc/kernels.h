@@ -105,7 +105,9 @@ int dot_f64(const double* x, const double* y, long n, double* scratch, double* r
 int lincomb_f64(long n, double a, const double* x, double b, const double* y, double c, const double* z, double* out,
                 cudaStream_t st);
 size_t bicgstab_workspace_doubles(long n);
+double* bicgstab_dot_scratch(double* ws, long n);  // scratch of dot_f64 inside a workspace
+// P (optional, NULL = identity): right preconditioner y = P x
 int bicgstab_run(MatVecFn A, void* ctx, double* x, const double* b, long n, double* tol, int* max_iter, int* code,
-                 double* ws, cudaStream_t st);
+                 double* ws, cudaStream_t st, MatVecFn P = nullptr, void* pctx = nullptr);
 
 }  // namespace ves3d

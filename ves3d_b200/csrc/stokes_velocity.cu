@@ -18,6 +18,8 @@
 #include <memory>
 #include <vector>
 
+#include <cusolverDn.h>
+
 #include "common.cuh"
 #include "kernels.h"
 #include "sh_tables.h"
@@ -112,6 +114,8 @@ struct TablesOwner {
 
 using namespace ves3d;
 
+constexpr int kPcStreams = 8;  // streams of the preconditioner factorisation
+
 struct ves3d_sv {
   int p = 0, pup = 0, prec = 0, device = 0;
   cudaStream_t stream = nullptr, own_stream = nullptr;
@@ -133,10 +137,29 @@ struct ves3d_sv {
   double dt = 0.01, kappa = 0.05, shear = 1.0;
   int far_force_fp64 = 0;      // 1: evaluate the far field in FP64 even in the mixed form
   int ir_outer = 0, ir_inner = 0;  // last mixed solve: outer refinements, inner iterations
+  // preconditioner of the implicit solve (VES3D_PRECOND_*); the self-block form stores one
+  // inverse per vesicle, [nv][n][n] column-major in FP32 (n = 4 nc)
+  int precond = 0;
+  bool self_only = false;      // stokes_apply evaluates the self part only (assembly)
+  float* pc_inv = nullptr;
+  double* pc_diag = nullptr;   // diagonal-spectral scales [4 nc]
+  long pc_cap = 0;
+  bool pc_valid = false;
+  double pc_ms[3] = {0, 0, 0};  // last build: total, assembly, factorisation (device ms)
+  cudaStream_t pc_stream[kPcStreams] = {};
+  cusolverDnHandle_t pc_solver[kPcStreams] = {};
+  cudaEvent_t pc_ev[3 + kPcStreams] = {};
   cudaEvent_t ev[8] = {};
   float ms[4] = {0, 0, 0, 0};
 
   ~ves3d_sv() {
+    free_precond();
+    for (auto& h : pc_solver)
+      if (h) cusolverDnDestroy(h);
+    for (auto& q : pc_stream)
+      if (q) cudaStreamDestroy(q);
+    for (auto& e : pc_ev)
+      if (e) cudaEventDestroy(e);
     free_implicit();
     free_buffers();
     free_scratch();
@@ -164,6 +187,14 @@ struct ves3d_sv {
     geo = wc = bws = nullptr;
     geo_cap = bws_cap = 0;
     geo_valid = false;
+  }
+  void free_precond() {
+    if (pc_inv) cudaFree(pc_inv);
+    dfree(pc_diag);
+    pc_inv = nullptr;
+    pc_diag = nullptr;
+    pc_cap = 0;
+    pc_valid = false;
   }
   void free_scratch() {
     double* ps[] = {R, Xu, Xut, Xup, K, C, SL3};
@@ -458,6 +489,7 @@ int ves3d_sv_set_src_coord(ves3d_sv* sv, const double* S, long n_ves, int is_dev
   sv->sl_valid = false;
   sv->parts_valid = false;
   sv->geo_valid = false;
+  sv->pc_valid = false;
   return VES3D_OK;
 }
 
@@ -829,6 +861,11 @@ int stokes_apply(ves3d_sv* sv, const double* f, double* out) {
   const size_t n = (size_t)sv->npts() * 3;
   VES3D_CK(cudaMemcpyAsync(sv->F, f, n * sizeof(double), cudaMemcpyDeviceToDevice, sv->stream));
   sv->have_den = true;
+  if (sv->self_only) {
+    // isolated vesicles: the singular self part alone
+    if (!sv->sl_valid && (s = run_setup(sv))) return s;
+    return run_self(sv, out, sv->den);
+  }
   if ((s = run_eval(sv))) return s;
   VES3D_CK(cudaMemcpyAsync(out, sv->V, n * sizeof(double), cudaMemcpyDeviceToDevice, sv->stream));
   return VES3D_OK;
@@ -935,6 +972,272 @@ int implicit_matvec_fp64_cb(void* ctx, const double* x, double* y) {
   return s;
 }
 
+unsigned grid_1d(long n) {
+  long b = (n + 255) / 256;
+  return (unsigned)(b < 4096 ? (b < 1 ? 1 : b) : 4096);
+}
+
+// ---- preconditioners of the implicit solve -------------------------------------------
+// Unknowns of the Galerkin system: [u coefficients (3 nv functions of nc); sigma
+// coefficients (nv functions of nc)]. Vesicle v's unknowns, local index i in [0, 4 nc):
+// i < 3 nc -> v 3 nc + i; else 3 nv nc + v nc + (i - 3 nc).
+__device__ __forceinline__ long sh_global(long v, long i, long nv, int nc) {
+  return i < 3 * nc ? v * 3 * nc + i : 3 * nv * nc + v * nc + (i - 3 * nc);
+}
+
+// e = unit vector at local index j of every vesicle
+__global__ void k_unit_columns(double* __restrict__ e, long nv, int nc, int j) {
+  const long v = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < nv) e[sh_global(v, j, nv, nc)] = 1.0;
+}
+
+// A[v] column j (column-major, n = 4 nc) = vesicle v's part of y
+__global__ void k_store_column(const double* __restrict__ y, long nv, int nc, int j, double* __restrict__ A) {
+  const long n = 4L * nc;
+  for (long g = (long)blockIdx.x * blockDim.x + threadIdx.x; g < nv * n; g += (long)gridDim.x * blockDim.x) {
+    const long v = g / n, i = g - v * n;
+    A[v * n * n + (long)j * n + i] = y[sh_global(v, i, nv, nc)];
+  }
+}
+
+// Constant tension is (up to quadrature error) a null mode of an isolated vesicle: the
+// single layer of 2 H n over a closed surface vanishes. Shift the sigma degree-0 diagonal
+// entry by the mean |diagonal| of the tension block so the block factors stably; the
+// preconditioner only steers the iteration along that mode.
+__global__ void k_shift_null_mode(double* __restrict__ A, long nv, int nc) {
+  const long v = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  const long n = 4L * nc;
+  double* Av = A + v * n * n;
+  double m = 0;
+  for (long i = 3L * nc; i < n; i++) m += fabs(Av[i * n + i]);
+  m /= nc;
+  const long i0 = 3L * nc;
+  Av[i0 * n + i0] += m > 0 ? m : 1.0;
+}
+
+__global__ void k_identity_blocks(double* __restrict__ A, long nv, long n) {
+  for (long g = (long)blockIdx.x * blockDim.x + threadIdx.x; g < nv * n * n; g += (long)gridDim.x * blockDim.x) {
+    const long r = g % (n * n);
+    A[g] = (r % n) == (r / n) ? 1.0 : 0.0;
+  }
+}
+
+__global__ void k_to_f32(const double* __restrict__ a, long n, float* __restrict__ b) {
+  for (long g = (long)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (long)gridDim.x * blockDim.x)
+    b[g] = (float)a[g];
+}
+
+// y_v = M_v x_v for every vesicle (M_v column-major FP32, n x n; x, y in the global
+// layout). Block (row tile of 256, vesicle): x_v staged in shared memory, each thread
+// walks the columns for its row, so every column read is one coalesced 1 KB segment.
+constexpr int kPcRows = 256;
+__global__ void __launch_bounds__(kPcRows) k_block_gemv(const float* __restrict__ M, const double* __restrict__ x,
+                                                        long nv, int nc, double* __restrict__ y) {
+  extern __shared__ double xs[];
+  const int n = 4 * nc;
+  const long v = blockIdx.y;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) xs[i] = x[sh_global(v, i, nv, nc)];
+  __syncthreads();
+  const int row = blockIdx.x * kPcRows + threadIdx.x;
+  if (row >= n) return;
+  const float* Mv = M + v * (long)n * n + row;
+  double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+  int j = 0;
+  for (; j + 4 <= n; j += 4) {
+    a0 = fma((double)Mv[(long)j * n], xs[j], a0);
+    a1 = fma((double)Mv[(long)(j + 1) * n], xs[j + 1], a1);
+    a2 = fma((double)Mv[(long)(j + 2) * n], xs[j + 2], a2);
+    a3 = fma((double)Mv[(long)(j + 3) * n], xs[j + 3], a3);
+  }
+  for (; j < n; j++) a0 = fma((double)Mv[(long)j * n], xs[j], a0);
+  y[sh_global(v, row, nv, nc)] = (a0 + a1) + (a2 + a3);
+}
+
+// Diagonal spectral scales of the reference (InterfacialVelocity::ConfigurePrecond,
+// src/InterfacialVelocity.cc:665-713), per coefficient of degree n:
+//   velocity: 1 / |1 - dt n^3| (1 where that is >= 1e3 or <= 1e-10)
+//   tension : (4n^2 - 1)(2n + 3) / ((n + 1)(2n^2 + 2n - 1) n)  (1 for n = 0 or ~0)
+__global__ void k_diag_precond(const double* __restrict__ x, long nv, int nc, const int* __restrict__ n_of_coef,
+                               double dt, double* __restrict__ y) {
+  const long tot = 4 * nv * nc;
+  for (long g = (long)blockIdx.x * blockDim.x + threadIdx.x; g < tot; g += (long)gridDim.x * blockDim.x) {
+    const bool vel = g < 3 * nv * nc;
+    const double n = (double)n_of_coef[g % nc];
+    double sc;
+    if (vel) {
+      double b = 1.0 / fabs(1.0 - dt * n * n * n);
+      b = fabs(b) < 1e3 ? b : 1.0;
+      sc = fabs(b) > 1e-10 ? b : 1.0;
+    } else {
+      double e = (4 * n * n - 1) * (2 * n + 3) / (n + 1) / (2 * n * n + 2 * n - 1);
+      e = n == 0 ? 1.0 : e / n;
+      sc = fabs(e) > 1e-10 ? e : 1.0;
+    }
+    y[g] = sc * x[g];
+  }
+}
+
+int precond_apply(void* ctx, const double* x, double* y) {
+  ves3d_sv* sv = (ves3d_sv*)ctx;
+  const int nc = ncoef_(sv->p);
+  const long nv = sv->nves;
+  if (sv->precond == VES3D_PRECOND_DIAG_SPECTRAL) {
+    k_diag_precond<<<grid_1d(4 * nv * nc), 256, 0, sv->stream>>>(x, nv, nc, sv->tab->d.n_of_coef, sv->dt, y);
+    VES3D_LAUNCHED();
+    return VES3D_OK;
+  }
+  const int n = 4 * nc;
+  dim3 grid((n + kPcRows - 1) / kPcRows, (unsigned)nv);
+  k_block_gemv<<<grid, kPcRows, n * sizeof(double), sv->stream>>>(sv->pc_inv, x, nv, nc, y);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
+// Per-vesicle inverse of the isolated-vesicle Galerkin operator (the implicit operator
+// with the self part of the single layer only): columns by applying that operator to
+// unit vectors (one column of every vesicle per application), LU with partial pivoting
+// (cuSOLVER getrf) and solves against the identity (getrs) in FP64, stored in FP32 -- the
+// preconditioner only steers the iteration; the tests on the true residual fix accuracy.
+int build_self_block_precond(ves3d_sv* sv) {
+  int s;
+  const int nc = ncoef_(sv->p), n = 4 * nc;
+  const long nv = sv->nves, nsh = sh_unknowns(sv), nn = (long)n * n;
+  if (sv->pc_cap < nv * nn) {
+    if (sv->pc_inv) cudaFree(sv->pc_inv);
+    sv->pc_inv = nullptr;
+    sv->pc_cap = 0;
+    VES3D_CK(cudaMalloc((void**)&sv->pc_inv, sizeof(float) * nv * nn));
+    sv->pc_cap = nv * nn;
+  }
+  if (!sv->pc_ev[0])
+    for (auto& ev : sv->pc_ev) VES3D_CK(cudaEventCreate(&ev));
+  for (int k = 0; k < kPcStreams; k++) {
+    if (!sv->pc_stream[k]) VES3D_CK(cudaStreamCreateWithFlags(&sv->pc_stream[k], cudaStreamNonBlocking));
+    if (!sv->pc_solver[k]) {
+      if (cusolverDnCreate(&sv->pc_solver[k]) != CUSOLVER_STATUS_SUCCESS) {
+        sv->pc_solver[k] = nullptr;
+        set_error("cusolverDnCreate failed");
+        return VES3D_ERR_CUDA;
+      }
+      if (cusolverDnSetStream(sv->pc_solver[k], sv->pc_stream[k]) != CUSOLVER_STATUS_SUCCESS) {
+        set_error("cusolverDnSetStream failed");
+        return VES3D_ERR_CUDA;
+      }
+    }
+  }
+  double *A = nullptr, *B = nullptr, *e = nullptr, *y = nullptr, *work = nullptr;
+  int *piv = nullptr, *info = nullptr;
+  if ((s = dalloc(&A, nv * nn))) return s;
+  if ((s = dalloc(&B, nv * nn)) || (s = dalloc(&e, nsh)) || (s = dalloc(&y, nsh)) ||
+      (s = dalloc(&piv, nv * (long)n)) || (s = dalloc(&info, nv))) {
+    dfree(A); dfree(B); dfree(e); dfree(y); dfree(piv);
+    return s;
+  }
+  VES3D_CK(cudaEventRecord(sv->pc_ev[0], sv->stream));
+  // columns of the isolated-vesicle operator, one per application, all vesicles at once
+  sv->self_only = true;
+  sv->far_force_fp64 = 1;
+  for (int j = 0; j < n && !s; j++) {
+    s = cuda_status(cudaMemsetAsync(e, 0, nsh * sizeof(double), sv->stream), "memset", __FILE__, __LINE__);
+    if (!s) {
+      k_unit_columns<<<(unsigned)((nv + 127) / 128), 128, 0, sv->stream>>>(e, nv, nc, j);
+      s = cuda_status(cudaGetLastError(), "k_unit_columns", __FILE__, __LINE__);
+      if (!s) launch_counter()++;
+    }
+    if (!s) s = implicit_matvec_sh(sv, e, y);
+    if (!s) {
+      k_store_column<<<grid_1d(nv * n), 256, 0, sv->stream>>>(y, nv, nc, j, A);
+      s = cuda_status(cudaGetLastError(), "k_store_column", __FILE__, __LINE__);
+      if (!s) launch_counter()++;
+    }
+  }
+  sv->self_only = false;
+  sv->far_force_fp64 = 0;
+  int lwork = 0;
+  if (!s && cusolverDnDgetrf_bufferSize(sv->pc_solver[0], n, n, A, n, &lwork) != CUSOLVER_STATUS_SUCCESS) {
+    set_error("cusolverDnDgetrf_bufferSize failed");
+    s = VES3D_ERR_CUDA;
+  }
+  lwork = std::max(lwork, 1);
+  if (!s) s = dalloc(&work, (size_t)lwork * kPcStreams);
+  if (!s) {
+    k_shift_null_mode<<<(unsigned)((nv + 127) / 128), 128, 0, sv->stream>>>(A, nv, nc);
+    s = cuda_status(cudaGetLastError(), "k_shift_null_mode", __FILE__, __LINE__);
+    if (!s) launch_counter()++;
+  }
+  if (!s) {
+    k_identity_blocks<<<grid_1d(nv * nn), 256, 0, sv->stream>>>(B, nv, n);
+    s = cuda_status(cudaGetLastError(), "k_identity_blocks", __FILE__, __LINE__);
+    if (!s) launch_counter()++;
+  }
+  // dense LU + solve against the identity, vesicles spread over kPcStreams streams (one
+  // factorisation of n ~ 10^3 does not fill the GPU)
+  if (!s) s = cuda_status(cudaEventRecord(sv->pc_ev[1], sv->stream), "event", __FILE__, __LINE__);
+  for (int k = 0; k < kPcStreams && !s; k++)
+    s = cuda_status(cudaStreamWaitEvent(sv->pc_stream[k], sv->pc_ev[1], 0), "wait", __FILE__, __LINE__);
+  for (long v = 0; v < nv && !s; v++) {
+    const int k = (int)(v % kPcStreams);
+    if (cusolverDnDgetrf(sv->pc_solver[k], n, n, A + v * nn, n, work + (long)k * lwork, piv + v * n, info + v) !=
+            CUSOLVER_STATUS_SUCCESS ||
+        cusolverDnDgetrs(sv->pc_solver[k], CUBLAS_OP_N, n, n, A + v * nn, n, piv + v * n, B + v * nn, n, info + v) !=
+            CUSOLVER_STATUS_SUCCESS) {
+      set_error("cuSOLVER getrf/getrs failed for vesicle %ld", v);
+      s = VES3D_ERR_CUDA;
+    }
+  }
+  // join (also after an error, so nothing is left running on the side streams)
+  for (int k = 0; k < kPcStreams; k++) {
+    cudaEventRecord(sv->pc_ev[3 + k], sv->pc_stream[k]);
+    cudaStreamWaitEvent(sv->stream, sv->pc_ev[3 + k], 0);
+  }
+  if (!s) {
+    k_to_f32<<<grid_1d(nv * nn), 256, 0, sv->stream>>>(B, nv * nn, sv->pc_inv);
+    s = cuda_status(cudaGetLastError(), "k_to_f32", __FILE__, __LINE__);
+    if (!s) launch_counter()++;
+  }
+  std::vector<int> hinfo(nv, 0);
+  if (!s)
+    s = cuda_status(cudaMemcpyAsync(hinfo.data(), info, nv * sizeof(int), cudaMemcpyDeviceToHost, sv->stream), "copy",
+                    __FILE__, __LINE__);
+  if (!s) s = cuda_status(cudaEventRecord(sv->pc_ev[2], sv->stream), "event", __FILE__, __LINE__);
+  cudaStreamSynchronize(sv->stream);
+  for (long v = 0; v < nv && !s; v++)
+    if (hinfo[v] != 0) {
+      set_error("self-block preconditioner: vesicle %ld has a singular isolated operator (info %d)", v, hinfo[v]);
+      s = VES3D_ERR_NUMERIC;
+    }
+  if (!s) {
+    float a = 0, b = 0;
+    cudaEventElapsedTime(&a, sv->pc_ev[0], sv->pc_ev[1]);
+    cudaEventElapsedTime(&b, sv->pc_ev[1], sv->pc_ev[2]);
+    sv->pc_ms[0] = a + b;
+    sv->pc_ms[1] = a;
+    sv->pc_ms[2] = b;
+    sv->pc_valid = true;
+  }
+  dfree(A);
+  dfree(B);
+  dfree(e);
+  dfree(y);
+  dfree(work);
+  dfree(piv);
+  dfree(info);
+  return s;
+}
+
+int ensure_precond(ves3d_sv* sv) {
+  if (sv->precond == VES3D_PRECOND_NONE || sv->pc_valid) return VES3D_OK;
+  if (sv->precond == VES3D_PRECOND_DIAG_SPECTRAL) {
+    sv->pc_ms[0] = sv->pc_ms[1] = sv->pc_ms[2] = 0;
+    sv->pc_valid = true;
+    return VES3D_OK;
+  }
+  return build_self_block_precond(sv);
+}
+
+MatVecFn precond_fn(ves3d_sv* sv) { return sv->precond == VES3D_PRECOND_NONE ? nullptr : precond_apply; }
+
 // Mixed-precision iterative refinement: outer residuals r = b - A x with the FP64
 // operator; inner BiCGStab with the mixed operator on A d = r to a relative tolerance of
 // 1e-2 (at most 150 iterations per correction); x += d. A correction that does not reduce the FP64 residual is undone and
@@ -952,7 +1255,7 @@ int mixed_refinement(ves3d_sv* sv, double* x, const double* b, long n, double* t
     return s;
   }
   double nb2 = 0;
-  s = dot_f64(b, b, n, ws + 8 * n, &nb2, sv->stream);
+  s = dot_f64(b, b, n, bicgstab_dot_scratch(ws, n), &nb2, sv->stream);
   const double normb = nb2 > 0 ? std::sqrt(nb2) : 1.0;
   int used = 0, outer = 0;
   bool fp64_inner = false;
@@ -963,7 +1266,7 @@ int mixed_refinement(ves3d_sv* sv, double* x, const double* b, long n, double* t
     if ((s = implicit_matvec_fp64_cb(sv, x, ax))) break;
     if ((s = lincomb_f64(n, 1.0, b, -1.0, ax, 0.0, nullptr, r, sv->stream))) break;
     double rr = 0;
-    if ((s = dot_f64(r, r, n, ws + 8 * n, &rr, sv->stream))) break;
+    if ((s = dot_f64(r, r, n, bicgstab_dot_scratch(ws, n), &rr, sv->stream))) break;
     const double cur = std::sqrt(rr) / normb;
     outer++;
     if (cur > relres) {
@@ -985,7 +1288,7 @@ int mixed_refinement(ves3d_sv* sv, double* x, const double* b, long n, double* t
     double itol = std::max(1e-2, 0.5 * target / relres);
     int imax = std::min(budget - used, 150), icode = 0;
     if ((s = bicgstab_run(fp64_inner ? implicit_matvec_fp64_cb : implicit_matvec_cb, sv, d, r, n, &itol, &imax,
-                          &icode, ws, sv->stream)))
+                          &icode, ws, sv->stream, precond_fn(sv), sv)))
       break;
     used += imax;
     if ((s = lincomb_f64(n, 1.0, x, 1.0, d, 0.0, nullptr, x, sv->stream))) break;
@@ -1016,9 +1319,28 @@ int ves3d_sv_set_implicit_params(ves3d_sv* sv, double dt, double kappa, double s
   int s = check_sv(sv);
   if (s) return s;
   VES3D_ARG(dt > 0 && kappa >= 0, "dt must be > 0 and kappa >= 0");
+  if (dt != sv->dt || kappa != sv->kappa) sv->pc_valid = false;
   sv->dt = dt;
   sv->kappa = kappa;
   sv->shear = shear_rate;
+  return VES3D_OK;
+}
+
+int ves3d_sv_set_precond(ves3d_sv* sv, int scheme) {
+  int s = check_sv(sv);
+  if (s) return s;
+  VES3D_ARG(scheme >= VES3D_PRECOND_NONE && scheme <= VES3D_PRECOND_SELF_BLOCK, "unknown preconditioner");
+  if (scheme != sv->precond) sv->pc_valid = false;
+  sv->precond = scheme;
+  return VES3D_OK;
+}
+
+int ves3d_sv_precond_info(ves3d_sv* sv, double* ms, size_t* bytes) {
+  int s = check_sv(sv);
+  if (s) return s;
+  VES3D_ARG(ms && bytes, "null argument");
+  for (int k = 0; k < 3; k++) ms[k] = sv->pc_ms[k];
+  *bytes = sv->precond == VES3D_PRECOND_SELF_BLOCK ? (size_t)sv->pc_cap * sizeof(float) : 0;
   return VES3D_OK;
 }
 
@@ -1124,9 +1446,11 @@ int ves3d_sv_implicit_solve(ves3d_sv* sv, const double* x0, double* x, double* t
   if (!s) s = implicit_rhs(sv, dg);
   sv->far_force_fp64 = 0;
   if (!s) s = grid_to_coef(sv, dg, db);
+  if (!s) s = ensure_precond(sv);
   if (!s) {
     if (sv->prec == VES3D_PREC_FP64)
-      s = bicgstab_run(implicit_matvec_cb, sv, dc, db, nsh, tol, max_iter, code, sv->bws, sv->stream);
+      s = bicgstab_run(implicit_matvec_cb, sv, dc, db, nsh, tol, max_iter, code, sv->bws, sv->stream,
+                       precond_fn(sv), sv);
     else
       s = mixed_refinement(sv, dc, db, nsh, tol, max_iter, code);
   }
@@ -1136,6 +1460,280 @@ int ves3d_sv_implicit_solve(ves3d_sv* sv, const double* x0, double* x, double* t
   dfree(dc);
   dfree(db);
   dfree(dg);
+  return s;
+}
+
+// ---- initial guesses of the implicit solve ------------------------------------------
+// Per-vesicle features and targets of the learned guess, and the residual-minimising
+// combination of candidate guesses (the true residual of the solver's own system decides
+// how much of each candidate is used; a useless candidate gets weight ~0).
+
+}  // extern "C"
+
+namespace {
+
+// feat[v][j] = coef[v][j] (3 nc per vesicle) with every degree-0 coefficient set to 0
+__global__ void k_pack_features(const double* __restrict__ coef, long n, int nc, float* __restrict__ feat) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    feat[i] = (i % nc) == 0 ? 0.f : (float)coef[i];
+}
+
+// tgt[v] = [cu[v] (3 nc); cs[v] (nc)]  <->  (cu, cs)
+__global__ void k_pack_targets(const double* __restrict__ cu, const double* __restrict__ cs, long nv, int nc,
+                               float* __restrict__ tgt, double* __restrict__ ou, double* __restrict__ os,
+                               const float* __restrict__ in) {
+  const long n = nv * 4 * nc;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const long v = i / (4 * nc);
+    const int j = (int)(i - v * 4 * nc);
+    if (in) {
+      const double x = (double)in[i];
+      if (j < 3 * nc) ou[v * 3 * nc + j] = x;
+      else os[v * nc + j - 3 * nc] = x;
+    } else {
+      tgt[i] = (float)(j < 3 * nc ? cu[v * 3 * nc + j] : cs[v * nc + j - 3 * nc]);
+    }
+  }
+}
+
+// Solve the n x n normal equations G a = h (n <= 8) by Gaussian elimination with partial
+// pivoting, after Jacobi scaling (unit diagonal, so candidates of very different size are
+// treated alike); a ridge of 1e-13 keeps dependent candidates from blowing the weights up.
+void small_solve(int n, std::vector<double> G, std::vector<double> h, std::vector<double>& a) {
+  std::vector<double> d(n);
+  for (int i = 0; i < n; i++) d[i] = G[i * n + i] > 0 ? 1.0 / std::sqrt(G[i * n + i]) : 0.0;
+  for (int i = 0; i < n; i++) {
+    h[i] *= d[i];
+    for (int j = 0; j < n; j++) G[i * n + j] *= d[i] * d[j];
+    G[i * n + i] += 1e-13;
+  }
+  for (int k = 0; k < n; k++) {
+    int piv = k;
+    for (int i = k + 1; i < n; i++)
+      if (std::fabs(G[i * n + k]) > std::fabs(G[piv * n + k])) piv = i;
+    if (piv != k) {
+      for (int j = 0; j < n; j++) std::swap(G[k * n + j], G[piv * n + j]);
+      std::swap(h[k], h[piv]);
+    }
+    const double d = G[k * n + k];
+    if (d == 0) continue;
+    for (int i = k + 1; i < n; i++) {
+      const double f = G[i * n + k] / d;
+      for (int j = k; j < n; j++) G[i * n + j] -= f * G[k * n + j];
+      h[i] -= f * h[k];
+    }
+  }
+  a.assign(n, 0.0);
+  for (int k = n - 1; k >= 0; k--) {
+    double t = h[k];
+    for (int j = k + 1; j < n; j++) t -= G[k * n + j] * a[j];
+    a[k] = G[k * n + k] != 0 ? t / G[k * n + k] : 0.0;
+  }
+  for (int i = 0; i < n; i++) a[i] *= d[i];
+}
+
+}  // namespace
+
+extern "C" {
+
+int ves3d_sv_guess_features(ves3d_sv* sv, float* feat, int is_device) {
+  int s = check_sv(sv);
+  if (s) return s;
+  VES3D_ARG(feat != nullptr, "feat is null");
+  if (!sv->have_src) {
+    set_error("no surfaces set");
+    return VES3D_ERR_STATE;
+  }
+  const long nv = sv->nves, nc = ncoef_(sv->p), n = nv * 3 * nc;
+  double* c = nullptr;
+  float* f = nullptr;
+  if ((s = dalloc(&c, n))) return s;
+  if ((s = dalloc(&f, n))) {
+    dfree(c);
+    return s;
+  }
+  s = grid2shc_p(sv, sv->X, 3 * nv, c);
+  if (!s) {
+    k_pack_features<<<grid_1d(n), 256, 0, sv->stream>>>(c, n, (int)nc, f);
+    s = cuda_status(cudaGetLastError(), "k_pack_features", __FILE__, __LINE__);
+    if (!s) launch_counter()++;
+  }
+  if (!s)
+    s = cuda_status(cudaMemcpyAsync(feat, f, n * sizeof(float),
+                                    is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, sv->stream),
+                    "copy", __FILE__, __LINE__);
+  cudaStreamSynchronize(sv->stream);
+  dfree(c);
+  dfree(f);
+  return s;
+}
+
+int ves3d_sv_guess_targets(ves3d_sv* sv, const double* x, float* tgt, int is_device) {
+  int s = check_sv(sv);
+  if (s) return s;
+  VES3D_ARG(x && tgt, "null argument");
+  if (!sv->have_src) {
+    set_error("no surfaces set");
+    return VES3D_ERR_STATE;
+  }
+  const long nv = sv->nves, nc = ncoef_(sv->p), N = sv->npts();
+  const int ng = ngrid_(sv->p);
+  double *g = nullptr, *ui = nullptr, *cu = nullptr;
+  float* t = nullptr;
+  if ((s = dalloc(&g, 4 * N))) return s;
+  if ((s = dalloc(&ui, 3 * N)) || (s = dalloc(&cu, 4 * nv * nc)) || (s = dalloc(&t, 4 * nv * nc))) {
+    dfree(g); dfree(ui); dfree(cu);
+    return s;
+  }
+  s = copy_in(g, x, 4 * N, is_device, sv->stream);
+  if (!s) s = launch_shear(sv->X, nv, ng, sv->shear, ui, sv->stream);
+  if (!s) s = lincomb_f64(3 * N, 1.0, g, -1.0, ui, 0.0, nullptr, g, sv->stream);
+  if (!s) s = grid2shc_p(sv, g, 3 * nv, cu);
+  if (!s) s = grid2shc_p(sv, g + 3 * N, nv, cu + 3 * nv * nc);
+  if (!s) {
+    k_pack_targets<<<grid_1d(4 * nv * nc), 256, 0, sv->stream>>>(cu, cu + 3 * nv * nc, nv, (int)nc, t, nullptr,
+                                                                  nullptr, nullptr);
+    s = cuda_status(cudaGetLastError(), "k_pack_targets", __FILE__, __LINE__);
+    if (!s) launch_counter()++;
+  }
+  if (!s)
+    s = cuda_status(cudaMemcpyAsync(tgt, t, 4 * nv * nc * sizeof(float),
+                                    is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, sv->stream),
+                    "copy", __FILE__, __LINE__);
+  cudaStreamSynchronize(sv->stream);
+  dfree(g);
+  dfree(ui);
+  dfree(cu);
+  dfree(t);
+  return s;
+}
+
+int ves3d_sv_guess_from_targets(ves3d_sv* sv, const float* tgt, double* x0, int is_device) {
+  int s = check_sv(sv);
+  if (s) return s;
+  VES3D_ARG(x0 && tgt, "null argument");
+  if (!sv->have_src) {
+    set_error("no surfaces set");
+    return VES3D_ERR_STATE;
+  }
+  const long nv = sv->nves, nc = ncoef_(sv->p), N = sv->npts();
+  const int ng = ngrid_(sv->p);
+  double *g = nullptr, *ui = nullptr, *cu = nullptr;
+  float* t = nullptr;
+  if ((s = dalloc(&g, 4 * N))) return s;
+  if ((s = dalloc(&ui, 3 * N)) || (s = dalloc(&cu, 4 * nv * nc)) || (s = dalloc(&t, 4 * nv * nc))) {
+    dfree(g); dfree(ui); dfree(cu);
+    return s;
+  }
+  s = cuda_status(cudaMemcpyAsync(t, tgt, 4 * nv * nc * sizeof(float),
+                                  is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, sv->stream),
+                  "copy", __FILE__, __LINE__);
+  if (!s) {
+    k_pack_targets<<<grid_1d(4 * nv * nc), 256, 0, sv->stream>>>(nullptr, nullptr, nv, (int)nc, nullptr, cu,
+                                                                  cu + 3 * nv * nc, t);
+    s = cuda_status(cudaGetLastError(), "k_pack_targets", __FILE__, __LINE__);
+    if (!s) launch_counter()++;
+  }
+  if (!s) s = coef_to_grid(sv, cu, g);
+  if (!s) s = launch_shear(sv->X, nv, ng, sv->shear, ui, sv->stream);
+  if (!s) s = lincomb_f64(3 * N, 1.0, g, 1.0, ui, 0.0, nullptr, g, sv->stream);
+  if (!s) s = copy_out(x0, g, 4 * N, is_device, sv->stream);
+  cudaStreamSynchronize(sv->stream);
+  dfree(g);
+  dfree(ui);
+  dfree(cu);
+  dfree(t);
+  return s;
+}
+
+int ves3d_sv_implicit_combine(ves3d_sv* sv, int n_cand, const double* const* cand, double* x0, double* weights,
+                              double* relres, int is_device) {
+  int s = check_sv(sv);
+  if (s) return s;
+  VES3D_ARG(n_cand >= 1 && n_cand <= 8, "n_cand must be in [1, 8]");
+  VES3D_ARG(cand && x0 && weights && relres, "null argument");
+  for (int i = 0; i < n_cand; i++) VES3D_ARG(cand[i] != nullptr, "null candidate");
+  if (!sv->have_src) {
+    set_error("no surfaces set");
+    return VES3D_ERR_STATE;
+  }
+  if ((s = ensure_geometry(sv))) return s;
+  ImplicitWork iw;
+  if ((s = implicit_work(sv, iw))) return s;
+  const long ng4 = 4 * sv->npts(), nsh = sh_unknowns(sv);
+  double *b = nullptr, *C = nullptr, *Y = nullptr, *dg = nullptr, *r = nullptr, *scr = nullptr;
+  if ((s = dalloc(&b, nsh))) return s;
+  if ((s = dalloc(&C, nsh * n_cand)) || (s = dalloc(&Y, nsh * n_cand)) || (s = dalloc(&dg, ng4)) ||
+      (s = dalloc(&r, nsh)) || (s = dalloc(&scr, 1024))) {
+    dfree(b); dfree(C); dfree(Y); dfree(dg); dfree(r);
+    return s;
+  }
+  // right-hand side and the candidates' images under the FP64 operator
+  sv->far_force_fp64 = 1;
+  s = implicit_rhs(sv, dg);
+  if (!s) s = grid_to_coef(sv, dg, b);
+  for (int i = 0; i < n_cand && !s; i++) {
+    s = copy_in(dg, cand[i], ng4, is_device, sv->stream);
+    if (!s) s = grid_to_coef(sv, dg, C + i * nsh);
+    if (!s) s = implicit_matvec_sh(sv, C + i * nsh, Y + i * nsh);
+  }
+  sv->far_force_fp64 = 0;
+  std::vector<double> G(n_cand * n_cand, 0.0), h(n_cand, 0.0), a;
+  std::vector<char> ok(n_cand, 1);
+  double bb = 0;
+  if (!s) s = dot_f64(b, b, nsh, scr, &bb, sv->stream);
+  const double nb = bb > 0 ? std::sqrt(bb) : 1.0;
+  for (int i = 0; i < n_cand && !s; i++) {
+    // residual of the candidate as given
+    s = lincomb_f64(nsh, 1.0, b, -1.0, Y + i * nsh, 0.0, nullptr, r, sv->stream);
+    double rr = 0;
+    if (!s) s = dot_f64(r, r, nsh, scr, &rr, sv->stream);
+    relres[i] = std::sqrt(rr) / nb;
+    if (!s) s = dot_f64(Y + i * nsh, b, nsh, scr, &h[i], sv->stream);
+    for (int j = 0; j <= i && !s; j++) {
+      s = dot_f64(Y + i * nsh, Y + j * nsh, nsh, scr, &G[i * n_cand + j], sv->stream);
+      G[j * n_cand + i] = G[i * n_cand + j];
+    }
+    if (!std::isfinite(G[i * n_cand + i]) || !std::isfinite(h[i])) ok[i] = 0;
+  }
+  if (!s) {
+    // drop non-finite candidates, solve the normal equations of the rest
+    std::vector<int> idx;
+    for (int i = 0; i < n_cand; i++)
+      if (ok[i] && G[i * n_cand + i] > 0) idx.push_back(i);
+    const int m = (int)idx.size();
+    std::vector<double> Gm(m * m), hm(m), am;
+    for (int i = 0; i < m; i++) {
+      hm[i] = h[idx[i]];
+      for (int j = 0; j < m; j++) Gm[i * m + j] = G[idx[i] * n_cand + idx[j]];
+    }
+    if (m) small_solve(m, Gm, hm, am);
+    for (int i = 0; i < n_cand; i++) weights[i] = 0.0;
+    for (int i = 0; i < m; i++) weights[idx[i]] = am[i];
+    // combined coefficients and their true residual
+    s = cuda_status(cudaMemsetAsync(dg, 0, nsh * sizeof(double), sv->stream), "memset", __FILE__, __LINE__);
+    if (!s) s = copy_in(r, b, nsh, 1, sv->stream);
+    for (int i = 0; i < m && !s; i++) {
+      s = lincomb_f64(nsh, 1.0, dg, am[i], C + idx[i] * nsh, 0.0, nullptr, dg, sv->stream);
+      if (!s) s = lincomb_f64(nsh, 1.0, r, -am[i], Y + idx[i] * nsh, 0.0, nullptr, r, sv->stream);
+    }
+    double rr = 0;
+    if (!s) s = dot_f64(r, r, nsh, scr, &rr, sv->stream);
+    relres[n_cand] = std::sqrt(rr) / nb;
+    if (!s) {
+      // dg holds coefficients; map to the grid through b's storage
+      s = copy_in(b, dg, nsh, 1, sv->stream);
+      if (!s) s = coef_to_grid(sv, b, dg);
+      if (!s) s = copy_out(x0, dg, ng4, is_device, sv->stream);
+    }
+  }
+  cudaStreamSynchronize(sv->stream);
+  dfree(b);
+  dfree(C);
+  dfree(Y);
+  dfree(dg);
+  dfree(r);
+  dfree(scr);
   return s;
 }
 

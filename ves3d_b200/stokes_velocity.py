@@ -157,6 +157,21 @@ class StokesVelocity:
         check(lib().ves3d_sv_surface_op(self._h, code, ptr, out.ctypes.data, 0), f"surface_op({op})")
         return out
 
+    PRECONDS = {"none": 0, "diag_spectral": 1, "self_block": 2}
+
+    def set_precond(self, scheme):
+        """Preconditioner of implicit_solve: "none", "diag_spectral" (the reference's
+        ImplicitPrecond) or "self_block" (per-vesicle inverse of the isolated operator)."""
+        code = self.PRECONDS[scheme] if isinstance(scheme, str) else int(scheme)
+        check(lib().ves3d_sv_set_precond(self._h, code), "set_precond")
+
+    def precond_info(self):
+        """Device time of the last preconditioner build (total, operator assembly, LU) and
+        the bytes the preconditioner holds."""
+        ms, nb = (ctypes.c_double * 3)(), ctypes.c_size_t(0)
+        check(lib().ves3d_sv_precond_info(self._h, ms, ctypes.byref(nb)), "precond_info")
+        return {"setup_ms": ms[0], "assembly_ms": ms[1], "factor_ms": ms[2], "bytes": nb.value}
+
     def solver_stats(self):
         o, i = ctypes.c_int(0), ctypes.c_int(0)
         check(lib().ves3d_sv_solver_stats(self._h, ctypes.byref(o), ctypes.byref(i)), "solver_stats")
@@ -176,6 +191,43 @@ class StokesVelocity:
         check(lib().ves3d_sv_implicit_solve(self._h, p0, x.ctypes.data, ctypes.byref(t), ctypes.byref(it),
                                             ctypes.byref(code), 0), "implicit_solve")
         return x, it.value, t.value, code.value
+
+    # ---- initial guesses ---------------------------------------------------------------
+    def guess_features(self):
+        """[n_ves][3 nc] float32: SH coefficients of the positions, degree 0 removed."""
+        out = np.empty((self.n_ves, 3 * ncoef(self.sh_order)), dtype=np.float32)
+        check(lib().ves3d_sv_guess_features(self._h, out.ctypes.data, 0), "guess_features")
+        return out
+
+    def guess_targets(self, x):
+        """[n_ves][4 nc] float32: SH coefficients of [u - u_inf; sigma] of the grid field x."""
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+        out = np.empty((self.n_ves, 4 * ncoef(self.sh_order)), dtype=np.float32)
+        check(lib().ves3d_sv_guess_targets(self._h, x.ctypes.data, out.ctypes.data, 0), "guess_targets")
+        return out
+
+    def guess_from_targets(self, tgt):
+        """Grid field [u; sigma] from target coefficients (inverse of guess_targets)."""
+        tgt = np.ascontiguousarray(tgt, dtype=np.float32).reshape(-1)
+        x0 = np.empty(4 * self.n_ves * ngrid(self.sh_order))
+        check(lib().ves3d_sv_guess_from_targets(self._h, tgt.ctypes.data, x0.ctypes.data, 0), "guess_from_targets")
+        return x0
+
+    def implicit_combine(self, candidates):
+        """Residual-minimising combination of candidate guesses (grid fields [u; sigma]).
+        Returns (x0, weights, relres): relres[i] is candidate i's own relative residual,
+        relres[-1] that of x0."""
+        cands = [np.ascontiguousarray(c, dtype=np.float64).reshape(-1) for c in candidates]
+        n = len(cands)
+        arr = (ctypes.c_void_p * n)(*[c.ctypes.data for c in cands])
+        x0 = np.empty_like(cands[0])
+        w = np.zeros(n)
+        r = np.zeros(n + 1)
+        check(lib().ves3d_sv_implicit_combine(self._h, n, arr, x0.ctypes.data,
+                                              w.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                              r.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 0),
+              "implicit_combine")
+        return x0, w, r
 
 
 class PolydisperseStokesVelocity:
