@@ -271,46 +271,94 @@ def sampled_error_vs_oracle(X, f, p, vel, nves_check=2, n_targets=256, seed=11):
     return worst
 
 
-IMPLICIT = dict(workload="c4_256ves_p16", dt=0.01, kappa=0.05, shear_rate=1.0, tol=1e-8, max_iter=500)
+IMPLICIT = dict(workload="c4_256ves_p16", dt=0.01, kappa=0.05, shear_rate=1.0, tol=1e-8, max_iter=1000)
+
+# implicit-step forms: (label, precision, preconditioner, guess policy)
+#   plain: the reference's configuration -- FP64, no preconditioner (the reference's
+#          diagonal spectral one does not converge on this workload within 600 iterations),
+#          zero guess on the first step, the previous solution afterwards
+#   fast : mixed precision, per-vesicle self-block preconditioner, learned guess combined
+#          with the previous solution by the true residual
+IMPLICIT_FORMS = [
+    ("plain_fp64", "fp64", "none", "previous"),
+    ("fp64_self_block", "fp64", "self_block", "previous"),
+    ("mixed_self_block_learned", "mixed", "self_block", "learned+previous"),
+]
 
 
-def implicit_step_measurement(precision, local, stream):
-    """Two globally implicit steps of the 256-vesicle p=16 suspension in shear flow: the
-    first from a zero initial guess, the second (after x += dt u) from the previous
-    step's solution. Device time per step: geometry + self-matrix build + right-hand side
-    + BiCGStab (Galerkin form) to the tolerance."""
+def implicit_step_measurement(local, stream, steps=2, forms=None):
+    """Globally implicit steps of the 256-vesicle p=16 suspension in shear flow (C4), each
+    form on its own trajectory from the same initial surfaces. Device time per step
+    (CUDA events on the context's stream): geometry + self-matrix build + preconditioner
+    build + guess + right-hand side + BiCGStab (Galerkin form) to the tolerance on the
+    true residual."""
     import torch
     from ves3d_b200 import workloads
+    from ves3d_b200.learned_guess import DEFAULT_WEIGHTS, LearnedGuess, initial_guess
     from ves3d_b200.stokes_velocity import StokesVelocity
-    X, _, p = workloads.make(IMPLICIT["workload"])
+    X0, _, p = workloads.make(IMPLICIT["workload"])
     ng = 2 * p * (p + 1)
-    nves = X.size // (3 * ng)
+    nves = X0.size // (3 * ng)
     N = nves * ng
-    sv = StokesVelocity(p, 2 * p, precision=precision, device=local)
-    sv.set_stream(stream.cuda_stream)
-    sv.set_implicit_params(IMPLICIT["dt"], IMPLICIT["kappa"], IMPLICIT["shear_rate"])
-    out = []
-    guess = None
-    for label in ("zero guess", "previous-step guess"):
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        sv.SetSrcCoord(X)
-        x, it, relres, code = sv.implicit_solve(x0=guess, tol=IMPLICIT["tol"], max_iter=IMPLICIT["max_iter"])
-        e1.record(stream)
-        torch.cuda.synchronize()
-        rec = {"guess": label, "ms": e0.elapsed_time(e1), "bicgstab_iterations": it, "relres": relres, "code": code}
-        if precision == "mixed":
-            st = sv.solver_stats()
-            rec["fp64_residual_evaluations"] = st["outer"]
-        out.append(rec)
-        X = X + IMPLICIT["dt"] * x[:3 * N]
-        guess = x
-    sv.close()
+    learned = None
+    import os
+    if os.path.exists(DEFAULT_WEIGHTS):
+        learned = LearnedGuess.load(DEFAULT_WEIGHTS)
+        if not learned.matches(p, IMPLICIT["dt"], IMPLICIT["kappa"], IMPLICIT["shear_rate"]):
+            learned = None
+    out = {}
+    for label, prec, pc, policy in (forms or IMPLICIT_FORMS):
+        sv = StokesVelocity(p, 2 * p, precision=prec, device=local)
+        sv.set_stream(stream.cuda_stream)
+        sv.set_implicit_params(IMPLICIT["dt"], IMPLICIT["kappa"], IMPLICIT["shear_rate"])
+        sv.set_precond(pc)
+        X = X0.copy()
+        prev = None
+        recs = []
+        for k in range(steps):
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            sv.SetSrcCoord(X)
+            info = {}
+            if policy == "learned+previous" and learned is not None:
+                x0, info = initial_guess(sv, learned=learned, previous=prev)
+                guess = "+".join(info["candidates"])
+            else:
+                x0, guess = prev, ("previous" if prev is not None else "zero")
+            x, it, relres, code = sv.implicit_solve(x0=x0, tol=IMPLICIT["tol"], max_iter=IMPLICIT["max_iter"])
+            e1.record(stream)
+            torch.cuda.synchronize()
+            rec = {"step": k + 1, "guess": guess, "ms": e0.elapsed_time(e1), "bicgstab_iterations": it,
+                   "relres": relres, "code": code}
+            if info:
+                rec["guess_relres"] = info["relres"]
+                rec["start_relres"] = info["relres_combined"]
+                rec["guess_weights"] = info["weights"]
+            if pc == "self_block":
+                pi = sv.precond_info()
+                rec["precond_build_ms"] = {"total": pi["setup_ms"], "assembly": pi["assembly_ms"],
+                                           "factorisation": pi["factor_ms"]}
+            if prec == "mixed":
+                rec["fp64_residual_evaluations"] = sv.solver_stats()["outer"]
+            recs.append(rec)
+            X = X + IMPLICIT["dt"] * x[:3 * N]
+            prev = x
+        sv.close()
+        out[label] = {"precision": prec, "preconditioner": pc, "guess_policy": policy, "steps": recs}
+    if learned is not None:
+        learned.close()
+    base = out.get("plain_fp64")
+    if base:
+        for label, v in out.items():
+            v["speedup_vs_plain_fp64"] = [b["ms"] / r["ms"] for b, r in zip(base["steps"], v["steps"])]
     return {"workload": f"{IMPLICIT['workload']}: {nves} vesicles p={p} ({N} points), shear u=(y,0,0), "
-                        f"kappa={IMPLICIT['kappa']}, dt={IMPLICIT['dt']}, BiCGStab tol {IMPLICIT['tol']}, "
-                        "Galerkin form", "steps": out}
+                        f"kappa={IMPLICIT['kappa']}, dt={IMPLICIT['dt']}, BiCGStab tol {IMPLICIT['tol']} "
+                        "(true residual of the Galerkin system)",
+            "learned_guess": None if learned is None else os.path.relpath(DEFAULT_WEIGHTS, os.path.dirname(
+                os.path.abspath(__file__))),
+            "forms": out}
 
 
 def polydisperse_measurement(precision, local, stream):
@@ -358,6 +406,60 @@ def polydisperse_measurement(precision, local, stream):
     return {"workload": f"c3_4096ves_poly: 4096 vesicles, p counts {counts}, {N} points, 20% volume fraction",
             "ms_per_eval": ms, "points_per_s": N / (ms * 1e-3), "stages_ms": st,
             "error_vs_fp64_oracle": {"max_rel": worst, "sample": "all points of 2 vesicles with p <= 16"}}
+
+
+def alt_precision_measurement(precision, X, f, p, local, stream, steps, warmup):
+    """The same C2 evaluation in the other precision form (device time per step, L2
+    flushed between steps), its far-field roofline fraction and its error against the
+    FP64 oracle on the sampled points."""
+    import torch
+    from ves3d_b200 import _lib
+    from ves3d_b200.stokes_velocity import StokesVelocity
+    dev = torch.device("cuda", local)
+    ng = 2 * p * (p + 1)
+    nves = X.size // (3 * ng)
+    N = nves * ng
+    sv = StokesVelocity(p, 2 * p, precision=precision, device=local)
+    sv.set_stream(stream.cuda_stream)
+    dX = torch.from_numpy(X).to(dev)
+    dF = torch.from_numpy(f).to(dev)
+    out = torch.empty_like(dX)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    for _ in range(warmup):
+        sv.SetSrcCoord(dX)
+        sv.SetDensitySL(dF)
+        sv(out)
+    times, far_ms, setup_ms, apply_ms = [], [], [], []
+    for _ in range(steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sv.SetSrcCoord(dX)
+        sv.SetDensitySL(dF)
+        sv(out)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+        st = sv.stage_times()
+        far_ms.append(st["far_ms"])
+        setup_ms.append(st["setup_ms"])
+        apply_ms.append(st["self_apply_ms"])
+    vel = out.cpu().numpy()
+    sv.close()
+    ms = statistics.mean(times)
+    far_avg = statistics.mean(far_ms)
+    achieved = FLOPS_PER_PAIR * far_pairs(nves, ng) / (far_avg * 1e-3) / 1e12
+    peak = _lib.measure_fma_peak(precision == "fp64")
+    return {"precision": precision, "dtype": "f64" if precision == "fp64" else "f32+f64",
+            "value": N / (ms * 1e-3), "unit": "points/s", "ms_per_step": ms, "steps": steps,
+            "stages_ms": {"self_build": statistics.mean(setup_ms), "self_apply": statistics.mean(apply_ms),
+                          "far_field": far_avg},
+            "far_roofline": {"kernel": "k_far_f64" if precision == "fp64" else "k_far_f32",
+                             "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak},
+            "error_vs_fp64_oracle": {"max_rel": sampled_error_vs_oracle(X, f, p, vel),
+                                     "sample": "2 vesicles: full velocity at 256 of their points"}}
 
 
 def run_ours(args, world, rank, local):
@@ -492,9 +594,15 @@ def run_ours(args, world, rank, local):
             "clocks": clocks,
             "peaks_tflops": {"fp64_fma": peak64, "fp32_fma": peak32},
         }
-        if not args.no_implicit:
-            result["implicit_step"] = implicit_step_measurement(args.precision, local, stream)
-        if not args.no_poly:
+        # single-GPU characterisations (the other precision form, the implicit step, the
+        # polydisperse suspension) run at N=1 only: with N>1 the line is the scaling point
+        if world == 1:
+            other = "mixed" if args.precision == "fp64" else "fp64"
+            result[other] = alt_precision_measurement(other, X, f, p, local, stream, args.steps,
+                                                      min(args.warmup, 2))
+        if world == 1 and not args.no_implicit:
+            result["implicit_step"] = implicit_step_measurement(local, stream)
+        if world == 1 and not args.no_poly:
             result["polydisperse"] = polydisperse_measurement(args.precision, local, stream)
         if world == 1 and not args.no_cpu_baseline:
             cb = cpu_reference_rate(X, f, p)

@@ -102,11 +102,16 @@ __global__ void __launch_bounds__(256) k_synthesis(const double* __restrict__ S,
   }
 }
 
+// Functions per CTA: as many as 96 KB of shared memory holds (at most 8), but no more
+// than keeps two CTAs per SM busy -- small batches (one vesicle's worth of functions in
+// an operator assembly) are otherwise latency-bound on a handful of CTAs.
 static int pick_fpb(size_t per_fun_doubles, long nfun) {
   size_t budget = 96 * 1024 / sizeof(double);
   int fpb = (int)(budget / per_fun_doubles);
   if (fpb < 1) fpb = 1;
   if (fpb > 8) fpb = 8;
+  const long fill = nfun / (2 * 148);
+  if (fill < fpb) fpb = (int)(fill < 1 ? 1 : fill);
   if (fpb > nfun) fpb = (int)nfun;
   return fpb;
 }
