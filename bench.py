@@ -42,6 +42,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-implicit", action="store_true", help="skip the implicit-step measurement")
     ap.add_argument("--no-poly", action="store_true", help="skip the polydisperse measurement")
+    ap.add_argument("--no-alt", action="store_true", help="skip the measurement of the other precision form")
     return ap.parse_args()
 
 
@@ -596,7 +597,7 @@ def run_ours(args, world, rank, local):
         }
         # single-GPU characterisations (the other precision form, the implicit step, the
         # polydisperse suspension) run at N=1 only: with N>1 the line is the scaling point
-        if world == 1:
+        if world == 1 and not args.no_alt:
             other = "mixed" if args.precision == "fp64" else "fp64"
             result[other] = alt_precision_measurement(other, X, f, p, local, stream, args.steps,
                                                       min(args.warmup, 2))

@@ -1016,10 +1016,10 @@ __global__ void k_shift_null_mode(double* __restrict__ A, long nv, int nc) {
   Av[i0 * n + i0] += m > 0 ? m : 1.0;
 }
 
-__global__ void k_identity_blocks_f32(float* __restrict__ A, long nv, long n) {
+__global__ void k_identity_blocks(double* __restrict__ A, long nv, long n) {
   for (long g = (long)blockIdx.x * blockDim.x + threadIdx.x; g < nv * n * n; g += (long)gridDim.x * blockDim.x) {
     const long r = g % (n * n);
-    A[g] = (r % n) == (r / n) ? 1.f : 0.f;
+    A[g] = (r % n) == (r / n) ? 1.0 : 0.0;
   }
 }
 
@@ -1096,10 +1096,10 @@ int precond_apply(void* ctx, const double* x, double* y) {
 
 // Per-vesicle inverse of the isolated-vesicle Galerkin operator (the implicit operator
 // with the self part of the single layer only): columns by applying that operator to
-// unit vectors in FP64 (one column of every vesicle per application), then LU with
-// partial pivoting (cuSOLVER getrf) and solves against the identity (getrs) in FP32 --
-// the preconditioner only steers the iteration; the tests on the true residual fix the
-// accuracy of the solution.
+// unit vectors in FP64 (one column of every vesicle per application), LU with partial
+// pivoting (cuSOLVER getrf) and solves against the identity (getrs) in FP64, stored in
+// FP32 -- the preconditioner only steers the iteration; the tests on the true residual
+// fix the accuracy of the solution.
 int build_self_block_precond(ves3d_sv* sv) {
   int s;
   const int nc = ncoef_(sv->p), n = 4 * nc;
@@ -1130,7 +1130,7 @@ int build_self_block_precond(ves3d_sv* sv) {
   double *A = nullptr, *B = nullptr, *e = nullptr, *y = nullptr;
   int *piv = nullptr, *info = nullptr;
   if ((s = dalloc(&A, nv * nn))) return s;
-  if ((s = dalloc(&B, (nv * nn + 1) / 2)) || (s = dalloc(&e, nsh)) || (s = dalloc(&y, nsh)) ||
+  if ((s = dalloc(&B, nv * nn)) || (s = dalloc(&e, nsh)) || (s = dalloc(&y, nsh)) ||
       (s = dalloc(&piv, nv * (long)n)) || (s = dalloc(&info, nv))) {
     dfree(A); dfree(B); dfree(e); dfree(y); dfree(piv);
     return s;
@@ -1155,45 +1155,35 @@ int build_self_block_precond(ves3d_sv* sv) {
   }
   sv->self_only = false;
   sv->far_force_fp64 = 0;
-  // FP32 copy of the operator (the preconditioner is stored and applied in FP32)
-  float* Af = reinterpret_cast<float*>(B);  // B (nv nn / 2 doubles) holds the FP32 copy
   if (!s) {
     k_shift_null_mode<<<(unsigned)((nv + 127) / 128), 128, 0, sv->stream>>>(A, nv, nc);
     s = cuda_status(cudaGetLastError(), "k_shift_null_mode", __FILE__, __LINE__);
     if (!s) launch_counter()++;
   }
   if (!s) {
-    k_to_f32<<<grid_1d(nv * nn), 256, 0, sv->stream>>>(A, nv * nn, Af);
-    s = cuda_status(cudaGetLastError(), "k_to_f32", __FILE__, __LINE__);
-    if (!s) launch_counter()++;
-  }
-  if (!s) {
-    k_identity_blocks_f32<<<grid_1d(nv * nn), 256, 0, sv->stream>>>(sv->pc_inv, nv, n);
+    k_identity_blocks<<<grid_1d(nv * nn), 256, 0, sv->stream>>>(B, nv, n);
     s = cuda_status(cudaGetLastError(), "k_identity_blocks", __FILE__, __LINE__);
     if (!s) launch_counter()++;
   }
   int lwork = 0;
-  if (!s && cusolverDnSgetrf_bufferSize(sv->pc_solver[0], n, n, Af, n, &lwork) != CUSOLVER_STATUS_SUCCESS) {
-    set_error("cusolverDnSgetrf_bufferSize failed");
+  if (!s && cusolverDnDgetrf_bufferSize(sv->pc_solver[0], n, n, A, n, &lwork) != CUSOLVER_STATUS_SUCCESS) {
+    set_error("cusolverDnDgetrf_bufferSize failed");
     s = VES3D_ERR_CUDA;
   }
-  lwork = std::max(lwork, 2);
-  float* work = reinterpret_cast<float*>(A);  // the FP64 operator is no longer needed
-  if (!s && (long)lwork * kPcStreams > 2 * nv * nn) {
-    set_error("cuSOLVER workspace larger than expected");
-    s = VES3D_ERR_NOMEM;
-  }
-  // dense LU + solve against the identity, vesicles spread over kPcStreams streams (one
-  // factorisation of n ~ 10^3 does not fill the GPU)
+  lwork = std::max(lwork, 1);
+  double* work = nullptr;
+  if (!s) s = dalloc(&work, (size_t)lwork * kPcStreams);
+  // dense LU + solve against the identity in FP64, vesicles spread over kPcStreams streams
+  // (one factorisation of n ~ 10^3 is latency-bound and does not fill the GPU)
   if (!s) s = cuda_status(cudaEventRecord(sv->pc_ev[1], sv->stream), "event", __FILE__, __LINE__);
   for (int k = 0; k < kPcStreams && !s; k++)
     s = cuda_status(cudaStreamWaitEvent(sv->pc_stream[k], sv->pc_ev[1], 0), "wait", __FILE__, __LINE__);
   for (long v = 0; v < nv && !s; v++) {
     const int k = (int)(v % kPcStreams);
-    if (cusolverDnSgetrf(sv->pc_solver[k], n, n, Af + v * nn, n, work + (long)k * lwork, piv + v * n, info + v) !=
+    if (cusolverDnDgetrf(sv->pc_solver[k], n, n, A + v * nn, n, work + (long)k * lwork, piv + v * n, info + v) !=
             CUSOLVER_STATUS_SUCCESS ||
-        cusolverDnSgetrs(sv->pc_solver[k], CUBLAS_OP_N, n, n, Af + v * nn, n, piv + v * n, sv->pc_inv + v * nn, n,
-                         info + v) != CUSOLVER_STATUS_SUCCESS) {
+        cusolverDnDgetrs(sv->pc_solver[k], CUBLAS_OP_N, n, n, A + v * nn, n, piv + v * n, B + v * nn, n, info + v) !=
+            CUSOLVER_STATUS_SUCCESS) {
       set_error("cuSOLVER getrf/getrs failed for vesicle %ld", v);
       s = VES3D_ERR_CUDA;
     }
@@ -1202,6 +1192,11 @@ int build_self_block_precond(ves3d_sv* sv) {
   for (int k = 0; k < kPcStreams; k++) {
     cudaEventRecord(sv->pc_ev[3 + k], sv->pc_stream[k]);
     cudaStreamWaitEvent(sv->stream, sv->pc_ev[3 + k], 0);
+  }
+  if (!s) {
+    k_to_f32<<<grid_1d(nv * nn), 256, 0, sv->stream>>>(B, nv * nn, sv->pc_inv);
+    s = cuda_status(cudaGetLastError(), "k_to_f32", __FILE__, __LINE__);
+    if (!s) launch_counter()++;
   }
   std::vector<int> hinfo(nv, 0);
   if (!s)
@@ -1227,6 +1222,7 @@ int build_self_block_precond(ves3d_sv* sv) {
   dfree(B);
   dfree(e);
   dfree(y);
+  dfree(work);
   dfree(piv);
   dfree(info);
   return s;
