@@ -62,7 +62,11 @@ struct RingCfg {
   static constexpr int OFF_Q = OFF_DLEG + NC * LG;
   static constexpr int OFF_P = OFF_Q + (SZ_A > SZ_K ? SZ_A : SZ_K);
   static constexpr int OFF_TRG = OFF_P + (SZ_X > SZ_C ? SZ_X : SZ_C);
-  static constexpr int TOTAL = OFF_TRG + 8;
+  // small index/weight tables read in every latitude group, kept on chip
+  static constexpr int OFF_SW = OFF_TRG + 8;                    // sing_w [L1]
+  static constexpr int OFF_BO = OFF_SW + L1;                    // blk_off [F0 + 1] (int)
+  static constexpr int OFF_JF = OFF_BO + (F0 + 2) / 2;          // jf_of_coef [NC] (unsigned char)
+  static constexpr int TOTAL = OFF_JF + (NC + 7) / 8;
   static constexpr size_t SMEM = (size_t)TOTAL * sizeof(double);
   static constexpr int NOUT = 12 * NC;
   static constexpr int OUT_PER_THREAD = (NOUT + 255) / 256;
@@ -84,8 +88,14 @@ __global__ void __launch_bounds__(256, 2) k_build_ring(const double* __restrict_
   double* sX = sm + G::OFF_P;
   double* sC = sm + G::OFF_P;
   double* trg = sm + G::OFF_TRG;
+  double* sSw = sm + G::OFF_SW;
+  int* sBo = reinterpret_cast<int*>(sm + G::OFF_BO);
+  unsigned char* sJf = reinterpret_cast<unsigned char*>(sm + G::OFF_JF);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const long rot = blockIdx.x;
+  for (int i = tid; i < G::L1; i += 256) sSw[i] = __ldg(T.sing_w + i);
+  for (int i = tid; i <= G::F0; i += 256) sBo[i] = __ldg(T.blk_off + i);
+  for (int i = tid; i < G::NC; i += 256) sJf[i] = (unsigned char)__ldg(T.jf_of_coef + i);
 
   // ---- rotated coefficients, DFT tables, pole targets ----------------------------------
   for (int i = tid; i < 3 * G::NC; i += 256) sR[i] = R[rot * 3 * G::NC + i];
@@ -113,8 +123,8 @@ __global__ void __launch_bounds__(256, 2) k_build_ring(const double* __restrict_
     for (int i = tid; i < G::NC * G::LG; i += 256) {
       const int l = i / G::NC, c = i - l * G::NC;
       const bool ok = l < nlat;
-      sLeg[i] = ok ? __ldg(T.syn1_leg + c * G::L1 + lat0 + l) : 0.0;
-      sdLeg[i] = ok ? __ldg(T.syn1_dleg + c * G::L1 + lat0 + l) : 0.0;
+      sLeg[i] = ok ? __ldg(T.syn1_leg_t + (lat0 + l) * G::NC + c) : 0.0;
+      sdLeg[i] = ok ? __ldg(T.syn1_dleg_t + (lat0 + l) * G::NC + c) : 0.0;
     }
     __syncthreads();
     // ---- Legendre synthesis of the group's latitudes: A[(l,d)][k], dA -----------------
@@ -123,7 +133,7 @@ __global__ void __launch_bounds__(256, 2) k_build_ring(const double* __restrict_
       double s = 0.0, d = 0.0;
       if (row < 3 * nlat) {
         const int l = row / 3, dd = row - 3 * l;
-        const int c0 = __ldg(T.blk_off + k), c1 = __ldg(T.blk_off + k + 1);
+        const int c0 = sBo[k], c1 = sBo[k + 1];
         const double* r = sR + dd * G::NC;
         for (int c = c0; c < c1; c++) {
           s = fma(r[c], sLeg[l * G::NC + c], s);
@@ -177,7 +187,7 @@ __global__ void __launch_bounds__(256, 2) k_build_ring(const double* __restrict_
         const double r2 = dx * dx + dy * dy + dz * dz;
         double rinv = 1.0 / sqrt(r2);
         if (r2 <= 2.220446049250313e-16) rinv = 0.0;
-        const double a1 = kInv8Pi * __ldg(T.sing_w + (t ? lat : G::P1 - lat)) * area * rinv;
+        const double a1 = kInv8Pi * sSw[t ? lat : G::P1 - lat] * area * rinv;
         const double a2 = a1 * rinv * rinv;
         double* k = sK + (l * 12 + t * 6) * G::LDK + j;
         k[0] = a1 + dx * dx * a2;
@@ -215,7 +225,7 @@ __global__ void __launch_bounds__(256, 2) k_build_ring(const double* __restrict_
       const int o = tid + q * 256;
       if (o < G::NOUT) {
         const int comp = o / G::NC, c = o - comp * G::NC;
-        const int jf = __ldg(T.jf_of_coef + c);
+        const int jf = sJf[c];
         double s = acc[q];
         for (int l = 0; l < nlat; l++) s = fma(sC[(l * 12 + comp) * G::LDC + jf], sLeg[l * G::NC + c], s);
         acc[q] = s;

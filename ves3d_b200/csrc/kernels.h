@@ -21,6 +21,8 @@ struct DevTables {
   int *mr_off = nullptr, *perm = nullptr, *perm_off = nullptr, *pos_in_block = nullptr;
   double *sing_w = nullptr, *smooth_w0 = nullptr, *qp = nullptr, *cos_tab = nullptr, *sin_tab = nullptr;
   double *syn0_d2leg = nullptr, *syn0_d2four = nullptr;
+  // syn1_leg / syn1_dleg transposed to [latitude][coefficient] (contiguous per latitude)
+  double *syn1_leg_t = nullptr, *syn1_dleg_t = nullptr;
 };
 
 // Geometry record per point: E, F, G (divided by W^2), W, n[3], cu[3], cv[3], H, K.

@@ -67,7 +67,8 @@ struct TablesOwner {
     void* ptrs[] = {d.ana_four, d.ana_leg, d.syn0_leg, d.syn0_dleg, d.syn0_four, d.syn0_dfour, d.syn1_leg,
                     d.syn1_dleg, d.syn1_four, d.syn1_dfour, d.synT_four, d.jf_of_coef, d.blk_off, d.m_of_coef,
                     d.n_of_coef, d.partner, d.is_sin, d.mr, d.mr_off, d.perm, d.perm_off, d.pos_in_block,
-                    d.sing_w, d.smooth_w0, d.qp, d.cos_tab, d.sin_tab, d.syn0_d2leg, d.syn0_d2four};
+                    d.sing_w, d.smooth_w0, d.qp, d.cos_tab, d.sin_tab, d.syn0_d2leg, d.syn0_d2four,
+                    d.syn1_leg_t, d.syn1_dleg_t};
     for (void* p : ptrs) dfree(p);
   }
   int upload(cudaStream_t st) {
@@ -83,6 +84,20 @@ struct TablesOwner {
     s |= dupload(&d.syn0_dfour, h.syn0.dfour, st);
     s |= dupload(&d.syn1_leg, h.syn1.leg, st);
     s |= dupload(&d.syn1_dleg, h.syn1.dleg, st);
+    {
+      // [coefficient][latitude] -> [latitude][coefficient]
+      const size_t nc = (size_t)ncoef_(h.p0), nl = (size_t)h.p1 + 1;
+      std::vector<double> a(nc * nl), b(nc * nl);
+      if (h.syn1.leg.size() == nc * nl && h.syn1.dleg.size() == nc * nl) {
+        for (size_t c = 0; c < nc; c++)
+          for (size_t l = 0; l < nl; l++) {
+            a[l * nc + c] = h.syn1.leg[c * nl + l];
+            b[l * nc + c] = h.syn1.dleg[c * nl + l];
+          }
+        s |= dupload(&d.syn1_leg_t, a, st);
+        s |= dupload(&d.syn1_dleg_t, b, st);
+      }
+    }
     s |= dupload(&d.syn1_four, h.syn1.four, st);
     s |= dupload(&d.syn1_dfour, h.syn1.dfour, st);
     s |= dupload(&d.synT_four, h.synT.four, st);
