@@ -3,6 +3,8 @@
 // that scatters the result into the per-vesicle self-matrix layout.
 // Math: SphericalHarmonics<Real>::RotateAll / StokesSingularInteg_ / RotateTranspose
 // (src/SphericalHarmonics.cc:363-541, 954-1180).
+#include <cstdlib>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -213,9 +215,151 @@ __global__ void __launch_bounds__(256) k_rotate_transpose_scatter(const double* 
   }
 }
 
+// VES3D_TC_ROTATE=0 selects the CUDA-core form of the rotate-transpose (for comparison).
+static bool tc_rotate_disabled() {
+  static const bool off = [] {
+    const char* e = getenv("VES3D_TC_ROTATE");
+    return e && e[0] == '0';
+  }();
+  return off;
+}
+
+__device__ __forceinline__ void dmma_rt(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+// Row stride >= n with stride = 4 (mod 16) doubles: conflict-free m8n8k4 A fragments.
+__host__ __device__ constexpr int pad4_16(int n) { return ((n + 11) / 16) * 16 + 4; }
+
+// RotateTranspose + inverse phase + Rearrange on the FP64 tensor cores. One CTA per
+// (latitude rotation t, vesicle v); rows are (pole, component, longitude j), processed in
+// blocks of cb components x p0 longitudes. A block's coefficients are staged degree-major
+// in shared memory; for every degree n the rotation back is one GEMM
+//     Out[row][b] = sum_k In[row][po(n) + k] * M_{t,n}[b][k]       (b, k < bn)
+// on mma.sync m8n8k4 (A = In from shared memory, B = M from the L1/L2-resident table,
+// masked to the block), written back in place after a barrier; reads of the K padding
+// land in the next degree's (finite) columns and meet zeros in B. Then the longitude
+// phase is undone and the values are scattered into the self-matrix grid layout, as in
+// k_rotate_transpose_scatter.
+__global__ void __launch_bounds__(256, 2) k_rotate_transpose_tc(const double* __restrict__ C, int p0, int cb, int ldi,
+                                                                DevTables T, double* __restrict__ SL3) {
+  extern __shared__ __align__(16) double sm[];
+  const int nc = p0 * (p0 + 2), ng = 2 * p0 * (p0 + 1);
+  const int rows = cb * p0, rows8 = (rows + 7) & ~7;
+  double* sIn = sm;                                                        // rows8 x ldi
+  unsigned short* sDm = reinterpret_cast<unsigned short*>(sm + (size_t)rows8 * ldi);  // nc
+  const int t = blockIdx.x;
+  const long v = blockIdx.y;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int grow = lane >> 2, gcol = lane & 3;
+  for (int c = tid; c < nc; c += 256)
+    sDm[c] = (unsigned short)(__ldg(T.perm_off + __ldg(T.n_of_coef + c)) + __ldg(T.pos_in_block + c));
+  // zero the K padding of every row and the padding rows once (never overwritten)
+  for (int i = tid; i < rows8 * ldi; i += 256) {
+    const int r = i / ldi, col = i - r * ldi;
+    if (r >= rows || col >= nc) sIn[i] = 0.0;
+  }
+  const int ci0[6] = {0, 0, 0, 1, 1, 2}, co0[6] = {0, 1, 2, 1, 2, 2};
+  const int mtiles = rows8 / 8;
+  for (int pole = 0; pole < 2; pole++) {
+    for (int comp0 = 0; comp0 < 6; comp0 += cb) {
+      __syncthreads();
+      // stage: In[(cc, j)][dm(c)] = C[v][t][j][pole][comp0 + cc][c]
+      for (int i = tid; i < rows * nc; i += 256) {
+        const int r = i / nc, c = i - r * nc;
+        const int cc = r / p0, j = r - cc * p0;
+        sIn[r * ldi + sDm[c]] =
+            C[((((v * (p0 + 1) + t) * p0 + j) * 2 + pole) * 6 + comp0 + cc) * (long)nc + c];
+      }
+      __syncthreads();
+      for (int n = 0; n <= p0; n++) {
+        const int po = __ldg(T.perm_off + n), bn = __ldg(T.perm_off + n + 1) - po;
+        const double* M = T.mr + __ldg(T.mr_off + t * (p0 + 1) + n);
+        const int ntiles = (bn + 7) / 8, ksteps = (bn + 3) / 4;
+        const int nitems = mtiles * ntiles;
+        // at most 3 items per warp held in registers across the barrier (nitems <= 24
+        // for rows8 <= 48 and bn <= 32; larger problems loop in rounds)
+        for (int base = 0; base < nitems; base += 24) {
+          double acc[3][2];
+          int item[3];
+#pragma unroll
+          for (int q = 0; q < 3; q++) {
+            item[q] = base + warp + 8 * q;
+            acc[q][0] = acc[q][1] = 0.0;
+            if (item[q] < nitems) {
+              const int mt = item[q] / ntiles, nt = item[q] - mt * ntiles;
+              const double* a = sIn + (mt * 8 + grow) * ldi + po + gcol;
+              const int nn = nt * 8 + grow;
+              for (int ks = 0; ks < ksteps; ks++) {
+                const int kk = ks * 4 + gcol;
+                const double b = (nn < bn && kk < bn) ? __ldg(M + nn * bn + kk) : 0.0;
+                dmma_rt(acc[q][0], acc[q][1], a[ks * 4], b);
+              }
+            }
+          }
+          __syncthreads();
+#pragma unroll
+          for (int q = 0; q < 3; q++) {
+            if (item[q] < nitems) {
+              const int mt = item[q] / ntiles, nt = item[q] - mt * ntiles;
+              const int row = mt * 8 + grow, col = nt * 8 + 2 * gcol;
+              if (row < rows) {
+                if (col < bn) sIn[row * ldi + po + col] = acc[q][0];
+                if (col + 1 < bn) sIn[row * ldi + po + col + 1] = acc[q][1];
+              }
+            }
+          }
+          __syncthreads();
+        }
+      }
+      // inverse phase and scatter; consecutive threads take consecutive j
+      for (int i = tid; i < rows * nc; i += 256) {
+        const int j = i % p0, rest = i / p0;
+        const int c = rest % nc, cc = rest / nc;
+        const double* in = sIn + (cc * p0 + j) * ldi;
+        const int pc = __ldg(T.partner + c);
+        double val;
+        if (pc < 0) {
+          val = in[sDm[c]];
+        } else {
+          const int q = (__ldg(T.m_of_coef + c) * j) % (2 * p0);
+          const double cs = __ldg(T.cos_tab + q), sn = __ldg(T.sin_tab + q);
+          if (!__ldg(T.is_sin + c))
+            val = in[sDm[c]] * cs - in[sDm[pc]] * sn;
+          else
+            val = in[sDm[pc]] * sn + in[sDm[c]] * cs;
+        }
+        const int grid = pole == 0 ? t * 2 * p0 + j : (p0 - t) * 2 * p0 + p0 + j;
+        const int comp = comp0 + cc;
+        const int cin = ci0[comp], cout = co0[comp];
+        SL3[(((v * 3 + cin) * nc + c) * 3 + cout) * (long)ng + grid] = val;
+        if (cin != cout) SL3[(((v * 3 + cout) * nc + c) * 3 + cin) * (long)ng + grid] = val;
+      }
+    }
+  }
+}
+
 int launch_rotate_transpose_scatter(const double* C, long nv, const DevTables& T, double* SL3, cudaStream_t st) {
   if (nv <= 0) return VES3D_OK;
   const int p0 = T.p0, nc = ncoef_(p0);
+  {
+    // tensor-core form: the largest component block (3, 2 or 1 components x p0 rows)
+    // whose staging fits two CTAs per SM; 6 must be a multiple of the block
+    const int ldi = pad4_16(nc + 3);
+    for (int cb : {3, 2, 1}) {
+      const int rows8 = ((cb * p0) + 7) & ~7;
+      const size_t smem = (size_t)rows8 * ldi * sizeof(double) + ((size_t)nc * 2 + 15) / 16 * 16;
+      if (smem <= 112 * 1024 && rows8 / 8 * ((2 * p0 + 7) / 8) <= 24 * 4 && !tc_rotate_disabled()) {
+        VES3D_CK(cudaFuncSetAttribute(k_rotate_transpose_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        dim3 grid(p0 + 1, (unsigned)nv);
+        k_rotate_transpose_tc<<<grid, 256, smem, st>>>(C, p0, cb, ldi, T, SL3);
+        VES3D_LAUNCHED();
+        return VES3D_OK;
+      }
+    }
+  }
   const int mpt = mr_per_t(T);
   // two CTAs per SM: keep shared memory under ~110 KB; whole groups of kRtJ rotations
   long budget = (110 * 1024) / (long)sizeof(double) - mpt;
