@@ -11,6 +11,8 @@
 // tables are small and read through the read-only cache.
 #include <cstdlib>
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -168,10 +170,14 @@ struct AnaTcCfg {
   static constexpr int ROWS = ((FB * NLAT + 7) / 8) * 8;
   static constexpr int LD = pad4m16(NLON);
   static constexpr int OFF_A = 0, OFF_F = ROWS * LD, OFF_M = 2 * ROWS * LD, OFF_L = OFF_M + NLON * LD;
-  static constexpr int TOTAL = OFF_L + NC * NLAT;
+  static constexpr int OFF_JF = OFF_L + NC * NLAT;  // jf [NC] (int)
+  static constexpr int TOTAL = OFF_JF + (NC + 1) / 2;
   static constexpr size_t SMEM = (size_t)TOTAL * sizeof(double);
 };
 
+// Persistent CTAs: the DFT and Legendre tables are staged once per CTA, which then walks
+// groups of FB functions (grid-stride). Per group: rows (function, latitude) x 2p DFT on
+// the tensor cores, then per-frequency Legendre sums on the CUDA cores.
 template <int P>
 __global__ void __launch_bounds__(256, 2) k_analysis_tc(const double* __restrict__ in, long nfun,
                                                         const double* __restrict__ four, const double* __restrict__ leg,
@@ -182,47 +188,64 @@ __global__ void __launch_bounds__(256, 2) k_analysis_tc(const double* __restrict
   double* sF = sm + G::OFF_F;
   double* sM = sm + G::OFF_M;
   double* sL = sm + G::OFF_L;
+  int* sJf = reinterpret_cast<int*>(sm + G::OFF_JF);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const long f0 = (long)blockIdx.x * G::FB;
-  const int nf = (int)min((long)G::FB, nfun - f0);
-  const double* src = in + f0 * G::NLAT * G::NLON;
-  for (int i = tid; i < G::ROWS * G::NLON; i += 256) {
-    const int r = i / G::NLON, j = i - r * G::NLON;
-    sA[r * G::LD + j] = r < nf * G::NLAT ? src[i] : 0.0;
-  }
   for (int i = tid; i < G::NLON * G::NLON; i += 256) {
     const int r = i / G::NLON, j = i - r * G::NLON;
     sM[r * G::LD + j] = __ldg(four + i);
   }
   for (int i = tid; i < G::NC * G::NLAT; i += 256) sL[i] = __ldg(leg + i);
-  __syncthreads();
+  for (int i = tid; i < G::NC; i += 256) sJf[i] = __ldg(jf + i);
   const int grow = lane >> 2, gcol = lane & 3;
   constexpr int MT = G::ROWS / 8, NT = G::NLON / 8;
-  for (int it = warp; it < MT * NT; it += 8) {
-    const int nt = it % NT, mt = it / NT;
-    const double* a = sA + (mt * 8 + grow) * G::LD + gcol;
-    const double* b = sM + gcol * G::LD + nt * 8 + grow;  // B[k][n] = four[k][n]
-    double c0 = 0, c1 = 0, d0 = 0, d1 = 0;
-#pragma unroll
-    for (int ks = 0; ks < G::NLON / 4; ks += 2) {
-      dmma_a(c0, c1, a[ks * 4], b[ks * 4 * G::LD]);
-      if (ks + 1 < G::NLON / 4) dmma_a(d0, d1, a[ks * 4 + 4], b[(ks * 4 + 4) * G::LD]);
+  const long ngroups = (nfun + G::FB - 1) / G::FB;
+  for (long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+    const long f0 = grp * G::FB;
+    const int nf = (int)min((long)G::FB, nfun - f0);
+    const double* src = in + f0 * G::NLAT * G::NLON;
+    __syncthreads();  // the previous group's sA / sF reads are done
+    for (int i = tid; i < G::ROWS * G::NLON; i += 256) {
+      const int r = i / G::NLON, j = i - r * G::NLON;
+      sA[r * G::LD + j] = r < nf * G::NLAT ? src[i] : 0.0;
     }
-    double* o = sF + (mt * 8 + grow) * G::LD + nt * 8 + 2 * gcol;
-    o[0] = c0 + d0;
-    o[1] = c1 + d1;
-  }
-  __syncthreads();
-  for (int i = tid; i < nf * G::NC; i += 256) {
-    const int f = i / G::NC, c = i - f * G::NC;
-    const int k = __ldg(jf + c);
-    const double* fr = sF + (f * G::NLAT) * G::LD + k;
-    const double* lr = sL + c * G::NLAT;
-    double s = 0.0;
+    __syncthreads();
+    for (int it = warp; it < MT * NT; it += 8) {
+      const int nt = it % NT, mt = it / NT;
+      const double* a = sA + (mt * 8 + grow) * G::LD + gcol;
+      const double* b = sM + gcol * G::LD + nt * 8 + grow;  // B[k][n] = four[k][n]
+      double c0 = 0, c1 = 0, d0 = 0, d1 = 0;
 #pragma unroll
-    for (int lat = 0; lat < G::NLAT; lat++) s = fma(fr[lat * G::LD], lr[lat], s);
-    out[(f0 + f) * G::NC + c] = s;
+      for (int ks = 0; ks < G::NLON / 4; ks += 2) {
+        dmma_a(c0, c1, a[ks * 4], b[ks * 4 * G::LD]);
+        if (ks + 1 < G::NLON / 4) dmma_a(d0, d1, a[ks * 4 + 4], b[(ks * 4 + 4) * G::LD]);
+      }
+      double* o = sF + (mt * 8 + grow) * G::LD + nt * 8 + 2 * gcol;
+      o[0] = c0 + d0;
+      o[1] = c1 + d1;
+    }
+    __syncthreads();
+    for (int i = tid; i < nf * G::NC; i += 256) {
+      const int f = i / G::NC, c = i - f * G::NC;
+      const int k = sJf[c];
+      const double* fr = sF + (f * G::NLAT) * G::LD + k;
+      const double* lr = sL + c * G::NLAT;
+      double s = 0.0;
+#pragma unroll
+      for (int lat = 0; lat < G::NLAT; lat++) s = fma(fr[lat * G::LD], lr[lat], s);
+      out[(f0 + f) * G::NC + c] = s;
+    }
   }
+}
+
+static int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
 }
 
 template <int P>
@@ -230,8 +253,9 @@ static int launch_ana_tc(const double* in, long nfun, const double* four, const 
                          double* out, cudaStream_t st) {
   using G = AnaTcCfg<P>;
   VES3D_CK(cudaFuncSetAttribute(k_analysis_tc<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM));
-  const long nblk = (nfun + G::FB - 1) / G::FB;
-  k_analysis_tc<P><<<(unsigned)nblk, 256, G::SMEM, st>>>(in, nfun, four, leg, jf, out);
+  const long ngroups = (nfun + G::FB - 1) / G::FB;
+  const long grid = std::min(ngroups, 2L * sm_count());
+  k_analysis_tc<P><<<(unsigned)grid, 256, G::SMEM, st>>>(in, nfun, four, leg, jf, out);
   VES3D_LAUNCHED();
   return VES3D_OK;
 }
