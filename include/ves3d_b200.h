@@ -158,9 +158,16 @@ int ves3d_sv_solver_stats(ves3d_sv* sv, int* outer, int* inner);
  * The solution's accuracy is set by the tolerance on the true residual in every case. */
 enum ves3d_precond { VES3D_PRECOND_NONE = 0, VES3D_PRECOND_DIAG_SPECTRAL = 1, VES3D_PRECOND_SELF_BLOCK = 2 };
 int ves3d_sv_set_precond(ves3d_sv* sv, int scheme);
+/* Rebuild the preconditioner only every `every` surface updates (default 1: after every
+ * ves3d_sv_set_src_coord). A lagged preconditioner is one built for surfaces a few time
+ * steps old; with right preconditioning it changes the iteration count, never the
+ * tolerance the solution meets. A change of vesicle count, dt or kappa always rebuilds. */
+int ves3d_sv_set_precond_refresh(ves3d_sv* sv, int every);
 /* Device time of the last preconditioner build, ms[3] = {total, operator assembly, LU
- * factorisation and inversion} in ms, and the bytes the preconditioner holds. */
-int ves3d_sv_precond_info(ves3d_sv* sv, double* ms, size_t* bytes);
+ * factorisation and inversion} in ms, the bytes the preconditioner holds, and (age, may
+ * be NULL) the surface updates since it was built (0: built for the current surfaces,
+ * -1: not built yet or invalidated). */
+int ves3d_sv_precond_info(ves3d_sv* sv, double* ms, size_t* bytes, int* age);
 
 /* ---------------------------------------------------------------------------
  * Initial guess of the implicit solve. The reference starts each solve from the previous

@@ -59,7 +59,8 @@ SIGNATURES = [
     ("ves3d_svp_stage_times", _i, [_vp, ctypes.POINTER(ctypes.c_float)]),
     ("ves3d_sv_solver_stats", _i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     ("ves3d_sv_set_precond", _i, [_vp, _i]),
-    ("ves3d_sv_precond_info", _i, [_vp, _dp, ctypes.POINTER(_sz)]),
+    ("ves3d_sv_precond_info", _i, [_vp, _dp, ctypes.POINTER(_sz), ctypes.POINTER(_i)]),
+    ("ves3d_sv_set_precond_refresh", _i, [_vp, _i]),
     ("ves3d_sv_guess_features", _i, [_vp, _vp, _i]),
     ("ves3d_sv_guess_targets", _i, [_vp, _vp, _vp, _i]),
     ("ves3d_sv_guess_from_targets", _i, [_vp, _vp, _vp, _i]),

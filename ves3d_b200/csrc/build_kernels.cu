@@ -180,12 +180,13 @@ __global__ void __launch_bounds__(256, 2) k_build_ring(const double* __restrict_
       const double ax = xt[0], ay = xt[G::LDX], az = xt[2 * G::LDX];
       const double bx = xp[0], by = xp[G::LDX], bz = xp[2 * G::LDX];
       const double nx = ay * bz - az * by, ny = az * bx - ax * bz, nz = ax * by - ay * bx;
-      const double area = sqrt(nx * nx + ny * ny + nz * nz);
+      const double n2 = nx * nx + ny * ny + nz * nz;
+      const double area = n2 * rsqrt_f64(n2);  // |X_theta x X_phi| > 0 on the upsampled grid
 #pragma unroll
       for (int t = 0; t < 2; t++) {
         const double dx = trg[t] - px, dy = trg[2 + t] - py, dz = trg[4 + t] - pz;
         const double r2 = dx * dx + dy * dy + dz * dz;
-        double rinv = 1.0 / sqrt(r2);
+        double rinv = rsqrt_f64(r2);
         if (r2 <= 2.220446049250313e-16) rinv = 0.0;
         const double a1 = kInv8Pi * sSw[t ? lat : G::P1 - lat] * area * rinv;
         const double a2 = a1 * rinv * rinv;

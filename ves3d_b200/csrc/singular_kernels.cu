@@ -224,6 +224,8 @@ static bool tc_rotate_disabled() {
   return off;
 }
 
+constexpr int kRtMaxK = 8;  // K steps of 4: rotation blocks up to 32 wide (p0 <= 16)
+
 __device__ __forceinline__ void dmma_rt(double& c0, double& c1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
                : "+d"(c0), "+d"(c1)
@@ -292,11 +294,16 @@ __global__ void __launch_bounds__(256, 2) k_rotate_transpose_tc(const double* __
               const int mt = item[q] / ntiles, nt = item[q] - mt * ntiles;
               const double* a = sIn + (mt * 8 + grow) * ldi + po + gcol;
               const int nn = nt * 8 + grow;
-              for (int ks = 0; ks < ksteps; ks++) {
+              // B fragments first (independent loads in flight together), then the MMAs
+              double bv[kRtMaxK];
+#pragma unroll
+              for (int ks = 0; ks < kRtMaxK; ks++) {
                 const int kk = ks * 4 + gcol;
-                const double b = (nn < bn && kk < bn) ? __ldg(M + nn * bn + kk) : 0.0;
-                dmma_rt(acc[q][0], acc[q][1], a[ks * 4], b);
+                bv[ks] = (ks < ksteps && nn < bn && kk < bn) ? __ldg(M + nn * bn + kk) : 0.0;
               }
+#pragma unroll
+              for (int ks = 0; ks < kRtMaxK; ks++)
+                if (ks < ksteps) dmma_rt(acc[q][0], acc[q][1], a[ks * 4], bv[ks]);
             }
           }
           __syncthreads();
@@ -351,7 +358,7 @@ int launch_rotate_transpose_scatter(const double* C, long nv, const DevTables& T
     for (int cb : {3, 2, 1}) {
       const int rows8 = ((cb * p0) + 7) & ~7;
       const size_t smem = (size_t)rows8 * ldi * sizeof(double) + ((size_t)nc * 2 + 15) / 16 * 16;
-      if (smem <= 112 * 1024 && rows8 / 8 * ((2 * p0 + 7) / 8) <= 24 * 4 && !tc_rotate_disabled()) {
+      if (p0 <= 16 && smem <= 112 * 1024 && !tc_rotate_disabled()) {
         VES3D_CK(cudaFuncSetAttribute(k_rotate_transpose_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         dim3 grid(p0 + 1, (unsigned)nv);
         k_rotate_transpose_tc<<<grid, 256, smem, st>>>(C, p0, cb, ldi, T, SL3);

@@ -160,6 +160,9 @@ struct ves3d_sv {
   double* pc_diag = nullptr;   // diagonal-spectral scales [4 nc]
   long pc_cap = 0;
   bool pc_valid = false;
+  int pc_refresh = 1;          // rebuild after this many surface updates (1 = every update)
+  int pc_age = 0;              // surface updates since the last build
+  long pc_nves = 0;            // vesicle count the preconditioner was built for
   double pc_ms[3] = {0, 0, 0};  // last build: total, assembly, factorisation (device ms)
   cudaStream_t pc_stream[kPcStreams] = {};
   cusolverDnHandle_t pc_solver[kPcStreams] = {};
@@ -504,7 +507,12 @@ int ves3d_sv_set_src_coord(ves3d_sv* sv, const double* S, long n_ves, int is_dev
   sv->sl_valid = false;
   sv->parts_valid = false;
   sv->geo_valid = false;
-  sv->pc_valid = false;
+  // a lagged preconditioner survives pc_refresh - 1 surface updates (right
+  // preconditioning: it steers the iteration only, the tolerance is on the true residual)
+  if (sv->pc_valid && sv->pc_nves == n_ves && sv->pc_age + 1 < sv->pc_refresh)
+    sv->pc_age++;
+  else
+    sv->pc_valid = false;
   return VES3D_OK;
 }
 
@@ -1232,6 +1240,8 @@ int build_self_block_precond(ves3d_sv* sv) {
     sv->pc_ms[1] = a;
     sv->pc_ms[2] = b;
     sv->pc_valid = true;
+    sv->pc_age = 0;
+    sv->pc_nves = nv;
   }
   dfree(A);
   dfree(B);
@@ -1248,6 +1258,8 @@ int ensure_precond(ves3d_sv* sv) {
   if (sv->precond == VES3D_PRECOND_DIAG_SPECTRAL) {
     sv->pc_ms[0] = sv->pc_ms[1] = sv->pc_ms[2] = 0;
     sv->pc_valid = true;
+    sv->pc_age = 0;
+    sv->pc_nves = sv->nves;
     return VES3D_OK;
   }
   return build_self_block_precond(sv);
@@ -1352,10 +1364,19 @@ int ves3d_sv_set_precond(ves3d_sv* sv, int scheme) {
   return VES3D_OK;
 }
 
-int ves3d_sv_precond_info(ves3d_sv* sv, double* ms, size_t* bytes) {
+int ves3d_sv_set_precond_refresh(ves3d_sv* sv, int every) {
+  int s = check_sv(sv);
+  if (s) return s;
+  VES3D_ARG(every >= 1, "refresh interval must be >= 1");
+  sv->pc_refresh = every;
+  return VES3D_OK;
+}
+
+int ves3d_sv_precond_info(ves3d_sv* sv, double* ms, size_t* bytes, int* age) {
   int s = check_sv(sv);
   if (s) return s;
   VES3D_ARG(ms && bytes, "null argument");
+  if (age) *age = sv->pc_valid ? sv->pc_age : -1;
   for (int k = 0; k < 3; k++) ms[k] = sv->pc_ms[k];
   *bytes = sv->precond == VES3D_PRECOND_SELF_BLOCK ? (size_t)sv->pc_cap * sizeof(float) : 0;
   return VES3D_OK;

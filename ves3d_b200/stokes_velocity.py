@@ -165,12 +165,17 @@ class StokesVelocity:
         code = self.PRECONDS[scheme] if isinstance(scheme, str) else int(scheme)
         check(lib().ves3d_sv_set_precond(self._h, code), "set_precond")
 
+    def set_precond_refresh(self, every):
+        """Rebuild the preconditioner only every `every` surface updates (lagged
+        preconditioner; the solve still meets its tolerance on the true residual)."""
+        check(lib().ves3d_sv_set_precond_refresh(self._h, int(every)), "set_precond_refresh")
+
     def precond_info(self):
         """Device time of the last preconditioner build (total, operator assembly, LU) and
         the bytes the preconditioner holds."""
-        ms, nb = (ctypes.c_double * 3)(), ctypes.c_size_t(0)
-        check(lib().ves3d_sv_precond_info(self._h, ms, ctypes.byref(nb)), "precond_info")
-        return {"setup_ms": ms[0], "assembly_ms": ms[1], "factor_ms": ms[2], "bytes": nb.value}
+        ms, nb, age = (ctypes.c_double * 3)(), ctypes.c_size_t(0), ctypes.c_int(0)
+        check(lib().ves3d_sv_precond_info(self._h, ms, ctypes.byref(nb), ctypes.byref(age)), "precond_info")
+        return {"setup_ms": ms[0], "assembly_ms": ms[1], "factor_ms": ms[2], "bytes": nb.value, "age": age.value}
 
     def solver_stats(self):
         o, i = ctypes.c_int(0), ctypes.c_int(0)
