@@ -43,6 +43,7 @@ def parse():
     ap.add_argument("--no-implicit", action="store_true", help="skip the implicit-step measurement")
     ap.add_argument("--no-poly", action="store_true", help="skip the polydisperse measurement")
     ap.add_argument("--no-alt", action="store_true", help="skip the measurement of the other precision form")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default far-field launch shape")
     return ap.parse_args()
 
 
@@ -484,6 +485,8 @@ def run_ours(args, world, rank, local):
     N = nves * ng
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
+    # the far-field launch shape is tuned during the warm-up (project autotuner)
+    _lib.set_autotune(not args.no_autotune)
     sv = StokesVelocity(p, 2 * p, precision=args.precision, device=local)
     sv.set_stream(stream.cuda_stream)
     dX = torch.from_numpy(X).to(dev)
@@ -601,6 +604,7 @@ def run_ours(args, world, rank, local):
             "error_vs_fp64_oracle": {"max_rel": err, "sample": "2 vesicles: full velocity at 256 of their points"},
             "clocks": clocks,
             "peaks_tflops": {"fp64_fma": peak64, "fp32_fma": peak32},
+            "far_launch_shapes": _lib.autotune_report(),
         }
         # single-GPU characterisations (the other precision form, the implicit step, the
         # polydisperse suspension) run at N=1 only: with N>1 the line is the scaling point

@@ -89,6 +89,25 @@ int ves3d_sv_device_buffer(ves3d_sv* sv, int which, double** ptr, size_t* n_elem
 /* Evaluate using the resident density buffer (which=1) and write the resident
  * velocity buffer (which=2); no host transfer. */
 int ves3d_sv_eval_resident(ves3d_sv* sv);
+/* Record the resident evaluation (density buffer -> velocity buffer: self part + far
+ * field) as a CUDA graph on the context's stream (must not be the legacy default stream);
+ * builds the self matrices first if needed and runs one eager evaluation. The graph reads
+ * the buffers in place: write new densities into the density buffer and relaunch.
+ * Invalidated by ves3d_sv_set_src_coord and ves3d_sv_set_stream. */
+int ves3d_sv_capture_eval(ves3d_sv* sv);
+/* Launch the captured evaluation on the context's stream, asynchronously (synchronise the
+ * stream before reading the velocity buffer). */
+int ves3d_sv_launch_eval_graph(ves3d_sv* sv);
+
+/* Far-field launch-shape autotuner (no reference counterpart), process-wide, off by
+ * default (or VES3D_AUTOTUNE=1): on the first far-field launch of a configuration
+ * (precision, points, vesicles and their sizes) every candidate shape -- waves of CTAs
+ * per SM in {4, 8, 16} x targets per CTA in {512, 1024} -- is timed once with CUDA events
+ * and the fastest is kept. Never tunes during stream capture. */
+int ves3d_set_autotune(int on);
+/* Text report of the tuned configurations, one line each ("key waves=W chunk=C ms=T");
+ * *len receives its length (buf may be NULL). */
+int ves3d_autotune_report(char* buf, size_t cap, size_t* len);
 
 /* ---------------------------------------------------------------------------
  * Polydisperse suspensions: vesicles of different SH orders p in one evaluation (the
@@ -126,6 +145,12 @@ enum ves3d_surface_op {
   VES3D_OP_IMPLICIT_MATVEC = 7, /* [u;sigma] -> [u - S f ; -div S f], f = linbend(dt u) + tension(sigma) */
   VES3D_OP_IMPLICIT_RHS = 8     /* (in unused) -> [u_inf + S f_b ; div(u_inf + S f_b)]       */
 };
+/* Surface integrals per vesicle (Surface::area / volume / getCenters, src/Surface.cc:378-440,
+ * with GaussLegendreIntegrator weights, src/GLIntegrator.cc:33-80): area[n_ves],
+ * volume[n_ves], centers[n_ves][3]; any may be NULL. The normal convention is that of
+ * Surface::updateFirstForms (x_u x x_v / W), which points inward on this grid, so volumes
+ * come out negative for the reference's parametrisation (its tests compare magnitudes). */
+int ves3d_sv_integrals(ves3d_sv* sv, double* area, double* volume, double* centers, int is_device);
 /* Parameters of the implicit step: time step, bending modulus, shear rate of the
  * background flow u = (rate * y, 0, 0). */
 int ves3d_sv_set_implicit_params(ves3d_sv* sv, double dt, double kappa, double shear_rate);

@@ -8,6 +8,8 @@ Formulas follow (reference file:line):
   surface gradient / divergence                Surface::grad / div         src/Surface.cc:325-379
   linearised mean curvature                    Surface::linearizedMeanCurv src/Surface.cc:530-569
   bending, linear bending, tension forces      InterfacialForce            src/InterfacialForce.cc:21-125
+  area, volume, centres                        Surface::area/volume/getCenters src/Surface.cc:378-440
+  surface quadrature                           GaussLegendreIntegrator     src/GLIntegrator.cc:33-80
   implicit matvec (solve for velocity)         ImplicitMatvecPhysical      src/InterfacialVelocity.cc:922-979
   right-hand side                              AssembleRhsVel              src/InterfacialVelocity.cc:716-771
   BiCGStab (preconditioned)                    BiCGStab::operator()        src/BiCGStab.cc:45-138
@@ -63,6 +65,20 @@ def synth(S, p, kind):
         m = (jf + 1) // 2
         B[:, :, jf] = S[:, off[jf]:off[jf + 1]] @ L[m]
     return (B @ F).reshape(nf, -1)
+
+
+def integrals(X, p):
+    """Per vesicle: area = int W, volume = int (x.n)/3 W, centre = int (|x|^2/2) n W / volume,
+    with the Gauss-Legendre surface weights w_i (2 pi / 2p) / sin(theta_i)
+    (Surface::area / volume / getCenters, src/Surface.cc:378-440; GaussLegendreIntegrator,
+    src/GLIntegrator.cc:33-80)."""
+    geo = geometry(X, p)
+    q = geo["W"] * sh.smooth_weights_grid(p)[None, :]
+    Xv = geo["X"]
+    area = q.sum(1)
+    vol = ((Xv * geo["n"]).sum(1) / 3.0 * q).sum(1)
+    cen = ((0.5 * (Xv * Xv).sum(1))[:, None, :] * geo["n"] * q[:, None, :]).sum(2) / vol[:, None]
+    return area, vol, cen
 
 
 def geometry(X, p):

@@ -23,7 +23,31 @@ def ellipsoid_pair(p):
     return np.concatenate([X, X + np.array([3.0, 0.3, -0.2])[:, None]]).reshape(-1)
 
 
+def dumbbell(reference_root="/root/reference"):
+    """The reference's dumbbell test surface (entry 0 of precomputed/shape_gallery_6.txt,
+    AxisMajor [3][7][12] at p = 6) and SurfaceTest's known answers for it
+    (test/SurfaceTest.cc:72, :79, relative tolerance 5e-8)."""
+    vals = []
+    with open(os.path.join(reference_root, "precomputed", "shape_gallery_6.txt")) as fh:
+        started = False
+        for line in fh:
+            line = line.strip()
+            if line.startswith("#"):
+                if started:
+                    break
+                started = "dumbbell" in line
+                continue
+            if started and line:
+                vals.append(float(line))
+    p = 6
+    X = np.asarray(vals[: 3 * 2 * p * (p + 1)])
+    assert X.size == 3 * 2 * p * (p + 1), X.size
+    np.savez_compressed(os.path.join(HERE, "ref_dumbbell_p6.npz"), p=p, X=X, area=16.2179377312307,
+                        volume=5.24886489292959, rtol=5e-8)
+
+
 def main():
+    dumbbell()
     assert reflib.available(), "build oracle/_ref first (make -C oracle/ref)"
     reflib.set_threads(os.cpu_count() or 1)
     # p = 6: two ellipsoids; quadrature rules, transforms, the self matrix of vesicle 0

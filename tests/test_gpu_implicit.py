@@ -180,3 +180,19 @@ def test_lagged_preconditioner():
             assert np.linalg.norm(r) / np.linalg.norm(b) < 3e-9
             X = X + 5 * DT * x[:X.size]
         assert ages == [0, 1, 2, 0]
+
+
+def test_integrals_match_oracle_and_dumbbell():
+    import os
+    X, _ = small_suspension(2, P, 50, spacing=2.8)
+    with StokesVelocity(P) as sv:
+        sv.SetSrcCoord(X)
+        a, v, c = sv.integrals()
+    ao, vo, co = su.integrals(X, P)
+    assert rel_err(a, ao) < 1e-12 and rel_err(v, vo) < 1e-12 and rel_err(c, co) < 1e-12
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_dumbbell_p6.npz"))
+    with StokesVelocity(6) as sv:
+        sv.SetSrcCoord(np.ascontiguousarray(d["X"]))
+        a, v, c = sv.integrals()
+    assert abs(a[0] / float(d["area"]) - 1) < float(d["rtol"])
+    assert abs(abs(v[0]) / float(d["volume"]) - 1) < float(d["rtol"])

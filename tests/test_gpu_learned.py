@@ -151,14 +151,17 @@ def test_learned_guess_saves_iterations(tmp_path):
     sv = StokesVelocity(P)
     sv.SetSrcCoord(X)
     sv.set_implicit_params(DT, KAPPA, RATE)
+    # with the self-block preconditioner convergence is smooth enough that a closer start
+    # shows up as fewer iterations (unpreconditioned counts vary by +-15% with the start)
+    sv.set_precond("self_block")
     _, it0, _, c0 = sv.implicit_solve(tol=1e-10, max_iter=2000)
     x0, info = initial_guess(sv, learned=g2)
     _, it1, _, c1 = sv.implicit_solve(x0=x0, tol=1e-10, max_iter=2000)
     assert c0 == 100 and c1 == 100
     # judged by the true residual: the learned start is far closer than the zero start
-    # (relative residual 1), and the solve from it is not longer
+    # (relative residual 1), and the solve from it is shorter
     assert info["relres_combined"] < 0.1, info
-    assert it1 <= it0, (it0, it1, info)
+    assert it1 < it0, (it0, it1, info)
     # a broken network: the fallback (previous solution) keeps the solve where it was
     g2.net.set_params(np.random.default_rng(1).standard_normal(g2.net.num_params()).astype(np.float32) * 10)
     xs, _, _, _ = sv.implicit_solve(tol=1e-10, max_iter=2000)

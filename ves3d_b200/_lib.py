@@ -38,6 +38,10 @@ SIGNATURES = [
     ("ves3d_sv_stage_times", _i, [_vp, ctypes.POINTER(ctypes.c_float)]),
     ("ves3d_sv_device_buffer", _i, [_vp, _i, ctypes.POINTER(_vp), ctypes.POINTER(_sz)]),
     ("ves3d_sv_eval_resident", _i, [_vp]),
+    ("ves3d_sv_capture_eval", _i, [_vp]),
+    ("ves3d_set_autotune", _i, [_i]),
+    ("ves3d_autotune_report", _i, [ctypes.c_char_p, _sz, ctypes.POINTER(_sz)]),
+    ("ves3d_sv_launch_eval_graph", _i, [_vp]),
     ("ves3d_sht_forward", _i, [_vp, _l, _i, _i, _vp, _vp]),
     ("ves3d_sht_backward", _i, [_vp, _l, _i, _i, _vp, _vp, _vp, _vp]),
     ("ves3d_cuda_stokes_f64", _i, [_i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
@@ -58,6 +62,7 @@ SIGNATURES = [
     ("ves3d_svp_eval", _i, [_vp, _vp, _i]),
     ("ves3d_svp_stage_times", _i, [_vp, ctypes.POINTER(ctypes.c_float)]),
     ("ves3d_sv_solver_stats", _i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
+    ("ves3d_sv_integrals", _i, [_vp, _vp, _vp, _vp, _i]),
     ("ves3d_sv_set_precond", _i, [_vp, _i]),
     ("ves3d_sv_precond_info", _i, [_vp, _dp, ctypes.POINTER(_sz), ctypes.POINTER(_i)]),
     ("ves3d_sv_set_precond_refresh", _i, [_vp, _i]),
@@ -122,4 +127,22 @@ def tables_export(p0, p1, name):
     check(lib().ves3d_tables_export(p0, p1, name.encode(), None, 0, ctypes.byref(n)), "tables_export")
     out = np.empty(n.value)
     check(lib().ves3d_tables_export(p0, p1, name.encode(), out.ctypes.data, out.size, ctypes.byref(n)), "tables_export")
+    return out
+
+
+def set_autotune(on):
+    """Turn the far-field launch-shape autotuner on or off (process-wide)."""
+    check(lib().ves3d_set_autotune(1 if on else 0), "set_autotune")
+
+
+def autotune_report():
+    """{configuration key: {"waves", "chunk", "ms"}} of the tuned far-field launches."""
+    n = ctypes.c_size_t(0)
+    check(lib().ves3d_autotune_report(None, 0, ctypes.byref(n)), "autotune_report")
+    buf = ctypes.create_string_buffer(n.value + 1)
+    check(lib().ves3d_autotune_report(buf, n.value + 1, ctypes.byref(n)), "autotune_report")
+    out = {}
+    for line in buf.value.decode().splitlines():
+        key, *fields = line.split()
+        out[key] = {k: float(v) if k == "ms" else int(v) for k, v in (f.split("=") for f in fields)}
     return out

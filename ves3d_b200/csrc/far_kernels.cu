@@ -18,6 +18,12 @@
 // (Blackwell f32x2 FMA: both targets of a thread in one instruction), the unrefined
 // hardware reciprocal square root, and the FP32 partial of every source tile added into
 // FP64 accumulators. Distinct vesicles must not share points in the mixed form.
+#include <atomic>
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <string>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -251,13 +257,20 @@ __global__ void k_far_reduce(const double* __restrict__ part, int nseg, const lo
   }
 }
 
-int far_segments(long nves, long N, int tile, int nthr, int* seg_tiles) {
+// Launch shape of the far field: how many waves of CTAs the source range is split into
+// (segments), and how many targets of a vesicle one CTA takes (two per thread).
+struct FarShape {
+  int waves = 8;
+  int chunk_max = 1024;
+};
+
+int far_segments(long nves, long N, int tile, int nthr, int waves, int* seg_tiles) {
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   const long ntiles = (N + tile - 1) / tile;
   const int per_sm = max(1, 2048 / max(nthr, 32));  // resident CTAs per SM if threads limit
-  const long want = (long)nsm * per_sm * 8;         // about eight waves
+  const long want = (long)nsm * per_sm * waves;
   long nseg = (want + nves - 1) / nves;
   if (nseg < 1) nseg = 1;
   if (nseg > ntiles) nseg = ntiles;
@@ -265,29 +278,28 @@ int far_segments(long nves, long N, int tile, int nthr, int* seg_tiles) {
   return (int)((ntiles + *seg_tiles - 1) / *seg_tiles);
 }
 
-static void chunking(int nt, int* nchunk, int* nthr) {
-  // targets of a vesicle in chunks of at most 1024 (two per thread, <= 512 threads)
-  *nchunk = (nt + 1023) / 1024;
+static void chunking(int nt, int chunk_max, int* nchunk, int* nthr) {
+  // targets of a vesicle in chunks of at most chunk_max (two per thread)
+  *nchunk = (nt + chunk_max - 1) / chunk_max;
   const int per_chunk = (nt + *nchunk - 1) / *nchunk;
   *nthr = 32 * ((((per_chunk + 1) / 2) + 31) / 32);
 }
 
-int launch_far_groups(bool mixed, const double* pos, const double* den, const long* off, long nves, long N,
-                      const FarGroup* groups, int ngroups, const double* add, double* out, double* far_out,
-                      double* part, long part_cap_segments, cudaStream_t st) {
-  if (N <= 0) return VES3D_OK;
+static int launch_far_shape(const FarShape& sh, bool mixed, const double* pos, const double* den, const long* off,
+                            long nves, long N, const FarGroup* groups, int ngroups, const double* add, double* out,
+                            double* far_out, double* part, long part_cap_segments, cudaStream_t st) {
   const int tile = mixed ? kTileF32 : kTileF64;
   // one segment layout for all groups, sized by the average vesicle
-  int nthr_avg = 0, nchunk_tot = 0;
+  long nthr_sum = 0, nchunk_tot = 0;
   for (int g = 0; g < ngroups; g++) {
     int nc, nt;
-    chunking(groups[g].nt, &nc, &nt);
-    nthr_avg += nt * groups[g].nv;
-    nchunk_tot += nc * groups[g].nv;
+    chunking(groups[g].nt, sh.chunk_max, &nc, &nt);
+    nthr_sum += (long)nt * groups[g].nv;
+    nchunk_tot += (long)nc * groups[g].nv;
   }
-  nthr_avg = (int)(nthr_avg / nves);
+  const int nthr_avg = (int)(nthr_sum / nves);
   int seg_tiles = 1;
-  int nseg = far_segments(nchunk_tot, N, tile, nthr_avg, &seg_tiles);
+  int nseg = far_segments(nchunk_tot, N, tile, nthr_avg, sh.waves, &seg_tiles);
   if (nseg > part_cap_segments) {
     const long ntiles = (N + tile - 1) / tile;
     seg_tiles = (int)((ntiles + part_cap_segments - 1) / part_cap_segments);
@@ -296,7 +308,7 @@ int launch_far_groups(bool mixed, const double* pos, const double* den, const lo
   for (int g = 0; g < ngroups; g++) {
     if (groups[g].nv <= 0) continue;
     int nchunk, nthr;
-    chunking(groups[g].nt, &nchunk, &nthr);
+    chunking(groups[g].nt, sh.chunk_max, &nchunk, &nthr);
     dim3 grid(nseg, (unsigned)groups[g].nv, nchunk);
     if (mixed)
       k_far_f32_seg<<<grid, nthr, 0, st>>>(pos, den, off, N, seg_tiles, (int)groups[g].v0, part);
@@ -307,6 +319,108 @@ int launch_far_groups(bool mixed, const double* pos, const double* den, const lo
   k_far_reduce<<<(unsigned)nves, 256, 0, st>>>(part, nseg, off, N, add, out, far_out);
   VES3D_LAUNCHED();
   return VES3D_OK;
+}
+
+// ---- autotuner of the launch shape ----------------------------------------------------
+// On the first launch of a configuration (precision, N, vesicles, group structure) with
+// autotuning on, every candidate shape is launched once and timed with CUDA events on the
+// caller's stream; the fastest is cached for the process. Off by default and never during
+// stream capture. Candidates differ only in how the source range is split, i.e. in the
+// grouping of the FP64 partial sums (results agree to rounding); a tuned configuration
+// always uses its one shape afterwards, so repeated evaluations stay bitwise identical.
+struct FarTuneEntry {
+  FarShape shape;
+  float ms = 0;
+};
+
+static std::mutex g_tune_mu;
+static std::map<std::string, FarTuneEntry> g_tuned;
+static std::atomic<int> g_autotune{-1};
+
+static bool autotune_on() {
+  int v = g_autotune.load();
+  if (v < 0) {
+    const char* e = getenv("VES3D_AUTOTUNE");
+    v = (e && e[0] == '1') ? 1 : 0;
+    g_autotune.store(v);
+  }
+  return v == 1;
+}
+
+static std::string tune_key(bool mixed, long nves, long N, const FarGroup* groups, int ngroups) {
+  std::string k = mixed ? "f32" : "f64";
+  k += ":N=" + std::to_string(N) + ":v=" + std::to_string(nves);
+  for (int g = 0; g < ngroups; g++) k += ":" + std::to_string(groups[g].nv) + "x" + std::to_string(groups[g].nt);
+  return k;
+}
+
+int launch_far_groups(bool mixed, const double* pos, const double* den, const long* off, long nves, long N,
+                      const FarGroup* groups, int ngroups, const double* add, double* out, double* far_out,
+                      double* part, long part_cap_segments, cudaStream_t st) {
+  if (N <= 0) return VES3D_OK;
+  FarShape shape;
+  if (autotune_on()) {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    VES3D_CK(cudaStreamIsCapturing(st, &cap));
+    const std::string key = tune_key(mixed, nves, N, groups, ngroups);
+    bool have = false;
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      auto it = g_tuned.find(key);
+      if (it != g_tuned.end()) {
+        shape = it->second.shape;
+        have = true;
+      }
+    }
+    if (!have && cap == cudaStreamCaptureStatusNone) {
+      const FarShape cands[] = {{4, 1024}, {8, 1024}, {16, 1024}, {4, 512}, {8, 512}, {16, 512}};
+      cudaEvent_t e0, e1;
+      VES3D_CK(cudaEventCreate(&e0));
+      VES3D_CK(cudaEventCreate(&e1));
+      FarTuneEntry best;
+      best.ms = 1e30f;
+      int s = VES3D_OK;
+      for (const FarShape& c : cands) {
+        cudaEventRecord(e0, st);
+        s = launch_far_shape(c, mixed, pos, den, off, nves, N, groups, ngroups, add, out, far_out, part,
+                             part_cap_segments, st);
+        if (s) break;
+        cudaEventRecord(e1, st);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best.ms) {
+          best.ms = ms;
+          best.shape = c;
+        }
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      if (s) return s;
+      {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tuned[key] = best;
+      }
+      shape = best.shape;
+    }
+  }
+  return launch_far_shape(shape, mixed, pos, den, off, nves, N, groups, ngroups, add, out, far_out, part,
+                          part_cap_segments, st);
+}
+
+int set_autotune(int on) {
+  g_autotune.store(on ? 1 : 0);
+  return VES3D_OK;
+}
+
+// "key waves chunk ms" per tuned configuration, one per line
+std::string autotune_report() {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  std::string r;
+  for (const auto& kv : g_tuned)
+    r += kv.first + " waves=" + std::to_string(kv.second.shape.waves) + " chunk=" +
+         std::to_string(kv.second.shape.chunk_max) + " ms=" + std::to_string(kv.second.ms) + "\n";
+  return r;
 }
 
 int launch_far(bool mixed, const double* pos, const double* den, const long* off, long nves, long N, int max_nt,

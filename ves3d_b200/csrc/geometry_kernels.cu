@@ -150,6 +150,60 @@ __global__ void k_shear(const double* __restrict__ X, long N, int ng, double rat
 
 #undef FOR_POINTS
 
+// Per vesicle (one CTA each): area = sum W q, volume = sum (x.n)/3 W q, centre =
+// sum (|x|^2/2) n W q / volume, with W n = x_u x x_v and the Gauss-Legendre surface
+// weights q (Surface::area / volume / getCenters, src/Surface.cc:378-440;
+// GaussLegendreIntegrator, src/GLIntegrator.cc:33-80). out[v] = {area, volume, cx, cy, cz}.
+// Fixed-order block reduction: the result is bitwise reproducible.
+__global__ void __launch_bounds__(256) k_integrals(const double* __restrict__ X, const double* __restrict__ Xu,
+                                                   const double* __restrict__ Xv, const double* __restrict__ w,
+                                                   int p, double* __restrict__ out) {
+  __shared__ double red[5][8];
+  const int ng = 2 * p * (p + 1);
+  const long v = blockIdx.x;
+  const long b = v * 3 * ng;
+  double acc[5] = {0, 0, 0, 0, 0};
+  for (int k = threadIdx.x; k < ng; k += blockDim.x) {
+    double x[3], a[3], c[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      x[d] = X[b + d * ng + k];
+      a[d] = Xu[b + d * ng + k];
+      c[d] = Xv[b + d * ng + k];
+    }
+    const double nx = a[1] * c[2] - a[2] * c[1], ny = a[2] * c[0] - a[0] * c[2], nz = a[0] * c[1] - a[1] * c[0];
+    const double q = w[k / (2 * p)];
+    const double W = sqrt(nx * nx + ny * ny + nz * nz);
+    const double h = 0.5 * (x[0] * x[0] + x[1] * x[1] + x[2] * x[2]) * q;
+    acc[0] += W * q;
+    acc[1] += (x[0] * nx + x[1] * ny + x[2] * nz) * (q / 3.0);
+    acc[2] += h * nx;
+    acc[3] += h * ny;
+    acc[4] += h * nz;
+  }
+#pragma unroll
+  for (int i = 0; i < 5; i++) {
+    double t = acc[i];
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    if ((threadIdx.x & 31) == 0) red[i][threadIdx.x >> 5] = t;
+  }
+  __syncthreads();
+  if (threadIdx.x < 5) {
+    double t = 0;
+    for (int w8 = 0; w8 < (int)(blockDim.x >> 5); w8++) t += red[threadIdx.x][w8];
+    red[threadIdx.x][0] = t;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const double vol = red[1][0];
+    out[v * 5] = red[0][0];
+    out[v * 5 + 1] = vol;
+    out[v * 5 + 2] = red[2][0] / vol;
+    out[v * 5 + 3] = red[3][0] / vol;
+    out[v * 5 + 4] = red[4][0] / vol;
+  }
+}
+
 static inline unsigned nblk(long n) { return (unsigned)((n + 255) / 256); }
 
 int launch_geometry(const double* xu, const double* xv, const double* xuu, const double* xuv, const double* xvv,
@@ -202,6 +256,14 @@ int launch_tension_combine(const double* sigma, const double* gsig, const double
   const long N = nv * ng;
   if (N <= 0) return VES3D_OK;
   k_tension_combine<<<nblk(N), 256, 0, st>>>(sigma, gsig, geo, N, ng, add, out);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
+int launch_integrals(const double* X, const double* Xu, const double* Xv, const double* w, long nv, int p,
+                     double* out, cudaStream_t st) {
+  if (nv <= 0) return VES3D_OK;
+  k_integrals<<<(unsigned)nv, 256, 0, st>>>(X, Xu, Xv, w, p, out);
   VES3D_LAUNCHED();
   return VES3D_OK;
 }

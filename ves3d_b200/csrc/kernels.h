@@ -1,5 +1,7 @@
 // Kernel launchers of the ves3d_b200 CUDA library (device pointers, one stream).
 #pragma once
+
+#include <string>
 #include <cuda_runtime.h>
 
 namespace ves3d {
@@ -76,6 +78,9 @@ struct FarGroup {
   long v0, nv;
   int nt;
 };
+// far-field launch-shape autotuner (far_kernels.cu)
+int set_autotune(int on);
+std::string autotune_report();
 int launch_far_groups(bool mixed, const double* pos, const double* den, const long* off, long nves, long N,
                       const FarGroup* groups, int ngroups, const double* add, double* out, double* far_out,
                       double* part, long part_cap_segments, cudaStream_t st);
@@ -101,6 +106,9 @@ int launch_bend_combine(const double* h, const double* lap, const double* geo, l
 int launch_tension_combine(const double* sigma, const double* gsig, const double* geo, long nv, int ng,
                            const double* add, double* out, cudaStream_t st);
 int launch_shear(const double* X, long nv, int ng, double rate, double* out, cudaStream_t st);
+// per vesicle {area, volume, centre x, y, z} (Xu latitude, Xv longitude derivatives)
+int launch_integrals(const double* X, const double* Xu, const double* Xv, const double* w, long nv, int p,
+                     double* out, cudaStream_t st);
 
 // BiCGStab (bicgstab.cu)
 int dot_f64(const double* x, const double* y, long n, double* scratch, double* result, cudaStream_t st);

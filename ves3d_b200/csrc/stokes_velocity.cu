@@ -165,12 +165,22 @@ struct ves3d_sv {
   long pc_nves = 0;            // vesicle count the preconditioner was built for
   double pc_ms[3] = {0, 0, 0};  // last build: total, assembly, factorisation (device ms)
   cudaStream_t pc_stream[kPcStreams] = {};
+  // CUDA graph of the resident evaluation (density buffer -> velocity buffer)
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  void drop_graph() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph) cudaGraphDestroy(graph);
+    graph_exec = nullptr;
+    graph = nullptr;
+  }
   cusolverDnHandle_t pc_solver[kPcStreams] = {};
   cudaEvent_t pc_ev[3 + kPcStreams] = {};
   cudaEvent_t ev[8] = {};
   float ms[4] = {0, 0, 0, 0};
 
   ~ves3d_sv() {
+    drop_graph();
     free_precond();
     for (auto& h : pc_solver)
       if (h) cusolverDnDestroy(h);
@@ -387,6 +397,15 @@ int run_self(ves3d_sv* sv, double* vself, double* den) {
   return launch_far_density(sv->F, sv->area, sv->nves, p0, T.smooth_w0, den, st);
 }
 
+// The evaluation proper, stream-ordered and free of host synchronisation (it is what the
+// CUDA graph of ves3d_sv_capture_eval records): self part, then the far field added to it.
+int run_eval_body(ves3d_sv* sv) {
+  int s;
+  if ((s = run_self(sv, sv->Vself, sv->den))) return s;
+  return launch_far(sv->prec == VES3D_PREC_MIXED && !sv->far_force_fp64, sv->pos, sv->den, sv->off, sv->nves,
+                    sv->npts(), ngrid_(sv->p), sv->Vself, sv->V, sv->Vfar, sv->part, kFarMaxSegments, sv->stream);
+}
+
 int run_eval(ves3d_sv* sv) {
   const int p0 = sv->p;
   cudaStream_t st = sv->stream;
@@ -474,6 +493,7 @@ int ves3d_sv_set_stream(ves3d_sv* sv, void* stream) {
   int s = check_sv(sv);
   if (s) return s;
   sv->stream = stream ? (cudaStream_t)stream : sv->own_stream;
+  sv->drop_graph();
   return VES3D_OK;
 }
 
@@ -507,6 +527,7 @@ int ves3d_sv_set_src_coord(ves3d_sv* sv, const double* S, long n_ves, int is_dev
   sv->sl_valid = false;
   sv->parts_valid = false;
   sv->geo_valid = false;
+  sv->drop_graph();
   // a lagged preconditioner survives pc_refresh - 1 surface updates (right
   // preconditioning: it steers the iteration only, the tolerance is on the true residual)
   if (sv->pc_valid && sv->pc_nves == n_ves && sv->pc_age + 1 < sv->pc_refresh)
@@ -552,6 +573,67 @@ int ves3d_sv_eval_resident(ves3d_sv* sv) {
   int s = check_sv(sv);
   if (s) return s;
   return run_eval(sv);
+}
+
+int ves3d_set_autotune(int on) { return set_autotune(on); }
+
+int ves3d_autotune_report(char* buf, size_t cap, size_t* len) {
+  VES3D_ARG(len != nullptr, "len is null");
+  const std::string r = autotune_report();
+  *len = r.size();
+  if (buf && cap) {
+    const size_t n = std::min(cap - 1, r.size());
+    memcpy(buf, r.data(), n);
+    buf[n] = 0;
+  }
+  return VES3D_OK;
+}
+
+int ves3d_sv_capture_eval(ves3d_sv* sv) {
+  int s = check_sv(sv);
+  if (s) return s;
+  if (!sv->have_src) {
+    set_error("no surfaces set");
+    return VES3D_ERR_STATE;
+  }
+  if (sv->stream == nullptr) {
+    set_error("graph capture needs a non-default stream");
+    return VES3D_ERR_STATE;
+  }
+  sv->drop_graph();
+  if (!sv->sl_valid && (s = run_setup(sv))) return s;
+  // one eager pass first: every launcher sets its kernel attributes outside the capture
+  sv->have_den = true;
+  if ((s = run_eval(sv))) return s;
+  VES3D_CK(cudaStreamBeginCapture(sv->stream, cudaStreamCaptureModeThreadLocal));
+  s = run_eval_body(sv);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(sv->stream, &g);
+  if (!s && e != cudaSuccess) s = cuda_status(e, "cudaStreamEndCapture", __FILE__, __LINE__);
+  if (s) {
+    if (g) cudaGraphDestroy(g);
+    return s;
+  }
+  sv->graph = g;
+  const cudaError_t ei = cudaGraphInstantiate(&sv->graph_exec, g, 0);
+  if (ei != cudaSuccess) {
+    sv->drop_graph();
+    return cuda_status(ei, "cudaGraphInstantiate", __FILE__, __LINE__);
+  }
+  return VES3D_OK;
+}
+
+int ves3d_sv_launch_eval_graph(ves3d_sv* sv) {
+  int s = check_sv(sv);
+  if (s) return s;
+  if (!sv->graph_exec) {
+    set_error("no captured evaluation (call ves3d_sv_capture_eval after setting the surfaces)");
+    return VES3D_ERR_STATE;
+  }
+  VES3D_CK(cudaGraphLaunch(sv->graph_exec, sv->stream));
+  VES3D_LAUNCHED();
+  sv->parts_valid = true;
+  return VES3D_OK;
 }
 
 int ves3d_sv_get_self_matrix(ves3d_sv* sv, double* SL, int is_device) {
@@ -1341,6 +1423,37 @@ int ves3d_sv_solver_stats(ves3d_sv* sv, int* outer, int* inner) {
   VES3D_ARG(sv && outer && inner, "null argument");
   *outer = sv->ir_outer;
   *inner = sv->ir_inner;
+  return VES3D_OK;
+}
+
+int ves3d_sv_integrals(ves3d_sv* sv, double* area, double* volume, double* centers, int is_device) {
+  int s = check_sv(sv);
+  if (s) return s;
+  if (!sv->have_src) {
+    set_error("no surfaces set");
+    return VES3D_ERR_STATE;
+  }
+  const long nv = sv->nves;
+  double* d = nullptr;
+  if ((s = dalloc(&d, 5 * nv))) return s;
+  s = launch_integrals(sv->X, sv->Xp, sv->Xt, sv->tab->d.smooth_w0, nv, sv->p, d, sv->stream);
+  std::vector<double> h(5 * nv);
+  if (!s)
+    s = cuda_status(cudaMemcpyAsync(h.data(), d, 5 * nv * sizeof(double), cudaMemcpyDeviceToHost, sv->stream),
+                    "copy", __FILE__, __LINE__);
+  if (!s) s = cuda_status(cudaStreamSynchronize(sv->stream), "sync", __FILE__, __LINE__);
+  dfree(d);
+  if (s) return s;
+  std::vector<double> a(nv), vo(nv), c(3 * nv);
+  for (long v = 0; v < nv; v++) {
+    a[v] = h[5 * v];
+    vo[v] = h[5 * v + 1];
+    for (int k = 0; k < 3; k++) c[3 * v + k] = h[5 * v + 2 + k];
+  }
+  const cudaMemcpyKind kind = is_device ? cudaMemcpyHostToDevice : cudaMemcpyHostToHost;
+  if (area) VES3D_CK(cudaMemcpy(area, a.data(), nv * sizeof(double), kind));
+  if (volume) VES3D_CK(cudaMemcpy(volume, vo.data(), nv * sizeof(double), kind));
+  if (centers) VES3D_CK(cudaMemcpy(centers, c.data(), 3 * nv * sizeof(double), kind));
   return VES3D_OK;
 }
 

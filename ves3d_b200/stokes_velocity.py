@@ -132,6 +132,15 @@ class StokesVelocity:
     def eval_resident(self):
         check(lib().ves3d_sv_eval_resident(self._h), "eval_resident")
 
+    def capture_eval(self):
+        """Record the resident evaluation (device density buffer -> device velocity
+        buffer) as a CUDA graph; relaunch it with launch_eval_graph()."""
+        check(lib().ves3d_sv_capture_eval(self._h), "capture_eval")
+
+    def launch_eval_graph(self):
+        """Launch the captured evaluation asynchronously on the context's stream."""
+        check(lib().ves3d_sv_launch_eval_graph(self._h), "launch_eval_graph")
+
     def set_stream(self, stream_ptr):
         check(lib().ves3d_sv_set_stream(self._h, stream_ptr), "set_stream")
 
@@ -176,6 +185,12 @@ class StokesVelocity:
         ms, nb, age = (ctypes.c_double * 3)(), ctypes.c_size_t(0), ctypes.c_int(0)
         check(lib().ves3d_sv_precond_info(self._h, ms, ctypes.byref(nb), ctypes.byref(age)), "precond_info")
         return {"setup_ms": ms[0], "assembly_ms": ms[1], "factor_ms": ms[2], "bytes": nb.value, "age": age.value}
+
+    def integrals(self):
+        """Per vesicle (area, volume, centre [n_ves][3]) of the current surfaces."""
+        a, v, c = np.empty(self.n_ves), np.empty(self.n_ves), np.empty((self.n_ves, 3))
+        check(lib().ves3d_sv_integrals(self._h, a.ctypes.data, v.ctypes.data, c.ctypes.data, 0), "integrals")
+        return a, v, c
 
     def solver_stats(self):
         o, i = ctypes.c_int(0), ctypes.c_int(0)
