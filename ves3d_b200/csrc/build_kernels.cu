@@ -32,6 +32,14 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
 // Row stride >= n with stride = 4 (mod 16) doubles.
 __host__ __device__ constexpr int pad16_4(int n) { return ((n + 11) / 16) * 16 + 4; }
 
+// Number of 8-wide n-tiles over the Fourier blocks of the order-p0 coefficient vector
+// (block lengths p0+1, then p0+1-m twice for m = 1..p0-1, then 1).
+__host__ __device__ constexpr int legt_ntiles(int p0) {
+  int t = (p0 + 1 + 7) / 8 + 1;
+  for (int m = 1; m < p0; m++) t += 2 * ((p0 + 1 - m + 7) / 8);
+  return t;
+}
+
 template <int P0>
 struct RingCfg {
   static constexpr int P1 = 2 * P0;
@@ -39,14 +47,21 @@ struct RingCfg {
   static constexpr int L1 = P1 + 1;           // latitudes of the upsampled grid
   static constexpr int F0 = 2 * P0;           // Fourier coefficients at order p0
   static constexpr int N1 = 2 * P1;           // longitudes of the upsampled grid
-  static constexpr int LG = 4;                // latitudes per group
+  static constexpr int LG = 4;                // latitudes per group (= K of one m8n8k4 step)
   static constexpr int NGRP = (L1 + LG - 1) / LG;
   static constexpr int ROWS1 = ((3 * LG + 7) / 8) * 8;   // (lat, d) rows of a group, m-tile padded
   static constexpr int LDA = pad16_4(F0);
   static constexpr int LDM = pad16_4(N1);
   static constexpr int LDX = pad16_4(N1);
   static constexpr int LDK = pad16_4(N1);
-  static constexpr int LDC = pad16_4(F0);
+  // C rows (lat, component) read down a column by the transposed-Legendre MMAs: an odd
+  // stride of F0 + 5 makes those fragment reads conflict-free
+  static constexpr int LDC = F0 + 5;
+  // coefficient rows (R, Legendre slices) padded to 4 mod 16 for the MMA fragments, with
+  // room for the K padding of the last Fourier block
+  static constexpr int LDR = pad16_4(NC + 3);
+  static constexpr int NTT = legt_ntiles(P0);             // n-tiles of the transposed Legendre
+  static constexpr int QMAX = (2 * NTT + 7) / 8;          // its accumulator tiles per warp
   // Shared memory, with buffers of disjoint lifetimes aliased:
   //   region Q: A/dA (Legendre synthesis -> G1)  then  K (kernel -> G2)
   //   region P: X/X_theta/X_phi (G1 -> kernel)   then  C (G2 -> Legendre sums)
@@ -55,21 +70,20 @@ struct RingCfg {
   static constexpr int SZ_X = 3 * ROWS1 * LDX;
   static constexpr int SZ_C = (LG * 12) * LDC;
   static constexpr int OFF_R = 0;
-  static constexpr int OFF_MF = OFF_R + 3 * NC;
+  static constexpr int OFF_MF = OFF_R + 3 * LDR;
   static constexpr int OFF_DMF = OFF_MF + F0 * LDM;
-  static constexpr int OFF_LEG = OFF_DMF + F0 * LDM;       // [LG][NC] slice of the latitude group
-  static constexpr int OFF_DLEG = OFF_LEG + NC * LG;
-  static constexpr int OFF_Q = OFF_DLEG + NC * LG;
+  static constexpr int OFF_LEG = OFF_DMF + F0 * LDM;       // [LG][LDR] slice of the latitude group
+  static constexpr int OFF_DLEG = OFF_LEG + LG * LDR;
+  static constexpr int OFF_Q = OFF_DLEG + LG * LDR;
   static constexpr int OFF_P = OFF_Q + (SZ_A > SZ_K ? SZ_A : SZ_K);
   static constexpr int OFF_TRG = OFF_P + (SZ_X > SZ_C ? SZ_X : SZ_C);
   // small index/weight tables read in every latitude group, kept on chip
   static constexpr int OFF_SW = OFF_TRG + 8;                    // sing_w [L1]
   static constexpr int OFF_BO = OFF_SW + L1;                    // blk_off [F0 + 1] (int)
-  static constexpr int OFF_JF = OFF_BO + (F0 + 2) / 2;          // jf_of_coef [NC] (unsigned char)
-  static constexpr int TOTAL = OFF_JF + (NC + 7) / 8;
+  static constexpr int OFF_TL = OFF_BO + (F0 + 2) / 2;          // n-tile list: (block, tile) [NTT] (uchar2)
+  static constexpr int TOTAL = OFF_TL + (NTT + 3) / 4;
   static constexpr size_t SMEM = (size_t)TOTAL * sizeof(double);
   static constexpr int NOUT = 12 * NC;
-  static constexpr int OUT_PER_THREAD = (NOUT + 255) / 256;
 };
 
 template <int P0>
@@ -90,15 +104,26 @@ __global__ void __launch_bounds__(256, 2) k_build_ring(const double* __restrict_
   double* trg = sm + G::OFF_TRG;
   double* sSw = sm + G::OFF_SW;
   int* sBo = reinterpret_cast<int*>(sm + G::OFF_BO);
-  unsigned char* sJf = reinterpret_cast<unsigned char*>(sm + G::OFF_JF);
+  uchar2* sTl = reinterpret_cast<uchar2*>(sm + G::OFF_TL);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const long rot = blockIdx.x;
   for (int i = tid; i < G::L1; i += 256) sSw[i] = __ldg(T.sing_w + i);
   for (int i = tid; i <= G::F0; i += 256) sBo[i] = __ldg(T.blk_off + i);
-  for (int i = tid; i < G::NC; i += 256) sJf[i] = (unsigned char)__ldg(T.jf_of_coef + i);
+  if (tid == 0) {
+    // n-tiles of the transposed Legendre: (Fourier block, 8-wide tile within it)
+    int j = 0;
+    for (int k = 0; k < G::F0; k++) {
+      const int len = __ldg(T.blk_off + k + 1) - __ldg(T.blk_off + k);
+      for (int nt = 0; nt * 8 < len && j < G::NTT; nt++) sTl[j++] = make_uchar2((unsigned char)k, (unsigned char)nt);
+    }
+  }
 
   // ---- rotated coefficients, DFT tables, pole targets ----------------------------------
-  for (int i = tid; i < 3 * G::NC; i += 256) sR[i] = R[rot * 3 * G::NC + i];
+  // rotated coefficients, rows padded to LDR (zeros beyond NC: K padding of the last block)
+  for (int i = tid; i < 3 * G::LDR; i += 256) {
+    const int d = i / G::LDR, c = i - d * G::LDR;
+    sR[i] = c < G::NC ? R[rot * 3 * G::NC + d * G::NC + c] : 0.0;
+  }
   for (int i = tid; i < G::F0 * G::N1; i += 256) {
     const int k = i / G::N1, j = i - k * G::N1;
     sMf[k * G::LDM + j] = __ldg(T.syn1_four + i);
@@ -108,40 +133,54 @@ __global__ void __launch_bounds__(256, 2) k_build_ring(const double* __restrict_
   if (tid < 6) {
     const int c = tid >> 1, t = tid & 1;
     double s = 0.0;
-    for (int n = 0; n <= P0; n++) s += sR[c * G::NC + n] * __ldg(T.qp + t * (P0 + 1) + n);
+    for (int n = 0; n <= P0; n++) s += sR[c * G::LDR + n] * __ldg(T.qp + t * (P0 + 1) + n);
     trg[c * 2 + t] = s;
   }
-  double acc[G::OUT_PER_THREAD];
+  // transposed-Legendre accumulators: tile warp + 8 q = (m-tile of components, n-tile)
+  double acc[G::QMAX][2];
 #pragma unroll
-  for (int q = 0; q < G::OUT_PER_THREAD; q++) acc[q] = 0.0;
+  for (int q = 0; q < G::QMAX; q++) acc[q][0] = acc[q][1] = 0.0;
 
   const int grow = lane >> 2, gcol = lane & 3;
   for (int g = 0; g < G::NGRP; g++) {
     const int lat0 = g * G::LG;
     const int nlat = min(G::LG, G::L1 - lat0);
     // ---- the group's slice of the Legendre tables -------------------------------------
-    for (int i = tid; i < G::NC * G::LG; i += 256) {
-      const int l = i / G::NC, c = i - l * G::NC;
-      const bool ok = l < nlat;
+    for (int i = tid; i < G::LDR * G::LG; i += 256) {
+      const int l = i / G::LDR, c = i - l * G::LDR;
+      const bool ok = l < nlat && c < G::NC;
       sLeg[i] = ok ? __ldg(T.syn1_leg_t + (lat0 + l) * G::NC + c) : 0.0;
       sdLeg[i] = ok ? __ldg(T.syn1_dleg_t + (lat0 + l) * G::NC + c) : 0.0;
     }
     __syncthreads();
-    // ---- Legendre synthesis of the group's latitudes: A[(l,d)][k], dA -----------------
-    for (int i = tid; i < G::ROWS1 * G::F0; i += 256) {
-      const int k = i % G::F0, row = i / G::F0;
-      double s = 0.0, d = 0.0;
-      if (row < 3 * nlat) {
-        const int l = row / 3, dd = row - 3 * l;
-        const int c0 = sBo[k], c1 = sBo[k + 1];
-        const double* r = sR + dd * G::NC;
-        for (int c = c0; c < c1; c++) {
-          s = fma(r[c], sLeg[l * G::NC + c], s);
-          d = fma(r[c], sdLeg[l * G::NC + c], d);
-        }
+    // ---- Legendre synthesis of the group's latitudes on tensor cores ------------------
+    // per Fourier block k: A[(l, d)][k] = sum_{c in block k} Leg[l][c] R[d][c] (and dA with
+    // the derivative table) is one m8n8k4 GEMM [lat x c] . [c x d], K = the block length;
+    // K padding reads the next block's (finite) Legendre values against zeros in B
+    for (int i = tid; i < (G::ROWS1 - 3 * nlat) * G::F0; i += 256) {
+      const int row = 3 * nlat + i / G::F0, k = i % G::F0;
+      sA[row * G::LDA + k] = 0.0;
+      sdA[row * G::LDA + k] = 0.0;
+    }
+    for (int it = warp; it < 2 * G::F0; it += 8) {
+      const int k = it >> 1, which = it & 1;
+      const int c0 = sBo[k], c1 = sBo[k + 1];
+      const double* L = (which ? sdLeg : sLeg) + grow * G::LDR + c0 + gcol;
+      const double* Rr = sR + grow * G::LDR + c0 + gcol;
+      double e0 = 0.0, e1 = 0.0;
+      for (int ks = 0; 4 * ks < c1 - c0; ks++) {
+        const int c = c0 + 4 * ks + gcol;
+        const double a = grow < nlat ? L[4 * ks] : 0.0;
+        const double b = (grow < 3 && c < c1) ? Rr[4 * ks] : 0.0;
+        dmma(e0, e1, a, b);
       }
-      sA[row * G::LDA + k] = s;
-      sdA[row * G::LDA + k] = d;
+      // C[l = grow][d = 2 gcol + {0, 1}]
+      double* out = which ? sdA : sA;
+      const int d0 = 2 * gcol;
+      if (grow < nlat) {
+        if (d0 < 3) out[(grow * 3 + d0) * G::LDA + k] = e0;
+        if (d0 + 1 < 3) out[(grow * 3 + d0 + 1) * G::LDA + k] = e1;
+      }
     }
     __syncthreads();
     // ---- DFT synthesis on tensor cores: X, X_theta (from A), X_phi (from dA) ------------
@@ -220,24 +259,37 @@ __global__ void __launch_bounds__(256, 2) k_build_ring(const double* __restrict_
       }
     }
     __syncthreads();
-    // ---- transposed Legendre sums, accumulated in registers -----------------------------
+    // ---- transposed Legendre sums on tensor cores, accumulated over the groups ---------
+    // Cout[comp][c] += sum_{l < LG} C[(l, comp)][k(c)] Leg[l][c]: per (m-tile of the 12
+    // components, n-tile of a Fourier block) one m8n8k4 step with K = the LG latitudes
 #pragma unroll
-    for (int q = 0; q < G::OUT_PER_THREAD; q++) {
-      const int o = tid + q * 256;
-      if (o < G::NOUT) {
-        const int comp = o / G::NC, c = o - comp * G::NC;
-        const int jf = sJf[c];
-        double s = acc[q];
-        for (int l = 0; l < nlat; l++) s = fma(sC[(l * 12 + comp) * G::LDC + jf], sLeg[l * G::NC + c], s);
-        acc[q] = s;
+    for (int q = 0; q < G::QMAX; q++) {
+      const int tile = warp + 8 * q;
+      if (tile < 2 * G::NTT) {
+        const int mt = tile / G::NTT;
+        const uchar2 kt = sTl[tile - mt * G::NTT];
+        const int k = kt.x, c0 = sBo[k], c1 = sBo[k + 1];
+        const int comp = mt * 8 + grow, l = gcol, c = c0 + kt.y * 8 + grow;
+        const double a = (comp < 12 && l < nlat) ? sC[(l * 12 + comp) * G::LDC + k] : 0.0;
+        const double b = (l < nlat && c < c1) ? sLeg[l * G::LDR + c] : 0.0;
+        dmma(acc[q][0], acc[q][1], a, b);
       }
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int q = 0; q < G::OUT_PER_THREAD; q++) {
-    const int o = tid + q * 256;
-    if (o < G::NOUT) C[rot * G::NOUT + o] = acc[q];
+  for (int q = 0; q < G::QMAX; q++) {
+    const int tile = warp + 8 * q;
+    if (tile < 2 * G::NTT) {
+      const int mt = tile / G::NTT;
+      const uchar2 kt = sTl[tile - mt * G::NTT];
+      const int c0 = sBo[kt.x], c1 = sBo[kt.x + 1];
+      const int comp = mt * 8 + grow, c = c0 + kt.y * 8 + 2 * gcol;
+      if (comp < 12) {
+        if (c < c1) C[rot * G::NOUT + comp * G::NC + c] = acc[q][0];
+        if (c + 1 < c1) C[rot * G::NOUT + comp * G::NC + c + 1] = acc[q][1];
+      }
+    }
   }
 }
 
