@@ -262,3 +262,24 @@ def test_far_field_autotuner():
         assert e["waves"] in (4, 8, 16) and e["chunk"] in (512, 1024) and e["ms"] > 0
     assert rel_err(v1, v_default) < 1e-13
     assert np.array_equal(v1, v2)
+
+
+@pytest.mark.parametrize("shape", [(4, 512, 4), (16, 1024, 4), (8, 512, 2)])
+def test_far_field_launch_shapes_agree(shape):
+    """Every launch shape the autotuner may pick (segments, targets per CTA, targets per
+    thread) computes the same far field as the default one to rounding, and matches the
+    oracle to 1e-12."""
+    p = 8
+    X, f = small_suspension(2, p, 73, spacing=2.7)
+    with StokesVelocity(p) as sv:
+        sv.SetSrcCoord(X)
+        sv.SetDensitySL(f)
+        v0 = sv()
+        _lib.set_far_shape(*shape)
+        try:
+            sv.SetDensitySL(f)
+            v1 = sv()
+        finally:
+            _lib.set_far_shape(0)
+    assert rel_err(v1, v0) < 1e-13
+    assert rel_err(v1, stokes.stokes_velocity_sl(X, f, p, 2 * p)) < 1e-12

@@ -40,6 +40,7 @@ SIGNATURES = [
     ("ves3d_sv_eval_resident", _i, [_vp]),
     ("ves3d_sv_capture_eval", _i, [_vp]),
     ("ves3d_set_autotune", _i, [_i]),
+    ("ves3d_set_far_shape", _i, [_i, _i, _i]),
     ("ves3d_autotune_report", _i, [ctypes.c_char_p, _sz, ctypes.POINTER(_sz)]),
     ("ves3d_sv_launch_eval_graph", _i, [_vp]),
     ("ves3d_sht_forward", _i, [_vp, _l, _i, _i, _vp, _vp]),
@@ -133,6 +134,11 @@ def tables_export(p0, p1, name):
 def set_autotune(on):
     """Turn the far-field launch-shape autotuner on or off (process-wide)."""
     check(lib().ves3d_set_autotune(1 if on else 0), "set_autotune")
+
+
+def set_far_shape(waves=0, chunk=0, targets_per_thread=0):
+    """Fix the far-field launch shape (waves=0: back to the default / autotuned one)."""
+    check(lib().ves3d_set_far_shape(int(waves), int(chunk), int(targets_per_thread)), "set_far_shape")
 
 
 def autotune_report():

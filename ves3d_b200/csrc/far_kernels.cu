@@ -23,6 +23,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -116,6 +117,70 @@ __global__ void __launch_bounds__(512) k_far_f64_seg(const double* __restrict__ 
     P[3 * ib] = B.x;
     P[3 * ib + 1] = B.y;
     P[3 * ib + 2] = B.z;
+  }
+}
+
+// Four targets per thread (a launch shape the autotuner may pick): twice the independent
+// FP64 chains and half the shared-memory reads per pair, at 98 registers.
+template <int TPT>
+__global__ void __launch_bounds__(512) k_far_f64_segT(const double* __restrict__ pos, const double* __restrict__ den,
+                                                     const long* __restrict__ off, long N, int seg_tiles, int v0,
+                                                     double* __restrict__ part) {
+  __shared__ __align__(16) double sm[kTileF64 * 6];
+  const int v = v0 + blockIdx.y, seg = blockIdx.x;
+  const long t0 = off[v], nt = off[v + 1] - t0;
+  const int nthr = blockDim.x;
+  const long c0 = (long)blockIdx.z * TPT * nthr;
+  // TPT targets per thread (independent FP64 chains; one shared-memory read per source)
+  double tx[TPT], ty[TPT], tz[TPT];
+  Acc64 acc[TPT];
+#pragma unroll
+  for (int q = 0; q < TPT; q++) {
+    const long i = c0 + threadIdx.x + (long)q * nthr;
+    const long l = t0 + (i < nt ? i : 0);
+    tx[q] = pos[3 * l];
+    ty[q] = pos[3 * l + 1];
+    tz[q] = pos[3 * l + 2];
+  }
+  const long ntiles = (N + kTileF64 - 1) / kTileF64;
+  const long tb = (long)seg * seg_tiles, te = min(tb + seg_tiles, ntiles);
+  for (long tile = tb; tile < te; tile++) {
+    const long s0 = tile * kTileF64;
+    const int ns = (int)min((long)kTileF64, N - s0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < ns; i += nthr) {
+      const long s = s0 + i;
+      double* d = sm + 6 * i;
+      d[0] = pos[3 * s];
+      d[1] = pos[3 * s + 1];
+      d[2] = pos[3 * s + 2];
+      d[3] = den[3 * s];
+      d[4] = den[3 * s + 1];
+      d[5] = den[3 * s + 2];
+    }
+    __syncthreads();
+    int a0, a1, b0, b1;
+    split_tile(s0, ns, t0, t0 + nt, a0, a1, b0, b1);
+#pragma unroll 2
+    for (int k = a0; k < a1; k++) {
+#pragma unroll
+      for (int q = 0; q < TPT; q++) pair64(sm + 6 * k, tx[q], ty[q], tz[q], acc[q]);
+    }
+#pragma unroll 2
+    for (int k = b0; k < b1; k++) {
+#pragma unroll
+      for (int q = 0; q < TPT; q++) pair64(sm + 6 * k, tx[q], ty[q], tz[q], acc[q]);
+    }
+  }
+  double* P = part + (long)seg * 3 * N;
+#pragma unroll
+  for (int q = 0; q < TPT; q++) {
+    const long i = c0 + threadIdx.x + (long)q * nthr;
+    if (i < nt) {
+      P[3 * (t0 + i)] = acc[q].x;
+      P[3 * (t0 + i) + 1] = acc[q].y;
+      P[3 * (t0 + i) + 2] = acc[q].z;
+    }
   }
 }
 
@@ -262,6 +327,7 @@ __global__ void k_far_reduce(const double* __restrict__ part, int nseg, const lo
 struct FarShape {
   int waves = 8;
   int chunk_max = 1024;
+  int tpt = 2;  // targets per thread (FP64 form: 2 or 4; the FP32 form packs 2)
 };
 
 int far_segments(long nves, long N, int tile, int nthr, int waves, int* seg_tiles) {
@@ -278,11 +344,11 @@ int far_segments(long nves, long N, int tile, int nthr, int waves, int* seg_tile
   return (int)((ntiles + *seg_tiles - 1) / *seg_tiles);
 }
 
-static void chunking(int nt, int chunk_max, int* nchunk, int* nthr) {
-  // targets of a vesicle in chunks of at most chunk_max (two per thread)
+static void chunking(int nt, int chunk_max, int tpt, int* nchunk, int* nthr) {
+  // targets of a vesicle in chunks of at most chunk_max (tpt per thread)
   *nchunk = (nt + chunk_max - 1) / chunk_max;
   const int per_chunk = (nt + *nchunk - 1) / *nchunk;
-  *nthr = 32 * ((((per_chunk + 1) / 2) + 31) / 32);
+  *nthr = 32 * ((((per_chunk + tpt - 1) / tpt) + 31) / 32);
 }
 
 static int launch_far_shape(const FarShape& sh, bool mixed, const double* pos, const double* den, const long* off,
@@ -293,7 +359,7 @@ static int launch_far_shape(const FarShape& sh, bool mixed, const double* pos, c
   long nthr_sum = 0, nchunk_tot = 0;
   for (int g = 0; g < ngroups; g++) {
     int nc, nt;
-    chunking(groups[g].nt, sh.chunk_max, &nc, &nt);
+    chunking(groups[g].nt, sh.chunk_max, mixed ? 2 : sh.tpt, &nc, &nt);
     nthr_sum += (long)nt * groups[g].nv;
     nchunk_tot += (long)nc * groups[g].nv;
   }
@@ -308,10 +374,12 @@ static int launch_far_shape(const FarShape& sh, bool mixed, const double* pos, c
   for (int g = 0; g < ngroups; g++) {
     if (groups[g].nv <= 0) continue;
     int nchunk, nthr;
-    chunking(groups[g].nt, sh.chunk_max, &nchunk, &nthr);
+    chunking(groups[g].nt, sh.chunk_max, mixed ? 2 : sh.tpt, &nchunk, &nthr);
     dim3 grid(nseg, (unsigned)groups[g].nv, nchunk);
     if (mixed)
       k_far_f32_seg<<<grid, nthr, 0, st>>>(pos, den, off, N, seg_tiles, (int)groups[g].v0, part);
+    else if (sh.tpt == 4)
+      k_far_f64_segT<4><<<grid, nthr, 0, st>>>(pos, den, off, N, seg_tiles, (int)groups[g].v0, part);
     else
       k_far_f64_seg<<<grid, nthr, 0, st>>>(pos, den, off, N, seg_tiles, (int)groups[g].v0, part);
     VES3D_LAUNCHED();
@@ -354,12 +422,30 @@ static std::string tune_key(bool mixed, long nves, long N, const FarGroup* group
   return k;
 }
 
+static FarShape g_forced{0, 0, 0};  // a caller-fixed shape (waves 0 = none)
+
+int set_far_shape(int waves, int chunk_max, int tpt) {
+  if (waves == 0) {
+    g_forced = FarShape{0, 0, 0};
+    return VES3D_OK;
+  }
+  if ((waves != 4 && waves != 8 && waves != 16) || (chunk_max != 512 && chunk_max != 1024) ||
+      (tpt != 2 && tpt != 4)) {
+    set_error("far shape: waves in {4, 8, 16}, chunk in {512, 1024}, targets per thread in {2, 4}");
+    return VES3D_ERR_ARG;
+  }
+  g_forced = FarShape{waves, chunk_max, tpt};
+  return VES3D_OK;
+}
+
 int launch_far_groups(bool mixed, const double* pos, const double* den, const long* off, long nves, long N,
                       const FarGroup* groups, int ngroups, const double* add, double* out, double* far_out,
                       double* part, long part_cap_segments, cudaStream_t st) {
   if (N <= 0) return VES3D_OK;
   FarShape shape;
-  if (autotune_on()) {
+  if (g_forced.waves) {
+    shape = g_forced;
+  } else if (autotune_on()) {
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     VES3D_CK(cudaStreamIsCapturing(st, &cap));
     const std::string key = tune_key(mixed, nves, N, groups, ngroups);
@@ -373,7 +459,12 @@ int launch_far_groups(bool mixed, const double* pos, const double* den, const lo
       }
     }
     if (!have && cap == cudaStreamCaptureStatusNone) {
-      const FarShape cands[] = {{4, 1024}, {8, 1024}, {16, 1024}, {4, 512}, {8, 512}, {16, 512}};
+      std::vector<FarShape> cands;
+      for (int tpt : {2, 4}) {
+        if (mixed && tpt != 2) continue;
+        for (int chunk : {1024, 512})
+          for (int waves : {4, 8, 16}) cands.push_back(FarShape{waves, chunk, tpt});
+      }
       cudaEvent_t e0, e1;
       VES3D_CK(cudaEventCreate(&e0));
       VES3D_CK(cudaEventCreate(&e1));
@@ -419,7 +510,8 @@ std::string autotune_report() {
   std::string r;
   for (const auto& kv : g_tuned)
     r += kv.first + " waves=" + std::to_string(kv.second.shape.waves) + " chunk=" +
-         std::to_string(kv.second.shape.chunk_max) + " ms=" + std::to_string(kv.second.ms) + "\n";
+         std::to_string(kv.second.shape.chunk_max) + " tpt=" + std::to_string(kv.second.shape.tpt) +
+         " ms=" + std::to_string(kv.second.ms) + "\n";
   return r;
 }
 

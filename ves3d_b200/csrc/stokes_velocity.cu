@@ -577,6 +577,10 @@ int ves3d_sv_eval_resident(ves3d_sv* sv) {
 
 int ves3d_set_autotune(int on) { return set_autotune(on); }
 
+int ves3d_set_far_shape(int waves, int chunk_max, int targets_per_thread) {
+  return set_far_shape(waves, chunk_max, targets_per_thread);
+}
+
 int ves3d_autotune_report(char* buf, size_t cap, size_t* len) {
   VES3D_ARG(len != nullptr, "len is null");
   const std::string r = autotune_report();
