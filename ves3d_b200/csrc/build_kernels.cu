@@ -146,11 +146,25 @@ __global__ void __launch_bounds__(256, 2) k_build_ring(const double* __restrict_
     const int lat0 = g * G::LG;
     const int nlat = min(G::LG, G::L1 - lat0);
     // ---- the group's slice of the Legendre tables -------------------------------------
-    for (int i = tid; i < G::LDR * G::LG; i += 256) {
-      const int l = i / G::LDR, c = i - l * G::LDR;
-      const bool ok = l < nlat && c < G::NC;
-      sLeg[i] = ok ? __ldg(T.syn1_leg_t + (lat0 + l) * G::NC + c) : 0.0;
-      sdLeg[i] = ok ? __ldg(T.syn1_dleg_t + (lat0 + l) * G::NC + c) : 0.0;
+    {
+      constexpr int U = (G::LDR * G::LG + 255) / 256;  // loads in flight per thread
+      double a[U], b[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int i = tid + u * 256;
+        const int l = i / G::LDR, c = i - l * G::LDR;
+        const bool ok = i < G::LDR * G::LG && l < nlat && c < G::NC;
+        a[u] = ok ? __ldg(T.syn1_leg_t + (lat0 + l) * G::NC + c) : 0.0;
+        b[u] = ok ? __ldg(T.syn1_dleg_t + (lat0 + l) * G::NC + c) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int i = tid + u * 256;
+        if (i < G::LDR * G::LG) {
+          sLeg[i] = a[u];
+          sdLeg[i] = b[u];
+        }
+      }
     }
     __syncthreads();
     // ---- Legendre synthesis of the group's latitudes on tensor cores ------------------

@@ -20,22 +20,45 @@ __global__ void __launch_bounds__(256) k_rotate_all(const double* __restrict__ S
   double* sS = sm;
   double* sB = sm + 3 * nc;
   double* sM = sm + 6 * nc;
+  double* sCs = sM + mr_per_t;                                     // cos_tab [2 p0]
+  double* sSn = sCs + 2 * p0;                                      // sin_tab [2 p0]
+  int* sMo = reinterpret_cast<int*>(sSn + 2 * p0);                 // mr_off of (t, n) - base [p0 + 1]
+  int* sPo = sMo + (p0 + 1);                                       // perm_off [p0 + 2]
+  short* sPc = reinterpret_cast<short*>(sPo + (p0 + 2));           // partner [nc]
+  unsigned short* sPerm = reinterpret_cast<unsigned short*>(sPc + nc);  // perm [nc]
+  unsigned char* sMs = reinterpret_cast<unsigned char*>(sPerm + nc);    // m | (is_sin << 7) [nc]
+  unsigned char* sN = sMs + nc;                                    // degree [nc]
+  unsigned char* sBp = sN + nc;                                    // position in block [nc]
   const int t = blockIdx.x;
   const long v = blockIdx.y;
   const int mbase = __ldg(T.mr_off + t * (p0 + 1));
   for (int i = threadIdx.x; i < 3 * nc; i += blockDim.x) sS[i] = S[v * 3 * nc + i];
   for (int i = threadIdx.x; i < mr_per_t; i += blockDim.x) sM[i] = __ldg(T.mr + mbase + i);
+  for (int i = threadIdx.x; i < 2 * p0; i += blockDim.x) {
+    sCs[i] = __ldg(T.cos_tab + i);
+    sSn[i] = __ldg(T.sin_tab + i);
+  }
+  for (int i = threadIdx.x; i <= p0; i += blockDim.x) sMo[i] = __ldg(T.mr_off + t * (p0 + 1) + i) - mbase;
+  for (int i = threadIdx.x; i <= p0 + 1; i += blockDim.x) sPo[i] = __ldg(T.perm_off + i);
+  for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+    sPc[c] = (short)__ldg(T.partner + c);
+    sPerm[c] = (unsigned short)__ldg(T.perm + c);
+    sMs[c] = (unsigned char)(__ldg(T.m_of_coef + c) | (__ldg(T.is_sin + c) ? 0x80 : 0));
+    sN[c] = (unsigned char)__ldg(T.n_of_coef + c);
+    sBp[c] = (unsigned char)__ldg(T.pos_in_block + c);
+  }
   __syncthreads();
   for (int j = 0; j < p0; j++) {
     for (int i = threadIdx.x; i < 3 * nc; i += blockDim.x) {
       const int d = i / nc, c = i % nc;
-      const int pc = __ldg(T.partner + c);
+      const int pc = sPc[c];
       if (pc < 0) {
         sB[i] = sS[i];
       } else {
-        const int q = (__ldg(T.m_of_coef + c) * j) % (2 * p0);
-        const double cs = __ldg(T.cos_tab + q), sn = __ldg(T.sin_tab + q);
-        if (!__ldg(T.is_sin + c)) {
+        const int ms = sMs[c];
+        const int q = ((ms & 0x7f) * j) % (2 * p0);
+        const double cs = sCs[q], sn = sSn[q];
+        if (!(ms & 0x80)) {
           sB[i] = sS[i] * cs + sS[d * nc + pc] * sn;
         } else {
           sB[i] = -sS[d * nc + pc] * sn + sS[i] * cs;
@@ -46,12 +69,12 @@ __global__ void __launch_bounds__(256) k_rotate_all(const double* __restrict__ S
     double* out = R + (((v * (p0 + 1) + t) * p0 + j) * 3) * (long)nc;
     for (int i = threadIdx.x; i < 3 * nc; i += blockDim.x) {
       const int d = i / nc, c = i % nc;
-      const int n = __ldg(T.n_of_coef + c), bp = __ldg(T.pos_in_block + c);
-      const int po = __ldg(T.perm_off + n), bn = __ldg(T.perm_off + n + 1) - po;
-      const double* M = sM + (__ldg(T.mr_off + t * (p0 + 1) + n) - mbase);
+      const int n = sN[c], bp = sBp[c];
+      const int po = sPo[n], bn = sPo[n + 1] - po;
+      const double* M = sM + sMo[n];
       const double* b = sB + d * nc;
       double s = 0.0;
-      for (int k = 0; k < bn; k++) s = fma(b[__ldg(T.perm + po + k)], M[k * bn + bp], s);
+      for (int k = 0; k < bn; k++) s = fma(b[sPerm[po + k]], M[k * bn + bp], s);
       out[i] = s;
     }
     __syncthreads();
@@ -64,7 +87,13 @@ int launch_rotate_all(const double* S, long nv, const DevTables& T, double* R, c
   if (nv <= 0) return VES3D_OK;
   const int p0 = T.p0;
   const int mpt = mr_per_t(T);
-  size_t smem = ((size_t)6 * ncoef_(p0) + mpt) * sizeof(double);
+  const size_t nc = ncoef_(p0);
+  if (p0 > 127) {  // the on-chip tables hold orders and block positions in one byte
+    set_error("rotation kernels support SH orders up to 127");
+    return VES3D_ERR_ARG;
+  }
+  const size_t smem = ((6 * nc + mpt + 4 * p0) * sizeof(double) + (2 * p0 + 3) * sizeof(int) + nc * 4 + nc * 3 + 15) /
+                      16 * 16;
   if (smem > 48 * 1024) VES3D_CK(cudaFuncSetAttribute(k_rotate_all, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid(p0 + 1, (unsigned)nv);
   k_rotate_all<<<grid, 256, smem, st>>>(S, p0, mpt, T, R);
@@ -251,13 +280,26 @@ __global__ void __launch_bounds__(256, 2) k_rotate_transpose_tc(const double* __
   const int nc = p0 * (p0 + 2), ng = 2 * p0 * (p0 + 1);
   const int rows = cb * p0, rows8 = (rows + 7) & ~7;
   double* sIn = sm;                                                        // rows8 x ldi
-  unsigned short* sDm = reinterpret_cast<unsigned short*>(sm + (size_t)rows8 * ldi);  // nc
+  double* sCs = sm + (size_t)rows8 * ldi;                                  // cos_tab [2 p0]
+  double* sSn = sCs + 2 * p0;                                              // sin_tab [2 p0]
+  unsigned short* sDm = reinterpret_cast<unsigned short*>(sSn + 2 * p0);   // degree-major position [nc]
+  short* sPc = reinterpret_cast<short*>(sDm + nc);                        // partner (or -1) [nc]
+  unsigned char* sMs = reinterpret_cast<unsigned char*>(sPc + nc);        // m | (is_sin << 7) [nc]
   const int t = blockIdx.x;
   const long v = blockIdx.y;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int grow = lane >> 2, gcol = lane & 3;
-  for (int c = tid; c < nc; c += 256)
+  // per-coefficient tables of the phase / scatter step, on chip (the L1 left beside the
+  // staging buffer is small, and every element needs them)
+  for (int c = tid; c < nc; c += 256) {
     sDm[c] = (unsigned short)(__ldg(T.perm_off + __ldg(T.n_of_coef + c)) + __ldg(T.pos_in_block + c));
+    sPc[c] = (short)__ldg(T.partner + c);
+    sMs[c] = (unsigned char)(__ldg(T.m_of_coef + c) | (__ldg(T.is_sin + c) ? 0x80 : 0));
+  }
+  for (int i = tid; i < 2 * p0; i += 256) {
+    sCs[i] = __ldg(T.cos_tab + i);
+    sSn[i] = __ldg(T.sin_tab + i);
+  }
   // zero the K padding of every row and the padding rows once (never overwritten)
   for (int i = tid; i < rows8 * ldi; i += 256) {
     const int r = i / ldi, col = i - r * ldi;
@@ -268,12 +310,27 @@ __global__ void __launch_bounds__(256, 2) k_rotate_transpose_tc(const double* __
   for (int pole = 0; pole < 2; pole++) {
     for (int comp0 = 0; comp0 < 6; comp0 += cb) {
       __syncthreads();
-      // stage: In[(cc, j)][dm(c)] = C[v][t][j][pole][comp0 + cc][c]
-      for (int i = tid; i < rows * nc; i += 256) {
-        const int r = i / nc, c = i - r * nc;
-        const int cc = r / p0, j = r - cc * p0;
-        sIn[r * ldi + sDm[c]] =
-            C[((((v * (p0 + 1) + t) * p0 + j) * 2 + pole) * 6 + comp0 + cc) * (long)nc + c];
+      // stage: In[(cc, j)][dm(c)] = C[v][t][j][pole][comp0 + cc][c], eight loads in flight
+      // per thread before the shared-memory stores
+      for (int i0 = tid; i0 < rows * nc; i0 += 256 * 8) {
+        double val[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          const int i = i0 + u * 256;
+          if (i < rows * nc) {
+            const int r = i / nc, c = i - r * nc;
+            const int cc = r / p0, j = r - cc * p0;
+            val[u] = C[((((v * (p0 + 1) + t) * p0 + j) * 2 + pole) * 6 + comp0 + cc) * (long)nc + c];
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          const int i = i0 + u * 256;
+          if (i < rows * nc) {
+            const int r = i / nc, c = i - r * nc;
+            sIn[r * ldi + sDm[c]] = val[u];
+          }
+        }
       }
       __syncthreads();
       for (int n = 0; n <= p0; n++) {
@@ -326,14 +383,15 @@ __global__ void __launch_bounds__(256, 2) k_rotate_transpose_tc(const double* __
         const int j = i % p0, rest = i / p0;
         const int c = rest % nc, cc = rest / nc;
         const double* in = sIn + (cc * p0 + j) * ldi;
-        const int pc = __ldg(T.partner + c);
+        const int pc = sPc[c];
         double val;
         if (pc < 0) {
           val = in[sDm[c]];
         } else {
-          const int q = (__ldg(T.m_of_coef + c) * j) % (2 * p0);
-          const double cs = __ldg(T.cos_tab + q), sn = __ldg(T.sin_tab + q);
-          if (!__ldg(T.is_sin + c))
+          const int ms = sMs[c];
+          const int q = ((ms & 0x7f) * j) % (2 * p0);
+          const double cs = sCs[q], sn = sSn[q];
+          if (!(ms & 0x80))
             val = in[sDm[c]] * cs - in[sDm[pc]] * sn;
           else
             val = in[sDm[pc]] * sn + in[sDm[c]] * cs;
@@ -357,8 +415,8 @@ int launch_rotate_transpose_scatter(const double* C, long nv, const DevTables& T
     const int ldi = pad4_16(nc + 3);
     for (int cb : {3, 2, 1}) {
       const int rows8 = ((cb * p0) + 7) & ~7;
-      const size_t smem = (size_t)rows8 * ldi * sizeof(double) + ((size_t)nc * 2 + 15) / 16 * 16;
-      if (p0 <= 16 && smem <= 112 * 1024 && !tc_rotate_disabled()) {
+      const size_t smem = ((size_t)rows8 * ldi + 4 * p0) * sizeof(double) + ((size_t)nc * 5 + 15) / 16 * 16;
+      if (p0 <= 16 && smem <= 113 * 1024 && !tc_rotate_disabled()) {
         VES3D_CK(cudaFuncSetAttribute(k_rotate_transpose_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         dim3 grid(p0 + 1, (unsigned)nv);
         k_rotate_transpose_tc<<<grid, 256, smem, st>>>(C, p0, cb, ldi, T, SL3);
