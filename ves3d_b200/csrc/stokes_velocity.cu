@@ -801,6 +801,7 @@ void ves3d_stokes_alltoall_f64(const double* src, const double* den, size_t np, 
     if (pot) fail();
     return;
   }
+  if (np == 0) return;  // nothing to compute
   InteractionWorkspace local;
   InteractionWorkspace* ws = &local;
   if (ctx) {
@@ -1384,6 +1385,11 @@ int mixed_refinement(ves3d_sv* sv, double* x, const double* b, long n, double* t
     if ((s = dot_f64(r, r, n, bicgstab_dot_scratch(ws, n), &rr, sv->stream))) break;
     const double cur = std::sqrt(rr) / normb;
     outer++;
+    if (cur != cur) {  // non-finite residual (BiCGSReturn RelresIsNan)
+      relres = cur;
+      *code = 104;
+      break;
+    }
     if (cur > relres) {
       // the last correction made things worse: undo it, continue with FP64 inner solves
       if ((s = lincomb_f64(n, 1.0, x, -1.0, d, 0.0, nullptr, x, sv->stream))) break;
