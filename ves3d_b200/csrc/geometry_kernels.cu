@@ -19,6 +19,10 @@ namespace ves3d {
   if (g >= (N)) return;                                               \
   const long v = g / ng, k = g - v * ng;
 
+// Fields may hold several copies of the suspension (batched operator applications):
+// field vesicle v uses the geometry of vesicle v % geo_nv.
+#define GEO_OF(v) (geo + ((v) % geo_nv) * kGeoComps * (long)ng + k)
+
 __global__ void k_geometry(const double* __restrict__ xu, const double* __restrict__ xv,
                            const double* __restrict__ xuu, const double* __restrict__ xuv,
                            const double* __restrict__ xvv, long N, int ng, double* __restrict__ geo) {
@@ -67,9 +71,9 @@ __global__ void k_geometry(const double* __restrict__ xu, const double* __restri
 
 // grad: out[v][c][k] = fu cu[c] + fv cv[c]   (fu, fv scalar fields [nv][ng])
 __global__ void k_grad_combine(const double* __restrict__ fu, const double* __restrict__ fv,
-                               const double* __restrict__ geo, long N, int ng, double* __restrict__ out) {
+                               const double* __restrict__ geo, long N, int ng, double* __restrict__ out, long geo_nv) {
   FOR_POINTS(N)
-  const double* o = geo + v * kGeoComps * (long)ng + k;
+  const double* o = GEO_OF(v);
   const double a = fu[g], b = fv[g];
 #pragma unroll
   for (int c = 0; c < 3; c++) out[v * 3 * ng + c * ng + k] = a * o[(7 + c) * ng] + b * o[(10 + c) * ng];
@@ -78,9 +82,9 @@ __global__ void k_grad_combine(const double* __restrict__ fu, const double* __re
 // div: out[g] = sum_c Fu[c] cu[c] + Fv[c] cv[c]   (Fu, Fv vector fields)
 __global__ void k_div_combine(const double* __restrict__ Fu, const double* __restrict__ Fv,
                               const double* __restrict__ geo, long N, int ng, double scale,
-                              double* __restrict__ out) {
+                              double* __restrict__ out, long geo_nv) {
   FOR_POINTS(N)
-  const double* o = geo + v * kGeoComps * (long)ng + k;
+  const double* o = GEO_OF(v);
   const long b = v * 3 * ng + k;
   double s = 0.0, t = 0.0;
 #pragma unroll
@@ -94,9 +98,9 @@ __global__ void k_div_combine(const double* __restrict__ Fu, const double* __res
 // linearised mean curvature: 0.5 (G (x_uu.n) - 2 F (x_uv.n) + E (x_vv.n))
 __global__ void k_linH_combine(const double* __restrict__ duu, const double* __restrict__ duv,
                                const double* __restrict__ dvv, const double* __restrict__ geo, long N, int ng,
-                               double* __restrict__ out) {
+                               double* __restrict__ out, long geo_nv) {
   FOR_POINTS(N)
-  const double* o = geo + v * kGeoComps * (long)ng + k;
+  const double* o = GEO_OF(v);
   const long b = v * 3 * ng + k;
   double a = 0, m = 0, c2 = 0;
 #pragma unroll
@@ -113,9 +117,9 @@ __global__ void k_linH_combine(const double* __restrict__ duu, const double* __r
 // written to out (AxisMajor vector) with out = add + that if add is given.
 __global__ void k_bend_combine(const double* __restrict__ h, const double* __restrict__ lap,
                                const double* __restrict__ geo, long N, int ng, double kappa,
-                               const double* __restrict__ add, double* __restrict__ out) {
+                               const double* __restrict__ add, double* __restrict__ out, long geo_nv) {
   FOR_POINTS(N)
-  const double* o = geo + v * kGeoComps * (long)ng + k;
+  const double* o = GEO_OF(v);
   const double H = o[13 * ng], K = o[14 * ng];
   const double s = kappa * (lap[g] + 2.0 * h[g] * (H * H - K));
 #pragma unroll
@@ -128,9 +132,9 @@ __global__ void k_bend_combine(const double* __restrict__ h, const double* __res
 // tension traction: 2 sigma H n + grad sigma (grad given as a vector field), added to add
 __global__ void k_tension_combine(const double* __restrict__ sigma, const double* __restrict__ gsig,
                                   const double* __restrict__ geo, long N, int ng, const double* __restrict__ add,
-                                  double* __restrict__ out) {
+                                  double* __restrict__ out, long geo_nv) {
   FOR_POINTS(N)
-  const double* o = geo + v * kGeoComps * (long)ng + k;
+  const double* o = GEO_OF(v);
   const double s = 2.0 * sigma[g] * o[13 * ng];
 #pragma unroll
   for (int c = 0; c < 3; c++) {
@@ -216,46 +220,46 @@ int launch_geometry(const double* xu, const double* xv, const double* xuu, const
 }
 
 int launch_grad_combine(const double* fu, const double* fv, const double* geo, long nv, int ng, double* out,
-                        cudaStream_t st) {
+                        cudaStream_t st, long geo_nv) {
   const long N = nv * ng;
   if (N <= 0) return VES3D_OK;
-  k_grad_combine<<<nblk(N), 256, 0, st>>>(fu, fv, geo, N, ng, out);
+  k_grad_combine<<<nblk(N), 256, 0, st>>>(fu, fv, geo, N, ng, out, geo_nv > 0 ? geo_nv : nv);
   VES3D_LAUNCHED();
   return VES3D_OK;
 }
 
 int launch_div_combine(const double* Fu, const double* Fv, const double* geo, long nv, int ng, double scale,
-                       double* out, cudaStream_t st) {
+                       double* out, cudaStream_t st, long geo_nv) {
   const long N = nv * ng;
   if (N <= 0) return VES3D_OK;
-  k_div_combine<<<nblk(N), 256, 0, st>>>(Fu, Fv, geo, N, ng, scale, out);
+  k_div_combine<<<nblk(N), 256, 0, st>>>(Fu, Fv, geo, N, ng, scale, out, geo_nv > 0 ? geo_nv : nv);
   VES3D_LAUNCHED();
   return VES3D_OK;
 }
 
 int launch_linH_combine(const double* duu, const double* duv, const double* dvv, const double* geo, long nv, int ng,
-                        double* out, cudaStream_t st) {
+                        double* out, cudaStream_t st, long geo_nv) {
   const long N = nv * ng;
   if (N <= 0) return VES3D_OK;
-  k_linH_combine<<<nblk(N), 256, 0, st>>>(duu, duv, dvv, geo, N, ng, out);
+  k_linH_combine<<<nblk(N), 256, 0, st>>>(duu, duv, dvv, geo, N, ng, out, geo_nv > 0 ? geo_nv : nv);
   VES3D_LAUNCHED();
   return VES3D_OK;
 }
 
 int launch_bend_combine(const double* h, const double* lap, const double* geo, long nv, int ng, double kappa,
-                        const double* add, double* out, cudaStream_t st) {
+                        const double* add, double* out, cudaStream_t st, long geo_nv) {
   const long N = nv * ng;
   if (N <= 0) return VES3D_OK;
-  k_bend_combine<<<nblk(N), 256, 0, st>>>(h, lap, geo, N, ng, kappa, add, out);
+  k_bend_combine<<<nblk(N), 256, 0, st>>>(h, lap, geo, N, ng, kappa, add, out, geo_nv > 0 ? geo_nv : nv);
   VES3D_LAUNCHED();
   return VES3D_OK;
 }
 
 int launch_tension_combine(const double* sigma, const double* gsig, const double* geo, long nv, int ng,
-                           const double* add, double* out, cudaStream_t st) {
+                           const double* add, double* out, cudaStream_t st, long geo_nv) {
   const long N = nv * ng;
   if (N <= 0) return VES3D_OK;
-  k_tension_combine<<<nblk(N), 256, 0, st>>>(sigma, gsig, geo, N, ng, add, out);
+  k_tension_combine<<<nblk(N), 256, 0, st>>>(sigma, gsig, geo, N, ng, add, out, geo_nv > 0 ? geo_nv : nv);
   VES3D_LAUNCHED();
   return VES3D_OK;
 }

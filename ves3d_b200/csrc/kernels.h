@@ -58,6 +58,8 @@ bool fused_build_supported(int p0, int p1);
 int launch_build_ring(const double* R, long nrot, const DevTables& T, double* C, cudaStream_t st);
 // V[v] = F[v] . SL[v] (src/StokesVelocity.cc:397-416), n = 3 Ncoef.
 int launch_self_gemv(const double* F, const double* SL, long nv, int n, double* V, cudaStream_t st);
+// nvec density vectors per vesicle, layout [q][nv][n]; nvec <= 8
+int launch_self_gemv_multi(const double* F, const double* SL, long nv, int nvec, int n, double* V, cudaStream_t st);
 // area element |X_theta x X_phi| and far-field sources: pos/den point-major [N][3],
 // den = f * area * smooth_w[lat]; X, f, Xt, Xp AxisMajor [nv][3][ng].
 int launch_far_sources(const double* X, const double* f, const double* Xt, const double* Xp, long nv, int p0,
@@ -97,15 +99,20 @@ int launch_direct_stokes_f64(int src_m, int trg_m, int n, int t_head, int t_tail
 int launch_geometry(const double* xu, const double* xv, const double* xuu, const double* xuv, const double* xvv,
                     long nv, int ng, double* geo, cudaStream_t st);
 int launch_grad_combine(const double* fu, const double* fv, const double* geo, long nv, int ng, double* out,
-                        cudaStream_t st);
+                        cudaStream_t st,
+    long geo_nv = 0);
 int launch_div_combine(const double* Fu, const double* Fv, const double* geo, long nv, int ng, double scale,
-                       double* out, cudaStream_t st);
+                       double* out, cudaStream_t st,
+    long geo_nv = 0);
 int launch_linH_combine(const double* duu, const double* duv, const double* dvv, const double* geo, long nv, int ng,
-                        double* out, cudaStream_t st);
+                        double* out, cudaStream_t st,
+    long geo_nv = 0);
 int launch_bend_combine(const double* h, const double* lap, const double* geo, long nv, int ng, double kappa,
-                        const double* add, double* out, cudaStream_t st);
+                        const double* add, double* out, cudaStream_t st,
+    long geo_nv = 0);
 int launch_tension_combine(const double* sigma, const double* gsig, const double* geo, long nv, int ng,
-                           const double* add, double* out, cudaStream_t st);
+                           const double* add, double* out, cudaStream_t st,
+    long geo_nv = 0);
 int launch_shear(const double* X, long nv, int ng, double rate, double* out, cudaStream_t st);
 // per vesicle {area, volume, centre x, y, z} (Xu latitude, Xv longitude derivatives)
 int launch_integrals(const double* X, const double* Xu, const double* Xv, const double* w, long nv, int p,

@@ -463,6 +463,51 @@ __global__ void __launch_bounds__(128) k_self_gemv(const double* __restrict__ F,
   V[v * n + col] = (s0 + s1) + (s2 + s3);
 }
 
+// Several density vectors per vesicle at once (batched operator applications):
+// V[q nv + v][col] = sum_row F[q nv + v][row] SL[v][row][col], q < nvec; every SL column is
+// read once for all nvec vectors (the single-vector form reads it per vector).
+constexpr int kGemvMaxVec = 8;
+__global__ void __launch_bounds__(128) k_self_gemv_multi(const double* __restrict__ F, const double* __restrict__ SL,
+                                                         long nv, int nvec, int n, double* __restrict__ V) {
+  extern __shared__ double sF[];  // [nvec][n]
+  const long v = blockIdx.y;
+  for (int i = threadIdx.x; i < nvec * n; i += blockDim.x) {
+    const int q = i / n, r = i - q * n;
+    sF[i] = F[((long)q * nv + v) * n + r];
+  }
+  __syncthreads();
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= n) return;
+  const double* M = SL + v * (long)n * n + col;
+  double acc[kGemvMaxVec];
+#pragma unroll
+  for (int q = 0; q < kGemvMaxVec; q++) acc[q] = 0.0;
+  for (int r = 0; r < n; r++) {
+    const double m = __ldg(M + (long)r * n);
+#pragma unroll
+    for (int q = 0; q < kGemvMaxVec; q++)
+      if (q < nvec) acc[q] = fma(sF[q * n + r], m, acc[q]);
+  }
+#pragma unroll
+  for (int q = 0; q < kGemvMaxVec; q++)
+    if (q < nvec) V[((long)q * nv + v) * n + col] = acc[q];
+}
+
+int launch_self_gemv_multi(const double* F, const double* SL, long nv, int nvec, int n, double* V, cudaStream_t st) {
+  if (nv <= 0 || nvec <= 0) return VES3D_OK;
+  if (nvec > kGemvMaxVec) {
+    set_error("launch_self_gemv_multi: at most %d vectors", kGemvMaxVec);
+    return VES3D_ERR_ARG;
+  }
+  dim3 grid((n + 127) / 128, (unsigned)nv);
+  const size_t smem = (size_t)nvec * n * sizeof(double);
+  if (smem > 48 * 1024)
+    VES3D_CK(cudaFuncSetAttribute(k_self_gemv_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_self_gemv_multi<<<grid, 128, smem, st>>>(F, SL, nv, nvec, n, V);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
 int launch_self_gemv(const double* F, const double* SL, long nv, int n, double* V, cudaStream_t st) {
   if (nv <= 0) return VES3D_OK;
   dim3 grid((n + 127) / 128, (unsigned)nv);

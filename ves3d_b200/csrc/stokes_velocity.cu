@@ -130,6 +130,7 @@ struct TablesOwner {
 using namespace ves3d;
 
 constexpr int kPcStreams = 32;  // streams of the preconditioner factorisation
+constexpr int kPcBatch = 8;     // operator columns per application in its assembly
 
 struct ves3d_sv {
   int p = 0, pup = 0, prec = 0, device = 0;
@@ -155,7 +156,6 @@ struct ves3d_sv {
   // preconditioner of the implicit solve (VES3D_PRECOND_*); the self-block form stores one
   // inverse per vesicle, [nv][n][n] column-major in FP32 (n = 4 nc)
   int precond = 0;
-  bool self_only = false;      // stokes_apply evaluates the self part only (assembly)
   float* pc_inv = nullptr;
   double* pc_diag = nullptr;   // diagonal-spectral scales [4 nc]
   long pc_cap = 0;
@@ -911,57 +911,105 @@ int ensure_geometry(ves3d_sv* sv) {
   return VES3D_OK;
 }
 
+// The space the implicit operator acts on: nv field vesicles with their work fields and
+// coefficient scratch. Normally the suspension itself; when several operator
+// applications are batched (the preconditioner assembly), nv = k nves field vesicles,
+// copy q of vesicle v at index q nves + v, which use the geometry record and the self
+// matrix of vesicle v.
+struct OpSpace {
+  long nv = 0;
+  double* w[8] = {};
+  double* wc = nullptr;
+  double* fc = nullptr;  // batched self part: density / velocity coefficients [nv][3 nc]
+  double* vc = nullptr;
+};
+
+OpSpace base_space(ves3d_sv* sv) {
+  OpSpace sp;
+  sp.nv = sv->nves;
+  for (int k = 0; k < 8; k++) sp.w[k] = sv->w[k];
+  sp.wc = sv->wc;
+  return sp;
+}
+
 // grad of a scalar field (in [nv][ng]) -> out [nv][3][ng]; uses w6, w7 and wc
-int op_grad(ves3d_sv* sv, const double* in, double* out) {
+int op_grad(ves3d_sv* sv, const OpSpace& sp, const double* in, double* out) {
   int s;
-  const long nv = sv->nves;
+  const long nv = sp.nv;
   const int ng = ngrid_(sv->p);
-  double *a = sv->w[6], *b = sv->w[7];
-  if ((s = grid2shc_p(sv, in, nv, sv->wc))) return s;
+  double *a = sp.w[6], *b = sp.w[7];
+  if ((s = grid2shc_p(sv, in, nv, sp.wc))) return s;
   // value into out (overwritten below), v-derivative into a, u-derivative into b
-  if ((s = synth_d(sv, sv->wc, nv, 0, out, a, b))) return s;
-  return launch_grad_combine(b, a, sv->geo, nv, ng, out, sv->stream);
+  if ((s = synth_d(sv, sp.wc, nv, 0, out, a, b))) return s;
+  return launch_grad_combine(b, a, sv->geo, nv, ng, out, sv->stream, sv->nves);
 }
 
 // div of a vector field (in [nv][3][ng]) -> out [nv][ng] times scale; uses w5, w6, w7, wc
-int op_div(ves3d_sv* sv, const double* in, double* out, double scale) {
+int op_div(ves3d_sv* sv, const OpSpace& sp, const double* in, double* out, double scale) {
   int s;
-  const long nv = sv->nves;
+  const long nv = sp.nv;
   const int ng = ngrid_(sv->p);
-  if ((s = grid2shc_p(sv, in, 3 * nv, sv->wc))) return s;
-  if ((s = synth_d(sv, sv->wc, 3 * nv, 0, sv->w[5], sv->w[6], sv->w[7]))) return s;
-  return launch_div_combine(sv->w[7], sv->w[6], sv->geo, nv, ng, scale, out, sv->stream);
+  if ((s = grid2shc_p(sv, in, 3 * nv, sp.wc))) return s;
+  if ((s = synth_d(sv, sp.wc, 3 * nv, 0, sp.w[5], sp.w[6], sp.w[7]))) return s;
+  return launch_div_combine(sp.w[7], sp.w[6], sv->geo, nv, ng, scale, out, sv->stream, sv->nves);
 }
 
 // linearised mean curvature of a displacement field; uses w4..w7, wc
-int op_linH(ves3d_sv* sv, const double* in, double* out) {
+int op_linH(ves3d_sv* sv, const OpSpace& sp, const double* in, double* out) {
   int s;
-  const long nv = sv->nves;
+  const long nv = sp.nv;
   const int ng = ngrid_(sv->p);
-  if ((s = grid2shc_p(sv, in, 3 * nv, sv->wc))) return s;
-  if ((s = synth_d(sv, sv->wc, 3 * nv, 1, sv->w[4], sv->w[5], sv->w[6]))) return s;  // u, uv, uu
-  if ((s = synth_d(sv, sv->wc, 3 * nv, 2, sv->w[7], nullptr, nullptr))) return s;    // vv
-  return launch_linH_combine(sv->w[6], sv->w[5], sv->w[7], sv->geo, nv, ng, out, sv->stream);
+  if ((s = grid2shc_p(sv, in, 3 * nv, sp.wc))) return s;
+  if ((s = synth_d(sv, sp.wc, 3 * nv, 1, sp.w[4], sp.w[5], sp.w[6]))) return s;  // u, uv, uu
+  if ((s = synth_d(sv, sp.wc, 3 * nv, 2, sp.w[7], nullptr, nullptr))) return s;    // vv
+  return launch_linH_combine(sp.w[6], sp.w[5], sp.w[7], sv->geo, nv, ng, out, sv->stream, sv->nves);
 }
 
 // bending traction of a scalar h (the mean curvature or its linearisation), added to add.
 // scratch: w3 (gradient), w2 (Laplacian)
-int op_bend_of(ves3d_sv* sv, const double* h, const double* add, double* out) {
+int op_bend_of(ves3d_sv* sv, const OpSpace& sp, const double* h, const double* add, double* out) {
   int s;
-  const long nv = sv->nves;
+  const long nv = sp.nv;
   const int ng = ngrid_(sv->p);
-  if ((s = op_grad(sv, h, sv->w[3]))) return s;
-  if ((s = op_div(sv, sv->w[3], sv->w[2], 1.0))) return s;
-  return launch_bend_combine(h, sv->w[2], sv->geo, nv, ng, sv->kappa, add, out, sv->stream);
+  if ((s = op_grad(sv, sp, h, sp.w[3]))) return s;
+  if ((s = op_div(sv, sp, sp.w[3], sp.w[2], 1.0))) return s;
+  return launch_bend_combine(h, sp.w[2], sv->geo, nv, ng, sv->kappa, add, out, sv->stream, sv->nves);
 }
 
 // tension traction of sigma added to add; scratch w3
-int op_tension(ves3d_sv* sv, const double* sigma, const double* add, double* out) {
+int op_tension(ves3d_sv* sv, const OpSpace& sp, const double* sigma, const double* add, double* out) {
   int s;
-  const long nv = sv->nves;
+  const long nv = sp.nv;
   const int ng = ngrid_(sv->p);
-  if ((s = op_grad(sv, sigma, sv->w[3]))) return s;
-  return launch_tension_combine(sigma, sv->w[3], sv->geo, nv, ng, add, out, sv->stream);
+  if ((s = op_grad(sv, sp, sigma, sp.w[3]))) return s;
+  return launch_tension_combine(sigma, sp.w[3], sv->geo, nv, ng, add, out, sv->stream, sv->nves);
+}
+
+int op_grad(ves3d_sv* sv, const double* in, double* out) { return op_grad(sv, base_space(sv), in, out); }
+int op_div(ves3d_sv* sv, const double* in, double* out, double scale) {
+  return op_div(sv, base_space(sv), in, out, scale);
+}
+int op_linH(ves3d_sv* sv, const double* in, double* out) { return op_linH(sv, base_space(sv), in, out); }
+int op_bend_of(ves3d_sv* sv, const double* h, const double* add, double* out) {
+  return op_bend_of(sv, base_space(sv), h, add, out);
+}
+int op_tension(ves3d_sv* sv, const double* sigma, const double* add, double* out) {
+  return op_tension(sv, base_space(sv), sigma, add, out);
+}
+
+// Self part of the single layer for every field vesicle of a batched space (the isolated
+// vesicles' operator; no far field): coefficients, one read of each self matrix for all
+// copies, synthesis.
+int stokes_self_batch(ves3d_sv* sv, const OpSpace& sp, const double* f, double* out) {
+  int s;
+  const DevTables& T = sv->tab->d;
+  const int p0 = sv->p, n = 3 * ncoef_(p0);
+  if (!sv->sl_valid && (s = run_setup(sv))) return s;
+  if ((s = launch_grid2shc(f, sp.nv * 3, p0, T.ana_four, T.ana_leg, T.jf_of_coef, sp.fc, sv->stream))) return s;
+  if ((s = launch_self_gemv_multi(sp.fc, sv->SL, sv->nves, (int)(sp.nv / sv->nves), n, sp.vc, sv->stream)))
+    return s;
+  return launch_synthesis(sp.vc, sp.nv * 3, p0, p0, T.syn0_leg, T.syn0_dleg, T.syn0_four, T.syn0_dfour, T.blk_off, out,
+                          nullptr, nullptr, sv->stream);
 }
 
 // Stokes single layer of a device density f (AxisMajor) -> out (device), through the
@@ -971,11 +1019,6 @@ int stokes_apply(ves3d_sv* sv, const double* f, double* out) {
   const size_t n = (size_t)sv->npts() * 3;
   VES3D_CK(cudaMemcpyAsync(sv->F, f, n * sizeof(double), cudaMemcpyDeviceToDevice, sv->stream));
   sv->have_den = true;
-  if (sv->self_only) {
-    // isolated vesicles: the singular self part alone
-    if (!sv->sl_valid && (s = run_setup(sv))) return s;
-    return run_self(sv, out, sv->den);
-  }
   if ((s = run_eval(sv))) return s;
   VES3D_CK(cudaMemcpyAsync(out, sv->V, n * sizeof(double), cudaMemcpyDeviceToDevice, sv->stream));
   return VES3D_OK;
@@ -1010,39 +1053,49 @@ int implicit_work(ves3d_sv* sv, ImplicitWork& iw) {
   return VES3D_OK;
 }
 
-// [u; sigma] -> [u - S f ; -div S f],  f = linbend(dt u) + tension(sigma)
+// [u; sigma] -> [u - S f ; -div S f],  f = linbend(dt u) + tension(sigma); S is the full
+// single layer, or the self part alone for a batched space (self_batch)
+int implicit_matvec(ves3d_sv* sv, const OpSpace& sp, const ImplicitWork& iw, bool self_batch, const double* x,
+                    double* y) {
+  int s;
+  const long N = sp.nv * ngrid_(sv->p);
+  const double* u = x;
+  const double* sig = x + 3 * N;
+  if ((s = lincomb_f64(3 * N, sv->dt, u, 0.0, u, 0.0, nullptr, iw.y, sv->stream))) return s;  // y = dt u
+  if ((s = op_linH(sv, sp, iw.y, iw.h))) return s;
+  if ((s = op_bend_of(sv, sp, iw.h, nullptr, iw.f))) return s;
+  if ((s = op_tension(sv, sp, sig, iw.f, iw.f))) return s;
+  if ((s = self_batch ? stokes_self_batch(sv, sp, iw.f, iw.Sf) : stokes_apply(sv, iw.f, iw.Sf))) return s;
+  if ((s = lincomb_f64(3 * N, 1.0, u, -1.0, iw.Sf, 0.0, nullptr, y, sv->stream))) return s;
+  return op_div(sv, sp, iw.Sf, y + 3 * N, -1.0);
+}
+
 int implicit_matvec(ves3d_sv* sv, const double* x, double* y) {
   int s;
   ImplicitWork iw;
   if ((s = implicit_work(sv, iw))) return s;
-  const long N = sv->npts();
-  const double* u = x;
-  const double* sig = x + 3 * N;
-  if ((s = lincomb_f64(3 * N, sv->dt, u, 0.0, u, 0.0, nullptr, iw.y, sv->stream))) return s;  // y = dt u
-  if ((s = op_linH(sv, iw.y, iw.h))) return s;
-  if ((s = op_bend_of(sv, iw.h, nullptr, iw.f))) return s;
-  if ((s = op_tension(sv, sig, iw.f, iw.f))) return s;
-  if ((s = stokes_apply(sv, iw.f, iw.Sf))) return s;
-  if ((s = lincomb_f64(3 * N, 1.0, u, -1.0, iw.Sf, 0.0, nullptr, y, sv->stream))) return s;
-  return op_div(sv, iw.Sf, y + 3 * N, -1.0);
+  return implicit_matvec(sv, base_space(sv), iw, false, x, y);
 }
 
 // Galerkin maps: SH coefficients [u (3 nv fun); sigma (nv fun)] <-> grid [u; sigma]
-int coef_to_grid(ves3d_sv* sv, const double* c, double* g) {
-  const long nv = sv->nves, N = sv->npts();
+int coef_to_grid(ves3d_sv* sv, long nv, const double* c, double* g) {
+  const long N = nv * ngrid_(sv->p);
   const long nc = ncoef_(sv->p);
   int s = synth_d(sv, c, 3 * nv, 0, g, nullptr, nullptr);
   if (s) return s;
   return synth_d(sv, c + 3 * nv * nc, nv, 0, g + 3 * N, nullptr, nullptr);
 }
 
-int grid_to_coef(ves3d_sv* sv, const double* g, double* c) {
-  const long nv = sv->nves, N = sv->npts();
+int grid_to_coef(ves3d_sv* sv, long nv, const double* g, double* c) {
+  const long N = nv * ngrid_(sv->p);
   const long nc = ncoef_(sv->p);
   int s = grid2shc_p(sv, g, 3 * nv, c);
   if (s) return s;
   return grid2shc_p(sv, g + 3 * N, nv, c + 3 * nv * nc);
 }
+
+int coef_to_grid(ves3d_sv* sv, const double* c, double* g) { return coef_to_grid(sv, sv->nves, c, g); }
+int grid_to_coef(ves3d_sv* sv, const double* g, double* c) { return grid_to_coef(sv, sv->nves, g, c); }
 
 // ImplicitApply, Galerkin form (src/InterfacialVelocity.cc:982-1052)
 int implicit_matvec_sh(ves3d_sv* sv, const double* c, double* y) {
@@ -1052,6 +1105,16 @@ int implicit_matvec_sh(ves3d_sv* sv, const double* c, double* y) {
   if ((s = coef_to_grid(sv, c, iw.g1))) return s;
   if ((s = implicit_matvec(sv, iw.g1, iw.g2))) return s;
   return grid_to_coef(sv, iw.g2, y);
+}
+
+// The same on a batched space with the self part only (the isolated-vesicle operator,
+// applied to sp.nv / nves coefficient vectors at once)
+int implicit_matvec_sh_self_batch(ves3d_sv* sv, const OpSpace& sp, const ImplicitWork& iw, const double* c,
+                                  double* y) {
+  int s;
+  if ((s = coef_to_grid(sv, sp.nv, c, iw.g1))) return s;
+  if ((s = implicit_matvec(sv, sp, iw, true, iw.g1, iw.g2))) return s;
+  return grid_to_coef(sv, sp.nv, iw.g2, y);
 }
 
 int implicit_rhs(ves3d_sv* sv, double* y) {
@@ -1095,20 +1158,29 @@ __device__ __forceinline__ long sh_global(long v, long i, long nv, int nc) {
   return i < 3 * nc ? v * 3 * nc + i : 3 * nv * nc + v * nc + (i - 3 * nc);
 }
 
-// e = unit vector at local index j of every vesicle
-__global__ void k_unit_columns(double* __restrict__ e, long nv, int nc, int j) {
-  const long v = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (v < nv) e[sh_global(v, j, nv, nc)] = 1.0;
+// Batched assembly: k copies of the suspension, copy q carries the unit vector of column
+// j0 + q of every vesicle (field vesicle q nv + v of a space of k nv vesicles)
+__device__ __forceinline__ long sh_global_b(long w, long i, long NV, int nc) {
+  return i < 3 * nc ? w * 3 * nc + i : 3 * NV * nc + w * nc + (i - 3 * nc);
 }
 
-// A[v] column j (column-major, n = 4 nc) = vesicle v's part of y
-__global__ void k_store_column(const double* __restrict__ y, long nv, int nc, int j, double* __restrict__ A) {
+__global__ void k_unit_columns_batch(double* __restrict__ e, long nv, int k, int nc, int j0, int kq) {
+  const long g = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (long)kq * nv) return;
+  const long q = g / nv, v = g - q * nv;
+  e[sh_global_b(q * nv + v, j0 + q, (long)k * nv, nc)] = 1.0;
+}
+
+__global__ void k_store_columns_batch(const double* __restrict__ y, long nv, int k, int nc, int j0, int kq,
+                                      double* __restrict__ A) {
   const long n = 4L * nc;
-  for (long g = (long)blockIdx.x * blockDim.x + threadIdx.x; g < nv * n; g += (long)gridDim.x * blockDim.x) {
-    const long v = g / n, i = g - v * n;
-    A[v * n * n + (long)j * n + i] = y[sh_global(v, i, nv, nc)];
+  for (long g = (long)blockIdx.x * blockDim.x + threadIdx.x; g < (long)kq * nv * n; g += (long)gridDim.x * blockDim.x) {
+    const long i = g % n, qv = g / n;
+    const long q = qv / nv, v = qv - q * nv;
+    A[v * n * n + (j0 + q) * n + i] = y[sh_global_b(q * nv + v, i, (long)k * nv, nc)];
   }
 }
+
 
 // Constant tension is (up to quadrature error) a null mode of an isolated vesicle: the
 // single layer of 2 H n over a closed surface vanishes. Shift the sigma degree-0 diagonal
@@ -1213,7 +1285,7 @@ int precond_apply(void* ctx, const double* x, double* y) {
 int build_self_block_precond(ves3d_sv* sv) {
   int s;
   const int nc = ncoef_(sv->p), n = 4 * nc;
-  const long nv = sv->nves, nsh = sh_unknowns(sv), nn = (long)n * n;
+  const long nv = sv->nves, nn = (long)n * n;
   if (sv->pc_cap < nv * nn) {
     if (sv->pc_inv) cudaFree(sv->pc_inv);
     sv->pc_inv = nullptr;
@@ -1237,34 +1309,65 @@ int build_self_block_precond(ves3d_sv* sv) {
       }
     }
   }
-  double *A = nullptr, *B = nullptr, *e = nullptr, *y = nullptr;
+  double *A = nullptr, *B = nullptr;
   int *piv = nullptr, *info = nullptr;
   if ((s = dalloc(&A, nv * nn))) return s;
-  if ((s = dalloc(&B, nv * nn)) || (s = dalloc(&e, nsh)) || (s = dalloc(&y, nsh)) ||
-      (s = dalloc(&piv, nv * (long)n)) || (s = dalloc(&info, nv))) {
-    dfree(A); dfree(B); dfree(e); dfree(y); dfree(piv);
+  if ((s = dalloc(&B, nv * nn)) || (s = dalloc(&piv, nv * (long)n)) || (s = dalloc(&info, nv))) {
+    dfree(A); dfree(B); dfree(piv);
     return s;
   }
   VES3D_CK(cudaEventRecord(sv->pc_ev[0], sv->stream));
-  // columns of the isolated-vesicle operator, one per application, all vesicles at once
-  sv->self_only = true;
-  sv->far_force_fp64 = 1;
-  for (int j = 0; j < n && !s; j++) {
-    s = cuda_status(cudaMemsetAsync(e, 0, nsh * sizeof(double), sv->stream), "memset", __FILE__, __LINE__);
+  // columns of the isolated-vesicle operator, kPcBatch per application: kPcBatch copies
+  // of the suspension (geometry and self matrices shared), copy q carrying the unit
+  // vector of column j0 + q of every vesicle; each self matrix is read once per batch
+  {
+    const int K = std::min(kPcBatch, n);
+    const int ng = ngrid_(sv->p);
+    OpSpace sp;
+    sp.nv = (long)K * nv;
+    const long Nv = sp.nv * ng, nshb = 4L * nc * sp.nv;
+    double* bb = nullptr;
+    const size_t need = (size_t)8 * 3 * Nv + 3 * (size_t)3 * nc * sp.nv + 18 * (size_t)Nv + 2 * (size_t)nshb;
+    if (!s) s = dalloc(&bb, need);
     if (!s) {
-      k_unit_columns<<<(unsigned)((nv + 127) / 128), 128, 0, sv->stream>>>(e, nv, nc, j);
-      s = cuda_status(cudaGetLastError(), "k_unit_columns", __FILE__, __LINE__);
-      if (!s) launch_counter()++;
+      double* q = bb;
+      for (int k = 0; k < 8; k++, q += 3 * Nv) sp.w[k] = q;
+      sp.wc = q;
+      q += 3L * nc * sp.nv;
+      sp.fc = q;
+      q += 3L * nc * sp.nv;
+      sp.vc = q;
+      q += 3L * nc * sp.nv;
+      ImplicitWork bw;
+      bw.f = q;
+      bw.Sf = q + 3 * Nv;
+      bw.h = q + 6 * Nv;
+      bw.y = q + 7 * Nv;
+      bw.g1 = q + 10 * Nv;
+      bw.g2 = q + 14 * Nv;
+      q += 18 * Nv;
+      double* eb = q;
+      double* yb = q + nshb;
+      for (int j0 = 0; j0 < n && !s; j0 += K) {
+        const int kq = std::min(K, n - j0);
+        s = cuda_status(cudaMemsetAsync(eb, 0, nshb * sizeof(double), sv->stream), "memset", __FILE__, __LINE__);
+        if (!s) {
+          k_unit_columns_batch<<<grid_1d((long)kq * nv), 256, 0, sv->stream>>>(eb, nv, K, nc, j0, kq);
+          s = cuda_status(cudaGetLastError(), "k_unit_columns_batch", __FILE__, __LINE__);
+          if (!s) launch_counter()++;
+        }
+        if (!s) s = implicit_matvec_sh_self_batch(sv, sp, bw, eb, yb);
+        if (!s) {
+          k_store_columns_batch<<<grid_1d((long)kq * nv * n), 256, 0, sv->stream>>>(yb, nv, K, nc, j0, kq, A);
+          s = cuda_status(cudaGetLastError(), "k_store_columns_batch", __FILE__, __LINE__);
+          if (!s) launch_counter()++;
+        }
+      }
     }
-    if (!s) s = implicit_matvec_sh(sv, e, y);
-    if (!s) {
-      k_store_column<<<grid_1d(nv * n), 256, 0, sv->stream>>>(y, nv, nc, j, A);
-      s = cuda_status(cudaGetLastError(), "k_store_column", __FILE__, __LINE__);
-      if (!s) launch_counter()++;
-    }
+    // the batch buffers are released after the stream's work (the factorisation follows)
+    cudaStreamSynchronize(sv->stream);
+    dfree(bb);
   }
-  sv->self_only = false;
-  sv->far_force_fp64 = 0;
   if (!s) {
     k_shift_null_mode<<<(unsigned)((nv + 127) / 128), 128, 0, sv->stream>>>(A, nv, nc);
     s = cuda_status(cudaGetLastError(), "k_shift_null_mode", __FILE__, __LINE__);
@@ -1332,8 +1435,6 @@ int build_self_block_precond(ves3d_sv* sv) {
   }
   dfree(A);
   dfree(B);
-  dfree(e);
-  dfree(y);
   dfree(work);
   dfree(piv);
   dfree(info);
