@@ -16,6 +16,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <vector>
 
 #include <cusolverDn.h>
@@ -164,7 +165,6 @@ struct ves3d_sv {
   int pc_age = 0;              // surface updates since the last build
   long pc_nves = 0;            // vesicle count the preconditioner was built for
   double pc_ms[3] = {0, 0, 0};  // last build: total, assembly, factorisation (device ms)
-  cudaStream_t pc_stream[kPcStreams] = {};
   // CUDA graph of the resident evaluation (density buffer -> velocity buffer)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
@@ -174,7 +174,6 @@ struct ves3d_sv {
     graph_exec = nullptr;
     graph = nullptr;
   }
-  cusolverDnHandle_t pc_solver[kPcStreams] = {};
   cudaEvent_t pc_ev[3 + kPcStreams] = {};
   cudaEvent_t ev[8] = {};
   float ms[4] = {0, 0, 0, 0};
@@ -182,10 +181,6 @@ struct ves3d_sv {
   ~ves3d_sv() {
     drop_graph();
     free_precond();
-    for (auto& h : pc_solver)
-      if (h) cusolverDnDestroy(h);
-    for (auto& q : pc_stream)
-      if (q) cudaStreamDestroy(q);
     for (auto& e : pc_ev)
       if (e) cudaEventDestroy(e);
     free_implicit();
@@ -1282,6 +1277,25 @@ int precond_apply(void* ctx, const double* x, double* y) {
 // pivoting (cuSOLVER getrf) and solves against the identity (getrs) in FP64, stored in
 // FP32 -- the preconditioner only steers the iteration; the tests on the true residual
 // fix the accuracy of the solution.
+// Streams and cuSOLVER handles of the preconditioner factorisation: one process-wide set
+// per device, created on first use and kept until exit (creating 32 handles costs ~0.1 s,
+// which every new operator context would otherwise pay); a mutex serialises their use.
+struct SolverPool {
+  std::mutex mu;
+  bool ready = false;
+  cudaStream_t st[kPcStreams] = {};
+  cusolverDnHandle_t h[kPcStreams] = {};
+};
+
+SolverPool& solver_pool(int device) {
+  static SolverPool* pools[64] = {};
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lk(mu);
+  SolverPool*& p = pools[(unsigned)device % 64];
+  if (!p) p = new SolverPool();  // intentionally never freed: handles live until exit
+  return *p;
+}
+
 int build_self_block_precond(ves3d_sv* sv) {
   int s;
   const int nc = ncoef_(sv->p), n = 4 * nc;
@@ -1295,20 +1309,27 @@ int build_self_block_precond(ves3d_sv* sv) {
   }
   if (!sv->pc_ev[0])
     for (auto& ev : sv->pc_ev) VES3D_CK(cudaEventCreate(&ev));
-  for (int k = 0; k < kPcStreams; k++) {
-    if (!sv->pc_stream[k]) VES3D_CK(cudaStreamCreateWithFlags(&sv->pc_stream[k], cudaStreamNonBlocking));
-    if (!sv->pc_solver[k]) {
-      if (cusolverDnCreate(&sv->pc_solver[k]) != CUSOLVER_STATUS_SUCCESS) {
-        sv->pc_solver[k] = nullptr;
-        set_error("cusolverDnCreate failed");
-        return VES3D_ERR_CUDA;
-      }
-      if (cusolverDnSetStream(sv->pc_solver[k], sv->pc_stream[k]) != CUSOLVER_STATUS_SUCCESS) {
-        set_error("cusolverDnSetStream failed");
-        return VES3D_ERR_CUDA;
+  SolverPool& pool = solver_pool(sv->device);
+  std::lock_guard<std::mutex> pool_lock(pool.mu);
+  if (!pool.ready) {
+    for (int k = 0; k < kPcStreams; k++) {
+      if (!pool.st[k]) VES3D_CK(cudaStreamCreateWithFlags(&pool.st[k], cudaStreamNonBlocking));
+      if (!pool.h[k]) {
+        if (cusolverDnCreate(&pool.h[k]) != CUSOLVER_STATUS_SUCCESS) {
+          pool.h[k] = nullptr;
+          set_error("cusolverDnCreate failed");
+          return VES3D_ERR_CUDA;
+        }
+        if (cusolverDnSetStream(pool.h[k], pool.st[k]) != CUSOLVER_STATUS_SUCCESS) {
+          set_error("cusolverDnSetStream failed");
+          return VES3D_ERR_CUDA;
+        }
       }
     }
+    pool.ready = true;
   }
+  cudaStream_t* pc_stream = pool.st;
+  cusolverDnHandle_t* pc_solver = pool.h;
   double *A = nullptr, *B = nullptr;
   int *piv = nullptr, *info = nullptr;
   if ((s = dalloc(&A, nv * nn))) return s;
@@ -1379,7 +1400,7 @@ int build_self_block_precond(ves3d_sv* sv) {
     if (!s) launch_counter()++;
   }
   int lwork = 0;
-  if (!s && cusolverDnDgetrf_bufferSize(sv->pc_solver[0], n, n, A, n, &lwork) != CUSOLVER_STATUS_SUCCESS) {
+  if (!s && cusolverDnDgetrf_bufferSize(pc_solver[0], n, n, A, n, &lwork) != CUSOLVER_STATUS_SUCCESS) {
     set_error("cusolverDnDgetrf_bufferSize failed");
     s = VES3D_ERR_CUDA;
   }
@@ -1390,12 +1411,12 @@ int build_self_block_precond(ves3d_sv* sv) {
   // (one factorisation of n ~ 10^3 is latency-bound and does not fill the GPU)
   if (!s) s = cuda_status(cudaEventRecord(sv->pc_ev[1], sv->stream), "event", __FILE__, __LINE__);
   for (int k = 0; k < kPcStreams && !s; k++)
-    s = cuda_status(cudaStreamWaitEvent(sv->pc_stream[k], sv->pc_ev[1], 0), "wait", __FILE__, __LINE__);
+    s = cuda_status(cudaStreamWaitEvent(pc_stream[k], sv->pc_ev[1], 0), "wait", __FILE__, __LINE__);
   for (long v = 0; v < nv && !s; v++) {
     const int k = (int)(v % kPcStreams);
-    if (cusolverDnDgetrf(sv->pc_solver[k], n, n, A + v * nn, n, work + (long)k * lwork, piv + v * n, info + v) !=
+    if (cusolverDnDgetrf(pc_solver[k], n, n, A + v * nn, n, work + (long)k * lwork, piv + v * n, info + v) !=
             CUSOLVER_STATUS_SUCCESS ||
-        cusolverDnDgetrs(sv->pc_solver[k], CUBLAS_OP_N, n, n, A + v * nn, n, piv + v * n, B + v * nn, n, info + v) !=
+        cusolverDnDgetrs(pc_solver[k], CUBLAS_OP_N, n, n, A + v * nn, n, piv + v * n, B + v * nn, n, info + v) !=
             CUSOLVER_STATUS_SUCCESS) {
       set_error("cuSOLVER getrf/getrs failed for vesicle %ld", v);
       s = VES3D_ERR_CUDA;
@@ -1403,7 +1424,7 @@ int build_self_block_precond(ves3d_sv* sv) {
   }
   // join (also after an error, so nothing is left running on the side streams)
   for (int k = 0; k < kPcStreams; k++) {
-    cudaEventRecord(sv->pc_ev[3 + k], sv->pc_stream[k]);
+    cudaEventRecord(sv->pc_ev[3 + k], pc_stream[k]);
     cudaStreamWaitEvent(sv->stream, sv->pc_ev[3 + k], 0);
   }
   if (!s) {
