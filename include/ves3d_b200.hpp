@@ -1,0 +1,163 @@
+/* ves3d_b200.hpp -- header-only C++ mirror of the reference's operator API over the C ABI
+ * of ves3d_b200.h, for dropping the B200 path into Ves3D's C++ code. It compiles as C++03
+ * (the reference's dialect: -std=gnu++03) and needs no CUDA headers.
+ *
+ *   reference (lu1and10/ves3d)                              here
+ *   StokesVelocity<Real> (include/StokesVelocity.h:9-44)     ves3d_b200::StokesVelocity<double>
+ *   SHTrans<Container, Mats> (include/SHTrans.h:21-63)       ves3d_b200::SHTrans<double>
+ *   Device<GPU>::DirectStokes (include/Device.h:205-209)     ves3d_b200::DirectStokes
+ *   InterfacialVelocity implicit solve (src/InterfacialVelocity.cc:203-1172)
+ *                                                            StokesVelocity::ImplicitSolve
+ *
+ * Containers: any type with operator[] and size() holding doubles contiguously (std::vector,
+ * the reference's Array-based containers through their begin()/size() via the pointer
+ * overloads). Failures throw ves3d_b200::Error carrying the C ABI status and message.
+ */
+#ifndef VES3D_B200_HPP
+#define VES3D_B200_HPP
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "ves3d_b200.h"
+
+namespace ves3d_b200 {
+
+class Error : public std::runtime_error {
+ public:
+  Error(int status, const std::string& what) : std::runtime_error(what), status_(status) {}
+  int status() const { return status_; }
+
+ private:
+  int status_;
+};
+
+inline void check(int status, const char* what) {
+  if (status != VES3D_OK) {
+    const char* msg = ves3d_last_error();
+    throw Error(status, std::string(what) + ": " + (msg ? msg : ""));
+  }
+}
+
+/* StokesVelocity<Real>: single-layer velocity of a suspension at its own surface points
+ * (surfaces and densities AxisMajor [n_ves][3][(p+1) 2p], as the reference's containers).
+ * The far field is the exact all-pairs sum (the reference's PVFMM is not used); box_size and
+ * repul_dist are accepted for signature compatibility, repulsion is not supported. */
+template <class Real>
+class StokesVelocity {
+ public:
+  StokesVelocity(int sh_order, int sh_order_up, Real box_size = -1, Real repul_dist = 1e-3,
+                 int precision = VES3D_PREC_FP64, int device = -1)
+      : sv_(0), p_(sh_order), nv_(0) {
+    (void)box_size;
+    (void)repul_dist;
+    check(ves3d_sv_create(sh_order, sh_order_up, precision, device, &sv_), "StokesVelocity");
+  }
+  ~StokesVelocity() { ves3d_sv_destroy(sv_); }
+
+  /* SetSrcCoord(S, sh_order_up_self, sh_order_up): the upsample orders are fixed at
+   * construction; passing different ones is an error. */
+  void SetSrcCoord(const Real* S, size_t n, int sh_order_up_self = -1, int sh_order_up = -1,
+                   bool on_device = false) {
+    (void)sh_order_up_self;
+    (void)sh_order_up;
+    const size_t per = 3 * (size_t)2 * p_ * (p_ + 1);
+    if (n == 0 || n % per) throw Error(VES3D_ERR_ARG, "SetSrcCoord: size is not a multiple of 3 (p+1) 2p");
+    nv_ = (long)(n / per);
+    check(ves3d_sv_set_src_coord(sv_, S, nv_, on_device ? 1 : 0), "SetSrcCoord");
+  }
+  template <class Vec>
+  void SetSrcCoord(const Vec& S, int sh_order_up_self = -1, int sh_order_up = -1) {
+    SetSrcCoord(&S[0], S.size(), sh_order_up_self, sh_order_up);
+  }
+
+  void SetDensitySL(const Real* f, bool add_repul = false, bool on_device = false) {
+    if (add_repul) throw Error(VES3D_ERR_ARG, "SetDensitySL: repulsion is not supported");
+    check(ves3d_sv_set_density_sl(sv_, f, on_device ? 1 : 0), "SetDensitySL");
+  }
+  template <class Vec>
+  void SetDensitySL(const Vec* force_single, bool add_repul = false) {
+    SetDensitySL(&(*force_single)[0], add_repul);
+  }
+
+  /* operator()(vel): velocity into a caller container of the surfaces' size. */
+  void operator()(Real* vel, bool on_device = false) { check(ves3d_sv_eval(sv_, vel, on_device ? 1 : 0), "eval"); }
+  template <class Vec>
+  void operator()(Vec& vel) {
+    operator()(&vel[0]);
+  }
+  /* operator()(): velocity in an internal host vector. */
+  const std::vector<Real>& operator()() {
+    vel_.resize((size_t)nv_ * 3 * 2 * p_ * (p_ + 1));
+    operator()(&vel_[0]);
+    return vel_;
+  }
+
+  /* The globally implicit step on the current surfaces (Galerkin form, BiCGStab):
+   * x0 (may be NULL: zero guess) and x are grid fields [u; sigma] of 4 N doubles. Returns
+   * the BiCGSReturn code (100 success); tol and max_iter are in/out as in BiCGStab. */
+  void SetImplicitParams(Real dt, Real bending_modulus, Real shear_rate) {
+    check(ves3d_sv_set_implicit_params(sv_, dt, bending_modulus, shear_rate), "SetImplicitParams");
+  }
+  void SetPrecond(int scheme, int refresh_every = 1) {
+    check(ves3d_sv_set_precond(sv_, scheme), "SetPrecond");
+    check(ves3d_sv_set_precond_refresh(sv_, refresh_every), "SetPrecond");
+  }
+  int ImplicitSolve(const Real* x0, Real* x, Real& tol, int& max_iter, bool on_device = false) {
+    int code = 0;
+    double t = tol;
+    check(ves3d_sv_implicit_solve(sv_, x0, x, &t, &max_iter, &code, on_device ? 1 : 0), "ImplicitSolve");
+    tol = t;
+    return code;
+  }
+
+  long NumVesicles() const { return nv_; }
+  ves3d_sv* handle() { return sv_; }
+
+ private:
+  StokesVelocity(const StokesVelocity&);
+  StokesVelocity& operator=(const StokesVelocity&);
+  ves3d_sv* sv_;
+  int p_;
+  long nv_;
+  std::vector<Real> vel_;
+};
+
+/* SHTrans<Real> on device pointers (forward = Grid2SHC, backward = SHC2Grid with the
+ * optional longitude / latitude derivatives of backward_dv / backward_du), in the
+ * coefficient order shared by the reference's SHTrans and SphericalHarmonics. */
+template <class Real>
+class SHTrans {
+ public:
+  explicit SHTrans(int sh_order, void* stream = 0) : p_(sh_order), stream_(stream) {}
+  int getShOrder() const { return p_; }
+  void forward(const Real* in, long n_funs, Real* shc) const {
+    check(ves3d_sht_forward(in, n_funs, p_, p_, shc, stream_), "SHTrans::forward");
+  }
+  void backward(const Real* shc, long n_funs, Real* out, Real* d_longitude = 0, Real* d_latitude = 0) const {
+    check(ves3d_sht_backward(shc, n_funs, p_, p_, out, d_longitude, d_latitude, stream_), "SHTrans::backward");
+  }
+  /* resampling p -> q (SHC2Grid(p, q)) */
+  void backward_to(int q, const Real* shc, long n_funs, Real* out) const {
+    check(ves3d_sht_backward(shc, n_funs, p_, q, out, 0, 0, stream_), "SHTrans::backward_to");
+  }
+
+ private:
+  int p_;
+  void* stream_;
+};
+
+/* Device<GPU>::DirectStokes(src, den, qw, src_stride, trg_stride, n_surfs, trg,
+ * trg_idx_head, trg_idx_tail, pot) on device pointers (cuda_stokes). */
+inline void DirectStokes(const double* src, const double* den, const double* qw, size_t src_stride,
+                         size_t trg_stride, size_t n_surfs, const double* trg, size_t trg_idx_head,
+                         size_t trg_idx_tail, double* pot, void* stream = 0) {
+  check(ves3d_cuda_stokes_f64((int)src_stride, (int)trg_stride, (int)n_surfs, (int)trg_idx_head, (int)trg_idx_tail,
+                              trg, src, den, pot, qw, stream),
+        "DirectStokes");
+}
+
+}  // namespace ves3d_b200
+
+#endif /* VES3D_B200_HPP */

@@ -1,0 +1,53 @@
+// C++ caller of the B200 path through include/ves3d_b200.hpp, written the way Ves3D's
+// C++ code uses StokesVelocity<Real> (SetSrcCoord / SetDensitySL / operator()).
+//   api_test --version            prints the library version (no GPU needed)
+//   api_test <in.bin> <out.bin>   in: int32 p, int32 n_ves, X[n], f[n] (doubles, AxisMajor);
+//                                 out: vel[n] then the implicit solution x[4 n / 3]
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "ves3d_b200.hpp"
+
+int main(int argc, char** argv) {
+  if (argc == 2 && std::strcmp(argv[1], "--version") == 0) {
+    std::printf("%d\n", ves3d_version());
+    return 0;
+  }
+  if (argc != 3) {
+    std::fprintf(stderr, "usage: api_test --version | api_test in.bin out.bin\n");
+    return 2;
+  }
+  std::FILE* fi = std::fopen(argv[1], "rb");
+  if (!fi) return 3;
+  int hdr[2];
+  if (std::fread(hdr, sizeof(int), 2, fi) != 2) return 3;
+  const int p = hdr[0], nv = hdr[1];
+  const size_t n = (size_t)nv * 3 * 2 * p * (p + 1);
+  std::vector<double> X(n), f(n), vel(n), x(4 * n / 3);
+  if (std::fread(&X[0], sizeof(double), n, fi) != n || std::fread(&f[0], sizeof(double), n, fi) != n) return 3;
+  std::fclose(fi);
+  try {
+    ves3d_b200::StokesVelocity<double> stokes(p, 2 * p);
+    stokes.SetSrcCoord(X);
+    stokes.SetDensitySL(&f);
+    stokes(vel);
+    // the reference's implicit step on the same surfaces, self-block preconditioned
+    stokes.SetImplicitParams(0.01, 0.05, 1.0);
+    stokes.SetPrecond(VES3D_PRECOND_SELF_BLOCK);
+    double tol = 1e-9;
+    int iters = 500;
+    const int code = stokes.ImplicitSolve(0, &x[0], tol, iters);
+    std::fprintf(stderr, "implicit: code %d, %d iterations, relres %.3e\n", code, iters, tol);
+    if (code != 100) return 4;
+  } catch (const ves3d_b200::Error& e) {
+    std::fprintf(stderr, "error %d: %s\n", e.status(), e.what());
+    return 5;
+  }
+  std::FILE* fo = std::fopen(argv[2], "wb");
+  if (!fo) return 3;
+  std::fwrite(&vel[0], sizeof(double), n, fo);
+  std::fwrite(&x[0], sizeof(double), x.size(), fo);
+  std::fclose(fo);
+  return 0;
+}
