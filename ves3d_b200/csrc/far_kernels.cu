@@ -30,8 +30,8 @@
 
 namespace ves3d {
 
-constexpr int kTileF64 = 128;
-constexpr int kTileF32 = 256;
+constexpr int kTileF64 = 256;
+constexpr int kTileF32 = 512;
 
 // Source sub-ranges of tile [s0, s0 + ns) that lie outside the excluded range [e0, e1).
 __device__ __forceinline__ void split_tile(long s0, int ns, long e0, long e1, int& a0, int& a1, int& b0, int& b1) {
