@@ -131,6 +131,12 @@ int ves3d_svp_setup(ves3d_svp* g);
 int ves3d_svp_eval(ves3d_svp* g, double* vel, int is_device);
 /* ms[0] self-matrix builds, ms[1] self parts, ms[2] far field, ms[3] whole last eval. */
 int ves3d_svp_stage_times(ves3d_svp* g, float* ms);
+/* The evaluation (self parts of every order group + the one far-field pass) recorded as a
+ * CUDA graph on the context's stream (builds the self matrices and runs one eager pass
+ * first); relaunch after ves3d_svp_set_density_sl with new densities. vel (may be NULL)
+ * receives the velocity; invalidated by ves3d_svp_set_src_coord. */
+int ves3d_svp_capture_eval(ves3d_svp* g);
+int ves3d_svp_launch_eval_graph(ves3d_svp* g, double* vel, int is_device);
 
 /* ---------------------------------------------------------------------------
  * Surface geometry, tractions and the globally implicit step on the context's surfaces

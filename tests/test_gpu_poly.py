@@ -42,3 +42,22 @@ def test_polydisperse_matches_uniform_operator():
         b.SetDensitySL(f)
         w = b()
     assert rel_err(w, u) < 1e-14
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_polydisperse_graph_matches_eager(poly_case, prec):
+    """The captured polydisperse evaluation, relaunched on new densities, equals the eager
+    evaluation bitwise (fixed-order reductions) and stays on the oracle."""
+    X, f, orders = poly_case
+    rng = np.random.default_rng(9)
+    with PolydisperseStokesVelocity(prec) as sv:
+        sv.SetSrcCoord(X, orders)
+        sv.SetDensitySL(f)
+        sv.capture_eval()
+        for _ in range(2):
+            g = rng.standard_normal(X.size)
+            sv.SetDensitySL(g)
+            vg = sv.launch_eval_graph()
+            ve = sv()
+            assert np.array_equal(vg, ve)
+    assert rel_err(ve, stokes.stokes_velocity_poly(X, g, orders)) < (1e-12 if prec == "fp64" else 1e-6)

@@ -2039,6 +2039,14 @@ struct ves3d_svp {
   bool have_den = false;
   cudaEvent_t ev[4] = {};
   float ms[4] = {0, 0, 0, 0};
+  cudaGraph_t graph = nullptr;  // captured evaluation (self parts of every group + far field)
+  cudaGraphExec_t graph_exec = nullptr;
+  void drop_graph() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph) cudaGraphDestroy(graph);
+    graph_exec = nullptr;
+    graph = nullptr;
+  }
   void free_global() {
     double* ps[] = {pos, den, vself, V, Vfar, part};
     for (double* q : ps) dfree(q);
@@ -2053,6 +2061,7 @@ struct ves3d_svp {
     gp.clear();
   }
   ~ves3d_svp() {
+    drop_graph();
     free_groups();
     free_global();
     for (auto& e : ev)
@@ -2093,6 +2102,7 @@ int ves3d_svp_destroy(ves3d_svp* g) {
 }
 
 int ves3d_svp_set_src_coord(ves3d_svp* g, const double* S, const int* orders, long n_ves, int is_device) {
+  if (g) g->drop_graph();
   VES3D_ARG(g && S && orders && n_ves >= 1, "bad arguments");
   VES3D_CK(cudaSetDevice(g->device));
   // runs of equal order
@@ -2187,6 +2197,71 @@ int ves3d_svp_setup(ves3d_svp* g) {
   return VES3D_OK;
 }
 
+static int svp_self_parts(ves3d_svp* g) {
+  for (size_t r = 0; r < g->grp.size(); r++) {
+    const int s = run_self(g->grp[r], g->vself + 3 * g->gpt0[r], g->den + 3 * g->gpt0[r]);
+    if (s) return s;
+  }
+  return VES3D_OK;
+}
+
+// one far-field pass over every point, launched per order group (block shape per group)
+static int svp_far(ves3d_svp* g) {
+  const bool mixed = g->prec == VES3D_PREC_MIXED;
+  std::vector<FarGroup> fg;
+  long v0 = 0;
+  for (size_t r = 0; r < g->grp.size(); r++) {
+    fg.push_back(FarGroup{v0, g->gnv[r], ngrid_(g->gp[r])});
+    v0 += g->gnv[r];
+  }
+  return launch_far_groups(mixed, g->pos, g->den, g->off, g->nves, g->N, fg.data(), (int)fg.size(), g->vself, g->V,
+                           g->Vfar, g->part, kFarMaxSegments, g->stream);
+}
+
+int ves3d_svp_capture_eval(ves3d_svp* g) {
+  VES3D_ARG(g != nullptr, "null context");
+  if (g->grp.empty() || !g->have_den) {
+    set_error("capture before set_src_coord / set_density_sl");
+    return VES3D_ERR_STATE;
+  }
+  VES3D_CK(cudaSetDevice(g->device));
+  g->drop_graph();
+  int s;
+  if ((s = ves3d_svp_setup(g))) return s;
+  // one eager pass first: kernel attributes are set outside the capture
+  if ((s = svp_self_parts(g)) || (s = svp_far(g))) return s;
+  VES3D_CK(cudaStreamSynchronize(g->stream));
+  VES3D_CK(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal));
+  s = svp_self_parts(g);
+  if (!s) s = svp_far(g);
+  cudaGraph_t gr = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(g->stream, &gr);
+  if (!s && e != cudaSuccess) s = cuda_status(e, "cudaStreamEndCapture", __FILE__, __LINE__);
+  if (s) {
+    if (gr) cudaGraphDestroy(gr);
+    return s;
+  }
+  g->graph = gr;
+  const cudaError_t ei = cudaGraphInstantiate(&g->graph_exec, gr, 0);
+  if (ei != cudaSuccess) {
+    g->drop_graph();
+    return cuda_status(ei, "cudaGraphInstantiate", __FILE__, __LINE__);
+  }
+  return VES3D_OK;
+}
+
+int ves3d_svp_launch_eval_graph(ves3d_svp* g, double* vel, int is_device) {
+  VES3D_ARG(g != nullptr, "null context");
+  if (!g->graph_exec) {
+    set_error("no captured evaluation (call ves3d_svp_capture_eval after setting surfaces and densities)");
+    return VES3D_ERR_STATE;
+  }
+  VES3D_CK(cudaSetDevice(g->device));
+  VES3D_CK(cudaGraphLaunch(g->graph_exec, g->stream));
+  VES3D_LAUNCHED();
+  return vel ? copy_out(vel, g->V, 3 * (size_t)g->N, is_device, g->stream) : VES3D_OK;
+}
+
 int ves3d_svp_eval(ves3d_svp* g, double* vel, int is_device) {
   VES3D_ARG(g && vel, "null argument");
   if (g->grp.empty() || !g->have_den) {
@@ -2198,19 +2273,9 @@ int ves3d_svp_eval(ves3d_svp* g, double* vel, int is_device) {
   VES3D_CK(cudaEventRecord(g->ev[0], g->stream));
   if ((s = ves3d_svp_setup(g))) return s;
   VES3D_CK(cudaEventRecord(g->ev[1], g->stream));
-  for (size_t r = 0; r < g->grp.size(); r++)
-    if ((s = run_self(g->grp[r], g->vself + 3 * g->gpt0[r], g->den + 3 * g->gpt0[r]))) return s;
+  if ((s = svp_self_parts(g))) return s;
   VES3D_CK(cudaEventRecord(g->ev[2], g->stream));
-  const bool mixed = g->prec == VES3D_PREC_MIXED;
-  std::vector<FarGroup> fg;
-  long v0 = 0;
-  for (size_t r = 0; r < g->grp.size(); r++) {
-    fg.push_back(FarGroup{v0, g->gnv[r], ngrid_(g->gp[r])});
-    v0 += g->gnv[r];
-  }
-  if ((s = launch_far_groups(mixed, g->pos, g->den, g->off, g->nves, g->N, fg.data(), (int)fg.size(), g->vself, g->V,
-                             g->Vfar, g->part, kFarMaxSegments, g->stream)))
-    return s;
+  if ((s = svp_far(g))) return s;
   VES3D_CK(cudaEventRecord(g->ev[3], g->stream));
   VES3D_CK(cudaEventSynchronize(g->ev[3]));
   VES3D_CK(cudaEventElapsedTime(&g->ms[0], g->ev[0], g->ev[1]));

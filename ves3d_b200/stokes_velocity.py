@@ -306,6 +306,18 @@ class PolydisperseStokesVelocity:
         check(lib().ves3d_svp_eval(self._h, p, dev), "StokesVelocity()")
         return out
 
+    def capture_eval(self):
+        """Record the evaluation (self parts + far field) as a CUDA graph."""
+        check(lib().ves3d_svp_capture_eval(self._h), "capture_eval")
+
+    def launch_eval_graph(self, out=None):
+        """Relaunch the captured evaluation (after SetDensitySL with new densities)."""
+        if out is None:
+            out = np.empty(3 * self.npoints())
+        p, dev, n = _ptr(out)
+        check(lib().ves3d_svp_launch_eval_graph(self._h, p, dev), "launch_eval_graph")
+        return out
+
     def stage_times(self):
         ms = (ctypes.c_float * 4)()
         check(lib().ves3d_svp_stage_times(self._h, ms), "stage_times")
