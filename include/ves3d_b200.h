@@ -146,7 +146,7 @@ int ves3d_svp_launch_eval_graph(ves3d_svp* g, double* vel, int is_device);
  * [n_ves][3][Ngrid]; the implicit unknown is [u (vector) ; sigma (scalar)].
  * ------------------------------------------------------------------------- */
 enum ves3d_surface_op {
-  VES3D_OP_GEOMETRY = 0,     /* out [n_ves][15][Ngrid]: E,F,G (/W^2), W, n, cu, cv, H, K   */
+  VES3D_OP_GEOMETRY = 0,     /* out [n_ves][15][Ngrid]: E,F,G (/W^2), W, n (outward), cu, cv, H, K (sphere of radius R: H = -1/R) */
   VES3D_OP_GRAD = 1,         /* scalar -> vector: surface gradient                         */
   VES3D_OP_DIV = 2,          /* vector -> scalar: surface divergence                       */
   VES3D_OP_LIN_MEANCURV = 3, /* vector -> scalar: linearised mean curvature                */
@@ -154,17 +154,21 @@ enum ves3d_surface_op {
   VES3D_OP_BENDING = 5,      /* (in unused) -> vector: bending traction of the surfaces    */
   VES3D_OP_TENSION = 6,      /* scalar -> vector: tension traction 2 sigma H n + grad sigma */
   VES3D_OP_IMPLICIT_MATVEC = 7, /* [u;sigma] -> [u - S f ; -div S f], f = linbend(dt u) + tension(sigma) */
-  VES3D_OP_IMPLICIT_RHS = 8     /* (in unused) -> [u_inf + S f_b ; div(u_inf + S f_b)]       */
+  VES3D_OP_IMPLICIT_RHS = 8,    /* (in unused) -> [u_inf + S f_b ; div(u_inf + S f_b)]       */
+  VES3D_OP_GRAVITY = 9          /* vector -> vector: excess_density (g . x) n                 */
 };
 /* Surface integrals per vesicle (Surface::area / volume / getCenters, src/Surface.cc:378-440,
  * with GaussLegendreIntegrator weights, src/GLIntegrator.cc:33-80): area[n_ves],
- * volume[n_ves], centers[n_ves][3]; any may be NULL. The normal convention is that of
- * Surface::updateFirstForms (x_u x x_v / W), which points inward on this grid, so volumes
- * come out negative for the reference's parametrisation (its tests compare magnitudes). */
+ * volume[n_ves], centers[n_ves][3]; any may be NULL. The normal is that of
+ * Surface::updateFirstForms (x_theta x x_phi / W, outward), so volumes are positive. */
 int ves3d_sv_integrals(ves3d_sv* sv, double* area, double* volume, double* centers, int is_device);
 /* Parameters of the implicit step: time step, bending modulus, shear rate of the
  * background flow u = (rate * y, 0, 0). */
 int ves3d_sv_set_implicit_params(ves3d_sv* sv, double dt, double kappa, double shear_rate);
+/* Gravity (InterfacialForce::gravityForce, src/InterfacialForce.cc:127-184): the traction
+ * excess_density (g . x) n enters the explicit jump with x = the positions and the
+ * linearised jump with x = dt u. Default excess_density 0 (off), g = (0, 0, -1). */
+int ves3d_sv_set_gravity(ves3d_sv* sv, double excess_density, double gx, double gy, double gz);
 int ves3d_sv_surface_op(ves3d_sv* sv, int op, const double* in, double* out, int is_device);
 /* Solve the implicit system with BiCGStab in its Galerkin form (unknowns: SH coefficients
  * of u and sigma, ImplicitApply src/InterfacialVelocity.cc:982-1052; the reference's

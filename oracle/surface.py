@@ -8,6 +8,7 @@ Formulas follow (reference file:line):
   surface gradient / divergence                Surface::grad / div         src/Surface.cc:325-379
   linearised mean curvature                    Surface::linearizedMeanCurv src/Surface.cc:530-569
   bending, linear bending, tension forces      InterfacialForce            src/InterfacialForce.cc:21-125
+  gravity traction (explicit and linearised)   InterfacialForce::gravityForce src/InterfacialForce.cc:127-184
   area, volume, centres                        Surface::area/volume/getCenters src/Surface.cc:378-440
   surface quadrature                           GaussLegendreIntegrator     src/GLIntegrator.cc:33-80
   implicit matvec (solve for velocity)         ImplicitMatvecPhysical      src/InterfacialVelocity.cc:922-979
@@ -16,9 +17,13 @@ Formulas follow (reference file:line):
 Derivatives come from the SphericalHarmonics tables of oracle/sh.py: u is the latitude
 direction (the Legendre derivative), v the longitude direction (the Fourier derivative),
 as SHTrans::FirstDerivatives / backward_du / backward_dv use them (src/SHTrans.cc:133-170).
+  low-pass filter (opt-in, filter_freq)        SHTrans::lowPassFilter      src/SHTrans.cc:8-32, :172-180
 Deliberate differences from the reference (the GPU path makes the same choices): forces
-are evaluated at order p (the reference upsamples to params.upsample_freq), and no
-low-pass filter is applied to curvatures, gradients and divergences.
+are evaluated at order p (the reference upsamples to params.upsample_freq), and by default
+no low-pass filter is applied to curvatures, gradients and divergences. geometry(X, p,
+filter_freq=f) turns the reference's filter on (coefficients of degree above f zeroed, the
+reference's default f = 2p/3) for H, K, grad, div and the linearised curvature, which is
+how the reference's own known answers for them are reproduced.
 """
 import numpy as np
 
@@ -81,8 +86,25 @@ def integrals(X, p):
     return area, vol, cen
 
 
-def geometry(X, p):
-    """Per point: normalised E, F, G (divided by W^2), W, normal, cu, cv, H, K."""
+def lowpass(f, p, freq):
+    """Zero the coefficients of degree > freq of scalar fields f [..][ng]
+    (SHTrans::lowPassFilter with filter_coeff_, src/SHTrans.cc:22-29, :172-180)."""
+    if freq is None:
+        return f
+    shape = np.shape(f)
+    S = sh.grid2shc(np.reshape(f, -1), p, p).reshape(-1, sh.ncoef(p))
+    off = sh.block_offsets(p)
+    for jf in range(2 * p):
+        m = (jf + 1) // 2
+        deg = m + np.arange(off[jf + 1] - off[jf])
+        S[:, off[jf]:off[jf + 1]][:, deg > freq] = 0.0
+    return sh.shc2grid(S.reshape(-1), p, p).reshape(shape)
+
+
+def geometry(X, p, filter_freq=None):
+    """Per point: normalised E, F, G (divided by W^2), W, normal, cu, cv, H, K. With
+    filter_freq set, H, K and the derived operators of this geometry are low-pass filtered
+    as the reference's Surface does."""
     ng = sh.ngrid(p)
     X = np.asarray(X, dtype=np.float64).reshape(-1, 3, ng)
     nv = X.shape[0]
@@ -94,16 +116,19 @@ def geometry(X, p):
     G = (xv * xv).sum(1)
     W2 = E * G - F * F
     W = np.sqrt(W2)
-    n = np.cross(xu, xv, axis=1) / W[:, None, :]
+    # the reference differentiates in theta (SHTrans::backward_du with d1legTrans, d/dtheta)
+    # where u here is -d/dtheta, so its normal x_theta x x_phi / W is -(x_u x x_v) / W:
+    # outward, and H of a sphere of radius R is -1/R
+    n = -np.cross(xu, xv, axis=1) / W[:, None, :]
     En, Fn, Gn = E / W2, F / W2, G / W2
     cu = Gn[:, None] * xu - Fn[:, None] * xv
     cv = En[:, None] * xv - Fn[:, None] * xu
     L = (d["uu"] * n).sum(1)
     M = (d["uv"] * n).sum(1)
     N = (d["vv"] * n).sum(1)
-    H = 0.5 * (Gn * L + En * N) - Fn * M
-    K = (L * N - M * M) / W2
-    return dict(p=p, E=En, F=Fn, G=Gn, W=W, n=n, cu=cu, cv=cv, H=H, K=K, X=X)
+    H = lowpass(0.5 * (Gn * L + En * N) - Fn * M, p, filter_freq)
+    K = lowpass((L * N - M * M) / W2, p, filter_freq)
+    return dict(p=p, E=En, F=Fn, G=Gn, W=W, n=n, cu=cu, cv=cv, H=H, K=K, X=X, filter_freq=filter_freq)
 
 
 def grad(f, geo):
@@ -113,7 +138,7 @@ def grad(f, geo):
     S = sh.grid2shc(f.reshape(-1), p, p)
     fu = synth(S, p, "u").reshape(f.shape)
     fv = synth(S, p, "v").reshape(f.shape)
-    return fu[:, None] * geo["cu"] + fv[:, None] * geo["cv"]
+    return lowpass(fu[:, None] * geo["cu"] + fv[:, None] * geo["cv"], p, geo.get("filter_freq"))
 
 
 def div(Fv, geo):
@@ -123,7 +148,7 @@ def div(Fv, geo):
     S = sh.grid2shc(Fv.reshape(-1), p, p)
     Fu = synth(S, p, "u").reshape(Fv.shape)
     Fvv = synth(S, p, "v").reshape(Fv.shape)
-    return (Fu * geo["cu"]).sum(1) + (Fvv * geo["cv"]).sum(1)
+    return lowpass((Fu * geo["cu"]).sum(1) + (Fvv * geo["cv"]).sum(1), p, geo.get("filter_freq"))
 
 
 def lin_mean_curv(xn, geo):
@@ -135,7 +160,7 @@ def lin_mean_curv(xn, geo):
     duu = (synth(S, p, "uu").reshape(xn.shape) * nrm).sum(1)
     duv = (synth(S, p, "uv").reshape(xn.shape) * nrm).sum(1)
     dvv = (synth(S, p, "vv").reshape(xn.shape) * nrm).sum(1)
-    return 0.5 * (geo["G"] * duu - 2.0 * geo["F"] * duv + geo["E"] * dvv)
+    return lowpass(0.5 * (geo["G"] * duu - 2.0 * geo["F"] * duv + geo["E"] * dvv), p, geo.get("filter_freq"))
 
 
 def bending_of(h, geo, kappa):
@@ -158,6 +183,14 @@ def tensile_force(sigma, geo):
     return 2.0 * (geo["H"] * sigma)[:, None] * geo["n"] + grad(sigma, geo)
 
 
+def gravity_force(x, geo, excess_density, g):
+    """Traction jump of gravity, excess_density (g . x) n (InterfacialForce::gravityForce,
+    src/InterfacialForce.cc:127-160); x is a vector field [nv][3][ng] (the positions in
+    the explicit jump, the displacement in the linearised one)."""
+    gx = np.einsum("c,vcn->vn", np.asarray(g, dtype=np.float64), x)
+    return excess_density * gx[:, None, :] * geo["n"]
+
+
 def shear_flow(X, rate):
     """u = (rate * y, 0, 0)."""
     X = np.asarray(X).reshape(-1, 3, X.size // 3 if X.ndim == 1 else X.shape[-1])
@@ -171,11 +204,12 @@ class ImplicitStep:
         u - S[f(dt u, sigma)] = u_inf + S[f_b(x)],     -div S[f] = div(u_inf + S[f_b])
     with f(y, sigma) = lin_bending(y) + tension(sigma)."""
 
-    def __init__(self, X, p, kappa, dt, shear_rate, SL=None):
+    def __init__(self, X, p, kappa, dt, shear_rate, SL=None, excess_density=0.0, gravity=(0.0, 0.0, -1.0)):
         self.p = p
         self.X = np.asarray(X, dtype=np.float64)
         self.geo = geometry(self.X, p)
         self.kappa, self.dt, self.rate = kappa, dt, shear_rate
+        self.drho, self.g = excess_density, np.asarray(gravity, dtype=np.float64)
         self.SL = SL if SL is not None else sh.stokes_singular_matrix(self.X, p, 2 * p)
         self.nv, _, self.ng = self.geo["n"].shape
 
@@ -189,6 +223,8 @@ class ImplicitStep:
     def matvec(self, z):
         u, sig = self.split(z)
         f = lin_bending_force(self.dt * u, self.geo, self.kappa) + tensile_force(sig, self.geo)
+        if self.drho:
+            f = f + gravity_force(self.dt * u, self.geo, self.drho, self.g)
         Sf = self.stokes(f).reshape(u.shape)
         return np.concatenate([(u - Sf).reshape(-1), (-div(Sf, self.geo)).reshape(-1)])
 
@@ -245,6 +281,8 @@ class ImplicitStep:
 
     def rhs(self):
         fb = bending_force(self.geo, self.kappa)
+        if self.drho:
+            fb = fb + gravity_force(self.X.reshape(self.nv, 3, self.ng), self.geo, self.drho, self.g)
         v = shear_flow(self.X.reshape(self.nv, 3, self.ng), self.rate) + self.stokes(fb).reshape(self.nv, 3, self.ng)
         return np.concatenate([v.reshape(-1), div(v, self.geo).reshape(-1)])
 

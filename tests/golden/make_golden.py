@@ -25,8 +25,9 @@ def ellipsoid_pair(p):
 
 def dumbbell(reference_root="/root/reference"):
     """The reference's dumbbell test surface (entry 0 of precomputed/shape_gallery_6.txt,
-    AxisMajor [3][7][12] at p = 6) and SurfaceTest's known answers for it
-    (test/SurfaceTest.cc:72, :79, relative tolerance 5e-8)."""
+    AxisMajor [3][7][12] at p = 6) and SurfaceTest's known answers for it (area and volume,
+    test/SurfaceTest.cc:72, :79; curvature, gradients and Laplacians, :91-116). The
+    reference test compares magnitudes (MaxAbs)."""
     vals = []
     with open(os.path.join(reference_root, "precomputed", "shape_gallery_6.txt")) as fh:
         started = False
@@ -42,8 +43,16 @@ def dumbbell(reference_root="/root/reference"):
     p = 6
     X = np.asarray(vals[: 3 * 2 * p * (p + 1)])
     assert X.size == 3 * 2 * p * (p + 1), X.size
+    # test/SurfaceTest.cc:72,79 (area, volume, 5e-8), :91 (max |H|, 8e-8), :98-116 (max |grad|
+    # and max |div grad| of the coordinate fields x, y, z, 1e-7), :138-150 (Lap X . n 1e-7,
+    # H - Lap X . n / 2 and H + div n / 2, 1e-6); the reference's surface filters at 2p/3
     np.savez_compressed(os.path.join(HERE, "ref_dumbbell_p6.npz"), p=p, X=X, area=16.2179377312307,
-                        volume=5.24886489292959, rtol=5e-8)
+                        volume=5.24886489292959, rtol=5e-8, max_abs_H=1.376627062, rtol_H=8e-8,
+                        max_abs_grad=np.array([1.01100423438481, 1.011004234384816, 1.004308085588217]),
+                        max_abs_lap=np.array([2.239995450856133, 2.239995450856133, 1.777133873450119]),
+                        rtol_grad=1e-7, max_abs_lap_dot_n=2.428980517523748,
+                        max_abs_H_minus_half_lap_dot_n=0.348685011112687,
+                        max_abs_H_plus_half_div_n=0.2437253515, rtol_mixed=1e-6)
 
 
 def main():

@@ -12,8 +12,11 @@ from tests.helpers import ellipsoid_pair, unit_sphere
 @pytest.mark.parametrize("p", [8, 12])
 def test_sphere_curvatures(p):
     g = su.geometry(2.0 * unit_sphere(p), p)
-    assert np.abs(g["H"] - 0.5).max() < 1e-12
+    # the reference's conventions: outward normal, H = -1/R on a sphere
+    assert np.abs(g["H"] + 0.5).max() < 1e-12
     assert np.abs(g["K"] - 0.25).max() < 1e-12
+    X = (2.0 * unit_sphere(p)).reshape(1, 3, -1)
+    assert np.abs((g["n"] * X).sum(1) - 2.0).max() < 1e-12
 
 
 def test_surface_divergence_of_position_is_two():
@@ -74,8 +77,38 @@ def test_integrals_dumbbell_known_answers():
     d = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_dumbbell_p6.npz"))
     area, vol, cen = su.integrals(d["X"], int(d["p"]))
     assert abs(area[0] / float(d["area"]) - 1) < float(d["rtol"])
-    assert abs(abs(vol[0]) / float(d["volume"]) - 1) < float(d["rtol"])
+    assert abs(vol[0] / float(d["volume"]) - 1) < float(d["rtol"])
     assert np.abs(cen).max() < 1e-8
+
+
+def test_dumbbell_curvature_and_operators_known_answers():
+    """SurfaceTest's dumbbell (test/SurfaceTest.cc:86-151), reproduced with the reference's
+    low-pass filter at 2p/3: max |H| (8e-8); max |grad x_i| and max |Lap x_i| for the three
+    coordinate fields (1e-7); max |Lap X . n| (1e-7); max |H - Lap X . n / 2| and
+    max |H + div n / 2| (1e-6; both fix the sign of H against the normal); the linearised
+    curvature of the position is H (1e-14)."""
+    import os
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_dumbbell_p6.npz"))
+    p = int(d["p"])
+    X = d["X"].reshape(1, 3, -1)
+    geo = su.geometry(X, p, filter_freq=2 * p // 3)
+    rel = lambda a, ref: abs(np.abs(a).max() / float(ref) - 1)
+    assert rel(geo["H"], d["max_abs_H"]) < float(d["rtol_H"])
+    lap = []
+    for c in range(3):
+        g = su.grad(X[:, c], geo)
+        lap.append(su.div(g, geo))
+        assert rel(g, d["max_abs_grad"][c]) < float(d["rtol_grad"])
+        assert rel(lap[-1], d["max_abs_lap"][c]) < float(d["rtol_grad"])
+    lap_dot_n = (np.stack(lap, 1) * geo["n"]).sum(1)
+    assert rel(lap_dot_n, d["max_abs_lap_dot_n"]) < float(d["rtol_grad"])
+    assert rel(geo["H"] - 0.5 * lap_dot_n, d["max_abs_H_minus_half_lap_dot_n"]) < float(d["rtol_mixed"])
+    assert rel(geo["H"] + 0.5 * su.div(geo["n"], geo), d["max_abs_H_plus_half_div_n"]) < float(d["rtol_mixed"])
+    assert np.abs(su.lin_mean_curv(X, geo) - geo["H"]).max() < 1e-14
+    # without the filter (the GPU path's choice) the same operators differ only by the
+    # filtered-out high degrees
+    geo0 = su.geometry(X, p)
+    assert rel(geo0["H"], d["max_abs_H"]) < 0.2
 
 
 def test_integrals_sphere_and_translation():
@@ -84,7 +117,7 @@ def test_integrals_sphere_and_translation():
     X = R * workloads.shape(p, np.zeros(3), deg=0).reshape(-1)
     area, vol, cen = su.integrals(X, p)
     assert abs(area[0] / (4 * np.pi * R * R) - 1) < 1e-12
-    assert abs(abs(vol[0]) / (4 / 3 * np.pi * R ** 3) - 1) < 1e-12
+    assert abs(vol[0] / (4 / 3 * np.pi * R ** 3) - 1) < 1e-12
     shift = np.array([0.5, -2.0, 1.25])
     Xs = (X.reshape(3, -1) + shift[:, None]).reshape(-1)
     a2, v2, c2 = su.integrals(Xs, p)

@@ -43,8 +43,9 @@ __global__ void k_geometry(const double* __restrict__ xu, const double* __restri
   const double W2 = E * G - F * F;
   const double W = sqrt(W2);
   const double En = E / W2, Fn = F / W2, Gn = G / W2;
-  double n[3] = {(au[1] * av[2] - au[2] * av[1]) / W, (au[2] * av[0] - au[0] * av[2]) / W,
-                 (au[0] * av[1] - au[1] * av[0]) / W};
+  // the reference's normal x_theta x x_phi / W (outward); u here is -d/dtheta
+  double n[3] = {(au[2] * av[1] - au[1] * av[2]) / W, (au[0] * av[2] - au[2] * av[0]) / W,
+                 (au[1] * av[0] - au[0] * av[1]) / W};
   double L = 0, M = 0, Nn = 0;
 #pragma unroll
   for (int c = 0; c < 3; c++) {
@@ -143,6 +144,22 @@ __global__ void k_tension_combine(const double* __restrict__ sigma, const double
   }
 }
 
+// gravity traction: excess_density (g . x) n for a vector field x, added to add
+// (InterfacialForce::gravityForce, src/InterfacialForce.cc:127-160)
+__global__ void k_gravity_combine(const double* __restrict__ x, const double* __restrict__ geo, long N, int ng,
+                                  double drho, double gx, double gy, double gz, const double* __restrict__ add,
+                                  double* __restrict__ out, long geo_nv) {
+  FOR_POINTS(N)
+  const double* o = GEO_OF(v);
+  const long b = v * 3 * ng + k;
+  const double s = drho * (gx * x[b] + gy * x[b + ng] + gz * x[b + 2 * ng]);
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const long i = b + c * ng;
+    out[i] = (add ? add[i] : 0.0) + s * o[(4 + c) * ng];
+  }
+}
+
 // u = (rate * y, 0, 0) on AxisMajor positions
 __global__ void k_shear(const double* __restrict__ X, long N, int ng, double rate, double* __restrict__ out) {
   FOR_POINTS(N)
@@ -175,7 +192,8 @@ __global__ void __launch_bounds__(256) k_integrals(const double* __restrict__ X,
       a[d] = Xu[b + d * ng + k];
       c[d] = Xv[b + d * ng + k];
     }
-    const double nx = a[1] * c[2] - a[2] * c[1], ny = a[2] * c[0] - a[0] * c[2], nz = a[0] * c[1] - a[1] * c[0];
+    // W n with the outward normal of Surface::updateFirstForms (u here is -d/dtheta)
+    const double nx = a[2] * c[1] - a[1] * c[2], ny = a[0] * c[2] - a[2] * c[0], nz = a[1] * c[0] - a[0] * c[1];
     const double q = w[k / (2 * p)];
     const double W = sqrt(nx * nx + ny * ny + nz * nz);
     const double h = 0.5 * (x[0] * x[0] + x[1] * x[1] + x[2] * x[2]) * q;
@@ -268,6 +286,16 @@ int launch_integrals(const double* X, const double* Xu, const double* Xv, const 
                      double* out, cudaStream_t st) {
   if (nv <= 0) return VES3D_OK;
   k_integrals<<<(unsigned)nv, 256, 0, st>>>(X, Xu, Xv, w, p, out);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
+int launch_gravity_combine(const double* x, const double* geo, long nv, int ng, double drho, const double* g,
+                           const double* add, double* out, cudaStream_t st, long geo_nv) {
+  const long N = nv * ng;
+  if (N <= 0) return VES3D_OK;
+  k_gravity_combine<<<nblk(N), 256, 0, st>>>(x, geo, N, ng, drho, g[0], g[1], g[2], add, out,
+                                             geo_nv > 0 ? geo_nv : nv);
   VES3D_LAUNCHED();
   return VES3D_OK;
 }

@@ -114,6 +114,9 @@ int launch_tension_combine(const double* sigma, const double* gsig, const double
                            const double* add, double* out, cudaStream_t st,
     long geo_nv = 0);
 int launch_shear(const double* X, long nv, int ng, double rate, double* out, cudaStream_t st);
+// out = add + drho (g . x) n  (g: host array of 3)
+int launch_gravity_combine(const double* x, const double* geo, long nv, int ng, double drho, const double* g,
+                           const double* add, double* out, cudaStream_t st, long geo_nv = 0);
 // per vesicle {area, volume, centre x, y, z} (Xu latitude, Xv longitude derivatives)
 int launch_integrals(const double* X, const double* Xu, const double* Xv, const double* w, long nv, int p,
                      double* out, cudaStream_t st);

@@ -152,6 +152,7 @@ struct ves3d_sv {
   long geo_cap = 0, bws_cap = 0;
   bool geo_valid = false;
   double dt = 0.01, kappa = 0.05, shear = 1.0;
+  double drho = 0.0, grav[3] = {0.0, 0.0, -1.0};  // excess density and gravity field
   int far_force_fp64 = 0;      // 1: evaluate the far field in FP64 even in the mixed form
   int ir_outer = 0, ir_inner = 0;  // last mixed solve: outer refinements, inner iterations
   // preconditioner of the implicit solve (VES3D_PRECOND_*); the self-block form stores one
@@ -1059,6 +1060,10 @@ int implicit_matvec(ves3d_sv* sv, const OpSpace& sp, const ImplicitWork& iw, boo
   if ((s = lincomb_f64(3 * N, sv->dt, u, 0.0, u, 0.0, nullptr, iw.y, sv->stream))) return s;  // y = dt u
   if ((s = op_linH(sv, sp, iw.y, iw.h))) return s;
   if ((s = op_bend_of(sv, sp, iw.h, nullptr, iw.f))) return s;
+  if (sv->drho != 0.0 &&
+      (s = launch_gravity_combine(iw.y, sv->geo, sp.nv, ngrid_(sv->p), sv->drho, sv->grav, iw.f, iw.f, sv->stream,
+                                  sv->nves)))
+    return s;
   if ((s = op_tension(sv, sp, sig, iw.f, iw.f))) return s;
   if ((s = self_batch ? stokes_self_batch(sv, sp, iw.f, iw.Sf) : stokes_apply(sv, iw.f, iw.Sf))) return s;
   if ((s = lincomb_f64(3 * N, 1.0, u, -1.0, iw.Sf, 0.0, nullptr, y, sv->stream))) return s;
@@ -1124,6 +1129,9 @@ int implicit_rhs(ves3d_sv* sv, double* y) {
     VES3D_CK(cudaMemcpyAsync(H + v * ng, sv->geo + (v * kGeoComps + 13) * (long)ng, ng * sizeof(double),
                              cudaMemcpyDeviceToDevice, sv->stream));
   if ((s = op_bend_of(sv, H, nullptr, iw.f))) return s;
+  if (sv->drho != 0.0 &&
+      (s = launch_gravity_combine(sv->X, sv->geo, sv->nves, ng, sv->drho, sv->grav, iw.f, iw.f, sv->stream)))
+    return s;
   if ((s = stokes_apply(sv, iw.f, iw.Sf))) return s;
   if ((s = launch_shear(sv->X, sv->nves, ng, sv->shear, y, sv->stream))) return s;
   if ((s = lincomb_f64(3 * N, 1.0, y, 1.0, iw.Sf, 0.0, nullptr, y, sv->stream))) return s;
@@ -1600,6 +1608,18 @@ int ves3d_sv_set_implicit_params(ves3d_sv* sv, double dt, double kappa, double s
   return VES3D_OK;
 }
 
+int ves3d_sv_set_gravity(ves3d_sv* sv, double excess_density, double gx, double gy, double gz) {
+  int s = check_sv(sv);
+  if (s) return s;
+  if (excess_density != sv->drho || gx != sv->grav[0] || gy != sv->grav[1] || gz != sv->grav[2])
+    sv->pc_valid = false;
+  sv->drho = excess_density;
+  sv->grav[0] = gx;
+  sv->grav[1] = gy;
+  sv->grav[2] = gz;
+  return VES3D_OK;
+}
+
 int ves3d_sv_set_precond(ves3d_sv* sv, int scheme) {
   int s = check_sv(sv);
   if (s) return s;
@@ -1649,6 +1669,7 @@ int ves3d_sv_surface_op(ves3d_sv* sv, int op, const double* in, double* out, int
     case VES3D_OP_TENSION: nin = N; nout = 3 * N; break;
     case VES3D_OP_IMPLICIT_MATVEC: nin = 4 * N; nout = 4 * N; break;
     case VES3D_OP_IMPLICIT_RHS: nout = 4 * N; break;
+    case VES3D_OP_GRAVITY: nin = 3 * N; nout = 3 * N; break;
     default: VES3D_ARG(false, "unknown surface op");
   }
   VES3D_ARG(nin == 0 || in != nullptr, "in is null");
@@ -1685,6 +1706,9 @@ int ves3d_sv_surface_op(ves3d_sv* sv, int op, const double* in, double* out, int
       case VES3D_OP_TENSION: st = op_tension(sv, din, nullptr, dout); break;
       case VES3D_OP_IMPLICIT_MATVEC: st = implicit_matvec(sv, din, dout); break;
       case VES3D_OP_IMPLICIT_RHS: st = implicit_rhs(sv, dout); break;
+      case VES3D_OP_GRAVITY:
+        st = launch_gravity_combine(din, sv->geo, sv->nves, ng, sv->drho, sv->grav, nullptr, dout, sv->stream);
+        break;
     }
   }
   if (!st) st = copy_out(out, dout, nout, is_device, sv->stream);

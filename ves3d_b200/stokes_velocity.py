@@ -146,16 +146,20 @@ class StokesVelocity:
 
     # --- surface geometry, tractions, implicit step ---------------------------------------
     OPS = {"geometry": 0, "grad": 1, "div": 2, "lin_mean_curv": 3, "lin_bending": 4, "bending": 5,
-           "tension": 6, "implicit_matvec": 7, "implicit_rhs": 8}
+           "tension": 6, "implicit_matvec": 7, "implicit_rhs": 8, "gravity": 9}
 
     def set_implicit_params(self, dt, kappa, shear_rate):
         check(lib().ves3d_sv_set_implicit_params(self._h, float(dt), float(kappa), float(shear_rate)),
               "set_implicit_params")
 
+    def set_gravity(self, excess_density, g=(0.0, 0.0, -1.0)):
+        """Excess density of the vesicles and the gravity field (sedimentation)."""
+        check(lib().ves3d_sv_set_gravity(self._h, float(excess_density), *[float(c) for c in g]), "set_gravity")
+
     def surface_op(self, op, field=None):
         ng = ngrid(self.sh_order)
         N = self.n_ves * ng
-        sizes = {0: 15 * N, 1: 3 * N, 2: N, 3: N, 4: 3 * N, 5: 3 * N, 6: 3 * N, 7: 4 * N, 8: 4 * N}
+        sizes = {0: 15 * N, 1: 3 * N, 2: N, 3: N, 4: 3 * N, 5: 3 * N, 6: 3 * N, 7: 4 * N, 8: 4 * N, 9: 3 * N}
         code = self.OPS[op] if isinstance(op, str) else int(op)
         out = np.empty(sizes[code])
         if field is None:
