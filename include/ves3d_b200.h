@@ -137,6 +137,22 @@ int ves3d_svp_stage_times(ves3d_svp* g, float* ms);
  * receives the velocity; invalidated by ves3d_svp_set_src_coord. */
 int ves3d_svp_capture_eval(ves3d_svp* g);
 int ves3d_svp_launch_eval_graph(ves3d_svp* g, double* vel, int is_device);
+/* The globally implicit step of a polydisperse suspension (the reference's
+ * InterfacialVelocity::updateImplicit over vesicles of one order,
+ * src/InterfacialVelocity.cc:203-330, here across orders): the forces of each vesicle at
+ * its own order, one single layer over every point between them, BiCGStab (FP64) or mixed
+ * iterative refinement (mixed context) over the order groups' SH coefficients. Grid vectors
+ * x0 (may be NULL: zero guess) and x are [u (the per-vesicle [3][ng_v] blocks); sigma (the
+ * per-vesicle [ng_v] blocks)], 4 N doubles. Parameters, gravity and the preconditioner
+ * (VES3D_PRECOND_*, rebuilt every refresh_every surface updates) apply to every order
+ * group; tol and max_iter are in/out as in ves3d_sv_implicit_solve. */
+int ves3d_svp_set_implicit_params(ves3d_svp* g, double dt, double bending_modulus, double shear_rate);
+int ves3d_svp_set_gravity(ves3d_svp* g, double excess_density, double gx, double gy, double gz);
+int ves3d_svp_set_precond(ves3d_svp* g, int scheme, int refresh_every);
+int ves3d_svp_implicit_solve(ves3d_svp* g, const double* x0, double* x, double* tol, int* max_iter, int* code,
+                             int is_device);
+/* Last solve: outer refinements (FP64 matvecs) and inner iterations. */
+int ves3d_svp_solver_stats(ves3d_svp* g, int* outer, int* inner);
 
 /* ---------------------------------------------------------------------------
  * Surface geometry, tractions and the globally implicit step on the context's surfaces

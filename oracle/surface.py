@@ -287,6 +287,99 @@ class ImplicitStep:
         return np.concatenate([v.reshape(-1), div(v, self.geo).reshape(-1)])
 
 
+class PolyImplicitStep:
+    """The implicit step of a polydisperse suspension: vesicles in runs of equal SH order (the
+    grouping of a polydisperse StokesVelocity), forces of each vesicle at its own order, and the
+    single layer over every point (each run's self part plus the all-pairs far field across
+    runs). Grid vectors are [u (per-vesicle [3][ng_v] blocks); sigma (per-vesicle [ng_v])];
+    coefficient vectors are, run after run, [u coefficients; sigma coefficients] of the run
+    (the layout of ImplicitStep.to_coef for each run)."""
+
+    def __init__(self, X, orders, kappa, dt, shear_rate, excess_density=0.0, gravity=(0.0, 0.0, -1.0)):
+        X = np.asarray(X, dtype=np.float64).reshape(-1)
+        orders = [int(q) for q in orders]
+        self.runs = []  # (p, first vesicle, vesicles, first point)
+        pt = 0
+        for v, q in enumerate(orders):
+            if not self.runs or self.runs[-1][0] != q:
+                self.runs.append([q, v, 0, pt])
+            self.runs[-1][2] += 1
+            pt += sh.ngrid(q)
+        self.N = pt
+        self.steps = [ImplicitStep(X[3 * r[3]:3 * (r[3] + r[2] * sh.ngrid(r[0]))], r[0], kappa, dt, shear_rate,
+                                   excess_density=excess_density, gravity=gravity) for r in self.runs]
+        self.X = X
+        self.off = np.concatenate([[0], np.cumsum([sh.ngrid(q) for q in orders])]).astype(np.int64)
+
+    def stokes(self, fs):
+        """Single layer of per-run tractions fs[r] ([nv][3][ng]) -> per-run velocities."""
+        D = np.concatenate([stokes.far_density(st.X, f.reshape(-1), st.p) for st, f in zip(self.steps, fs)])
+        farv = stokes.far(self.X, D, self.off)  # [N][3]
+        out = []
+        for r, (st, f) in zip(self.runs, zip(self.steps, fs)):
+            ng = sh.ngrid(r[0])
+            fv = farv[r[3]:r[3] + r[2] * ng].reshape(r[2], ng, 3).transpose(0, 2, 1)
+            out.append(sh.self_apply(st.SL, f.reshape(-1), st.p).reshape(r[2], 3, ng) + fv)
+        return out
+
+    def split(self, z):
+        us, ss = [], []
+        for r in self.runs:
+            n = r[2] * sh.ngrid(r[0])
+            us.append(z[3 * r[3]:3 * (r[3] + n)].reshape(r[2], 3, -1))
+            ss.append(z[3 * self.N + r[3]:3 * self.N + r[3] + n].reshape(r[2], -1))
+        return us, ss
+
+    def join(self, us, ss):
+        return np.concatenate([np.concatenate([u.reshape(-1) for u in us]), np.concatenate([q.reshape(-1) for q in ss])])
+
+    def matvec(self, z):
+        us, ss = self.split(z)
+        fs = []
+        for st, u, sig in zip(self.steps, us, ss):
+            f = lin_bending_force(st.dt * u, st.geo, st.kappa) + tensile_force(sig, st.geo)
+            if st.drho:
+                f = f + gravity_force(st.dt * u, st.geo, st.drho, st.g)
+            fs.append(f)
+        Sf = self.stokes(fs)
+        return self.join([u - v for u, v in zip(us, Sf)], [-div(v, st.geo) for st, v in zip(self.steps, Sf)])
+
+    def rhs(self):
+        fs = []
+        for st in self.steps:
+            fb = bending_force(st.geo, st.kappa)
+            if st.drho:
+                fb = fb + gravity_force(st.X.reshape(st.nv, 3, st.ng), st.geo, st.drho, st.g)
+            fs.append(fb)
+        Sf = self.stokes(fs)
+        vs = [shear_flow(st.X.reshape(st.nv, 3, st.ng), st.rate) + v for st, v in zip(self.steps, Sf)]
+        return self.join(vs, [div(v, st.geo) for st, v in zip(self.steps, vs)])
+
+    def to_coef(self, z):
+        us, ss = self.split(z)
+        return np.concatenate([st.to_coef(np.concatenate([u.reshape(-1), q.reshape(-1)]))
+                               for st, u, q in zip(self.steps, us, ss)])
+
+    def to_grid(self, c):
+        us, ss, k = [], [], 0
+        for r, st in zip(self.runs, self.steps):
+            n = 4 * r[2] * sh.ncoef(r[0])
+            g = st.to_grid(c[k:k + n])
+            k += n
+            us.append(g[:3 * st.nv * st.ng])
+            ss.append(g[3 * st.nv * st.ng:])
+        return self.join(us, ss)
+
+    def matvec_sh(self, c):
+        return self.to_coef(self.matvec(self.to_grid(c)))
+
+    def solve(self, x0=None, tol=1e-8, max_iter=300):
+        b = self.to_coef(self.rhs())
+        c0 = np.zeros_like(b) if x0 is None else self.to_coef(np.asarray(x0, dtype=np.float64))
+        c, code, it, rr = bicgstab(self.matvec_sh, b, c0, tol, max_iter)
+        return self.to_grid(c), code, it, rr
+
+
 def bicgstab(A, b, x0, tol, max_iter, P=None):
     """Preconditioned BiCGStab, the reference's iteration (src/BiCGStab.cc:45-138).
     Returns (x, status, iterations, relres); status 100 success, 101 max iterations,

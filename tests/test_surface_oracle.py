@@ -123,3 +123,24 @@ def test_integrals_sphere_and_translation():
     a2, v2, c2 = su.integrals(Xs, p)
     assert abs(a2[0] - area[0]) < 1e-12 * area[0] and abs(v2[0] - vol[0]) < 1e-12 * abs(vol[0])
     assert np.abs(c2[0] - cen[0] - shift).max() < 1e-12
+
+
+def test_poly_implicit_step_single_order_is_uniform():
+    """The oracle's polydisperse implicit step with one order is ImplicitStep exactly, and
+    with two orders its operator is linear and its coefficient maps invert each other."""
+    from tests.helpers import small_suspension
+    from ves3d_b200 import workloads
+    X, _ = small_suspension(2, 6, 61, spacing=2.7)
+    nv = X.size // (3 * 2 * 6 * 7)
+    P = su.PolyImplicitStep(X, [6] * nv, 0.05, 0.01, 1.0, excess_density=1.0)
+    S = su.ImplicitStep(X, 6, 0.05, 0.01, 1.0, excess_density=1.0)
+    z = np.random.default_rng(1).standard_normal(4 * X.size // 3)
+    assert np.abs(P.matvec(z) - S.matvec(z)).max() == 0.0
+    assert np.abs(P.rhs() - S.rhs()).max() == 0.0
+    X2, _, orders = workloads.polydisperse(3, orders=(4, 6), radius=(0.8, 1.2), volume_fraction=0.05, seed=5)
+    Q = su.PolyImplicitStep(X2, orders, 0.05, 0.01, 0.0, excess_density=1.0)
+    rng = np.random.default_rng(2)
+    a, b = rng.standard_normal((2, 4 * X2.size // 3))
+    assert np.abs(Q.matvec(2 * a - b) - (2 * Q.matvec(a) - Q.matvec(b))).max() < 1e-12 * np.abs(Q.matvec(a)).max()
+    c = Q.to_coef(a)
+    assert np.abs(Q.to_coef(Q.to_grid(c)) - c).max() < 1e-12

@@ -1049,10 +1049,11 @@ int implicit_work(ves3d_sv* sv, ImplicitWork& iw) {
   return VES3D_OK;
 }
 
-// [u; sigma] -> [u - S f ; -div S f],  f = linbend(dt u) + tension(sigma); S is the full
-// single layer, or the self part alone for a batched space (self_batch)
-int implicit_matvec(ves3d_sv* sv, const OpSpace& sp, const ImplicitWork& iw, bool self_batch, const double* x,
-                    double* y) {
+// The implicit operator [u; sigma] -> [u - S f ; -div S f] with f = linbend(dt u) +
+// gravity(dt u) + tension(sigma), in two phases around the single layer S (so that a
+// polydisperse suspension can apply one S over all its order groups):
+// forces: iw.f = f(x)
+int implicit_forces(ves3d_sv* sv, const OpSpace& sp, const ImplicitWork& iw, const double* x) {
   int s;
   const long N = sp.nv * ngrid_(sv->p);
   const double* u = x;
@@ -1064,10 +1065,25 @@ int implicit_matvec(ves3d_sv* sv, const OpSpace& sp, const ImplicitWork& iw, boo
       (s = launch_gravity_combine(iw.y, sv->geo, sp.nv, ngrid_(sv->p), sv->drho, sv->grav, iw.f, iw.f, sv->stream,
                                   sv->nves)))
     return s;
-  if ((s = op_tension(sv, sp, sig, iw.f, iw.f))) return s;
+  return op_tension(sv, sp, sig, iw.f, iw.f);
+}
+
+// finish: y = [u - Sf; -div Sf]
+int implicit_finish(ves3d_sv* sv, const OpSpace& sp, const double* x, const double* Sf, double* y) {
+  int s;
+  const long N = sp.nv * ngrid_(sv->p);
+  if ((s = lincomb_f64(3 * N, 1.0, x, -1.0, Sf, 0.0, nullptr, y, sv->stream))) return s;
+  return op_div(sv, sp, Sf, y + 3 * N, -1.0);
+}
+
+// S is the context's full single layer, or the self part alone for a batched space
+// (self_batch)
+int implicit_matvec(ves3d_sv* sv, const OpSpace& sp, const ImplicitWork& iw, bool self_batch, const double* x,
+                    double* y) {
+  int s;
+  if ((s = implicit_forces(sv, sp, iw, x))) return s;
   if ((s = self_batch ? stokes_self_batch(sv, sp, iw.f, iw.Sf) : stokes_apply(sv, iw.f, iw.Sf))) return s;
-  if ((s = lincomb_f64(3 * N, 1.0, u, -1.0, iw.Sf, 0.0, nullptr, y, sv->stream))) return s;
-  return op_div(sv, sp, iw.Sf, y + 3 * N, -1.0);
+  return implicit_finish(sv, sp, x, iw.Sf, y);
 }
 
 int implicit_matvec(ves3d_sv* sv, const double* x, double* y) {
@@ -1117,25 +1133,38 @@ int implicit_matvec_sh_self_batch(ves3d_sv* sv, const OpSpace& sp, const Implici
   return grid_to_coef(sv, sp.nv, iw.g2, y);
 }
 
+// Right-hand side [u_inf + S f_b; div(u_inf + S f_b)] (AssembleRhsVel,
+// src/InterfacialVelocity.cc:716-771), again in two phases around S:
+// forces: iw.f = f_b = bending traction of H (+ the explicit gravity jump on X)
+int rhs_forces(ves3d_sv* sv, const ImplicitWork& iw) {
+  int s;
+  const int ng = ngrid_(sv->p);
+  // H is geometry component 13 of every vesicle's record: one strided copy
+  VES3D_CK(cudaMemcpy2DAsync(iw.h, ng * sizeof(double), sv->geo + 13L * ng, kGeoComps * ng * sizeof(double),
+                             ng * sizeof(double), (size_t)sv->nves, cudaMemcpyDeviceToDevice, sv->stream));
+  if ((s = op_bend_of(sv, iw.h, nullptr, iw.f))) return s;
+  if (sv->drho != 0.0 &&
+      (s = launch_gravity_combine(sv->X, sv->geo, sv->nves, ng, sv->drho, sv->grav, iw.f, iw.f, sv->stream)))
+    return s;
+  return VES3D_OK;
+}
+
+// finish: y = [u_inf + Sf; div(u_inf + Sf)]
+int rhs_finish(ves3d_sv* sv, const double* Sf, double* y) {
+  int s;
+  const long N = sv->npts();
+  if ((s = launch_shear(sv->X, sv->nves, ngrid_(sv->p), sv->shear, y, sv->stream))) return s;
+  if ((s = lincomb_f64(3 * N, 1.0, y, 1.0, Sf, 0.0, nullptr, y, sv->stream))) return s;
+  return op_div(sv, y, y + 3 * N, 1.0);
+}
+
 int implicit_rhs(ves3d_sv* sv, double* y) {
   int s;
   ImplicitWork iw;
   if ((s = implicit_work(sv, iw))) return s;
-  const long N = sv->npts();
-  const int ng = ngrid_(sv->p);
-  // f_b = bending traction of the mean curvature H (geo component 13)
-  double* H = iw.h;
-  for (long v = 0; v < sv->nves; v++)
-    VES3D_CK(cudaMemcpyAsync(H + v * ng, sv->geo + (v * kGeoComps + 13) * (long)ng, ng * sizeof(double),
-                             cudaMemcpyDeviceToDevice, sv->stream));
-  if ((s = op_bend_of(sv, H, nullptr, iw.f))) return s;
-  if (sv->drho != 0.0 &&
-      (s = launch_gravity_combine(sv->X, sv->geo, sv->nves, ng, sv->drho, sv->grav, iw.f, iw.f, sv->stream)))
-    return s;
+  if ((s = rhs_forces(sv, iw))) return s;
   if ((s = stokes_apply(sv, iw.f, iw.Sf))) return s;
-  if ((s = launch_shear(sv->X, sv->nves, ng, sv->shear, y, sv->stream))) return s;
-  if ((s = lincomb_f64(3 * N, 1.0, y, 1.0, iw.Sf, 0.0, nullptr, y, sv->stream))) return s;
-  return op_div(sv, y, y + 3 * N, 1.0);
+  return rhs_finish(sv, iw.Sf, y);
 }
 
 int implicit_matvec_cb(void* ctx, const double* x, double* y) { return implicit_matvec_sh((ves3d_sv*)ctx, x, y); }
@@ -1484,16 +1513,30 @@ int ensure_precond(ves3d_sv* sv) {
 
 MatVecFn precond_fn(ves3d_sv* sv) { return sv->precond == VES3D_PRECOND_NONE ? nullptr : precond_apply; }
 
+// The operators of one implicit system: the inner-solve operator in the context's
+// precision, the same operator with the FP64 far field (outer residuals) and the right
+// preconditioner (may be null), all on one context and stream.
+struct SolveOps {
+  MatVecFn mixed = nullptr;
+  MatVecFn fp64 = nullptr;
+  MatVecFn P = nullptr;
+  void* ctx = nullptr;
+  cudaStream_t st = nullptr;
+};
+
 // Mixed-precision iterative refinement: outer residuals r = b - A x with the FP64
 // operator; inner BiCGStab with the mixed operator on A d = r to a relative tolerance of
-// 1e-2 (at most 150 iterations per correction); x += d. A correction that does not reduce the FP64 residual is undone and
-// the remaining work falls back to FP64 inner solves. *tol in: target relative residual;
-// out: achieved. *max_iter in: bound on inner iterations in total; out: inner iterations
-// used (FP64 matvecs of the outer loop are reported through ves3d_sv::ir_outer).
-int mixed_refinement(ves3d_sv* sv, double* x, const double* b, long n, double* tol, int* max_iter, int* code) {
+// 1e-2 (at most 150 iterations per correction); x += d. A correction that does not reduce
+// the FP64 residual is undone and the remaining work falls back to FP64 inner solves.
+// *tol in: target relative residual; out: achieved. *max_iter in: bound on inner
+// iterations in total; out: inner iterations used; outer refinements (FP64 matvecs) go to
+// *outer_out.
+int mixed_refinement(const SolveOps& ops, double* x, const double* b, long n, double* tol, int* max_iter, int* code,
+                     int* outer_out, int* inner_out) {
   int s;
   const double target = *tol;
   const int budget = *max_iter;
+  cudaStream_t st = ops.st;
   double *r = nullptr, *d = nullptr, *ax = nullptr, *ws = nullptr;
   if ((s = dalloc(&r, n))) return s;
   if ((s = dalloc(&d, n)) || (s = dalloc(&ax, n)) || (s = dalloc(&ws, bicgstab_workspace_doubles(n)))) {
@@ -1501,7 +1544,7 @@ int mixed_refinement(ves3d_sv* sv, double* x, const double* b, long n, double* t
     return s;
   }
   double nb2 = 0;
-  s = dot_f64(b, b, n, bicgstab_dot_scratch(ws, n), &nb2, sv->stream);
+  s = dot_f64(b, b, n, bicgstab_dot_scratch(ws, n), &nb2, st);
   const double normb = nb2 > 0 ? std::sqrt(nb2) : 1.0;
   int used = 0, outer = 0;
   bool fp64_inner = false;
@@ -1509,10 +1552,10 @@ int mixed_refinement(ves3d_sv* sv, double* x, const double* b, long n, double* t
   *code = 101;
   while (!s && outer < 30) {
     // FP64 residual
-    if ((s = implicit_matvec_fp64_cb(sv, x, ax))) break;
-    if ((s = lincomb_f64(n, 1.0, b, -1.0, ax, 0.0, nullptr, r, sv->stream))) break;
+    if ((s = ops.fp64(ops.ctx, x, ax))) break;
+    if ((s = lincomb_f64(n, 1.0, b, -1.0, ax, 0.0, nullptr, r, st))) break;
     double rr = 0;
-    if ((s = dot_f64(r, r, n, bicgstab_dot_scratch(ws, n), &rr, sv->stream))) break;
+    if ((s = dot_f64(r, r, n, bicgstab_dot_scratch(ws, n), &rr, st))) break;
     const double cur = std::sqrt(rr) / normb;
     outer++;
     if (cur != cur) {  // non-finite residual (BiCGSReturn RelresIsNan)
@@ -1522,7 +1565,7 @@ int mixed_refinement(ves3d_sv* sv, double* x, const double* b, long n, double* t
     }
     if (cur > relres) {
       // the last correction made things worse: undo it, continue with FP64 inner solves
-      if ((s = lincomb_f64(n, 1.0, x, -1.0, d, 0.0, nullptr, x, sv->stream))) break;
+      if ((s = lincomb_f64(n, 1.0, x, -1.0, d, 0.0, nullptr, x, st))) break;
       fp64_inner = true;
       continue;
     }
@@ -1535,24 +1578,34 @@ int mixed_refinement(ves3d_sv* sv, double* x, const double* b, long n, double* t
     // inner solve for the correction, from zero, to 1e-2 of the current residual (or the
     // target): the FP32 far field is accurate to ~1e-5 for dipole-dominated densities, so
     // each correction only has to make a modest, reliable reduction
-    VES3D_CK(cudaMemsetAsync(d, 0, n * sizeof(double), sv->stream));
+    VES3D_CK(cudaMemsetAsync(d, 0, n * sizeof(double), st));
     double itol = std::max(1e-2, 0.5 * target / relres);
     int imax = std::min(budget - used, 150), icode = 0;
-    if ((s = bicgstab_run(fp64_inner ? implicit_matvec_fp64_cb : implicit_matvec_cb, sv, d, r, n, &itol, &imax,
-                          &icode, ws, sv->stream, precond_fn(sv), sv)))
+    if ((s = bicgstab_run(fp64_inner ? ops.fp64 : ops.mixed, ops.ctx, d, r, n, &itol, &imax, &icode, ws, st, ops.P,
+                          ops.ctx)))
       break;
     used += imax;
-    if ((s = lincomb_f64(n, 1.0, x, 1.0, d, 0.0, nullptr, x, sv->stream))) break;
+    if ((s = lincomb_f64(n, 1.0, x, 1.0, d, 0.0, nullptr, x, st))) break;
   }
   *tol = relres;
   *max_iter = used;
-  sv->ir_outer = outer;
-  sv->ir_inner = used;
+  if (outer_out) *outer_out = outer;
+  if (inner_out) *inner_out = used;
   dfree(r);
   dfree(d);
   dfree(ax);
   dfree(ws);
   return s;
+}
+
+int mixed_refinement(ves3d_sv* sv, double* x, const double* b, long n, double* tol, int* max_iter, int* code) {
+  SolveOps ops;
+  ops.mixed = implicit_matvec_cb;
+  ops.fp64 = implicit_matvec_fp64_cb;
+  ops.P = precond_fn(sv);
+  ops.ctx = sv;
+  ops.st = sv->stream;
+  return mixed_refinement(ops, x, b, n, tol, max_iter, code, &sv->ir_outer, &sv->ir_inner);
 }
 
 }  // namespace
@@ -2065,6 +2118,13 @@ struct ves3d_svp {
   float ms[4] = {0, 0, 0, 0};
   cudaGraph_t graph = nullptr;  // captured evaluation (self parts of every group + far field)
   cudaGraphExec_t graph_exec = nullptr;
+  // implicit step: parameters pushed to every order group before a solve
+  double dt = 0.01, kappa = 0.05, shear = 1.0, drho = 0.0, grav[3] = {0.0, 0.0, -1.0};
+  int precond = 0, pc_refresh = 1;
+  int far_force_fp64 = 0, ir_outer = 0, ir_inner = 0;
+  std::vector<long> coff;  // first SH unknown of each group's [u; sigma] coefficients
+  double* sws = nullptr;   // solve workspace: BiCGStab, coefficients, right-hand side, grid
+  long sws_cap = 0;
   void drop_graph() {
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (graph) cudaGraphDestroy(graph);
@@ -2088,6 +2148,7 @@ struct ves3d_svp {
     drop_graph();
     free_groups();
     free_global();
+    dfree(sws);
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
     if (stream) cudaStreamDestroy(stream);
@@ -2231,7 +2292,7 @@ static int svp_self_parts(ves3d_svp* g) {
 
 // one far-field pass over every point, launched per order group (block shape per group)
 static int svp_far(ves3d_svp* g) {
-  const bool mixed = g->prec == VES3D_PREC_MIXED;
+  const bool mixed = g->prec == VES3D_PREC_MIXED && !g->far_force_fp64;
   std::vector<FarGroup> fg;
   long v0 = 0;
   for (size_t r = 0; r < g->grp.size(); r++) {
@@ -2317,3 +2378,225 @@ int ves3d_svp_stage_times(ves3d_svp* g, float* ms) {
 
 }  // extern "C"
 
+
+// ---- implicit step of a polydisperse suspension -------------------------------------
+// Every order group keeps its own geometry, tractions, self matrices and preconditioner;
+// the single layer between the force and finish phases is one evaluation over all points
+// (each group's self part plus the far field across groups). Unknowns: the groups' SH
+// coefficient vectors [u; sigma] one after another (group r at coff[r]); grid vectors
+// [u (per-vesicle [3][ng] blocks, all points); sigma (all points)].
+namespace {
+
+int svp_prepare_implicit(ves3d_svp* g) {
+  int s;
+  if ((s = ves3d_svp_setup(g))) return s;
+  g->coff.assign(g->grp.size() + 1, 0);
+  for (size_t r = 0; r < g->grp.size(); r++) {
+    ves3d_sv* sv = g->grp[r];
+    if ((s = ves3d_sv_set_implicit_params(sv, g->dt, g->kappa, g->shear))) return s;
+    if ((s = ves3d_sv_set_gravity(sv, g->drho, g->grav[0], g->grav[1], g->grav[2]))) return s;
+    if ((s = ves3d_sv_set_precond(sv, g->precond))) return s;
+    if ((s = ves3d_sv_set_precond_refresh(sv, g->pc_refresh))) return s;
+    if ((s = ensure_geometry(sv))) return s;
+    ImplicitWork iw;
+    if ((s = implicit_work(sv, iw))) return s;
+    g->coff[r + 1] = g->coff[r] + sh_unknowns(sv);
+  }
+  return VES3D_OK;
+}
+
+// g->V = S[f] over the whole suspension, f = every group's iw.f
+int svp_stokes(ves3d_svp* g) {
+  int s;
+  for (ves3d_sv* sv : g->grp) {
+    ImplicitWork iw;
+    if ((s = implicit_work(sv, iw))) return s;
+    VES3D_CK(cudaMemcpyAsync(sv->F, iw.f, 3 * (size_t)sv->npts() * sizeof(double), cudaMemcpyDeviceToDevice,
+                             g->stream));
+    sv->have_den = true;
+  }
+  if ((s = svp_self_parts(g))) return s;
+  return svp_far(g);
+}
+
+int svp_matvec_sh(ves3d_svp* g, const double* c, double* y) {
+  int s;
+  for (size_t r = 0; r < g->grp.size(); r++) {
+    ves3d_sv* sv = g->grp[r];
+    ImplicitWork iw;
+    if ((s = implicit_work(sv, iw))) return s;
+    if ((s = coef_to_grid(sv, c + g->coff[r], iw.g1))) return s;
+    if ((s = implicit_forces(sv, base_space(sv), iw, iw.g1))) return s;
+  }
+  if ((s = svp_stokes(g))) return s;
+  for (size_t r = 0; r < g->grp.size(); r++) {
+    ves3d_sv* sv = g->grp[r];
+    ImplicitWork iw;
+    if ((s = implicit_work(sv, iw))) return s;
+    if ((s = implicit_finish(sv, base_space(sv), iw.g1, g->V + 3 * g->gpt0[r], iw.g2))) return s;
+    if ((s = grid_to_coef(sv, iw.g2, y + g->coff[r]))) return s;
+  }
+  return VES3D_OK;
+}
+
+int svp_matvec_cb(void* ctx, const double* x, double* y) { return svp_matvec_sh((ves3d_svp*)ctx, x, y); }
+
+int svp_matvec_fp64_cb(void* ctx, const double* x, double* y) {
+  ves3d_svp* g = (ves3d_svp*)ctx;
+  g->far_force_fp64 = 1;
+  const int s = svp_matvec_sh(g, x, y);
+  g->far_force_fp64 = 0;
+  return s;
+}
+
+int svp_precond_cb(void* ctx, const double* x, double* y) {
+  ves3d_svp* g = (ves3d_svp*)ctx;
+  for (size_t r = 0; r < g->grp.size(); r++) {
+    const int s = precond_apply(g->grp[r], x + g->coff[r], y + g->coff[r]);
+    if (s) return s;
+  }
+  return VES3D_OK;
+}
+
+// right-hand side in coefficients (FP64 far field)
+int svp_rhs(ves3d_svp* g, double* b) {
+  int s;
+  for (ves3d_sv* sv : g->grp) {
+    ImplicitWork iw;
+    if ((s = implicit_work(sv, iw))) return s;
+    if ((s = rhs_forces(sv, iw))) return s;
+  }
+  g->far_force_fp64 = 1;
+  s = svp_stokes(g);
+  g->far_force_fp64 = 0;
+  if (s) return s;
+  for (size_t r = 0; r < g->grp.size(); r++) {
+    ves3d_sv* sv = g->grp[r];
+    ImplicitWork iw;
+    if ((s = implicit_work(sv, iw))) return s;
+    if ((s = rhs_finish(sv, g->V + 3 * g->gpt0[r], iw.g2))) return s;
+    if ((s = grid_to_coef(sv, iw.g2, b + g->coff[r]))) return s;
+  }
+  return VES3D_OK;
+}
+
+// global grid vector [u; sigma] <-> group coefficient vectors
+int svp_grid_to_coef(ves3d_svp* g, const double* x, double* c) {
+  int s;
+  for (size_t r = 0; r < g->grp.size(); r++) {
+    ves3d_sv* sv = g->grp[r];
+    ImplicitWork iw;
+    if ((s = implicit_work(sv, iw))) return s;
+    const size_t n = (size_t)sv->npts();
+    VES3D_CK(cudaMemcpyAsync(iw.g1, x + 3 * g->gpt0[r], 3 * n * sizeof(double), cudaMemcpyDeviceToDevice, g->stream));
+    VES3D_CK(cudaMemcpyAsync(iw.g1 + 3 * n, x + 3 * g->N + g->gpt0[r], n * sizeof(double), cudaMemcpyDeviceToDevice,
+                             g->stream));
+    if ((s = grid_to_coef(sv, iw.g1, c + g->coff[r]))) return s;
+  }
+  return VES3D_OK;
+}
+
+int svp_coef_to_grid(ves3d_svp* g, const double* c, double* x) {
+  int s;
+  for (size_t r = 0; r < g->grp.size(); r++) {
+    ves3d_sv* sv = g->grp[r];
+    ImplicitWork iw;
+    if ((s = implicit_work(sv, iw))) return s;
+    const size_t n = (size_t)sv->npts();
+    if ((s = coef_to_grid(sv, c + g->coff[r], iw.g1))) return s;
+    VES3D_CK(cudaMemcpyAsync(x + 3 * g->gpt0[r], iw.g1, 3 * n * sizeof(double), cudaMemcpyDeviceToDevice, g->stream));
+    VES3D_CK(cudaMemcpyAsync(x + 3 * g->N + g->gpt0[r], iw.g1 + 3 * n, n * sizeof(double), cudaMemcpyDeviceToDevice,
+                             g->stream));
+  }
+  return VES3D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ves3d_svp_set_implicit_params(ves3d_svp* g, double dt, double kappa, double shear_rate) {
+  VES3D_ARG(g != nullptr, "null context");
+  VES3D_ARG(dt > 0 && kappa >= 0, "dt must be > 0 and kappa >= 0");
+  g->dt = dt;
+  g->kappa = kappa;
+  g->shear = shear_rate;
+  return VES3D_OK;
+}
+
+int ves3d_svp_set_gravity(ves3d_svp* g, double excess_density, double gx, double gy, double gz) {
+  VES3D_ARG(g != nullptr, "null context");
+  g->drho = excess_density;
+  g->grav[0] = gx;
+  g->grav[1] = gy;
+  g->grav[2] = gz;
+  return VES3D_OK;
+}
+
+int ves3d_svp_set_precond(ves3d_svp* g, int scheme, int refresh_every) {
+  VES3D_ARG(g != nullptr, "null context");
+  VES3D_ARG(scheme >= VES3D_PRECOND_NONE && scheme <= VES3D_PRECOND_SELF_BLOCK, "unknown preconditioner");
+  VES3D_ARG(refresh_every >= 1, "refresh interval must be >= 1");
+  g->precond = scheme;
+  g->pc_refresh = refresh_every;
+  return VES3D_OK;
+}
+
+int ves3d_svp_solver_stats(ves3d_svp* g, int* outer, int* inner) {
+  VES3D_ARG(g && outer && inner, "null argument");
+  *outer = g->ir_outer;
+  *inner = g->ir_inner;
+  return VES3D_OK;
+}
+
+int ves3d_svp_implicit_solve(ves3d_svp* g, const double* x0, double* x, double* tol, int* max_iter, int* code,
+                             int is_device) {
+  VES3D_ARG(g && x && tol && max_iter && code, "null argument");
+  if (g->grp.empty()) {
+    set_error("no surfaces set");
+    return VES3D_ERR_STATE;
+  }
+  VES3D_CK(cudaSetDevice(g->device));
+  int s;
+  if ((s = svp_prepare_implicit(g))) return s;
+  const long nsh = g->coff.back(), ng4 = 4 * g->N, nws = bicgstab_workspace_doubles(nsh);
+  const long need = nws + 2 * nsh + ng4;
+  if (g->sws_cap < need) {
+    dfree(g->sws);
+    g->sws = nullptr;
+    g->sws_cap = 0;
+    if ((s = dalloc(&g->sws, need))) return s;
+    g->sws_cap = need;
+  }
+  double *ws = g->sws, *dc = ws + nws, *db = dc + nsh, *dg = db + nsh;
+  if (x0) {
+    s = copy_in(dg, x0, ng4, is_device, g->stream);
+    if (!s) s = svp_grid_to_coef(g, dg, dc);
+  } else {
+    s = cuda_status(cudaMemsetAsync(dc, 0, nsh * sizeof(double), g->stream), "memset", __FILE__, __LINE__);
+  }
+  if (!s) s = svp_rhs(g, db);
+  for (size_t r = 0; r < g->grp.size() && !s; r++) s = ensure_precond(g->grp[r]);
+  const MatVecFn P = g->precond == VES3D_PRECOND_NONE ? nullptr : svp_precond_cb;
+  if (!s) {
+    if (g->prec == VES3D_PREC_FP64) {
+      s = bicgstab_run(svp_matvec_cb, g, dc, db, nsh, tol, max_iter, code, ws, g->stream, P, g);
+      g->ir_outer = 0;
+      g->ir_inner = *max_iter;
+    } else {
+      SolveOps ops;
+      ops.mixed = svp_matvec_cb;
+      ops.fp64 = svp_matvec_fp64_cb;
+      ops.P = P;
+      ops.ctx = g;
+      ops.st = g->stream;
+      s = mixed_refinement(ops, dc, db, nsh, tol, max_iter, code, &g->ir_outer, &g->ir_inner);
+    }
+  }
+  if (!s) s = svp_coef_to_grid(g, dc, dg);
+  if (!s) s = copy_out(x, dg, ng4, is_device, g->stream);
+  cudaStreamSynchronize(g->stream);
+  return s;
+}
+
+}  // extern "C"

@@ -326,3 +326,40 @@ class PolydisperseStokesVelocity:
         ms = (ctypes.c_float * 4)()
         check(lib().ves3d_svp_stage_times(self._h, ms), "stage_times")
         return {"setup_ms": ms[0], "self_ms": ms[1], "far_ms": ms[2], "eval_ms": ms[3]}
+
+    # ---- implicit step -----------------------------------------------------------------
+    def set_implicit_params(self, dt, kappa, shear_rate):
+        check(lib().ves3d_svp_set_implicit_params(self._h, float(dt), float(kappa), float(shear_rate)),
+              "set_implicit_params")
+
+    def set_gravity(self, excess_density, g=(0.0, 0.0, -1.0)):
+        check(lib().ves3d_svp_set_gravity(self._h, float(excess_density), *[float(c) for c in g]), "set_gravity")
+
+    def set_precond(self, scheme, refresh_every=1):
+        """"none", "diag_spectral" or "self_block" for every order group, rebuilt every
+        refresh_every surface updates."""
+        code = StokesVelocity.PRECONDS[scheme] if isinstance(scheme, str) else int(scheme)
+        check(lib().ves3d_svp_set_precond(self._h, code, int(refresh_every)), "set_precond")
+
+    def solver_stats(self):
+        o, i = ctypes.c_int(0), ctypes.c_int(0)
+        check(lib().ves3d_svp_solver_stats(self._h, ctypes.byref(o), ctypes.byref(i)), "solver_stats")
+        return {"outer": o.value, "inner": i.value}
+
+    def implicit_solve(self, x0=None, tol=1e-8, max_iter=200):
+        """Solve the implicit system of the whole suspension for [u; sigma] (u: the
+        per-vesicle [3][ng] blocks of all points, then sigma); returns (x, iterations,
+        relres, code)."""
+        x = np.empty(4 * self.npoints())
+        t = ctypes.c_double(tol)
+        it = ctypes.c_int(max_iter)
+        code = ctypes.c_int(0)
+        p0 = None
+        if x0 is not None:
+            x0 = np.ascontiguousarray(x0, dtype=np.float64).reshape(-1)
+            if x0.size != x.size:
+                raise ValueError("x0 size does not match the surfaces")
+            p0 = x0.ctypes.data
+        check(lib().ves3d_svp_implicit_solve(self._h, p0, x.ctypes.data, ctypes.byref(t), ctypes.byref(it),
+                                             ctypes.byref(code), 0), "implicit_solve")
+        return x, it.value, t.value, code.value
