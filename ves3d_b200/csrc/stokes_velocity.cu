@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
@@ -1524,10 +1525,21 @@ struct SolveOps {
   cudaStream_t st = nullptr;
 };
 
+// VES3D_SOLVER_TRACE=1 in the environment: one line per refinement step on stderr
+bool solver_trace() {
+  static const bool on = [] {
+    const char* e = std::getenv("VES3D_SOLVER_TRACE");
+    return e && *e && *e != '0';
+  }();
+  return on;
+}
+
 // Mixed-precision iterative refinement: outer residuals r = b - A x with the FP64
 // operator; inner BiCGStab with the mixed operator on A d = r to a relative tolerance of
 // 1e-2 (at most 150 iterations per correction); x += d. A correction that does not reduce
-// the FP64 residual is undone and the remaining work falls back to FP64 inner solves.
+// the FP64 residual is undone (the residual before it is kept, so undoing costs no
+// operator application) and retried once with the mixed operator to 1e-3; a second
+// failure in a row switches to FP64 inner solves of at most 50 iterations each.
 // *tol in: target relative residual; out: achieved. *max_iter in: bound on inner
 // iterations in total; out: inner iterations used; outer refinements (FP64 matvecs) go to
 // *outer_out.
@@ -1537,17 +1549,17 @@ int mixed_refinement(const SolveOps& ops, double* x, const double* b, long n, do
   const double target = *tol;
   const int budget = *max_iter;
   cudaStream_t st = ops.st;
-  double *r = nullptr, *d = nullptr, *ax = nullptr, *ws = nullptr;
+  double *r = nullptr, *rp = nullptr, *d = nullptr, *ax = nullptr, *ws = nullptr;
   if ((s = dalloc(&r, n))) return s;
-  if ((s = dalloc(&d, n)) || (s = dalloc(&ax, n)) || (s = dalloc(&ws, bicgstab_workspace_doubles(n)))) {
-    dfree(r); dfree(d); dfree(ax);
+  if ((s = dalloc(&rp, n)) || (s = dalloc(&d, n)) || (s = dalloc(&ax, n)) ||
+      (s = dalloc(&ws, bicgstab_workspace_doubles(n)))) {
+    dfree(r); dfree(rp); dfree(d); dfree(ax);
     return s;
   }
   double nb2 = 0;
   s = dot_f64(b, b, n, bicgstab_dot_scratch(ws, n), &nb2, st);
   const double normb = nb2 > 0 ? std::sqrt(nb2) : 1.0;
-  int used = 0, outer = 0;
-  bool fp64_inner = false;
+  int used = 0, outer = 0, fails = 0;
   double relres = 1e300;
   *code = 101;
   while (!s && outer < 30) {
@@ -1558,32 +1570,42 @@ int mixed_refinement(const SolveOps& ops, double* x, const double* b, long n, do
     if ((s = dot_f64(r, r, n, bicgstab_dot_scratch(ws, n), &rr, st))) break;
     const double cur = std::sqrt(rr) / normb;
     outer++;
+    if (solver_trace())
+      std::fprintf(stderr, "[ves3d refine] outer %d FP64 relres %.3e (inner iterations so far %d)\n", outer, cur,
+                   used);
     if (cur != cur) {  // non-finite residual (BiCGSReturn RelresIsNan)
       relres = cur;
       *code = 104;
       break;
     }
     if (cur > relres) {
-      // the last correction made things worse: undo it, continue with FP64 inner solves
+      // the last correction made things worse: undo it and restore the residual before it
       if ((s = lincomb_f64(n, 1.0, x, -1.0, d, 0.0, nullptr, x, st))) break;
-      fp64_inner = true;
-      continue;
-    }
-    relres = cur;
-    if (relres < target) {
-      *code = 100;
-      break;
+      VES3D_CK(cudaMemcpyAsync(r, rp, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      fails++;
+    } else {
+      relres = cur;
+      fails = 0;
+      if (relres < target) {
+        *code = 100;
+        break;
+      }
+      VES3D_CK(cudaMemcpyAsync(rp, r, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     }
     if (used >= budget) break;
     // inner solve for the correction, from zero, to 1e-2 of the current residual (or the
     // target): the FP32 far field is accurate to ~1e-5 for dipole-dominated densities, so
     // each correction only has to make a modest, reliable reduction
     VES3D_CK(cudaMemsetAsync(d, 0, n * sizeof(double), st));
-    double itol = std::max(1e-2, 0.5 * target / relres);
-    int imax = std::min(budget - used, 150), icode = 0;
+    const bool fp64_inner = fails >= 2;
+    double itol = std::max(fails == 1 ? 1e-3 : 1e-2, 0.5 * target / relres);
+    int imax = std::min(budget - used, fp64_inner ? 50 : 150), icode = 0;
     if ((s = bicgstab_run(fp64_inner ? ops.fp64 : ops.mixed, ops.ctx, d, r, n, &itol, &imax, &icode, ws, st, ops.P,
                           ops.ctx)))
       break;
+    if (solver_trace())
+      std::fprintf(stderr, "[ves3d refine]   inner (%s) %d iterations, code %d, relres %.3e\n",
+                   fp64_inner ? "FP64" : "mixed", imax, icode, itol);
     used += imax;
     if ((s = lincomb_f64(n, 1.0, x, 1.0, d, 0.0, nullptr, x, st))) break;
   }
@@ -1592,6 +1614,7 @@ int mixed_refinement(const SolveOps& ops, double* x, const double* b, long n, do
   if (outer_out) *outer_out = outer;
   if (inner_out) *inner_out = used;
   dfree(r);
+  dfree(rp);
   dfree(d);
   dfree(ax);
   dfree(ws);
