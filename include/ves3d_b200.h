@@ -166,8 +166,9 @@ enum ves3d_surface_op {
   VES3D_OP_GRAD = 1,         /* scalar -> vector: surface gradient                         */
   VES3D_OP_DIV = 2,          /* vector -> scalar: surface divergence                       */
   VES3D_OP_LIN_MEANCURV = 3, /* vector -> scalar: linearised mean curvature                */
-  VES3D_OP_LIN_BENDING = 4,  /* vector -> vector: linear bending traction (kappa)          */
-  VES3D_OP_BENDING = 5,      /* (in unused) -> vector: bending traction of the surfaces    */
+  VES3D_OP_LIN_BENDING = 4,  /* vector -> vector: linear bending traction -kappa (Lap h + 2h(H^2-K)) n, h = H_lin(x) */
+  VES3D_OP_BENDING = 5,      /* (in unused) -> vector: bending traction -kappa (Lap H + 2H(H^2-K)) n
+                              * (bending_coeff = -bending_modulus, src/VesicleProps.cc:39-41) */
   VES3D_OP_TENSION = 6,      /* scalar -> vector: tension traction 2 sigma H n + grad sigma */
   VES3D_OP_IMPLICIT_MATVEC = 7, /* [u;sigma] -> [u - S f ; -div S f], f = linbend(dt u) + tension(sigma) */
   VES3D_OP_IMPLICIT_RHS = 8,    /* (in unused) -> [u_inf + S f_b ; div(u_inf + S f_b)]       */

@@ -8,6 +8,7 @@ Formulas follow (reference file:line):
   surface gradient / divergence                Surface::grad / div         src/Surface.cc:325-379
   linearised mean curvature                    Surface::linearizedMeanCurv src/Surface.cc:530-569
   bending, linear bending, tension forces      InterfacialForce            src/InterfacialForce.cc:21-125
+  bending coefficient -kappa                   VesicleProperties::update   src/VesicleProps.cc:39-41
   gravity traction (explicit and linearised)   InterfacialForce::gravityForce src/InterfacialForce.cc:127-184
   area, volume, centres                        Surface::area/volume/getCenters src/Surface.cc:378-440
   surface quadrature                           GaussLegendreIntegrator     src/GLIntegrator.cc:33-80
@@ -164,10 +165,13 @@ def lin_mean_curv(xn, geo):
 
 
 def bending_of(h, geo, kappa):
-    """kappa (Lap_s h + 2 h (H^2 - K)) n  (InterfacialForce::bendingForce / linearBendingForce)."""
+    """-kappa (Lap_s h + 2 h (H^2 - K)) n  (InterfacialForce::bendingForce / linearBendingForce,
+    src/InterfacialForce.cc:21-90, scaled by bending_coeff = -bending_modulus,
+    src/VesicleProps.cc:39-41): with the outward normal and H = -1/R on a sphere this is the
+    restoring traction, which lowers the bending energy of a relaxing vesicle."""
     lap = div(grad(h, geo), geo)
     s = lap + 2.0 * h * (geo["H"] ** 2 - geo["K"])
-    return kappa * s[:, None] * geo["n"]
+    return -kappa * s[:, None] * geo["n"]
 
 
 def bending_force(geo, kappa):

@@ -222,3 +222,28 @@ def test_gravity_sedimentation_step():
     assert np.linalg.norm(r) / np.linalg.norm(b) < 3e-9
     # the suspension sinks: mean vertical velocity negative
     assert x[:X.size].reshape(-1, 3, geo["H"].shape[1])[:, 2].mean() < 0
+
+
+def test_time_steps_follow_the_oracle_trajectory():
+    """Three implicit steps of a pair of relaxing vesicles (no background flow): positions
+    after every step follow the oracle's trajectory, and the bending energy falls."""
+    from oracle import sh
+    X, _ = small_suspension(2, P, 54, spacing=2.8)
+    Xo = X.copy()
+    qw = sh.smooth_weights_grid(P)
+    energies = []
+    with StokesVelocity(P) as sv:
+        sv.set_implicit_params(DT, KAPPA, 0.0)
+        for _ in range(3):
+            sv.SetSrcCoord(X)
+            x, it, relres, code = sv.implicit_solve(tol=1e-11, max_iter=800)
+            assert code == 100
+            st = su.ImplicitStep(Xo, P, KAPPA, DT, 0.0)
+            xo, co, io, ro = st.solve(tol=1e-11, max_iter=800)
+            assert co == 100
+            g = st.geo
+            energies.append((g["H"] ** 2 * g["W"] * qw).sum())
+            X = X + DT * x[:X.size]
+            Xo = Xo + DT * xo[:X.size]
+            assert rel_err(X, Xo) < 1e-11
+    assert energies[0] > energies[1] > energies[2]

@@ -144,3 +144,27 @@ def test_poly_implicit_step_single_order_is_uniform():
     assert np.abs(Q.matvec(2 * a - b) - (2 * Q.matvec(a) - Q.matvec(b))).max() < 1e-12 * np.abs(Q.matvec(a)).max()
     c = Q.to_coef(a)
     assert np.abs(Q.to_coef(Q.to_grid(c)) - c).max() < 1e-12
+
+
+def test_relaxing_vesicle_loses_bending_energy():
+    """The bending traction is restoring (the reference's bending_coeff = -bending_modulus,
+    src/VesicleProps.cc:39-41): implicit steps of a free, perturbed ellipsoid lower its
+    bending energy every step and keep its area and volume (local inextensibility)."""
+    from ves3d_b200 import workloads
+    p, dt = 8, 0.01
+    X = workloads.shape(p, np.zeros(3), semi_axes=(1.0, 1.0, 0.6), deg=4, amp=0.05,
+                        rng=np.random.default_rng(1)).reshape(-1)
+    qw = sh.smooth_weights_grid(p)
+    E, A, V = [], [], []
+    for _ in range(3):
+        st = su.ImplicitStep(X, p, 0.05, dt, 0.0)
+        x, code, it, rr = st.solve(tol=1e-10, max_iter=500)
+        assert code == 100
+        g = st.geo
+        E.append((g["H"] ** 2 * g["W"] * qw).sum())
+        a, v, _ = su.integrals(X, p)
+        A.append(a[0])
+        V.append(v[0])
+        X = X + dt * x[:X.size]
+    assert E[0] > E[1] > E[2]
+    assert abs(A[-1] / A[0] - 1) < 1e-5 and abs(V[-1] / V[0] - 1) < 1e-5

@@ -114,15 +114,17 @@ __global__ void k_linH_combine(const double* __restrict__ duu, const double* __r
   out[g] = 0.5 * (o[2 * ng] * a - 2.0 * o[1 * ng] * m + o[0 * ng] * c2);
 }
 
-// bending traction from h and its Laplace-Beltrami lap: kappa (lap + 2 h (H^2 - K)) n,
-// written to out (AxisMajor vector) with out = add + that if add is given.
+// bending traction from h and its Laplace-Beltrami lap: -kappa (lap + 2 h (H^2 - K)) n
+// (InterfacialForce::bendingForce scaled by bending_coeff = -bending_modulus,
+// src/VesicleProps.cc:39-41; restoring with the outward normal), written to out
+// (AxisMajor vector) with out = add + that if add is given; kappa is the bending modulus.
 __global__ void k_bend_combine(const double* __restrict__ h, const double* __restrict__ lap,
                                const double* __restrict__ geo, long N, int ng, double kappa,
                                const double* __restrict__ add, double* __restrict__ out, long geo_nv) {
   FOR_POINTS(N)
   const double* o = GEO_OF(v);
   const double H = o[13 * ng], K = o[14 * ng];
-  const double s = kappa * (lap[g] + 2.0 * h[g] * (H * H - K));
+  const double s = -kappa * (lap[g] + 2.0 * h[g] * (H * H - K));
 #pragma unroll
   for (int c = 0; c < 3; c++) {
     const long i = v * 3 * ng + c * ng + k;
