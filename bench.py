@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-implicit", action="store_true", help="skip the implicit-step measurement")
     ap.add_argument("--no-poly", action="store_true", help="skip the polydisperse measurement")
+    ap.add_argument("--no-sed", action="store_true", help="skip the sedimentation (implicit polydisperse) measurement")
+    ap.add_argument("--sed-steps", type=int, default=2)
     ap.add_argument("--no-alt", action="store_true", help="skip the measurement of the other precision form")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default far-field launch shape")
     return ap.parse_args()
@@ -444,6 +446,80 @@ def polydisperse_measurement(precision, local, stream):
             "error_vs_fp64_oracle": {"max_rel": worst, "sample": "all points of 2 vesicles with p <= 16"}}
 
 
+SEDIMENTATION = dict(workload="c5_2048ves_sed", dt=0.01, kappa=0.05, excess_density=1.0, gravity=(0.0, 0.0, -1.0),
+                     tol=1e-8, max_iter=1000, precond="self_block", refresh=10, total_steps=200)
+
+
+def sedimentation_measurement(local, stream, steps=2):
+    """Implicit steps of the sedimenting 2048-vesicle suspension (p in {12,16}, 25% volume
+    fraction, gravity -z, excess density 1) in the mixed form: one polydisperse implicit
+    solve per step (self-block preconditioner rebuilt every 10 steps, previous-step guess
+    after the first), positions advanced by dt u. Device time per step (surface update,
+    self matrices, preconditioner when due, solve), iterations, and at the final step the
+    mixed single-layer evaluation against the FP64 one on N(0,1) densities."""
+    import torch
+    from ves3d_b200 import workloads
+    from ves3d_b200.stokes_velocity import PolydisperseStokesVelocity
+    c = SEDIMENTATION
+    cfg = workloads.POLYDISPERSE[c["workload"]]
+    X, _, orders = workloads.polydisperse(**cfg)
+    N = X.size // 3
+    sv = PolydisperseStokesVelocity("mixed", device=local)
+    sv.set_implicit_params(c["dt"], c["kappa"], 0.0)
+    sv.set_gravity(c["excess_density"], c["gravity"])
+    sv.set_precond(c["precond"], c["refresh"])
+    recs, xp = [], None
+    for k in range(steps):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sv.SetSrcCoord(X, orders)
+        x, it, rr, code = sv.implicit_solve(x0=xp, tol=c["tol"], max_iter=c["max_iter"])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        st = sv.solver_stats()
+        recs.append({"step": k + 1, "ms": e0.elapsed_time(e1), "inner_iterations": it, "fp64_refinements": st["outer"],
+                     "relres_fp64": rr, "code": code, "guess": "zero" if xp is None else "previous step"})
+        X = X + c["dt"] * x[:X.size]
+        xp = x
+    uz = float(np.mean(np.concatenate([x[3 * o + 2 * n:3 * o + 3 * n] for o, n in _vesicle_spans(orders)])))
+    # velocity error of the mixed evaluation at the final surfaces
+    f = np.random.default_rng(cfg["seed"] + 7).standard_normal(X.size)
+    sv.SetSrcCoord(X, orders)
+    sv.SetDensitySL(f)
+    vm = sv()
+    sv.close()
+    with PolydisperseStokesVelocity("fp64", device=local) as s64:
+        s64.SetSrcCoord(X, orders)
+        s64.SetDensitySL(f)
+        v64 = s64()
+    err = float(np.abs(vm - v64).max() / np.abs(v64).max())
+    ms = [r["ms"] for r in recs]
+    later = ms[1:] if len(ms) > 1 else ms
+    counts = {int(p): int((orders == p).sum()) for p in np.unique(orders)}
+    return {"workload": f"{c['workload']}: 2048 vesicles, p counts {counts}, {N} points, 25% volume fraction, "
+                        f"gravity -z, excess density 1, dt {c['dt']}, bending modulus {c['kappa']}",
+            "form": "mixed (FP32 far field in the inner solves, FP64 refinement residuals), self-block "
+                    "preconditioner (FP32, rebuilt every 10 steps), previous-step guess",
+            "steps": recs, "ms_per_step": statistics.mean(later),
+            "point_steps_per_s": N / (statistics.mean(later) * 1e-3),
+            "mean_inner_iterations": statistics.mean(r["inner_iterations"] for r in recs),
+            "extrapolated_s_for_200_steps": statistics.mean(later) * 1e-3 * c["total_steps"],
+            "extrapolated": f"{steps} of {c['total_steps']} steps run; the total is the mean later-step time x 200",
+            "mean_vertical_velocity": uz,
+            "velocity_error_final_step": {"max_rel": err, "what": "mixed vs FP64 single-layer evaluation, "
+                                          "N(0,1) densities on the final surfaces, all points"}}
+
+
+def _vesicle_spans(orders):
+    o = 0
+    for p in orders:
+        n = 2 * int(p) * (int(p) + 1)
+        yield o, n
+        o += n
+
+
 def alt_precision_measurement(precision, X, f, p, local, stream, steps, warmup):
     """The same C2 evaluation in the other precision form (device time per step, L2
     flushed between steps), its far-field roofline fraction and its error against the
@@ -646,6 +722,8 @@ def run_ours(args, world, rank, local):
             result["implicit_step"] = implicit_step_measurement(local, stream)
         if world == 1 and not args.no_poly:
             result["polydisperse"] = polydisperse_measurement(args.precision, local, stream)
+        if world == 1 and not args.no_sed:
+            result["sedimentation"] = sedimentation_measurement(local, stream, args.sed_steps)
         if world == 1 and not args.no_cpu_baseline:
             cb = cpu_reference_rate(X, f, p)
             result["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}

@@ -110,6 +110,9 @@ CONFIGS = {
 POLYDISPERSE = {
     # 4096 vesicles, p ~ U{8,12,16,24}, radii ~ U[0.7,1.3], SH-perturbed ellipsoids, 20% volume fraction
     "c3_4096ves_poly": dict(n_ves=4096, seed=1002),
+    # 2048 vesicles, p ~ U{12,16}, radii ~ U[0.7,1.3], 25% volume fraction: the sedimentation
+    # workload (gravity -z, excess density 1, bending modulus 0.05, dt 0.01)
+    "c5_2048ves_sed": dict(n_ves=2048, orders=(12, 16), radius=(0.7, 1.3), volume_fraction=0.25, seed=1004),
 }
 
 
