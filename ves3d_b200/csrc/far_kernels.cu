@@ -189,13 +189,18 @@ __global__ void __launch_bounds__(512) k_far_f64_segT(const double* __restrict__
 // ------------------------------------------------------------------------------------
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 
-__global__ void __launch_bounds__(512) k_far_f32_seg(const double* __restrict__ pos, const double* __restrict__ den,
-                                                     const long* __restrict__ off, long N, int seg_tiles, int v0,
-                                                     double* __restrict__ part) {
+// NP packed target pairs per thread (2 NP targets): target j of thread i in chunk c0 is
+// c0 + i + j * blockDim.x. NP = 2 reads each staged source once for four targets and gives
+// the scheduler two independent chains per source.
+template <int NP>
+__global__ void __launch_bounds__(512) k_far_f32_segT(const double* __restrict__ pos, const double* __restrict__ den,
+                                                      const long* __restrict__ off, long N, int seg_tiles, int v0,
+                                                      double* __restrict__ part) {
   // one source = 6 broadcast float2: (x,x) (y,y) (z,z) (dx,dx) (dy,dy) (dz,dz)
   __shared__ __align__(16) float2 sm[kTileF32 * 6];
   __shared__ double cen[3];
   __shared__ double red[3][32];
+  constexpr int T = 2 * NP;
   const int v = v0 + blockIdx.y, seg = blockIdx.x;
   const long t0 = off[v], nt = off[v + 1] - t0;
   const int nthr = blockDim.x;
@@ -227,15 +232,20 @@ __global__ void __launch_bounds__(512) k_far_f32_seg(const double* __restrict__ 
     __syncthreads();
   }
   const double cx = cen[0], cy = cen[1], cz = cen[2];
-  const long c0 = (long)blockIdx.z * 2 * nthr;
-  const long ia = t0 + c0 + threadIdx.x, ib = ia + nthr;
-  const bool va = c0 + threadIdx.x < nt, vb = c0 + threadIdx.x + nthr < nt;
-  const long la = va ? ia : t0, lb = vb ? ib : t0;
-  // negated targets, packed (lane x = target a, lane y = target b)
-  const float2 ntx = make_float2((float)(cx - pos[3 * la]), (float)(cx - pos[3 * lb]));
-  const float2 nty = make_float2((float)(cy - pos[3 * la + 1]), (float)(cy - pos[3 * lb + 1]));
-  const float2 ntz = make_float2((float)(cz - pos[3 * la + 2]), (float)(cz - pos[3 * lb + 2]));
-  double Ax = 0, Ay = 0, Az = 0, Bx = 0, By = 0, Bz = 0;
+  const long c0 = (long)blockIdx.z * T * nthr;
+  // negated targets, packed (lane x = target 2q, lane y = target 2q + 1 of the thread)
+  float2 ntx[NP], nty[NP], ntz[NP];
+#pragma unroll
+  for (int q = 0; q < NP; q++) {
+    const long ja = c0 + threadIdx.x + (long)(2 * q) * nthr, jb = ja + nthr;
+    const long la = t0 + (ja < nt ? ja : 0), lb = t0 + (jb < nt ? jb : 0);
+    ntx[q] = make_float2((float)(cx - pos[3 * la]), (float)(cx - pos[3 * lb]));
+    nty[q] = make_float2((float)(cy - pos[3 * la + 1]), (float)(cy - pos[3 * lb + 1]));
+    ntz[q] = make_float2((float)(cz - pos[3 * la + 2]), (float)(cz - pos[3 * lb + 2]));
+  }
+  double A[T][3];
+#pragma unroll
+  for (int j = 0; j < T; j++) A[j][0] = A[j][1] = A[j][2] = 0.0;
   const long ntiles = (N + kTileF32 - 1) / kTileF32;
   const long tb = (long)seg * seg_tiles, te = min(tb + seg_tiles, ntiles);
   for (long tile = tb; tile < te; tile++) {
@@ -255,51 +265,59 @@ __global__ void __launch_bounds__(512) k_far_f32_seg(const double* __restrict__ 
     __syncthreads();
     int r0[2], r1[2];
     split_tile(s0, ns, t0, t0 + nt, r0[0], r1[0], r0[1], r1[1]);
-    float2 ux = f2(0.f), uy = f2(0.f), uz = f2(0.f);
+    float2 ux[NP], uy[NP], uz[NP];
+#pragma unroll
+    for (int q = 0; q < NP; q++) ux[q] = uy[q] = uz[q] = f2(0.f);
 #pragma unroll
     for (int part_i = 0; part_i < 2; part_i++) {
 #pragma unroll 4
       for (int k = r0[part_i]; k < r1[part_i]; k++) {
-        const float4* q = reinterpret_cast<const float4*>(sm + 6 * k);
-        const float4 q0 = q[0], q1 = q[1], q2 = q[2];
+        const float4* qs = reinterpret_cast<const float4*>(sm + 6 * k);
+        const float4 q0 = qs[0], q1 = qs[1], q2 = qs[2];
         const float2 sx = make_float2(q0.x, q0.y), sy = make_float2(q0.z, q0.w);
         const float2 sz = make_float2(q1.x, q1.y), dx_ = make_float2(q1.z, q1.w);
         const float2 dy_ = make_float2(q2.x, q2.y), dz_ = make_float2(q2.z, q2.w);
-        const float2 rx = __fadd2_rn(sx, ntx), ry = __fadd2_rn(sy, nty), rz = __fadd2_rn(sz, ntz);
-        float2 r2 = __fmul2_rn(rx, rx);
-        r2 = __ffma2_rn(ry, ry, r2);
-        r2 = __ffma2_rn(rz, rz, r2);
-        // hardware reciprocal square root, unrefined: its error (a few 1e-7 relative per
-        // pair) averages out in the sum and stays below the FP32 rounding of the
-        // coordinates; a Newton step would cost ~20% more FP32 instructions per pair
-        const float2 y = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
-        const float2 y2 = __fmul2_rn(y, y);
-        float2 dot = __fmul2_rn(rx, dx_);
-        dot = __ffma2_rn(ry, dy_, dot);
-        dot = __ffma2_rn(rz, dz_, dot);
-        const float2 cc = __fmul2_rn(dot, y2);
-        ux = __ffma2_rn(__ffma2_rn(cc, rx, dx_), y, ux);
-        uy = __ffma2_rn(__ffma2_rn(cc, ry, dy_), y, uy);
-        uz = __ffma2_rn(__ffma2_rn(cc, rz, dz_), y, uz);
+#pragma unroll
+        for (int q = 0; q < NP; q++) {
+          const float2 rx = __fadd2_rn(sx, ntx[q]), ry = __fadd2_rn(sy, nty[q]), rz = __fadd2_rn(sz, ntz[q]);
+          float2 r2 = __fmul2_rn(rx, rx);
+          r2 = __ffma2_rn(ry, ry, r2);
+          r2 = __ffma2_rn(rz, rz, r2);
+          // unrefined hardware reciprocal square root: its error (a few 1e-7 relative per
+          // pair) averages out in the sum and stays below the FP32 rounding of the
+          // coordinates; a Newton step would cost ~20% more FP32 instructions per pair
+          const float2 y = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
+          const float2 y2 = __fmul2_rn(y, y);
+          float2 dot = __fmul2_rn(rx, dx_);
+          dot = __ffma2_rn(ry, dy_, dot);
+          dot = __ffma2_rn(rz, dz_, dot);
+          const float2 cc = __fmul2_rn(dot, y2);
+          ux[q] = __ffma2_rn(__ffma2_rn(cc, rx, dx_), y, ux[q]);
+          uy[q] = __ffma2_rn(__ffma2_rn(cc, ry, dy_), y, uy[q]);
+          uz[q] = __ffma2_rn(__ffma2_rn(cc, rz, dz_), y, uz[q]);
+        }
       }
     }
-    Ax += ux.x;
-    Ay += uy.x;
-    Az += uz.x;
-    Bx += ux.y;
-    By += uy.y;
-    Bz += uz.y;
+#pragma unroll
+    for (int q = 0; q < NP; q++) {
+      A[2 * q][0] += ux[q].x;
+      A[2 * q][1] += uy[q].x;
+      A[2 * q][2] += uz[q].x;
+      A[2 * q + 1][0] += ux[q].y;
+      A[2 * q + 1][1] += uy[q].y;
+      A[2 * q + 1][2] += uz[q].y;
+    }
   }
   double* P = part + (long)seg * 3 * N;
-  if (va) {
-    P[3 * ia] = Ax;
-    P[3 * ia + 1] = Ay;
-    P[3 * ia + 2] = Az;
-  }
-  if (vb) {
-    P[3 * ib] = Bx;
-    P[3 * ib + 1] = By;
-    P[3 * ib + 2] = Bz;
+#pragma unroll
+  for (int j = 0; j < T; j++) {
+    const long jj = c0 + threadIdx.x + (long)j * nthr;
+    if (jj < nt) {
+      const long g = t0 + jj;
+      P[3 * g] = A[j][0];
+      P[3 * g + 1] = A[j][1];
+      P[3 * g + 2] = A[j][2];
+    }
   }
 }
 
@@ -327,7 +345,7 @@ __global__ void k_far_reduce(const double* __restrict__ part, int nseg, const lo
 struct FarShape {
   int waves = 8;
   int chunk_max = 1024;
-  int tpt = 2;  // targets per thread (FP64 form: 2 or 4; the FP32 form packs 2)
+  int tpt = 2;  // targets per thread, 2 or 4 (the FP32 form packs them in pairs)
 };
 
 int far_segments(long nves, long N, int tile, int nthr, int waves, int* seg_tiles) {
@@ -359,7 +377,7 @@ static int launch_far_shape(const FarShape& sh, bool mixed, const double* pos, c
   long nthr_sum = 0, nchunk_tot = 0;
   for (int g = 0; g < ngroups; g++) {
     int nc, nt;
-    chunking(groups[g].nt, sh.chunk_max, mixed ? 2 : sh.tpt, &nc, &nt);
+    chunking(groups[g].nt, sh.chunk_max, sh.tpt, &nc, &nt);
     nthr_sum += (long)nt * groups[g].nv;
     nchunk_tot += (long)nc * groups[g].nv;
   }
@@ -374,10 +392,12 @@ static int launch_far_shape(const FarShape& sh, bool mixed, const double* pos, c
   for (int g = 0; g < ngroups; g++) {
     if (groups[g].nv <= 0) continue;
     int nchunk, nthr;
-    chunking(groups[g].nt, sh.chunk_max, mixed ? 2 : sh.tpt, &nchunk, &nthr);
+    chunking(groups[g].nt, sh.chunk_max, sh.tpt, &nchunk, &nthr);
     dim3 grid(nseg, (unsigned)groups[g].nv, nchunk);
-    if (mixed)
-      k_far_f32_seg<<<grid, nthr, 0, st>>>(pos, den, off, N, seg_tiles, (int)groups[g].v0, part);
+    if (mixed && sh.tpt == 4)
+      k_far_f32_segT<2><<<grid, nthr, 0, st>>>(pos, den, off, N, seg_tiles, (int)groups[g].v0, part);
+    else if (mixed)
+      k_far_f32_segT<1><<<grid, nthr, 0, st>>>(pos, den, off, N, seg_tiles, (int)groups[g].v0, part);
     else if (sh.tpt == 4)
       k_far_f64_segT<4><<<grid, nthr, 0, st>>>(pos, den, off, N, seg_tiles, (int)groups[g].v0, part);
     else
@@ -461,7 +481,6 @@ int launch_far_groups(bool mixed, const double* pos, const double* den, const lo
     if (!have && cap == cudaStreamCaptureStatusNone) {
       std::vector<FarShape> cands;
       for (int tpt : {2, 4}) {
-        if (mixed && tpt != 2) continue;
         for (int chunk : {1024, 512})
           for (int waves : {4, 8, 16}) cands.push_back(FarShape{waves, chunk, tpt});
       }
