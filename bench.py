@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--no-implicit", action="store_true", help="skip the implicit-step measurement")
     ap.add_argument("--no-poly", action="store_true", help="skip the polydisperse measurement")
     ap.add_argument("--no-sed", action="store_true", help="skip the sedimentation (implicit polydisperse) measurement")
-    ap.add_argument("--sed-steps", type=int, default=2)
+    ap.add_argument("--sed-steps", type=int, default=3)
     ap.add_argument("--no-alt", action="store_true", help="skip the measurement of the other precision form")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default far-field launch shape")
     return ap.parse_args()
@@ -453,8 +453,9 @@ SEDIMENTATION = dict(workload="c5_2048ves_sed", dt=0.01, kappa=0.05, excess_dens
 def sedimentation_measurement(local, stream, steps=2):
     """Implicit steps of the sedimenting 2048-vesicle suspension (p in {12,16}, 25% volume
     fraction, gravity -z, excess density 1) in the mixed form: one polydisperse implicit
-    solve per step (self-block preconditioner rebuilt every 10 steps, previous-step guess
-    after the first), positions advanced by dt u. Device time per step (surface update,
+    solve per step (self-block preconditioner rebuilt every 10 steps; guess: zero, then the
+    previous solution, then the residual-minimising combination of the two previous ones),
+    positions advanced by dt u. Device time per step (surface update,
     self matrices, preconditioner when due, solve), iterations, and at the final step the
     mixed single-layer evaluation against the FP64 one on N(0,1) densities."""
     import torch
@@ -468,22 +469,33 @@ def sedimentation_measurement(local, stream, steps=2):
     sv.set_implicit_params(c["dt"], c["kappa"], 0.0)
     sv.set_gravity(c["excess_density"], c["gravity"])
     sv.set_precond(c["precond"], c["refresh"])
-    recs, xp = [], None
+    recs, hist = [], []
     for k in range(steps):
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         sv.SetSrcCoord(X, orders)
-        x, it, rr, code = sv.implicit_solve(x0=xp, tol=c["tol"], max_iter=c["max_iter"])
+        extra = {}
+        if len(hist) >= 2:
+            # residual-minimising combination of the two previous solutions (their span
+            # holds the linear extrapolation in time)
+            x0, w, rr0 = sv.implicit_combine([hist[-1], hist[-2]])
+            extra = {"guess": "combination of the 2 previous solutions", "guess_weights": [float(a) for a in w],
+                     "guess_relres": {"previous": float(rr0[0]), "combination": float(rr0[-1])}}
+        else:
+            x0 = hist[-1] if hist else None
+            extra = {"guess": "previous step" if hist else "zero"}
+        x, it, rr, code = sv.implicit_solve(x0=x0, tol=c["tol"], max_iter=c["max_iter"])
         e1.record(stream)
         torch.cuda.synchronize()
         st = sv.solver_stats()
-        recs.append({"step": k + 1, "ms": e0.elapsed_time(e1), "inner_iterations": it, "fp64_refinements": st["outer"],
-                     "relres_fp64": rr, "code": code, "guess": "zero" if xp is None else "previous step"})
+        recs.append(dict({"step": k + 1, "ms": e0.elapsed_time(e1), "inner_iterations": it,
+                          "fp64_refinements": st["outer"], "relres_fp64": rr, "code": code}, **extra))
         X = X + c["dt"] * x[:X.size]
-        xp = x
+        hist = (hist + [x])[-2:]
     uz = float(np.mean(np.concatenate([x[3 * o + 2 * n:3 * o + 3 * n] for o, n in _vesicle_spans(orders)])))
+    del hist
     # velocity error of the mixed evaluation at the final surfaces
     f = np.random.default_rng(cfg["seed"] + 7).standard_normal(X.size)
     sv.SetSrcCoord(X, orders)
@@ -496,17 +508,19 @@ def sedimentation_measurement(local, stream, steps=2):
         v64 = s64()
     err = float(np.abs(vm - v64).max() / np.abs(v64).max())
     ms = [r["ms"] for r in recs]
-    later = ms[1:] if len(ms) > 1 else ms
+    # the steady form of a step is the one with two previous solutions (third step on)
+    later = ms[2:] if len(ms) > 2 else ms[1:] if len(ms) > 1 else ms
     counts = {int(p): int((orders == p).sum()) for p in np.unique(orders)}
     return {"workload": f"{c['workload']}: 2048 vesicles, p counts {counts}, {N} points, 25% volume fraction, "
                         f"gravity -z, excess density 1, dt {c['dt']}, bending modulus {c['kappa']}",
             "form": "mixed (FP32 far field in the inner solves, FP64 refinement residuals), self-block "
-                    "preconditioner (FP32, rebuilt every 10 steps), previous-step guess",
+                    "preconditioner (FP32, rebuilt every 10 steps), guess from the previous solutions",
             "steps": recs, "ms_per_step": statistics.mean(later),
             "point_steps_per_s": N / (statistics.mean(later) * 1e-3),
             "mean_inner_iterations": statistics.mean(r["inner_iterations"] for r in recs),
             "extrapolated_s_for_200_steps": statistics.mean(later) * 1e-3 * c["total_steps"],
-            "extrapolated": f"{steps} of {c['total_steps']} steps run; the total is the mean later-step time x 200",
+            "extrapolated": f"{steps} of {c['total_steps']} steps run; the total is the mean time of the steps from "
+                            f"the third on (two previous solutions available) x {c['total_steps']}",
             "mean_vertical_velocity": uz,
             "velocity_error_final_step": {"max_rel": err, "what": "mixed vs FP64 single-layer evaluation, "
                                           "N(0,1) densities on the final surfaces, all points"}}

@@ -153,6 +153,14 @@ int ves3d_svp_implicit_solve(ves3d_svp* g, const double* x0, double* x, double* 
                              int is_device);
 /* Last solve: outer refinements (FP64 matvecs) and inner iterations. */
 int ves3d_svp_solver_stats(ves3d_svp* g, int* outer, int* inner);
+/* Residual-minimising combination of n_cand (1..8) candidate grid vectors as the start of
+ * the next ves3d_svp_implicit_solve (as ves3d_sv_implicit_combine; e.g. the last two
+ * solutions, whose span holds the linear extrapolation in time). Candidate images come from
+ * the operator the inner solves use (FP32 far field in a mixed context); the FP64
+ * right-hand side is kept for the solve on the same surfaces. weights[n_cand]; relres
+ * [n_cand + 1]: each candidate's relative residual, then the combination's. */
+int ves3d_svp_implicit_combine(ves3d_svp* g, int n_cand, const double* const* cand, double* x0, double* weights,
+                               double* relres, int is_device);
 
 /* ---------------------------------------------------------------------------
  * Surface geometry, tractions and the globally implicit step on the context's surfaces

@@ -90,3 +90,40 @@ def test_poly_single_order_is_the_uniform_step():
         xb, ib, rb, cb = b.implicit_solve(tol=1e-10, max_iter=600)
     assert ca == cb == 100
     assert rel_err(xb[:X.size], xa[:X.size]) < 1e-8
+
+
+def test_poly_combination_of_guesses(case):
+    """The residual-minimising combination over the polydisperse operator: a converged
+    solution among the candidates gets weight ~1 and the combination keeps its residual;
+    a non-finite candidate gets weight 0; two earlier solutions of a moving suspension
+    (whose span holds the linear extrapolation in time) start the next solve closer than
+    the last one alone."""
+    X, orders, step, b = case
+    with PolydisperseStokesVelocity("fp64") as sv:
+        sv.SetSrcCoord(X, orders)
+        sv.set_implicit_params(DT, KAPPA, 0.0)
+        sv.set_gravity(1.0, (0.0, 0.0, -1.0))
+        sv.set_precond("self_block")
+        x, it, relres, code = sv.implicit_solve(tol=1e-10, max_iter=600)
+        junk = np.random.default_rng(3).standard_normal(x.size)
+        bad = np.full(x.size, np.nan)
+        x0, w, rr = sv.implicit_combine([junk, x, bad])
+        assert abs(w[1] - 1.0) < 1e-6 and w[2] == 0.0 and abs(w[0]) < 1e-6
+        assert rr[-1] < 1e-9 and not np.isfinite(rr[2])
+        assert true_relres(step, b, x0) < 3e-9
+        # three steps: the combination of the two previous solutions against the last one
+        Xk, sols = X.copy(), []
+        for k in range(3):
+            sv.SetSrcCoord(Xk, orders)
+            if k < 2:
+                xk, _, _, ck = sv.implicit_solve(x0=sols[-1] if sols else None, tol=1e-10, max_iter=600)
+                assert ck == 100
+                sols.append(xk)
+                Xk = Xk + DT * xk[:X.size]
+        x0, w, rr = sv.implicit_combine([sols[-1], sols[-2]])
+        assert rr[-1] < 0.5 * rr[0], (w, rr)
+        xn, itn, rn, cn = sv.implicit_solve(x0=x0, tol=1e-10, max_iter=600)
+        assert cn == 100
+        stepn = su.PolyImplicitStep(Xk, orders, KAPPA, DT, 0.0, excess_density=1.0, gravity=(0.0, 0.0, -1.0))
+        bn = stepn.to_coef(stepn.rhs())
+        assert true_relres(stepn, bn, xn) < 3e-10

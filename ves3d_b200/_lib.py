@@ -70,6 +70,7 @@ SIGNATURES = [
     ("ves3d_svp_set_precond", _i, [_vp, _i, _i]),
     ("ves3d_svp_implicit_solve", _i, [_vp, _vp, _vp, ctypes.POINTER(_d), ctypes.POINTER(_i), ctypes.POINTER(_i), _i]),
     ("ves3d_svp_solver_stats", _i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
+    ("ves3d_svp_implicit_combine", _i, [_vp, _i, ctypes.POINTER(_vp), _vp, _vp, _vp, _i]),
     ("ves3d_sv_solver_stats", _i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     ("ves3d_sv_integrals", _i, [_vp, _vp, _vp, _vp, _i]),
     ("ves3d_sv_set_precond", _i, [_vp, _i]),

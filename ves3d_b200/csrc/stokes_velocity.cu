@@ -2148,6 +2148,11 @@ struct ves3d_svp {
   std::vector<long> coff;  // first SH unknown of each group's [u; sigma] coefficients
   double* sws = nullptr;   // solve workspace: BiCGStab, coefficients, right-hand side, grid
   long sws_cap = 0;
+  // right-hand side (coefficients) of the current surfaces and parameters, kept between a
+  // guess combination and the solve that follows it
+  double* rhs = nullptr;
+  long rhs_cap = 0;
+  bool rhs_valid = false;
   void drop_graph() {
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (graph) cudaGraphDestroy(graph);
@@ -2172,6 +2177,7 @@ struct ves3d_svp {
     free_groups();
     free_global();
     dfree(sws);
+    dfree(rhs);
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
     if (stream) cudaStreamDestroy(stream);
@@ -2210,7 +2216,10 @@ int ves3d_svp_destroy(ves3d_svp* g) {
 }
 
 int ves3d_svp_set_src_coord(ves3d_svp* g, const double* S, const int* orders, long n_ves, int is_device) {
-  if (g) g->drop_graph();
+  if (g) {
+    g->drop_graph();
+    g->rhs_valid = false;
+  }
   VES3D_ARG(g && S && orders && n_ves >= 1, "bad arguments");
   VES3D_CK(cudaSetDevice(g->device));
   // runs of equal order
@@ -2481,8 +2490,30 @@ int svp_precond_cb(void* ctx, const double* x, double* y) {
   return VES3D_OK;
 }
 
-// right-hand side in coefficients (FP64 far field)
+// right-hand side in coefficients (FP64 far field), from the cache when the surfaces and
+// parameters are unchanged since it was computed
+int svp_rhs_compute(ves3d_svp* g, double* b);
 int svp_rhs(ves3d_svp* g, double* b) {
+  int s;
+  const long nsh = g->coff.back();
+  if (g->rhs_valid && g->rhs_cap >= nsh) {
+    VES3D_CK(cudaMemcpyAsync(b, g->rhs, nsh * sizeof(double), cudaMemcpyDeviceToDevice, g->stream));
+    return VES3D_OK;
+  }
+  if ((s = svp_rhs_compute(g, b))) return s;
+  if (g->rhs_cap < nsh) {
+    dfree(g->rhs);
+    g->rhs = nullptr;
+    g->rhs_cap = 0;
+    if ((s = dalloc(&g->rhs, nsh))) return s;
+    g->rhs_cap = nsh;
+  }
+  VES3D_CK(cudaMemcpyAsync(g->rhs, b, nsh * sizeof(double), cudaMemcpyDeviceToDevice, g->stream));
+  g->rhs_valid = true;
+  return VES3D_OK;
+}
+
+int svp_rhs_compute(ves3d_svp* g, double* b) {
   int s;
   for (ves3d_sv* sv : g->grp) {
     ImplicitWork iw;
@@ -2544,6 +2575,7 @@ int ves3d_svp_set_implicit_params(ves3d_svp* g, double dt, double kappa, double 
   g->dt = dt;
   g->kappa = kappa;
   g->shear = shear_rate;
+  g->rhs_valid = false;
   return VES3D_OK;
 }
 
@@ -2553,6 +2585,7 @@ int ves3d_svp_set_gravity(ves3d_svp* g, double excess_density, double gx, double
   g->grav[0] = gx;
   g->grav[1] = gy;
   g->grav[2] = gz;
+  g->rhs_valid = false;
   return VES3D_OK;
 }
 
@@ -2619,6 +2652,97 @@ int ves3d_svp_implicit_solve(ves3d_svp* g, const double* x0, double* x, double* 
   if (!s) s = svp_coef_to_grid(g, dc, dg);
   if (!s) s = copy_out(x, dg, ng4, is_device, g->stream);
   cudaStreamSynchronize(g->stream);
+  return s;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+// Residual-minimising combination of candidate guesses for the next implicit solve of a
+// polydisperse suspension (the uniform form: ves3d_sv_implicit_combine). The candidates'
+// images come from the operator the inner solves use (the FP32 far field in a mixed
+// context: a guess needs no more, and the solve that follows judges its result in FP64);
+// the right-hand side is FP64 and is kept for that solve.
+int ves3d_svp_implicit_combine(ves3d_svp* g, int n_cand, const double* const* cand, double* x0, double* weights,
+                               double* relres, int is_device) {
+  VES3D_ARG(g != nullptr, "null context");
+  VES3D_ARG(n_cand >= 1 && n_cand <= 8, "n_cand must be in [1, 8]");
+  VES3D_ARG(cand && x0 && weights && relres, "null argument");
+  for (int i = 0; i < n_cand; i++) VES3D_ARG(cand[i] != nullptr, "null candidate");
+  if (g->grp.empty()) {
+    set_error("no surfaces set");
+    return VES3D_ERR_STATE;
+  }
+  VES3D_CK(cudaSetDevice(g->device));
+  int s;
+  if ((s = svp_prepare_implicit(g))) return s;
+  const long nsh = g->coff.back(), ng4 = 4 * g->N;
+  double *b = nullptr, *C = nullptr, *Y = nullptr, *dg = nullptr, *r = nullptr, *scr = nullptr;
+  if ((s = dalloc(&b, nsh))) return s;
+  if ((s = dalloc(&C, nsh * n_cand)) || (s = dalloc(&Y, nsh * n_cand)) || (s = dalloc(&dg, ng4)) ||
+      (s = dalloc(&r, nsh)) || (s = dalloc(&scr, 1024))) {
+    dfree(b); dfree(C); dfree(Y); dfree(dg); dfree(r);
+    return s;
+  }
+  s = svp_rhs(g, b);
+  for (int i = 0; i < n_cand && !s; i++) {
+    s = copy_in(dg, cand[i], ng4, is_device, g->stream);
+    if (!s) s = svp_grid_to_coef(g, dg, C + i * nsh);
+    if (!s) s = svp_matvec_sh(g, C + i * nsh, Y + i * nsh);
+  }
+  std::vector<double> G(n_cand * n_cand, 0.0), h(n_cand, 0.0), a;
+  std::vector<char> ok(n_cand, 1);
+  double bb = 0;
+  if (!s) s = dot_f64(b, b, nsh, scr, &bb, g->stream);
+  const double nb = bb > 0 ? std::sqrt(bb) : 1.0;
+  for (int i = 0; i < n_cand && !s; i++) {
+    s = lincomb_f64(nsh, 1.0, b, -1.0, Y + i * nsh, 0.0, nullptr, r, g->stream);
+    double rr = 0;
+    if (!s) s = dot_f64(r, r, nsh, scr, &rr, g->stream);
+    relres[i] = std::sqrt(rr) / nb;
+    if (!s) s = dot_f64(Y + i * nsh, b, nsh, scr, &h[i], g->stream);
+    for (int j = 0; j <= i && !s; j++) {
+      s = dot_f64(Y + i * nsh, Y + j * nsh, nsh, scr, &G[i * n_cand + j], g->stream);
+      G[j * n_cand + i] = G[i * n_cand + j];
+    }
+    if (!std::isfinite(G[i * n_cand + i]) || !std::isfinite(h[i])) ok[i] = 0;
+  }
+  if (!s) {
+    std::vector<int> idx;
+    for (int i = 0; i < n_cand; i++)
+      if (ok[i] && G[i * n_cand + i] > 0) idx.push_back(i);
+    const int m = (int)idx.size();
+    std::vector<double> Gm(m * m), hm(m), am;
+    for (int i = 0; i < m; i++) {
+      hm[i] = h[idx[i]];
+      for (int j = 0; j < m; j++) Gm[i * m + j] = G[idx[i] * n_cand + idx[j]];
+    }
+    if (m) small_solve(m, Gm, hm, am);
+    for (int i = 0; i < n_cand; i++) weights[i] = 0.0;
+    for (int i = 0; i < m; i++) weights[idx[i]] = am[i];
+    s = cuda_status(cudaMemsetAsync(dg, 0, nsh * sizeof(double), g->stream), "memset", __FILE__, __LINE__);
+    if (!s) s = copy_in(r, b, nsh, 1, g->stream);
+    for (int i = 0; i < m && !s; i++) {
+      s = lincomb_f64(nsh, 1.0, dg, am[i], C + idx[i] * nsh, 0.0, nullptr, dg, g->stream);
+      if (!s) s = lincomb_f64(nsh, 1.0, r, -am[i], Y + idx[i] * nsh, 0.0, nullptr, r, g->stream);
+    }
+    double rr = 0;
+    if (!s) s = dot_f64(r, r, nsh, scr, &rr, g->stream);
+    relres[n_cand] = std::sqrt(rr) / nb;
+    if (!s) {
+      s = copy_in(b, dg, nsh, 1, g->stream);  // coefficients of the combination
+      if (!s) s = svp_coef_to_grid(g, b, dg);
+      if (!s) s = copy_out(x0, dg, ng4, is_device, g->stream);
+    }
+  }
+  cudaStreamSynchronize(g->stream);
+  dfree(b);
+  dfree(C);
+  dfree(Y);
+  dfree(dg);
+  dfree(r);
+  dfree(scr);
   return s;
 }
 

@@ -363,3 +363,20 @@ class PolydisperseStokesVelocity:
         check(lib().ves3d_svp_implicit_solve(self._h, p0, x.ctypes.data, ctypes.byref(t), ctypes.byref(it),
                                              ctypes.byref(code), 0), "implicit_solve")
         return x, it.value, t.value, code.value
+
+    def implicit_combine(self, candidates):
+        """Residual-minimising combination of candidate guesses (grid vectors [u; sigma] of
+        the whole suspension), e.g. the last two solutions. Returns (x0, weights, relres)."""
+        cands = [np.ascontiguousarray(c, dtype=np.float64).reshape(-1) for c in candidates]
+        n = len(cands)
+        if any(c.size != 4 * self.npoints() for c in cands):
+            raise ValueError("candidate size does not match the surfaces")
+        arr = (ctypes.c_void_p * n)(*[c.ctypes.data for c in cands])
+        x0 = np.empty_like(cands[0])
+        w = np.zeros(n)
+        r = np.zeros(n + 1)
+        check(lib().ves3d_svp_implicit_combine(self._h, n, arr, x0.ctypes.data,
+                                               w.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                               r.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 0),
+              "implicit_combine")
+        return x0, w, r
