@@ -144,6 +144,7 @@ struct ves3d_sv {
   double *Sx = nullptr, *Xt = nullptr, *Xp = nullptr, *area = nullptr, *pos = nullptr, *den = nullptr;
   double *SL = nullptr, *Fc = nullptr, *Vc = nullptr, *part = nullptr;
   long* off = nullptr;  // [nves+1] point offsets of the vesicles
+  long off_nves = -1;   // vesicle count the offsets were uploaded for
   // setup scratch (one chunk of vesicles)
   long chunk = 0;
   double *R = nullptr, *Xu = nullptr, *Xut = nullptr, *Xup = nullptr, *K = nullptr, *C = nullptr, *SL3 = nullptr;
@@ -200,6 +201,7 @@ struct ves3d_sv {
     off = nullptr;
     X = F = V = Vself = Vfar = Sx = Xt = Xp = area = pos = den = SL = Fc = Vc = part = nullptr;
     cap_ves = 0;
+    off_nves = -1;
   }
   void free_implicit() {
     dfree(geo);
@@ -290,6 +292,7 @@ size_t scratch_per_vesicle(int p0, int p1, bool fused) {
 
 int alloc_scratch(ves3d_sv* sv) {
   const long want = sv->nves;
+  if (sv->chunk >= want) return VES3D_OK;  // the whole suspension in one chunk already
   const bool fused = use_fused(sv);
   size_t per = scratch_per_vesicle(sv->p, sv->pup, fused) * sizeof(double);
   size_t free_b = 0, total_b = 0;
@@ -504,11 +507,12 @@ int ves3d_sv_set_src_coord(ves3d_sv* sv, const double* S, long n_ves, int is_dev
   const int p0 = sv->p, ng = ngrid_(p0);
   const DevTables& T = sv->tab->d;
   if ((s = copy_in(sv->X, S, (size_t)n_ves * 3 * ng, is_device, sv->stream))) return s;
-  {
+  if (sv->off_nves != n_ves) {  // point offsets of the vesicles, uploaded when the count changes
     std::vector<long> off(n_ves + 1);
     for (long v = 0; v <= n_ves; v++) off[v] = v * ng;
     VES3D_CK(cudaMemcpyAsync(sv->off, off.data(), off.size() * sizeof(long), cudaMemcpyHostToDevice, sv->stream));
     VES3D_CK(cudaStreamSynchronize(sv->stream));
+    sv->off_nves = n_ves;
   }
   if ((s = launch_grid2shc(sv->X, n_ves * 3, p0, T.ana_four, T.ana_leg, T.jf_of_coef, sv->Sx, sv->stream)))
     return s;
