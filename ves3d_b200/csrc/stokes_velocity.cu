@@ -297,9 +297,10 @@ int alloc_scratch(ves3d_sv* sv) {
   size_t per = scratch_per_vesicle(sv->p, sv->pup, fused) * sizeof(double);
   size_t free_b = 0, total_b = 0;
   VES3D_CK(cudaMemGetInfo(&free_b, &total_b));
-  // Scratch budget for one chunk of the self-matrix build: 8 GiB by default, capped at a
-  // third of free memory; VES3D_SCRATCH_MB overrides (e.g. to keep profiler captures small).
-  size_t budget = (size_t)8 << 30;
+  // Scratch budget for one chunk of the self-matrix build: 16 GiB by default (the 512
+  // vesicles of p = 16 take 10.6 GB, one chunk), capped at a third of free memory;
+  // VES3D_SCRATCH_MB overrides (e.g. to keep profiler captures small).
+  size_t budget = (size_t)16 << 30;
   if (const char* env = getenv("VES3D_SCRATCH_MB")) {
     long mb = atol(env);
     if (mb > 0) budget = (size_t)mb << 20;
