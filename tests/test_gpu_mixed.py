@@ -11,7 +11,7 @@ pytestmark = pytest.mark.gpu
 MIXED_TOL = 1e-6
 
 
-@pytest.mark.parametrize("nside,p,seed", [(2, 6, 21), (2, 12, 22)])
+@pytest.mark.parametrize("nside,p,seed", [(2, 6, 21), (2, 12, 22), (2, 12, 31), (3, 8, 34)])
 def test_mixed_vs_oracle(nside, p, seed):
     X, f = small_suspension(nside, p, seed)
     with StokesVelocity(p, precision="mixed") as sv:

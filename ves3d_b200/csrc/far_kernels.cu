@@ -16,7 +16,7 @@
 // Mixed form: coordinates relative to the target vesicle's centroid (differences taken
 // in FP64, rounded to FP32 once per source per CTA), the pair arithmetic in packed FP32
 // (Blackwell f32x2 FMA: both targets of a thread in one instruction), the unrefined
-// hardware reciprocal square root, and the FP32 partial of every source tile added into
+// hardware reciprocal square root, and the FP32 partial of every 120-source sub-tile added into
 // FP64 accumulators. Distinct vesicles must not share points in the mixed form.
 #include <atomic>
 #include <cstdlib>
@@ -31,7 +31,13 @@
 namespace ves3d {
 
 constexpr int kTileF64 = 256;
-constexpr int kTileF32 = 512;
+// FP32 form: 960 sources staged per pair of barriers (46 KB of shared memory, three CTAs
+// per SM), summed in FP32 over sub-tiles of 120 and the sub-tile sums added in FP64.
+// Measured against 512-source tiles summed whole in FP32: 12% shorter launches at 512
+// vesicles, and the far field's error against FP64 about halved (worst of five small
+// suspensions 5.4e-7 instead of 1.09e-6; a sub-tile of 480 gave 1.13e-6 at the same speed)
+constexpr int kTileF32 = 960;
+constexpr int kSubF32 = 120;
 
 // Source sub-ranges of tile [s0, s0 + ns) that lie outside the excluded range [e0, e1).
 __device__ __forceinline__ void split_tile(long s0, int ns, long e0, long e1, int& a0, int& a1, int& b0, int& b1) {
@@ -265,51 +271,55 @@ __global__ void __launch_bounds__(512) k_far_f32_segT(const double* __restrict__
     __syncthreads();
     int r0[2], r1[2];
     split_tile(s0, ns, t0, t0 + nt, r0[0], r1[0], r0[1], r1[1]);
-    float2 ux[NP], uy[NP], uz[NP];
+    for (int sb = 0; sb < ns; sb += kSubF32) {
+      const int se = min(sb + kSubF32, ns);
+      float2 ux[NP], uy[NP], uz[NP];
 #pragma unroll
-    for (int q = 0; q < NP; q++) ux[q] = uy[q] = uz[q] = f2(0.f);
+      for (int q = 0; q < NP; q++) ux[q] = uy[q] = uz[q] = f2(0.f);
 #pragma unroll
-    for (int part_i = 0; part_i < 2; part_i++) {
+      for (int part_i = 0; part_i < 2; part_i++) {
+        const int k0 = max(r0[part_i], sb), k1 = min(r1[part_i], se);
 #pragma unroll 4
-      for (int k = r0[part_i]; k < r1[part_i]; k++) {
-        const float4* qs = reinterpret_cast<const float4*>(sm + 6 * k);
-        const float4 q0 = qs[0], q1 = qs[1], q2 = qs[2];
-        const float2 sx = make_float2(q0.x, q0.y), sy = make_float2(q0.z, q0.w);
-        const float2 sz = make_float2(q1.x, q1.y), dx_ = make_float2(q1.z, q1.w);
-        const float2 dy_ = make_float2(q2.x, q2.y), dz_ = make_float2(q2.z, q2.w);
+        for (int k = k0; k < k1; k++) {
+          const float4* qs = reinterpret_cast<const float4*>(sm + 6 * k);
+          const float4 q0 = qs[0], q1 = qs[1], q2 = qs[2];
+          const float2 sx = make_float2(q0.x, q0.y), sy = make_float2(q0.z, q0.w);
+          const float2 sz = make_float2(q1.x, q1.y), dx_ = make_float2(q1.z, q1.w);
+          const float2 dy_ = make_float2(q2.x, q2.y), dz_ = make_float2(q2.z, q2.w);
 #pragma unroll
-        for (int q = 0; q < NP; q++) {
-          // the differences as scalar adds: the packed ops keep one FMA pipe busy (76% of
-          // cycles) and the scalar ones can go to the other (measured 1% faster)
-          const float2 rx = make_float2(__fadd_rn(sx.x, ntx[q].x), __fadd_rn(sx.y, ntx[q].y));
-          const float2 ry = make_float2(__fadd_rn(sy.x, nty[q].x), __fadd_rn(sy.y, nty[q].y));
-          const float2 rz = make_float2(__fadd_rn(sz.x, ntz[q].x), __fadd_rn(sz.y, ntz[q].y));
-          float2 r2 = __fmul2_rn(rx, rx);
-          r2 = __ffma2_rn(ry, ry, r2);
-          r2 = __ffma2_rn(rz, rz, r2);
-          // unrefined hardware reciprocal square root: its error (a few 1e-7 relative per
-          // pair) averages out in the sum and stays below the FP32 rounding of the
-          // coordinates; a Newton step would cost ~20% more FP32 instructions per pair
-          const float2 y = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
-          const float2 y2 = __fmul2_rn(y, y);
-          float2 dot = __fmul2_rn(rx, dx_);
-          dot = __ffma2_rn(ry, dy_, dot);
-          dot = __ffma2_rn(rz, dz_, dot);
-          const float2 cc = __fmul2_rn(dot, y2);
-          ux[q] = __ffma2_rn(__ffma2_rn(cc, rx, dx_), y, ux[q]);
-          uy[q] = __ffma2_rn(__ffma2_rn(cc, ry, dy_), y, uy[q]);
-          uz[q] = __ffma2_rn(__ffma2_rn(cc, rz, dz_), y, uz[q]);
+          for (int q = 0; q < NP; q++) {
+            // the differences as scalar adds: the packed ops keep one FMA pipe busy (76% of
+            // cycles) and the scalar ones can go to the other (measured 1% faster)
+            const float2 rx = make_float2(__fadd_rn(sx.x, ntx[q].x), __fadd_rn(sx.y, ntx[q].y));
+            const float2 ry = make_float2(__fadd_rn(sy.x, nty[q].x), __fadd_rn(sy.y, nty[q].y));
+            const float2 rz = make_float2(__fadd_rn(sz.x, ntz[q].x), __fadd_rn(sz.y, ntz[q].y));
+            float2 r2 = __fmul2_rn(rx, rx);
+            r2 = __ffma2_rn(ry, ry, r2);
+            r2 = __ffma2_rn(rz, rz, r2);
+            // unrefined hardware reciprocal square root: its error (a few 1e-7 relative per
+            // pair) averages out in the sum and stays below the FP32 rounding of the
+            // coordinates; a Newton step would cost ~20% more FP32 instructions per pair
+            const float2 y = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
+            const float2 y2 = __fmul2_rn(y, y);
+            float2 dot = __fmul2_rn(rx, dx_);
+            dot = __ffma2_rn(ry, dy_, dot);
+            dot = __ffma2_rn(rz, dz_, dot);
+            const float2 cc = __fmul2_rn(dot, y2);
+            ux[q] = __ffma2_rn(__ffma2_rn(cc, rx, dx_), y, ux[q]);
+            uy[q] = __ffma2_rn(__ffma2_rn(cc, ry, dy_), y, uy[q]);
+            uz[q] = __ffma2_rn(__ffma2_rn(cc, rz, dz_), y, uz[q]);
+          }
         }
       }
-    }
 #pragma unroll
-    for (int q = 0; q < NP; q++) {
-      A[2 * q][0] += ux[q].x;
-      A[2 * q][1] += uy[q].x;
-      A[2 * q][2] += uz[q].x;
-      A[2 * q + 1][0] += ux[q].y;
-      A[2 * q + 1][1] += uy[q].y;
-      A[2 * q + 1][2] += uz[q].y;
+      for (int q = 0; q < NP; q++) {
+        A[2 * q][0] += ux[q].x;
+        A[2 * q][1] += uy[q].x;
+        A[2 * q][2] += uz[q].x;
+        A[2 * q + 1][0] += ux[q].y;
+        A[2 * q + 1][1] += uy[q].y;
+        A[2 * q + 1][2] += uz[q].y;
+      }
     }
   }
   double* P = part + (long)seg * 3 * N;
