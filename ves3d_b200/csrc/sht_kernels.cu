@@ -199,16 +199,36 @@ __global__ void __launch_bounds__(256, 2) k_analysis_tc(const double* __restrict
   const int grow = lane >> 2, gcol = lane & 3;
   constexpr int MT = G::ROWS / 8, NT = G::NLON / 8;
   const long ngroups = (nfun + G::FB - 1) / G::FB;
+  // software pipeline: the next group's grid values are loaded into registers while the
+  // current group goes through the DFT and Legendre phases (the kernel was bound by the
+  // latency of these loads: shared memory allows two CTAs per SM)
+  constexpr int U = (G::ROWS * G::NLON + 255) / 256;
+  double pre[U];
+  auto load_group = [&](long g) {
+    const long f0 = g * G::FB;
+    const int nf = g < ngroups ? (int)min((long)G::FB, nfun - f0) : 0;
+    const double* src = in + (nf ? f0 : 0) * G::NLAT * G::NLON;  // no loads past the last group
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int i = tid + u * 256;
+      pre[u] = (i < G::ROWS * G::NLON && i / G::NLON < nf * G::NLAT) ? src[i] : 0.0;
+    }
+  };
+  load_group(blockIdx.x);
   for (long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
     const long f0 = grp * G::FB;
     const int nf = (int)min((long)G::FB, nfun - f0);
-    const double* src = in + f0 * G::NLAT * G::NLON;
     __syncthreads();  // the previous group's sA / sF reads are done
-    for (int i = tid; i < G::ROWS * G::NLON; i += 256) {
-      const int r = i / G::NLON, j = i - r * G::NLON;
-      sA[r * G::LD + j] = r < nf * G::NLAT ? src[i] : 0.0;
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int i = tid + u * 256;
+      if (i < G::ROWS * G::NLON) {
+        const int r = i / G::NLON, j = i - r * G::NLON;
+        sA[r * G::LD + j] = pre[u];
+      }
     }
     __syncthreads();
+    load_group(grp + gridDim.x);
     for (int it = warp; it < MT * NT; it += 8) {
       const int nt = it % NT, mt = it / NT;
       const double* a = sA + (mt * 8 + grow) * G::LD + gcol;
