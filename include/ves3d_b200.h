@@ -299,6 +299,22 @@ int ves3d_sht_forward(const double* X, long n_fun, int p0, int p1, double* S, vo
  * (X_theta) and latitude (X_phi) derivatives as named by the reference; NULL skips. */
 int ves3d_sht_backward(const double* S, long n_fun, int p0, int p1, double* X, double* X_theta,
                        double* X_phi, void* stream);
+/* SHTrans's frequency filters (constructor, src/SHTrans.cc:8-45) written to a host array of
+ * p(p+2) values in the per-function coefficient order (Fourier blocks, degrees ascending):
+ * exponent <= 0 gives lowPassFilter's hard cut (1 for degree n <= filter_freq, else 0),
+ * exponent > 0 lowPassFilterPoly's 1 - (n/filter_freq)^exponent for n < filter_freq, else 0
+ * (the reference's default exponent is 4); filter_freq -1 means 2p/3. Host only. */
+int ves3d_sht_filter_coeffs(int p, int filter_freq, double exponent, double* coeff);
+/* SHTrans::ScaleFreq (src/SHTrans.cc:190-223): shc_out[f][c] = shc_in[f][c] * scale[c] for
+ * n_fun functions of p(p+2) coefficients; device pointers, in place allowed. The arrays are
+ * function-major (the layout of ves3d_sht_forward); the reference's SHTrans keeps each
+ * frequency block of all functions together, with the same per-function scale order. */
+int ves3d_sht_scale_freq(const double* shc_in, long n_fun, int p, const double* scale, double* shc_out,
+                         void* stream);
+/* SHTrans::lowPassFilter / lowPassFilterPoly (src/SHTrans.cc:172-188) of grid functions at
+ * order p: analysis, the filter of ves3d_sht_filter_coeffs, synthesis; in place allowed. */
+int ves3d_sht_lowpass(const double* in, long n_fun, int p, int filter_freq, double exponent, double* out,
+                      void* stream);
 
 /* ---------------------------------------------------------------------------
  * Direct Stokes sums on device pointers.

@@ -125,13 +125,37 @@ class StokesVelocity {
 };
 
 /* SHTrans<Real> on device pointers (forward = Grid2SHC, backward = SHC2Grid with the
- * optional longitude / latitude derivatives of backward_dv / backward_du), in the
- * coefficient order shared by the reference's SHTrans and SphericalHarmonics. */
+ * optional longitude / latitude derivatives of backward_dv / backward_du, the low-pass
+ * filters and ScaleFreq), in the per-function coefficient order shared by the reference's
+ * SHTrans and SphericalHarmonics; coefficient arrays are function-major. */
 template <class Real>
 class SHTrans {
  public:
-  explicit SHTrans(int sh_order, void* stream = 0) : p_(sh_order), stream_(stream) {}
+  /* filter_freq -1 means 2p/3 and filter_exponent is lowPassFilterPoly's exponent, with the
+   * reference constructor's defaults (SHTrans(p, mats, filter_freq, filter_exponent)) */
+  explicit SHTrans(int sh_order, void* stream = 0, int filter_freq = -1, Real filter_exponent = 4.0)
+      : p_(sh_order), stream_(stream), freq_(filter_freq < 0 ? 2 * sh_order / 3 : filter_freq),
+        exponent_(filter_exponent) {}
   int getShOrder() const { return p_; }
+  int getShFilterFreq() const { return freq_; }
+  Real getShFilterExponent() const { return exponent_; }
+  /* the two filters on the host, p(p+2) values each (hard cut / polynomial) */
+  void filterCoeffs(std::vector<Real>& hard, std::vector<Real>& poly) const {
+    hard.resize((size_t)p_ * (p_ + 2));
+    poly.resize(hard.size());
+    check(ves3d_sht_filter_coeffs(p_, freq_, 0.0, &hard[0]), "SHTrans::filterCoeffs");
+    check(ves3d_sht_filter_coeffs(p_, freq_, exponent_, &poly[0]), "SHTrans::filterCoeffs");
+  }
+  void lowPassFilter(const Real* in, long n_funs, Real* out) const {
+    check(ves3d_sht_lowpass(in, n_funs, p_, freq_, 0.0, out, stream_), "SHTrans::lowPassFilter");
+  }
+  void lowPassFilterPoly(const Real* in, long n_funs, Real* out) const {
+    check(ves3d_sht_lowpass(in, n_funs, p_, freq_, exponent_, out, stream_), "SHTrans::lowPassFilterPoly");
+  }
+  /* scaling_coeff: device array of p(p+2) values */
+  void ScaleFreq(const Real* shc_in, long n_funs, const Real* scaling_coeff, Real* shc_out) const {
+    check(ves3d_sht_scale_freq(shc_in, n_funs, p_, scaling_coeff, shc_out, stream_), "SHTrans::ScaleFreq");
+  }
   void forward(const Real* in, long n_funs, Real* shc) const {
     check(ves3d_sht_forward(in, n_funs, p_, p_, shc, stream_), "SHTrans::forward");
   }
@@ -146,6 +170,8 @@ class SHTrans {
  private:
   int p_;
   void* stream_;
+  int freq_;
+  Real exponent_;
 };
 
 /* Device<GPU>::DirectStokes(src, den, qw, src_stride, trg_stride, n_surfs, trg,

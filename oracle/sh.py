@@ -222,6 +222,35 @@ def _fourier_block_ids(p):
     return [(jf + 1) // 2 for jf in range(2 * p)]
 
 
+def filter_coeffs(p, freq=-1, exponent=None):
+    """SHTrans's frequency filters in the per-function coefficient order (src/SHTrans.cc:
+    8-45): freq -1 means 2p/3 (integer division); exponent None is the hard cut of
+    lowPassFilter (keep degrees n <= freq), a number the polynomial filter of
+    lowPassFilterPoly (1 - (n/freq)^exponent for n < freq, else 0)."""
+    freq = 2 * p // 3 if freq == -1 else freq
+    off = block_offsets(p)
+    c = np.empty(ncoef(p))
+    for jf in range(2 * p):
+        m = (jf + 1) // 2
+        deg = m + np.arange(off[jf + 1] - off[jf])
+        if exponent is None:
+            c[off[jf]:off[jf + 1]] = np.where(deg > freq, 0.0, 1.0)
+        else:
+            c[off[jf]:off[jf + 1]] = np.where(deg >= freq, 0.0, 1.0 - (deg / freq) ** exponent)
+    return c
+
+
+def scale_freq(S, p, coeff):
+    """SHTrans::ScaleFreq (src/SHTrans.cc:190-223) on function-major coefficients."""
+    return (np.asarray(S, dtype=np.float64).reshape(-1, ncoef(p)) * np.asarray(coeff)[None, :]).reshape(-1)
+
+
+def low_pass(X, p, freq=-1, exponent=None):
+    """SHTrans::lowPassFilter / lowPassFilterPoly (src/SHTrans.cc:172-188): analysis, scaling,
+    synthesis of grid functions [n_fun][(p+1) 2p]."""
+    return shc2grid(scale_freq(grid2shc(X, p, p), p, filter_coeffs(p, freq, exponent)), p, p)
+
+
 def grid2shc(X, p0, p1):
     """Analysis: grid at order p0 -> coefficients at order p1 (src/SphericalHarmonics.cc:152-235)."""
     X = np.asarray(X, dtype=np.float64).reshape(-1, p0 + 1, 2 * p0)

@@ -92,14 +92,7 @@ def lowpass(f, p, freq):
     (SHTrans::lowPassFilter with filter_coeff_, src/SHTrans.cc:22-29, :172-180)."""
     if freq is None:
         return f
-    shape = np.shape(f)
-    S = sh.grid2shc(np.reshape(f, -1), p, p).reshape(-1, sh.ncoef(p))
-    off = sh.block_offsets(p)
-    for jf in range(2 * p):
-        m = (jf + 1) // 2
-        deg = m + np.arange(off[jf + 1] - off[jf])
-        S[:, off[jf]:off[jf + 1]][:, deg > freq] = 0.0
-    return sh.shc2grid(S.reshape(-1), p, p).reshape(shape)
+    return sh.low_pass(np.reshape(f, -1), p, freq).reshape(np.shape(f))
 
 
 def geometry(X, p, filter_freq=None):

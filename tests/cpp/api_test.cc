@@ -1,9 +1,11 @@
 // C++ caller of the B200 path through include/ves3d_b200.hpp, written the way Ves3D's
 // C++ code uses StokesVelocity<Real> (SetSrcCoord / SetDensitySL / operator()).
 //   api_test --version            prints the library version (no GPU needed)
+//   api_test --filter p f e       prints SHTrans's two filters (no GPU needed)
 //   api_test <in.bin> <out.bin>   in: int32 p, int32 n_ves, X[n], f[n] (doubles, AxisMajor);
 //                                 out: vel[n] then the implicit solution x[4 n / 3]
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -12,6 +14,16 @@
 int main(int argc, char** argv) {
   if (argc == 2 && std::strcmp(argv[1], "--version") == 0) {
     std::printf("%d\n", ves3d_version());
+    return 0;
+  }
+  if (argc == 5 && std::strcmp(argv[1], "--filter") == 0) {
+    // SHTrans filters on the host: p, filter_freq, exponent -> hard and polynomial rows
+    ves3d_b200::SHTrans<double> sht(std::atoi(argv[2]), 0, std::atoi(argv[3]), std::atof(argv[4]));
+    std::vector<double> hard, poly;
+    sht.filterCoeffs(hard, poly);
+    for (size_t i = 0; i < hard.size(); i++) std::printf("%.17g%c", hard[i], i + 1 < hard.size() ? ' ' : '\n');
+    for (size_t i = 0; i < poly.size(); i++) std::printf("%.17g%c", poly[i], i + 1 < poly.size() ? ' ' : '\n');
+    std::printf("%d %.17g\n", sht.getShFilterFreq(), sht.getShFilterExponent());
     return 0;
   }
   if (argc != 3) {

@@ -25,6 +25,22 @@ def test_cpp_api_builds_as_cpp03_and_links(tmp_path):
     assert int(out.strip()) >= 1
 
 
+def test_cpp_shtrans_filters_match_oracle(tmp_path):
+    """SHTrans's filter coefficients through the C++ mirror (host only) against the oracle,
+    with the reference constructor's defaults (filter_freq -1 = 2p/3, exponent 4)."""
+    from oracle import sh
+    exe = build_api_test(tmp_path)
+    for p, freq, e in ((6, -1, 4.0), (12, 5, 2.5), (16, -1, 4.0)):
+        out = subprocess.run([exe, "--filter", str(p), str(freq), str(e)], capture_output=True, text=True,
+                             check=True).stdout.split("\n")
+        hard = np.array(out[0].split(), dtype=float)
+        poly = np.array(out[1].split(), dtype=float)
+        f_out, e_out = out[2].split()
+        assert int(f_out) == (2 * p // 3 if freq == -1 else freq) and float(e_out) == e
+        assert np.array_equal(hard, sh.filter_coeffs(p, freq))
+        assert np.abs(poly - sh.filter_coeffs(p, freq, e)).max() < 1e-15
+
+
 @pytest.mark.gpu
 def test_cpp_api_matches_oracle(tmp_path):
     from oracle import stokes, surface as su

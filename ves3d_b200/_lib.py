@@ -45,6 +45,9 @@ SIGNATURES = [
     ("ves3d_sv_launch_eval_graph", _i, [_vp]),
     ("ves3d_sht_forward", _i, [_vp, _l, _i, _i, _vp, _vp]),
     ("ves3d_sht_backward", _i, [_vp, _l, _i, _i, _vp, _vp, _vp, _vp]),
+    ("ves3d_sht_filter_coeffs", _i, [_i, _i, _d, _vp]),
+    ("ves3d_sht_scale_freq", _i, [_vp, _l, _i, _vp, _vp, _vp]),
+    ("ves3d_sht_lowpass", _i, [_vp, _l, _i, _i, _d, _vp, _vp]),
     ("ves3d_cuda_stokes_f64", _i, [_i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("ves3d_stokes_alltoall_f64", None, [_vp, _vp, _sz, _vp, ctypes.POINTER(_vp)]),
     ("ves3d_interaction_free", None, [ctypes.POINTER(_vp)]),
@@ -137,6 +140,15 @@ def tables_export(p0, p1, name):
     check(lib().ves3d_tables_export(p0, p1, name.encode(), None, 0, ctypes.byref(n)), "tables_export")
     out = np.empty(n.value)
     check(lib().ves3d_tables_export(p0, p1, name.encode(), out.ctypes.data, out.size, ctypes.byref(n)), "tables_export")
+    return out
+
+
+def filter_coeffs(p, freq=-1, exponent=0.0):
+    """SHTrans filter coefficients [p(p+2)] (host): exponent <= 0 the hard cut of
+    lowPassFilter, > 0 the polynomial filter of lowPassFilterPoly; freq -1 means 2p/3."""
+    import numpy as np
+    out = np.empty(p * (p + 2))
+    check(lib().ves3d_sht_filter_coeffs(int(p), int(freq), float(exponent), out.ctypes.data), "filter_coeffs")
     return out
 
 

@@ -38,6 +38,8 @@ int launch_analysis(const double* in, long nfun, int pin, int pout, const double
 // VES3D_TC_ANALYSIS=0 forces the generic kernel.
 int launch_grid2shc(const double* in, long nfun, int p, const double* four, const double* leg, const int* jf,
                     double* out, cudaStream_t st);
+// shc_out[f][c] = shc_in[f][c] * scale[c] for nfun functions of nc coefficients
+int launch_scale_freq(const double* in, long nfun, int nc, const double* scale, double* out, cudaStream_t st);
 int launch_synthesis(const double* S, long nfun, int p0, int q, const double* leg, const double* dleg,
                      const double* four, const double* dfour, const int* blk_off, double* X, double* Xt,
                      double* Xp, cudaStream_t st);

@@ -257,6 +257,22 @@ __global__ void __launch_bounds__(256, 2) k_analysis_tc(const double* __restrict
   }
 }
 
+// shc_out[f][c] = shc_in[f][c] scale[c] (in place allowed): SHTrans::ScaleFreq on
+// function-major coefficient arrays
+__global__ void k_scale_freq(const double* in, long n, int nc, const double* __restrict__ scale, double* out) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    out[i] = in[i] * __ldg(scale + i % nc);
+}
+
+int launch_scale_freq(const double* in, long nfun, int nc, const double* scale, double* out, cudaStream_t st) {
+  const long n = nfun * nc;
+  if (n <= 0) return VES3D_OK;
+  const long b = std::min((n + 255) / 256, 4096L);
+  k_scale_freq<<<(unsigned)b, 256, 0, st>>>(in, n, nc, scale, out);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
 static int sm_count() {
   static int n = 0;
   if (!n) {

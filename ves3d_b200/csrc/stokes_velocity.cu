@@ -746,6 +746,62 @@ int ves3d_sht_backward(const double* S, long n_fun, int p0, int p1, double* X, d
   return VES3D_OK;
 }
 
+int ves3d_sht_filter_coeffs(int p, int filter_freq, double exponent, double* coeff) {
+  VES3D_ARG(coeff != nullptr, "coeff is null");
+  VES3D_ARG(p >= 1 && p <= 128, "order must be in [1, 128]");
+  const int freq = filter_freq == -1 ? 2 * p / 3 : filter_freq;
+  VES3D_ARG(freq >= 0, "filter frequency must be >= 0 (or -1 for 2p/3)");
+  int i = 0;
+  for (int jf = 0; jf < 2 * p; jf++) {
+    const int m = (jf + 1) / 2;
+    for (int n = m; n <= p; n++, i++) {
+      if (exponent <= 0)
+        coeff[i] = n > freq ? 0.0 : 1.0;  // lowPassFilter: degrees above freq removed
+      else
+        coeff[i] = n >= freq ? 0.0 : 1.0 - std::pow((double)n / freq, exponent);
+    }
+  }
+  return VES3D_OK;
+}
+
+int ves3d_sht_scale_freq(const double* shc_in, long n_fun, int p, const double* scale, double* shc_out,
+                         void* stream) {
+  VES3D_ARG(shc_in && scale && shc_out, "null pointer");
+  VES3D_ARG(p >= 1 && p <= 128, "order must be in [1, 128]");
+  VES3D_ARG(n_fun >= 0, "n_fun < 0");
+  cudaStream_t st = (cudaStream_t)stream;
+  int s = launch_scale_freq(shc_in, n_fun, ncoef_(p), scale, shc_out, st);
+  if (s) return s;
+  VES3D_CK(cudaStreamSynchronize(st));
+  return VES3D_OK;
+}
+
+int ves3d_sht_lowpass(const double* in, long n_fun, int p, int filter_freq, double exponent, double* out,
+                      void* stream) {
+  VES3D_ARG(in && out, "null pointer");
+  VES3D_ARG(p >= 1 && p <= 128, "order must be in [1, 128]");
+  VES3D_ARG(n_fun >= 0, "n_fun < 0");
+  if (n_fun == 0) return VES3D_OK;
+  const int nc = ncoef_(p);
+  std::vector<double> coeff(nc);
+  int s = ves3d_sht_filter_coeffs(p, filter_freq, exponent, coeff.data());
+  if (s) return s;
+  cudaStream_t st = (cudaStream_t)stream;
+  double *dc = nullptr, *shc = nullptr;
+  if ((s = dupload(&dc, coeff, st))) return s;
+  if ((s = dalloc(&shc, (size_t)n_fun * nc))) {
+    dfree(dc);
+    return s;
+  }
+  s = ves3d_sht_forward(in, n_fun, p, p, shc, stream);
+  if (!s) s = ves3d_sht_scale_freq(shc, n_fun, p, dc, shc, stream);
+  if (!s) s = ves3d_sht_backward(shc, n_fun, p, p, out, nullptr, nullptr, stream);
+  cudaStreamSynchronize(st);
+  dfree(dc);
+  dfree(shc);
+  return s;
+}
+
 int ves3d_tables_export(int p0, int p1, const char* name, double* out, size_t cap, size_t* n) {
   VES3D_ARG(name != nullptr && n != nullptr, "null argument");
   VES3D_ARG(p0 >= 2 && p0 <= 64 && p1 >= p0 && p1 <= 128, "orders out of range");

@@ -254,6 +254,51 @@ class StokesVelocity:
         return x0, w, r
 
 
+class SHTrans:
+    """SHTrans (include/SHTrans.h:21-63) on CUDA float64 tensors: grid functions
+    [n_fun][(p+1) 2p], coefficients function-major [n_fun][p(p+2)]. filter_freq -1 means
+    2p/3; filter_exponent is lowPassFilterPoly's exponent (the reference's default 4)."""
+
+    def __init__(self, sh_order, filter_freq=-1, filter_exponent=4.0, stream=None):
+        self.p = int(sh_order)
+        self.filter_freq = int(filter_freq)
+        self.filter_exponent = float(filter_exponent)
+        self.stream = stream
+
+    def _nfun(self, t, per):
+        p_, dev, n = _ptr(t)
+        if not dev or n % per:
+            raise ValueError("expected a CUDA float64 tensor of whole functions")
+        return p_, n // per
+
+    def forward(self, grid, shc):
+        g, n = self._nfun(grid, ngrid(self.p))
+        c, _ = self._nfun(shc, ncoef(self.p))
+        check(lib().ves3d_sht_forward(g, n, self.p, self.p, c, self.stream), "SHTrans.forward")
+
+    def backward(self, shc, grid):
+        c, n = self._nfun(shc, ncoef(self.p))
+        g, _ = self._nfun(grid, ngrid(self.p))
+        check(lib().ves3d_sht_backward(c, n, self.p, self.p, g, None, None, self.stream), "SHTrans.backward")
+
+    def ScaleFreq(self, shc_in, scale, shc_out):
+        a, n = self._nfun(shc_in, ncoef(self.p))
+        b, _ = self._nfun(shc_out, ncoef(self.p))
+        sc, _, _ = _ptr(scale)
+        check(lib().ves3d_sht_scale_freq(a, n, self.p, sc, b, self.stream), "SHTrans.ScaleFreq")
+
+    def lowPassFilter(self, grid_in, grid_out):
+        a, n = self._nfun(grid_in, ngrid(self.p))
+        b, _ = self._nfun(grid_out, ngrid(self.p))
+        check(lib().ves3d_sht_lowpass(a, n, self.p, self.filter_freq, 0.0, b, self.stream), "lowPassFilter")
+
+    def lowPassFilterPoly(self, grid_in, grid_out):
+        a, n = self._nfun(grid_in, ngrid(self.p))
+        b, _ = self._nfun(grid_out, ngrid(self.p))
+        check(lib().ves3d_sht_lowpass(a, n, self.p, self.filter_freq, self.filter_exponent, b, self.stream),
+              "lowPassFilterPoly")
+
+
 class PolydisperseStokesVelocity:
     """Single-layer velocity of a suspension whose vesicles have different SH orders.
     Arrays are the per-vesicle AxisMajor blocks concatenated in vesicle order; vesicles of
