@@ -148,6 +148,8 @@ int ves3d_svp_launch_eval_graph(ves3d_svp* g, double* vel, int is_device);
  * group; tol and max_iter are in/out as in ves3d_sv_implicit_solve. */
 int ves3d_svp_set_implicit_params(ves3d_svp* g, double dt, double bending_modulus, double shear_rate);
 int ves3d_svp_set_gravity(ves3d_svp* g, double excess_density, double gx, double gy, double gz);
+/* ves3d_sv_set_surface_filter for every order group (-1: 2p/3 of each group's order). */
+int ves3d_svp_set_surface_filter(ves3d_svp* g, int filter_freq);
 int ves3d_svp_set_precond(ves3d_svp* g, int scheme, int refresh_every);
 int ves3d_svp_implicit_solve(ves3d_svp* g, const double* x0, double* x, double* tol, int* max_iter, int* code,
                              int is_device);
@@ -193,6 +195,12 @@ int ves3d_sv_set_implicit_params(ves3d_sv* sv, double dt, double kappa, double s
 /* Gravity (InterfacialForce::gravityForce, src/InterfacialForce.cc:127-184): the traction
  * excess_density (g . x) n enters the explicit jump with x = the positions and the
  * linearised jump with x = dt u. Default excess_density 0 (off), g = (0, 0, -1). */
+/* The reference Surface's low-pass filter (SHTrans::lowPassFilter at diff_filter_freq,
+ * src/Surface.cc:310-311, :336, :371, :564) on H, K, surface gradients, divergences and the
+ * linearised curvature of the geometry ops and the implicit step: 0 turns it off (the
+ * default), -1 keeps degrees <= 2p/3 (the reference's default), a positive value is the
+ * highest degree kept. The reference also upsamples the forces; this path stays at p. */
+int ves3d_sv_set_surface_filter(ves3d_sv* sv, int filter_freq);
 int ves3d_sv_set_gravity(ves3d_sv* sv, double excess_density, double gx, double gy, double gz);
 int ves3d_sv_surface_op(ves3d_sv* sv, int op, const double* in, double* out, int is_device);
 /* Solve the implicit system with BiCGStab in its Galerkin form (unknowns: SH coefficients

@@ -201,10 +201,11 @@ class ImplicitStep:
         u - S[f(dt u, sigma)] = u_inf + S[f_b(x)],     -div S[f] = div(u_inf + S[f_b])
     with f(y, sigma) = lin_bending(y) + tension(sigma)."""
 
-    def __init__(self, X, p, kappa, dt, shear_rate, SL=None, excess_density=0.0, gravity=(0.0, 0.0, -1.0)):
+    def __init__(self, X, p, kappa, dt, shear_rate, SL=None, excess_density=0.0, gravity=(0.0, 0.0, -1.0),
+                 filter_freq=None):
         self.p = p
         self.X = np.asarray(X, dtype=np.float64)
-        self.geo = geometry(self.X, p)
+        self.geo = geometry(self.X, p, filter_freq)
         self.kappa, self.dt, self.rate = kappa, dt, shear_rate
         self.drho, self.g = excess_density, np.asarray(gravity, dtype=np.float64)
         self.SL = SL if SL is not None else sh.stokes_singular_matrix(self.X, p, 2 * p)

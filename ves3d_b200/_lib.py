@@ -70,6 +70,8 @@ SIGNATURES = [
     ("ves3d_svp_launch_eval_graph", _i, [_vp, _vp, _i]),
     ("ves3d_svp_set_implicit_params", _i, [_vp, _d, _d, _d]),
     ("ves3d_svp_set_gravity", _i, [_vp, _d, _d, _d, _d]),
+    ("ves3d_svp_set_surface_filter", _i, [_vp, _i]),
+    ("ves3d_sv_set_surface_filter", _i, [_vp, _i]),
     ("ves3d_svp_set_precond", _i, [_vp, _i, _i]),
     ("ves3d_svp_implicit_solve", _i, [_vp, _vp, _vp, ctypes.POINTER(_d), ctypes.POINTER(_i), ctypes.POINTER(_i), _i]),
     ("ves3d_svp_solver_stats", _i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i)]),

@@ -155,6 +155,10 @@ struct ves3d_sv {
   bool geo_valid = false;
   double dt = 0.01, kappa = 0.05, shear = 1.0;
   double drho = 0.0, grav[3] = {0.0, 0.0, -1.0};  // excess density and gravity field
+  // the reference Surface's low-pass filter of H, K, grad, div and the linearised
+  // curvature (0: off; else the highest degree kept) and its coefficients [nc] on device
+  int filter_freq = 0;
+  double* filt = nullptr;
   int far_force_fp64 = 0;      // 1: evaluate the far field in FP64 even in the mixed form
   int ir_outer = 0, ir_inner = 0;  // last mixed solve: outer refinements, inner iterations
   // preconditioner of the implicit solve (VES3D_PRECOND_*); the self-block form stores one
@@ -182,6 +186,7 @@ struct ves3d_sv {
   float ms[4] = {0, 0, 0, 0};
 
   ~ves3d_sv() {
+    dfree(filt);
     drop_graph();
     free_precond();
     for (auto& e : pc_ev)
@@ -953,6 +958,18 @@ int grid2shc_p(ves3d_sv* sv, const double* in, long nfun, double* out) {
   return launch_grid2shc(in, nfun, sv->p, T.ana_four, T.ana_leg, T.jf_of_coef, out, sv->stream);
 }
 
+// The reference Surface's low-pass filter (SHTrans::lowPassFilter at diff_filter_freq,
+// src/Surface.cc:310-311, :336, :371, :564) of nfun grid functions in place, through the
+// coefficient scratch wc (room for nfun functions); nothing when the filter is off.
+int filter_fields(ves3d_sv* sv, double* wc, double* f, long nfun) {
+  if (!sv->filter_freq || nfun <= 0) return VES3D_OK;
+  int s;
+  const int nc = ncoef_(sv->p);
+  if ((s = grid2shc_p(sv, f, nfun, wc))) return s;
+  if ((s = launch_scale_freq(wc, nfun, nc, sv->filt, wc, sv->stream))) return s;
+  return synth_d(sv, wc, nfun, 0, f, nullptr, nullptr);
+}
+
 int ensure_geometry(ves3d_sv* sv) {
   int s;
   if ((s = ensure_implicit_buffers(sv))) return s;
@@ -965,6 +982,17 @@ int ensure_geometry(ves3d_sv* sv) {
   if ((s = synth_d(sv, sv->Sx, nf, 1, w[3], w[4], w[5]))) return s;
   if ((s = synth_d(sv, sv->Sx, nf, 2, w[6], nullptr, nullptr))) return s;
   if ((s = launch_geometry(w[2], w[1], w[5], w[4], w[6], nv, ng, sv->geo, sv->stream))) return s;
+  if (sv->filter_freq) {
+    // H and K (record components 13, 14) filtered as Surface::updateAll does
+    const size_t row = ng * sizeof(double), pitch = kGeoComps * row;
+    for (int k = 0; k < 2; k++)
+      VES3D_CK(cudaMemcpy2DAsync(w[0] + k * nv * ng, row, sv->geo + (13L + k) * ng, pitch, row, (size_t)nv,
+                                 cudaMemcpyDeviceToDevice, sv->stream));
+    if ((s = filter_fields(sv, sv->wc, w[0], 2 * nv))) return s;
+    for (int k = 0; k < 2; k++)
+      VES3D_CK(cudaMemcpy2DAsync(sv->geo + (13L + k) * ng, pitch, w[0] + k * nv * ng, row, row, (size_t)nv,
+                                 cudaMemcpyDeviceToDevice, sv->stream));
+  }
   sv->geo_valid = true;
   return VES3D_OK;
 }
@@ -999,7 +1027,8 @@ int op_grad(ves3d_sv* sv, const OpSpace& sp, const double* in, double* out) {
   if ((s = grid2shc_p(sv, in, nv, sp.wc))) return s;
   // value into out (overwritten below), v-derivative into a, u-derivative into b
   if ((s = synth_d(sv, sp.wc, nv, 0, out, a, b))) return s;
-  return launch_grad_combine(b, a, sv->geo, nv, ng, out, sv->stream, sv->nves);
+  if ((s = launch_grad_combine(b, a, sv->geo, nv, ng, out, sv->stream, sv->nves))) return s;
+  return filter_fields(sv, sp.wc, out, 3 * nv);
 }
 
 // div of a vector field (in [nv][3][ng]) -> out [nv][ng] times scale; uses w5, w6, w7, wc
@@ -1009,7 +1038,8 @@ int op_div(ves3d_sv* sv, const OpSpace& sp, const double* in, double* out, doubl
   const int ng = ngrid_(sv->p);
   if ((s = grid2shc_p(sv, in, 3 * nv, sp.wc))) return s;
   if ((s = synth_d(sv, sp.wc, 3 * nv, 0, sp.w[5], sp.w[6], sp.w[7]))) return s;
-  return launch_div_combine(sp.w[7], sp.w[6], sv->geo, nv, ng, scale, out, sv->stream, sv->nves);
+  if ((s = launch_div_combine(sp.w[7], sp.w[6], sv->geo, nv, ng, scale, out, sv->stream, sv->nves))) return s;
+  return filter_fields(sv, sp.wc, out, nv);
 }
 
 // linearised mean curvature of a displacement field; uses w4..w7, wc
@@ -1020,7 +1050,8 @@ int op_linH(ves3d_sv* sv, const OpSpace& sp, const double* in, double* out) {
   if ((s = grid2shc_p(sv, in, 3 * nv, sp.wc))) return s;
   if ((s = synth_d(sv, sp.wc, 3 * nv, 1, sp.w[4], sp.w[5], sp.w[6]))) return s;  // u, uv, uu
   if ((s = synth_d(sv, sp.wc, 3 * nv, 2, sp.w[7], nullptr, nullptr))) return s;    // vv
-  return launch_linH_combine(sp.w[6], sp.w[5], sp.w[7], sv->geo, nv, ng, out, sv->stream, sv->nves);
+  if ((s = launch_linH_combine(sp.w[6], sp.w[5], sp.w[7], sv->geo, nv, ng, out, sv->stream, sv->nves))) return s;
+  return filter_fields(sv, sp.wc, out, nv);
 }
 
 // bending traction of a scalar h (the mean curvature or its linearisation), added to add.
@@ -1745,6 +1776,27 @@ int ves3d_sv_set_implicit_params(ves3d_sv* sv, double dt, double kappa, double s
   return VES3D_OK;
 }
 
+int ves3d_sv_set_surface_filter(ves3d_sv* sv, int filter_freq) {
+  int s = check_sv(sv);
+  if (s) return s;
+  VES3D_ARG(filter_freq >= -1, "filter frequency: 0 (off), -1 (2p/3) or the highest degree kept");
+  const int f = filter_freq == -1 ? 2 * sv->p / 3 : filter_freq;
+  if (f == sv->filter_freq) return VES3D_OK;
+  if (f) {
+    const int nc = ncoef_(sv->p);
+    std::vector<double> c(nc);
+    if ((s = ves3d_sht_filter_coeffs(sv->p, f, 0.0, c.data()))) return s;
+    dfree(sv->filt);
+    sv->filt = nullptr;
+    if ((s = dupload(&sv->filt, c, sv->stream))) return s;
+    VES3D_CK(cudaStreamSynchronize(sv->stream));
+  }
+  sv->filter_freq = f;
+  sv->geo_valid = false;
+  sv->pc_valid = false;
+  return VES3D_OK;
+}
+
 int ves3d_sv_set_gravity(ves3d_sv* sv, double excess_density, double gx, double gy, double gz) {
   int s = check_sv(sv);
   if (s) return s;
@@ -2204,7 +2256,7 @@ struct ves3d_svp {
   cudaGraphExec_t graph_exec = nullptr;
   // implicit step: parameters pushed to every order group before a solve
   double dt = 0.01, kappa = 0.05, shear = 1.0, drho = 0.0, grav[3] = {0.0, 0.0, -1.0};
-  int precond = 0, pc_refresh = 1;
+  int precond = 0, pc_refresh = 1, filter_freq = 0;
   int far_force_fp64 = 0, ir_outer = 0, ir_inner = 0;
   std::vector<long> coff;  // first SH unknown of each group's [u; sigma] coefficients
   double* sws = nullptr;   // solve workspace: BiCGStab, coefficients, right-hand side, grid
@@ -2490,6 +2542,7 @@ int svp_prepare_implicit(ves3d_svp* g) {
     if ((s = ves3d_sv_set_gravity(sv, g->drho, g->grav[0], g->grav[1], g->grav[2]))) return s;
     if ((s = ves3d_sv_set_precond(sv, g->precond))) return s;
     if ((s = ves3d_sv_set_precond_refresh(sv, g->pc_refresh))) return s;
+    if ((s = ves3d_sv_set_surface_filter(sv, g->filter_freq))) return s;
     if ((s = ensure_geometry(sv))) return s;
     ImplicitWork iw;
     if ((s = implicit_work(sv, iw))) return s;
@@ -2646,6 +2699,14 @@ int ves3d_svp_set_gravity(ves3d_svp* g, double excess_density, double gx, double
   g->grav[0] = gx;
   g->grav[1] = gy;
   g->grav[2] = gz;
+  g->rhs_valid = false;
+  return VES3D_OK;
+}
+
+int ves3d_svp_set_surface_filter(ves3d_svp* g, int filter_freq) {
+  VES3D_ARG(g != nullptr, "null context");
+  VES3D_ARG(filter_freq >= -1, "filter frequency: 0 (off), -1 (2p/3) or the highest degree kept");
+  g->filter_freq = filter_freq;
   g->rhs_valid = false;
   return VES3D_OK;
 }

@@ -156,6 +156,11 @@ class StokesVelocity:
         """Excess density of the vesicles and the gravity field (sedimentation)."""
         check(lib().ves3d_sv_set_gravity(self._h, float(excess_density), *[float(c) for c in g]), "set_gravity")
 
+    def set_surface_filter(self, filter_freq=-1):
+        """The reference Surface's low-pass filter on H, K, gradients, divergences and the
+        linearised curvature: 0 off (default), -1 degrees <= 2p/3, n > 0 degrees <= n."""
+        check(lib().ves3d_sv_set_surface_filter(self._h, int(filter_freq)), "set_surface_filter")
+
     def surface_op(self, op, field=None):
         ng = ngrid(self.sh_order)
         N = self.n_ves * ng
@@ -379,6 +384,9 @@ class PolydisperseStokesVelocity:
 
     def set_gravity(self, excess_density, g=(0.0, 0.0, -1.0)):
         check(lib().ves3d_svp_set_gravity(self._h, float(excess_density), *[float(c) for c in g]), "set_gravity")
+
+    def set_surface_filter(self, filter_freq=-1):
+        check(lib().ves3d_svp_set_surface_filter(self._h, int(filter_freq)), "set_surface_filter")
 
     def set_precond(self, scheme, refresh_every=1):
         """"none", "diag_spectral" or "self_block" for every order group, rebuilt every
