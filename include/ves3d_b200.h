@@ -199,7 +199,11 @@ int ves3d_sv_set_implicit_params(ves3d_sv* sv, double dt, double kappa, double s
  * src/Surface.cc:310-311, :336, :371, :564) on H, K, surface gradients, divergences and the
  * linearised curvature of the geometry ops and the implicit step: 0 turns it off (the
  * default), -1 keeps degrees <= 2p/3 (the reference's default), a positive value is the
- * highest degree kept. The reference also upsamples the forces; this path stays at p. */
+ * highest degree kept. For the Surface-level operations (SurfaceTest's quantities). The
+ * implicit step is best left unfiltered: the reference computes its forces at the
+ * upsampled order 2p and filters at 2/3 of that (4p/3), which removes nothing resolved at
+ * order p, while a filter at 2p/3 of p leaves the tension modes above the filter degree
+ * without force and the implicit system singular (BiCGStab then stops at max_iter). */
 int ves3d_sv_set_surface_filter(ves3d_sv* sv, int filter_freq);
 int ves3d_sv_set_gravity(ves3d_sv* sv, double excess_density, double gx, double gy, double gz);
 int ves3d_sv_surface_op(ves3d_sv* sv, int op, const double* in, double* out, int is_device);
