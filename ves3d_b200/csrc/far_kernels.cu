@@ -376,6 +376,13 @@ int far_segments(long nves, long N, int tile, int nthr, int waves, int* seg_tile
   return (int)((ntiles + *seg_tiles - 1) / *seg_tiles);
 }
 
+int launch_far_reduce(const double* part, int nseg, const long* off, long nves, long N, const double* add, double* out,
+                      double* far_out, cudaStream_t st) {
+  k_far_reduce<<<(unsigned)nves, 256, 0, st>>>(part, nseg, off, N, add, out, far_out);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
 static void chunking(int nt, int chunk_max, int tpt, int* nchunk, int* nthr) {
   // targets of a vesicle in chunks of at most chunk_max (tpt per thread)
   *nchunk = (nt + chunk_max - 1) / chunk_max;
@@ -383,9 +390,12 @@ static void chunking(int nt, int chunk_max, int tpt, int* nchunk, int* nthr) {
   *nthr = 32 * ((((per_chunk + tpt - 1) / tpt) + 31) / 32);
 }
 
+// With nseg_out null the segments' partials are reduced on st; otherwise the segments
+// alone are launched and their count returned, for a launch_far_reduce elsewhere.
 static int launch_far_shape(const FarShape& sh, bool mixed, const double* pos, const double* den, const long* off,
                             long nves, long N, const FarGroup* groups, int ngroups, const double* add, double* out,
-                            double* far_out, double* part, long part_cap_segments, cudaStream_t st) {
+                            double* far_out, double* part, long part_cap_segments, cudaStream_t st,
+                            int* nseg_out = nullptr) {
   const int tile = mixed ? kTileF32 : kTileF64;
   // one segment layout for all groups, sized by the average vesicle
   long nthr_sum = 0, nchunk_tot = 0;
@@ -418,9 +428,11 @@ static int launch_far_shape(const FarShape& sh, bool mixed, const double* pos, c
       k_far_f64_seg<<<grid, nthr, 0, st>>>(pos, den, off, N, seg_tiles, (int)groups[g].v0, part);
     VES3D_LAUNCHED();
   }
-  k_far_reduce<<<(unsigned)nves, 256, 0, st>>>(part, nseg, off, N, add, out, far_out);
-  VES3D_LAUNCHED();
-  return VES3D_OK;
+  if (nseg_out) {
+    *nseg_out = nseg;
+    return VES3D_OK;
+  }
+  return launch_far_reduce(part, nseg, off, nves, N, add, out, far_out, st);
 }
 
 // ---- autotuner of the launch shape ----------------------------------------------------
@@ -474,7 +486,7 @@ int set_far_shape(int waves, int chunk_max, int tpt) {
 
 int launch_far_groups(bool mixed, const double* pos, const double* den, const long* off, long nves, long N,
                       const FarGroup* groups, int ngroups, const double* add, double* out, double* far_out,
-                      double* part, long part_cap_segments, cudaStream_t st) {
+                      double* part, long part_cap_segments, cudaStream_t st, int* nseg_out) {
   if (N <= 0) return VES3D_OK;
   FarShape shape;
   if (g_forced.waves) {
@@ -506,8 +518,11 @@ int launch_far_groups(bool mixed, const double* pos, const double* den, const lo
       int s = VES3D_OK;
       for (const FarShape& c : cands) {
         cudaEventRecord(e0, st);
+        // candidates are timed on their segment kernels alone (the reduce is the same
+        // for every shape, and its outputs may not be given when the caller reduces later)
+        int cand_nseg = 0;
         s = launch_far_shape(c, mixed, pos, den, off, nves, N, groups, ngroups, add, out, far_out, part,
-                             part_cap_segments, st);
+                             part_cap_segments, st, &cand_nseg);
         if (s) break;
         cudaEventRecord(e1, st);
         cudaEventSynchronize(e1);
@@ -529,7 +544,7 @@ int launch_far_groups(bool mixed, const double* pos, const double* den, const lo
     }
   }
   return launch_far_shape(shape, mixed, pos, den, off, nves, N, groups, ngroups, add, out, far_out, part,
-                          part_cap_segments, st);
+                          part_cap_segments, st, nseg_out);
 }
 
 int set_autotune(int on) {
@@ -550,9 +565,10 @@ std::string autotune_report() {
 
 int launch_far(bool mixed, const double* pos, const double* den, const long* off, long nves, long N, int max_nt,
                const double* add, double* out, double* far_out, double* part, long part_cap_segments,
-               cudaStream_t st) {
+               cudaStream_t st, int* nseg_out) {
   FarGroup g{0, nves, max_nt};
-  return launch_far_groups(mixed, pos, den, off, nves, N, &g, 1, add, out, far_out, part, part_cap_segments, st);
+  return launch_far_groups(mixed, pos, den, off, nves, N, &g, 1, add, out, far_out, part, part_cap_segments, st,
+                           nseg_out);
 }
 
 }  // namespace ves3d

@@ -73,9 +73,13 @@ int launch_far_density(const double* f, const double* area, long nv, int p0, con
 // sources; far_out (may be null) receives the far part alone. off [nves+1] point offsets,
 // max_nt the largest vesicle; part is a [part_cap_segments][N][3] FP64 work buffer.
 // mixed selects the packed-FP32 pair arithmetic with FP64 accumulation.
+// With nseg_out given, only the segment kernels run (no reduce) and their count comes back
+// for launch_far_reduce, which may then run on another stream after the self part.
 int launch_far(bool mixed, const double* pos, const double* den, const long* off, long nves, long N, int max_nt,
                const double* add, double* out, double* far_out, double* part, long part_cap_segments,
-               cudaStream_t st);
+               cudaStream_t st, int* nseg_out = nullptr);
+int launch_far_reduce(const double* part, int nseg, const long* off, long nves, long N, const double* add, double* out,
+                      double* far_out, cudaStream_t st);
 constexpr long kFarMaxSegments = 32;
 // Vesicles [v0, v0 + nv) all with nt points: one far-field launch each, sized for nt.
 struct FarGroup {
@@ -88,7 +92,7 @@ int set_far_shape(int waves, int chunk_max, int tpt);
 std::string autotune_report();
 int launch_far_groups(bool mixed, const double* pos, const double* den, const long* off, long nves, long N,
                       const FarGroup* groups, int ngroups, const double* add, double* out, double* far_out,
-                      double* part, long part_cap_segments, cudaStream_t st);
+                      double* part, long part_cap_segments, cudaStream_t st, int* nseg_out = nullptr);
 // out = a + b elementwise.
 int launch_add(const double* a, const double* b, long n, double* out, cudaStream_t st);
 // All pairs, point-major in/out (StokesAlltoAll semantics).

@@ -137,6 +137,10 @@ constexpr int kPcBatch = 8;     // operator columns per application in its assem
 struct ves3d_sv {
   int p = 0, pup = 0, prec = 0, device = 0;
   cudaStream_t stream = nullptr, own_stream = nullptr;
+  // the far field runs on this stream beside the self-matrix build and the self part
+  // (they share no inputs and use different pipes); fork and join events
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::unique_ptr<TablesOwner> tab;
   long nves = 0, cap_ves = 0;
   // resident buffers
@@ -197,6 +201,9 @@ struct ves3d_sv {
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
     tab.reset();
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (side) cudaStreamDestroy(side);
     if (own_stream) cudaStreamDestroy(own_stream);
   }
   void free_buffers() {
@@ -403,33 +410,69 @@ int run_self(ves3d_sv* sv, double* vself, double* den) {
   return launch_far_density(sv->F, sv->area, sv->nves, p0, T.smooth_w0, den, st);
 }
 
-// The evaluation proper, stream-ordered and free of host synchronisation (it is what the
-// CUDA graph of ves3d_sv_capture_eval records): self part, then the far field added to it.
-int run_eval_body(ves3d_sv* sv) {
+// Self part alone: Vself = SHC2Grid(Grid2SHC(F) . SL) on the context's stream.
+int run_self_apply(ves3d_sv* sv) {
+  const DevTables& T = sv->tab->d;
+  const int p0 = sv->p, n = 3 * ncoef_(p0);
+  cudaStream_t st = sv->stream;
   int s;
-  if ((s = run_self(sv, sv->Vself, sv->den))) return s;
-  return launch_far(sv->prec == VES3D_PREC_MIXED && !sv->far_force_fp64, sv->pos, sv->den, sv->off, sv->nves,
-                    sv->npts(), ngrid_(sv->p), sv->Vself, sv->V, sv->Vfar, sv->part, kFarMaxSegments, sv->stream);
+  if ((s = launch_grid2shc(sv->F, sv->nves * 3, p0, T.ana_four, T.ana_leg, T.jf_of_coef, sv->Fc, st))) return s;
+  if ((s = launch_self_gemv(sv->Fc, sv->SL, sv->nves, n, sv->Vc, st))) return s;
+  return launch_synthesis(sv->Vc, sv->nves * 3, p0, p0, T.syn0_leg, T.syn0_dleg, T.syn0_four, T.syn0_dfour,
+                          T.blk_off, sv->Vself, nullptr, nullptr, st);
+}
+
+// Fork: the weighted density and the far-field segments on the side stream, which waits
+// for everything the context's stream has queued (surfaces, densities, the previous
+// evaluation's reduce). ev_far[0..1] (may be null) bracket the segment kernels.
+int fork_far(ves3d_sv* sv, int* nseg, cudaEvent_t ev_far0, cudaEvent_t ev_far1) {
+  const DevTables& T = sv->tab->d;
+  int s;
+  VES3D_CK(cudaEventRecord(sv->ev_fork, sv->stream));
+  VES3D_CK(cudaStreamWaitEvent(sv->side, sv->ev_fork, 0));
+  if ((s = launch_far_density(sv->F, sv->area, sv->nves, sv->p, T.smooth_w0, sv->den, sv->side))) return s;
+  if (ev_far0) VES3D_CK(cudaEventRecord(ev_far0, sv->side));
+  if ((s = launch_far(sv->prec == VES3D_PREC_MIXED && !sv->far_force_fp64, sv->pos, sv->den, sv->off, sv->nves,
+                      sv->npts(), ngrid_(sv->p), nullptr, nullptr, nullptr, sv->part, kFarMaxSegments, sv->side,
+                      nseg)))
+    return s;
+  if (ev_far1) VES3D_CK(cudaEventRecord(ev_far1, sv->side));
+  VES3D_CK(cudaEventRecord(sv->ev_join, sv->side));
+  return VES3D_OK;
+}
+
+// Join: the reduce of the far partials, added to the self part, on the context's stream.
+int join_far(ves3d_sv* sv, int nseg) {
+  VES3D_CK(cudaStreamWaitEvent(sv->stream, sv->ev_join, 0));
+  return launch_far_reduce(sv->part, nseg, sv->off, sv->nves, sv->npts(), sv->Vself, sv->V, sv->Vfar, sv->stream);
+}
+
+// The evaluation proper, stream-ordered and free of host synchronisation (it is what the
+// CUDA graph of ves3d_sv_capture_eval records): the far field forked to the side stream,
+// the self part on the context's stream, joined by the reduce.
+int run_eval_body(ves3d_sv* sv) {
+  int s, nseg = 0;
+  if ((s = fork_far(sv, &nseg, nullptr, nullptr))) return s;
+  if ((s = run_self_apply(sv))) return s;
+  return join_far(sv, nseg);
 }
 
 int run_eval(ves3d_sv* sv) {
-  const int p0 = sv->p;
   cudaStream_t st = sv->stream;
-  int s;
+  int s, nseg = 0;
   if (!sv->have_src || !sv->have_den) {
     set_error("eval before set_src_coord / set_density_sl");
     return VES3D_ERR_STATE;
   }
+  // the far field first, on the side stream: it overlaps the self-matrix build (FP64
+  // tensor cores and FP64 pipe) with its FP32 / FP64 FMA work; events ev[4], ev[5] bracket
+  // its segment kernels (the roofline denominator)
+  if ((s = fork_far(sv, &nseg, sv->ev[4], sv->ev[5]))) return s;
   if (!sv->sl_valid && (s = run_setup(sv))) return s;
   VES3D_CK(cudaEventRecord(sv->ev[2], st));
-  if ((s = run_self(sv, sv->Vself, sv->den))) return s;
+  if ((s = run_self_apply(sv))) return s;
   VES3D_CK(cudaEventRecord(sv->ev[3], st));
-  // events bracket the far-field kernel alone: its duration is the roofline denominator
-  VES3D_CK(cudaEventRecord(sv->ev[4], st));
-  if ((s = launch_far(sv->prec == VES3D_PREC_MIXED && !sv->far_force_fp64, sv->pos, sv->den, sv->off, sv->nves, sv->npts(), ngrid_(p0),
-                      sv->Vself, sv->V, sv->Vfar, sv->part, kFarMaxSegments, st)))
-    return s;
-  VES3D_CK(cudaEventRecord(sv->ev[5], st));
+  if ((s = join_far(sv, nseg))) return s;
   VES3D_CK(cudaEventRecord(sv->ev[6], st));
   VES3D_CK(cudaEventSynchronize(sv->ev[6]));
   VES3D_CK(cudaEventElapsedTime(&sv->ms[1], sv->ev[2], sv->ev[3]));
@@ -478,6 +521,9 @@ int ves3d_sv_create(int sh_order, int sh_order_up, int precision, int device, ve
   sv->device = device;
   VES3D_CK(cudaStreamCreateWithFlags(&sv->own_stream, cudaStreamNonBlocking));
   sv->stream = sv->own_stream;
+  VES3D_CK(cudaStreamCreateWithFlags(&sv->side, cudaStreamNonBlocking));
+  VES3D_CK(cudaEventCreateWithFlags(&sv->ev_fork, cudaEventDisableTiming));
+  VES3D_CK(cudaEventCreateWithFlags(&sv->ev_join, cudaEventDisableTiming));
   for (auto& ev : sv->ev) VES3D_CK(cudaEventCreate(&ev));
   sv->tab.reset(new TablesOwner());
   build_tables(sh_order, sh_order_up, sv->tab->h);
