@@ -86,9 +86,11 @@ struct RingCfg {
   static constexpr int NOUT = 12 * NC;
 };
 
+// Persistent: each CTA stages the DFT tables and the small index tables once, then walks
+// rotations blockIdx.x, blockIdx.x + gridDim.x, ...
 template <int P0>
 __global__ void __launch_bounds__(256, 2) k_build_ring(const double* __restrict__ R, DevTables T,
-                                                       double* __restrict__ C) {
+                                                       double* __restrict__ C, long nrot) {
   using G = RingCfg<P0>;
   extern __shared__ __align__(16) double sm[];
   double* sR = sm + G::OFF_R;
@@ -106,7 +108,6 @@ __global__ void __launch_bounds__(256, 2) k_build_ring(const double* __restrict_
   int* sBo = reinterpret_cast<int*>(sm + G::OFF_BO);
   uchar2* sTl = reinterpret_cast<uchar2*>(sm + G::OFF_TL);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const long rot = blockIdx.x;
   for (int i = tid; i < G::L1; i += 256) sSw[i] = __ldg(T.sing_w + i);
   for (int i = tid; i <= G::F0; i += 256) sBo[i] = __ldg(T.blk_off + i);
   if (tid == 0) {
@@ -118,16 +119,19 @@ __global__ void __launch_bounds__(256, 2) k_build_ring(const double* __restrict_
     }
   }
 
-  // ---- rotated coefficients, DFT tables, pole targets ----------------------------------
-  // rotated coefficients, rows padded to LDR (zeros beyond NC: K padding of the last block)
-  for (int i = tid; i < 3 * G::LDR; i += 256) {
-    const int d = i / G::LDR, c = i - d * G::LDR;
-    sR[i] = c < G::NC ? R[rot * 3 * G::NC + d * G::NC + c] : 0.0;
-  }
+  // ---- DFT tables (once per CTA) ----------------------------------------------------------
   for (int i = tid; i < G::F0 * G::N1; i += 256) {
     const int k = i / G::N1, j = i - k * G::N1;
     sMf[k * G::LDM + j] = __ldg(T.syn1_four + i);
     sdMf[k * G::LDM + j] = __ldg(T.syn1_dfour + i);
+  }
+  for (long rot = blockIdx.x; rot < nrot; rot += gridDim.x) {
+  // ---- rotated coefficients, pole targets ------------------------------------------------
+  // rotated coefficients, rows padded to LDR (zeros beyond NC: K padding of the last block);
+  // the previous rotation's last reads of sR ended at its final barrier
+  for (int i = tid; i < 3 * G::LDR; i += 256) {
+    const int d = i / G::LDR, c = i - d * G::LDR;
+    sR[i] = c < G::NC ? R[rot * 3 * G::NC + d * G::NC + c] : 0.0;
   }
   __syncthreads();
   if (tid < 6) {
@@ -305,13 +309,31 @@ __global__ void __launch_bounds__(256, 2) k_build_ring(const double* __restrict_
       }
     }
   }
+  }  // rotations
+}
+
+// Persistent CTAs per SM: 2 fill the shared memory (the default: 52.1 ms per build at 512
+// vesicles, p = 16); 1 leaves room beside each for two far-field CTAs when the far field
+// runs concurrently (VES3D_RING_CTAS=1 with VES3D_FAR_OVERLAP=1: 97.6 ms per evaluation
+// step against 100.9 serial)
+static int ring_ctas_per_sm() {
+  static int n = 0;
+  if (!n) {
+    const char* e = getenv("VES3D_RING_CTAS");
+    n = (e && (e[0] == '1' || e[0] == '2') && !e[1]) ? e[0] - '0' : 2;
+  }
+  return n;
 }
 
 template <int P0>
 static int launch_ring(const double* R, long nrot, const DevTables& T, double* C, cudaStream_t st) {
   using G = RingCfg<P0>;
   VES3D_CK(cudaFuncSetAttribute(k_build_ring<P0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM));
-  k_build_ring<P0><<<(unsigned)nrot, 256, G::SMEM, st>>>(R, T, C);
+  int dev = 0, nsm = 148;
+  VES3D_CK(cudaGetDevice(&dev));
+  VES3D_CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const long grid = std::min(nrot, (long)nsm * ring_ctas_per_sm());
+  k_build_ring<P0><<<(unsigned)grid, 256, G::SMEM, st>>>(R, T, C, nrot);
   VES3D_LAUNCHED();
   return VES3D_OK;
 }
