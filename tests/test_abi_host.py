@@ -47,6 +47,31 @@ def test_argument_errors():
     assert _lib.lib().ves3d_sv_eval(None, None, 0) == 1
 
 
+def test_argument_errors_of_the_implicit_and_filter_entry_points():
+    """Null contexts and out-of-range arguments come back as VES3D_ERR_ARG (1) with a
+    message, before any device work: the polydisperse implicit step, the guess
+    combination, the Surface filter and the SHTrans filters."""
+    L = _lib.lib()
+    d = ctypes.c_double(1e-8)
+    i = ctypes.c_int(10)
+    assert L.ves3d_svp_set_implicit_params(None, 0.01, 0.05, 1.0) == 1
+    assert L.ves3d_svp_set_gravity(None, 1.0, 0.0, 0.0, -1.0) == 1
+    assert L.ves3d_svp_set_precond(None, 2, 1) == 1
+    assert L.ves3d_svp_set_surface_filter(None, -1) == 1
+    assert L.ves3d_svp_implicit_solve(None, None, None, ctypes.byref(d), ctypes.byref(i), ctypes.byref(i), 0) == 1
+    assert L.ves3d_svp_implicit_combine(None, 2, None, None, None, None, 0) == 1
+    assert L.ves3d_svp_solver_stats(None, ctypes.byref(i), ctypes.byref(i)) == 1
+    assert L.ves3d_sv_set_surface_filter(None, -1) == 1
+    out = np.empty(16 * 18)
+    assert L.ves3d_sht_filter_coeffs(0, -1, 0.0, out.ctypes.data) == 1
+    assert L.ves3d_sht_filter_coeffs(16, -2, 0.0, out.ctypes.data) == 1
+    assert L.ves3d_sht_filter_coeffs(16, -1, 0.0, None) == 1
+    assert b"coeff" in L.ves3d_last_error()
+    assert L.ves3d_sht_lowpass(None, 1, 16, -1, 0.0, None, None) == 1
+    assert L.ves3d_sht_scale_freq(None, 1, 16, None, None, None) == 1
+    assert L.ves3d_sht_lowpass(out.ctypes.data, -1, 16, -1, 0.0, out.ctypes.data, None) == 1
+
+
 @pytest.mark.parametrize("p,p1", [(6, 12), (12, 24), (16, 32)])
 def test_host_tables_match_oracle(p, p1):
     T = _lib.tables_export
