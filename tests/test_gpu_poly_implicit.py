@@ -1,6 +1,6 @@
 """The implicit step of a polydisperse suspension (vesicles of different SH orders, forces
 at each vesicle's own order, one single layer over all points) against the CPU oracle's
-PolyImplicitStep: every solve is judged by its true residual through the oracle's Galerkin
+PolyImplicitStep: every solve is checked by its true residual through the oracle's Galerkin
 operator, FP64 throughout."""
 import numpy as np
 import pytest
