@@ -158,7 +158,7 @@ def test_learned_guess_saves_iterations(tmp_path):
     x0, info = initial_guess(sv, learned=g2)
     _, it1, _, c1 = sv.implicit_solve(x0=x0, tol=1e-10, max_iter=2000)
     assert c0 == 100 and c1 == 100
-    # judged by the true residual: the learned start is far closer than the zero start
+    # measured by the true residual: the learned start is far closer than the zero start
     # (relative residual 1), and the solve from it is shorter
     assert info["relres_combined"] < 0.1, info
     assert it1 < it0, (it0, it1, info)

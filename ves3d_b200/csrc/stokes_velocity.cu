@@ -2862,7 +2862,7 @@ extern "C" {
 // Residual-minimising combination of candidate guesses for the next implicit solve of a
 // polydisperse suspension (the uniform form: ves3d_sv_implicit_combine). The candidates'
 // images come from the operator the inner solves use (the FP32 far field in a mixed
-// context: a guess needs no more, and the solve that follows judges its result in FP64);
+// context: a guess needs no more, and the solve that follows checks its result in FP64);
 // the right-hand side is FP64 and is kept for that solve.
 int ves3d_svp_implicit_combine(ves3d_svp* g, int n_cand, const double* const* cand, double* x0, double* weights,
                                double* relres, int is_device) {
