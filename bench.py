@@ -197,16 +197,20 @@ def cpu_reference_rate(X, f, p, budget_s=20.0):
     per_thread = 64
     t_far = None
     while True:
-        nt = per_thread * cores
+        # a small workload has fewer targets than the sample wants: take all of them, on
+        # as many threads as there are targets
+        per_thread = max(1, min(per_thread, N // cores)) if N >= cores else 1
+        thr = max(1, min(cores, N // per_thread))
+        nt = per_thread * thr
         idx = rng.choice(N, size=nt, replace=False)
         trg = pos[:, idx]
         if kind == "reference":
-            src_rep = np.ascontiguousarray(np.broadcast_to(pos[None], (cores, 3, N)).reshape(-1))
-            den_rep = np.ascontiguousarray(np.broadcast_to(den[None], (cores, 3, N)).reshape(-1))
-            trg_rep = np.ascontiguousarray(trg.reshape(3, cores, per_thread).transpose(1, 0, 2).reshape(-1))
+            src_rep = np.ascontiguousarray(np.broadcast_to(pos[None], (thr, 3, N)).reshape(-1))
+            den_rep = np.ascontiguousarray(np.broadcast_to(den[None], (thr, 3, N)).reshape(-1))
+            trg_rep = np.ascontiguousarray(trg.reshape(3, thr, per_thread).transpose(1, 0, 2).reshape(-1))
             qw = np.ones(N)
             t3 = time.perf_counter()
-            reflib.direct_stokes(N, per_thread, cores, 0, per_thread, qw, trg_rep, src_rep, den_rep)
+            reflib.direct_stokes(N, per_thread, thr, 0, per_thread, qw, trg_rep, src_rep, den_rep)
             t4 = time.perf_counter()
         else:
             from oracle import stokes
@@ -214,7 +218,7 @@ def cpu_reference_rate(X, f, p, budget_s=20.0):
             stokes.far(X, f, np.arange(nves + 1) * ng, idx)
             t4 = time.perf_counter()
         t_far = (t4 - t3) * N / nt * (1.0 + 1.0 / nves)
-        if (t4 - t3) > 6.0 or per_thread >= 16384:
+        if (t4 - t3) > 6.0 or per_thread >= 16384 or nt + thr > N:
             break
         per_thread = int(per_thread * min(16.0, max(2.0, 8.0 / max(t4 - t3, 1e-3))))
     total = t_build + t_apply + t_far
