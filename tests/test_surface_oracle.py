@@ -168,3 +168,43 @@ def test_relaxing_vesicle_loses_bending_energy():
         X = X + dt * x[:X.size]
     assert E[0] > E[1] > E[2]
     assert abs(A[-1] / A[0] - 1) < 1e-5 and abs(V[-1] / V[0] - 1) < 1e-5
+
+
+def test_low_pass_filters():
+    """SHTrans's filters (oracle restatement): the hard cut keeps exactly the degrees up to
+    the cut and is idempotent; the polynomial filter weights degree n by 1 - (n/f)^e and
+    removes degrees >= f; both act per coefficient (ScaleFreq)."""
+    p = 12
+    rng = np.random.default_rng(4)
+    X = rng.standard_normal(3 * 2 * p * (p + 1))
+    hard = sh.low_pass(X, p)
+    assert np.abs(sh.low_pass(hard, p) - hard).max() < 1e-13
+    S = sh.grid2shc(hard, p, p).reshape(3, -1)
+    off = sh.block_offsets(p)
+    deg = np.concatenate([(jf + 1) // 2 + np.arange(off[jf + 1] - off[jf]) for jf in range(2 * p)])
+    assert np.abs(S[:, deg > 2 * p // 3]).max() < 1e-13
+    S0 = sh.grid2shc(X, p, p).reshape(3, -1)
+    assert np.abs(S[:, deg <= 2 * p // 3] - S0[:, deg <= 2 * p // 3]).max() < 1e-13
+    c = sh.filter_coeffs(p, 6, 4.0)
+    assert np.allclose(c[deg < 6], 1 - (deg[deg < 6] / 6.0) ** 4) and np.all(c[deg >= 6] == 0)
+    Sp = sh.grid2shc(sh.low_pass(X, p, 6, 4.0), p, p).reshape(3, -1)
+    assert np.abs(Sp - S0 * c[None, :]).max() < 1e-12
+
+
+def test_poly_sedimentation_solve_sinks():
+    """The oracle's polydisperse implicit step under gravity (-z, excess density 1): BiCGStab
+    meets the tolerance and the suspension sinks; without gravity and flow nothing moves
+    but the relaxation of the shapes."""
+    from ves3d_b200 import workloads
+    X, _, orders = workloads.polydisperse(3, orders=(4, 6), radius=(0.8, 1.2), volume_fraction=0.05, seed=8)
+    step = su.PolyImplicitStep(X, orders, 0.05, 0.01, 0.0, excess_density=1.0)
+    x, code, it, rr = step.solve(tol=1e-9, max_iter=600)
+    assert code == 100 and rr < 1e-9
+    us, _ = step.split(x)
+    uz = np.concatenate([u[:, 2].reshape(-1) for u in us])
+    assert uz.mean() < 0
+    rest = su.PolyImplicitStep(X, orders, 0.05, 0.01, 0.0)
+    x0, code0, _, _ = rest.solve(tol=1e-9, max_iter=600)
+    u0, _ = rest.split(x0)
+    assert code0 == 100
+    assert np.abs(np.concatenate([u[:, 2].reshape(-1) for u in u0]).mean()) < 0.1 * abs(uz.mean())
