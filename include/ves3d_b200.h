@@ -311,6 +311,13 @@ int ves3d_sht_forward(const double* X, long n_fun, int p0, int p1, double* S, vo
  * (X_theta) and latitude (X_phi) derivatives as named by the reference; NULL skips. */
 int ves3d_sht_backward(const double* S, long n_fun, int p0, int p1, double* X, double* X_theta,
                        double* X_phi, void* stream);
+/* SphericalHarmonics::RotateAll (src/SphericalHarmonics.cc:363-449), the coefficient
+ * rotation behind MovePole (include/MovePole.h:16-23): every vector field of S (device,
+ * [n_vec][3][p(p+2)] coefficients) rotated so that each grid point (latitude t = 0..p,
+ * longitude j = 0..p-1) moves to the north pole (its antipode to the south pole), into R
+ * (device, [n_vec][p+1][p][3][p(p+2)]). MovePole::operator()(t, j, ...) for j < p is the
+ * (t, j) slice. Builds the order-p rotation tables for the call. */
+int ves3d_sht_rotate_all(const double* S, long n_vec, int p, double* R, void* stream);
 /* SHTrans's frequency filters (constructor, src/SHTrans.cc:8-45) written to a host array of
  * p(p+2) values in the per-function coefficient order (Fourier blocks, degrees ascending):
  * exponent <= 0 gives lowPassFilter's hard cut (1 for degree n <= filter_freq, else 0),

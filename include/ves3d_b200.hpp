@@ -174,6 +174,12 @@ class SHTrans {
   Real exponent_;
 };
 
+/* SphericalHarmonics::RotateAll / MovePole on device pointers: S [n_vec][3][p(p+2)] ->
+ * R [n_vec][p+1][p][3][p(p+2)], grid point (t, j) moved to the pole. */
+inline void RotateAll(const double* S, long n_vec, int p, double* R, void* stream = 0) {
+  check(ves3d_sht_rotate_all(S, n_vec, p, R, stream), "RotateAll");
+}
+
 /* Device<GPU>::DirectStokes(src, den, qw, src_stride, trg_stride, n_surfs, trg,
  * trg_idx_head, trg_idx_tail, pot) on device pointers (cuda_stokes). */
 inline void DirectStokes(const double* src, const double* den, const double* qw, size_t src_stride,

@@ -45,6 +45,7 @@ SIGNATURES = [
     ("ves3d_sv_launch_eval_graph", _i, [_vp]),
     ("ves3d_sht_forward", _i, [_vp, _l, _i, _i, _vp, _vp]),
     ("ves3d_sht_backward", _i, [_vp, _l, _i, _i, _vp, _vp, _vp, _vp]),
+    ("ves3d_sht_rotate_all", _i, [_vp, _l, _i, _vp, _vp]),
     ("ves3d_sht_filter_coeffs", _i, [_i, _i, _d, _vp]),
     ("ves3d_sht_scale_freq", _i, [_vp, _l, _i, _vp, _vp, _vp]),
     ("ves3d_sht_lowpass", _i, [_vp, _l, _i, _i, _d, _vp, _vp]),

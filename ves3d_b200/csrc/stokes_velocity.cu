@@ -829,6 +829,22 @@ int ves3d_sht_backward(const double* S, long n_fun, int p0, int p1, double* X, d
   return VES3D_OK;
 }
 
+int ves3d_sht_rotate_all(const double* S, long n_vec, int p, double* R, void* stream) {
+  VES3D_ARG(S && R, "null pointer");
+  VES3D_ARG(p >= 1 && p <= 127, "order must be in [1, 127]");
+  VES3D_ARG(n_vec >= 0, "n_vec < 0");
+  if (n_vec == 0) return VES3D_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  TablesOwner tab;  // rotation blocks and phase tables of order p (freed on return)
+  build_tables(p, 2 * p, tab.h);
+  int s = tab.upload(st);
+  if (!s) s = launch_rotate_all(S, n_vec, tab.d, R, st);
+  const cudaError_t e = cudaStreamSynchronize(st);
+  if (s) return s;
+  VES3D_CK(e);
+  return VES3D_OK;
+}
+
 int ves3d_sht_filter_coeffs(int p, int filter_freq, double exponent, double* coeff) {
   VES3D_ARG(coeff != nullptr, "coeff is null");
   VES3D_ARG(p >= 1 && p <= 128, "order must be in [1, 128]");

@@ -292,6 +292,15 @@ class SHTrans:
         sc, _, _ = _ptr(scale)
         check(lib().ves3d_sht_scale_freq(a, n, self.p, sc, b, self.stream), "SHTrans.ScaleFreq")
 
+    def RotateAll(self, shc, out):
+        """SphericalHarmonics::RotateAll: vector fields [n][3][p(p+2)] -> every rotation
+        [n][p+1][p][3][p(p+2)] (grid point (t, j) to the pole; MovePole's (t, j) slice)."""
+        a, n = self._nfun(shc, 3 * ncoef(self.p))
+        b, m = self._nfun(out, 3 * ncoef(self.p))
+        if m != n * self.p * (self.p + 1):
+            raise ValueError("output must hold p(p+1) rotations of every vector field")
+        check(lib().ves3d_sht_rotate_all(a, n, self.p, b, self.stream), "SHTrans.RotateAll")
+
     def lowPassFilter(self, grid_in, grid_out):
         a, n = self._nfun(grid_in, ngrid(self.p))
         b, _ = self._nfun(grid_out, ngrid(self.p))
