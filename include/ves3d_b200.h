@@ -336,6 +336,26 @@ int ves3d_sht_lowpass(const double* in, long n_fun, int p, int filter_freq, doub
                       void* stream);
 
 /* ---------------------------------------------------------------------------
+ * Device<GPU> primitives (include/Device.h:81-253) on device pointers; each returns when
+ * its work on the stream is done.
+ * ------------------------------------------------------------------------- */
+/* Device::axpy (:158-160): out[i] = a x[i] + y[i], out may be y. */
+int ves3d_dev_axpy(double a, const double* x, const double* y, size_t length, double* out, void* stream);
+/* Device::AlgebraicDot (:228-229): *result (host) = sum_i x[i] y[i], fixed-order reduction. */
+int ves3d_dev_algebraic_dot(const double* x, const double* y, size_t length, double* result, void* stream);
+/* Device::Transpose (:225-226): out[j height + i] = in[i width + j], out of place. */
+int ves3d_dev_transpose(const double* in, size_t height, size_t width, double* out, void* stream);
+/* Device::Reduce (:181-183; src/DeviceCPU.cc:444-497): the smooth surface integral
+ * x_dw[s x_dim + d] = sum_i x[(s x_dim + d) stride + i] w[s stride + i] quad_w[i] for ns
+ * surfaces, or with x NULL x_dw[s] = sum_i w[s stride + i] quad_w[i] (the areas). */
+int ves3d_dev_reduce(const double* x, int x_dim, const double* w, const double* quad_w, size_t stride, size_t ns,
+                     double* x_dw, void* stream);
+/* Device::gemm (:199-203): C = alpha op(A) op(B) + beta C in column-major BLAS semantics
+ * (trans 'N', 'T' or 'C'), through cuBLAS. */
+int ves3d_dev_gemm(char trans_a, char trans_b, int m, int n, int k, double alpha, const double* A, int lda,
+                   const double* B, int ldb, double beta, double* C, int ldc, void* stream);
+
+/* ---------------------------------------------------------------------------
  * Direct Stokes sums on device pointers.
  * ves3d_cuda_stokes: same arguments and meaning as the reference's
  *   cuda_stokes(int src_m, int trg_m, int n, int t_head, int t_tail, const T* T,

@@ -174,6 +174,42 @@ class SHTrans {
   Real exponent_;
 };
 
+/* Device<GPU> (include/Device.h:81-253): the primitives a caller of the operators uses,
+ * on device pointers, with the reference's signatures (gemm takes its BLAS arguments by
+ * pointer as the reference's does). */
+class Device {
+ public:
+  explicit Device(void* stream = 0) : stream_(stream) {}
+  double* axpy(double a, const double* x, const double* y, size_t length, double* out) const {
+    check(ves3d_dev_axpy(a, x, y, length, out, stream_), "Device::axpy");
+    return out;
+  }
+  double AlgebraicDot(const double* x, const double* y, size_t length) const {
+    double r = 0;
+    check(ves3d_dev_algebraic_dot(x, y, length, &r, stream_), "Device::AlgebraicDot");
+    return r;
+  }
+  double* Transpose(const double* in, size_t height, size_t width, double* out) const {
+    check(ves3d_dev_transpose(in, height, width, out, stream_), "Device::Transpose");
+    return out;
+  }
+  double* Reduce(const double* x, int x_dim, const double* w, const double* quad_w, size_t stride, size_t ns,
+                 double* x_dw) const {
+    check(ves3d_dev_reduce(x, x_dim, w, quad_w, stride, ns, x_dw, stream_), "Device::Reduce");
+    return x_dw;
+  }
+  double* gemm(const char* transA, const char* transB, const int* m, const int* n, const int* k, const double* alpha,
+               const double* A, const int* lda, const double* B, const int* ldb, const double* beta, double* C,
+               const int* ldc) const {
+    check(ves3d_dev_gemm(*transA, *transB, *m, *n, *k, *alpha, A, *lda, B, *ldb, *beta, C, *ldc, stream_),
+          "Device::gemm");
+    return C;
+  }
+
+ private:
+  void* stream_;
+};
+
 /* SphericalHarmonics::RotateAll / MovePole on device pointers: S [n_vec][3][p(p+2)] ->
  * R [n_vec][p+1][p][3][p(p+2)], grid point (t, j) moved to the pole. */
 inline void RotateAll(const double* S, long n_vec, int p, double* R, void* stream = 0) {

@@ -70,6 +70,12 @@ def test_argument_errors_of_the_implicit_and_filter_entry_points():
     assert L.ves3d_sht_lowpass(None, 1, 16, -1, 0.0, None, None) == 1
     assert L.ves3d_sht_scale_freq(None, 1, 16, None, None, None) == 1
     assert L.ves3d_sht_lowpass(out.ctypes.data, -1, 16, -1, 0.0, out.ctypes.data, None) == 1
+    # Device primitives
+    assert L.ves3d_dev_axpy(1.0, None, None, 4, None, None) == 1
+    assert L.ves3d_dev_transpose(out.ctypes.data, 2, 2, out.ctypes.data, None) == 1
+    assert L.ves3d_dev_reduce(None, 0, None, None, 4, 1, None, None) == 1
+    assert L.ves3d_dev_gemm(b"X", b"N", 2, 2, 2, 1.0, None, 2, None, 2, 0.0, None, 2, None) == 1
+    assert L.ves3d_dev_gemm(b"N", b"N", -1, 2, 2, 1.0, None, 2, None, 2, 0.0, None, 2, None) == 1
 
 
 @pytest.mark.parametrize("p,p1", [(6, 12), (12, 24), (16, 32)])

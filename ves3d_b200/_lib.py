@@ -46,6 +46,11 @@ SIGNATURES = [
     ("ves3d_sht_forward", _i, [_vp, _l, _i, _i, _vp, _vp]),
     ("ves3d_sht_backward", _i, [_vp, _l, _i, _i, _vp, _vp, _vp, _vp]),
     ("ves3d_sht_rotate_all", _i, [_vp, _l, _i, _vp, _vp]),
+    ("ves3d_dev_axpy", _i, [_d, _vp, _vp, ctypes.c_size_t, _vp, _vp]),
+    ("ves3d_dev_algebraic_dot", _i, [_vp, _vp, ctypes.c_size_t, ctypes.POINTER(_d), _vp]),
+    ("ves3d_dev_transpose", _i, [_vp, ctypes.c_size_t, ctypes.c_size_t, _vp, _vp]),
+    ("ves3d_dev_reduce", _i, [_vp, _i, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _vp, _vp]),
+    ("ves3d_dev_gemm", _i, [ctypes.c_char, ctypes.c_char, _i, _i, _i, _d, _vp, _i, _vp, _i, _d, _vp, _i, _vp]),
     ("ves3d_sht_filter_coeffs", _i, [_i, _i, _d, _vp]),
     ("ves3d_sht_scale_freq", _i, [_vp, _l, _i, _vp, _vp, _vp]),
     ("ves3d_sht_lowpass", _i, [_vp, _l, _i, _i, _d, _vp, _vp]),
