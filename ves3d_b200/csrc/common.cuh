@@ -2,6 +2,7 @@
 // text, a global launch counter, and device helpers.
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <atomic>
 #include <cstdio>
@@ -41,6 +42,15 @@ inline int cuda_status(cudaError_t e, const char* what, const char* file, int li
       return VES3D_ERR_ARG;                                                     \
     }                                                                           \
   } while (0)
+
+// NVTX range over a scope ("ves3d <phase>"), for timelines in a profiler; without one
+// attached the push and pop do nothing (NVTX 3 is header-only).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 constexpr double kInv8Pi = 0.039788735772973836;  // 1/(8 pi)
 

@@ -365,6 +365,7 @@ int copy_out(double* dst, const double* src, size_t n, int is_device, cudaStream
 int alloc_scratch(ves3d_sv* sv);
 
 int run_setup(ves3d_sv* sv) {
+  NvtxRange nvtx("ves3d build");
   const DevTables& T = sv->tab->d;
   const int p0 = sv->p, p1 = sv->pup, nc = ncoef_(p0), ng = ngrid_(p0), M1 = ngrid_(p1);
   const long npr = (long)p0 * (p0 + 1);
@@ -419,6 +420,7 @@ int run_self(ves3d_sv* sv, double* vself, double* den) {
 
 // Self part alone: Vself = SHC2Grid(Grid2SHC(F) . SL) on the context's stream.
 int run_self_apply(ves3d_sv* sv) {
+  NvtxRange nvtx("ves3d self");
   const DevTables& T = sv->tab->d;
   const int p0 = sv->p, n = 3 * ncoef_(p0);
   cudaStream_t st = sv->stream;
@@ -433,6 +435,7 @@ int run_self_apply(ves3d_sv* sv) {
 // for everything the context's stream has queued (surfaces, densities, the previous
 // evaluation's reduce). ev_far[0..1] (may be null) bracket the segment kernels.
 int fork_far(ves3d_sv* sv, int* nseg, cudaEvent_t ev_far0, cudaEvent_t ev_far1) {
+  NvtxRange nvtx("ves3d far");
   const DevTables& T = sv->tab->d;
   int s;
   cudaStream_t fs = sv->overlap ? sv->side : sv->stream;
@@ -582,6 +585,7 @@ int ves3d_sv_set_stream(ves3d_sv* sv, void* stream) {
 }
 
 int ves3d_sv_set_src_coord(ves3d_sv* sv, const double* S, long n_ves, int is_device) {
+  NvtxRange nvtx("ves3d set_src_coord");
   int s = check_sv(sv);
   if (s) return s;
   VES3D_ARG(S != nullptr, "S is null");
@@ -1521,6 +1525,7 @@ SolverPool& solver_pool(int device) {
 }
 
 int build_self_block_precond(ves3d_sv* sv) {
+  NvtxRange nvtx("ves3d precond");
   int s;
   const int nc = ncoef_(sv->p), n = 4 * nc;
   const long nv = sv->nves, nn = (long)n * n;
@@ -1749,6 +1754,7 @@ int mixed_refinement(const SolveOps& ops, double* x, const double* b, long n, do
   double relres = 1e300;
   *code = 101;
   while (!s && outer < 30) {
+    NvtxRange nvtx("ves3d refine");
     // FP64 residual
     if ((s = ops.fp64(ops.ctx, x, ax))) break;
     if ((s = lincomb_f64(n, 1.0, b, -1.0, ax, 0.0, nullptr, r, st))) break;
@@ -2003,6 +2009,7 @@ int ves3d_sv_surface_op(ves3d_sv* sv, int op, const double* in, double* out, int
 
 int ves3d_sv_implicit_solve(ves3d_sv* sv, const double* x0, double* x, double* tol, int* max_iter, int* code,
                             int is_device) {
+  NvtxRange nvtx("ves3d implicit_solve");
   int s = check_sv(sv);
   if (s) return s;
   VES3D_ARG(x && tol && max_iter && code, "null argument");
@@ -2531,6 +2538,7 @@ static int svp_self_parts(ves3d_svp* g) {
 
 // one far-field pass over every point, launched per order group (block shape per group)
 static int svp_far(ves3d_svp* g) {
+  NvtxRange nvtx("ves3d far");
   const bool mixed = g->prec == VES3D_PREC_MIXED && !g->far_force_fp64;
   std::vector<FarGroup> fg;
   long v0 = 0;
@@ -2823,6 +2831,7 @@ int ves3d_svp_solver_stats(ves3d_svp* g, int* outer, int* inner) {
 
 int ves3d_svp_implicit_solve(ves3d_svp* g, const double* x0, double* x, double* tol, int* max_iter, int* code,
                              int is_device) {
+  NvtxRange nvtx("ves3d svp implicit_solve");
   VES3D_ARG(g && x && tol && max_iter && code, "null argument");
   if (g->grp.empty()) {
     set_error("no surfaces set");
