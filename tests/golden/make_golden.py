@@ -55,8 +55,19 @@ def dumbbell(reference_root="/root/reference"):
                         max_abs_H_plus_half_div_n=0.2437253515, rtol_mixed=1e-6)
 
 
+def streamable(ref_stream=None):
+    """The reference's own Streamable ASCII output (oracle/_ref/ref_stream, built from
+    src/Array.cc, Scalars.cc, Vectors.cc by oracle/ref/Makefile): a Vectors of 2 vectors at
+    p = 4 and a Scalars, written as its checkpoints are (scientific, 16 digits)."""
+    import subprocess
+    ref_stream = ref_stream or os.path.join(os.path.dirname(os.path.dirname(HERE)), "oracle", "_ref", "ref_stream")
+    out = os.path.join(HERE, "ref_stream_p4.txt")
+    subprocess.check_call([ref_stream, "pack", "4", "2", out], env=dict(os.environ, VES3D_DIR="/root/reference"))
+
+
 def main():
     dumbbell()
+    streamable()
     assert reflib.available(), "build oracle/_ref first (make -C oracle/ref)"
     reflib.set_threads(os.cpu_count() or 1)
     # p = 6: two ellipsoids; quadrature rules, transforms, the self matrix of vesicle 0
