@@ -29,7 +29,8 @@ enum ves3d_status {
   VES3D_ERR_NOMEM = 3,    /* device or pinned host allocation failed */
   VES3D_ERR_STATE = 4,    /* call out of order (e.g. eval before set_src_coord) */
   VES3D_ERR_NODEV = 5,    /* no CUDA device / not an sm_100 device */
-  VES3D_ERR_NUMERIC = 6   /* non-finite input or result detected */
+  VES3D_ERR_NUMERIC = 6,  /* non-finite input or result detected */
+  VES3D_ERR_IO = 7        /* a file could not be written */
 };
 
 enum ves3d_precision {
@@ -334,6 +335,10 @@ int ves3d_sht_scale_freq(const double* shc_in, long n_fun, int p, const double* 
  * order p: analysis, the filter of ves3d_sht_filter_coeffs, synthesis; in place allowed. */
 int ves3d_sht_lowpass(const double* in, long n_fun, int p, int filter_freq, double exponent, double* out,
                       void* stream);
+/* SphericalHarmonics::SHC2Pole (src/SphericalHarmonics.cc:325-360): P[2 f + t] = the value
+ * of function f at x = -1 (t = 0) and x = +1 (t = 1), from the m = 0 block of its order-p
+ * coefficients S ([n_fun][p(p+2)], the layout of ves3d_sht_forward). Device pointers. */
+int ves3d_sht_pole(const double* S, long n_fun, int p, double* P, void* stream);
 
 /* ---------------------------------------------------------------------------
  * Device<GPU> primitives (include/Device.h:81-253) on device pointers; each returns when
@@ -393,6 +398,26 @@ int ves3d_stokes_alltoall_device_f64(const double* src, const double* den, size_
 #define VES3D_NOALLOC_MAX_POINTS 524288
 int ves3d_stokes_alltoall_noalloc_f64(const double* src, const double* den, size_t np, double* pot,
                                       void* stream);
+
+/* ---------------------------------------------------------------------------
+ * VTK output of surfaces (WriteVTK, src/StokesVelocity.cc:773-993): one XML PolyData file
+ * <fname>_<rank as 6 digits>.vtp per rank with raw appended data, and from rank 0 the index
+ * <fname>.pvtp naming the n_ranks pieces. Per vesicle the points are the (p1+1) x 2p1 grid
+ * of order p1 (latitude-major) followed by the poles at x = -1 and x = +1; the polygons are
+ * 2p1 pairs of pole triangles, then p1 x 2p1 quads. The optional field becomes the point
+ * data "value" (3 components). With period > 0 each vesicle is shifted by the multiple of
+ * period nearest its mean point (the field is not shifted).
+ * ------------------------------------------------------------------------- */
+/* The writer alone, host only (no GPU needed): host arrays X1 (and V1)
+ * [n_ves][3][(p1+1) 2p1] of grid values at order p1 and Xp (and Vp) [n_ves][3][2] of pole
+ * values (x = -1, then x = +1); V1 and Vp NULL write no point data. */
+int ves3d_vtk_write_grid(const double* X1, const double* Xp, const double* V1, const double* Vp, long n_ves,
+                         int p1, const char* fname, double period, int rank, int n_ranks);
+/* WriteVTK(S, p0, p1, fname, period, v_ptr, comm): positions X (and the optional field V,
+ * NULL for none) [n_ves][3][(p0+1) 2p0] at order p0, host or device pointers, taken to order
+ * p1 on the GPU (Grid2SHC at p0, SHC2Grid at p1, SHC2Pole) and written as above. */
+int ves3d_vtk_write(const double* X, const double* V, long n_ves, int p0, int p1, const char* fname, double period,
+                    int rank, int n_ranks, int is_device);
 
 /* ---------------------------------------------------------------------------
  * Diagnostics (host only, no GPU needed): copy one of the FP64 operator tables the

@@ -166,6 +166,10 @@ class SHTrans {
   void backward_to(int q, const Real* shc, long n_funs, Real* out) const {
     check(ves3d_sht_backward(shc, n_funs, p_, q, out, 0, 0, stream_), "SHTrans::backward_to");
   }
+  /* SphericalHarmonics::SHC2Pole: pole[2 f + t] = function f at x = -1 (t = 0), x = +1 (t = 1) */
+  void SHC2Pole(const Real* shc, long n_funs, Real* pole) const {
+    check(ves3d_sht_pole(shc, n_funs, p_, pole, stream_), "SHTrans::SHC2Pole");
+  }
 
  private:
   int p_;
@@ -214,6 +218,22 @@ class Device {
  * R [n_vec][p+1][p][3][p(p+2)], grid point (t, j) moved to the pole. */
 inline void RotateAll(const double* S, long n_vec, int p, double* R, void* stream = 0) {
   check(ves3d_sht_rotate_all(S, n_vec, p, R, stream), "RotateAll");
+}
+
+/* WriteVTK(S, p0, p1, fname, period, v_ptr, comm) (src/StokesVelocity.cc:773-993): the
+ * surfaces S (and the field v, or NULL) of order p0, host arrays [n_ves][3][(p0+1) 2p0],
+ * taken to order p1 on the GPU and written as <fname>_<rank>.vtp, plus <fname>.pvtp from
+ * rank 0. The communicator becomes its rank and size. */
+template <class Vec>
+void WriteVTK(const Vec& S, long p0, long p1, const char* fname, double period = 0, const Vec* v_ptr = 0,
+              int rank = 0, int n_ranks = 1) {
+  const size_t per = (size_t)3 * 2 * p0 * (p0 + 1);
+  if (S.size() % per) throw Error(VES3D_ERR_ARG, "WriteVTK: size is not a multiple of 3 (p0+1) 2p0");
+  if (v_ptr && v_ptr->size() != S.size()) throw Error(VES3D_ERR_ARG, "WriteVTK: field size differs from S");
+  const long n_ves = (long)(S.size() / per);
+  check(ves3d_vtk_write(n_ves ? &S[0] : 0, v_ptr && n_ves ? &(*v_ptr)[0] : 0, n_ves, (int)p0, (int)p1, fname, period,
+                        rank, n_ranks, /*is_device=*/0),
+        "WriteVTK");
 }
 
 /* Device<GPU>::DirectStokes(src, den, qw, src_stride, trg_stride, n_surfs, trg,

@@ -4,12 +4,32 @@
 //   api_test --filter p f e       prints SHTrans's two filters (no GPU needed)
 //   api_test <in.bin> <out.bin>   in: int32 p, int32 n_ves, X[n], f[n] (doubles, AxisMajor);
 //                                 out: vel[n] then the implicit solution x[4 n / 3]
+//   api_test --vtk <in.bin> p1 f  WriteVTK of in.bin's surfaces (field: its f) at order p1
+//                                 into f_000000.vtp and f.pvtp
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <vector>
 
 #include "ves3d_b200.hpp"
+
+// in.bin: int32 p, int32 n_ves, X[n], f[n] (doubles, AxisMajor); false on a short file
+static bool read_input(const char* path, int& p, int& nv, std::vector<double>& X, std::vector<double>& f) {
+  std::FILE* fi = std::fopen(path, "rb");
+  if (!fi) return false;
+  int hdr[2];
+  bool ok = std::fread(hdr, sizeof(int), 2, fi) == 2;
+  if (ok) {
+    p = hdr[0];
+    nv = hdr[1];
+    const size_t n = (size_t)nv * 3 * 2 * p * (p + 1);
+    X.resize(n);
+    f.resize(n);
+    ok = std::fread(&X[0], sizeof(double), n, fi) == n && std::fread(&f[0], sizeof(double), n, fi) == n;
+  }
+  std::fclose(fi);
+  return ok;
+}
 
 int main(int argc, char** argv) {
   if (argc == 2 && std::strcmp(argv[1], "--version") == 0) {
@@ -26,19 +46,27 @@ int main(int argc, char** argv) {
     std::printf("%d %.17g\n", sht.getShFilterFreq(), sht.getShFilterExponent());
     return 0;
   }
+  if (argc == 5 && std::strcmp(argv[1], "--vtk") == 0) {
+    int p = 0, nv = 0;
+    std::vector<double> X, f;
+    if (!read_input(argv[2], p, nv, X, f)) return 3;
+    try {
+      ves3d_b200::WriteVTK(X, p, std::atoi(argv[3]), argv[4], 0.0, &f);
+    } catch (const ves3d_b200::Error& e) {
+      std::fprintf(stderr, "%s\n", e.what());
+      return 1;
+    }
+    return 0;
+  }
   if (argc != 3) {
     std::fprintf(stderr, "usage: api_test --version | api_test in.bin out.bin\n");
     return 2;
   }
-  std::FILE* fi = std::fopen(argv[1], "rb");
-  if (!fi) return 3;
-  int hdr[2];
-  if (std::fread(hdr, sizeof(int), 2, fi) != 2) return 3;
-  const int p = hdr[0], nv = hdr[1];
-  const size_t n = (size_t)nv * 3 * 2 * p * (p + 1);
-  std::vector<double> X(n), f(n), vel(n), x(4 * n / 3);
-  if (std::fread(&X[0], sizeof(double), n, fi) != n || std::fread(&f[0], sizeof(double), n, fi) != n) return 3;
-  std::fclose(fi);
+  int p = 0, nv = 0;
+  std::vector<double> X, f;
+  if (!read_input(argv[1], p, nv, X, f)) return 3;
+  const size_t n = X.size();
+  std::vector<double> vel(n), x(4 * n / 3);
   try {
     ves3d_b200::StokesVelocity<double> stokes(p, 2 * p);
     stokes.SetSrcCoord(X);

@@ -8,7 +8,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libves3d_b200.so")
 
 VES3D_OK = 0
-STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_NOMEM", 4: "ERR_STATE", 5: "ERR_NODEV", 6: "ERR_NUMERIC"}
+STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_NOMEM", 4: "ERR_STATE", 5: "ERR_NODEV", 6: "ERR_NUMERIC",
+          7: "ERR_IO"}
 PREC_FP64 = 0
 PREC_MIXED = 1
 
@@ -54,6 +55,9 @@ SIGNATURES = [
     ("ves3d_sht_filter_coeffs", _i, [_i, _i, _d, _vp]),
     ("ves3d_sht_scale_freq", _i, [_vp, _l, _i, _vp, _vp, _vp]),
     ("ves3d_sht_lowpass", _i, [_vp, _l, _i, _i, _d, _vp, _vp]),
+    ("ves3d_sht_pole", _i, [_vp, _l, _i, _vp, _vp]),
+    ("ves3d_vtk_write_grid", _i, [_vp, _vp, _vp, _vp, _l, _i, ctypes.c_char_p, _d, _i, _i]),
+    ("ves3d_vtk_write", _i, [_vp, _vp, _l, _i, _i, ctypes.c_char_p, _d, _i, _i, _i]),
     ("ves3d_cuda_stokes_f64", _i, [_i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("ves3d_stokes_alltoall_f64", None, [_vp, _vp, _sz, _vp, ctypes.POINTER(_vp)]),
     ("ves3d_interaction_free", None, [ctypes.POINTER(_vp)]),

@@ -7,7 +7,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libves3d_b200.so")
 SOURCES = ["sh_tables.cc", "sht_kernels.cu", "singular_kernels.cu", "direct_kernels.cu", "far_kernels.cu", "build_kernels.cu", "stokes_velocity.cu",
-           "peak_probe.cu", "noalloc.cu", "geometry_kernels.cu", "bicgstab.cu", "mlp.cu", "device_prims.cu"]
+           "peak_probe.cu", "noalloc.cu", "geometry_kernels.cu", "bicgstab.cu", "mlp.cu", "device_prims.cu",
+           "vtk_output.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared", "-Wno-deprecated-gpu-targets"]
 

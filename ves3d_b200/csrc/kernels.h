@@ -40,6 +40,9 @@ int launch_grid2shc(const double* in, long nfun, int p, const double* four, cons
                     double* out, cudaStream_t st);
 // shc_out[f][c] = shc_in[f][c] * scale[c] for nfun functions of nc coefficients
 int launch_scale_freq(const double* in, long nfun, int nc, const double* scale, double* out, cudaStream_t st);
+// SHC2Pole: P[2 f + t] = values of function f at x = -1 (t = 0) and x = +1 (t = 1) from its
+// order-p0 coefficients; qp = [2][p0+1] pole weights.
+int launch_shc2pole(const double* S, long nfun, int p0, const double* qp, double* P, cudaStream_t st);
 int launch_synthesis(const double* S, long nfun, int p0, int q, const double* leg, const double* dleg,
                      const double* four, const double* dfour, const int* blk_off, double* X, double* Xt,
                      double* Xp, cudaStream_t st);

@@ -226,6 +226,17 @@ void host_grid2shc(const AnalysisTables& A, const double* X, long nfun, double* 
   }
 }
 
+void pole_table(int p0, std::vector<double>& qp) {
+  const double s2p = std::sqrt(2.0 * kPi);
+  const double xm[2] = {-1.0, 1.0};
+  std::vector<double> alp((size_t)(p0 + 1) * (p0 + 2) / 2);
+  qp.assign((size_t)2 * (p0 + 1), 0.0);
+  for (int t = 0; t < 2; t++) {
+    legpoly(&xm[t], nullptr, 1, p0, alp.data());
+    for (int n = 0; n <= p0; n++) qp[(size_t)t * (p0 + 1) + n] = alp[n] * s2p;
+  }
+}
+
 void build_tables(int p0, int p1, ShTables& T) {
   T.p0 = p0;
   T.p1 = p1;
@@ -387,15 +398,7 @@ void build_tables(int p0, int p1, ShTables& T) {
   }
   T.smooth_w0.assign(p0 + 1, 0.0);
   for (int i = 0; i <= p0; i++) T.smooth_w0[i] = T.w0[i] * kPi / p0 / std::sqrt(1.0 - T.x0[i] * T.x0[i]);
-  {
-    double xm[2] = {-1.0, 1.0};
-    std::vector<double> alp(na);
-    T.qp.assign((size_t)2 * (p0 + 1), 0.0);
-    for (int t = 0; t < 2; t++) {
-      legpoly(&xm[t], nullptr, 1, p0, alp.data());
-      for (int n = 0; n <= p0; n++) T.qp[(size_t)t * (p0 + 1) + n] = alp[n] * s2p;
-    }
-  }
+  pole_table(p0, T.qp);
   T.cos_tab.assign(2 * p0, 0.0);
   T.sin_tab.assign(2 * p0, 0.0);
   for (int q = 0; q < 2 * p0; q++) {

@@ -72,6 +72,9 @@ struct ShTables {
 };
 
 void build_tables(int p0, int p1, ShTables& T);
+// SHC2Pole's weights (src/SphericalHarmonics.cc:325-338): [2][p0+1], the m = 0 block's
+// normalised Legendre functions times sqrt(2 pi) at x = -1 (row 0) and x = +1 (row 1).
+void pole_table(int p0, std::vector<double>& qp);
 
 // Stand-alone transform tables for SHC2Grid(p0, q) and Grid2SHC(pin, pout).
 void build_synth_tables(int p0, int q, SynthTables& S);

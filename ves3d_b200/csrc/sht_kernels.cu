@@ -273,6 +273,33 @@ int launch_scale_freq(const double* in, long nfun, int nc, const double* scale, 
   return VES3D_OK;
 }
 
+// SHC2Pole (src/SphericalHarmonics.cc:325-360): the values of every function at x = -1
+// and x = +1 from its m = 0 block, P[2f + t] = sum_n S[f][n] qp[t][n], summed in degree order
+// like the reference. One thread per function; the data is n_fun (p0 + 1) doubles, so the
+// strided reads cost nothing next to the transforms around it.
+__global__ void k_shc2pole(const double* __restrict__ S, long nfun, int nc, int p0, const double* __restrict__ qp,
+                           double* __restrict__ P) {
+  for (long f = blockIdx.x * (long)blockDim.x + threadIdx.x; f < nfun; f += (long)gridDim.x * blockDim.x) {
+    const double* s = S + f * nc;
+    double a = 0.0, b = 0.0;
+    for (int n = 0; n <= p0; n++) {
+      const double c = s[n];
+      a += c * qp[n];
+      b += c * qp[p0 + 1 + n];
+    }
+    P[2 * f] = a;
+    P[2 * f + 1] = b;
+  }
+}
+
+int launch_shc2pole(const double* S, long nfun, int p0, const double* qp, double* P, cudaStream_t st) {
+  if (nfun <= 0) return VES3D_OK;
+  const long b = std::min((nfun + 255) / 256, 4096L);
+  k_shc2pole<<<(unsigned)b, 256, 0, st>>>(S, nfun, p0 * (p0 + 2), p0, qp, P);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
 static int sm_count() {
   static int n = 0;
   if (!n) {

@@ -905,6 +905,24 @@ int ves3d_sht_lowpass(const double* in, long n_fun, int p, int filter_freq, doub
   return s;
 }
 
+int ves3d_sht_pole(const double* S, long n_fun, int p, double* P, void* stream) {
+  VES3D_ARG(S && P, "null pointer");
+  VES3D_ARG(p >= 1 && p <= 128, "order must be in [1, 128]");
+  VES3D_ARG(n_fun >= 0, "n_fun < 0");
+  if (n_fun == 0) return VES3D_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  std::vector<double> qp;
+  pole_table(p, qp);
+  double* dq = nullptr;
+  int s = dupload(&dq, qp, st);
+  if (!s) s = launch_shc2pole(S, n_fun, p, dq, P, st);
+  const cudaError_t e = cudaStreamSynchronize(st);
+  dfree(dq);
+  if (s) return s;
+  VES3D_CK(e);
+  return VES3D_OK;
+}
+
 int ves3d_tables_export(int p0, int p1, const char* name, double* out, size_t cap, size_t* n) {
   VES3D_ARG(name != nullptr && n != nullptr, "null argument");
   VES3D_ARG(p0 >= 2 && p0 <= 64 && p1 >= p0 && p1 <= 128, "orders out of range");
