@@ -12,6 +12,7 @@
 //   ref_singular_sl     SphericalHarmonics<double>::StokesSingularInteg  :863 (SL and/or DL)
 //   ref_alltoall        StokesAlltoAll (double)                    src/CPUKernels.cc:1011
 //   ref_direct_stokes   DirectStokesKernel (double)               src/CPUKernels.cc:123
+//   ref_direct_stokes_dl DirectStokesDoubleLayerKernel (double)   src/CPUKernels.cc:1060
 //   ref_bicgstab_dense  BiCGStab<Container, MatVec, Precond>  src/BiCGStab.cc:45-138
 //   ref_stokes_velocity_sl  the non-FMM StokesVelocity composition:
 //       u = SHC2Grid(Grid2SHC(f) . SLMatrix)                        (src/StokesVelocity.cc:385-473)
@@ -105,6 +106,14 @@ int ref_direct_stokes(int src_stride, int trg_stride, int n_surfs, int trg_idx_h
                       const double* qw, const double* trg, const double* src, const double* den,
                       double* pot) {
   DirectStokesKernel(src_stride, trg_stride, n_surfs, trg_idx_head, trg_idx_tail, qw, trg, src, den, pot);
+  return 0;
+}
+
+extern "C" int ref_direct_stokes_dl(int src_stride, int trg_stride, int n_surfs, int trg_idx_head,
+                                    int trg_idx_tail, const double* qw, const double* trg, const double* src,
+                                    const double* norm, const double* den, double* pot) {
+  DirectStokesDoubleLayerKernel(src_stride, trg_stride, n_surfs, trg_idx_head, trg_idx_tail, qw, trg, src, norm, den,
+                                pot);
   return 0;
 }
 

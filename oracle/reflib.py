@@ -29,7 +29,7 @@ def _load(path):
     L = ctypes.CDLL(path)
     for name in ("ref_grid2shc", "ref_shc2grid", "ref_shc2pole", "ref_rotate_all",
                  "ref_legendre_nodes", "ref_legendre_weights", "ref_singular_weights",
-                 "ref_singular_matrices", "ref_alltoall", "ref_direct_stokes",
+                 "ref_singular_matrices", "ref_alltoall", "ref_direct_stokes", "ref_direct_stokes_dl",
                  "ref_area_weights", "ref_self_apply", "ref_far_sl",
                  "ref_stokes_velocity_sl", "ref_set_threads"):
         getattr(L, name).restype = ctypes.c_int
@@ -129,6 +129,15 @@ def direct_stokes(src_stride, trg_stride, n_surfs, head, tail, qw, trg, src, den
     pot = np.zeros(3 * n_surfs * trg_stride)
     c = ctypes.c_int
     lib().ref_direct_stokes(c(src_stride), c(trg_stride), c(n_surfs), c(head), c(tail), _p(qw), _p(trg), _p(src), _p(den), _p(pot))
+    return pot
+
+
+def direct_stokes_dl(src_stride, trg_stride, n_surfs, head, tail, qw, trg, src, norm, den):
+    """DirectStokesDoubleLayerKernel (double); qw None for the unweighted form."""
+    pot = np.zeros(3 * n_surfs * trg_stride)
+    c = ctypes.c_int
+    lib().ref_direct_stokes_dl(c(src_stride), c(trg_stride), c(n_surfs), c(head), c(tail), _p(qw), _p(trg), _p(src),
+                               _p(norm), _p(den), _p(pot))
     return pot
 
 

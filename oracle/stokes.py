@@ -46,7 +46,8 @@ def direct_lib():
     if _direct is None:
         build_direct()
         _direct = ctypes.CDLL(DIRECT_SO)
-        for n in ("oracle_alltoall", "oracle_direct_stokes", "oracle_far"):
+        for n in ("oracle_alltoall", "oracle_direct_stokes", "oracle_far", "oracle_direct_stokes_dl",
+                  "oracle_far_dl"):
             getattr(_direct, n).restype = None
     return _direct
 
@@ -122,6 +123,51 @@ def stokes_velocity_sl(X, f, p, p_up=None, SL=None):
     if SL is None:
         SL = sh.stokes_singular_matrix(X, p, p_up)
     return sh.self_apply(SL, f, p) + far_velocity(X, f, p)
+
+
+def direct_stokes_dl(src_stride, trg_stride, n_surfs, head, tail, qw, trg, src, norm, den):
+    """DirectStokesDoubleLayerKernel: per-surface double layer, qw None for no weights."""
+    pot = np.zeros(3 * n_surfs * trg_stride)
+    c = ctypes.c_int
+    direct_lib().oracle_direct_stokes_dl(c(src_stride), c(trg_stride), c(n_surfs), c(head), c(tail),
+                                         None if qw is None else _p(np.ascontiguousarray(qw, np.float64)),
+                                         _p(np.ascontiguousarray(trg, np.float64)),
+                                         _p(np.ascontiguousarray(src, np.float64)),
+                                         _p(np.ascontiguousarray(norm, np.float64)),
+                                         _p(np.ascontiguousarray(den, np.float64)), _p(pot))
+    return pot
+
+
+def unit_normal(X, p):
+    """(X_theta x X_phi) / |X_theta x X_phi| on the order-p grid, AxisMajor like X: the
+    outward normal (src/StokesVelocity.cc:245-275)."""
+    ng = sh.ngrid(p)
+    S = sh.grid2shc(X, p, p)
+    _, Xt, Xp = sh.shc2grid(S, p, p, grads=True)
+    n = np.cross(Xt.reshape(-1, 3, ng), Xp.reshape(-1, 3, ng), axis=1)
+    return (n / np.sqrt((n * n).sum(axis=1))[:, None, :]).reshape(-1)
+
+
+def far_dl_velocity(X, g, p):
+    """Far double layer at every point, AxisMajor: the points of the other vesicles with unit
+    normals and densities g * area * qw (the single layer's composition)."""
+    ng = sh.ngrid(p)
+    nves = np.asarray(X).size // (3 * ng)
+    D = far_density(X, g, p)
+    out = np.empty(3 * nves * ng)
+    direct_lib().oracle_far_dl(_p(np.ascontiguousarray(X, np.float64)), _p(unit_normal(X, p)), _p(D),
+                               ctypes.c_long(nves), uniform_offsets(nves, p).ctypes.data_as(_lp), _p(out))
+    return out.reshape(nves, ng, 3).transpose(0, 2, 1).reshape(-1)
+
+
+def stokes_velocity_dl(X, g, p, p_up=None, DL=None):
+    """Full FP64 double-layer velocity at the surface grid points, AxisMajor: the self part
+    by the DL matrix (src/StokesVelocity.cc:418-436) plus the far double layer."""
+    if p_up is None:
+        p_up = 2 * p
+    if DL is None:
+        DL = sh.stokes_singular_matrix(X, p, p_up, single=False)
+    return sh.self_apply(DL, g, p) + far_dl_velocity(X, g, p)
 
 
 def stokes_velocity_poly(X, f, orders):

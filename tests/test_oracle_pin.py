@@ -140,3 +140,83 @@ def test_full_composition_c1(ref):
     ours = stokes.stokes_velocity_sl(X, f, p)
     theirs, _ = ref.stokes_velocity_sl(X, f, p, 2 * p)
     assert rel_err(ours, theirs) < REF_SELF_NOISE
+
+
+# ---- double layer -------------------------------------------------------------------
+
+@pytest.mark.parametrize("p", [6, 12])
+def test_double_layer_self_vs_reference(ref, p):
+    """The oracle's DL self matrix (StokesSingularInteg with DLMatrix) against the
+    reference's, through the self velocity, within the reference's self-part noise."""
+    X = ellipsoid_pair(p)
+    g = np.random.default_rng(p).standard_normal(X.size)
+    _, DL = ref.singular_matrices(X, p, 2 * p, sl=False, dl=True)
+    theirs = ref.self_apply(DL, g, p)
+    assert rel_err(sh.self_apply(sh.stokes_singular_matrix(X, p, 2 * p, single=False), g, p), theirs) < REF_SELF_NOISE
+    ours_u = sh.self_apply(sh.stokes_singular_matrix(X, p, 2 * p, single=False, stable=False), g, p)
+    assert rel_err(ours_u, theirs) < REF_SELF_NOISE
+
+
+def test_double_layer_direct_vs_reference(ref):
+    """oracle_direct_stokes_dl against DirectStokesDoubleLayerKernel, with and without
+    weights, a coincident pair included."""
+    rng = np.random.default_rng(11)
+    ns, nt, nv = 40, 30, 3
+    S = rng.standard_normal(3 * ns * nv)
+    T = rng.standard_normal(3 * nt * nv)
+    T[0], T[nt], T[2 * nt] = S[0], S[ns], S[2 * ns]  # target 0 of surface 0 on source 0
+    N = rng.standard_normal(3 * ns * nv)
+    D = rng.standard_normal(3 * ns * nv)
+    Q = rng.uniform(0.5, 1.5, ns)
+    for q in (Q, None):
+        a = stokes.direct_stokes_dl(ns, nt, nv, 0, 25, q, T, S, N, D)
+        b = ref.direct_stokes_dl(ns, nt, nv, 0, 25, q, T, S, N, D)
+        assert rel_err(a, b) < FAR_TOL
+
+
+@pytest.mark.parametrize("p", [6, 8])
+def test_far_double_layer_vs_reference(ref, p):
+    """The far double layer (other vesicles only) = the reference's DL kernel over all
+    points as one surface minus its per-vesicle sums."""
+    from tests.helpers import small_suspension
+    X, g = small_suspension(2, p, seed=5)
+    ng = sh.ngrid(p)
+    nv = X.size // (3 * ng)
+    N = stokes.unit_normal(X, p)
+    D = stokes.far_density(X, g, p)
+
+    def whole(A):
+        return A.reshape(nv, 3, ng).transpose(1, 0, 2).reshape(-1)
+
+    allp = ref.direct_stokes_dl(nv * ng, nv * ng, 1, 0, nv * ng, None, whole(X), whole(X), whole(N), whole(D))
+    allp = allp.reshape(3, nv, ng).transpose(1, 0, 2).reshape(-1)
+    own = ref.direct_stokes_dl(ng, ng, nv, 0, ng, None, X, X, N, D)
+    assert rel_err(stokes.far_dl_velocity(X, g, p), allp - own) < 1e-12
+    assert rel_err(N.reshape(nv, 3, ng) * sh.area_element(X, p)[:, None, :],
+                   np.cross(*[a.reshape(nv, 3, ng) for a in sh.shc2grid(sh.grid2shc(X, p, p), p, p, grads=True)[1:]],
+                            axis=1)) < PRIM_TOL
+
+
+@pytest.mark.parametrize("p,tol", [(8, 5e-4), (12, 1e-5), (16, 1e-7)])
+def test_double_layer_of_constant_densities(p, tol):
+    """Gauss's identity for the Stokes double layer: a constant density c on a closed
+    surface gives -c/2 on the surface (outward normal) and nothing outside it, so with a
+    constant per vesicle the total (self + far) is -c_v/2 on every vesicle; the error
+    falls spectrally with p (measured 1.7e-4, 2.1e-6, 2.1e-8)."""
+    from tests.helpers import small_suspension
+    X, _ = small_suspension(2, p, seed=3)
+    ng = sh.ngrid(p)
+    nv = X.size // (3 * ng)
+    C = np.random.default_rng(1).standard_normal((nv, 3))
+    g = np.repeat(C[:, :, None], ng, axis=2).reshape(-1)
+    u = stokes.stokes_velocity_dl(X, g, p).reshape(nv, 3, ng)
+    assert np.abs(u + 0.5 * C[:, :, None]).max() < tol
+
+
+def test_double_layer_sphere_identity():
+    p = 8
+    X = unit_sphere(p)
+    c = np.array([0.3, -1.0, 0.5])
+    g = np.repeat(c[:, None], sh.ngrid(p), axis=1).reshape(-1)
+    u = sh.self_apply(sh.stokes_singular_matrix(X, p, 2 * p, single=False), g, p).reshape(3, -1)
+    assert np.abs(u + 0.5 * c[:, None]).max() < 1e-13
