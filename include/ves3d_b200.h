@@ -46,10 +46,11 @@ long long ves3d_kernel_launches(void);
 /* ---------------------------------------------------------------------------
  * StokesVelocity operator context.
  * Replaces StokesVelocity<Real> (include/StokesVelocity.h:16-44,
- * src/StokesVelocity.cc:11-539) for surface targets, single layer:
+ * src/StokesVelocity.cc:11-539) for surface targets, single and double layer:
  *   StokesVelocity(sh_order, sh_order_up)      -> ves3d_sv_create
  *   SetSrcCoord(S, up_self, up)                -> ves3d_sv_set_src_coord
  *   SetDensitySL(f)                            -> ves3d_sv_set_density_sl
+ *   SetDensityDL(f)                            -> ves3d_sv_set_density_dl
  *   operator()(vel)                            -> ves3d_sv_eval
  * The far field is the exact all-pairs sum over other vesicles' grid points
  * (StokesAlltoAll - DirectStokesKernel, src/InterfacialVelocity.cc:1261-1291) in
@@ -70,6 +71,17 @@ int ves3d_sv_set_stream(ves3d_sv* sv, void* stream);
 int ves3d_sv_set_src_coord(ves3d_sv* sv, const double* S, long n_ves, int is_device);
 /* Single-layer density, same layout as the surfaces (src/StokesVelocity.cc:66-97). */
 int ves3d_sv_set_density_sl(ves3d_sv* sv, const double* f, int is_device);
+/* Double-layer density, same layout (src/StokesVelocity.cc:107-142); NULL turns the double
+ * layer off. While set, ves3d_sv_eval adds its velocity: the self part through the DL
+ * matrices of StokesSingularInteg (src/StokesVelocity.cc:418-436) and the far part as the
+ * exact FP64 sum over the other vesicles' points of the reference's double-layer kernel
+ * (stokes_dl_uKernel, src/PVFMMInterface.cc:285-360) with unit outward normals and
+ * densities times area and smooth weights (in both precision forms). Cleared by
+ * ves3d_sv_set_src_coord; the implicit step applies the single layer alone. */
+int ves3d_sv_set_density_dl(ves3d_sv* sv, const double* f, int is_device);
+/* Copy the double-layer self matrices out, [n_ves][3Ncoef][3Ncoef] (needs a double-layer
+ * density; builds them if the surfaces changed). */
+int ves3d_sv_get_dl_matrix(ves3d_sv* sv, double* DL, int is_device);
 /* Velocity at the surface points, same layout (src/StokesVelocity.cc:164-539).
  * Builds the self matrices first if the surfaces changed. */
 int ves3d_sv_eval(ves3d_sv* sv, double* vel, int is_device);
@@ -369,6 +381,15 @@ int ves3d_dev_gemm(char trans_a, char trans_b, int m, int n, int k, double alpha
  *   (include/Device.h:205-209): per-surface single layer with weights Q, targets
  *   [t_head, t_tail) of each surface, AxisMajor strides src_m / trg_m, n surfaces.
  * ------------------------------------------------------------------------- */
+/* ves3d_cuda_stokes_double_layer: the reference's cuda_stokes_double_layer(int src_m, int
+ *   trg_m, int n, int t_head, int t_tail, T, S, N, D, U, Q) (src/CudaKernels.cu:895-918, i.e.
+ *   Device<GPU>::DirectStokesDoubleLayer, src/DeviceGPU.cc:263-271; the declaration in
+ *   include/CudaKernels.h:42 omits trg_m): per surface, targets [t_head, t_tail), sources
+ *   with unit normals N and densities D, weights Q (NULL: none),
+ *   U = 3/(4 pi) sum (r.n)(r.d) r / |r|^5 with r = target - source. */
+int ves3d_cuda_stokes_double_layer_f64(int src_m, int trg_m, int n, int t_head, int t_tail, const double* T,
+                                       const double* S, const double* N, const double* D, double* U, const double* Q,
+                                       void* stream);
 int ves3d_cuda_stokes_f64(int src_m, int trg_m, int n, int t_head, int t_tail, const double* T,
                           const double* S, const double* D, double* U, const double* Q, void* stream);
 

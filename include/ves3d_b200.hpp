@@ -80,6 +80,14 @@ class StokesVelocity {
   void SetDensitySL(const Vec* force_single, bool add_repul = false) {
     SetDensitySL(&(*force_single)[0], add_repul);
   }
+  /* SetDensityDL(f): the double-layer density, NULL to turn the double layer off. */
+  void SetDensityDL(const Real* f, bool on_device = false) {
+    check(ves3d_sv_set_density_dl(sv_, f, on_device ? 1 : 0), "SetDensityDL");
+  }
+  template <class Vec>
+  void SetDensityDL(const Vec* force_double) {
+    SetDensityDL(force_double ? &(*force_double)[0] : (const Real*)0);
+  }
 
   /* operator()(vel): velocity into a caller container of the surfaces' size. */
   void operator()(Real* vel, bool on_device = false) { check(ves3d_sv_eval(sv_, vel, on_device ? 1 : 0), "eval"); }
@@ -244,6 +252,17 @@ inline void DirectStokes(const double* src, const double* den, const double* qw,
   check(ves3d_cuda_stokes_f64((int)src_stride, (int)trg_stride, (int)n_surfs, (int)trg_idx_head, (int)trg_idx_tail,
                               trg, src, den, pot, qw, stream),
         "DirectStokes");
+}
+
+/* Device<GPU>::DirectStokesDoubleLayer(src, norm, den, qw, src_stride, trg_stride, n_surfs,
+ * trg, trg_idx_head, trg_idx_tail, pot) on device pointers (cuda_stokes_double_layer);
+ * qw may be NULL. */
+inline void DirectStokesDoubleLayer(const double* src, const double* norm, const double* den, const double* qw,
+                                    size_t src_stride, size_t trg_stride, size_t n_surfs, const double* trg,
+                                    size_t trg_idx_head, size_t trg_idx_tail, double* pot, void* stream = 0) {
+  check(ves3d_cuda_stokes_double_layer_f64((int)src_stride, (int)trg_stride, (int)n_surfs, (int)trg_idx_head,
+                                           (int)trg_idx_tail, trg, src, norm, den, pot, qw, stream),
+        "DirectStokesDoubleLayer");
 }
 
 }  // namespace ves3d_b200

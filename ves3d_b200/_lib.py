@@ -32,6 +32,8 @@ SIGNATURES = [
     ("ves3d_sv_set_stream", _i, [_vp, _vp]),
     ("ves3d_sv_set_src_coord", _i, [_vp, _vp, _l, _i]),
     ("ves3d_sv_set_density_sl", _i, [_vp, _vp, _i]),
+    ("ves3d_sv_set_density_dl", _i, [_vp, _vp, _i]),
+    ("ves3d_sv_get_dl_matrix", _i, [_vp, _vp, _i]),
     ("ves3d_sv_eval", _i, [_vp, _vp, _i]),
     ("ves3d_sv_setup", _i, [_vp]),
     ("ves3d_sv_get_self_matrix", _i, [_vp, _vp, _i]),
@@ -59,6 +61,7 @@ SIGNATURES = [
     ("ves3d_vtk_write_grid", _i, [_vp, _vp, _vp, _vp, _l, _i, ctypes.c_char_p, _d, _i, _i]),
     ("ves3d_vtk_write", _i, [_vp, _vp, _l, _i, _i, ctypes.c_char_p, _d, _i, _i, _i]),
     ("ves3d_cuda_stokes_f64", _i, [_i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
+    ("ves3d_cuda_stokes_double_layer_f64", _i, [_i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("ves3d_stokes_alltoall_f64", None, [_vp, _vp, _sz, _vp, ctypes.POINTER(_vp)]),
     ("ves3d_interaction_free", None, [ctypes.POINTER(_vp)]),
     ("ves3d_stokes_alltoall_device_f64", _i, [_vp, _vp, _sz, _vp, _vp]),

@@ -53,6 +53,7 @@ struct NvtxRange {
 };
 
 constexpr double kInv8Pi = 0.039788735772973836;  // 1/(8 pi)
+constexpr double kDl = 0.238732414637843;         // 3/(4 pi), the double-layer kernel's constant
 
 // Hardware reciprocal square root in its flush-to-zero form (PTX rsqrt.approx.ftz.f32):
 // no subnormal handling around the MUFU op. Every caller passes squared distances far

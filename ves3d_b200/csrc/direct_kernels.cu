@@ -127,6 +127,114 @@ int launch_direct_stokes_f64(int src_m, int trg_m, int n, int t_head, int t_tail
   return VES3D_OK;
 }
 
+// Double-layer pair (DirectStokesDoubleLayerKernel, src/CPUKernels.cc:1060-1120;
+// stokes_double_layer, src/CudaKernels.cu:783-868): r = x_t - x_s,
+// u_t += (r . n_s)(r . d_s) r / |r|^5, scaled by 3/(4 pi) after the sum; a coincident pair
+// contributes nothing.
+__device__ __forceinline__ void pair_dl_f64(double tx, double ty, double tz, const double* sp, const double* sn,
+                                            const double* sd, PairAcc& a) {
+  const double dx = tx - sp[0], dy = ty - sp[1], dz = tz - sp[2];
+  const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
+  double rinv = rsqrt_f64(r2);
+  rinv = r2 > 0.0 ? rinv : 0.0;
+  const double rinv2 = rinv * rinv;
+  const double q = fma(dz, sn[2], fma(dy, sn[1], dx * sn[0])) * fma(dz, sd[2], fma(dy, sd[1], dx * sd[0])) *
+                   (rinv2 * rinv2 * rinv);
+  a.x = fma(dx, q, a.x);
+  a.y = fma(dy, q, a.y);
+  a.z = fma(dz, q, a.z);
+}
+
+// Device<GPU>::DirectStokesDoubleLayer / cuda_stokes_double_layer (src/CudaKernels.cu:895-918,
+// src/DeviceGPU.cc:263-271): per surface v, targets t in [t_head, t_tail) of T[v] (stride
+// trg_m), sources all src_m points of S[v] with normals N and densities D (times Q when
+// given). grid = (target chunks, n surfaces).
+__global__ void __launch_bounds__(kFarBS) k_direct_stokes_dl_f64(int src_m, int trg_m, int t_head, int t_tail,
+                                                                 const double* __restrict__ T,
+                                                                 const double* __restrict__ S,
+                                                                 const double* __restrict__ N,
+                                                                 const double* __restrict__ D, double* __restrict__ U,
+                                                                 const double* __restrict__ Q) {
+  __shared__ double sp[kFarBS * 3];
+  __shared__ double sn[kFarBS * 3];
+  __shared__ double sd[kFarBS * 3];
+  const long v = blockIdx.y;
+  const int t = t_head + blockIdx.x * kFarBS + threadIdx.x;
+  const bool active = t < t_tail;
+  const double* Tv = T + v * 3 * (long)trg_m;
+  const double* Sv = S + v * 3 * (long)src_m;
+  const double* Nv = N + v * 3 * (long)src_m;
+  const double* Dv = D + v * 3 * (long)src_m;
+  double tx = 0, ty = 0, tz = 0;
+  if (active) {
+    tx = Tv[t];
+    ty = Tv[trg_m + t];
+    tz = Tv[2 * trg_m + t];
+  }
+  PairAcc acc;
+  for (int s0 = 0; s0 < src_m; s0 += kFarBS) {
+    const int ns = min(kFarBS, src_m - s0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < ns; i += kFarBS) {
+      const int s = s0 + i;
+      const double q = Q ? Q[s] : 1.0;
+      sp[3 * i] = Sv[s];
+      sp[3 * i + 1] = Sv[src_m + s];
+      sp[3 * i + 2] = Sv[2 * src_m + s];
+      sn[3 * i] = Nv[s];
+      sn[3 * i + 1] = Nv[src_m + s];
+      sn[3 * i + 2] = Nv[2 * src_m + s];
+      sd[3 * i] = Dv[s] * q;
+      sd[3 * i + 1] = Dv[src_m + s] * q;
+      sd[3 * i + 2] = Dv[2 * src_m + s] * q;
+    }
+    __syncthreads();
+    if (!active) continue;
+    for (int k = 0; k < ns; k++) pair_dl_f64(tx, ty, tz, sp + 3 * k, sn + 3 * k, sd + 3 * k, acc);
+  }
+  if (!active) return;
+  double* Uv = U + v * 3 * (long)trg_m;
+  Uv[t] = acc.x * kDl;
+  Uv[trg_m + t] = acc.y * kDl;
+  Uv[2 * trg_m + t] = acc.z * kDl;
+}
+
+int launch_direct_stokes_dl_f64(int src_m, int trg_m, int n, int t_head, int t_tail, const double* T,
+                                const double* S, const double* N, const double* D, double* U, const double* Q,
+                                cudaStream_t st) {
+  if (n <= 0 || t_tail <= t_head) return VES3D_OK;
+  dim3 grid((t_tail - t_head + kFarBS - 1) / kFarBS, n);
+  k_direct_stokes_dl_f64<<<grid, kFarBS, 0, st>>>(src_m, trg_m, t_head, t_tail, T, S, N, D, U, Q);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
+// Unit outward normals, point-major (src/StokesVelocity.cc:245-275).
+__global__ void k_unit_normals(const double* __restrict__ Xt, const double* __restrict__ Xp, long nv, int p0,
+                               double* __restrict__ nrm) {
+  const int ng = 2 * p0 * (p0 + 1);
+  const long g = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= nv * ng) return;
+  const long v = g / ng;
+  const int k = (int)(g - v * ng);
+  const long b = v * 3 * ng + k;
+  const double ax = Xt[b], ay = Xt[b + ng], az = Xt[b + 2 * ng];
+  const double bx = Xp[b], by = Xp[b + ng], bz = Xp[b + 2 * ng];
+  const double nx = ay * bz - az * by, ny = az * bx - ax * bz, nz = ax * by - ay * bx;
+  const double inv = 1.0 / sqrt(nx * nx + ny * ny + nz * nz);
+  nrm[3 * g] = nx * inv;
+  nrm[3 * g + 1] = ny * inv;
+  nrm[3 * g + 2] = nz * inv;
+}
+
+int launch_unit_normals(const double* Xt, const double* Xp, long nv, int p0, double* nrm, cudaStream_t st) {
+  const long N = nv * ngrid_(p0);
+  if (N <= 0) return VES3D_OK;
+  k_unit_normals<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(Xt, Xp, nv, p0, nrm);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
 // area = |X_theta x X_phi|; pos point-major; den = f * area * w[lat].
 __global__ void k_far_sources(const double* __restrict__ X, const double* __restrict__ f,
                               const double* __restrict__ Xt, const double* __restrict__ Xp, long nv, int p0,

@@ -126,6 +126,86 @@ __global__ void __launch_bounds__(512) k_far_f64_seg(const double* __restrict__ 
   }
 }
 
+// ------------------------------------------------------------------------------------
+// Double layer, FP64 (stokes_dl_uKernel, src/PVFMMInterface.cc:285-360, over the points of
+// the other vesicles): with r = x_t - x_s, u_t = 3/(4 pi) sum_s (r . n_s)(r . d_s) r / |r|^5,
+// n_s the unit outward normal and d_s the density times area and smooth weight; a coincident
+// pair contributes nothing. Same decomposition as k_far_f64_seg; nine values per staged
+// source (position, normal, density) and the partial sums left unscaled.
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ void pair_dl64(const double* s, double tx, double ty, double tz, Acc64& a) {
+  const double dx = tx - s[0], dy = ty - s[1], dz = tz - s[2];
+  const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
+  double rinv = rsqrt_f64(r2);
+  rinv = r2 > 0.0 ? rinv : 0.0;
+  const double rinv2 = rinv * rinv;
+  const double q = fma(dz, s[5], fma(dy, s[4], dx * s[3])) * fma(dz, s[8], fma(dy, s[7], dx * s[6])) *
+                   (rinv2 * rinv2 * rinv);
+  a.x = fma(dx, q, a.x);
+  a.y = fma(dy, q, a.y);
+  a.z = fma(dz, q, a.z);
+}
+
+// grid (segments, vesicles, target chunks of 2*blockDim targets); pos, nrm, dden
+// point-major [N][3]; part [seg][N][3].
+__global__ void __launch_bounds__(512) k_far_dl_f64_seg(const double* __restrict__ pos, const double* __restrict__ nrm,
+                                                        const double* __restrict__ dden, const long* __restrict__ off,
+                                                        long N, int seg_tiles, double* __restrict__ part) {
+  __shared__ __align__(16) double sm[kTileF64 * 9];
+  const int v = blockIdx.y, seg = blockIdx.x;
+  const long t0 = off[v], nt = off[v + 1] - t0;
+  const int nthr = blockDim.x;
+  const long c0 = (long)blockIdx.z * 2 * nthr;
+  const long ia = t0 + c0 + threadIdx.x, ib = ia + nthr;
+  const bool va = c0 + threadIdx.x < nt, vb = c0 + threadIdx.x + nthr < nt;
+  const long la = va ? ia : t0, lb = vb ? ib : t0;
+  const double ax_ = pos[3 * la], ay_ = pos[3 * la + 1], az_ = pos[3 * la + 2];
+  const double bx_ = pos[3 * lb], by_ = pos[3 * lb + 1], bz_ = pos[3 * lb + 2];
+  Acc64 A, B;
+  const long ntiles = (N + kTileF64 - 1) / kTileF64;
+  const long tb = (long)seg * seg_tiles, te = min(tb + seg_tiles, ntiles);
+  for (long tile = tb; tile < te; tile++) {
+    const long s0 = tile * kTileF64;
+    const int ns = (int)min((long)kTileF64, N - s0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < ns; i += nthr) {
+      const long s = s0 + i;
+      double* d = sm + 9 * i;
+      d[0] = pos[3 * s];
+      d[1] = pos[3 * s + 1];
+      d[2] = pos[3 * s + 2];
+      d[3] = nrm[3 * s];
+      d[4] = nrm[3 * s + 1];
+      d[5] = nrm[3 * s + 2];
+      d[6] = dden[3 * s];
+      d[7] = dden[3 * s + 1];
+      d[8] = dden[3 * s + 2];
+    }
+    __syncthreads();
+    int a0, a1, b0, b1;
+    split_tile(s0, ns, t0, t0 + nt, a0, a1, b0, b1);
+    for (int k = a0; k < a1; k++) {
+      pair_dl64(sm + 9 * k, ax_, ay_, az_, A);
+      pair_dl64(sm + 9 * k, bx_, by_, bz_, B);
+    }
+    for (int k = b0; k < b1; k++) {
+      pair_dl64(sm + 9 * k, ax_, ay_, az_, A);
+      pair_dl64(sm + 9 * k, bx_, by_, bz_, B);
+    }
+  }
+  double* P = part + (long)seg * 3 * N;
+  if (va) {
+    P[3 * ia] = A.x;
+    P[3 * ia + 1] = A.y;
+    P[3 * ia + 2] = A.z;
+  }
+  if (vb) {
+    P[3 * ib] = B.x;
+    P[3 * ib + 1] = B.y;
+    P[3 * ib + 2] = B.z;
+  }
+}
+
 // Four targets per thread (a launch shape the autotuner may pick): twice the independent
 // FP64 chains and half the shared-memory reads per pair, at 98 registers.
 template <int TPT>
@@ -338,7 +418,8 @@ __global__ void __launch_bounds__(512) k_far_f32_segT(const double* __restrict__
 // out (AxisMajor per vesicle) = add + (1/8pi) sum over segments in order. One CTA per
 // vesicle; vesicle v holds points [off[v], off[v+1]) as [3][n_v] from 3*off[v].
 __global__ void k_far_reduce(const double* __restrict__ part, int nseg, const long* __restrict__ off, long N,
-                             const double* __restrict__ add, double* __restrict__ out, double* __restrict__ far_out) {
+                             const double* __restrict__ add, double* __restrict__ out, double* __restrict__ far_out,
+                             const double* __restrict__ part2, int nseg2, double scale2) {
   const int v = blockIdx.x;
   const long t0 = off[v], nt = off[v + 1] - t0;
   for (long i = threadIdx.x; i < 3 * nt; i += blockDim.x) {
@@ -348,6 +429,11 @@ __global__ void k_far_reduce(const double* __restrict__ part, int nseg, const lo
     double s = 0.0;
     for (int q = 0; q < nseg; q++) s += part[(long)q * 3 * N + 3 * g + c];
     s *= kInv8Pi;
+    if (part2) {  // a second set of partials (the double layer) with its own constant
+      double s2 = 0.0;
+      for (int q = 0; q < nseg2; q++) s2 += part2[(long)q * 3 * N + 3 * g + c];
+      s += s2 * scale2;
+    }
     const long o = 3 * t0 + c * nt + k;
     if (far_out) far_out[o] = s;
     out[o] = (add ? add[o] : 0.0) + s;
@@ -377,8 +463,8 @@ int far_segments(long nves, long N, int tile, int nthr, int waves, int* seg_tile
 }
 
 int launch_far_reduce(const double* part, int nseg, const long* off, long nves, long N, const double* add, double* out,
-                      double* far_out, cudaStream_t st) {
-  k_far_reduce<<<(unsigned)nves, 256, 0, st>>>(part, nseg, off, N, add, out, far_out);
+                      double* far_out, cudaStream_t st, const double* part2, int nseg2, double scale2) {
+  k_far_reduce<<<(unsigned)nves, 256, 0, st>>>(part, nseg, off, N, add, out, far_out, part2, nseg2, scale2);
   VES3D_LAUNCHED();
   return VES3D_OK;
 }
@@ -561,6 +647,26 @@ std::string autotune_report() {
          std::to_string(kv.second.shape.chunk_max) + " tpt=" + std::to_string(kv.second.shape.tpt) +
          " ms=" + std::to_string(kv.second.ms) + "\n";
   return r;
+}
+
+int launch_far_dl(const double* pos, const double* nrm, const double* dden, const long* off, long nves, long N,
+                  int max_nt, double* part, long part_cap_segments, cudaStream_t st, int* nseg_out) {
+  *nseg_out = 0;
+  if (N <= 0 || nves <= 0) return VES3D_OK;
+  int nchunk, nthr;
+  chunking(max_nt, 1024, 2, &nchunk, &nthr);
+  int seg_tiles = 1;
+  int nseg = far_segments((long)nchunk * nves, N, kTileF64, nthr, 8, &seg_tiles);
+  if (nseg > part_cap_segments) {
+    const long ntiles = (N + kTileF64 - 1) / kTileF64;
+    seg_tiles = (int)((ntiles + part_cap_segments - 1) / part_cap_segments);
+    nseg = (int)((ntiles + seg_tiles - 1) / seg_tiles);
+  }
+  dim3 grid(nseg, (unsigned)nves, nchunk);
+  k_far_dl_f64_seg<<<grid, nthr, 0, st>>>(pos, nrm, dden, off, N, seg_tiles, part);
+  VES3D_LAUNCHED();
+  *nseg_out = nseg;
+  return VES3D_OK;
 }
 
 int launch_far(bool mixed, const double* pos, const double* den, const long* off, long nves, long N, int max_nt,

@@ -54,6 +54,9 @@ int launch_rotate_all(const double* S, long nv, const DevTables& T, double* R, c
 // X, Xt, Xp [nrot][3][M1], R [nrot][3][Ncoef] -> K [nrot][2][6][M1].
 int launch_singular_sl(const double* X, const double* Xt, const double* Xp, const double* R, long nrot,
                        const DevTables& T, double* K, cudaStream_t st);
+// the same pole-target kernel for the double layer (DLMatrix of StokesSingularInteg)
+int launch_singular_dl(const double* X, const double* Xt, const double* Xp, const double* R, long nrot,
+                       const DevTables& T, double* K, cudaStream_t st);
 // RotateTranspose with dof = 12 (:452-541) fused with the Rearrange (:1090-1172):
 // C [nv][p0+1][p0][2][6][Ncoef] -> SL3 [nv][3][Ncoef][3][Ngrid].
 int launch_rotate_transpose_scatter(const double* C, long nv, const DevTables& T, double* SL3, cudaStream_t st);
@@ -62,7 +65,8 @@ int launch_rotate_transpose_scatter(const double* C, long nv, const DevTables& T
 bool fused_build_supported(int p0, int p1);
 int launch_build_ring(const double* R, long nrot, const DevTables& T, double* C, cudaStream_t st);
 // V[v] = F[v] . SL[v] (src/StokesVelocity.cc:397-416), n = 3 Ncoef.
-int launch_self_gemv(const double* F, const double* SL, long nv, int n, double* V, cudaStream_t st);
+int launch_self_gemv(const double* F, const double* SL, long nv, int n, double* V, cudaStream_t st,
+                     bool accumulate = false);
 // nvec density vectors per vesicle, layout [q][nv][n]; nvec <= 8
 int launch_self_gemv_multi(const double* F, const double* SL, long nv, int nvec, int n, double* V, cudaStream_t st);
 // area element |X_theta x X_phi| and far-field sources: pos/den point-major [N][3],
@@ -82,7 +86,22 @@ int launch_far(bool mixed, const double* pos, const double* den, const long* off
                const double* add, double* out, double* far_out, double* part, long part_cap_segments,
                cudaStream_t st, int* nseg_out = nullptr);
 int launch_far_reduce(const double* part, int nseg, const long* off, long nves, long N, const double* add, double* out,
-                      double* far_out, cudaStream_t st);
+                      double* far_out, cudaStream_t st, const double* part2 = nullptr, int nseg2 = 0,
+                      double scale2 = 0.0);
+// Far double layer over the points of the other vesicles (FP64): pos, unit normals nrm and
+// densities dden (times area and weights) point-major; the segments' unscaled partials go to
+// part (at most part_cap_segments), their count to *nseg_out, for launch_far_reduce's second
+// set with scale kDl.
+int launch_far_dl(const double* pos, const double* nrm, const double* dden, const long* off, long nves, long N,
+                  int max_nt, double* part, long part_cap_segments, cudaStream_t st, int* nseg_out);
+// Unit outward normals (X_theta x X_phi) / |X_theta x X_phi| of nv surfaces at order p0,
+// AxisMajor derivatives in, point-major [N][3] out.
+int launch_unit_normals(const double* Xt, const double* Xp, long nv, int p0, double* nrm, cudaStream_t st);
+// Device<GPU>::DirectStokesDoubleLayer (cuda_stokes_double_layer): per surface, AxisMajor,
+// sources with unit normals N and densities D, weights Q (null: none).
+int launch_direct_stokes_dl_f64(int src_m, int trg_m, int n, int t_head, int t_tail, const double* T,
+                                const double* S, const double* N, const double* D, double* U, const double* Q,
+                                cudaStream_t st);
 constexpr long kFarMaxSegments = 32;
 // Vesicles [v0, v0 + nv) all with nt points: one far-field launch each, sized for nt.
 struct FarGroup {

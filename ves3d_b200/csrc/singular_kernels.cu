@@ -102,13 +102,16 @@ int launch_rotate_all(const double* S, long nv, const DevTables& T, double* R, c
 }
 
 // One CTA per rotated surface. Pole targets from the m = 0 block (SHC2Pole, :325-360),
-// then for every upsampled source point s (latitude j0) and pole t:
-//   SL components  a1 + r_a r_b a2 with a1 = qs * area / (8 pi |r|), a2 = a1 / |r|^2,
-//   qs = SingularWeights(p1)[t ? j0 : p1 - j0], |r|^-1 := 0 when |r|^2 <= 2^-52.
-__global__ void __launch_bounds__(256) k_singular_sl(const double* __restrict__ X, const double* __restrict__ Xt,
-                                                     const double* __restrict__ Xp, const double* __restrict__ R,
-                                                     int p0, int p1, const double* __restrict__ qp,
-                                                     const double* __restrict__ sw, double* __restrict__ K) {
+// then for every upsampled source point s (latitude j0) and pole t, with r = target - source,
+// n = X_theta x X_phi (area-weighted outward normal), qs = SingularWeights(p1)[t ? j0 : p1 - j0]
+// and |r|^-1 := 0 when |r|^2 <= 2^-52 (src/SphericalHarmonics.cc:989-1068):
+//   single layer  a1 + r_a r_b a2 with a1 = qs |n| / (8 pi |r|), a2 = a1 / |r|^2
+//   double layer  r_a r_b q      with q  = 3 qs (n . r) / (4 pi |r|^5)
+template <bool DL>
+__global__ void __launch_bounds__(256) k_singular(const double* __restrict__ X, const double* __restrict__ Xt,
+                                                  const double* __restrict__ Xp, const double* __restrict__ R,
+                                                  int p0, int p1, const double* __restrict__ qp,
+                                                  const double* __restrict__ sw, double* __restrict__ K) {
   __shared__ double trg[6];
   const long rot = blockIdx.x;
   const int nc = p0 * (p0 + 2), M1 = 2 * p1 * (p1 + 1);
@@ -131,7 +134,7 @@ __global__ void __launch_bounds__(256) k_singular_sl(const double* __restrict__ 
     const double ax = xt[s], ay = xt[M1 + s], az = xt[2 * M1 + s];
     const double bx = xp[s], by = xp[M1 + s], bz = xp[2 * M1 + s];
     const double nx = ay * bz - az * by, ny = az * bx - ax * bz, nz = ax * by - ay * bx;
-    const double area = sqrt(nx * nx + ny * ny + nz * nz);
+    const double area = DL ? 0.0 : sqrt(nx * nx + ny * ny + nz * nz);
 #pragma unroll
     for (int t = 0; t < 2; t++) {
       const double dx = trg[t] - px, dy = trg[2 + t] - py, dz = trg[4 + t] - pz;
@@ -139,15 +142,25 @@ __global__ void __launch_bounds__(256) k_singular_sl(const double* __restrict__ 
       double rinv = 1.0 / sqrt(r2);
       if (r2 <= eps) rinv = 0.0;
       const double rinv2 = rinv * rinv;
-      const double a1 = kInv8Pi * __ldg(sw + (t ? j0 : p1 - j0)) * area * rinv;
-      const double a2 = a1 * rinv2;
       double* kt = k + (long)t * 6 * M1;
-      kt[s] = a1 + dx * dx * a2;
-      kt[M1 + s] = dx * dy * a2;
-      kt[2 * M1 + s] = dx * dz * a2;
-      kt[3 * M1 + s] = a1 + dy * dy * a2;
-      kt[4 * M1 + s] = dy * dz * a2;
-      kt[5 * M1 + s] = a1 + dz * dz * a2;
+      if (DL) {
+        const double q = kDl * __ldg(sw + (t ? j0 : p1 - j0)) * (nx * dx + ny * dy + nz * dz) * (rinv2 * rinv2 * rinv);
+        kt[s] = dx * dx * q;
+        kt[M1 + s] = dx * dy * q;
+        kt[2 * M1 + s] = dx * dz * q;
+        kt[3 * M1 + s] = dy * dy * q;
+        kt[4 * M1 + s] = dy * dz * q;
+        kt[5 * M1 + s] = dz * dz * q;
+      } else {
+        const double a1 = kInv8Pi * __ldg(sw + (t ? j0 : p1 - j0)) * area * rinv;
+        const double a2 = a1 * rinv2;
+        kt[s] = a1 + dx * dx * a2;
+        kt[M1 + s] = dx * dy * a2;
+        kt[2 * M1 + s] = dx * dz * a2;
+        kt[3 * M1 + s] = a1 + dy * dy * a2;
+        kt[4 * M1 + s] = dy * dz * a2;
+        kt[5 * M1 + s] = a1 + dz * dz * a2;
+      }
     }
   }
 }
@@ -155,7 +168,15 @@ __global__ void __launch_bounds__(256) k_singular_sl(const double* __restrict__ 
 int launch_singular_sl(const double* X, const double* Xt, const double* Xp, const double* R, long nrot,
                        const DevTables& T, double* K, cudaStream_t st) {
   if (nrot <= 0) return VES3D_OK;
-  k_singular_sl<<<(unsigned)nrot, 256, 0, st>>>(X, Xt, Xp, R, T.p0, T.p1, T.qp, T.sing_w, K);
+  k_singular<false><<<(unsigned)nrot, 256, 0, st>>>(X, Xt, Xp, R, T.p0, T.p1, T.qp, T.sing_w, K);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
+int launch_singular_dl(const double* X, const double* Xt, const double* Xp, const double* R, long nrot,
+                       const DevTables& T, double* K, cudaStream_t st) {
+  if (nrot <= 0) return VES3D_OK;
+  k_singular<true><<<(unsigned)nrot, 256, 0, st>>>(X, Xt, Xp, R, T.p0, T.p1, T.qp, T.sing_w, K);
   VES3D_LAUNCHED();
   return VES3D_OK;
 }
@@ -442,6 +463,7 @@ int launch_rotate_transpose_scatter(const double* C, long nv, const DevTables& T
 }
 
 // V[v][col] = sum_row F[v][row] * SL[v][row][col]; one thread per output column.
+template <bool ACC>
 __global__ void __launch_bounds__(128) k_self_gemv(const double* __restrict__ F, const double* __restrict__ SL,
                                                    int n, double* __restrict__ V) {
   extern __shared__ double sF[];
@@ -460,7 +482,8 @@ __global__ void __launch_bounds__(128) k_self_gemv(const double* __restrict__ F,
     s3 = fma(sF[r + 3], __ldg(M + (long)(r + 3) * n), s3);
   }
   for (; r < n; r++) s0 = fma(sF[r], __ldg(M + (long)r * n), s0);
-  V[v * n + col] = (s0 + s1) + (s2 + s3);
+  const double sum = (s0 + s1) + (s2 + s3);
+  V[v * n + col] = ACC ? V[v * n + col] + sum : sum;
 }
 
 // Several density vectors per vesicle at once (batched operator applications):
@@ -508,12 +531,19 @@ int launch_self_gemv_multi(const double* F, const double* SL, long nv, int nvec,
   return VES3D_OK;
 }
 
-int launch_self_gemv(const double* F, const double* SL, long nv, int n, double* V, cudaStream_t st) {
+int launch_self_gemv(const double* F, const double* SL, long nv, int n, double* V, cudaStream_t st, bool accumulate) {
   if (nv <= 0) return VES3D_OK;
   dim3 grid((n + 127) / 128, (unsigned)nv);
   size_t smem = (size_t)n * sizeof(double);
-  if (smem > 48 * 1024) VES3D_CK(cudaFuncSetAttribute(k_self_gemv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_self_gemv<<<grid, 128, smem, st>>>(F, SL, n, V);
+  if (accumulate) {
+    if (smem > 48 * 1024)
+      VES3D_CK(cudaFuncSetAttribute(k_self_gemv<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_self_gemv<true><<<grid, 128, smem, st>>>(F, SL, n, V);
+  } else {
+    if (smem > 48 * 1024)
+      VES3D_CK(cudaFuncSetAttribute(k_self_gemv<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_self_gemv<false><<<grid, 128, smem, st>>>(F, SL, n, V);
+  }
   VES3D_LAUNCHED();
   return VES3D_OK;
 }

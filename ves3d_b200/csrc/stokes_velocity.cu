@@ -152,6 +152,14 @@ struct ves3d_sv {
   double *X = nullptr, *F = nullptr, *V = nullptr, *Vself = nullptr, *Vfar = nullptr;
   double *Sx = nullptr, *Xt = nullptr, *Xp = nullptr, *area = nullptr, *pos = nullptr, *den = nullptr;
   double *SL = nullptr, *Fc = nullptr, *Vc = nullptr, *part = nullptr;
+  // double layer (allocated when a double-layer density is first set): density G and its
+  // coefficients Gc, the self matrices DL, unit normals and weighted densities of the far
+  // sum (point-major) and its segment partials
+  double *G = nullptr, *Gc = nullptr, *DL = nullptr, *nrm = nullptr, *dden = nullptr, *part_dl = nullptr;
+  long dl_cap = 0;
+  bool have_dl = false, dl_valid = false;
+  int nseg_dl = 0;
+  float dl_ms = 0;  // last double-layer self-matrix build (device ms)
   long* off = nullptr;  // [nves+1] point offsets of the vesicles
   long off_nves = -1;   // vesicle count the offsets were uploaded for
   // setup scratch (one chunk of vesicles)
@@ -213,7 +221,15 @@ struct ves3d_sv {
     if (hi) cudaStreamDestroy(hi);
     if (own_stream) cudaStreamDestroy(own_stream);
   }
+  void free_dl() {
+    double* ps[] = {G, Gc, DL, nrm, dden, part_dl};
+    for (double* q : ps) dfree(q);
+    G = Gc = DL = nrm = dden = part_dl = nullptr;
+    dl_cap = 0;
+    have_dl = dl_valid = false;
+  }
   void free_buffers() {
+    free_dl();
     double* ps[] = {X, F, V, Vself, Vfar, Sx, Xt, Xp, area, pos, den, SL, Fc, Vc, part};
     for (double* q : ps) dfree(q);
     dfree(off);
@@ -291,6 +307,27 @@ int alloc_resident(ves3d_sv* sv, long nves) {
   return VES3D_OK;
 }
 
+// Double-layer buffers for the resident capacity (first double-layer density).
+int alloc_dl(ves3d_sv* sv) {
+  if (sv->dl_cap >= sv->cap_ves && sv->DL) return VES3D_OK;
+  sv->free_dl();
+  const long nves = sv->cap_ves;
+  const size_t ng = ngrid_(sv->p), n = 3 * (size_t)ncoef_(sv->p), fld = (size_t)nves * 3 * ng;
+  int s = 0;
+  s |= dalloc(&sv->G, fld);
+  s |= dalloc(&sv->Gc, (size_t)nves * n);
+  s |= dalloc(&sv->DL, (size_t)nves * n * n);
+  s |= dalloc(&sv->nrm, fld);
+  s |= dalloc(&sv->dden, fld);
+  s |= dalloc(&sv->part_dl, (size_t)kFarMaxSegments * fld);
+  if (s) {
+    sv->free_dl();
+    return s;
+  }
+  sv->dl_cap = nves;
+  return VES3D_OK;
+}
+
 // The fused per-rotation build is used when it is instantiated for (p, p_up);
 // VES3D_FUSED_BUILD=0 forces the unfused stage-by-stage pipeline (A/B checks).
 bool use_fused(const ves3d_sv* sv) {
@@ -311,8 +348,12 @@ size_t scratch_per_vesicle(int p0, int p1, bool fused) {
 
 int alloc_scratch(ves3d_sv* sv) {
   const long want = sv->nves;
-  if (sv->chunk >= want) return VES3D_OK;  // the whole suspension in one chunk already
-  const bool fused = use_fused(sv);
+  // the double layer is built stage by stage: those stage buffers are kept while a
+  // double-layer density is set (the fused single-layer build needs a subset of them)
+  const bool stages = !use_fused(sv) || sv->have_dl;
+  const bool layout_ok = !stages || sv->K != nullptr;
+  if (sv->chunk >= want && layout_ok) return VES3D_OK;  // the whole suspension in one chunk already
+  const bool fused = !stages;
   size_t per = scratch_per_vesicle(sv->p, sv->pup, fused) * sizeof(double);
   size_t free_b = 0, total_b = 0;
   VES3D_CK(cudaMemGetInfo(&free_b, &total_b));
@@ -328,7 +369,7 @@ int alloc_scratch(ves3d_sv* sv) {
   long chunk = (long)(budget / per);
   if (chunk < 1) chunk = 1;
   if (chunk > want) chunk = want;
-  if (chunk <= sv->chunk) return VES3D_OK;
+  if (chunk <= sv->chunk && layout_ok) return VES3D_OK;
   sv->free_scratch();
   const size_t npr = (size_t)sv->p * (sv->p + 1), nc = ncoef_(sv->p), M1 = ngrid_(sv->pup), ng = ngrid_(sv->p);
   int s = 0;
@@ -363,16 +404,24 @@ int copy_out(double* dst, const double* src, size_t n, int is_device, cudaStream
 }
 
 int alloc_scratch(ves3d_sv* sv);
+int run_setup(ves3d_sv* sv, bool dl = false);
 
-int run_setup(ves3d_sv* sv) {
-  NvtxRange nvtx("ves3d build");
+// The self matrices of every vesicle: the single layer (SL), or with dl the double layer
+// (DL, always by the stage-by-stage pipeline).
+int run_setup(ves3d_sv* sv, bool dl) {
+  NvtxRange nvtx(dl ? "ves3d build dl" : "ves3d build");
   const DevTables& T = sv->tab->d;
   const int p0 = sv->p, p1 = sv->pup, nc = ncoef_(p0), ng = ngrid_(p0), M1 = ngrid_(p1);
   const long npr = (long)p0 * (p0 + 1);
   cudaStream_t st = sv->stream;
   int s = alloc_scratch(sv);
   if (s) return s;
-  const bool fused = use_fused(sv);
+  const bool fused = !dl && use_fused(sv);
+  double* M = dl ? sv->DL : sv->SL;
+  if ((!fused && !sv->K) || !M) {
+    set_error("internal: self-matrix build without its buffers");
+    return VES3D_ERR_STATE;
+  }
   VES3D_CK(cudaEventRecord(sv->ev[0], st));
   for (long v0 = 0; v0 < sv->nves; v0 += sv->chunk) {
     const long nb = std::min(sv->chunk, sv->nves - v0);
@@ -384,21 +433,25 @@ int run_setup(ves3d_sv* sv) {
       if ((s = launch_synthesis(sv->R, nrot * 3, p0, p1, T.syn1_leg, T.syn1_dleg, T.syn1_four, T.syn1_dfour,
                                 T.blk_off, sv->Xu, sv->Xut, sv->Xup, st)))
         return s;
-      if ((s = launch_singular_sl(sv->Xu, sv->Xut, sv->Xup, sv->R, nrot, T, sv->K, st))) return s;
+      if ((s = (dl ? launch_singular_dl : launch_singular_sl)(sv->Xu, sv->Xut, sv->Xup, sv->R, nrot, T, sv->K, st)))
+        return s;
       if ((s = launch_analysis(sv->K, nrot * 12, p1, p0, T.synT_four, T.syn1_leg, T.jf_of_coef, sv->C, st)))
         return s;
     }
     if ((s = launch_rotate_transpose_scatter(sv->C, nb, T, sv->SL3, st))) return s;
     if ((s = launch_grid2shc(sv->SL3, nb * 3 * nc * 3, p0, T.ana_four, T.ana_leg, T.jf_of_coef,
-                             sv->SL + v0 * (long)(3 * nc) * (3 * nc), st)))
+                             M + v0 * (long)(3 * nc) * (3 * nc), st)))
       return s;
     (void)ng;
     (void)M1;
   }
   VES3D_CK(cudaEventRecord(sv->ev[1], st));
   VES3D_CK(cudaEventSynchronize(sv->ev[1]));
-  VES3D_CK(cudaEventElapsedTime(&sv->ms[0], sv->ev[0], sv->ev[1]));
-  sv->sl_valid = true;
+  VES3D_CK(cudaEventElapsedTime(dl ? &sv->dl_ms : &sv->ms[0], sv->ev[0], sv->ev[1]));
+  if (dl)
+    sv->dl_valid = true;
+  else
+    sv->sl_valid = true;
   return VES3D_OK;
 }
 
@@ -418,8 +471,9 @@ int run_self(ves3d_sv* sv, double* vself, double* den) {
   return launch_far_density(sv->F, sv->area, sv->nves, p0, T.smooth_w0, den, st);
 }
 
-// Self part alone: Vself = SHC2Grid(Grid2SHC(F) . SL) on the context's stream.
-int run_self_apply(ves3d_sv* sv) {
+// Self part alone: Vself = SHC2Grid(Grid2SHC(F) . SL [+ Grid2SHC(G) . DL]) on the
+// context's stream (src/StokesVelocity.cc:385-452: SL_vel + DL_vel in coefficients).
+int run_self_apply(ves3d_sv* sv, bool dl) {
   NvtxRange nvtx("ves3d self");
   const DevTables& T = sv->tab->d;
   const int p0 = sv->p, n = 3 * ncoef_(p0);
@@ -427,6 +481,10 @@ int run_self_apply(ves3d_sv* sv) {
   int s;
   if ((s = launch_grid2shc(sv->F, sv->nves * 3, p0, T.ana_four, T.ana_leg, T.jf_of_coef, sv->Fc, st))) return s;
   if ((s = launch_self_gemv(sv->Fc, sv->SL, sv->nves, n, sv->Vc, st))) return s;
+  if (dl) {
+    if ((s = launch_grid2shc(sv->G, sv->nves * 3, p0, T.ana_four, T.ana_leg, T.jf_of_coef, sv->Gc, st))) return s;
+    if ((s = launch_self_gemv(sv->Gc, sv->DL, sv->nves, n, sv->Vc, st, /*accumulate=*/true))) return s;
+  }
   return launch_synthesis(sv->Vc, sv->nves * 3, p0, p0, T.syn0_leg, T.syn0_dleg, T.syn0_four, T.syn0_dfour,
                           T.blk_off, sv->Vself, nullptr, nullptr, st);
 }
@@ -434,7 +492,7 @@ int run_self_apply(ves3d_sv* sv) {
 // Fork: the weighted density and the far-field segments on the side stream, which waits
 // for everything the context's stream has queued (surfaces, densities, the previous
 // evaluation's reduce). ev_far[0..1] (may be null) bracket the segment kernels.
-int fork_far(ves3d_sv* sv, int* nseg, cudaEvent_t ev_far0, cudaEvent_t ev_far1) {
+int fork_far(ves3d_sv* sv, int* nseg, cudaEvent_t ev_far0, cudaEvent_t ev_far1, bool dl) {
   NvtxRange nvtx("ves3d far");
   const DevTables& T = sv->tab->d;
   int s;
@@ -447,6 +505,14 @@ int fork_far(ves3d_sv* sv, int* nseg, cudaEvent_t ev_far0, cudaEvent_t ev_far1) 
                       sv->npts(), ngrid_(sv->p), nullptr, nullptr, nullptr, sv->part, kFarMaxSegments, fs, nseg)))
     return s;
   if (ev_far1) VES3D_CK(cudaEventRecord(ev_far1, fs));
+  sv->nseg_dl = 0;
+  if (dl) {  // the far double layer (FP64) after the single layer's segments
+    if ((s = launch_unit_normals(sv->Xt, sv->Xp, sv->nves, sv->p, sv->nrm, fs))) return s;
+    if ((s = launch_far_density(sv->G, sv->area, sv->nves, sv->p, T.smooth_w0, sv->dden, fs))) return s;
+    if ((s = launch_far_dl(sv->pos, sv->nrm, sv->dden, sv->off, sv->nves, sv->npts(), ngrid_(sv->p), sv->part_dl,
+                           kFarMaxSegments, fs, &sv->nseg_dl)))
+      return s;
+  }
   VES3D_CK(cudaEventRecord(sv->ev_join, fs));
   return VES3D_OK;
 }
@@ -467,22 +533,26 @@ int run_setup_hi(ves3d_sv* sv) {
 }
 
 // Join: the reduce of the far partials, added to the self part, on the context's stream.
-int join_far(ves3d_sv* sv, int nseg) {
+int join_far(ves3d_sv* sv, int nseg, bool dl) {
   VES3D_CK(cudaStreamWaitEvent(sv->stream, sv->ev_join, 0));
-  return launch_far_reduce(sv->part, nseg, sv->off, sv->nves, sv->npts(), sv->Vself, sv->V, sv->Vfar, sv->stream);
+  return launch_far_reduce(sv->part, nseg, sv->off, sv->nves, sv->npts(), sv->Vself, sv->V, sv->Vfar, sv->stream,
+                           dl ? sv->part_dl : nullptr, dl ? sv->nseg_dl : 0, kDl);
 }
 
 // The evaluation proper, stream-ordered and free of host synchronisation (it is what the
 // CUDA graph of ves3d_sv_capture_eval records): the far field forked to the side stream,
 // the self part on the context's stream, joined by the reduce.
-int run_eval_body(ves3d_sv* sv) {
+int run_eval_body(ves3d_sv* sv, bool dl) {
   int s, nseg = 0;
-  if ((s = fork_far(sv, &nseg, nullptr, nullptr))) return s;
-  if ((s = run_self_apply(sv))) return s;
-  return join_far(sv, nseg);
+  if ((s = fork_far(sv, &nseg, nullptr, nullptr, dl))) return s;
+  if ((s = run_self_apply(sv, dl))) return s;
+  return join_far(sv, nseg, dl);
 }
 
-int run_eval(ves3d_sv* sv) {
+// One evaluation; dl adds the double layer of the density G (the operator's own
+// evaluation when a double-layer density is set; the implicit step applies the single
+// layer alone).
+int run_eval(ves3d_sv* sv, bool dl) {
   cudaStream_t st = sv->stream;
   int s, nseg = 0;
   if (!sv->have_src || !sv->have_den) {
@@ -492,12 +562,17 @@ int run_eval(ves3d_sv* sv) {
   // the far field first (on the side stream when overlapping the self-matrix build, else
   // on the context's stream); events ev[4], ev[5] bracket its segment kernels (the
   // roofline denominator)
-  if ((s = fork_far(sv, &nseg, sv->ev[4], sv->ev[5]))) return s;
+  if (dl && !sv->have_dl) {
+    set_error("double layer requested without a double-layer density");
+    return VES3D_ERR_STATE;
+  }
+  if ((s = fork_far(sv, &nseg, sv->ev[4], sv->ev[5], dl))) return s;
   if (!sv->sl_valid && (s = run_setup_hi(sv))) return s;
+  if (dl && !sv->dl_valid && (s = run_setup(sv, true))) return s;
   VES3D_CK(cudaEventRecord(sv->ev[2], st));
-  if ((s = run_self_apply(sv))) return s;
+  if ((s = run_self_apply(sv, dl))) return s;
   VES3D_CK(cudaEventRecord(sv->ev[3], st));
-  if ((s = join_far(sv, nseg))) return s;
+  if ((s = join_far(sv, nseg, dl))) return s;
   VES3D_CK(cudaEventRecord(sv->ev[6], st));
   VES3D_CK(cudaEventSynchronize(sv->ev[6]));
   VES3D_CK(cudaEventElapsedTime(&sv->ms[1], sv->ev[2], sv->ev[3]));
@@ -613,6 +688,8 @@ int ves3d_sv_set_src_coord(ves3d_sv* sv, const double* S, long n_ves, int is_dev
   VES3D_CK(cudaStreamSynchronize(sv->stream));
   sv->have_src = true;
   sv->have_den = false;
+  sv->have_dl = false;  // densities belong to the surfaces they were set for
+  sv->dl_valid = false;
   sv->sl_valid = false;
   sv->parts_valid = false;
   sv->geo_valid = false;
@@ -640,6 +717,40 @@ int ves3d_sv_set_density_sl(ves3d_sv* sv, const double* f, int is_device) {
   return VES3D_OK;
 }
 
+int ves3d_sv_set_density_dl(ves3d_sv* sv, const double* g, int is_device) {
+  int s = check_sv(sv);
+  if (s) return s;
+  if (!sv->have_src) {
+    set_error("set_density_dl before set_src_coord");
+    return VES3D_ERR_STATE;
+  }
+  if (!g) {  // SetDensityDL(NULL): the double layer off
+    if (sv->have_dl) sv->drop_graph();
+    sv->have_dl = false;
+    sv->parts_valid = false;
+    return VES3D_OK;
+  }
+  if ((s = alloc_dl(sv))) return s;
+  if ((s = copy_in(sv->G, g, (size_t)sv->npts() * 3, is_device, sv->stream))) return s;
+  if (!sv->have_dl) sv->drop_graph();  // a captured evaluation without the double layer
+  sv->have_dl = true;
+  sv->parts_valid = false;
+  return VES3D_OK;
+}
+
+int ves3d_sv_get_dl_matrix(ves3d_sv* sv, double* DL, int is_device) {
+  int s = check_sv(sv);
+  if (s) return s;
+  VES3D_ARG(DL != nullptr, "DL is null");
+  if (!sv->have_src || !sv->have_dl) {
+    set_error("no surfaces or no double-layer density set");
+    return VES3D_ERR_STATE;
+  }
+  if (!sv->dl_valid && (s = run_setup(sv, true))) return s;
+  const size_t n = 3 * (size_t)ncoef_(sv->p);
+  return copy_out(DL, sv->DL, (size_t)sv->nves * n * n, is_device, sv->stream);
+}
+
 int ves3d_sv_setup(ves3d_sv* sv) {
   int s = check_sv(sv);
   if (s) return s;
@@ -654,14 +765,14 @@ int ves3d_sv_eval(ves3d_sv* sv, double* vel, int is_device) {
   int s = check_sv(sv);
   if (s) return s;
   VES3D_ARG(vel != nullptr, "vel is null");
-  if ((s = run_eval(sv))) return s;
+  if ((s = run_eval(sv, sv->have_dl))) return s;
   return copy_out(vel, sv->V, (size_t)sv->npts() * 3, is_device, sv->stream);
 }
 
 int ves3d_sv_eval_resident(ves3d_sv* sv) {
   int s = check_sv(sv);
   if (s) return s;
-  return run_eval(sv);
+  return run_eval(sv, sv->have_dl);
 }
 
 int ves3d_set_autotune(int on) { return set_autotune(on); }
@@ -697,9 +808,9 @@ int ves3d_sv_capture_eval(ves3d_sv* sv) {
   if (!sv->sl_valid && (s = run_setup(sv))) return s;
   // one eager pass first: every launcher sets its kernel attributes outside the capture
   sv->have_den = true;
-  if ((s = run_eval(sv))) return s;
+  if ((s = run_eval(sv, sv->have_dl))) return s;
   VES3D_CK(cudaStreamBeginCapture(sv->stream, cudaStreamCaptureModeThreadLocal));
-  s = run_eval_body(sv);
+  s = run_eval_body(sv, sv->have_dl);
   cudaGraph_t g = nullptr;
   const cudaError_t e = cudaStreamEndCapture(sv->stream, &g);
   if (!s && e != cudaSuccess) s = cuda_status(e, "cudaStreamEndCapture", __FILE__, __LINE__);
@@ -958,6 +1069,15 @@ int ves3d_cuda_stokes_f64(int src_m, int trg_m, int n, int t_head, int t_tail, c
   VES3D_ARG(src_m >= 0 && trg_m >= 0 && n >= 0, "negative size");
   VES3D_ARG(t_head >= 0 && t_tail <= trg_m && t_head <= t_tail, "target range outside [0, trg_m]");
   return launch_direct_stokes_f64(src_m, trg_m, n, t_head, t_tail, T, S, D, U, Q, (cudaStream_t)stream);
+}
+
+int ves3d_cuda_stokes_double_layer_f64(int src_m, int trg_m, int n, int t_head, int t_tail, const double* T,
+                                       const double* S, const double* N, const double* D, double* U, const double* Q,
+                                       void* stream) {
+  VES3D_ARG(T && S && N && D && U, "null pointer");
+  VES3D_ARG(src_m >= 0 && trg_m >= 0 && n >= 0, "negative size");
+  VES3D_ARG(t_head >= 0 && t_tail <= trg_m && t_head <= t_tail, "target range outside [0, trg_m]");
+  return launch_direct_stokes_dl_f64(src_m, trg_m, n, t_head, t_tail, T, S, N, D, U, Q, (cudaStream_t)stream);
 }
 
 int ves3d_stokes_alltoall_device_f64(const double* src, const double* den, size_t np, double* pot, void* stream) {
@@ -1224,7 +1344,7 @@ int stokes_apply(ves3d_sv* sv, const double* f, double* out) {
   const size_t n = (size_t)sv->npts() * 3;
   VES3D_CK(cudaMemcpyAsync(sv->F, f, n * sizeof(double), cudaMemcpyDeviceToDevice, sv->stream));
   sv->have_den = true;
-  if ((s = run_eval(sv))) return s;
+  if ((s = run_eval(sv, /*dl=*/false))) return s;
   VES3D_CK(cudaMemcpyAsync(out, sv->V, n * sizeof(double), cudaMemcpyDeviceToDevice, sv->stream));
   return VES3D_OK;
 }

@@ -93,6 +93,17 @@ class StokesVelocity:
             raise ValueError("density size does not match the surfaces")
         check(lib().ves3d_sv_set_density_sl(self._h, p, dev), "SetDensitySL")
 
+    def SetDensityDL(self, g):
+        """Double-layer density (same layout as the surfaces), or None to turn the double
+        layer off; while set, the evaluation adds its velocity."""
+        if g is None:
+            check(lib().ves3d_sv_set_density_dl(self._h, None, 0), "SetDensityDL")
+            return
+        p, dev, n = _ptr(g)
+        if n != self.n_ves * 3 * ngrid(self.sh_order):
+            raise ValueError("density size does not match the surfaces")
+        check(lib().ves3d_sv_set_density_dl(self._h, p, dev), "SetDensityDL")
+
     def __call__(self, out=None):
         if out is None:
             out = np.empty(self.n_ves * 3 * ngrid(self.sh_order))
@@ -110,6 +121,14 @@ class StokesVelocity:
         n = 3 * ncoef(self.sh_order)
         out = np.empty((self.n_ves, n, n))
         check(lib().ves3d_sv_get_self_matrix(self._h, out.ctypes.data, 0), "self_matrix")
+        return out
+
+    def dl_matrix(self):
+        """The double-layer self matrices [n_ves][3 Ncoef][3 Ncoef] (a double-layer density
+        must be set)."""
+        n = 3 * ncoef(self.sh_order)
+        out = np.empty((self.n_ves, n, n))
+        check(lib().ves3d_sv_get_dl_matrix(self._h, out.ctypes.data, 0), "dl_matrix")
         return out
 
     def parts(self):
