@@ -65,9 +65,43 @@ def streamable(ref_stream=None):
     subprocess.check_call([ref_stream, "pack", "4", "2", out], env=dict(os.environ, VES3D_DIR="/root/reference"))
 
 
+def double_layer():
+    """The reference's double layer: the DL self matrix of vesicle 0 and the DL self velocity
+    of two ellipsoids at p = 6 (StokesSingularInteg with DLMatrix), and the far double layer
+    of an 8-vesicle p = 6 suspension from DirectStokesDoubleLayerKernel over all points as
+    one surface minus its per-vesicle sums, with unit normals from the reference's
+    SHC2Grid derivatives and densities times its area element and weights."""
+    reflib.set_threads(os.cpu_count() or 1)
+    p = 6
+    X = ellipsoid_pair(p)
+    g = np.random.default_rng(16).standard_normal(X.size)
+    _, DL = reflib.singular_matrices(X, p, 2 * p, sl=False, dl=True)
+    n = 3 * p * (p + 2)
+    vel_self = reflib.self_apply(DL, g, p)
+    Xs, _ = workloads.suspension(2, p, 3.0, semi_axes=(1.0, 1.0, 0.6), deg=4, amp=0.05, seed=17)
+    gs = np.random.default_rng(18).standard_normal(Xs.size)
+    ng = 2 * p * (p + 1)
+    nv = Xs.size // (3 * ng)
+    _, Xt, Xp = reflib.shc2grid(reflib.grid2shc(Xs, p, p), p, p, grads=True)
+    nrm = np.cross(Xt.reshape(nv, 3, ng), Xp.reshape(nv, 3, ng), axis=1)
+    nrm = (nrm / np.sqrt((nrm * nrm).sum(axis=1))[:, None, :]).reshape(-1)
+    area, qw = reflib.area_weights(Xs, p)
+    den = (gs.reshape(nv, 3, ng) * (area.reshape(nv, 1, ng) * qw.reshape(1, 1, ng))).reshape(-1)
+
+    def whole(A):
+        return np.ascontiguousarray(A.reshape(nv, 3, ng).transpose(1, 0, 2).reshape(-1))
+
+    allp = reflib.direct_stokes_dl(nv * ng, nv * ng, 1, 0, nv * ng, None, whole(Xs), whole(Xs), whole(nrm), whole(den))
+    allp = allp.reshape(3, nv, ng).transpose(1, 0, 2).reshape(-1)
+    own = reflib.direct_stokes_dl(ng, ng, nv, 0, ng, None, Xs, Xs, nrm, den)
+    np.savez_compressed(os.path.join(HERE, "ref_p6_double_layer.npz"), p=p, X=X, g=g, DL0=DL[: n * n],
+                        vel_self=vel_self, Xs=Xs, gs=gs, far_dl=allp - own)
+
+
 def main():
     dumbbell()
     streamable()
+    double_layer()
     assert reflib.available(), "build oracle/_ref first (make -C oracle/ref)"
     reflib.set_threads(os.cpu_count() or 1)
     # p = 6: two ellipsoids; quadrature rules, transforms, the self matrix of vesicle 0

@@ -56,3 +56,18 @@ def test_golden_inputs_match_generator(gc1):
     from ves3d_b200 import workloads
     X, f, p = workloads.make("c1_8ves_p12")
     assert np.array_equal(X, gc1["X"]) and np.array_equal(f, gc1["f"])
+
+
+@pytest.fixture(scope="module")
+def gdl():
+    return dict(np.load(os.path.join(HERE, "ref_p6_double_layer.npz")))
+
+
+def test_golden_double_layer(gdl):
+    """The oracle's DL self matrix, DL self velocity and far double layer against the
+    reference's (StokesSingularInteg with DLMatrix; DirectStokesDoubleLayerKernel)."""
+    p = int(gdl["p"])
+    DL = sh.stokes_singular_matrix(gdl["X"], p, 2 * p, single=False)
+    assert rel_err(DL[0].reshape(-1), gdl["DL0"]) < REF_SELF_NOISE
+    assert rel_err(sh.self_apply(DL, gdl["g"], p), gdl["vel_self"]) < REF_SELF_NOISE
+    assert rel_err(stokes.far_dl_velocity(gdl["Xs"], gdl["gs"], p), gdl["far_dl"]) < 1e-12

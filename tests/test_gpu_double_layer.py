@@ -129,3 +129,30 @@ def test_direct_stokes_double_layer_matches_oracle(weighted):
     torch.cuda.synchronize()
     ref = stokes.direct_stokes_dl(ns, nt, nv, head, tail, Q, T, S, N, D)
     assert rel_err(U.cpu().numpy(), ref) < TOL
+
+
+def test_double_layer_against_the_reference_fixture():
+    """The GPU double layer against the reference's own outputs (tests/golden/
+    ref_p6_double_layer.npz): the DL self matrix and self velocity within the reference's
+    self-part noise (5e-9), the far double layer at 1e-12."""
+    import os
+    gdl = dict(np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_p6_double_layer.npz")))
+    p = int(gdl["p"])
+    n = 3 * p * (p + 2)
+    with StokesVelocity(p, 2 * p) as sv:
+        sv.SetSrcCoord(gdl["X"])
+        sv.SetDensitySL(np.zeros_like(gdl["X"]))
+        sv.SetDensityDL(gdl["g"])
+        DL = sv.dl_matrix()
+        vel = sv()
+        vself, _ = sv.parts()
+    assert rel_err(DL[0].reshape(-1), gdl["DL0"]) < 5e-9
+    assert rel_err(vself, gdl["vel_self"]) < 5e-9  # the single-layer density is zero
+    with StokesVelocity(p, 2 * p) as sv:
+        sv.SetSrcCoord(gdl["Xs"])
+        sv.SetDensitySL(np.zeros_like(gdl["Xs"]))
+        sv.SetDensityDL(gdl["gs"])
+        sv()
+        _, vfar = sv.parts()
+    assert rel_err(vfar, gdl["far_dl"]) < TOL
+    assert n == DL.shape[1] and vel.size == gdl["X"].size
