@@ -199,10 +199,15 @@ def shear_flow(X, rate):
 class ImplicitStep:
     """Globally implicit step solving for the velocity (pseudospectral form):
         u - S[f(dt u, sigma)] = u_inf + S[f_b(x)],     -div S[f] = div(u_inf + S[f_b])
-    with f(y, sigma) = lin_bending(y) + tension(sigma)."""
+    with f(y, sigma) = lin_bending(y) + tension(sigma).
+
+    With a viscosity contrast lambda (scalar or per vesicle; VesicleProps.cc:27-49) the
+    operator becomes (ImplicitApply, src/InterfacialVelocity.cc:934-966)
+        (1 + lambda)/2 u - S[f] - D[(1 - lambda) u],   -div(S[f] + D[(1 - lambda) u])
+    and the right-hand side is unchanged (AssembleRhsVel, :717-745)."""
 
     def __init__(self, X, p, kappa, dt, shear_rate, SL=None, excess_density=0.0, gravity=(0.0, 0.0, -1.0),
-                 filter_freq=None):
+                 filter_freq=None, viscosity_contrast=None):
         self.p = p
         self.X = np.asarray(X, dtype=np.float64)
         self.geo = geometry(self.X, p, filter_freq)
@@ -210,6 +215,17 @@ class ImplicitStep:
         self.drho, self.g = excess_density, np.asarray(gravity, dtype=np.float64)
         self.SL = SL if SL is not None else sh.stokes_singular_matrix(self.X, p, 2 * p)
         self.nv, _, self.ng = self.geo["n"].shape
+        lam = np.broadcast_to(np.asarray(1.0 if viscosity_contrast is None else viscosity_contrast, np.float64),
+                              (self.nv,)).copy()
+        self.contrast = bool(np.any(np.abs(lam - 1.0) > 1e-12))  # has_contrast (VesicleProps.cc:45-49)
+        self.vel_coeff = (0.5 + 0.5 * lam)[:, None, None]
+        self.dl_coeff = (1.0 - lam)[:, None, None]
+        self._DL = None
+
+    def stokes_dl(self, g):
+        if self._DL is None:
+            self._DL = sh.stokes_singular_matrix(self.X, self.p, 2 * self.p, single=False)
+        return stokes.stokes_velocity_dl(self.X, g.reshape(-1), self.p, DL=self._DL)
 
     def stokes(self, f):
         return sh.self_apply(self.SL, f.reshape(-1), self.p) + stokes.far_velocity(self.X, f.reshape(-1), self.p)
@@ -224,6 +240,9 @@ class ImplicitStep:
         if self.drho:
             f = f + gravity_force(self.dt * u, self.geo, self.drho, self.g)
         Sf = self.stokes(f).reshape(u.shape)
+        if self.contrast:
+            Sf = Sf + self.stokes_dl(self.dl_coeff * u).reshape(u.shape)
+            return np.concatenate([(self.vel_coeff * u - Sf).reshape(-1), (-div(Sf, self.geo)).reshape(-1)])
         return np.concatenate([(u - Sf).reshape(-1), (-div(Sf, self.geo)).reshape(-1)])
 
     def precond_scales(self):
