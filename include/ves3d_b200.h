@@ -219,6 +219,14 @@ int ves3d_sv_set_implicit_params(ves3d_sv* sv, double dt, double kappa, double s
  * without force and the implicit system singular (BiCGStab then stops at max_iter). */
 int ves3d_sv_set_surface_filter(ves3d_sv* sv, int filter_freq);
 int ves3d_sv_set_gravity(ves3d_sv* sv, double excess_density, double gx, double gy, double gz);
+/* Viscosity contrast of the vesicles (interior / exterior viscosity; VesicleProps,
+ * src/VesicleProps.cc:17-49): n = 1 value for all vesicles or one per vesicle, NULL (or
+ * n = 0) for none. With a contrast other than 1 the implicit operator becomes
+ * [(1 + l)/2 u - S[f] - D[(1 - l) u]; -div(S[f] + D[(1 - l) u])] (ImplicitApply,
+ * src/InterfacialVelocity.cc:934-966) with the double layer of ves3d_sv_set_density_dl; the
+ * right-hand side is unchanged (AssembleRhsVel, :717-745). The solve then uses the
+ * context's double-layer density buffer (a density set before is cleared). */
+int ves3d_sv_set_viscosity_contrast(ves3d_sv* sv, const double* lambda, long n);
 int ves3d_sv_surface_op(ves3d_sv* sv, int op, const double* in, double* out, int is_device);
 /* Solve the implicit system with BiCGStab in its Galerkin form (unknowns: SH coefficients
  * of u and sigma, ImplicitApply src/InterfacialVelocity.cc:982-1052; the reference's

@@ -108,6 +108,10 @@ class StokesVelocity {
   void SetImplicitParams(Real dt, Real bending_modulus, Real shear_rate) {
     check(ves3d_sv_set_implicit_params(sv_, dt, bending_modulus, shear_rate), "SetImplicitParams");
   }
+  /* the vesicles' viscosity contrast: one value for all, or one per vesicle (n values) */
+  void SetViscosityContrast(const Real* lambda, long n) {
+    check(ves3d_sv_set_viscosity_contrast(sv_, lambda, n), "SetViscosityContrast");
+  }
   void SetPrecond(int scheme, int refresh_every = 1) {
     check(ves3d_sv_set_precond(sv_, scheme), "SetPrecond");
     check(ves3d_sv_set_precond_refresh(sv_, refresh_every), "SetPrecond");

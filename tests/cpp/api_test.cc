@@ -74,6 +74,7 @@ int main(int argc, char** argv) {
     stokes(vel);
     stokes.SetDensityDL((const std::vector<double>*)0);  // InterfacialVelocity's call without contrast
     // the reference's implicit step on the same surfaces, self-block preconditioned
+    stokes.SetViscosityContrast((const double*)0, 0);  // no contrast
     stokes.SetImplicitParams(0.01, 0.05, 1.0);
     stokes.SetPrecond(VES3D_PRECOND_SELF_BLOCK);
     double tol = 1e-9;

@@ -70,7 +70,8 @@ def test_argument_errors_of_the_implicit_and_filter_entry_points():
     assert L.ves3d_sht_lowpass(None, 1, 16, -1, 0.0, None, None) == 1
     assert L.ves3d_sht_scale_freq(None, 1, 16, None, None, None) == 1
     assert L.ves3d_sht_lowpass(out.ctypes.data, -1, 16, -1, 0.0, out.ctypes.data, None) == 1
-    # double layer
+    # double layer and viscosity contrast
+    assert L.ves3d_sv_set_viscosity_contrast(None, None, 0) == 1
     assert L.ves3d_sv_set_density_dl(None, None, 0) == 1
     assert L.ves3d_sv_get_dl_matrix(None, None, 0) == 1
     assert L.ves3d_cuda_stokes_double_layer_f64(4, 4, 1, 0, 4, None, None, None, None, None, None, None) == 1

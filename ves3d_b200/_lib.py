@@ -70,6 +70,7 @@ SIGNATURES = [
     ("ves3d_stokes_alltoall_noalloc_f64", _i, [_vp, _vp, _sz, _vp, _vp]),
     ("ves3d_sv_set_implicit_params", _i, [_vp, _d, _d, _d]),
     ("ves3d_sv_set_gravity", _i, [_vp, _d, _d, _d, _d]),
+    ("ves3d_sv_set_viscosity_contrast", _i, [_vp, _vp, _l]),
     ("ves3d_sv_surface_op", _i, [_vp, _i, _vp, _vp, _i]),
     ("ves3d_sv_implicit_solve", _i, [_vp, _vp, _vp, ctypes.POINTER(_d), ctypes.POINTER(_i), ctypes.POINTER(_i), _i]),
     ("ves3d_svp_create", _i, [_i, _i, ctypes.POINTER(_vp)]),

@@ -294,6 +294,22 @@ int launch_far_density(const double* f, const double* area, long nv, int p0, con
   return VES3D_OK;
 }
 
+__global__ void k_scale_vesicles(const double* __restrict__ x, long n, long per, const double* __restrict__ c, long nc,
+                                 const double* __restrict__ z, double beta, double* __restrict__ out) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double v = c[(i / per) % nc] * x[i];
+  out[i] = z ? fma(beta, z[i], v) : v;
+}
+
+int launch_scale_vesicles(const double* x, long n, long per, const double* c, long nc, const double* z, double beta,
+                          double* out, cudaStream_t st) {
+  if (n <= 0) return VES3D_OK;
+  k_scale_vesicles<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(x, n, per, c, nc, z, beta, out);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
 __global__ void k_add(const double* __restrict__ a, const double* __restrict__ b, long n, double* __restrict__ out) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = a[i] + b[i];

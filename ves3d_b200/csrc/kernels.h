@@ -68,7 +68,12 @@ int launch_build_ring(const double* R, long nrot, const DevTables& T, double* C,
 int launch_self_gemv(const double* F, const double* SL, long nv, int n, double* V, cudaStream_t st,
                      bool accumulate = false);
 // nvec density vectors per vesicle, layout [q][nv][n]; nvec <= 8
-int launch_self_gemv_multi(const double* F, const double* SL, long nv, int nvec, int n, double* V, cudaStream_t st);
+int launch_self_gemv_multi(const double* F, const double* SL, long nv, int nvec, int n, double* V, cudaStream_t st,
+                           bool accumulate = false);
+// out[i] = c[(i / per) % nc] x[i] + beta z[i] (z null: the first term alone): a per-vesicle
+// coefficient (nc vesicles, per values each, repeated over batched copies)
+int launch_scale_vesicles(const double* x, long n, long per, const double* c, long nc, const double* z, double beta,
+                          double* out, cudaStream_t st);
 // area element |X_theta x X_phi| and far-field sources: pos/den point-major [N][3],
 // den = f * area * smooth_w[lat]; X, f, Xt, Xp AxisMajor [nv][3][ng].
 int launch_far_sources(const double* X, const double* f, const double* Xt, const double* Xp, long nv, int p0,

@@ -490,6 +490,7 @@ __global__ void __launch_bounds__(128) k_self_gemv(const double* __restrict__ F,
 // V[q nv + v][col] = sum_row F[q nv + v][row] SL[v][row][col], q < nvec; every SL column is
 // read once for all nvec vectors (the single-vector form reads it per vector).
 constexpr int kGemvMaxVec = 8;
+template <bool ACC>
 __global__ void __launch_bounds__(128) k_self_gemv_multi(const double* __restrict__ F, const double* __restrict__ SL,
                                                          long nv, int nvec, int n, double* __restrict__ V) {
   extern __shared__ double sF[];  // [nvec][n]
@@ -513,10 +514,14 @@ __global__ void __launch_bounds__(128) k_self_gemv_multi(const double* __restric
   }
 #pragma unroll
   for (int q = 0; q < kGemvMaxVec; q++)
-    if (q < nvec) V[((long)q * nv + v) * n + col] = acc[q];
+    if (q < nvec) {
+      double* o = V + ((long)q * nv + v) * n + col;
+      *o = ACC ? *o + acc[q] : acc[q];
+    }
 }
 
-int launch_self_gemv_multi(const double* F, const double* SL, long nv, int nvec, int n, double* V, cudaStream_t st) {
+int launch_self_gemv_multi(const double* F, const double* SL, long nv, int nvec, int n, double* V, cudaStream_t st,
+                           bool accumulate) {
   if (nv <= 0 || nvec <= 0) return VES3D_OK;
   if (nvec > kGemvMaxVec) {
     set_error("launch_self_gemv_multi: at most %d vectors", kGemvMaxVec);
@@ -524,9 +529,15 @@ int launch_self_gemv_multi(const double* F, const double* SL, long nv, int nvec,
   }
   dim3 grid((n + 127) / 128, (unsigned)nv);
   const size_t smem = (size_t)nvec * n * sizeof(double);
-  if (smem > 48 * 1024)
-    VES3D_CK(cudaFuncSetAttribute(k_self_gemv_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_self_gemv_multi<<<grid, 128, smem, st>>>(F, SL, nv, nvec, n, V);
+  if (accumulate) {
+    if (smem > 48 * 1024)
+      VES3D_CK(cudaFuncSetAttribute(k_self_gemv_multi<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_self_gemv_multi<true><<<grid, 128, smem, st>>>(F, SL, nv, nvec, n, V);
+  } else {
+    if (smem > 48 * 1024)
+      VES3D_CK(cudaFuncSetAttribute(k_self_gemv_multi<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_self_gemv_multi<false><<<grid, 128, smem, st>>>(F, SL, nv, nvec, n, V);
+  }
   VES3D_LAUNCHED();
   return VES3D_OK;
 }

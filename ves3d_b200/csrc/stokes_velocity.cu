@@ -160,6 +160,12 @@ struct ves3d_sv {
   bool have_dl = false, dl_valid = false;
   int nseg_dl = 0;
   float dl_ms = 0;  // last double-layer self-matrix build (device ms)
+  // viscosity contrast of the implicit step (VesicleProps, src/VesicleProps.cc:17-49): lambda
+  // per vesicle (one value: all), and on device vel_coeff = (1 + l)/2, dl_coeff = 1 - l
+  std::vector<double> lam;
+  bool contrast = false;
+  double *velc = nullptr, *dlc = nullptr;
+  long contrast_nves = -1;  // vesicle count the device coefficients were made for
   long* off = nullptr;  // [nves+1] point offsets of the vesicles
   long off_nves = -1;   // vesicle count the offsets were uploaded for
   // setup scratch (one chunk of vesicles)
@@ -204,6 +210,8 @@ struct ves3d_sv {
 
   ~ves3d_sv() {
     dfree(filt);
+    dfree(velc);
+    dfree(dlc);
     drop_graph();
     free_precond();
     for (auto& e : pc_ev)
@@ -350,7 +358,7 @@ int alloc_scratch(ves3d_sv* sv) {
   const long want = sv->nves;
   // the double layer is built stage by stage: those stage buffers are kept while a
   // double-layer density is set (the fused single-layer build needs a subset of them)
-  const bool stages = !use_fused(sv) || sv->have_dl;
+  const bool stages = !use_fused(sv) || sv->have_dl || sv->contrast;
   const bool layout_ok = !stages || sv->K != nullptr;
   if (sv->chunk >= want && layout_ok) return VES3D_OK;  // the whole suspension in one chunk already
   const bool fused = !stages;
@@ -562,7 +570,7 @@ int run_eval(ves3d_sv* sv, bool dl) {
   // the far field first (on the side stream when overlapping the self-matrix build, else
   // on the context's stream); events ev[4], ev[5] bracket its segment kernels (the
   // roofline denominator)
-  if (dl && !sv->have_dl) {
+  if (dl && !sv->G) {
     set_error("double layer requested without a double-layer density");
     return VES3D_ERR_STATE;
   }
@@ -1325,26 +1333,36 @@ int op_tension(ves3d_sv* sv, const double* sigma, const double* add, double* out
 // Self part of the single layer for every field vesicle of a batched space (the isolated
 // vesicles' operator; no far field): coefficients, one read of each self matrix for all
 // copies, synthesis.
-int stokes_self_batch(ves3d_sv* sv, const OpSpace& sp, const double* f, double* out) {
+int stokes_self_batch(ves3d_sv* sv, const OpSpace& sp, const double* f, double* out, const double* g = nullptr) {
   int s;
   const DevTables& T = sv->tab->d;
   const int p0 = sv->p, n = 3 * ncoef_(p0);
   if (!sv->sl_valid && (s = run_setup(sv))) return s;
+  if (g && !sv->dl_valid && (s = run_setup(sv, true))) return s;
   if ((s = launch_grid2shc(f, sp.nv * 3, p0, T.ana_four, T.ana_leg, T.jf_of_coef, sp.fc, sv->stream))) return s;
   if ((s = launch_self_gemv_multi(sp.fc, sv->SL, sv->nves, (int)(sp.nv / sv->nves), n, sp.vc, sv->stream)))
     return s;
+  if (g) {  // the double layer's self part of density g, added in coefficients
+    if ((s = launch_grid2shc(g, sp.nv * 3, p0, T.ana_four, T.ana_leg, T.jf_of_coef, sp.fc, sv->stream))) return s;
+    if ((s = launch_self_gemv_multi(sp.fc, sv->DL, sv->nves, (int)(sp.nv / sv->nves), n, sp.vc, sv->stream,
+                                    /*accumulate=*/true)))
+      return s;
+  }
   return launch_synthesis(sp.vc, sp.nv * 3, p0, p0, T.syn0_leg, T.syn0_dleg, T.syn0_four, T.syn0_dfour, T.blk_off, out,
                           nullptr, nullptr, sv->stream);
 }
 
 // Stokes single layer of a device density f (AxisMajor) -> out (device), through the
 // context's cached self matrices and far field.
-int stokes_apply(ves3d_sv* sv, const double* f, double* out) {
+// With dl, the double layer of the density already in the context's buffer G is added; the
+// buffer is the operator's from then on (the context's double-layer density is cleared).
+int stokes_apply(ves3d_sv* sv, const double* f, double* out, bool dl = false) {
   int s;
   const size_t n = (size_t)sv->npts() * 3;
   VES3D_CK(cudaMemcpyAsync(sv->F, f, n * sizeof(double), cudaMemcpyDeviceToDevice, sv->stream));
   sv->have_den = true;
-  if ((s = run_eval(sv, /*dl=*/false))) return s;
+  if (dl) sv->have_dl = false;
+  if ((s = run_eval(sv, dl))) return s;
   VES3D_CK(cudaMemcpyAsync(out, sv->V, n * sizeof(double), cudaMemcpyDeviceToDevice, sv->stream));
   return VES3D_OK;
 }
@@ -1407,12 +1425,55 @@ int implicit_finish(ves3d_sv* sv, const OpSpace& sp, const double* x, const doub
 
 // S is the context's full single layer, or the self part alone for a batched space
 // (self_batch)
+int ensure_contrast(ves3d_sv* sv);
+
 int implicit_matvec(ves3d_sv* sv, const OpSpace& sp, const ImplicitWork& iw, bool self_batch, const double* x,
                     double* y) {
   int s;
   if ((s = implicit_forces(sv, sp, iw, x))) return s;
-  if ((s = self_batch ? stokes_self_batch(sv, sp, iw.f, iw.Sf) : stokes_apply(sv, iw.f, iw.Sf))) return s;
-  return implicit_finish(sv, sp, x, iw.Sf, y);
+  if (!sv->contrast) {
+    if ((s = self_batch ? stokes_self_batch(sv, sp, iw.f, iw.Sf) : stokes_apply(sv, iw.f, iw.Sf))) return s;
+    return implicit_finish(sv, sp, x, iw.Sf, y);
+  }
+  // viscosity contrast (ImplicitApply, src/InterfacialVelocity.cc:934-966):
+  // Sf = S[f] + D[(1 - l) u], y = [(1 + l)/2 u - Sf; -div Sf]. iw.y (dt u) is free after the forces.
+  const long N = sp.nv * ngrid_(sv->p), per = 3L * ngrid_(sv->p);
+  if ((s = ensure_contrast(sv)) || (s = alloc_dl(sv))) return s;
+  if (self_batch) {
+    if ((s = launch_scale_vesicles(x, 3 * N, per, sv->dlc, sv->nves, nullptr, 0.0, iw.y, sv->stream))) return s;
+    if ((s = stokes_self_batch(sv, sp, iw.f, iw.Sf, iw.y))) return s;
+  } else {
+    if ((s = launch_scale_vesicles(x, 3 * N, per, sv->dlc, sv->nves, nullptr, 0.0, sv->G, sv->stream))) return s;
+    if ((s = stokes_apply(sv, iw.f, iw.Sf, /*dl=*/true))) return s;
+  }
+  if ((s = launch_scale_vesicles(x, 3 * N, per, sv->velc, sv->nves, iw.Sf, -1.0, y, sv->stream))) return s;
+  return op_div(sv, sp, iw.Sf, y + 3 * N, -1.0);
+}
+
+// Device coefficients of the viscosity contrast for the current vesicle count.
+int ensure_contrast(ves3d_sv* sv) {
+  if (sv->contrast_nves == sv->nves && sv->velc) return VES3D_OK;
+  const long nv = sv->nves;
+  if (sv->lam.size() != 1 && (long)sv->lam.size() != nv) {
+    set_error("viscosity contrast was set for %ld vesicles, the surfaces have %ld", (long)sv->lam.size(), nv);
+    return VES3D_ERR_STATE;
+  }
+  std::vector<double> vc(nv), dc(nv);
+  for (long v = 0; v < nv; v++) {
+    const double l = sv->lam.size() == 1 ? sv->lam[0] : sv->lam[v];
+    vc[v] = 0.5 + 0.5 * l;  // VesicleProps.cc:27-32
+    dc[v] = 1.0 - l;        // :34-39
+  }
+  dfree(sv->velc);
+  dfree(sv->dlc);
+  sv->velc = sv->dlc = nullptr;
+  sv->contrast_nves = -1;
+  int s = dupload(&sv->velc, vc, sv->stream);
+  if (!s) s = dupload(&sv->dlc, dc, sv->stream);
+  if (s) return s;
+  VES3D_CK(cudaStreamSynchronize(sv->stream));
+  sv->contrast_nves = nv;
+  return VES3D_OK;
 }
 
 int implicit_matvec(ves3d_sv* sv, const double* x, double* y) {
@@ -2044,6 +2105,26 @@ int ves3d_sv_set_gravity(ves3d_sv* sv, double excess_density, double gx, double 
   sv->grav[0] = gx;
   sv->grav[1] = gy;
   sv->grav[2] = gz;
+  return VES3D_OK;
+}
+
+int ves3d_sv_set_viscosity_contrast(ves3d_sv* sv, const double* lambda, long n) {
+  int s = check_sv(sv);
+  if (s) return s;
+  if (!lambda || n == 0) {
+    sv->lam.clear();
+    sv->contrast = false;
+    sv->pc_valid = false;
+    return VES3D_OK;
+  }
+  VES3D_ARG(n == 1 || (sv->have_src && n == sv->nves), "n must be 1 or the number of vesicles");
+  for (long i = 0; i < n; i++) VES3D_ARG(std::isfinite(lambda[i]) && lambda[i] > 0.0, "contrast must be positive");
+  sv->lam.assign(lambda, lambda + n);
+  bool any = false;
+  for (double l : sv->lam) any |= std::fabs(l - 1.0) > 1e-12;  // has_contrast, VesicleProps.cc:45-49
+  sv->contrast = any;
+  sv->contrast_nves = -1;
+  sv->pc_valid = false;  // the self-block preconditioner is built from the operator
   return VES3D_OK;
 }
 

@@ -175,6 +175,14 @@ class StokesVelocity:
         """Excess density of the vesicles and the gravity field (sedimentation)."""
         check(lib().ves3d_sv_set_gravity(self._h, float(excess_density), *[float(c) for c in g]), "set_gravity")
 
+    def set_viscosity_contrast(self, lam):
+        """Viscosity contrast of the implicit step: one value, one per vesicle, or None."""
+        if lam is None:
+            check(lib().ves3d_sv_set_viscosity_contrast(self._h, None, 0), "set_viscosity_contrast")
+            return
+        a = np.ascontiguousarray(np.atleast_1d(np.asarray(lam, dtype=np.float64)))
+        check(lib().ves3d_sv_set_viscosity_contrast(self._h, a.ctypes.data, a.size), "set_viscosity_contrast")
+
     def set_surface_filter(self, filter_freq=-1):
         """The reference Surface's low-pass filter on H, K, gradients, divergences and the
         linearised curvature: 0 off (default), -1 degrees <= 2p/3, n > 0 degrees <= n."""
