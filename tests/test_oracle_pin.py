@@ -220,3 +220,22 @@ def test_double_layer_sphere_identity():
     g = np.repeat(c[:, None], sh.ngrid(p), axis=1).reshape(-1)
     u = sh.self_apply(sh.stokes_singular_matrix(X, p, 2 * p, single=False), g, p).reshape(3, -1)
     assert np.abs(u + 0.5 * c[:, None]).max() < 1e-13
+
+
+def test_reference_double_layer_test_setup():
+    """The setup of the reference's test/StokesDoubleLayerTest.cc:59-170 (p = 6, a unit sphere
+    sampled at equispaced latitudes (i+1) pi/8 about the x axis, density 1 in every
+    component), whose known answer is |velocity| = 1/2 within 0.03. With the outward normal
+    X_theta x X_phi of StokesVelocity the double layer is -1/2 (1.8e-5 here); the test
+    asserts +1/2 through Surface::getNormal() and DirectStokesDoubleLayer, i.e. with the
+    normal of the opposite orientation."""
+    p = 6
+    i = np.arange(p + 1)[:, None]
+    j = np.arange(2 * p)[None, :]
+    th = (i + 1) * np.pi / (p + 2)
+    X = np.stack([np.cos(th) + 0 * j, np.sin(th) * np.sin(j * np.pi / p), np.sin(th) * np.cos(j * np.pi / p)])
+    X = X.reshape(-1)
+    n = stokes.unit_normal(X, p).reshape(3, -1)
+    assert (n * X.reshape(3, -1)).sum(axis=0).min() > 0.99  # outward
+    u = sh.self_apply(sh.stokes_singular_matrix(X, p, 2 * p, single=False), np.ones(X.size), p)
+    assert np.abs(u + 0.5).max() < 0.03 and np.abs(u + 0.5).max() < 1e-4
