@@ -239,3 +239,20 @@ def test_reference_double_layer_test_setup():
     assert (n * X.reshape(3, -1)).sum(axis=0).min() > 0.99  # outward
     u = sh.self_apply(sh.stokes_singular_matrix(X, p, 2 * p, single=False), np.ones(X.size), p)
     assert np.abs(u + 0.5).max() < 0.03 and np.abs(u + 0.5).max() < 1e-4
+
+
+def test_reference_double_layer_kernel_sign(ref):
+    """The reference's DirectStokesDoubleLayerKernel with outward unit normals and density 1
+    (times area and weights) gives -1 at a sphere's centre: D[c] = -c inside, -c/2 on the
+    surface, the convention of the DL matrices and of this build."""
+    p = 16
+    X = unit_sphere(p)
+    ng = sh.ngrid(p)
+    n = stokes.unit_normal(X, p)
+    w = sh.area_element(X, p).reshape(-1) * sh.smooth_weights_grid(p)
+    den = np.tile(w, 3)
+    T = X.copy()
+    T[0] = T[ng] = T[2 * ng] = 0.0  # target 0 at the centre
+    u = ref.direct_stokes_dl(ng, ng, 1, 0, 1, None, T, X, n, den)
+    assert abs(u[0] + 1) < 1e-12 and abs(u[ng] + 1) < 1e-12 and abs(u[2 * ng] + 1) < 1e-12
+    assert rel_err(stokes.direct_stokes_dl(ng, ng, 1, 0, 1, None, T, X, n, den), u) < FAR_TOL
