@@ -332,6 +332,12 @@ int ves3d_sht_forward(const double* X, long n_fun, int p0, int p1, double* S, vo
  * (X_theta) and latitude (X_phi) derivatives as named by the reference; NULL skips. */
 int ves3d_sht_backward(const double* S, long n_fun, int p0, int p1, double* X, double* X_theta,
                        double* X_phi, void* stream);
+/* SHTrans::backward_d2u / backward_d2v / backward_duv (include/SHTrans.h:21-63): second
+ * derivatives on the order-p grid of order-p coefficients S ([n_fun][p(p+2)], device),
+ * u the latitude and v the longitude of the grid as in SHTrans; any output may be NULL.
+ * Device pointers; builds the order-p tables for the call. */
+int ves3d_sht_backward_d2(const double* S, long n_fun, int p, double* X_uu, double* X_vv, double* X_uv,
+                          void* stream);
 /* SphericalHarmonics::RotateAll (src/SphericalHarmonics.cc:363-449), the coefficient
  * rotation behind MovePole (include/MovePole.h:16-23): every vector field of S (device,
  * [n_vec][3][p(p+2)] coefficients) rotated so that each grid point (latitude t = 0..p,

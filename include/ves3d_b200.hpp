@@ -178,6 +178,16 @@ class SHTrans {
   void backward_to(int q, const Real* shc, long n_funs, Real* out) const {
     check(ves3d_sht_backward(shc, n_funs, p_, q, out, 0, 0, stream_), "SHTrans::backward_to");
   }
+  /* second derivatives (u latitude, v longitude) */
+  void backward_d2u(const Real* shc, long n_funs, Real* out) const {
+    check(ves3d_sht_backward_d2(shc, n_funs, p_, out, 0, 0, stream_), "SHTrans::backward_d2u");
+  }
+  void backward_d2v(const Real* shc, long n_funs, Real* out) const {
+    check(ves3d_sht_backward_d2(shc, n_funs, p_, 0, out, 0, stream_), "SHTrans::backward_d2v");
+  }
+  void backward_duv(const Real* shc, long n_funs, Real* out) const {
+    check(ves3d_sht_backward_d2(shc, n_funs, p_, 0, 0, out, stream_), "SHTrans::backward_duv");
+  }
   /* SphericalHarmonics::SHC2Pole: pole[2 f + t] = function f at x = -1 (t = 0), x = +1 (t = 1) */
   void SHC2Pole(const Real* shc, long n_funs, Real* pole) const {
     check(ves3d_sht_pole(shc, n_funs, p_, pole, stream_), "SHTrans::SHC2Pole");

@@ -33,6 +33,11 @@ static bool read_input(const char* path, int& p, int& nv, std::vector<double>& X
 
 int main(int argc, char** argv) {
   if (argc == 2 && std::strcmp(argv[1], "--version") == 0) {
+    // instantiate the device-pointer members of the SHTrans mirror (a compile check)
+    typedef ves3d_b200::SHTrans<double> Sht;
+    void (Sht::*d2[4])(const double*, long, double*) const = {&Sht::backward_d2u, &Sht::backward_d2v,
+                                                                &Sht::backward_duv, &Sht::SHC2Pole};
+    (void)d2;
     std::printf("%d\n", ves3d_version());
     return 0;
   }

@@ -68,6 +68,9 @@ def test_argument_errors_of_the_implicit_and_filter_entry_points():
     assert L.ves3d_sht_filter_coeffs(16, -1, 0.0, None) == 1
     assert b"coeff" in L.ves3d_last_error()
     assert L.ves3d_sht_lowpass(None, 1, 16, -1, 0.0, None, None) == 1
+    assert L.ves3d_sht_backward_d2(None, 1, 6, None, None, None, None) == 1
+    assert L.ves3d_sht_backward_d2(out.ctypes.data, 1, 6, None, None, None, None) == 1
+    assert L.ves3d_sht_backward_d2(out.ctypes.data, 1, 0, out.ctypes.data, None, None, None) == 1
     assert L.ves3d_sht_scale_freq(None, 1, 16, None, None, None) == 1
     assert L.ves3d_sht_lowpass(out.ctypes.data, -1, 16, -1, 0.0, out.ctypes.data, None) == 1
     # double layer and viscosity contrast

@@ -58,3 +58,22 @@ def test_rotate_all_matches_oracle(p):
     out = torch.empty(ref.size, dtype=torch.float64, device="cuda")
     SHTrans(p).RotateAll(torch.from_numpy(S).cuda(), out)
     assert rel_err(out.cpu().numpy(), ref) < 1e-12
+
+
+@pytest.mark.parametrize("p", [6, 12, 16])
+def test_second_derivatives_match_oracle(p):
+    """ves3d_sht_backward_d2 (SHTrans::backward_d2u / d2v / duv) against the oracle's
+    synthesis of second derivatives (oracle/surface.py synth), 1e-12 relative."""
+    import torch
+    from oracle import surface as su
+    from ves3d_b200.stokes_velocity import SHTrans
+    rng = np.random.default_rng(p + 3)
+    nf = 5
+    S = rng.standard_normal(nf * sh.ncoef(p))
+    outs = {k: torch.empty(nf * sh.ngrid(p), dtype=torch.float64, device="cuda") for k in ("uu", "vv", "uv")}
+    SHTrans(p).backward_d2(torch.from_numpy(S).cuda(), **outs)
+    for k, t in outs.items():
+        assert rel_err(t.cpu().numpy(), su.synth(S, p, k).reshape(-1)) < 1e-12, k
+    only = torch.empty(nf * sh.ngrid(p), dtype=torch.float64, device="cuda")
+    SHTrans(p).backward_d2(torch.from_numpy(S).cuda(), vv=only)  # one output alone
+    assert torch.equal(only, outs["vv"])

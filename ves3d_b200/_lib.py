@@ -58,6 +58,7 @@ SIGNATURES = [
     ("ves3d_sht_scale_freq", _i, [_vp, _l, _i, _vp, _vp, _vp]),
     ("ves3d_sht_lowpass", _i, [_vp, _l, _i, _i, _d, _vp, _vp]),
     ("ves3d_sht_pole", _i, [_vp, _l, _i, _vp, _vp]),
+    ("ves3d_sht_backward_d2", _i, [_vp, _l, _i, _vp, _vp, _vp, _vp]),
     ("ves3d_vtk_write_grid", _i, [_vp, _vp, _vp, _vp, _l, _i, ctypes.c_char_p, _d, _i, _i]),
     ("ves3d_vtk_write", _i, [_vp, _vp, _l, _i, _i, ctypes.c_char_p, _d, _i, _i, _i]),
     ("ves3d_cuda_stokes_f64", _i, [_i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),

@@ -968,6 +968,35 @@ int ves3d_sht_rotate_all(const double* S, long n_vec, int p, double* R, void* st
   return VES3D_OK;
 }
 
+int ves3d_sht_backward_d2(const double* S, long n_fun, int p, double* X_uu, double* X_vv, double* X_uv,
+                          void* stream) {
+  VES3D_ARG(S && (X_uu || X_vv || X_uv), "null pointer");
+  VES3D_ARG(p >= 1 && p <= 127, "order must be in [1, 127]");
+  VES3D_ARG(n_fun >= 0, "n_fun < 0");
+  if (n_fun == 0) return VES3D_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  TablesOwner tab;  // order-p synthesis tables with their second derivatives (freed on return)
+  build_tables(p, 2 * p, tab.h);
+  int s = tab.upload(st);
+  const DevTables& T = tab.d;
+  double* xu = nullptr;  // X_u, computed alongside X_uv and X_uu (not returned)
+  if (!s && (X_uu || X_uv)) {
+    s = dalloc(&xu, (size_t)n_fun * ngrid_(p));
+    // values from d/du P (X_u), their v-derivative (X_uv), and d2/du2 P (X_uu)
+    if (!s)
+      s = launch_synthesis(S, n_fun, p, p, T.syn0_dleg, T.syn0_d2leg, T.syn0_four, T.syn0_dfour, T.blk_off, xu, X_uv,
+                           X_uu, st);
+  }
+  if (!s && X_vv)
+    s = launch_synthesis(S, n_fun, p, p, T.syn0_leg, T.syn0_leg, T.syn0_d2four, T.syn0_d2four, T.blk_off, X_vv,
+                         nullptr, nullptr, st);
+  const cudaError_t e = cudaStreamSynchronize(st);
+  dfree(xu);
+  if (s) return s;
+  VES3D_CK(e);
+  return VES3D_OK;
+}
+
 int ves3d_sht_filter_coeffs(int p, int filter_freq, double exponent, double* coeff) {
   VES3D_ARG(coeff != nullptr, "coeff is null");
   VES3D_ARG(p >= 1 && p <= 128, "order must be in [1, 128]");

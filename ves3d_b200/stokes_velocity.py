@@ -313,6 +313,21 @@ class SHTrans:
         g, _ = self._nfun(grid, ngrid(self.p))
         check(lib().ves3d_sht_backward(c, n, self.p, self.p, g, None, None, self.stream), "SHTrans.backward")
 
+    def backward_d2(self, shc, uu=None, vv=None, uv=None):
+        """backward_d2u / d2v / duv: second derivatives (u latitude, v longitude) into the
+        given grid tensors (any of them None)."""
+        c, n = self._nfun(shc, ncoef(self.p))
+        outs = []
+        for t in (uu, vv, uv):
+            if t is None:
+                outs.append(None)
+            else:
+                g, m = self._nfun(t, ngrid(self.p))
+                if m != n:
+                    raise ValueError("output does not hold one grid function per coefficient vector")
+                outs.append(g)
+        check(lib().ves3d_sht_backward_d2(c, n, self.p, *outs, self.stream), "SHTrans.backward_d2")
+
     def ScaleFreq(self, shc_in, scale, shc_out):
         a, n = self._nfun(shc_in, ncoef(self.p))
         b, _ = self._nfun(shc_out, ncoef(self.p))
