@@ -85,6 +85,18 @@ int ves3d_sv_get_dl_matrix(ves3d_sv* sv, double* DL, int is_device);
 /* Velocity at the surface points, same layout (src/StokesVelocity.cc:164-539).
  * Builds the self matrices first if the surfaces changed. */
 int ves3d_sv_eval(ves3d_sv* sv, double* vel, int is_device);
+/* The self part's upsampling order (sh_order_up_self, src/StokesVelocity.cc:26-57): new
+ * operator tables, the self matrices rebuilt on next use. */
+int ves3d_sv_set_order_up(ves3d_sv* sv, int sh_order_up);
+int ves3d_sv_get_order_up(ves3d_sv* sv, int* sh_order_up);
+/* StokesVelocity::MonitorError(tol) (src/StokesVelocity.cc:553-685): evaluates the double
+ * layer of density 1 (single layer off), whose exact value is -1/2 on each surface and 0
+ * on the others; err3 (may be NULL) = {max|self + 1/2|, 0 (no near-singular correction in
+ * this build), max|far|}, *total (may be NULL) their sum. Moves the self upsampling order
+ * by 2 up when the self error is above tol, down below tol/2, as the reference; the far
+ * field is exact on the order-p grid and has no order to adapt. The densities set before
+ * are restored. */
+int ves3d_sv_monitor_error(ves3d_sv* sv, double tol, double* err3, double* total);
 /* Build the self matrices now (the reference builds them lazily inside operator()). */
 int ves3d_sv_setup(ves3d_sv* sv);
 /* Copy the self matrices out, [n_ves][3Ncoef][3Ncoef]. */

@@ -80,6 +80,12 @@ class StokesVelocity {
   void SetDensitySL(const Vec* force_single, bool add_repul = false) {
     SetDensitySL(&(*force_single)[0], add_repul);
   }
+  /* MonitorError(tol): the double layer of density 1 against -1/2; adapts the self order */
+  Real MonitorError(Real tol) {
+    double total = 0;
+    check(ves3d_sv_monitor_error(sv_, tol, 0, &total), "MonitorError");
+    return (Real)total;
+  }
   /* SetDensityDL(f): the double-layer density, NULL to turn the double layer off. */
   void SetDensityDL(const Real* f, bool on_device = false) {
     check(ves3d_sv_set_density_dl(sv_, f, on_device ? 1 : 0), "SetDensityDL");

@@ -38,6 +38,9 @@ int main(int argc, char** argv) {
     void (Sht::*d2[4])(const double*, long, double*) const = {&Sht::backward_d2u, &Sht::backward_d2v,
                                                                 &Sht::backward_duv, &Sht::SHC2Pole};
     (void)d2;
+    typedef ves3d_b200::StokesVelocity<double> Sv;
+    double (Sv::*monitor)(double) = &Sv::MonitorError;
+    (void)monitor;
     std::printf("%d\n", ves3d_version());
     return 0;
   }

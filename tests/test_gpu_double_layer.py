@@ -156,3 +156,35 @@ def test_double_layer_against_the_reference_fixture():
         _, vfar = sv.parts()
     assert rel_err(vfar, gdl["far_dl"]) < TOL
     assert n == DL.shape[1] and vel.size == gdl["X"].size
+
+
+def test_monitor_error_lowers_the_order_on_a_sphere():
+    """MonitorError on one sphere: the double layer of density 1 is -1/2 to rounding, so the
+    self order drops by 2 (error below tol/2); the single-layer density set before survives,
+    and the operator at the new order matches the oracle at that order."""
+    from tests.helpers import unit_sphere
+    p = 12
+    X = unit_sphere(p)
+    f = np.random.default_rng(3).standard_normal(X.size)
+    with StokesVelocity(p) as sv:
+        sv.SetSrcCoord(X)
+        sv.SetDensitySL(f)
+        v0 = sv()
+        total, err = sv.MonitorError(1e-6)
+        assert err[0] < 1e-10 and err[1] == 0.0 and err[2] == 0.0 and total == err[0]
+        assert sv.sh_order_up == 2 * p - 2
+        v1 = sv()
+    assert rel_err(v0, stokes.stokes_velocity_sl(X, f, p, 2 * p)) < TOL
+    assert rel_err(v1, stokes.stokes_velocity_sl(X, f, p, 2 * p - 2)) < TOL
+
+
+def test_monitor_error_raises_the_order_above_tol():
+    """On eight non-spherical vesicles at p = 8 the self error exceeds a tiny tol, so the
+    order rises by 2; the far part of constant densities vanishes to the quadrature error."""
+    p = 8
+    X, _ = small_suspension(2, p, 3)
+    with StokesVelocity(p) as sv:
+        sv.SetSrcCoord(X)
+        total, err = sv.MonitorError(1e-14)
+        assert sv.sh_order_up == 2 * p + 2
+        assert err[0] > 1e-14 and err[2] < 5e-3 and abs(total - err[0] - err[2]) < 1e-15

@@ -34,6 +34,9 @@ SIGNATURES = [
     ("ves3d_sv_set_density_sl", _i, [_vp, _vp, _i]),
     ("ves3d_sv_set_density_dl", _i, [_vp, _vp, _i]),
     ("ves3d_sv_get_dl_matrix", _i, [_vp, _vp, _i]),
+    ("ves3d_sv_set_order_up", _i, [_vp, _i]),
+    ("ves3d_sv_get_order_up", _i, [_vp, ctypes.POINTER(_i)]),
+    ("ves3d_sv_monitor_error", _i, [_vp, _d, _vp, ctypes.POINTER(_d)]),
     ("ves3d_sv_eval", _i, [_vp, _vp, _i]),
     ("ves3d_sv_setup", _i, [_vp]),
     ("ves3d_sv_get_self_matrix", _i, [_vp, _vp, _i]),

@@ -759,6 +759,97 @@ int ves3d_sv_get_dl_matrix(ves3d_sv* sv, double* DL, int is_device) {
   return copy_out(DL, sv->DL, (size_t)sv->nves * n * n, is_device, sv->stream);
 }
 
+int ves3d_sv_set_order_up(ves3d_sv* sv, int sh_order_up) {
+  int s = check_sv(sv);
+  if (s) return s;
+  VES3D_ARG(sh_order_up >= sv->p && sh_order_up <= 128, "sh_order_up must be in [sh_order, 128]");
+  if (sh_order_up == sv->pup) return VES3D_OK;
+  std::unique_ptr<TablesOwner> t(new TablesOwner());
+  build_tables(sv->p, sh_order_up, t->h);
+  if ((s = t->upload(sv->stream))) return s;
+  VES3D_CK(cudaDeviceSynchronize());  // nothing queued still reads the old tables
+  sv->tab = std::move(t);
+  sv->pup = sh_order_up;
+  sv->sl_valid = sv->dl_valid = false;  // self matrices of the new order on next use
+  sv->parts_valid = false;
+  sv->pc_valid = false;
+  sv->free_scratch();  // its size depends on the order
+  sv->drop_graph();
+  return VES3D_OK;
+}
+
+int ves3d_sv_monitor_error(ves3d_sv* sv, double tol, double* err3, double* total) {
+  int s = check_sv(sv);
+  if (s) return s;
+  VES3D_ARG(std::isfinite(tol) && tol > 0.0, "tol must be positive");
+  if (!sv->have_src) {
+    set_error("monitor_error before set_src_coord");
+    return VES3D_ERR_STATE;
+  }
+  NvtxRange nvtx("ves3d monitor");
+  const size_t n = (size_t)sv->npts() * 3;
+  if ((s = alloc_dl(sv))) return s;
+  // save the densities (src/StokesVelocity.cc:556-562)
+  const bool had_den = sv->have_den, had_dl = sv->have_dl;
+  std::vector<double> keepF, keepG;
+  if (had_den) {
+    keepF.resize(n);
+    if ((s = copy_out(keepF.data(), sv->F, n, 0, sv->stream))) return s;
+  }
+  if (had_dl) {
+    keepG.resize(n);
+    if ((s = copy_out(keepG.data(), sv->G, n, 0, sv->stream))) return s;
+  }
+  // no single layer, double-layer density 1 (:564-578)
+  const std::vector<double> ones(n, 1.0);
+  VES3D_CK(cudaMemsetAsync(sv->F, 0, n * sizeof(double), sv->stream));
+  if ((s = copy_in(sv->G, ones.data(), n, 0, sv->stream))) return s;
+  sv->have_den = sv->have_dl = true;
+  s = run_eval(sv, true);
+  std::vector<double> vs(n), vf(n);
+  if (!s) s = copy_out(vs.data(), sv->Vself, n, 0, sv->stream);
+  if (!s) s = copy_out(vf.data(), sv->Vfar, n, 0, sv->stream);
+  // restore (:627-633)
+  int r = VES3D_OK;
+  if (had_den) r = copy_in(sv->F, keepF.data(), n, 0, sv->stream);
+  if (!r && had_dl) r = copy_in(sv->G, keepG.data(), n, 0, sv->stream);
+  if (!r) r = cuda_status(cudaStreamSynchronize(sv->stream), "restore densities", __FILE__, __LINE__);
+  sv->have_den = had_den;
+  sv->have_dl = had_dl;
+  sv->parts_valid = false;
+  if (s) return s;
+  if (r) return r;
+  // error norms (:615-622): the self part against -1/2, the far part against 0; this build
+  // has no near-singular correction (its norm is 0)
+  double e0 = 0.0, e2 = 0.0;
+  for (size_t i = 0; i < n; i++) {
+    e0 = std::max(e0, std::fabs(vs[i] + 0.5));
+    e2 = std::max(e2, std::fabs(vf[i]));
+  }
+  // the self order follows the error (:636-645); the far field here is exact on the order-p
+  // grid and has no order of its own
+  int pup = sv->pup;
+  if (e0 > tol)
+    pup += 2;
+  else if (e0 < 0.5 * tol)
+    pup -= 2;
+  pup = std::max(sv->p, std::min(pup, 128));
+  if (pup != sv->pup && (s = ves3d_sv_set_order_up(sv, pup))) return s;
+  if (err3) {
+    err3[0] = e0;
+    err3[1] = 0.0;
+    err3[2] = e2;
+  }
+  if (total) *total = e0 + e2;
+  return VES3D_OK;
+}
+
+int ves3d_sv_get_order_up(ves3d_sv* sv, int* sh_order_up) {
+  VES3D_ARG(sv != nullptr && sh_order_up != nullptr, "null argument");
+  *sh_order_up = sv->pup;
+  return VES3D_OK;
+}
+
 int ves3d_sv_setup(ves3d_sv* sv) {
   int s = check_sv(sv);
   if (s) return s;

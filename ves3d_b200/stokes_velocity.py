@@ -44,7 +44,8 @@ def ncoef(p):
 
 
 class StokesVelocity:
-    """Single-layer Stokes velocity of a suspension of vesicles at their own surface points."""
+    """Stokes velocity (single layer, and double layer when a density is set) of a suspension
+    of vesicles at their own surface points."""
 
     def __init__(self, sh_order, sh_order_up=-1, precision="fp64", device=-1):
         prec = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}[precision]
@@ -122,6 +123,25 @@ class StokesVelocity:
         out = np.empty((self.n_ves, n, n))
         check(lib().ves3d_sv_get_self_matrix(self._h, out.ctypes.data, 0), "self_matrix")
         return out
+
+    def set_order_up(self, sh_order_up):
+        """The self part's upsampling order; the self matrices are rebuilt on next use."""
+        check(lib().ves3d_sv_set_order_up(self._h, int(sh_order_up)), "set_order_up")
+        self._sync_order()
+
+    def _sync_order(self):
+        o = ctypes.c_int()
+        check(lib().ves3d_sv_get_order_up(self._h, ctypes.byref(o)), "get_order_up")
+        self.sh_order_up = o.value
+
+    def MonitorError(self, tol):
+        """StokesVelocity::MonitorError: the double layer of density 1 against its exact value;
+        returns (total, [self, near (0), far]) and adapts the self upsampling order."""
+        err = np.zeros(3)
+        tot = ctypes.c_double()
+        check(lib().ves3d_sv_monitor_error(self._h, float(tol), err.ctypes.data, ctypes.byref(tot)), "MonitorError")
+        self._sync_order()
+        return tot.value, err
 
     def dl_matrix(self):
         """The double-layer self matrices [n_ves][3 Ncoef][3 Ncoef] (a double-layer density
