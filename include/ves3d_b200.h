@@ -85,6 +85,15 @@ int ves3d_sv_get_dl_matrix(ves3d_sv* sv, double* DL, int is_device);
 /* Velocity at the surface points, same layout (src/StokesVelocity.cc:164-539).
  * Builds the self matrices first if the surfaces changed. */
 int ves3d_sv_eval(ves3d_sv* sv, double* vel, int is_device);
+/* StokesVelocity::SetTrgCoord(T) (src/StokesVelocity.cc:146-161): off-surface targets,
+ * point-major [n_trg][3]; NULL (or n_trg = 0) returns to the surface points. Kept across
+ * ves3d_sv_set_src_coord. */
+int ves3d_sv_set_trg_coord(ves3d_sv* sv, const double* T, long n_trg, int is_device);
+/* Velocity at the targets, point-major [n_trg][3]: the smooth quadrature over every surface
+ * point (FP64) of the single layer and, when set, the double layer. The reference corrects
+ * targets near a surface with its NearSingular module, which this build does not have:
+ * the result is accurate only away from the surfaces (a few grid spacings). */
+int ves3d_sv_eval_trg(ves3d_sv* sv, double* vel, int is_device);
 /* The self part's upsampling order (sh_order_up_self, src/StokesVelocity.cc:26-57): new
  * operator tables, the self matrices rebuilt on next use. */
 int ves3d_sv_set_order_up(ves3d_sv* sv, int sh_order_up);

@@ -80,6 +80,12 @@ class StokesVelocity {
   void SetDensitySL(const Vec* force_single, bool add_repul = false) {
     SetDensitySL(&(*force_single)[0], add_repul);
   }
+  /* SetTrgCoord(T): off-surface targets [n][3] (NULL: the surface); EvalTrg: their velocities
+   * (accurate away from the surfaces) */
+  void SetTrgCoord(const Real* T, long n_trg, bool on_device = false) {
+    check(ves3d_sv_set_trg_coord(sv_, T, n_trg, on_device ? 1 : 0), "SetTrgCoord");
+  }
+  void EvalTrg(Real* vel, bool on_device = false) { check(ves3d_sv_eval_trg(sv_, vel, on_device ? 1 : 0), "EvalTrg"); }
   /* MonitorError(tol): the double layer of density 1 against -1/2; adapts the self order */
   Real MonitorError(Real tol) {
     double total = 0;

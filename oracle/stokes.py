@@ -170,6 +170,29 @@ def stokes_velocity_dl(X, g, p, p_up=None, DL=None):
     return sh.self_apply(DL, g, p) + far_dl_velocity(X, g, p)
 
 
+def target_velocity(X, f, p, T, g=None):
+    """Velocity at off-surface targets T ([M][3], point-major, as SetTrgCoord,
+    src/StokesVelocity.cc:146-161) by the smooth quadrature over every surface point: the
+    single layer of f * area * qw (DirectStokesKernel over all points as one surface) plus,
+    with g, the double layer of g * area * qw (DirectStokesDoubleLayerKernel). No
+    near-singular correction: accurate away from the surfaces. Returns [M][3]."""
+    ng = sh.ngrid(p)
+    nv = np.asarray(X).size // (3 * ng)
+    N = nv * ng
+    T = np.asarray(T, np.float64).reshape(-1, 3)
+    M = T.shape[0]
+
+    def whole(A):
+        return np.ascontiguousarray(np.asarray(A).reshape(nv, 3, ng).transpose(1, 0, 2).reshape(-1))
+
+    Tw = np.ascontiguousarray(T.T.reshape(-1))
+    u = direct_stokes(N, M, 1, 0, M, np.ones(N), Tw, whole(X), whole(far_density(X, f, p)))
+    if g is not None:
+        u = u + direct_stokes_dl(N, M, 1, 0, M, None, Tw, whole(X), whole(unit_normal(X, p)),
+                                 whole(far_density(X, g, p)))
+    return u.reshape(3, M).T.reshape(-1)
+
+
 def stokes_velocity_poly(X, f, orders):
     """FP64 velocity of a polydisperse suspension (per-vesicle AxisMajor blocks concatenated;
     each vesicle's self part at its own order, p_up = 2p)."""

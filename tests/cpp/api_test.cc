@@ -40,7 +40,11 @@ int main(int argc, char** argv) {
     (void)d2;
     typedef ves3d_b200::StokesVelocity<double> Sv;
     double (Sv::*monitor)(double) = &Sv::MonitorError;
+    void (Sv::*set_trg)(const double*, long, bool) = &Sv::SetTrgCoord;
+    void (Sv::*eval_trg)(double*, bool) = &Sv::EvalTrg;
     (void)monitor;
+    (void)set_trg;
+    (void)eval_trg;
     std::printf("%d\n", ves3d_version());
     return 0;
   }

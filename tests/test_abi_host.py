@@ -73,6 +73,11 @@ def test_argument_errors_of_the_implicit_and_filter_entry_points():
     assert L.ves3d_sht_backward_d2(out.ctypes.data, 1, 0, out.ctypes.data, None, None, None) == 1
     assert L.ves3d_sht_scale_freq(None, 1, 16, None, None, None) == 1
     assert L.ves3d_sht_lowpass(out.ctypes.data, -1, 16, -1, 0.0, out.ctypes.data, None) == 1
+    # targets, self order and monitor
+    assert L.ves3d_sv_set_trg_coord(None, None, 0, 0) == 1
+    assert L.ves3d_sv_eval_trg(None, None, 0) == 1
+    assert L.ves3d_sv_set_order_up(None, 24) == 1
+    assert L.ves3d_sv_monitor_error(None, 1e-6, None, None) == 1
     # double layer and viscosity contrast
     assert L.ves3d_sv_set_viscosity_contrast(None, None, 0) == 1
     assert L.ves3d_sv_set_density_dl(None, None, 0) == 1

@@ -256,3 +256,23 @@ def test_reference_double_layer_kernel_sign(ref):
     u = ref.direct_stokes_dl(ng, ng, 1, 0, 1, None, T, X, n, den)
     assert abs(u[0] + 1) < 1e-12 and abs(u[ng] + 1) < 1e-12 and abs(u[2 * ng] + 1) < 1e-12
     assert rel_err(stokes.direct_stokes_dl(ng, ng, 1, 0, 1, None, T, X, n, den), u) < FAR_TOL
+
+
+def test_target_velocity_identities():
+    """Off-surface targets (SetTrgCoord) on a sphere of radius a = 2 with uniform density:
+    the single layer is (2/3) a f inside and, on the axis of f at distance r outside,
+    (a^2/r - a^4/(3 r^3)) f (the flow of the translating sphere it equals); the double layer
+    of a constant c is -c inside and 0 outside."""
+    p = 12
+    a = 2.0
+    X = a * unit_sphere(p)
+    f = np.zeros((3, sh.ngrid(p)))
+    f[0] = 1.0
+    T = np.array([[0.0, 0.0, 0.0], [0.3, -0.2, 0.1], [5.0, 0.0, 0.0]])
+    u = stokes.target_velocity(X, f.reshape(-1), p, T).reshape(-1, 3)
+    assert np.abs(u[:2, 0] - 2.0 * a / 3.0).max() < 1e-12 and np.abs(u[:2, 1:]).max() < 1e-12
+    assert abs(u[2, 0] - (a * a / 5.0 - a ** 4 / (3 * 125.0))) < 1e-9  # quadrature: 7.6e-11 here
+    c = np.array([0.3, -1.0, 0.5])
+    g = np.repeat(c[:, None], sh.ngrid(p), axis=1).reshape(-1)
+    v = stokes.target_velocity(X, np.zeros(X.size), p, T, g).reshape(-1, 3)
+    assert np.abs(v[:2] + c).max() < 1e-12 and np.abs(v[2]).max() < 1e-8

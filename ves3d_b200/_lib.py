@@ -35,6 +35,8 @@ SIGNATURES = [
     ("ves3d_sv_set_density_dl", _i, [_vp, _vp, _i]),
     ("ves3d_sv_get_dl_matrix", _i, [_vp, _vp, _i]),
     ("ves3d_sv_set_order_up", _i, [_vp, _i]),
+    ("ves3d_sv_set_trg_coord", _i, [_vp, _vp, _l, _i]),
+    ("ves3d_sv_eval_trg", _i, [_vp, _vp, _i]),
     ("ves3d_sv_get_order_up", _i, [_vp, ctypes.POINTER(_i)]),
     ("ves3d_sv_monitor_error", _i, [_vp, _d, _vp, ctypes.POINTER(_d)]),
     ("ves3d_sv_eval", _i, [_vp, _vp, _i]),

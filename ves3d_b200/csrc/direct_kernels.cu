@@ -209,6 +209,61 @@ int launch_direct_stokes_dl_f64(int src_m, int trg_m, int n, int t_head, int t_t
   return VES3D_OK;
 }
 
+// Velocity at M off-surface targets (point-major) from all N surface points (point-major):
+// the single layer of den and, with nrm, the double layer of unit normals nrm and densities
+// dden (both densities times area and weights). One target per thread, sources staged in
+// shared memory.
+__global__ void __launch_bounds__(kFarBS) k_targets_f64(const double* __restrict__ pos, const double* __restrict__ den,
+                                                        const double* __restrict__ nrm, const double* __restrict__ dden,
+                                                        long N, const double* __restrict__ trg, long M,
+                                                        double* __restrict__ out) {
+  __shared__ double sp[kFarBS * 3];
+  __shared__ double sd[kFarBS * 3];
+  __shared__ double sn[kFarBS * 3];
+  __shared__ double sg[kFarBS * 3];
+  const long m = (long)blockIdx.x * kFarBS + threadIdx.x;
+  const bool active = m < M;
+  const bool dl = nrm != nullptr;
+  double tx = 0, ty = 0, tz = 0;
+  if (active) {
+    tx = trg[3 * m];
+    ty = trg[3 * m + 1];
+    tz = trg[3 * m + 2];
+  }
+  PairAcc a, b;
+  for (long s0 = 0; s0 < N; s0 += kFarBS) {
+    const int ns = (int)min((long)kFarBS, N - s0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < 3 * ns; i += kFarBS) {
+      sp[i] = pos[3 * s0 + i];
+      sd[i] = den[3 * s0 + i];
+      if (dl) {
+        sn[i] = nrm[3 * s0 + i];
+        sg[i] = dden[3 * s0 + i];
+      }
+    }
+    __syncthreads();
+    if (!active) continue;
+    for (int k = 0; k < ns; k++) {
+      pair_f64(tx, ty, tz, sp[3 * k], sp[3 * k + 1], sp[3 * k + 2], sd[3 * k], sd[3 * k + 1], sd[3 * k + 2], false,
+               a);
+      if (dl) pair_dl_f64(tx, ty, tz, sp + 3 * k, sn + 3 * k, sg + 3 * k, b);
+    }
+  }
+  if (!active) return;
+  out[3 * m] = a.x * kInv8Pi + (dl ? b.x * kDl : 0.0);
+  out[3 * m + 1] = a.y * kInv8Pi + (dl ? b.y * kDl : 0.0);
+  out[3 * m + 2] = a.z * kInv8Pi + (dl ? b.z * kDl : 0.0);
+}
+
+int launch_targets_f64(const double* pos, const double* den, const double* nrm, const double* dden, long N,
+                       const double* trg, long M, double* out, cudaStream_t st) {
+  if (M <= 0) return VES3D_OK;
+  k_targets_f64<<<(unsigned)((M + kFarBS - 1) / kFarBS), kFarBS, 0, st>>>(pos, den, nrm, dden, N, trg, M, out);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
 // Unit outward normals, point-major (src/StokesVelocity.cc:245-275).
 __global__ void k_unit_normals(const double* __restrict__ Xt, const double* __restrict__ Xp, long nv, int p0,
                                double* __restrict__ nrm) {

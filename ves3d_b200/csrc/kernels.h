@@ -99,6 +99,11 @@ int launch_far_reduce(const double* part, int nseg, const long* off, long nves, 
 // set with scale kDl.
 int launch_far_dl(const double* pos, const double* nrm, const double* dden, const long* off, long nves, long N,
                   int max_nt, double* part, long part_cap_segments, cudaStream_t st, int* nseg_out);
+// Velocity at M off-surface targets (point-major [M][3]) from N surface points: single
+// layer of den, plus with nrm non-null the double layer of nrm and dden (all point-major,
+// densities times area and weights).
+int launch_targets_f64(const double* pos, const double* den, const double* nrm, const double* dden, long N,
+                       const double* trg, long M, double* out, cudaStream_t st);
 // Unit outward normals (X_theta x X_phi) / |X_theta x X_phi| of nv surfaces at order p0,
 // AxisMajor derivatives in, point-major [N][3] out.
 int launch_unit_normals(const double* Xt, const double* Xp, long nv, int p0, double* nrm, cudaStream_t st);

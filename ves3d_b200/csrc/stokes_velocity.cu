@@ -164,6 +164,9 @@ struct ves3d_sv {
   // per vesicle (one value: all), and on device vel_coeff = (1 + l)/2, dl_coeff = 1 - l
   std::vector<double> lam;
   bool contrast = false;
+  // off-surface targets (SetTrgCoord): point-major [trg_n][3] and their velocities
+  double *trg = nullptr, *vtrg = nullptr;
+  long trg_n = 0, trg_cap = 0;
   double *velc = nullptr, *dlc = nullptr;
   long contrast_nves = -1;  // vesicle count the device coefficients were made for
   long* off = nullptr;  // [nves+1] point offsets of the vesicles
@@ -212,6 +215,8 @@ struct ves3d_sv {
     dfree(filt);
     dfree(velc);
     dfree(dlc);
+    dfree(trg);
+    dfree(vtrg);
     drop_graph();
     free_precond();
     for (auto& e : pc_ev)
@@ -757,6 +762,50 @@ int ves3d_sv_get_dl_matrix(ves3d_sv* sv, double* DL, int is_device) {
   if (!sv->dl_valid && (s = run_setup(sv, true))) return s;
   const size_t n = 3 * (size_t)ncoef_(sv->p);
   return copy_out(DL, sv->DL, (size_t)sv->nves * n * n, is_device, sv->stream);
+}
+
+int ves3d_sv_set_trg_coord(ves3d_sv* sv, const double* T, long n_trg, int is_device) {
+  int s = check_sv(sv);
+  if (s) return s;
+  if (!T || n_trg == 0) {  // SetTrgCoord(NULL): the surface points again
+    sv->trg_n = 0;
+    return VES3D_OK;
+  }
+  VES3D_ARG(n_trg > 0, "n_trg < 0");
+  if (n_trg > sv->trg_cap) {
+    dfree(sv->trg);
+    dfree(sv->vtrg);
+    sv->trg = sv->vtrg = nullptr;
+    sv->trg_cap = 0;
+    if ((s = dalloc(&sv->trg, 3 * (size_t)n_trg)) || (s = dalloc(&sv->vtrg, 3 * (size_t)n_trg))) return s;
+    sv->trg_cap = n_trg;
+  }
+  if ((s = copy_in(sv->trg, T, 3 * (size_t)n_trg, is_device, sv->stream))) return s;
+  sv->trg_n = n_trg;
+  return VES3D_OK;
+}
+
+int ves3d_sv_eval_trg(ves3d_sv* sv, double* vel, int is_device) {
+  int s = check_sv(sv);
+  if (s) return s;
+  VES3D_ARG(vel != nullptr, "vel is null");
+  if (!sv->have_src || !sv->have_den || sv->trg_n <= 0) {
+    set_error("eval_trg needs surfaces, a single-layer density and targets");
+    return VES3D_ERR_STATE;
+  }
+  NvtxRange nvtx("ves3d targets");
+  const DevTables& T = sv->tab->d;
+  cudaStream_t st = sv->stream;
+  if ((s = launch_far_density(sv->F, sv->area, sv->nves, sv->p, T.smooth_w0, sv->den, st))) return s;
+  const double *nrm = nullptr, *dden = nullptr;
+  if (sv->have_dl) {
+    if ((s = launch_unit_normals(sv->Xt, sv->Xp, sv->nves, sv->p, sv->nrm, st))) return s;
+    if ((s = launch_far_density(sv->G, sv->area, sv->nves, sv->p, T.smooth_w0, sv->dden, st))) return s;
+    nrm = sv->nrm;
+    dden = sv->dden;
+  }
+  if ((s = launch_targets_f64(sv->pos, sv->den, nrm, dden, sv->npts(), sv->trg, sv->trg_n, sv->vtrg, st))) return s;
+  return copy_out(vel, sv->vtrg, 3 * (size_t)sv->trg_n, is_device, st);
 }
 
 int ves3d_sv_set_order_up(ves3d_sv* sv, int sh_order_up) {

@@ -124,6 +124,27 @@ class StokesVelocity:
         check(lib().ves3d_sv_get_self_matrix(self._h, out.ctypes.data, 0), "self_matrix")
         return out
 
+    def SetTrgCoord(self, T):
+        """Off-surface targets, [M][3] (numpy or CUDA tensor), or None for the surface points.
+        eval_targets() returns their velocities (accurate away from the surfaces: no
+        near-singular correction)."""
+        if T is None:
+            check(lib().ves3d_sv_set_trg_coord(self._h, None, 0, 0), "SetTrgCoord")
+            self.n_trg = 0
+            return
+        p, dev, n = _ptr(T)
+        if n % 3:
+            raise ValueError("targets must be [M][3]")
+        check(lib().ves3d_sv_set_trg_coord(self._h, p, n // 3, dev), "SetTrgCoord")
+        self.n_trg = n // 3
+
+    def eval_targets(self, out=None):
+        if out is None:
+            out = np.empty(3 * getattr(self, "n_trg", 0))
+        p, dev, n = _ptr(out)
+        check(lib().ves3d_sv_eval_trg(self._h, p, dev), "eval_targets")
+        return out
+
     def set_order_up(self, sh_order_up):
         """The self part's upsampling order; the self matrices are rebuilt on next use."""
         check(lib().ves3d_sv_set_order_up(self._h, int(sh_order_up)), "set_order_up")
