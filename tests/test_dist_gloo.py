@@ -2,6 +2,7 @@
 import os
 import socket
 
+import numpy as np
 import pytest
 import torch.multiprocessing as mp
 
@@ -26,6 +27,44 @@ def _worker(rank, world, port, q):
     dist.barrier()
     dist.destroy_process_group()
     q.put((rank, tmax, seed))
+
+
+def _vtk_worker(rank, world, port, base, q):
+    import datetime
+    import numpy as np
+    import torch.distributed as dist
+    from ves3d_b200 import vtk
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    p1, nv = 3, rank + 1  # each rank writes its own vesicles
+    X1 = np.full(nv * 3 * 2 * p1 * (p1 + 1), float(rank))
+    vtk.write_grid(X1, np.zeros(nv * 6), p1, base)  # rank and size from the process group
+    dist.barrier()
+    dist.destroy_process_group()
+    q.put(rank)
+
+
+@pytest.mark.timeout(120)
+def test_vtk_output_from_two_ranks(tmp_path):
+    """Each rank writes its piece <base>_<rank>.vtp; rank 0 writes the index naming both."""
+    from ves3d_b200 import vtk
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    base = str(tmp_path / "frame")
+    procs = [ctx.Process(target=_vtk_worker, args=(r, 2, port, base, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    assert sorted(q.get(timeout=90) for _ in procs) == [0, 1]
+    for p in procs:
+        p.join(timeout=30)
+        assert p.exitcode == 0
+    assert vtk.read_pvtp(base + ".pvtp") == ["frame_000000.vtp", "frame_000001.vtp"]
+    for r in range(2):
+        d = vtk.read_vtp(base + "_%06d.vtp" % r)
+        npt = 2 * 3 * 4 + 2
+        assert d["points"].shape == ((r + 1) * npt, 3)
+        assert np.all(d["points"][: 2 * 3 * 4] == float(r))
 
 
 @pytest.mark.timeout(120)

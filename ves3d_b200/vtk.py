@@ -49,9 +49,11 @@ def WriteVTK(S, p0, p1, fname, period=0.0, v=None, rank=None, n_ranks=None):
           "WriteVTK")
 
 
-def write_grid(X1, Xp, p1, fname, V1=None, Vp=None, period=0.0, rank=0, n_ranks=1):
+def write_grid(X1, Xp, p1, fname, V1=None, Vp=None, period=0.0, rank=None, n_ranks=None):
     """The writer alone on host arrays (no GPU): X1 (and V1) [n_ves][3][(p1+1) 2p1] grid values
-    of order p1, Xp (and Vp) [n_ves][3][2] pole values (x = -1, then x = +1)."""
+    of order p1, Xp (and Vp) [n_ves][3][2] pole values (x = -1, then x = +1); rank and size
+    as WriteVTK's."""
+    rank, n_ranks = _rank_size(rank, n_ranks)
     X1 = np.ascontiguousarray(X1, dtype=np.float64)
     Xp = np.ascontiguousarray(Xp, dtype=np.float64)
     ng = 2 * p1 * (p1 + 1)
