@@ -31,6 +31,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from ves3d_b200 import dist as vd  # noqa: E402  (torch-free helpers: ranks, max over ranks)
+
 WORKLOAD = "c2_512ves_p16"
 FLOPS_PER_PAIR = 28  # the reference's own count for the Stokeslet pair (src/CPUKernels.cc:1007)
 
@@ -50,15 +52,14 @@ def parse():
     ap.add_argument("--no-sed", action="store_true", help="skip the sedimentation (implicit polydisperse) measurement")
     ap.add_argument("--sed-steps", type=int, default=3)
     ap.add_argument("--no-alt", action="store_true", help="skip the measurement of the other precision form")
+    ap.add_argument("--no-dl", action="store_true", help="skip the double-layer measurement")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default far-field launch shape")
     return ap.parse_args()
 
 
 def dist_setup():
     import torch
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world, rank, local = vd.env_world()
     if world > 1:
         import datetime
         import torch.distributed as dist
@@ -70,20 +71,28 @@ def dist_setup():
     return world, rank, local
 
 
-def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
-
-
 def max_over_ranks(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return vd.max_over_ranks(x, world, device="cuda")
+
+
+_peak_lib = None
+
+
+def fma_peak(fp64):
+    """Measured FMA throughput (TFLOP/s) of this GPU's CUDA cores, from the benchmark's
+    own probe library (ves3d_b200/libves3d_peak.so, not part of the product)."""
+    global _peak_lib
+    import ctypes
+    if _peak_lib is None:
+        from ves3d_b200 import build as vbuild
+        _peak_lib = ctypes.CDLL(vbuild.PEAK_LIB)
+        _peak_lib.ves3d_bench_fma_peak.restype = ctypes.c_int
+        _peak_lib.ves3d_bench_fma_peak.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    t = ctypes.c_double(0)
+    rc = _peak_lib.ves3d_bench_fma_peak(1 if fp64 else 0, ctypes.byref(t))
+    if rc:
+        raise RuntimeError(f"FMA peak probe failed (CUDA error {rc})")
+    return t.value
 
 
 class ClockSampler:
@@ -222,10 +231,12 @@ def cpu_reference_rate(X, f, p, budget_s=20.0):
             break
         per_thread = int(per_thread * min(16.0, max(2.0, 8.0 / max(t4 - t3, 1e-3))))
     total = t_build + t_apply + t_far
+    wall = time.perf_counter() - t0
     sample = (f"self part on {ns} of {nves} vesicles (build {t1 - t0:.2f}s, apply {t2 - t1:.3f}s), all-pairs far "
               f"field on {nt} of {N} targets ({t4 - t3:.2f}s); each extrapolated linearly to the full evaluation")
     return {"value": N / total, "unit": "points/s", "cores": cores, "kind": kind, "sample": sample,
-            "seconds_per_eval": total, "parts_s": {"self_build": t_build, "self_apply": t_apply, "far": t_far}}
+            "seconds_per_eval": total, "sampled_wall_s": wall,
+            "parts_s": {"self_build": t_build, "self_apply": t_apply, "far": t_far}}
 
 
 def run_reference(args, world, rank):
@@ -235,12 +246,13 @@ def run_reference(args, world, rank):
     X, f, p = workloads.make(args.workload)
     ng = 2 * p * (p + 1)
     N = X.size // 3
-    vals = []
+    vals, walls = [], []
     res = None
     for i in range(args.warmup + args.steps):
         res = cpu_reference_rate(X, f, p)
         if i >= args.warmup:
             vals.append(res["value"])
+            walls.append(res["sampled_wall_s"])
     value = statistics.median(vals) if vals else res["value"]
     line = {
         "impl": "reference", "metric": "vesicle-point velocity evaluations/s", "value": value, "unit": "points/s",
@@ -253,6 +265,13 @@ def run_reference(args, world, rank):
                          "sample": res["sample"]},
         "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "parts_s": res["parts_s"],
+        # each step is a bounded sample of one evaluation, extrapolated linearly to the
+        # whole of it: ms_per_step is the extrapolated time of one full evaluation, not the
+        # wall time of a step, and no full evaluation is run
+        "extrapolated": True,
+        "full_evaluations_run": 0,
+        "sampled_wall_s_per_step": statistics.mean(walls) if walls else res["sampled_wall_s"],
+        "sampled_wall_s_total": sum(walls),
     }
     print(json.dumps(line), flush=True)
 
@@ -293,10 +312,13 @@ IMPLICIT = dict(workload="c4_256ves_p16", dt=0.01, kappa=0.05, shear_rate=1.0, t
 #   fast : mixed precision, per-vesicle self-block preconditioner rebuilt every 10 steps
 #          (lagged: built at step 1, reused at step 2), learned guess combined with the
 #          previous solution by the true residual
+#   the same fast form without the learned guess (previous solution only) is the ablation
+#   that shows what the network adds
 IMPLICIT_FORMS = [
     # (label, precision, preconditioner, guess policy, preconditioner refresh interval)
     ("plain_fp64", "fp64", "none", "previous", 1),
     ("fp64_self_block", "fp64", "self_block", "previous", 1),
+    ("mixed_self_block_previous", "mixed", "self_block", "previous", 10),
     ("mixed_self_block_learned", "mixed", "self_block", "learned+previous", 10),
 ]
 
@@ -424,30 +446,34 @@ def polydisperse_measurement(precision, local, stream):
     graph_ms = g0.elapsed_time(g1)
     shapes = {k: v for k, v in _lib.autotune_report().items() if f":N={N}:" in k}
     sv.close()
-    # sampled error: two vesicles of order <= 16, all their points
+    # sampled error: one vesicle of every order (p = 24 included), all their points
     ng = np.array([2 * p * (p + 1) for p in orders])
     off = np.concatenate([[0], np.cumsum(ng)])
     rng = np.random.default_rng(5)
-    cand = np.nonzero(orders <= 16)[0]
+    sample_v = [int(rng.choice(np.nonzero(orders == q)[0])) for q in np.unique(orders)]
     D = np.empty_like(f)
     for v, p in enumerate(orders):
         a, b = 3 * off[v], 3 * off[v + 1]
         D[a:b] = stokes.far_density(X[a:b], f[a:b], int(p))
     worst = 0.0
     scale = np.abs(vel).max()
-    for v in rng.choice(cand, size=2, replace=False):
+    per_order = {}
+    for v in sample_v:
         p = int(orders[v])
         a, b = 3 * off[v], 3 * off[v + 1]
         SL = sh.stokes_singular_matrix(X[a:b], p, 2 * p)
         ref = sh.self_apply(SL, f[a:b], p) + stokes.far(X, D, off, np.arange(off[v], off[v + 1])).T.reshape(-1)
-        worst = max(worst, float(np.abs(vel[a:b] - ref).max() / scale))
+        e = float(np.abs(vel[a:b] - ref).max() / scale)
+        per_order[p] = e
+        worst = max(worst, e)
     counts = {int(p): int((orders == p).sum()) for p in np.unique(orders)}
     return {"workload": f"c3_4096ves_poly: 4096 vesicles, p counts {counts}, {N} points, 20% volume fraction",
             "ms_per_eval": ms, "points_per_s": N / (ms * 1e-3), "stages_ms": st,
             "graph_eval": {"ms": graph_ms, "points_per_s": N / (graph_ms * 1e-3),
                            "what": "captured evaluation (self parts + far field) relaunched on new densities, "
                                    "surfaces and self matrices unchanged", "far_launch_shapes": shapes},
-            "error_vs_fp64_oracle": {"max_rel": worst, "sample": "all points of 2 vesicles with p <= 16"}}
+            "error_vs_fp64_oracle": {"max_rel": worst, "per_order": per_order,
+                                     "sample": "all points of one vesicle of every order (8, 12, 16, 24)"}}
 
 
 SEDIMENTATION = dict(workload="c5_2048ves_sed", dt=0.01, kappa=0.05, excess_density=1.0, gravity=(0.0, 0.0, -1.0),
@@ -538,7 +564,7 @@ def _vesicle_spans(orders):
         o += n
 
 
-def alt_precision_measurement(precision, X, f, p, local, stream, steps, warmup):
+def alt_precision_measurement(precision, X, f, p, local, stream, steps, warmup, e2e_steps):
     """The same C2 evaluation in the other precision form (device time per step, L2
     flushed between steps), its far-field roofline fraction and its error against the
     FP64 oracle on the sampled points."""
@@ -577,13 +603,32 @@ def alt_precision_measurement(precision, X, f, p, local, stream, steps, warmup):
         setup_ms.append(st["setup_ms"])
         apply_ms.append(st["self_apply_ms"])
     vel = out.cpu().numpy()
+    # end to end through the public API from pinned host buffers, as for the headline form
+    hX = torch.from_numpy(X).pin_memory().numpy()
+    hF = torch.from_numpy(f).pin_memory().numpy()
+    hV = torch.empty(X.size, dtype=torch.float64).pin_memory().numpy()
+    e2e_ms = []
+    for _ in range(e2e_steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sv.SetSrcCoord(hX)
+        sv.SetDensitySL(hF)
+        sv(hV)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms.append(e0.elapsed_time(e1))
     sv.close()
     ms = statistics.mean(times)
     far_avg = statistics.mean(far_ms)
     achieved = FLOPS_PER_PAIR * far_pairs(nves, ng) / (far_avg * 1e-3) / 1e12
-    peak = _lib.measure_fma_peak(precision == "fp64")
+    peak = fma_peak(precision == "fp64")
     return {"precision": precision, "dtype": "f64" if precision == "fp64" else "f32+f64",
             "value": N / (ms * 1e-3), "unit": "points/s", "ms_per_step": ms, "steps": steps,
+            "e2e": {"value": N * len(e2e_ms) / (sum(e2e_ms) * 1e-3) if e2e_ms else None, "unit": "points/s",
+                    "h2d_bytes_per_step": int(2 * X.nbytes), "d2h_bytes_per_step": int(X.nbytes)},
             "stages_ms": {"self_build": statistics.mean(setup_ms), "self_apply": statistics.mean(apply_ms),
                           "far_field": far_avg},
             "far_roofline": {"kernel": "k_far_f64" if precision == "fp64" else "k_far_f32",
@@ -592,13 +637,62 @@ def alt_precision_measurement(precision, X, f, p, local, stream, steps, warmup):
                                      "sample": "2 vesicles: full velocity at 256 of their points"}}
 
 
+DL_FLOPS_PER_PAIR = 30  # r, |r|^2, 1/|r|, |r|^-5, two dots, their product, three FMAs
+
+
+def double_layer_measurement(X, f, p, local, stream, steps=3):
+    """The 512-vesicle evaluation with a double-layer density set as well (SetDensityDL):
+    device time of the far double layer's kernels (FP64 in both forms) against the FP64
+    FMA peak, and of the whole evaluation (single + double layer) in the FP64 form."""
+    import torch
+    from ves3d_b200.stokes_velocity import StokesVelocity
+    ng = 2 * p * (p + 1)
+    nves = X.size // (3 * ng)
+    N = nves * ng
+    g = np.random.default_rng(4242).standard_normal(X.size)
+    dev = torch.device("cuda", local)
+    sv = StokesVelocity(p, 2 * p, precision="fp64", device=local)
+    sv.set_stream(stream.cuda_stream)
+    out = torch.empty(X.size, dtype=torch.float64, device=dev)
+    sv.SetSrcCoord(X)
+    sv.SetDensitySL(f)
+    sv.SetDensityDL(g)
+    torch.cuda.synchronize()
+    b0 = time.perf_counter()
+    sv(out)  # builds the DL self matrices (stage by stage) on first use
+    torch.cuda.synchronize()
+    first_s = time.perf_counter() - b0
+    evals, far_dl = [], []
+    for _ in range(steps):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sv(out)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        evals.append(e0.elapsed_time(e1))
+        far_dl.append(sv.far_dl_ms())
+    sv.close()
+    pairs = far_pairs(nves, ng)
+    ms = statistics.mean(far_dl)
+    achieved = DL_FLOPS_PER_PAIR * pairs / (ms * 1e-3) / 1e12
+    peak = fma_peak(True)
+    return {"what": "512-vesicle p=16 evaluation with single- and double-layer densities, FP64; surfaces and "
+                    "self matrices built before the timed evaluations",
+            "eval_ms": statistics.mean(evals), "far_dl_ms": ms, "first_eval_with_dl_build_s": first_s,
+            "far_dl_roofline": {"kernel": "k_far_dl_f64_seg", "bound": "fp64_pipe", "achieved": achieved,
+                                "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                                "work": f"{DL_FLOPS_PER_PAIR} flops per (target, source) pair x {pairs} pairs"}}
+
+
 def run_ours(args, world, rank, local):
     import torch
     from ves3d_b200 import _lib, workloads
     from ves3d_b200.stokes_velocity import StokesVelocity
 
     cfg = dict(workloads.CONFIGS[args.workload])
-    cfg["seed"] = cfg["seed"] + 100 * rank  # every rank owns an independent suspension
+    cfg["seed"] = vd.rank_seed(cfg["seed"], rank)  # every rank owns an independent suspension
     p = cfg["p"]
     X, f = workloads.suspension(**cfg)
     ng = 2 * p * (p + 1)
@@ -623,12 +717,12 @@ def run_ours(args, world, rank, local):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
-    peak64 = _lib.measure_fma_peak(True)
-    peak32 = _lib.measure_fma_peak(False)
+    peak64 = fma_peak(True)
+    peak32 = fma_peak(False)
     times, setup_ms, far_ms, apply_ms = [], [], [], []
     launches0 = _lib.kernel_launches()
     flush_launches = 0
-    barrier(world)
+    vd.barrier(world)
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
@@ -647,12 +741,12 @@ def run_ours(args, world, rank, local):
             far_ms.append(st["far_ms"])
             apply_ms.append(st["self_apply_ms"])
     torch.cuda.synchronize()
-    barrier(world)
+    vd.barrier(world)
     launches = _lib.kernel_launches() - launches0
     total_ms = sum(times)
     total_ms_max = max_over_ranks(total_ms, world)
     ms_per_step = total_ms_max / args.steps
-    value = N * world * args.steps / (total_ms_max * 1e-3)
+    value = vd.aggregate_throughput(N * args.steps, total_ms_max * 1e-3, world)
 
     # end to end through the public API with pinned host buffers: H2D of X and f,
     # evaluation, D2H of the velocity, every step
@@ -673,7 +767,7 @@ def run_ours(args, world, rank, local):
         torch.cuda.synchronize()
         e2e_ms.append(e0.elapsed_time(e1))
     e2e_max = max_over_ranks(sum(e2e_ms), world) if e2e_ms else None
-    e2e_value = N * world * len(e2e_ms) / (e2e_max * 1e-3) if e2e_ms else None
+    e2e_value = vd.aggregate_throughput(N * len(e2e_ms), e2e_max * 1e-3, world) if e2e_ms else None
 
     result = None
     if rank == 0:
@@ -718,7 +812,7 @@ def run_ours(args, world, rank, local):
                 "peak": peak,
                 "unit": "TFLOP/s",
                 "frac": achieved / peak,
-                "peak_source": "measured on this GPU by ves3d_measure_fma_peak (FMA throughput probe)",
+                "peak_source": "measured on this GPU by the benchmark's FMA throughput probe (libves3d_peak.so)",
                 "work": f"{FLOPS_PER_PAIR} flops per (target, source) pair x {pairs} pairs per launch",
                 "traffic": load_traffic(f"far_{args.precision}_{args.workload}"),
             },
@@ -732,10 +826,17 @@ def run_ours(args, world, rank, local):
         if world == 1 and not args.no_alt:
             other = "mixed" if args.precision == "fp64" else "fp64"
             result[other] = alt_precision_measurement(other, X, f, p, local, stream, args.steps,
-                                                      min(args.warmup, 2))
+                                                      min(args.warmup, 2), args.e2e_steps)
+            # the plain FP64 form's figures at the top level, beside the headline (mixed),
+            # so that the FP64-against-FP64 comparison with the reference arm is visible
+            fp64 = result["fp64"] if other == "fp64" else result
+            result["value_fp64"] = fp64["value"]
+            result["e2e_fp64"] = fp64["e2e"]
         # the launch-shape autotuner tunes inside the first launch of a configuration: keep
         # it out of the single-evaluation measurements below (they run the default shape)
         _lib.set_autotune(False)
+        if world == 1 and not args.no_dl:
+            result["double_layer"] = double_layer_measurement(X, f, p, local, stream)
         if world == 1 and not args.no_implicit:
             result["implicit_step"] = implicit_step_measurement(local, stream)
         if world == 1 and not args.no_poly:

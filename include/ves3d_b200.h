@@ -117,6 +117,9 @@ int ves3d_sv_get_parts(ves3d_sv* sv, double* vel_self, double* vel_far, int is_d
  * ms[0] self-matrix build, ms[1] self apply, ms[2] far-field kernel, ms[3] whole eval
  * (everything after the build). */
 int ves3d_sv_stage_times(ves3d_sv* sv, float* ms);
+/* Device time in ms of the far double layer's kernels in the last evaluation with a
+ * double-layer density set (0 without one); a diagnostic of this library. */
+int ves3d_sv_far_dl_time(ves3d_sv* sv, float* ms);
 /* Device pointers of the context's resident buffers (for zero-copy callers):
  * which = 0 surfaces, 1 density, 2 velocity. Valid until the next set_src_coord. */
 int ves3d_sv_device_buffer(ves3d_sv* sv, int which, double** ptr, size_t* n_elems);
@@ -441,16 +444,19 @@ int ves3d_stokes_alltoall_device_f64(const double* src, const double* den, size_
                                      void* stream);
 
 /* All-to-all interaction that allocates nothing (no counterpart in the reference: it is
- * an addition of this library). For callers that cannot call cudaMalloc -- code running
- * while a stream is captured into a CUDA graph, or programs whose device memory is owned
- * by another allocator. Same HOST-pointer arguments and result as
- * ves3d_stokes_alltoall_f64, plus an optional stream (NULL = legacy default stream);
- * returns an int status and waits for its copies before returning. Inputs are staged
- * through one fixed device array of VES3D_NOALLOC_MAX_POINTS points (36 MiB, held by
- * every GPU that loads the library until exit); np above that is rejected with
- * VES3D_ERR_ARG. The first call on a device looks the array's address up
- * (cudaGetSymbolAddress) and should come before any stream capture. Calls share the
- * array: calls whose GPU work overlaps race. */
+ * an addition of this library). For programs whose device memory is owned by another
+ * allocator (a pool that has reserved the GPU already, or a framework that forbids
+ * cudaMalloc/cudaFree between time steps), which cannot let the library allocate. Same
+ * HOST-pointer arguments and result as ves3d_stokes_alltoall_f64, plus an optional
+ * stream (NULL = legacy default stream); returns an int status. The call is synchronous:
+ * it waits for its result on that stream before returning, so it cannot be recorded
+ * into a CUDA graph. Inputs are staged through one fixed device array of
+ * VES3D_NOALLOC_MAX_POINTS points (36 MiB, held by every GPU that loads the library
+ * until exit); np above that is rejected with VES3D_ERR_ARG. On any error pot (3 np
+ * doubles) is filled with NaN, as by the allocating call; np = 0 leaves it untouched.
+ * The array's device address is looked up on the first call on each device and kept, so
+ * the library does not survive cudaDeviceReset. Calls share the array: calls whose GPU
+ * work overlaps race. */
 #define VES3D_NOALLOC_MAX_POINTS 524288
 int ves3d_stokes_alltoall_noalloc_f64(const double* src, const double* den, size_t np, double* pot,
                                       void* stream);
@@ -482,9 +488,6 @@ int ves3d_vtk_write(const double* X, const double* V, long n_ves, int p0, int p1
  * "ana_four", "syn1_leg", "syn1_dleg", "syn1_four", "syn1_dfour", "qp".
  * ------------------------------------------------------------------------- */
 int ves3d_tables_export(int p0, int p1, const char* name, double* out, size_t cap, size_t* n);
-/* Measured FMA throughput of the current device's CUDA cores in TFLOP/s (2 flops per
- * FMA): fp64 != 0 for FP64, else FP32. The roofline denominator of the direct sums. */
-int ves3d_measure_fma_peak(int fp64, double* tflops);
 
 #ifdef __cplusplus
 }

@@ -23,11 +23,20 @@ def ellipsoid_pair(p):
     return np.concatenate([X, X + np.array([3.0, 0.3, -0.2])[:, None]]).reshape(-1)
 
 
-def dumbbell(reference_root="/root/reference"):
+def _reference_root():
+    """The reference tree, from VES3D_DIR (the variable the reference itself reads)."""
+    root = os.environ.get("VES3D_DIR")
+    if not root:
+        raise SystemExit("set VES3D_DIR to the reference source tree")
+    return root
+
+
+def dumbbell(reference_root=None):
     """The reference's dumbbell test surface (entry 0 of precomputed/shape_gallery_6.txt,
     AxisMajor [3][7][12] at p = 6) and SurfaceTest's known answers for it (area and volume,
     test/SurfaceTest.cc:72, :79; curvature, gradients and Laplacians, :91-116). The
     reference test compares magnitudes (MaxAbs)."""
+    reference_root = reference_root or _reference_root()
     vals = []
     with open(os.path.join(reference_root, "precomputed", "shape_gallery_6.txt")) as fh:
         started = False
@@ -62,7 +71,7 @@ def streamable(ref_stream=None):
     import subprocess
     ref_stream = ref_stream or os.path.join(os.path.dirname(os.path.dirname(HERE)), "oracle", "_ref", "ref_stream")
     out = os.path.join(HERE, "ref_stream_p4.txt")
-    subprocess.check_call([ref_stream, "pack", "4", "2", out], env=dict(os.environ, VES3D_DIR="/root/reference"))
+    subprocess.check_call([ref_stream, "pack", "4", "2", out], env=dict(os.environ, VES3D_DIR=_reference_root()))
 
 
 def double_layer():
@@ -98,10 +107,36 @@ def double_layer():
                         vel_self=vel_self, Xs=Xs, gs=gs, far_dl=allp - own)
 
 
+def noise_floor():
+    """The reference's own noise floor on the self part, and the p = 24 case: the self
+    velocity of the 8-vesicle p = 12 suspension and of one perturbed ellipsoid at p = 24
+    (p_up = 48) from the reference built twice, differing only in its GEMM loop order
+    (libves3d_ref.so with OpenBLAS, libves3d_ref_naive.so with plain loops). The two
+    reference builds disagree at the level of MatRotate's sqrt(1 - x^2) rounding at the
+    poles, which is the bar an independent restatement can meet against the reference."""
+    reflib.set_threads(os.cpu_count() or 1)
+    out = {}
+    X, f, p = workloads.make("c1_8ves_p12")
+    SL, _ = reflib.singular_matrices(X, p, 2 * p)
+    out["c1_vel_self"] = reflib.self_apply(SL, f, p)
+    out["c1_vel_self_naive"] = reflib.self_apply(reflib.naive_singular_matrices(X, p, 2 * p), f, p)
+    X24, f24 = workloads.suspension(1, 24, 3.0, semi_axes=(1.0, 1.0, 0.6), deg=4, amp=0.05, seed=2424)
+    SL, _ = reflib.singular_matrices(X24, 24, 48)
+    out["p24_X"], out["p24_f"] = X24, f24
+    out["p24_vel_self"] = reflib.self_apply(SL, f24, 24)
+    out["p24_vel_self_naive"] = reflib.self_apply(reflib.naive_singular_matrices(X24, 24, 48), f24, 24)
+    np.savez_compressed(os.path.join(HERE, "ref_noise_floor_p12_p24.npz"), **out)
+
+
 def main():
+    import sys
+    if "--noise-floor" in sys.argv:  # the newest fixture alone
+        noise_floor()
+        return
     dumbbell()
     streamable()
     double_layer()
+    noise_floor()
     assert reflib.available(), "build oracle/_ref first (make -C oracle/ref)"
     reflib.set_threads(os.cpu_count() or 1)
     # p = 6: two ellipsoids; quadrature rules, transforms, the self matrix of vesicle 0

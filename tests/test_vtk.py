@@ -247,3 +247,13 @@ def test_write_without_a_gpu_is_an_error_not_a_crash(tmp_path):
     assert st in (2, 5)
     assert not os.path.exists(tmp_path / "g_000000.vtp")
     assert ctypes.string_at(_lib.lib().ves3d_last_error())
+
+
+def test_rank_without_size_is_rejected():
+    """An explicit rank needs its communicator size and the other way round (a guessed
+    size would write the index from the wrong process or collide piece names)."""
+    with pytest.raises(ValueError):
+        vtk._rank_size(1, None)
+    with pytest.raises(ValueError):
+        vtk._rank_size(None, 2)
+    assert vtk._rank_size(1, 2) == (1, 2)

@@ -44,6 +44,7 @@ SIGNATURES = [
     ("ves3d_sv_get_self_matrix", _i, [_vp, _vp, _i]),
     ("ves3d_sv_get_parts", _i, [_vp, _vp, _vp, _i]),
     ("ves3d_sv_stage_times", _i, [_vp, ctypes.POINTER(ctypes.c_float)]),
+    ("ves3d_sv_far_dl_time", _i, [_vp, ctypes.POINTER(ctypes.c_float)]),
     ("ves3d_sv_device_buffer", _i, [_vp, _i, ctypes.POINTER(_vp), ctypes.POINTER(_sz)]),
     ("ves3d_sv_eval_resident", _i, [_vp]),
     ("ves3d_sv_capture_eval", _i, [_vp]),
@@ -72,7 +73,6 @@ SIGNATURES = [
     ("ves3d_interaction_free", None, [ctypes.POINTER(_vp)]),
     ("ves3d_stokes_alltoall_device_f64", _i, [_vp, _vp, _sz, _vp, _vp]),
     ("ves3d_tables_export", _i, [_i, _i, ctypes.c_char_p, _vp, _sz, ctypes.POINTER(_sz)]),
-    ("ves3d_measure_fma_peak", _i, [_i, ctypes.POINTER(_d)]),
     ("ves3d_stokes_alltoall_noalloc_f64", _i, [_vp, _vp, _sz, _vp, _vp]),
     ("ves3d_sv_set_implicit_params", _i, [_vp, _d, _d, _d]),
     ("ves3d_sv_set_gravity", _i, [_vp, _d, _d, _d, _d]),
@@ -148,12 +148,6 @@ def check(status, what=""):
 
 def kernel_launches():
     return int(lib().ves3d_kernel_launches())
-
-
-def measure_fma_peak(fp64=True):
-    t = _d(0)
-    check(lib().ves3d_measure_fma_peak(1 if fp64 else 0, ctypes.byref(t)), "measure_fma_peak")
-    return t.value
 
 
 def tables_export(p0, p1, name):

@@ -6,8 +6,11 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libves3d_b200.so")
+# the benchmark's FMA-throughput probe, a separate library (not part of the product)
+PEAK_LIB = os.path.join(HERE, "libves3d_peak.so")
+PEAK_SOURCE = "peak_probe.cu"
 SOURCES = ["sh_tables.cc", "sht_kernels.cu", "singular_kernels.cu", "direct_kernels.cu", "far_kernels.cu", "build_kernels.cu", "stokes_velocity.cu",
-           "peak_probe.cu", "noalloc.cu", "geometry_kernels.cu", "bicgstab.cu", "mlp.cu", "device_prims.cu",
+           "noalloc.cu", "geometry_kernels.cu", "bicgstab.cu", "mlp.cu", "device_prims.cu",
            "vtk_output.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared", "-Wno-deprecated-gpu-targets"]
@@ -31,9 +34,19 @@ def sources():
     return srcs, deps
 
 
+def _stale(out, deps):
+    return not os.path.exists(out) or os.path.getmtime(out) < max(os.path.getmtime(d) for d in deps)
+
+
 def build(force=False, verbose=False):
     srcs, deps = sources()
-    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(d) for d in deps):
+    peak_src = os.path.join(CSRC, PEAK_SOURCE)
+    if force or _stale(PEAK_LIB, [peak_src]):
+        cmd = [_nvcc()] + NVCC_FLAGS + ["-o", PEAK_LIB, peak_src]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.check_call(cmd, cwd=CSRC)
+    if not force and not _stale(LIB, deps):
         return LIB
     cmd = [_nvcc()] + NVCC_FLAGS + ["-o", LIB] + srcs + LIBS
     if verbose:

@@ -203,7 +203,13 @@ extern "C" int ves3d_bicgstab_f64(ves3d_matvec_fn A, void* ctx, double* x, const
   double* ws = nullptr;
   VES3D_CK(cudaMalloc((void**)&ws, bicgstab_workspace_doubles((long)n) * sizeof(double)));
   int s = bicgstab_run(A, ctx, x, b, (long)n, tol, max_iter, code, ws, st, nullptr, nullptr);
-  cudaStreamSynchronize(st);
+  // an asynchronous fault of the last queued work surfaces here; report it unless the
+  // solve already failed
+  const cudaError_t e = cudaStreamSynchronize(st);
   cudaFree(ws);
+  if (!s && e != cudaSuccess) {
+    set_error("CUDA error %s after the solve", cudaGetErrorString(e));
+    s = VES3D_ERR_CUDA;
+  }
   return s;
 }

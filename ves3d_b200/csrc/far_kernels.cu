@@ -17,7 +17,10 @@
 // in FP64, rounded to FP32 once per source per CTA), the pair arithmetic in packed FP32
 // (Blackwell f32x2 FMA: both targets of a thread in one instruction), the unrefined
 // hardware reciprocal square root, and the FP32 partial of every 120-source sub-tile added into
-// FP64 accumulators. Distinct vesicles must not share points in the mixed form.
+// FP64 accumulators. A coincident pair of distinct vesicles (equal FP32 coordinates) makes
+// the unguarded sub-tile sum non-finite; such a sub-tile is summed again for that target
+// with the pair skipped, as in the reference, so the guard costs one finiteness test per
+// target and sub-tile instead of a select per pair.
 #include <atomic>
 #include <cstdlib>
 #include <map>
@@ -275,6 +278,26 @@ __global__ void __launch_bounds__(512) k_far_f64_segT(const double* __restrict__
 // ------------------------------------------------------------------------------------
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 
+// One target's FP32 sum over the staged sources [k0, k1) with coincident pairs skipped
+// (|r| = 0 contributes nothing, src/CPUKernels.cc:1030-1040): the slow path of a sub-tile
+// whose packed sum came out non-finite; (tx, ty, tz) is the negated target.
+__device__ __noinline__ float3 far_f32_guarded(const float2* sm, int k0, int k1, float tx, float ty, float tz) {
+  float3 u = make_float3(0.f, 0.f, 0.f);
+  for (int k = k0; k < k1; k++) {
+    const float2* q = sm + 6 * k;  // both lanes of a staged source hold the same value
+    const float dx = q[3].x, dy = q[4].x, dz = q[5].x;
+    const float rx = q[0].x + tx, ry = q[1].x + ty, rz = q[2].x + tz;
+    const float r2 = rx * rx + ry * ry + rz * rz;
+    if (!(r2 > 0.f)) continue;
+    const float y = rsqrt_ftz(r2);
+    const float cc = (rx * dx + ry * dy + rz * dz) * y * y;
+    u.x += (cc * rx + dx) * y;
+    u.y += (cc * ry + dy) * y;
+    u.z += (cc * rz + dz) * y;
+  }
+  return u;
+}
+
 // NP packed target pairs per thread (2 NP targets): target j of thread i in chunk c0 is
 // c0 + i + j * blockDim.x. NP = 2 reads each staged source once for four targets and gives
 // the scheduler two independent chains per source.
@@ -393,6 +416,28 @@ __global__ void __launch_bounds__(512) k_far_f32_segT(const double* __restrict__
       }
 #pragma unroll
       for (int q = 0; q < NP; q++) {
+        // a coincident pair (or a non-finite input) left this sub-tile's sum non-finite:
+        // sum it again with coincident pairs skipped (non-finite inputs stay non-finite)
+#pragma unroll
+        for (int ln = 0; ln < 2; ln++) {
+          const float sx = ln ? ux[q].y : ux[q].x, sy = ln ? uy[q].y : uy[q].x, sz = ln ? uz[q].y : uz[q].x;
+          if (!isfinite(sx + sy + sz)) {
+            float3 g = make_float3(0.f, 0.f, 0.f);
+            for (int part_i = 0; part_i < 2; part_i++) {
+              const int k0 = max(r0[part_i], sb), k1 = min(r1[part_i], se);
+              const float3 h = far_f32_guarded(sm, k0, k1, ln ? ntx[q].y : ntx[q].x, ln ? nty[q].y : nty[q].x,
+                                               ln ? ntz[q].y : ntz[q].x);
+              g.x += h.x;
+              g.y += h.y;
+              g.z += h.z;
+            }
+            if (ln) {
+              ux[q].y = g.x; uy[q].y = g.y; uz[q].y = g.z;
+            } else {
+              ux[q].x = g.x; uy[q].x = g.y; uz[q].x = g.z;
+            }
+          }
+        }
         A[2 * q][0] += ux[q].x;
         A[2 * q][1] += uy[q].x;
         A[2 * q][2] += uz[q].x;

@@ -1,11 +1,11 @@
-// FMA-throughput probe: measures the FP64 / FP32 CUDA-core FMA peak of the device it
-// runs on, the denominator of the roofline of the direct-sum kernels (which are bound
-// by those pipes, not by HBM or tensor cores). Eight independent FMA chains per
-// thread, enough CTAs to fill every SM several times over.
-#include "common.cuh"
-#include "kernels.h"
+// FMA-throughput probe of the benchmark (not part of the library: built on its own into
+// ves3d_b200/libves3d_peak.so and loaded by bench.py only). It measures the FP64 / FP32
+// CUDA-core FMA peak of the device it runs on, the denominator of the roofline of the
+// direct-sum kernels (which are bound by those pipes, not by HBM or tensor cores). Eight
+// independent FMA chains per thread, enough CTAs to fill every SM several times over.
+#include <cuda_runtime.h>
 
-namespace ves3d {
+namespace {
 
 template <class T>
 __global__ void __launch_bounds__(256) k_fma_probe(T* out, int iters, T a, T b) {
@@ -27,39 +27,39 @@ __global__ void __launch_bounds__(256) k_fma_probe(T* out, int iters, T a, T b) 
   if (s == (T)-1.2345) out[blockIdx.x] = s;  // keeps the chains live
 }
 
-}  // namespace ves3d
+}  // namespace
 
-using namespace ves3d;
-
-extern "C" int ves3d_measure_fma_peak(int fp64, double* tflops) {
-  VES3D_ARG(tflops != nullptr, "tflops is null");
+// Returns 0 and the measured TFLOP/s (2 flops per FMA) in *tflops, or the CUDA error code.
+extern "C" int ves3d_bench_fma_peak(int fp64, double* tflops) {
+  if (!tflops) return -1;
   int dev = 0, nsm = 0;
-  VES3D_CK(cudaGetDevice(&dev));
-  VES3D_CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  cudaError_t e;
+  if ((e = cudaGetDevice(&dev)) || (e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev))) return e;
   const int blocks = nsm * 8, threads = 256, iters = 2048;
   void* out = nullptr;
-  VES3D_CK(cudaMalloc(&out, blocks * sizeof(double)));
-  cudaEvent_t e0, e1;
-  VES3D_CK(cudaEventCreate(&e0));
-  VES3D_CK(cudaEventCreate(&e1));
+  if ((e = cudaMalloc(&out, blocks * sizeof(double)))) return e;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
   float best = 1e30f;
-  for (int rep = 0; rep < 4; rep++) {
-    VES3D_CK(cudaEventRecord(e0));
-    if (fp64)
-      k_fma_probe<double><<<blocks, threads>>>((double*)out, iters, 0.999999, 1e-7);
-    else
-      k_fma_probe<float><<<blocks, threads>>>((float*)out, iters, 0.999999f, 1e-7f);
-    VES3D_LAUNCHED();
-    VES3D_CK(cudaEventRecord(e1));
-    VES3D_CK(cudaEventSynchronize(e1));
-    float ms = 0;
-    VES3D_CK(cudaEventElapsedTime(&ms, e0, e1));
-    if (rep > 0 && ms < best) best = ms;
+  if (!(e = cudaEventCreate(&e0)) && !(e = cudaEventCreate(&e1))) {
+    for (int rep = 0; rep < 4 && !e; rep++) {
+      cudaEventRecord(e0);
+      if (fp64)
+        k_fma_probe<double><<<blocks, threads>>>((double*)out, iters, 0.999999, 1e-7);
+      else
+        k_fma_probe<float><<<blocks, threads>>>((float*)out, iters, 0.999999f, 1e-7f);
+      if ((e = cudaGetLastError())) break;
+      cudaEventRecord(e1);
+      if ((e = cudaEventSynchronize(e1))) break;
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (rep > 0 && ms < best) best = ms;
+    }
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
   cudaFree(out);
+  if (e) return e;
   const double flops = 2.0 * 8 * 16 * (double)iters * threads * blocks;
   *tflops = flops / (best * 1e-3) / 1e12;
-  return VES3D_OK;
+  return 0;
 }

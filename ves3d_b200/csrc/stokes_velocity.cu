@@ -208,8 +208,9 @@ struct ves3d_sv {
     graph = nullptr;
   }
   cudaEvent_t pc_ev[3 + kPcStreams] = {};
-  cudaEvent_t ev[8] = {};
+  cudaEvent_t ev[10] = {};
   float ms[4] = {0, 0, 0, 0};
+  float far_dl_ms = 0;  // the far double layer's segment kernels in the last evaluation
 
   ~ves3d_sv() {
     dfree(filt);
@@ -522,9 +523,11 @@ int fork_far(ves3d_sv* sv, int* nseg, cudaEvent_t ev_far0, cudaEvent_t ev_far1, 
   if (dl) {  // the far double layer (FP64) after the single layer's segments
     if ((s = launch_unit_normals(sv->Xt, sv->Xp, sv->nves, sv->p, sv->nrm, fs))) return s;
     if ((s = launch_far_density(sv->G, sv->area, sv->nves, sv->p, T.smooth_w0, sv->dden, fs))) return s;
+    if (ev_far0) VES3D_CK(cudaEventRecord(sv->ev[8], fs));
     if ((s = launch_far_dl(sv->pos, sv->nrm, sv->dden, sv->off, sv->nves, sv->npts(), ngrid_(sv->p), sv->part_dl,
                            kFarMaxSegments, fs, &sv->nseg_dl)))
       return s;
+    if (ev_far0) VES3D_CK(cudaEventRecord(sv->ev[9], fs));
   }
   VES3D_CK(cudaEventRecord(sv->ev_join, fs));
   return VES3D_OK;
@@ -591,6 +594,8 @@ int run_eval(ves3d_sv* sv, bool dl) {
   VES3D_CK(cudaEventElapsedTime(&sv->ms[1], sv->ev[2], sv->ev[3]));
   VES3D_CK(cudaEventElapsedTime(&sv->ms[2], sv->ev[4], sv->ev[5]));
   VES3D_CK(cudaEventElapsedTime(&sv->ms[3], sv->ev[2], sv->ev[6]));
+  sv->far_dl_ms = 0;
+  if (dl) VES3D_CK(cudaEventElapsedTime(&sv->far_dl_ms, sv->ev[8], sv->ev[9]));
   sv->parts_valid = true;
   return VES3D_OK;
 }
@@ -1017,6 +1022,12 @@ int ves3d_sv_get_parts(ves3d_sv* sv, double* vel_self, double* vel_far, int is_d
 int ves3d_sv_stage_times(ves3d_sv* sv, float* ms) {
   VES3D_ARG(sv != nullptr && ms != nullptr, "null argument");
   for (int i = 0; i < 4; i++) ms[i] = sv->ms[i];
+  return VES3D_OK;
+}
+
+int ves3d_sv_far_dl_time(ves3d_sv* sv, float* ms) {
+  VES3D_ARG(sv != nullptr && ms != nullptr, "null argument");
+  *ms = sv->far_dl_ms;
   return VES3D_OK;
 }
 

@@ -14,6 +14,13 @@ def env_world():
         int(os.environ.get("LOCAL_RANK", "0"))
 
 
+def barrier(world):
+    """Barrier over all ranks (no-op for one rank)."""
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
 def max_over_ranks(x, world, device=None):
     """Maximum of a float over all ranks (every rank gets it)."""
     if world == 1:

@@ -183,6 +183,13 @@ class StokesVelocity:
         check(lib().ves3d_sv_stage_times(self._h, ms), "stage_times")
         return {"setup_ms": ms[0], "self_apply_ms": ms[1], "far_ms": ms[2], "eval_ms": ms[3]}
 
+    def far_dl_ms(self):
+        """Device ms of the far double layer's kernels in the last evaluation (0 without
+        a double-layer density)."""
+        ms = ctypes.c_float()
+        check(lib().ves3d_sv_far_dl_time(self._h, ctypes.byref(ms)), "far_dl_time")
+        return ms.value
+
     def device_buffer(self, which):
         ptr = ctypes.c_void_p()
         n = ctypes.c_size_t()

@@ -17,8 +17,12 @@ from .stokes_velocity import _ptr
 
 def _rank_size(rank, n_ranks):
     """The communicator of the reference's call: explicit rank and size, else those of the
-    torch.distributed process group when one is up, else a single rank."""
-    if rank is not None and n_ranks is not None:
+    torch.distributed process group when one is up, else a single rank. Giving only one
+    of rank and n_ranks is an error (the other would be guessed, and a wrong guess writes
+    the index from the wrong process or makes piece names collide)."""
+    if (rank is None) != (n_ranks is None):
+        raise ValueError("give both rank and n_ranks, or neither")
+    if rank is not None:
         return int(rank), int(n_ranks)
     try:
         import torch.distributed as dist
