@@ -65,3 +65,46 @@ def test_mixed_deterministic():
         a = sv()
         b = sv()
     assert np.array_equal(a, b)
+
+
+def test_tensor_core_build_vs_fp64_and_oracle():
+    """The mixed form builds its p = 16 self matrices with the DFT GEMMs on the tcgen05
+    tensor cores (split-BF16, FP32 accumulation): self matrices against the FP64 build,
+    velocity against the FP64 oracle, both within the mixed form's 1e-6."""
+    p = 16
+    X, f = small_suspension(2, p, 61)
+    with StokesVelocity(p, precision="fp64") as sv:
+        sv.SetSrcCoord(X)
+        SL64 = sv.self_matrix()
+    with StokesVelocity(p, precision="mixed") as sv:
+        sv.SetSrcCoord(X)
+        SLm = sv.self_matrix()
+        sv.SetDensitySL(f)
+        vel = sv()
+        vself, _ = sv.parts()
+    ref_self = sh.self_apply(sh.stokes_singular_matrix(X, p, 2 * p), f, p)
+    ref = ref_self + stokes.far_velocity(X, f, p)
+    assert 0 < rel_err(SLm, SL64) < MIXED_TOL  # a different build, within the bar
+    assert rel_err(vself, ref_self) < MIXED_TOL
+    assert rel_err(vel, ref) < MIXED_TOL
+
+
+def test_tensor_core_build_is_deterministic_and_matches_fp64_ring_env(monkeypatch):
+    """Two tensor-core builds give the same bits; VES3D_TC_BUILD=0 falls back to the FP64
+    ring in the mixed form (the A/B switch)."""
+    p = 16
+    X, _ = small_suspension(1, p, 62)
+    with StokesVelocity(p, precision="mixed") as sv:
+        sv.SetSrcCoord(X)
+        a = sv.self_matrix()
+        sv.SetSrcCoord(X)
+        b = sv.self_matrix()
+    assert np.array_equal(a, b)
+    monkeypatch.setenv("VES3D_TC_BUILD", "0")
+    with StokesVelocity(p, precision="mixed") as sv:
+        sv.SetSrcCoord(X)
+        c = sv.self_matrix()
+    with StokesVelocity(p, precision="fp64") as sv:
+        sv.SetSrcCoord(X)
+        d = sv.self_matrix()
+    assert np.array_equal(c, d)

@@ -18,6 +18,11 @@
 // kind in tcgen05). Fragment layout (PTX ISA, m8n8k4 .f64): A: a0 = A[lane/4][lane%4];
 // B: b0 = B[lane%4][lane/4]; C: {c0, c1} = C[lane/4][2(lane%4) + {0, 1}]. Shared-memory
 // row strides are padded to 4 mod 16 doubles so those loads are bank-conflict free.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cstdint>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -336,6 +341,625 @@ static int launch_ring(const double* R, long nrot, const DevTables& T, double* C
   k_build_ring<P0><<<(unsigned)grid, 256, G::SMEM, st>>>(R, T, C, nrot);
   VES3D_LAUNCHED();
   return VES3D_OK;
+}
+
+// ======================================================================================
+// Mixed form of the fused build on the fifth-generation tensor cores (tcgen05).
+//
+// The two DFT GEMMs of a rotation -- the synthesis of X, X_theta, X_phi on the upsampled
+// grid (K = 2 p0 Fourier coefficients) and the transposed DFT of the 12 kernel components
+// (K = 2 p1 longitudes) -- are 89% of the ring's multiply-adds. Here they run as
+// tcgen05.mma kind::f16 products with BF16 operands split three ways and FP32
+// accumulation in tensor memory (TMEM):
+//     a = a0 + a1 + a2 (a0 = bf16(a), a1 = bf16(a - a0), a2 = bf16(a - a0 - a1)),
+//     A.B ~ sum over i + j <= 2 of Ai.Bj   (six products, smallest first),
+// which represents each operand to ~2^-24 relative. Three products (i + j <= 1, the
+// "3xBF16" form) leave ~2^-16 and measured 2.5e-6 relative error on the self velocity;
+// six measure below 1e-7 (numpy emulation of this kernel's arithmetic on the
+// 512-vesicle p = 16 suspension).
+//
+// Positions are synthesised relative to the pole target of their hemisphere (the m = 0
+// Fourier column is shifted by the target before the split, X = D + c added back in
+// FP64), so that r = target - source near the pole -- where the singular kernel
+// amplifies relative errors of the positions by |X| / |r| -- carries the GEMM's relative
+// error of |r|, not of |X| (which includes the vesicle's centre). Kept in FP64: the
+// Legendre synthesis and the transposed Legendre sums (FP64 tensor cores, mma.sync
+// m8n8k4), the pole targets, the singular kernel and its quadrature weights.
+//
+// One CTA per SM, persistent over rotations. Per rotation:
+//   R (FP64, bulk-copied by TMA, next rotation prefetched)
+//   -> Legendre synthesis per latitude group (table slices bulk-copied, double-buffered)
+//      -> A, dA split to BF16 in shared memory (UMMA K-major layout, no swizzle)
+//   -> GEMM 1: [X | X_theta] = A [Mf | dMf], X_phi = dA Mf         (TMEM cols 0..191)
+//   -> per chunk of 16 longitudes: TMEM -> shared, FP64 kernel at 33 x 16 points,
+//      12 components split to BF16 -> GEMM 2 accumulating C = K Mf^T   (TMEM 192..287)
+//   -> TMEM -> shared (FP32), transposed Legendre sums (FP64) -> C [12][Nc] in HBM.
+// The last upsampled latitude (p1 + 1 = 33 rows do not fit the 32 lanes of a warp
+// quarter) takes its transposed DFT in FP64 on the CUDA cores.
+//
+// Every wait is bounded (about a second of %globaltimer); a wait that runs out sets
+// g_tc_build_error, the CTA stops, waits (bounded) for its copies and MMAs, frees its
+// TMEM and returns, and the host reports the error.
+// ======================================================================================
+__device__ int g_tc_build_error = 0;
+
+namespace tc {
+
+__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t gtimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(saddr(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(saddr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+constexpr uint64_t kWaitNs = 1000000000ull;  // a second: MMAs and copies here take microseconds
+
+// Bounded wait for the phase of the given parity; false when the limit ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  if (mbar_test(bar, parity)) return true;
+  const uint64_t t0 = gtimer();
+  while (!mbar_test(bar, parity))
+    if (gtimer() - t0 > kWaitNs) return false;
+  return true;
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(bar)), "r"(bytes) : "memory");
+}
+
+// 1-D bulk copy global -> shared through the TMA engine, completing on an mbarrier
+// (addresses 16-byte aligned, size a multiple of 16).
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   saddr(dst)),
+               "l"(src), "r"(bytes), "r"(saddr(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// Shared-memory matrix descriptor of a K-major operand without swizzle: core matrices of
+// 8 rows x 16 bytes, lbo = byte distance between K-adjacent core matrices, sbo = between
+// 8-row groups; bit 46 = descriptor version of sm_100.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor: kind::f16, A and B BF16, D FP32, both K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(saddr(bar))
+               : "memory");
+}
+
+// 16 consecutive FP32 columns of this thread's TMEM lane (32x32b shape).
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// Byte offset of element (row, k) of a K-major no-swizzle operand with kcols columns
+// (core matrices K-adjacent at 128 B, 8-row groups at kcols * 16 B).
+__host__ __device__ constexpr uint32_t umma_off(int row, int k, int kcols) {
+  return (uint32_t)((row >> 3) * (kcols * 16) + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+
+// Three-way BF16 split of an FP64 value, stored at byte offset off of three operand
+// buffers stride bytes apart.
+__device__ __forceinline__ void store_split3(unsigned char* base, uint32_t stride, uint32_t off, double v) {
+  const __nv_bfloat16 h0 = __double2bfloat16(v);
+  double r = v - (double)__bfloat162float(h0);
+  const __nv_bfloat16 h1 = __double2bfloat16(r);
+  r -= (double)__bfloat162float(h1);
+  const __nv_bfloat16 h2 = __double2bfloat16(r);
+  *reinterpret_cast<__nv_bfloat16*>(base + off) = h0;
+  *reinterpret_cast<__nv_bfloat16*>(base + stride + off) = h1;
+  *reinterpret_cast<__nv_bfloat16*>(base + 2 * stride + off) = h2;
+}
+
+// Split products (i, j), i + j <= 2, smallest first.
+__constant__ int kSplitI[6] = {2, 1, 0, 1, 0, 0};
+__constant__ int kSplitJ[6] = {0, 1, 2, 0, 1, 0};
+
+}  // namespace tc
+
+template <int P0>
+struct RingTcCfg {
+  using G = RingCfg<P0>;
+  static constexpr int P1 = 2 * P0, L1 = P1 + 1, F0 = 2 * P0, N1 = 2 * P1, NC = P0 * (P0 + 2);
+  static_assert(P0 == 16, "the tensor-core ring is laid out for p = 16 (33 upsampled latitudes)");
+  static constexpr int LG = 4, NGRP = (L1 + LG - 1) / LG;
+  static constexpr int LDR = G::LDR;     // FP64 coefficient rows (R, Legendre slices)
+  static constexpr int LDC = F0 + 5;     // FP32 rows of the transposed-DFT result
+  static constexpr int JC = 16;          // longitudes per kernel chunk (K of one GEMM-2 step)
+  static constexpr int NCH = N1 / JC;    // chunks per rotation
+  static constexpr int KROWS = 12 * 32;  // GEMM-2 rows (component, latitude < 32): 3 M-tiles
+  // operand sizes (bytes, one split)
+  static constexpr int SZ_A = 128 * F0 * 2;       // A or dA: 128 rows x K = F0
+  static constexpr int SZ_B12 = 128 * F0 * 2;     // [Mf | dMf]^T: N = 2 N1 = 128 rows x K = F0
+  static constexpr int SZ_BT = F0 * N1 * 2;       // Mf: N = F0 rows x K = N1
+  static constexpr int SZ_K = KROWS * JC * 2;     // one chunk of kernel values
+  static constexpr int SXS_LD = JC + 1;           // FP32 surface values [9][lat][SXS_LD]
+  static constexpr int SZ_XS = 9 * L1 * SXS_LD * 4;
+  static constexpr int SZ_C = L1 * 12 * LDC * 4;  // FP32 transposed-DFT result [lat][comp][LDC]
+  // byte offsets (operand buffers 1024-aligned)
+  static constexpr int OFF_B12 = 0;
+  static constexpr int OFF_BT = OFF_B12 + 3 * SZ_B12;
+  static constexpr int OFF_U = OFF_BT + 3 * SZ_BT;           // union region
+  static constexpr int OFF_A = OFF_U;                        // 3 splits of A, then 3 of dA
+  static constexpr int OFF_K0 = OFF_U;                       // chunk buffer 0 (3 splits)
+  static constexpr int OFF_K1 = OFF_K0 + 3 * SZ_K;           // chunk buffer 1
+  static constexpr int OFF_XS = OFF_K1 + 3 * SZ_K;
+  static constexpr int U_END = OFF_XS + SZ_XS;
+  static_assert(6 * SZ_A <= OFF_XS - OFF_U, "A/dA must fit in the chunk buffers");
+  static_assert(SZ_C <= OFF_XS - OFF_U, "C must fit in the chunk buffers");
+  static constexpr int OFF_R = (U_END + 127) / 128 * 128;    // 2 x [3][LDR] FP64
+  static constexpr int OFF_LEG = OFF_R + 2 * 3 * LDR * 8;    // 2 buffers x (leg, dleg) x [LG][LDR] FP64
+  static constexpr int OFF_K32 = OFF_LEG + 2 * 2 * LG * LDR * 8;  // [12][N1] FP64 (last latitude)
+  static constexpr int OFF_MISC = OFF_K32 + 12 * N1 * 8;
+  // misc: trg[6], cen[6] (doubles), sSw[L1] (double), sBo[F0+1] (int), sTl[NTT] (uchar2),
+  // mbarriers (7 x 8 B), TMEM address, abort flag
+  static constexpr int OFF_TRG = OFF_MISC;
+  static constexpr int OFF_CEN = OFF_TRG + 6 * 8;
+  static constexpr int OFF_SW = OFF_CEN + 6 * 8;
+  static constexpr int OFF_BO = OFF_SW + L1 * 8;
+  static constexpr int OFF_TL = OFF_BO + ((F0 + 1) * 4 + 7) / 8 * 8;
+  static constexpr int OFF_BAR = OFF_TL + (G::NTT * 2 + 7) / 8 * 8;
+  static constexpr int OFF_TMEM = OFF_BAR + 7 * 8;
+  static constexpr int SMEM = OFF_TMEM + 16;
+  static constexpr uint32_t TMEM_COLS = 512;
+  static constexpr int COL_X = 0, COL_XT = N1, COL_XP = 2 * N1, COL_T = 3 * N1;
+  static_assert(COL_T + 3 * F0 <= (int)TMEM_COLS, "TMEM columns");
+};
+
+template <int P0>
+__global__ void __launch_bounds__(256, 1) k_build_ring_tc(const double* __restrict__ R, DevTables T,
+                                                          double* __restrict__ C, long nrot) {
+  using G = RingCfg<P0>;
+  using H = RingTcCfg<P0>;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char* sB12 = smem + H::OFF_B12;
+  unsigned char* sBT = smem + H::OFF_BT;
+  unsigned char* sA = smem + H::OFF_A;                 // splits at sA + i * SZ_A
+  unsigned char* sdA = smem + H::OFF_A + 3 * H::SZ_A;  // splits at sdA + i * SZ_A
+  float* sXs = reinterpret_cast<float*>(smem + H::OFF_XS);
+  float* sC = reinterpret_cast<float*>(smem + H::OFF_U);
+  double* sRb = reinterpret_cast<double*>(smem + H::OFF_R);
+  double* sLegb = reinterpret_cast<double*>(smem + H::OFF_LEG);
+  double* sK32 = reinterpret_cast<double*>(smem + H::OFF_K32);
+  double* trg = reinterpret_cast<double*>(smem + H::OFF_TRG);
+  double* cen = reinterpret_cast<double*>(smem + H::OFF_CEN);
+  double* sSw = reinterpret_cast<double*>(smem + H::OFF_SW);
+  int* sBo = reinterpret_cast<int*>(smem + H::OFF_BO);
+  uchar2* sTl = reinterpret_cast<uchar2*>(smem + H::OFF_TL);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + H::OFF_BAR);
+  uint64_t* bar_mma1 = bars;      // GEMM 1 done
+  uint64_t* bar_k = bars + 1;     // [2] GEMM-2 chunk buffers free
+  uint64_t* bar_r = bars + 3;     // [2] R buffers loaded
+  uint64_t* bar_leg = bars + 5;   // [2] Legendre slice buffers loaded
+  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(smem + H::OFF_TMEM);
+  int* s_abort = reinterpret_cast<int*>(smem + H::OFF_TMEM + 4);
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int grow = lane >> 2, gcol = lane & 3;
+  constexpr int NC = H::NC, LDR = H::LDR, F0 = H::F0, N1 = H::N1, L1 = H::L1, LG = H::LG;
+
+  // ---- set-up: TMEM, barriers, constant operands and tables ---------------------------
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc::saddr(s_tmem)),
+                 "r"(H::TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int i = 0; i < 7; i++) tc::mbar_init(bars + i);
+    *s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // [Mf | dMf]^T and Mf as split BF16 operands: B12 row n < N1 is Mf[.][n], n >= N1 dMf[.][n - N1]
+  for (int i = tid; i < 2 * N1 * F0; i += 256) {
+    const int n = i / F0, k = i - n * F0;
+    const double v = n < N1 ? __ldg(T.syn1_four + k * N1 + n) : __ldg(T.syn1_dfour + k * N1 + n - N1);
+    tc::store_split3(sB12, H::SZ_B12, tc::umma_off(n, k, F0), v);
+  }
+  for (int i = tid; i < F0 * N1; i += 256) {
+    const int n = i / N1, k = i - n * N1;  // BT[jf][j] = Mf[jf][j]
+    tc::store_split3(sBT, H::SZ_BT, tc::umma_off(n, k, N1), __ldg(T.syn1_four + i));
+  }
+  for (int i = tid; i < L1; i += 256) sSw[i] = __ldg(T.sing_w + i);
+  for (int i = tid; i <= F0; i += 256) sBo[i] = __ldg(T.blk_off + i);
+  if (tid == 0) {
+    int j = 0;
+    for (int k = 0; k < F0; k++) {
+      const int len = __ldg(T.blk_off + k + 1) - __ldg(T.blk_off + k);
+      for (int nt = 0; nt * 8 < len && j < G::NTT; nt++) sTl[j++] = make_uchar2((unsigned char)k, (unsigned char)nt);
+    }
+  }
+  // K padding of R and of the Legendre slices (columns NC..LDR-1): zeros, never overwritten
+  for (int i = tid; i < 2 * 3 * (LDR - NC); i += 256) sRb[(i / (LDR - NC)) * LDR + NC + i % (LDR - NC)] = 0.0;
+  for (int i = tid; i < 2 * 2 * LG * (LDR - NC); i += 256) sLegb[(i / (LDR - NC)) * LDR + NC + i % (LDR - NC)] = 0.0;
+  tc::fence_async_smem();
+  tc::tc_before_sync();
+  __syncthreads();
+  tc::tc_after_sync();
+  const uint32_t tmem = *s_tmem;
+  const double mf00 = __ldg(T.syn1_four);  // the constant m = 0 Fourier row
+
+  // issue the bulk copies of R (rotation rot) into buffer b, and of Legendre slice g into buffer b
+  auto issue_r = [&](long rot, int b) {
+    double* dst = sRb + b * 3 * LDR;
+    tc::mbar_expect_tx(bar_r + b, 3 * NC * 8);
+    for (int d = 0; d < 3; d++) tc::bulk_g2s(dst + d * LDR, R + (rot * 3 + d) * NC, NC * 8, bar_r + b);
+  };
+  auto issue_leg = [&](int g, int b) {
+    const int lat0 = g * LG, nlat = min(LG, L1 - lat0);
+    double* dst = sLegb + b * 2 * LG * LDR;
+    tc::mbar_expect_tx(bar_leg + b, 2 * nlat * NC * 8);
+    for (int l = 0; l < nlat; l++) {
+      tc::bulk_g2s(dst + l * LDR, T.syn1_leg_t + (long)(lat0 + l) * NC, NC * 8, bar_leg + b);
+      tc::bulk_g2s(dst + (LG + l) * LDR, T.syn1_dleg_t + (long)(lat0 + l) * NC, NC * 8, bar_leg + b);
+    }
+  };
+  // phases waited for per barrier, and phases issued (uniform over the CTA: every issue
+  // decision below depends only on loop indices)
+  uint32_t n_r[2] = {0, 0}, n_leg[2] = {0, 0}, n_k[2] = {0, 0}, n_mma1 = 0;
+  uint32_t i_r[2] = {0, 0}, i_leg[2] = {0, 0}, i_k[2] = {0, 0}, i_mma1 = 0;
+  int gi = 0;  // running Legendre slice counter; slice g = gi % NGRP lives in buffer gi & 1
+  bool ok = true;
+  auto wait = [&](uint64_t* bar, uint32_t& cnt) {
+    if (!tc::mbar_wait(bar, cnt & 1)) {
+      atomicExch(&g_tc_build_error, 1);
+      *s_abort = 1;
+    }
+    cnt++;
+  };
+  auto sync_ok = [&]() {
+    __syncthreads();
+    return *s_abort == 0;
+  };
+  if (blockIdx.x < nrot) {
+    if (tid == 0) {
+      issue_r(blockIdx.x, 0);
+      issue_leg(0, 0);
+    }
+    i_r[0]++;
+    i_leg[0]++;
+  }
+  long it = 0;
+  for (long rot = blockIdx.x; rot < nrot && ok; rot += gridDim.x, it++) {
+    const int rb = (int)(it & 1);
+    double* sR = sRb + rb * 3 * LDR;
+    wait(bar_r + rb, n_r[rb]);
+    if (rot + gridDim.x < nrot) {
+      if (tid == 0) issue_r(rot + gridDim.x, rb ^ 1);
+      i_r[rb ^ 1]++;
+    }
+    if (!(ok = sync_ok())) break;
+    if (tid < 6) {
+      const int c = tid >> 1, t = tid & 1;
+      double s = 0.0;
+      for (int n = 0; n <= P0; n++) s += sR[c * LDR + n] * __ldg(T.qp + t * (P0 + 1) + n);
+      trg[c * 2 + t] = s;
+    }
+    __syncthreads();
+    if (tid < 6) cen[tid] = trg[(tid % 3) * 2 + tid / 3];  // cen[h * 3 + d]: target of hemisphere h
+    // ---- pass 1: Legendre synthesis (FP64 tensor cores) -> split BF16 A, dA ------------
+    for (int g = 0; g < H::NGRP; g++, gi++) {
+      const int b = gi & 1, lat0 = g * LG, nlat = min(LG, L1 - lat0);
+      const double* sLeg = sLegb + b * 2 * LG * LDR;
+      const double* sdLeg = sLeg + LG * LDR;
+      wait(bar_leg + b, n_leg[b]);
+      if (tid == 0) issue_leg((g + 1) % H::NGRP, b ^ 1);
+      i_leg[b ^ 1]++;
+      __syncthreads();
+      for (int itm = warp; itm < 2 * F0; itm += 8) {
+        const int k = itm >> 1, which = itm & 1;
+        const int c0 = sBo[k], c1 = sBo[k + 1];
+        const double* Lp = (which ? sdLeg : sLeg) + grow * LDR + c0 + gcol;
+        const double* Rr = sR + grow * LDR + c0 + gcol;
+        double e0 = 0.0, e1 = 0.0;
+        for (int ks = 0; 4 * ks < c1 - c0; ks++) {
+          const int c = c0 + 4 * ks + gcol;
+          const double a = grow < nlat ? Lp[4 * ks] : 0.0;
+          const double bb = (grow < 3 && c < c1) ? Rr[4 * ks] : 0.0;
+          dmma(e0, e1, a, bb);
+        }
+        if (grow < nlat) {
+          const int lat = lat0 + grow;
+          const int h = 2 * lat > H::P1 ? 1 : 0;  // hemisphere: the pole target it is centred on
+#pragma unroll
+          for (int q = 0; q < 2; q++) {
+            const int d = 2 * gcol + q;
+            if (d < 3) {
+              double v = q ? e1 : e0;
+              if (!which && k == 0) v -= cen[h * 3 + d] / mf00;
+              const int row = lat < 32 ? d * 32 + lat : 96 + d;
+              tc::store_split3(which ? sdA : sA, H::SZ_A, tc::umma_off(row, k, F0), v);
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+    // ---- GEMM 1 on the tensor cores ------------------------------------------------------
+    tc::fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tc::tc_after_sync();
+      constexpr uint32_t id128 = tc::idesc_bf16(128, 2 * N1), id64 = tc::idesc_bf16(128, N1);
+      constexpr uint32_t SBO = F0 * 16;
+      for (int pr = 0; pr < 6; pr++) {
+        const int i = tc::kSplitI[pr], j = tc::kSplitJ[pr];
+        for (int s = 0; s < F0 / 16; s++) {
+          const uint64_t da = tc::umma_desc(tc::saddr(sA + i * H::SZ_A) + s * 256, 128, SBO);
+          const uint64_t db = tc::umma_desc(tc::saddr(sB12 + j * H::SZ_B12) + s * 256, 128, SBO);
+          tc::mma_bf16(tmem + H::COL_X, da, db, id128, (pr | s) ? 1u : 0u);
+        }
+      }
+      for (int pr = 0; pr < 6; pr++) {
+        const int i = tc::kSplitI[pr], j = tc::kSplitJ[pr];
+        for (int s = 0; s < F0 / 16; s++) {
+          const uint64_t da = tc::umma_desc(tc::saddr(sdA + i * H::SZ_A) + s * 256, 128, SBO);
+          const uint64_t db = tc::umma_desc(tc::saddr(sB12 + j * H::SZ_B12) + s * 256, 128, SBO);
+          tc::mma_bf16(tmem + H::COL_XP, da, db, id64, (pr | s) ? 1u : 0u);
+        }
+      }
+      tc::mma_commit(bar_mma1);
+    }
+    i_mma1++;
+    wait(bar_mma1, n_mma1);
+    if (!(ok = sync_ok())) break;
+    tc::tc_after_sync();
+    // ---- per chunk of longitudes: kernel values and GEMM 2 ------------------------------
+    for (int ch = 0; ch < H::NCH && ok; ch++) {
+      const int kb = ch & 1;
+      unsigned char* sK = smem + (kb ? H::OFF_K1 : H::OFF_K0);
+      // (a) surfaces of the chunk: TMEM -> shared (warp quarter q reads lanes 32q..32q+31)
+      {
+        const int q = warp & 3;
+        const int row = 32 * q + lane;
+        const int d = q < 3 ? q : lane, lat = q < 3 ? lane : 32;
+        const bool live = q < 3 || lane < 3;
+        float v[16];
+        const uint32_t lanes = (uint32_t)(32 * q) << 16;
+        if (warp < 4) {
+          tc::tmem_ld16(tmem + lanes + H::COL_X + ch * H::JC, v);
+          if (live)
+            for (int jj = 0; jj < H::JC; jj++) sXs[(0 * 3 + d) * L1 * H::SXS_LD + lat * H::SXS_LD + jj] = v[jj];
+          tc::tmem_ld16(tmem + lanes + H::COL_XT + ch * H::JC, v);
+          if (live)
+            for (int jj = 0; jj < H::JC; jj++) sXs[(1 * 3 + d) * L1 * H::SXS_LD + lat * H::SXS_LD + jj] = v[jj];
+        } else {
+          tc::tmem_ld16(tmem + lanes + H::COL_XP + ch * H::JC, v);
+          if (live)
+            for (int jj = 0; jj < H::JC; jj++) sXs[(2 * 3 + d) * L1 * H::SXS_LD + lat * H::SXS_LD + jj] = v[jj];
+        }
+        (void)row;
+      }
+      if (ch >= 2) wait(bar_k + kb, n_k[kb]);  // the MMAs of chunk ch - 2 have read this buffer
+      tc::tc_before_sync();
+      if (!(ok = sync_ok())) break;
+      // (b) singular kernel (FP64) at the chunk's 33 x 16 points -> split BF16 chunk operand
+      for (int pnt = tid; pnt < L1 * H::JC; pnt += 256) {
+        const int lat = pnt / H::JC, jj = pnt - lat * H::JC;
+        const int h = 2 * lat > H::P1 ? 1 : 0;
+        const float* xs = sXs + lat * H::SXS_LD + jj;
+        constexpr int VS = L1 * H::SXS_LD;
+        const double px = xs[0], py = xs[VS], pz = xs[2 * VS];  // centred on the hemisphere's target
+        const double ax = xs[3 * VS], ay = xs[4 * VS], az = xs[5 * VS];
+        const double bx = xs[6 * VS], by = xs[7 * VS], bz = xs[8 * VS];
+        const double nx = ay * bz - az * by, ny = az * bx - ax * bz, nz = ax * by - ay * bx;
+        const double n2 = nx * nx + ny * ny + nz * nz;
+        const double area = n2 * rsqrt_f64(n2);
+        double kv[12];
+#pragma unroll
+        for (int t = 0; t < 2; t++) {
+          // r = target_t - (centre_h + D) with target_t - centre_h exact (0 when t == h)
+          const double dx = (trg[t] - cen[h * 3]) - px, dy = (trg[2 + t] - cen[h * 3 + 1]) - py,
+                       dz = (trg[4 + t] - cen[h * 3 + 2]) - pz;
+          const double r2 = dx * dx + dy * dy + dz * dz;
+          double rinv = rsqrt_f64(r2);
+          if (r2 <= 2.220446049250313e-16) rinv = 0.0;
+          const double a1 = kInv8Pi * sSw[t ? lat : H::P1 - lat] * area * rinv;
+          const double a2 = a1 * rinv * rinv;
+          kv[t * 6 + 0] = a1 + dx * dx * a2;
+          kv[t * 6 + 1] = dx * dy * a2;
+          kv[t * 6 + 2] = dx * dz * a2;
+          kv[t * 6 + 3] = a1 + dy * dy * a2;
+          kv[t * 6 + 4] = dy * dz * a2;
+          kv[t * 6 + 5] = a1 + dz * dz * a2;
+        }
+        if (lat < 32) {
+#pragma unroll
+          for (int comp = 0; comp < 12; comp++)
+            tc::store_split3(sK, H::SZ_K, tc::umma_off(comp * 32 + lat, jj, H::JC), kv[comp]);
+        } else {
+#pragma unroll
+          for (int comp = 0; comp < 12; comp++) sK32[comp * N1 + ch * H::JC + jj] = kv[comp];
+        }
+      }
+      tc::fence_async_smem();
+      __syncthreads();
+      if (tid == 0) {
+        tc::tc_after_sync();
+        constexpr uint32_t id32 = tc::idesc_bf16(128, F0);
+        for (int tt = 0; tt < 3; tt++) {
+          for (int pr = 0; pr < 6; pr++) {
+            const int i = tc::kSplitI[pr], j = tc::kSplitJ[pr];
+            const uint64_t da = tc::umma_desc(tc::saddr(sK + i * H::SZ_K) + tt * 128 * H::JC * 2, 128, H::JC * 16);
+            const uint64_t db = tc::umma_desc(tc::saddr(sBT + j * H::SZ_BT) + ch * (H::JC / 8) * 128, 128, N1 * 16);
+            tc::mma_bf16(tmem + H::COL_T + tt * F0, da, db, id32, (ch | pr) ? 1u : 0u);
+          }
+        }
+        tc::mma_commit(bar_k + kb);
+      }
+      i_k[kb]++;
+    }
+    if (!ok) break;
+    // the last two chunks' MMAs (buffers 0 and 1) before TMEM is read and the buffers reused
+    wait(bar_k + 0, n_k[0]);
+    wait(bar_k + 1, n_k[1]);
+    if (!(ok = sync_ok())) break;
+    tc::tc_after_sync();
+    // ---- transposed-DFT result -> shared (FP32); the last latitude in FP64 ----------------
+    if (warp < 4) {
+      const int q = warp;
+      float v[16];
+      for (int tt = 0; tt < 3; tt++) {
+        const int comp = 4 * tt + q, lat = lane;  // row comp * 32 + lat of tile tt
+        for (int half = 0; half < 2; half++) {
+          tc::tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + H::COL_T + tt * F0 + half * 16, v);
+          for (int x = 0; x < 16; x++) sC[(lat * 12 + comp) * H::LDC + half * 16 + x] = v[x];
+        }
+      }
+    } else {
+      for (int o = tid - 128; o < 12 * F0; o += 128) {
+        const int comp = o / F0, jf = o - comp * F0;
+        const double* kr = sK32 + comp * N1;
+        const double* mf = T.syn1_four + jf * N1;
+        double s = 0.0;
+        for (int j = 0; j < N1; j++) s = fma(kr[j], __ldg(mf + j), s);
+        sC[(32 * 12 + comp) * H::LDC + jf] = (float)s;
+      }
+    }
+    tc::tc_before_sync();
+    __syncthreads();
+    // ---- pass 2: transposed Legendre sums (FP64 tensor cores) ---------------------------
+    double acc[G::QMAX][2];
+#pragma unroll
+    for (int q = 0; q < G::QMAX; q++) acc[q][0] = acc[q][1] = 0.0;
+    for (int g = 0; g < H::NGRP; g++, gi++) {
+      const int b = gi & 1, lat0 = g * LG, nlat = min(LG, L1 - lat0);
+      const double* sLeg = sLegb + b * 2 * LG * LDR;
+      wait(bar_leg + b, n_leg[b]);
+      if (tid == 0) issue_leg((g + 1) % H::NGRP, b ^ 1);
+      i_leg[b ^ 1]++;
+      if (!(ok = sync_ok())) break;
+#pragma unroll
+      for (int q = 0; q < G::QMAX; q++) {
+        const int tile = warp + 8 * q;
+        if (tile < 2 * G::NTT) {
+          const int mt = tile / G::NTT;
+          const uchar2 kt = sTl[tile - mt * G::NTT];
+          const int k = kt.x, c0 = sBo[k], c1 = sBo[k + 1];
+          const int comp = mt * 8 + grow, l = gcol, c = c0 + kt.y * 8 + grow;
+          const double a = (comp < 12 && l < nlat) ? (double)sC[((lat0 + l) * 12 + comp) * H::LDC + k] : 0.0;
+          const double bb = (l < nlat && c < c1) ? sLeg[l * LDR + c] : 0.0;
+          dmma(acc[q][0], acc[q][1], a, bb);
+        }
+      }
+      __syncthreads();
+    }
+    if (!ok) break;
+#pragma unroll
+    for (int q = 0; q < G::QMAX; q++) {
+      const int tile = warp + 8 * q;
+      if (tile < 2 * G::NTT) {
+        const int mt = tile / G::NTT;
+        const uchar2 kt = sTl[tile - mt * G::NTT];
+        const int c0 = sBo[kt.x], c1 = sBo[kt.x + 1];
+        const int comp = mt * 8 + grow, c = c0 + kt.y * 8 + 2 * gcol;
+        if (comp < 12) {
+          if (c < c1) C[rot * G::NOUT + comp * NC + c] = acc[q][0];
+          if (c + 1 < c1) C[rot * G::NOUT + comp * NC + c + 1] = acc[q][1];
+        }
+      }
+    }
+  }
+  // ---- drain: copies and MMAs issued but not waited for (the Legendre slice prefetched
+  // past the last rotation; after an abort, whatever was in flight), each wait bounded;
+  // then TMEM is freed ------------------------------------------------------------------
+  {
+    bool drained = true;
+    auto drain = [&](uint64_t* bar, uint32_t& waited, uint32_t issued) {
+      while (drained && waited < issued) {
+        if (!tc::mbar_wait(bar, waited & 1)) {
+          atomicExch(&g_tc_build_error, 1);
+          drained = false;
+        }
+        waited++;
+      }
+    };
+    for (int b = 0; b < 2; b++) {
+      drain(bar_r + b, n_r[b], i_r[b]);
+      drain(bar_leg + b, n_leg[b], i_leg[b]);
+      drain(bar_k + b, n_k[b], i_k[b]);
+    }
+    drain(bar_mma1, n_mma1, i_mma1);
+  }
+  tc::tc_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tc::tc_after_sync();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(H::TMEM_COLS) : "memory");
+  }
+}
+
+bool tc_build_supported(int p0, int p1) { return p0 == 16 && p1 == 32; }
+
+int launch_build_ring_tc(const double* R, long nrot, const DevTables& T, double* C, cudaStream_t st) {
+  if (nrot <= 0) return VES3D_OK;
+  if (!tc_build_supported(T.p0, T.p1)) {
+    set_error("tensor-core build not laid out for p = %d, p_up = %d", T.p0, T.p1);
+    return VES3D_ERR_ARG;
+  }
+  using H = RingTcCfg<16>;
+  VES3D_CK(cudaFuncSetAttribute(k_build_ring_tc<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, H::SMEM));
+  int dev = 0, nsm = 148;
+  VES3D_CK(cudaGetDevice(&dev));
+  VES3D_CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const long grid = std::min(nrot, (long)nsm);
+  k_build_ring_tc<16><<<(unsigned)grid, 256, H::SMEM, st>>>(R, T, C, nrot);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
+int tc_build_error(bool reset) {
+  int v = 0;
+  VES3D_CK(cudaMemcpyFromSymbol(&v, g_tc_build_error, sizeof(int)));
+  if (v && reset) {
+    const int zero = 0;
+    VES3D_CK(cudaMemcpyToSymbol(g_tc_build_error, &zero, sizeof(int)));
+  }
+  return v;
 }
 
 bool fused_build_supported(int p0, int p1) {

@@ -18,9 +18,9 @@
 // (Blackwell f32x2 FMA: both targets of a thread in one instruction), the unrefined
 // hardware reciprocal square root, and the FP32 partial of every 120-source sub-tile added into
 // FP64 accumulators. A coincident pair of distinct vesicles (equal FP32 coordinates) makes
-// the unguarded sub-tile sum non-finite; such a sub-tile is summed again for that target
-// with the pair skipped, as in the reference, so the guard costs one finiteness test per
-// target and sub-tile instead of a select per pair.
+// the unguarded sum non-finite; such a target's segment is summed again with the pair
+// skipped, as in the reference, so the guard costs one finiteness test per target and
+// segment instead of a select per pair.
 #include <atomic>
 #include <cstdlib>
 #include <map>
@@ -278,24 +278,37 @@ __global__ void __launch_bounds__(512) k_far_f64_segT(const double* __restrict__
 // ------------------------------------------------------------------------------------
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 
-// One target's FP32 sum over the staged sources [k0, k1) with coincident pairs skipped
-// (|r| = 0 contributes nothing, src/CPUKernels.cc:1030-1040): the slow path of a sub-tile
-// whose packed sum came out non-finite; (tx, ty, tz) is the negated target.
-__device__ __noinline__ float3 far_f32_guarded(const float2* sm, int k0, int k1, float tx, float ty, float tz) {
-  float3 u = make_float3(0.f, 0.f, 0.f);
-  for (int k = k0; k < k1; k++) {
-    const float2* q = sm + 6 * k;  // both lanes of a staged source hold the same value
-    const float dx = q[3].x, dy = q[4].x, dz = q[5].x;
-    const float rx = q[0].x + tx, ry = q[1].x + ty, rz = q[2].x + tz;
+// One target's sum over the sources [s0, s1) outside [e0, e1) with coincident pairs
+// skipped (|r| = 0 contributes nothing, as in StokesAlltoAll, src/CPUKernels.cc:1030-1040),
+// in the pair arithmetic of the mixed kernel (FP32 coordinates relative to the centroid
+// (cx, cy, cz), FP32 sums per 120 sources, FP64 across them); (tx, ty, tz) is the negated
+// target. The slow path of a target whose segment sum came out non-finite.
+__device__ __forceinline__ double3 far_f32_guarded(const double* __restrict__ pos, const double* __restrict__ den,
+                                                long s0, long s1, long e0, long e1, double cx, double cy, double cz,
+                                                float tx, float ty, float tz) {
+  double ax = 0.0, ay = 0.0, az = 0.0;
+  float ux = 0.f, uy = 0.f, uz = 0.f;
+  int cnt = 0;
+  for (long s = s0; s < s1; s++) {
+    if (s >= e0 && s < e1) continue;
+    const float rx = (float)(pos[3 * s] - cx) + tx, ry = (float)(pos[3 * s + 1] - cy) + ty,
+                rz = (float)(pos[3 * s + 2] - cz) + tz;
+    const float dx = (float)den[3 * s], dy = (float)den[3 * s + 1], dz = (float)den[3 * s + 2];
     const float r2 = rx * rx + ry * ry + rz * rz;
-    if (!(r2 > 0.f)) continue;
-    const float y = rsqrt_ftz(r2);
-    const float cc = (rx * dx + ry * dy + rz * dz) * y * y;
-    u.x += (cc * rx + dx) * y;
-    u.y += (cc * ry + dy) * y;
-    u.z += (cc * rz + dz) * y;
+    if (r2 > 0.f) {
+      const float y = rsqrt_ftz(r2);
+      const float c = (rx * dx + ry * dy + rz * dz) * y * y;
+      ux += (c * rx + dx) * y;
+      uy += (c * ry + dy) * y;
+      uz += (c * rz + dz) * y;
+    }
+    if (++cnt == kSubF32) {
+      ax += ux; ay += uy; az += uz;
+      ux = uy = uz = 0.f;
+      cnt = 0;
+    }
   }
-  return u;
+  return make_double3(ax + ux, ay + uy, az + uz);
 }
 
 // NP packed target pairs per thread (2 NP targets): target j of thread i in chunk c0 is
@@ -416,28 +429,6 @@ __global__ void __launch_bounds__(512) k_far_f32_segT(const double* __restrict__
       }
 #pragma unroll
       for (int q = 0; q < NP; q++) {
-        // a coincident pair (or a non-finite input) left this sub-tile's sum non-finite:
-        // sum it again with coincident pairs skipped (non-finite inputs stay non-finite)
-#pragma unroll
-        for (int ln = 0; ln < 2; ln++) {
-          const float sx = ln ? ux[q].y : ux[q].x, sy = ln ? uy[q].y : uy[q].x, sz = ln ? uz[q].y : uz[q].x;
-          if (!isfinite(sx + sy + sz)) {
-            float3 g = make_float3(0.f, 0.f, 0.f);
-            for (int part_i = 0; part_i < 2; part_i++) {
-              const int k0 = max(r0[part_i], sb), k1 = min(r1[part_i], se);
-              const float3 h = far_f32_guarded(sm, k0, k1, ln ? ntx[q].y : ntx[q].x, ln ? nty[q].y : nty[q].x,
-                                               ln ? ntz[q].y : ntz[q].x);
-              g.x += h.x;
-              g.y += h.y;
-              g.z += h.z;
-            }
-            if (ln) {
-              ux[q].y = g.x; uy[q].y = g.y; uz[q].y = g.z;
-            } else {
-              ux[q].x = g.x; uy[q].x = g.y; uz[q].x = g.z;
-            }
-          }
-        }
         A[2 * q][0] += ux[q].x;
         A[2 * q][1] += uy[q].x;
         A[2 * q][2] += uz[q].x;
@@ -445,6 +436,25 @@ __global__ void __launch_bounds__(512) k_far_f32_segT(const double* __restrict__
         A[2 * q + 1][1] += uy[q].y;
         A[2 * q + 1][2] += uz[q].y;
       }
+    }
+  }
+  // A coincident pair left a target's segment sum non-finite: sum the segment again for
+  // that target with coincident pairs skipped (non-finite inputs stay non-finite). One
+  // test per target and segment; no instruction in the pair loop.
+#pragma unroll
+  for (int j = 0; j < T; j++) {
+    const long jj = c0 + threadIdx.x + (long)j * nthr;
+    if (jj < nt && !isfinite(A[j][0] + A[j][1] + A[j][2])) {
+      const long g = t0 + jj;
+      // the centroid from shared memory again: keeping it in registers across the pair
+      // loop would cost the loop registers
+      const double gx = cen[0], gy = cen[1], gz = cen[2];
+      const double3 a = far_f32_guarded(pos, den, tb * kTileF32, min(te * kTileF32, N), t0, t0 + nt, gx, gy, gz,
+                                        (float)(gx - pos[3 * g]), (float)(gy - pos[3 * g + 1]),
+                                        (float)(gz - pos[3 * g + 2]));
+      A[j][0] = a.x;
+      A[j][1] = a.y;
+      A[j][2] = a.z;
     }
   }
   double* P = part + (long)seg * 3 * N;

@@ -64,6 +64,12 @@ int launch_rotate_transpose_scatter(const double* C, long nv, const DevTables& T
 // i.e. upsampled synthesis + singular kernel + transposed synthesis in one kernel.
 bool fused_build_supported(int p0, int p1);
 int launch_build_ring(const double* R, long nrot, const DevTables& T, double* C, cudaStream_t st);
+// Mixed form of the fused build: the DFT GEMMs on tcgen05 tensor cores as split-BF16
+// products with FP32 accumulation (Legendre sums, kernel and targets FP64); same layouts.
+bool tc_build_supported(int p0, int p1);
+int launch_build_ring_tc(const double* R, long nrot, const DevTables& T, double* C, cudaStream_t st);
+// Error flag of the tensor-core build (a bounded wait ran out), optionally reset.
+int tc_build_error(bool reset);
 // V[v] = F[v] . SL[v] (src/StokesVelocity.cc:397-416), n = 3 Ncoef.
 int launch_self_gemv(const double* F, const double* SL, long nv, int n, double* V, cudaStream_t st,
                      bool accumulate = false);

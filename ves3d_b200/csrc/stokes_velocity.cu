@@ -175,6 +175,9 @@ struct ves3d_sv {
   long chunk = 0;
   double *R = nullptr, *Xu = nullptr, *Xut = nullptr, *Xup = nullptr, *K = nullptr, *C = nullptr, *SL3 = nullptr;
   bool have_src = false, have_den = false, sl_valid = false, parts_valid = false;
+  // sl_tc: the current self matrices come from the tensor-core build of the mixed form;
+  // implicit_on: implicit parameters were set, whose FP64 residuals need FP64 self matrices
+  bool sl_tc = false, implicit_on = false;
   // implicit step: geometry record and work fields (allocated on first use)
   double *geo = nullptr, *wc = nullptr, *w[8] = {nullptr}, *bws = nullptr;
   long geo_cap = 0, bws_cap = 0;
@@ -350,6 +353,23 @@ bool use_fused(const ves3d_sv* sv) {
   return fused_build_supported(sv->p, sv->pup);
 }
 
+// The mixed form builds with the DFT GEMMs on tcgen05 tensor cores where that kernel is
+// laid out for (p, p_up); VES3D_TC_BUILD=0 keeps the FP64 ring (A/B checks).
+bool use_tc_build(const ves3d_sv* sv) {
+  if (sv->prec != VES3D_PREC_MIXED || sv->implicit_on || !tc_build_supported(sv->p, sv->pup)) return false;
+  const char* env = getenv("VES3D_TC_BUILD");
+  return !(env && env[0] == '0');
+}
+
+// A context that takes implicit steps keeps FP64 self matrices: the mixed refinement's
+// outer residuals are those of the FP64 system. Self matrices from the tensor-core build
+// are rebuilt on next use.
+void mark_implicit(ves3d_sv* sv) {
+  if (sv->implicit_on) return;
+  sv->implicit_on = true;
+  if (sv->sl_tc) sv->sl_valid = false;
+}
+
 // Doubles of setup scratch per vesicle.
 size_t scratch_per_vesicle(int p0, int p1, bool fused) {
   const size_t npr = (size_t)p0 * (p0 + 1), nc = ncoef_(p0), M1 = ngrid_(p1), ng = ngrid_(p0);
@@ -431,6 +451,7 @@ int run_setup(ves3d_sv* sv, bool dl) {
   int s = alloc_scratch(sv);
   if (s) return s;
   const bool fused = !dl && use_fused(sv);
+  const bool tc = fused && use_tc_build(sv);
   double* M = dl ? sv->DL : sv->SL;
   if ((!fused && !sv->K) || !M) {
     set_error("internal: self-matrix build without its buffers");
@@ -441,7 +462,9 @@ int run_setup(ves3d_sv* sv, bool dl) {
     const long nb = std::min(sv->chunk, sv->nves - v0);
     const long nrot = nb * npr;
     if ((s = launch_rotate_all(sv->Sx + v0 * 3 * nc, nb, T, sv->R, st))) return s;
-    if (fused) {
+    if (fused && tc) {
+      if ((s = launch_build_ring_tc(sv->R, nrot, T, sv->C, st))) return s;
+    } else if (fused) {
       if ((s = launch_build_ring(sv->R, nrot, T, sv->C, st))) return s;
     } else {
       if ((s = launch_synthesis(sv->R, nrot * 3, p0, p1, T.syn1_leg, T.syn1_dleg, T.syn1_four, T.syn1_dfour,
@@ -462,10 +485,16 @@ int run_setup(ves3d_sv* sv, bool dl) {
   VES3D_CK(cudaEventRecord(sv->ev[1], st));
   VES3D_CK(cudaEventSynchronize(sv->ev[1]));
   VES3D_CK(cudaEventElapsedTime(dl ? &sv->dl_ms : &sv->ms[0], sv->ev[0], sv->ev[1]));
-  if (dl)
+  if (tc && tc_build_error(true)) {
+    set_error("self-matrix build on the tensor cores: a bounded wait of the kernel ran out");
+    return VES3D_ERR_CUDA;
+  }
+  if (dl) {
     sv->dl_valid = true;
-  else
+  } else {
     sv->sl_valid = true;
+    sv->sl_tc = tc;
+  }
   return VES3D_OK;
 }
 
@@ -2249,6 +2278,7 @@ int ves3d_sv_set_implicit_params(ves3d_sv* sv, double dt, double kappa, double s
   if (s) return s;
   VES3D_ARG(dt > 0 && kappa >= 0, "dt must be > 0 and kappa >= 0");
   if (dt != sv->dt || kappa != sv->kappa) sv->pc_valid = false;
+  mark_implicit(sv);
   sv->dt = dt;
   sv->kappa = kappa;
   sv->shear = shear_rate;
@@ -3035,6 +3065,7 @@ namespace {
 
 int svp_prepare_implicit(ves3d_svp* g) {
   int s;
+  for (ves3d_sv* sv : g->grp) mark_implicit(sv);  // FP64 self matrices before the setup
   if ((s = ves3d_svp_setup(g))) return s;
   g->coff.assign(g->grp.size() + 1, 0);
   for (size_t r = 0; r < g->grp.size(); r++) {
