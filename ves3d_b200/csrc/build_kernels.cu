@@ -366,14 +366,18 @@ static int launch_ring(const double* R, long nrot, const DevTables& T, double* C
 // Legendre synthesis and the transposed Legendre sums (FP64 tensor cores, mma.sync
 // m8n8k4), the pole targets, the singular kernel and its quadrature weights.
 //
-// One CTA per SM, persistent over rotations. Per rotation:
-//   R (FP64, bulk-copied by TMA, next rotation prefetched)
-//   -> Legendre synthesis per latitude group (table slices bulk-copied, double-buffered)
-//      -> A, dA split to BF16 in shared memory (UMMA K-major layout, no swizzle)
+// One CTA of 16 warps per SM, persistent over rotations, with the Legendre tables resident
+// in shared memory (the m = 0 block in FP64: it carries the vesicle's position; the other
+// blocks in FP32: they multiply shape-sized coefficients) and the DFT tables as split BF16
+// operands. Per rotation:
+//   R (FP64, bulk-copied by TMA, the next rotation's prefetched)
+//   -> Legendre synthesis (FP64 tensor cores) -> A, dA split to BF16 in shared memory
+//      (UMMA K-major layout, no swizzle)
 //   -> GEMM 1: [X | X_theta] = A [Mf | dMf], X_phi = dA Mf         (TMEM cols 0..191)
 //   -> per chunk of 16 longitudes: TMEM -> shared, FP64 kernel at 33 x 16 points,
-//      12 components split to BF16 -> GEMM 2 accumulating C = K Mf^T   (TMEM 192..287)
-//   -> TMEM -> shared (FP32), transposed Legendre sums (FP64) -> C [12][Nc] in HBM.
+//      12 components split to BF16 -> GEMM 2 accumulating C = K Mf^T   (TMEM 192..287),
+//      overlapping the next chunk's TMEM reads
+//   -> TMEM -> shared (FP32), transposed Legendre sums (FP64 tensor cores) -> C [12][Nc].
 // The last upsampled latitude (p1 + 1 = 33 rows do not fit the 32 lanes of a warp
 // quarter) takes its transposed DFT in FP64 on the CUDA cores.
 //
@@ -482,14 +486,14 @@ __host__ __device__ constexpr uint32_t umma_off(int row, int k, int kcols) {
   return (uint32_t)((row >> 3) * (kcols * 16) + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
 }
 
-// Three-way BF16 split of an FP64 value, stored at byte offset off of three operand
-// buffers stride bytes apart.
-__device__ __forceinline__ void store_split3(unsigned char* base, uint32_t stride, uint32_t off, double v) {
-  const __nv_bfloat16 h0 = __double2bfloat16(v);
-  double r = v - (double)__bfloat162float(h0);
-  const __nv_bfloat16 h1 = __double2bfloat16(r);
-  r -= (double)__bfloat162float(h1);
-  const __nv_bfloat16 h2 = __double2bfloat16(r);
+// Three-way BF16 split of a value rounded to FP32 (its 24-bit significand is covered
+// exactly: v = h0 + h1 + h2 with each residual exact in FP32), stored at byte offset off
+// of three operand buffers stride bytes apart.
+__device__ __forceinline__ void store_split3(unsigned char* base, uint32_t stride, uint32_t off, float v) {
+  const __nv_bfloat16 h0 = __float2bfloat16_rn(v);
+  const float r1 = v - __bfloat162float(h0);
+  const __nv_bfloat16 h1 = __float2bfloat16_rn(r1);
+  const __nv_bfloat16 h2 = __float2bfloat16_rn(r1 - __bfloat162float(h1));
   *reinterpret_cast<__nv_bfloat16*>(base + off) = h0;
   *reinterpret_cast<__nv_bfloat16*>(base + stride + off) = h1;
   *reinterpret_cast<__nv_bfloat16*>(base + 2 * stride + off) = h2;
@@ -506,12 +510,17 @@ struct RingTcCfg {
   using G = RingCfg<P0>;
   static constexpr int P1 = 2 * P0, L1 = P1 + 1, F0 = 2 * P0, N1 = 2 * P1, NC = P0 * (P0 + 2);
   static_assert(P0 == 16, "the tensor-core ring is laid out for p = 16 (33 upsampled latitudes)");
+  static constexpr int NTHR = 512, NWARP = NTHR / 32;
   static constexpr int LG = 4, NGRP = (L1 + LG - 1) / LG;
-  static constexpr int LDR = G::LDR;     // FP64 coefficient rows (R, Legendre slices)
+  static constexpr int LDR = G::LDR;     // FP64 coefficient rows of R (4 mod 16 doubles)
+  static constexpr int M0 = P0 + 1;      // the m = 0 Fourier block: coefficients 0..P0
+  static constexpr int LD0 = 20;         // FP64 m = 0 table rows (>= M0 + 3, 4 mod 16)
+  static constexpr int LDF = 292;        // FP32 table rows (>= NC + 3, 4 mod 32 floats)
   static constexpr int LDC = F0 + 5;     // FP32 rows of the transposed-DFT result
   static constexpr int JC = 16;          // longitudes per kernel chunk (K of one GEMM-2 step)
   static constexpr int NCH = N1 / JC;    // chunks per rotation
   static constexpr int KROWS = 12 * 32;  // GEMM-2 rows (component, latitude < 32): 3 M-tiles
+  static constexpr int QMAX = (2 * G::NTT + NWARP - 1) / NWARP;  // transposed-Legendre tiles per warp
   // operand sizes (bytes, one split)
   static constexpr int SZ_A = 128 * F0 * 2;       // A or dA: 128 rows x K = F0
   static constexpr int SZ_B12 = 128 * F0 * 2;     // [Mf | dMf]^T: N = 2 N1 = 128 rows x K = F0
@@ -520,38 +529,36 @@ struct RingTcCfg {
   static constexpr int SXS_LD = JC + 1;           // FP32 surface values [9][lat][SXS_LD]
   static constexpr int SZ_XS = 9 * L1 * SXS_LD * 4;
   static constexpr int SZ_C = L1 * 12 * LDC * 4;  // FP32 transposed-DFT result [lat][comp][LDC]
-  // byte offsets (operand buffers 1024-aligned)
+  // byte offsets; the union region U holds A/dA (pass 1 -> GEMM 1), then the chunk buffer
+  // and the chunk's surface values (-> GEMM 2), then C (-> pass 2)
   static constexpr int OFF_B12 = 0;
   static constexpr int OFF_BT = OFF_B12 + 3 * SZ_B12;
-  static constexpr int OFF_U = OFF_BT + 3 * SZ_BT;           // union region
-  static constexpr int OFF_A = OFF_U;                        // 3 splits of A, then 3 of dA
-  static constexpr int OFF_K0 = OFF_U;                       // chunk buffer 0 (3 splits)
-  static constexpr int OFF_K1 = OFF_K0 + 3 * SZ_K;           // chunk buffer 1
-  static constexpr int OFF_XS = OFF_K1 + 3 * SZ_K;
-  static constexpr int U_END = OFF_XS + SZ_XS;
-  static_assert(6 * SZ_A <= OFF_XS - OFF_U, "A/dA must fit in the chunk buffers");
-  static_assert(SZ_C <= OFF_XS - OFF_U, "C must fit in the chunk buffers");
-  static constexpr int OFF_R = (U_END + 127) / 128 * 128;    // 2 x [3][LDR] FP64
-  static constexpr int OFF_LEG = OFF_R + 2 * 3 * LDR * 8;    // 2 buffers x (leg, dleg) x [LG][LDR] FP64
-  static constexpr int OFF_K32 = OFF_LEG + 2 * 2 * LG * LDR * 8;  // [12][N1] FP64 (last latitude)
-  static constexpr int OFF_MISC = OFF_K32 + 12 * N1 * 8;
-  // misc: trg[6], cen[6] (doubles), sSw[L1] (double), sBo[F0+1] (int), sTl[NTT] (uchar2),
-  // mbarriers (7 x 8 B), TMEM address, abort flag
-  static constexpr int OFF_TRG = OFF_MISC;
+  static constexpr int OFF_U = OFF_BT + 3 * SZ_BT;
+  static constexpr int OFF_A = OFF_U;
+  static constexpr int OFF_K = OFF_U;
+  static constexpr int OFF_XS = OFF_K + 3 * SZ_K;
+  static constexpr int U_SZ = std::max(std::max(6 * SZ_A, 3 * SZ_K + SZ_XS), SZ_C);
+  static constexpr int OFF_R = (OFF_U + U_SZ + 127) / 128 * 128;  // 2 x [3][LDR] FP64
+  static constexpr int OFF_T0 = OFF_R + 2 * 3 * LDR * 8;          // FP64 m = 0 tables: leg, dleg [L1][LD0]
+  static constexpr int OFF_TF = OFF_T0 + 2 * L1 * LD0 * 8;        // FP32 tables: leg, dleg [L1][LDF]
+  static constexpr int OFF_K32 = OFF_TF + 2 * L1 * LDF * 4;       // [12][N1] FP64 (last latitude)
+  static constexpr int OFF_TRG = OFF_K32 + 12 * N1 * 8;
   static constexpr int OFF_CEN = OFF_TRG + 6 * 8;
   static constexpr int OFF_SW = OFF_CEN + 6 * 8;
   static constexpr int OFF_BO = OFF_SW + L1 * 8;
   static constexpr int OFF_TL = OFF_BO + ((F0 + 1) * 4 + 7) / 8 * 8;
   static constexpr int OFF_BAR = OFF_TL + (G::NTT * 2 + 7) / 8 * 8;
-  static constexpr int OFF_TMEM = OFF_BAR + 7 * 8;
+  static constexpr int NBAR = 4;  // GEMM 1, GEMM 2, R buffers 0 and 1
+  static constexpr int OFF_TMEM = OFF_BAR + NBAR * 8;
   static constexpr int SMEM = OFF_TMEM + 16;
   static constexpr uint32_t TMEM_COLS = 512;
   static constexpr int COL_X = 0, COL_XT = N1, COL_XP = 2 * N1, COL_T = 3 * N1;
   static_assert(COL_T + 3 * F0 <= (int)TMEM_COLS, "TMEM columns");
+  static_assert(SMEM <= 227 * 1024, "shared memory");
 };
 
 template <int P0>
-__global__ void __launch_bounds__(256, 1) k_build_ring_tc(const double* __restrict__ R, DevTables T,
+__global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restrict__ R, DevTables T,
                                                           double* __restrict__ C, long nrot) {
   using G = RingCfg<P0>;
   using H = RingTcCfg<P0>;
@@ -560,10 +567,12 @@ __global__ void __launch_bounds__(256, 1) k_build_ring_tc(const double* __restri
   unsigned char* sBT = smem + H::OFF_BT;
   unsigned char* sA = smem + H::OFF_A;                 // splits at sA + i * SZ_A
   unsigned char* sdA = smem + H::OFF_A + 3 * H::SZ_A;  // splits at sdA + i * SZ_A
+  unsigned char* sK = smem + H::OFF_K;                 // splits at sK + i * SZ_K
   float* sXs = reinterpret_cast<float*>(smem + H::OFF_XS);
   float* sC = reinterpret_cast<float*>(smem + H::OFF_U);
   double* sRb = reinterpret_cast<double*>(smem + H::OFF_R);
-  double* sLegb = reinterpret_cast<double*>(smem + H::OFF_LEG);
+  double* sT0 = reinterpret_cast<double*>(smem + H::OFF_T0);  // leg, then dleg: [L1][LD0]
+  float* sTF = reinterpret_cast<float*>(smem + H::OFF_TF);    // leg, then dleg: [L1][LDF]
   double* sK32 = reinterpret_cast<double*>(smem + H::OFF_K32);
   double* trg = reinterpret_cast<double*>(smem + H::OFF_TRG);
   double* cen = reinterpret_cast<double*>(smem + H::OFF_CEN);
@@ -571,16 +580,17 @@ __global__ void __launch_bounds__(256, 1) k_build_ring_tc(const double* __restri
   int* sBo = reinterpret_cast<int*>(smem + H::OFF_BO);
   uchar2* sTl = reinterpret_cast<uchar2*>(smem + H::OFF_TL);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + H::OFF_BAR);
-  uint64_t* bar_mma1 = bars;      // GEMM 1 done
-  uint64_t* bar_k = bars + 1;     // [2] GEMM-2 chunk buffers free
-  uint64_t* bar_r = bars + 3;     // [2] R buffers loaded
-  uint64_t* bar_leg = bars + 5;   // [2] Legendre slice buffers loaded
+  uint64_t* bar_mma1 = bars;     // GEMM 1 done
+  uint64_t* bar_k = bars + 1;    // GEMM 2 of the last chunk done (the chunk buffer is free)
+  uint64_t* bar_r = bars + 2;    // [2] R buffers loaded
   uint32_t* s_tmem = reinterpret_cast<uint32_t*>(smem + H::OFF_TMEM);
   int* s_abort = reinterpret_cast<int*>(smem + H::OFF_TMEM + 4);
 
+  constexpr int NTHR = H::NTHR, NWARP = H::NWARP;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int grow = lane >> 2, gcol = lane & 3;
-  constexpr int NC = H::NC, LDR = H::LDR, F0 = H::F0, N1 = H::N1, L1 = H::L1, LG = H::LG;
+  constexpr int NC = H::NC, LDR = H::LDR, F0 = H::F0, N1 = H::N1, L1 = H::L1, LG = H::LG, M0 = H::M0;
+  constexpr int LD0 = H::LD0, LDF = H::LDF;
 
   // ---- set-up: TMEM, barriers, constant operands and tables ---------------------------
   if (warp == 0) {
@@ -590,22 +600,35 @@ __global__ void __launch_bounds__(256, 1) k_build_ring_tc(const double* __restri
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 0) {
-    for (int i = 0; i < 7; i++) tc::mbar_init(bars + i);
+    for (int i = 0; i < H::NBAR; i++) tc::mbar_init(bars + i);
     *s_abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   // [Mf | dMf]^T and Mf as split BF16 operands: B12 row n < N1 is Mf[.][n], n >= N1 dMf[.][n - N1]
-  for (int i = tid; i < 2 * N1 * F0; i += 256) {
+  for (int i = tid; i < 2 * N1 * F0; i += NTHR) {
     const int n = i / F0, k = i - n * F0;
     const double v = n < N1 ? __ldg(T.syn1_four + k * N1 + n) : __ldg(T.syn1_dfour + k * N1 + n - N1);
-    tc::store_split3(sB12, H::SZ_B12, tc::umma_off(n, k, F0), v);
+    tc::store_split3(sB12, H::SZ_B12, tc::umma_off(n, k, F0), (float)v);
   }
-  for (int i = tid; i < F0 * N1; i += 256) {
+  for (int i = tid; i < F0 * N1; i += NTHR) {
     const int n = i / N1, k = i - n * N1;  // BT[jf][j] = Mf[jf][j]
-    tc::store_split3(sBT, H::SZ_BT, tc::umma_off(n, k, N1), __ldg(T.syn1_four + i));
+    tc::store_split3(sBT, H::SZ_BT, tc::umma_off(n, k, N1), (float)__ldg(T.syn1_four + i));
   }
-  for (int i = tid; i < L1; i += 256) sSw[i] = __ldg(T.sing_w + i);
-  for (int i = tid; i <= F0; i += 256) sBo[i] = __ldg(T.blk_off + i);
+  // Legendre tables resident for the CTA's life: the m = 0 block in FP64 (it carries the
+  // vesicle's position), the other blocks in FP32 (their values multiply shape-sized
+  // coefficients; measured no change in the self velocity's error); zero K padding
+  for (int i = tid; i < 2 * L1 * LD0; i += NTHR) {
+    const int tb = i / (L1 * LD0), r = i - tb * L1 * LD0, lat = r / LD0, c = r - lat * LD0;
+    const double* src = tb ? T.syn1_dleg_t : T.syn1_leg_t;
+    sT0[i] = c < M0 ? __ldg(src + (long)lat * NC + c) : 0.0;
+  }
+  for (int i = tid; i < 2 * L1 * LDF; i += NTHR) {
+    const int tb = i / (L1 * LDF), r = i - tb * L1 * LDF, lat = r / LDF, c = r - lat * LDF;
+    const double* src = tb ? T.syn1_dleg_t : T.syn1_leg_t;
+    sTF[i] = (c >= M0 && c < NC) ? (float)__ldg(src + (long)lat * NC + c) : 0.f;
+  }
+  for (int i = tid; i < L1; i += NTHR) sSw[i] = __ldg(T.sing_w + i);
+  for (int i = tid; i <= F0; i += NTHR) sBo[i] = __ldg(T.blk_off + i);
   if (tid == 0) {
     int j = 0;
     for (int k = 0; k < F0; k++) {
@@ -613,9 +636,8 @@ __global__ void __launch_bounds__(256, 1) k_build_ring_tc(const double* __restri
       for (int nt = 0; nt * 8 < len && j < G::NTT; nt++) sTl[j++] = make_uchar2((unsigned char)k, (unsigned char)nt);
     }
   }
-  // K padding of R and of the Legendre slices (columns NC..LDR-1): zeros, never overwritten
-  for (int i = tid; i < 2 * 3 * (LDR - NC); i += 256) sRb[(i / (LDR - NC)) * LDR + NC + i % (LDR - NC)] = 0.0;
-  for (int i = tid; i < 2 * 2 * LG * (LDR - NC); i += 256) sLegb[(i / (LDR - NC)) * LDR + NC + i % (LDR - NC)] = 0.0;
+  // K padding of R (columns NC..LDR-1): zeros, never overwritten by the copies
+  for (int i = tid; i < 2 * 3 * (LDR - NC); i += NTHR) sRb[(i / (LDR - NC)) * LDR + NC + i % (LDR - NC)] = 0.0;
   tc::fence_async_smem();
   tc::tc_before_sync();
   __syncthreads();
@@ -623,26 +645,15 @@ __global__ void __launch_bounds__(256, 1) k_build_ring_tc(const double* __restri
   const uint32_t tmem = *s_tmem;
   const double mf00 = __ldg(T.syn1_four);  // the constant m = 0 Fourier row
 
-  // issue the bulk copies of R (rotation rot) into buffer b, and of Legendre slice g into buffer b
   auto issue_r = [&](long rot, int b) {
     double* dst = sRb + b * 3 * LDR;
     tc::mbar_expect_tx(bar_r + b, 3 * NC * 8);
     for (int d = 0; d < 3; d++) tc::bulk_g2s(dst + d * LDR, R + (rot * 3 + d) * NC, NC * 8, bar_r + b);
   };
-  auto issue_leg = [&](int g, int b) {
-    const int lat0 = g * LG, nlat = min(LG, L1 - lat0);
-    double* dst = sLegb + b * 2 * LG * LDR;
-    tc::mbar_expect_tx(bar_leg + b, 2 * nlat * NC * 8);
-    for (int l = 0; l < nlat; l++) {
-      tc::bulk_g2s(dst + l * LDR, T.syn1_leg_t + (long)(lat0 + l) * NC, NC * 8, bar_leg + b);
-      tc::bulk_g2s(dst + (LG + l) * LDR, T.syn1_dleg_t + (long)(lat0 + l) * NC, NC * 8, bar_leg + b);
-    }
-  };
-  // phases waited for per barrier, and phases issued (uniform over the CTA: every issue
-  // decision below depends only on loop indices)
-  uint32_t n_r[2] = {0, 0}, n_leg[2] = {0, 0}, n_k[2] = {0, 0}, n_mma1 = 0;
-  uint32_t i_r[2] = {0, 0}, i_leg[2] = {0, 0}, i_k[2] = {0, 0}, i_mma1 = 0;
-  int gi = 0;  // running Legendre slice counter; slice g = gi % NGRP lives in buffer gi & 1
+  // phases waited for per barrier and issued (uniform over the CTA: every issue decision
+  // depends only on loop indices)
+  uint32_t n_r[2] = {0, 0}, n_k = 0, n_mma1 = 0;
+  uint32_t i_r[2] = {0, 0}, i_k = 0, i_mma1 = 0;
   bool ok = true;
   auto wait = [&](uint64_t* bar, uint32_t& cnt) {
     if (!tc::mbar_wait(bar, cnt & 1)) {
@@ -656,17 +667,13 @@ __global__ void __launch_bounds__(256, 1) k_build_ring_tc(const double* __restri
     return *s_abort == 0;
   };
   if (blockIdx.x < nrot) {
-    if (tid == 0) {
-      issue_r(blockIdx.x, 0);
-      issue_leg(0, 0);
-    }
+    if (tid == 0) issue_r(blockIdx.x, 0);
     i_r[0]++;
-    i_leg[0]++;
   }
   long it = 0;
   for (long rot = blockIdx.x; rot < nrot && ok; rot += gridDim.x, it++) {
     const int rb = (int)(it & 1);
-    double* sR = sRb + rb * 3 * LDR;
+    const double* sR = sRb + rb * 3 * LDR;
     wait(bar_r + rb, n_r[rb]);
     if (rot + gridDim.x < nrot) {
       if (tid == 0) issue_r(rot + gridDim.x, rb ^ 1);
@@ -681,43 +688,47 @@ __global__ void __launch_bounds__(256, 1) k_build_ring_tc(const double* __restri
     }
     __syncthreads();
     if (tid < 6) cen[tid] = trg[(tid % 3) * 2 + tid / 3];  // cen[h * 3 + d]: target of hemisphere h
+    __syncthreads();
     // ---- pass 1: Legendre synthesis (FP64 tensor cores) -> split BF16 A, dA ------------
-    for (int g = 0; g < H::NGRP; g++, gi++) {
-      const int b = gi & 1, lat0 = g * LG, nlat = min(LG, L1 - lat0);
-      const double* sLeg = sLegb + b * 2 * LG * LDR;
-      const double* sdLeg = sLeg + LG * LDR;
-      wait(bar_leg + b, n_leg[b]);
-      if (tid == 0) issue_leg((g + 1) % H::NGRP, b ^ 1);
-      i_leg[b ^ 1]++;
-      __syncthreads();
-      for (int itm = warp; itm < 2 * F0; itm += 8) {
-        const int k = itm >> 1, which = itm & 1;
-        const int c0 = sBo[k], c1 = sBo[k + 1];
-        const double* Lp = (which ? sdLeg : sLeg) + grow * LDR + c0 + gcol;
-        const double* Rr = sR + grow * LDR + c0 + gcol;
-        double e0 = 0.0, e1 = 0.0;
+    // items (Fourier block k, value/derivative, latitude group), no barrier between them
+    for (int itm = warp; itm < 2 * F0 * H::NGRP; itm += NWARP) {
+      const int g = itm / (2 * F0), kw = itm - g * 2 * F0;
+      const int k = kw >> 1, which = kw & 1;
+      const int lat0 = g * LG, nlat = min(LG, L1 - lat0);
+      const int c0 = sBo[k], c1 = sBo[k + 1];
+      const int lrow = lat0 + (grow < nlat ? grow : 0);
+      const double* Rr = sR + grow * LDR + c0 + gcol;
+      double e0 = 0.0, e1 = 0.0;
+      if (k == 0) {
+        const double* Lp = sT0 + (which * L1 + lrow) * LD0 + gcol;
+        for (int ks = 0; 4 * ks < M0; ks++) {
+          const double a = grow < nlat ? Lp[4 * ks] : 0.0;
+          const double bb = (grow < 3 && 4 * ks + gcol < M0) ? Rr[4 * ks] : 0.0;
+          dmma(e0, e1, a, bb);
+        }
+      } else {
+        const float* Lp = sTF + (which * L1 + lrow) * LDF + c0 + gcol;
         for (int ks = 0; 4 * ks < c1 - c0; ks++) {
           const int c = c0 + 4 * ks + gcol;
-          const double a = grow < nlat ? Lp[4 * ks] : 0.0;
+          const double a = grow < nlat ? (double)Lp[4 * ks] : 0.0;
           const double bb = (grow < 3 && c < c1) ? Rr[4 * ks] : 0.0;
           dmma(e0, e1, a, bb);
         }
-        if (grow < nlat) {
-          const int lat = lat0 + grow;
-          const int h = 2 * lat > H::P1 ? 1 : 0;  // hemisphere: the pole target it is centred on
+      }
+      if (grow < nlat) {
+        const int lat = lat0 + grow;
+        const int h = 2 * lat > H::P1 ? 1 : 0;  // hemisphere: the pole target it is centred on
 #pragma unroll
-          for (int q = 0; q < 2; q++) {
-            const int d = 2 * gcol + q;
-            if (d < 3) {
-              double v = q ? e1 : e0;
-              if (!which && k == 0) v -= cen[h * 3 + d] / mf00;
-              const int row = lat < 32 ? d * 32 + lat : 96 + d;
-              tc::store_split3(which ? sdA : sA, H::SZ_A, tc::umma_off(row, k, F0), v);
-            }
+        for (int q = 0; q < 2; q++) {
+          const int d = 2 * gcol + q;
+          if (d < 3) {
+            double v = q ? e1 : e0;
+            if (!which && k == 0) v -= cen[h * 3 + d] / mf00;
+            const int row = lat < 32 ? d * 32 + lat : 96 + d;
+            tc::store_split3(which ? sdA : sA, H::SZ_A, tc::umma_off(row, k, F0), (float)v);
           }
         }
       }
-      __syncthreads();
     }
     // ---- GEMM 1 on the tensor cores ------------------------------------------------------
     tc::fence_async_smem();
@@ -729,17 +740,11 @@ __global__ void __launch_bounds__(256, 1) k_build_ring_tc(const double* __restri
       for (int pr = 0; pr < 6; pr++) {
         const int i = tc::kSplitI[pr], j = tc::kSplitJ[pr];
         for (int s = 0; s < F0 / 16; s++) {
+          const uint64_t db = tc::umma_desc(tc::saddr(sB12 + j * H::SZ_B12) + s * 256, 128, SBO);
           const uint64_t da = tc::umma_desc(tc::saddr(sA + i * H::SZ_A) + s * 256, 128, SBO);
-          const uint64_t db = tc::umma_desc(tc::saddr(sB12 + j * H::SZ_B12) + s * 256, 128, SBO);
           tc::mma_bf16(tmem + H::COL_X, da, db, id128, (pr | s) ? 1u : 0u);
-        }
-      }
-      for (int pr = 0; pr < 6; pr++) {
-        const int i = tc::kSplitI[pr], j = tc::kSplitJ[pr];
-        for (int s = 0; s < F0 / 16; s++) {
-          const uint64_t da = tc::umma_desc(tc::saddr(sdA + i * H::SZ_A) + s * 256, 128, SBO);
-          const uint64_t db = tc::umma_desc(tc::saddr(sB12 + j * H::SZ_B12) + s * 256, 128, SBO);
-          tc::mma_bf16(tmem + H::COL_XP, da, db, id64, (pr | s) ? 1u : 0u);
+          const uint64_t dd = tc::umma_desc(tc::saddr(sdA + i * H::SZ_A) + s * 256, 128, SBO);
+          tc::mma_bf16(tmem + H::COL_XP, dd, db, id64, (pr | s) ? 1u : 0u);
         }
       }
       tc::mma_commit(bar_mma1);
@@ -750,35 +755,26 @@ __global__ void __launch_bounds__(256, 1) k_build_ring_tc(const double* __restri
     tc::tc_after_sync();
     // ---- per chunk of longitudes: kernel values and GEMM 2 ------------------------------
     for (int ch = 0; ch < H::NCH && ok; ch++) {
-      const int kb = ch & 1;
-      unsigned char* sK = smem + (kb ? H::OFF_K1 : H::OFF_K0);
-      // (a) surfaces of the chunk: TMEM -> shared (warp quarter q reads lanes 32q..32q+31)
-      {
-        const int q = warp & 3;
-        const int row = 32 * q + lane;
+      // (a) surfaces of the chunk: TMEM -> shared; warp w reads lane quarter w % 4, the
+      // variable w / 4 (X, X_theta, X_phi)
+      if (warp < 12) {
+        const int q = warp & 3, var = warp >> 2;
         const int d = q < 3 ? q : lane, lat = q < 3 ? lane : 32;
         const bool live = q < 3 || lane < 3;
         float v[16];
-        const uint32_t lanes = (uint32_t)(32 * q) << 16;
-        if (warp < 4) {
-          tc::tmem_ld16(tmem + lanes + H::COL_X + ch * H::JC, v);
-          if (live)
-            for (int jj = 0; jj < H::JC; jj++) sXs[(0 * 3 + d) * L1 * H::SXS_LD + lat * H::SXS_LD + jj] = v[jj];
-          tc::tmem_ld16(tmem + lanes + H::COL_XT + ch * H::JC, v);
-          if (live)
-            for (int jj = 0; jj < H::JC; jj++) sXs[(1 * 3 + d) * L1 * H::SXS_LD + lat * H::SXS_LD + jj] = v[jj];
-        } else {
-          tc::tmem_ld16(tmem + lanes + H::COL_XP + ch * H::JC, v);
-          if (live)
-            for (int jj = 0; jj < H::JC; jj++) sXs[(2 * 3 + d) * L1 * H::SXS_LD + lat * H::SXS_LD + jj] = v[jj];
+        const int col = (var == 0 ? H::COL_X : var == 1 ? H::COL_XT : H::COL_XP) + ch * H::JC;
+        tc::tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + col, v);
+        if (live) {
+          float* o = sXs + (var * 3 + d) * L1 * H::SXS_LD + lat * H::SXS_LD;
+#pragma unroll
+          for (int jj = 0; jj < H::JC; jj++) o[jj] = v[jj];
         }
-        (void)row;
       }
-      if (ch >= 2) wait(bar_k + kb, n_k[kb]);  // the MMAs of chunk ch - 2 have read this buffer
       tc::tc_before_sync();
+      if (ch > 0) wait(bar_k, n_k);  // GEMM 2 of the previous chunk has read the chunk buffer
       if (!(ok = sync_ok())) break;
       // (b) singular kernel (FP64) at the chunk's 33 x 16 points -> split BF16 chunk operand
-      for (int pnt = tid; pnt < L1 * H::JC; pnt += 256) {
+      for (int pnt = tid; pnt < L1 * H::JC; pnt += NTHR) {
         const int lat = pnt / H::JC, jj = pnt - lat * H::JC;
         const int h = 2 * lat > H::P1 ? 1 : 0;
         const float* xs = sXs + lat * H::SXS_LD + jj;
@@ -810,7 +806,7 @@ __global__ void __launch_bounds__(256, 1) k_build_ring_tc(const double* __restri
         if (lat < 32) {
 #pragma unroll
           for (int comp = 0; comp < 12; comp++)
-            tc::store_split3(sK, H::SZ_K, tc::umma_off(comp * 32 + lat, jj, H::JC), kv[comp]);
+            tc::store_split3(sK, H::SZ_K, tc::umma_off(comp * 32 + lat, jj, H::JC), (float)kv[comp]);
         } else {
 #pragma unroll
           for (int comp = 0; comp < 12; comp++) sK32[comp * N1 + ch * H::JC + jj] = kv[comp];
@@ -821,37 +817,36 @@ __global__ void __launch_bounds__(256, 1) k_build_ring_tc(const double* __restri
       if (tid == 0) {
         tc::tc_after_sync();
         constexpr uint32_t id32 = tc::idesc_bf16(128, F0);
-        for (int tt = 0; tt < 3; tt++) {
-          for (int pr = 0; pr < 6; pr++) {
-            const int i = tc::kSplitI[pr], j = tc::kSplitJ[pr];
+        for (int pr = 0; pr < 6; pr++) {
+          const int i = tc::kSplitI[pr], j = tc::kSplitJ[pr];
+          const uint64_t db = tc::umma_desc(tc::saddr(sBT + j * H::SZ_BT) + ch * (H::JC / 8) * 128, 128, N1 * 16);
+          for (int tt = 0; tt < 3; tt++) {
             const uint64_t da = tc::umma_desc(tc::saddr(sK + i * H::SZ_K) + tt * 128 * H::JC * 2, 128, H::JC * 16);
-            const uint64_t db = tc::umma_desc(tc::saddr(sBT + j * H::SZ_BT) + ch * (H::JC / 8) * 128, 128, N1 * 16);
             tc::mma_bf16(tmem + H::COL_T + tt * F0, da, db, id32, (ch | pr) ? 1u : 0u);
           }
         }
-        tc::mma_commit(bar_k + kb);
+        tc::mma_commit(bar_k);
       }
-      i_k[kb]++;
+      i_k++;
     }
     if (!ok) break;
-    // the last two chunks' MMAs (buffers 0 and 1) before TMEM is read and the buffers reused
-    wait(bar_k + 0, n_k[0]);
-    wait(bar_k + 1, n_k[1]);
+    wait(bar_k, n_k);  // the last chunk's GEMM 2 before TMEM is read and the region reused
     if (!(ok = sync_ok())) break;
     tc::tc_after_sync();
     // ---- transposed-DFT result -> shared (FP32); the last latitude in FP64 ----------------
-    if (warp < 4) {
-      const int q = warp;
+    if (warp < 12) {
+      const int q = warp & 3, tt = warp >> 2;
+      const int comp = 4 * tt + q, lat = lane;  // row comp * 32 + lat of tile tt
       float v[16];
-      for (int tt = 0; tt < 3; tt++) {
-        const int comp = 4 * tt + q, lat = lane;  // row comp * 32 + lat of tile tt
-        for (int half = 0; half < 2; half++) {
-          tc::tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + H::COL_T + tt * F0 + half * 16, v);
-          for (int x = 0; x < 16; x++) sC[(lat * 12 + comp) * H::LDC + half * 16 + x] = v[x];
-        }
+#pragma unroll
+      for (int half = 0; half < 2; half++) {
+        tc::tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + H::COL_T + tt * F0 + half * 16, v);
+        float* o = sC + (lat * 12 + comp) * H::LDC + half * 16;
+#pragma unroll
+        for (int x = 0; x < 16; x++) o[x] = v[x];
       }
     } else {
-      for (int o = tid - 128; o < 12 * F0; o += 128) {
+      for (int o = tid - 12 * 32; o < 12 * F0; o += NTHR - 12 * 32) {
         const int comp = o / F0, jf = o - comp * F0;
         const double* kr = sK32 + comp * N1;
         const double* mf = T.syn1_four + jf * N1;
@@ -862,36 +857,31 @@ __global__ void __launch_bounds__(256, 1) k_build_ring_tc(const double* __restri
     }
     tc::tc_before_sync();
     __syncthreads();
-    // ---- pass 2: transposed Legendre sums (FP64 tensor cores) ---------------------------
-    double acc[G::QMAX][2];
+    // ---- pass 2: transposed Legendre sums (FP64 tensor cores), no barrier inside ---------
+    double acc[H::QMAX][2];
 #pragma unroll
-    for (int q = 0; q < G::QMAX; q++) acc[q][0] = acc[q][1] = 0.0;
-    for (int g = 0; g < H::NGRP; g++, gi++) {
-      const int b = gi & 1, lat0 = g * LG, nlat = min(LG, L1 - lat0);
-      const double* sLeg = sLegb + b * 2 * LG * LDR;
-      wait(bar_leg + b, n_leg[b]);
-      if (tid == 0) issue_leg((g + 1) % H::NGRP, b ^ 1);
-      i_leg[b ^ 1]++;
-      if (!(ok = sync_ok())) break;
+    for (int q = 0; q < H::QMAX; q++) acc[q][0] = acc[q][1] = 0.0;
+    for (int g = 0; g < H::NGRP; g++) {
+      const int lat0 = g * LG, nlat = min(LG, L1 - lat0);
+      const int l = gcol, lat = lat0 + (l < nlat ? l : 0);
 #pragma unroll
-      for (int q = 0; q < G::QMAX; q++) {
-        const int tile = warp + 8 * q;
+      for (int q = 0; q < H::QMAX; q++) {
+        const int tile = warp + NWARP * q;
         if (tile < 2 * G::NTT) {
           const int mt = tile / G::NTT;
           const uchar2 kt = sTl[tile - mt * G::NTT];
           const int k = kt.x, c0 = sBo[k], c1 = sBo[k + 1];
-          const int comp = mt * 8 + grow, l = gcol, c = c0 + kt.y * 8 + grow;
-          const double a = (comp < 12 && l < nlat) ? (double)sC[((lat0 + l) * 12 + comp) * H::LDC + k] : 0.0;
-          const double bb = (l < nlat && c < c1) ? sLeg[l * LDR + c] : 0.0;
+          const int comp = mt * 8 + grow, c = c0 + kt.y * 8 + grow;
+          const double a = (comp < 12 && l < nlat) ? (double)sC[(lat * 12 + comp) * H::LDC + k] : 0.0;
+          double bb = 0.0;
+          if (l < nlat && c < c1) bb = k == 0 ? sT0[lat * LD0 + c] : (double)sTF[lat * LDF + c];
           dmma(acc[q][0], acc[q][1], a, bb);
         }
       }
-      __syncthreads();
     }
-    if (!ok) break;
 #pragma unroll
-    for (int q = 0; q < G::QMAX; q++) {
-      const int tile = warp + 8 * q;
+    for (int q = 0; q < H::QMAX; q++) {
+      const int tile = warp + NWARP * q;
       if (tile < 2 * G::NTT) {
         const int mt = tile / G::NTT;
         const uchar2 kt = sTl[tile - mt * G::NTT];
@@ -903,10 +893,10 @@ __global__ void __launch_bounds__(256, 1) k_build_ring_tc(const double* __restri
         }
       }
     }
+    __syncthreads();  // pass 2's reads of C before the next rotation's pass 1 overwrites it
   }
-  // ---- drain: copies and MMAs issued but not waited for (the Legendre slice prefetched
-  // past the last rotation; after an abort, whatever was in flight), each wait bounded;
-  // then TMEM is freed ------------------------------------------------------------------
+  // ---- drain: copies and MMAs issued but not waited for (after an abort, whatever was in
+  // flight), each wait bounded; then TMEM is freed -------------------------------------
   {
     bool drained = true;
     auto drain = [&](uint64_t* bar, uint32_t& waited, uint32_t issued) {
@@ -918,11 +908,8 @@ __global__ void __launch_bounds__(256, 1) k_build_ring_tc(const double* __restri
         waited++;
       }
     };
-    for (int b = 0; b < 2; b++) {
-      drain(bar_r + b, n_r[b], i_r[b]);
-      drain(bar_leg + b, n_leg[b], i_leg[b]);
-      drain(bar_k + b, n_k[b], i_k[b]);
-    }
+    for (int b = 0; b < 2; b++) drain(bar_r + b, n_r[b], i_r[b]);
+    drain(bar_k, n_k, i_k);
     drain(bar_mma1, n_mma1, i_mma1);
   }
   tc::tc_before_sync();
@@ -947,7 +934,7 @@ int launch_build_ring_tc(const double* R, long nrot, const DevTables& T, double*
   VES3D_CK(cudaGetDevice(&dev));
   VES3D_CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   const long grid = std::min(nrot, (long)nsm);
-  k_build_ring_tc<16><<<(unsigned)grid, 256, H::SMEM, st>>>(R, T, C, nrot);
+  k_build_ring_tc<16><<<(unsigned)grid, H::NTHR, H::SMEM, st>>>(R, T, C, nrot);
   VES3D_LAUNCHED();
   return VES3D_OK;
 }
