@@ -363,23 +363,24 @@ static int launch_ring(const double* R, long nrot, const DevTables& T, double* C
 // FP64), so that r = target - source near the pole -- where the singular kernel
 // amplifies relative errors of the positions by |X| / |r| -- carries the GEMM's relative
 // error of |r|, not of |X| (which includes the vesicle's centre). Kept in FP64: the
-// Legendre synthesis and the transposed Legendre sums (FP64 tensor cores, mma.sync
-// m8n8k4), the pole targets, the singular kernel and its quadrature weights.
+// Legendre synthesis and the transposed Legendre sums (FP64 FMA: their per-block shapes
+// fill an m8n8k4 tile to a fifth), the pole targets, the singular kernel and its
+// quadrature weights.
 //
 // One CTA of 16 warps per SM, persistent over rotations, with the Legendre tables resident
 // in shared memory (the m = 0 block in FP64: it carries the vesicle's position; the other
 // blocks in FP32: they multiply shape-sized coefficients) and the DFT tables as split BF16
 // operands. Per rotation:
 //   R (FP64, bulk-copied by TMA, the next rotation's prefetched)
-//   -> Legendre synthesis (FP64 tensor cores) -> A, dA split to BF16 in shared memory
+//   -> Legendre synthesis (FP64 FMA) -> A, dA split to BF16 in shared memory
 //      (UMMA K-major layout, no swizzle)
 //   -> GEMM 1: [X | X_theta] = A [Mf | dMf], X_phi = dA Mf         (TMEM cols 0..191)
 //   -> per chunk of 16 longitudes: TMEM -> shared, FP64 kernel at 33 x 16 points,
 //      12 components split to BF16 -> GEMM 2 accumulating C = K Mf^T   (TMEM 192..287),
 //      overlapping the next chunk's TMEM reads
-//   -> TMEM -> shared (FP32), transposed Legendre sums (FP64 tensor cores) -> C [12][Nc].
+//   -> TMEM -> shared (FP32), transposed Legendre sums (FP64 FMA) -> C [12][Nc].
 // The last upsampled latitude (p1 + 1 = 33 rows do not fit the 32 lanes of a warp
-// quarter) takes its transposed DFT in FP64 on the CUDA cores.
+// quarter) takes its kernel and transposed DFT in FP64 on the CUDA cores.
 //
 // Every wait is bounded (about a second of %globaltimer); a wait that runs out sets
 // g_tc_build_error, the CTA stops, waits (bounded) for its copies and MMAs, frees its
@@ -511,23 +512,22 @@ struct RingTcCfg {
   static constexpr int P1 = 2 * P0, L1 = P1 + 1, F0 = 2 * P0, N1 = 2 * P1, NC = P0 * (P0 + 2);
   static_assert(P0 == 16, "the tensor-core ring is laid out for p = 16 (33 upsampled latitudes)");
   static constexpr int NTHR = 512, NWARP = NTHR / 32;
-  static constexpr int LG = 4, NGRP = (L1 + LG - 1) / LG;
-  static constexpr int LDR = G::LDR;     // FP64 coefficient rows of R (4 mod 16 doubles)
+  static constexpr int LDR = G::LDR;     // FP64 coefficient rows of R
   static constexpr int M0 = P0 + 1;      // the m = 0 Fourier block: coefficients 0..P0
-  static constexpr int LD0 = 20;         // FP64 m = 0 table rows (>= M0 + 3, 4 mod 16)
-  static constexpr int LDF = 292;        // FP32 table rows (>= NC + 3, 4 mod 32 floats)
+  static constexpr int LD0 = M0;         // FP64 m = 0 table rows (odd: conflict-free columns)
+  static constexpr int LDF = NC + 1;     // FP32 table rows (odd)
   static constexpr int LDC = F0 + 5;     // FP32 rows of the transposed-DFT result
   static constexpr int JC = 16;          // longitudes per kernel chunk (K of one GEMM-2 step)
   static constexpr int NCH = N1 / JC;    // chunks per rotation
   static constexpr int KROWS = 12 * 32;  // GEMM-2 rows (component, latitude < 32): 3 M-tiles
-  static constexpr int QMAX = (2 * G::NTT + NWARP - 1) / NWARP;  // transposed-Legendre tiles per warp
+  static_assert(32 * JC == NTHR, "one chunk point per thread");
   // operand sizes (bytes, one split)
   static constexpr int SZ_A = 128 * F0 * 2;       // A or dA: 128 rows x K = F0
   static constexpr int SZ_B12 = 128 * F0 * 2;     // [Mf | dMf]^T: N = 2 N1 = 128 rows x K = F0
   static constexpr int SZ_BT = F0 * N1 * 2;       // Mf: N = F0 rows x K = N1
   static constexpr int SZ_K = KROWS * JC * 2;     // one chunk of kernel values
-  static constexpr int SXS_LD = JC + 1;           // FP32 surface values [9][lat][SXS_LD]
-  static constexpr int SZ_XS = 9 * L1 * SXS_LD * 4;
+  static constexpr int SXS_LD = JC + 1;           // FP32 surface values [9][32 lat][SXS_LD]
+  static constexpr int SZ_XS = 9 * 32 * SXS_LD * 4;
   static constexpr int SZ_C = L1 * 12 * LDC * 4;  // FP32 transposed-DFT result [lat][comp][LDC]
   // byte offsets; the union region U holds A/dA (pass 1 -> GEMM 1), then the chunk buffer
   // and the chunk's surface values (-> GEMM 2), then C (-> pass 2)
@@ -541,13 +541,14 @@ struct RingTcCfg {
   static constexpr int OFF_R = (OFF_U + U_SZ + 127) / 128 * 128;  // 2 x [3][LDR] FP64
   static constexpr int OFF_T0 = OFF_R + 2 * 3 * LDR * 8;          // FP64 m = 0 tables: leg, dleg [L1][LD0]
   static constexpr int OFF_TF = OFF_T0 + 2 * L1 * LD0 * 8;        // FP32 tables: leg, dleg [L1][LDF]
-  static constexpr int OFF_K32 = OFF_TF + 2 * L1 * LDF * 4;       // [12][N1] FP64 (last latitude)
+  static constexpr int OFF_X32 = OFF_TF + (2 * L1 * LDF * 4 + 7) / 8 * 8;  // last latitude: [9][N1] FP32
+  static constexpr int OFF_K32 = OFF_X32 + 9 * N1 * 4;            // its kernel values [12][N1] FP64
   static constexpr int OFF_TRG = OFF_K32 + 12 * N1 * 8;
   static constexpr int OFF_CEN = OFF_TRG + 6 * 8;
   static constexpr int OFF_SW = OFF_CEN + 6 * 8;
   static constexpr int OFF_BO = OFF_SW + L1 * 8;
-  static constexpr int OFF_TL = OFF_BO + ((F0 + 1) * 4 + 7) / 8 * 8;
-  static constexpr int OFF_BAR = OFF_TL + (G::NTT * 2 + 7) / 8 * 8;
+  static constexpr int OFF_JF = OFF_BO + ((F0 + 1) * 4 + 7) / 8 * 8;   // Fourier block of each coefficient
+  static constexpr int OFF_BAR = OFF_JF + (NC + 7) / 8 * 8;
   static constexpr int NBAR = 4;  // GEMM 1, GEMM 2, R buffers 0 and 1
   static constexpr int OFF_TMEM = OFF_BAR + NBAR * 8;
   static constexpr int SMEM = OFF_TMEM + 16;
@@ -556,6 +557,33 @@ struct RingTcCfg {
   static_assert(COL_T + 3 * F0 <= (int)TMEM_COLS, "TMEM columns");
   static_assert(SMEM <= 227 * 1024, "shared memory");
 };
+
+// The singular kernel (FP64) of one pole target t at one upsampled point: positions D
+// relative to the centre of the point's hemisphere h, the tangents, the latitude's
+// singular weight; out[6] the weighted single-layer tensor (src/SphericalHarmonics.cc:989-1068).
+__device__ __forceinline__ void ring_kernel_sl(double px, double py, double pz, double area, const double* trg,
+                                               const double* cen, int h, int t, double w, double* out) {
+  // r = target_t - (centre_h + D) with target_t - centre_h exact (0 when t == h)
+  const double dx = (trg[t] - cen[h * 3]) - px, dy = (trg[2 + t] - cen[h * 3 + 1]) - py,
+               dz = (trg[4 + t] - cen[h * 3 + 2]) - pz;
+  const double r2 = dx * dx + dy * dy + dz * dz;
+  double rinv = rsqrt_f64(r2);
+  if (r2 <= 2.220446049250313e-16) rinv = 0.0;
+  const double a1 = kInv8Pi * w * area * rinv;
+  const double a2 = a1 * rinv * rinv;
+  out[0] = a1 + dx * dx * a2;
+  out[1] = dx * dy * a2;
+  out[2] = dx * dz * a2;
+  out[3] = a1 + dy * dy * a2;
+  out[4] = dy * dz * a2;
+  out[5] = a1 + dz * dz * a2;
+}
+
+__device__ __forceinline__ double area_of(double ax, double ay, double az, double bx, double by, double bz) {
+  const double nx = ay * bz - az * by, ny = az * bx - ax * bz, nz = ax * by - ay * bx;
+  const double n2 = nx * nx + ny * ny + nz * nz;
+  return n2 * rsqrt_f64(n2);  // |X_theta x X_phi| > 0 on the upsampled grid
+}
 
 template <int P0>
 __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restrict__ R, DevTables T,
@@ -573,12 +601,13 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
   double* sRb = reinterpret_cast<double*>(smem + H::OFF_R);
   double* sT0 = reinterpret_cast<double*>(smem + H::OFF_T0);  // leg, then dleg: [L1][LD0]
   float* sTF = reinterpret_cast<float*>(smem + H::OFF_TF);    // leg, then dleg: [L1][LDF]
+  float* sX32 = reinterpret_cast<float*>(smem + H::OFF_X32);
   double* sK32 = reinterpret_cast<double*>(smem + H::OFF_K32);
   double* trg = reinterpret_cast<double*>(smem + H::OFF_TRG);
   double* cen = reinterpret_cast<double*>(smem + H::OFF_CEN);
   double* sSw = reinterpret_cast<double*>(smem + H::OFF_SW);
   int* sBo = reinterpret_cast<int*>(smem + H::OFF_BO);
-  uchar2* sTl = reinterpret_cast<uchar2*>(smem + H::OFF_TL);
+  unsigned char* sJf = smem + H::OFF_JF;
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + H::OFF_BAR);
   uint64_t* bar_mma1 = bars;     // GEMM 1 done
   uint64_t* bar_k = bars + 1;    // GEMM 2 of the last chunk done (the chunk buffer is free)
@@ -586,11 +615,10 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
   uint32_t* s_tmem = reinterpret_cast<uint32_t*>(smem + H::OFF_TMEM);
   int* s_abort = reinterpret_cast<int*>(smem + H::OFF_TMEM + 4);
 
-  constexpr int NTHR = H::NTHR, NWARP = H::NWARP;
+  constexpr int NTHR = H::NTHR;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int grow = lane >> 2, gcol = lane & 3;
-  constexpr int NC = H::NC, LDR = H::LDR, F0 = H::F0, N1 = H::N1, L1 = H::L1, LG = H::LG, M0 = H::M0;
-  constexpr int LD0 = H::LD0, LDF = H::LDF;
+  constexpr int NC = H::NC, LDR = H::LDR, F0 = H::F0, N1 = H::N1, L1 = H::L1, M0 = H::M0;
+  constexpr int LD0 = H::LD0, LDF = H::LDF, LDC = H::LDC;
 
   // ---- set-up: TMEM, barriers, constant operands and tables ---------------------------
   if (warp == 0) {
@@ -616,28 +644,18 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
   }
   // Legendre tables resident for the CTA's life: the m = 0 block in FP64 (it carries the
   // vesicle's position), the other blocks in FP32 (their values multiply shape-sized
-  // coefficients; measured no change in the self velocity's error); zero K padding
+  // coefficients; no change in the self velocity's error measured)
   for (int i = tid; i < 2 * L1 * LD0; i += NTHR) {
     const int tb = i / (L1 * LD0), r = i - tb * L1 * LD0, lat = r / LD0, c = r - lat * LD0;
-    const double* src = tb ? T.syn1_dleg_t : T.syn1_leg_t;
-    sT0[i] = c < M0 ? __ldg(src + (long)lat * NC + c) : 0.0;
+    sT0[i] = __ldg((tb ? T.syn1_dleg_t : T.syn1_leg_t) + (long)lat * NC + c);
   }
   for (int i = tid; i < 2 * L1 * LDF; i += NTHR) {
     const int tb = i / (L1 * LDF), r = i - tb * L1 * LDF, lat = r / LDF, c = r - lat * LDF;
-    const double* src = tb ? T.syn1_dleg_t : T.syn1_leg_t;
-    sTF[i] = (c >= M0 && c < NC) ? (float)__ldg(src + (long)lat * NC + c) : 0.f;
+    sTF[i] = c < NC ? (float)__ldg((tb ? T.syn1_dleg_t : T.syn1_leg_t) + (long)lat * NC + c) : 0.f;
   }
   for (int i = tid; i < L1; i += NTHR) sSw[i] = __ldg(T.sing_w + i);
   for (int i = tid; i <= F0; i += NTHR) sBo[i] = __ldg(T.blk_off + i);
-  if (tid == 0) {
-    int j = 0;
-    for (int k = 0; k < F0; k++) {
-      const int len = __ldg(T.blk_off + k + 1) - __ldg(T.blk_off + k);
-      for (int nt = 0; nt * 8 < len && j < G::NTT; nt++) sTl[j++] = make_uchar2((unsigned char)k, (unsigned char)nt);
-    }
-  }
-  // K padding of R (columns NC..LDR-1): zeros, never overwritten by the copies
-  for (int i = tid; i < 2 * 3 * (LDR - NC); i += NTHR) sRb[(i / (LDR - NC)) * LDR + NC + i % (LDR - NC)] = 0.0;
+  for (int i = tid; i < NC; i += NTHR) sJf[i] = (unsigned char)__ldg(T.jf_of_coef + i);
   tc::fence_async_smem();
   tc::tc_before_sync();
   __syncthreads();
@@ -689,46 +707,44 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
     __syncthreads();
     if (tid < 6) cen[tid] = trg[(tid % 3) * 2 + tid / 3];  // cen[h * 3 + d]: target of hemisphere h
     __syncthreads();
-    // ---- pass 1: Legendre synthesis (FP64 tensor cores) -> split BF16 A, dA ------------
-    // items (Fourier block k, value/derivative, latitude group), no barrier between them
-    for (int itm = warp; itm < 2 * F0 * H::NGRP; itm += NWARP) {
-      const int g = itm / (2 * F0), kw = itm - g * 2 * F0;
-      const int k = kw >> 1, which = kw & 1;
-      const int lat0 = g * LG, nlat = min(LG, L1 - lat0);
-      const int c0 = sBo[k], c1 = sBo[k + 1];
-      const int lrow = lat0 + (grow < nlat ? grow : 0);
-      const double* Rr = sR + grow * LDR + c0 + gcol;
-      double e0 = 0.0, e1 = 0.0;
+    // ---- pass 1: Legendre synthesis (FP64 FMA) -> split BF16 A, dA -----------------------
+    // item (Fourier block k, latitude): a warp takes 32 latitudes of one block (the same
+    // trip count; conflict-free table columns), the last latitude of every block follows
+    for (int itm = tid; itm < F0 * L1; itm += NTHR) {
+      const int k = itm < F0 * 32 ? itm >> 5 : itm - F0 * 32;
+      const int lat = itm < F0 * 32 ? itm & 31 : 32;
+      double e0 = 0.0, e1 = 0.0, e2 = 0.0, f0 = 0.0, f1 = 0.0, f2 = 0.0;
       if (k == 0) {
-        const double* Lp = sT0 + (which * L1 + lrow) * LD0 + gcol;
-        for (int ks = 0; 4 * ks < M0; ks++) {
-          const double a = grow < nlat ? Lp[4 * ks] : 0.0;
-          const double bb = (grow < 3 && 4 * ks + gcol < M0) ? Rr[4 * ks] : 0.0;
-          dmma(e0, e1, a, bb);
+        const double* L = sT0 + lat * LD0;
+        const double* dL = sT0 + (L1 + lat) * LD0;
+        for (int c = 0; c < M0; c++) {
+          const double l = L[c], dl = dL[c], r0 = sR[c], r1 = sR[LDR + c], r2 = sR[2 * LDR + c];
+          e0 = fma(l, r0, e0); e1 = fma(l, r1, e1); e2 = fma(l, r2, e2);
+          f0 = fma(dl, r0, f0); f1 = fma(dl, r1, f1); f2 = fma(dl, r2, f2);
         }
+        // centred on the hemisphere's pole target: X - c enters through the m = 0 column
+        const int h = 2 * lat > H::P1 ? 1 : 0;
+        e0 -= cen[h * 3] / mf00;
+        e1 -= cen[h * 3 + 1] / mf00;
+        e2 -= cen[h * 3 + 2] / mf00;
       } else {
-        const float* Lp = sTF + (which * L1 + lrow) * LDF + c0 + gcol;
-        for (int ks = 0; 4 * ks < c1 - c0; ks++) {
-          const int c = c0 + 4 * ks + gcol;
-          const double a = grow < nlat ? (double)Lp[4 * ks] : 0.0;
-          const double bb = (grow < 3 && c < c1) ? Rr[4 * ks] : 0.0;
-          dmma(e0, e1, a, bb);
+        const float* L = sTF + lat * LDF;
+        const float* dL = sTF + (L1 + lat) * LDF;
+        const int c1 = sBo[k + 1];
+        for (int c = sBo[k]; c < c1; c++) {
+          const double l = L[c], dl = dL[c], r0 = sR[c], r1 = sR[LDR + c], r2 = sR[2 * LDR + c];
+          e0 = fma(l, r0, e0); e1 = fma(l, r1, e1); e2 = fma(l, r2, e2);
+          f0 = fma(dl, r0, f0); f1 = fma(dl, r1, f1); f2 = fma(dl, r2, f2);
         }
       }
-      if (grow < nlat) {
-        const int lat = lat0 + grow;
-        const int h = 2 * lat > H::P1 ? 1 : 0;  // hemisphere: the pole target it is centred on
-#pragma unroll
-        for (int q = 0; q < 2; q++) {
-          const int d = 2 * gcol + q;
-          if (d < 3) {
-            double v = q ? e1 : e0;
-            if (!which && k == 0) v -= cen[h * 3 + d] / mf00;
-            const int row = lat < 32 ? d * 32 + lat : 96 + d;
-            tc::store_split3(which ? sdA : sA, H::SZ_A, tc::umma_off(row, k, F0), (float)v);
-          }
-        }
-      }
+      const int rb0 = lat < 32 ? lat : 96;  // row of d = 0; d adds 32 (lat < 32) or 1 (lat 32)
+      const int rs = lat < 32 ? 32 : 1;
+      tc::store_split3(sA, H::SZ_A, tc::umma_off(rb0, k, F0), (float)e0);
+      tc::store_split3(sA, H::SZ_A, tc::umma_off(rb0 + rs, k, F0), (float)e1);
+      tc::store_split3(sA, H::SZ_A, tc::umma_off(rb0 + 2 * rs, k, F0), (float)e2);
+      tc::store_split3(sdA, H::SZ_A, tc::umma_off(rb0, k, F0), (float)f0);
+      tc::store_split3(sdA, H::SZ_A, tc::umma_off(rb0 + rs, k, F0), (float)f1);
+      tc::store_split3(sdA, H::SZ_A, tc::umma_off(rb0 + 2 * rs, k, F0), (float)f2);
     }
     // ---- GEMM 1 on the tensor cores ------------------------------------------------------
     tc::fence_async_smem();
@@ -755,17 +771,19 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
     tc::tc_after_sync();
     // ---- per chunk of longitudes: kernel values and GEMM 2 ------------------------------
     for (int ch = 0; ch < H::NCH && ok; ch++) {
-      // (a) surfaces of the chunk: TMEM -> shared; warp w reads lane quarter w % 4, the
-      // variable w / 4 (X, X_theta, X_phi)
+      // (a) surfaces of the chunk: TMEM -> shared; warp w reads lane quarter w % 4 of the
+      // variable w / 4 (X, X_theta, X_phi); quarter 3 holds the last latitude (lanes 0..2)
       if (warp < 12) {
         const int q = warp & 3, var = warp >> 2;
-        const int d = q < 3 ? q : lane, lat = q < 3 ? lane : 32;
-        const bool live = q < 3 || lane < 3;
         float v[16];
         const int col = (var == 0 ? H::COL_X : var == 1 ? H::COL_XT : H::COL_XP) + ch * H::JC;
         tc::tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + col, v);
-        if (live) {
-          float* o = sXs + (var * 3 + d) * L1 * H::SXS_LD + lat * H::SXS_LD;
+        if (q < 3) {
+          float* o = sXs + ((var * 3 + q) * 32 + lane) * H::SXS_LD;
+#pragma unroll
+          for (int jj = 0; jj < H::JC; jj++) o[jj] = v[jj];
+        } else if (lane < 3) {
+          float* o = sX32 + (var * 3 + lane) * N1 + ch * H::JC;
 #pragma unroll
           for (int jj = 0; jj < H::JC; jj++) o[jj] = v[jj];
         }
@@ -773,43 +791,22 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
       tc::tc_before_sync();
       if (ch > 0) wait(bar_k, n_k);  // GEMM 2 of the previous chunk has read the chunk buffer
       if (!(ok = sync_ok())) break;
-      // (b) singular kernel (FP64) at the chunk's 33 x 16 points -> split BF16 chunk operand
-      for (int pnt = tid; pnt < L1 * H::JC; pnt += NTHR) {
-        const int lat = pnt / H::JC, jj = pnt - lat * H::JC;
+      // (b) singular kernel (FP64) at the chunk's 32 x 16 points (one per thread) -> split
+      // BF16 chunk operand
+      {
+        const int lat = tid >> 4, jj = tid & 15;
         const int h = 2 * lat > H::P1 ? 1 : 0;
         const float* xs = sXs + lat * H::SXS_LD + jj;
-        constexpr int VS = L1 * H::SXS_LD;
-        const double px = xs[0], py = xs[VS], pz = xs[2 * VS];  // centred on the hemisphere's target
-        const double ax = xs[3 * VS], ay = xs[4 * VS], az = xs[5 * VS];
-        const double bx = xs[6 * VS], by = xs[7 * VS], bz = xs[8 * VS];
-        const double nx = ay * bz - az * by, ny = az * bx - ax * bz, nz = ax * by - ay * bx;
-        const double n2 = nx * nx + ny * ny + nz * nz;
-        const double area = n2 * rsqrt_f64(n2);
-        double kv[12];
+        constexpr int VS = 32 * H::SXS_LD;
+        const double area = area_of(xs[3 * VS], xs[4 * VS], xs[5 * VS], xs[6 * VS], xs[7 * VS], xs[8 * VS]);
+        const double px = xs[0], py = xs[VS], pz = xs[2 * VS];
 #pragma unroll
         for (int t = 0; t < 2; t++) {
-          // r = target_t - (centre_h + D) with target_t - centre_h exact (0 when t == h)
-          const double dx = (trg[t] - cen[h * 3]) - px, dy = (trg[2 + t] - cen[h * 3 + 1]) - py,
-                       dz = (trg[4 + t] - cen[h * 3 + 2]) - pz;
-          const double r2 = dx * dx + dy * dy + dz * dz;
-          double rinv = rsqrt_f64(r2);
-          if (r2 <= 2.220446049250313e-16) rinv = 0.0;
-          const double a1 = kInv8Pi * sSw[t ? lat : H::P1 - lat] * area * rinv;
-          const double a2 = a1 * rinv * rinv;
-          kv[t * 6 + 0] = a1 + dx * dx * a2;
-          kv[t * 6 + 1] = dx * dy * a2;
-          kv[t * 6 + 2] = dx * dz * a2;
-          kv[t * 6 + 3] = a1 + dy * dy * a2;
-          kv[t * 6 + 4] = dy * dz * a2;
-          kv[t * 6 + 5] = a1 + dz * dz * a2;
-        }
-        if (lat < 32) {
+          double kv[6];
+          ring_kernel_sl(px, py, pz, area, trg, cen, h, t, sSw[t ? lat : H::P1 - lat], kv);
 #pragma unroll
-          for (int comp = 0; comp < 12; comp++)
-            tc::store_split3(sK, H::SZ_K, tc::umma_off(comp * 32 + lat, jj, H::JC), (float)kv[comp]);
-        } else {
-#pragma unroll
-          for (int comp = 0; comp < 12; comp++) sK32[comp * N1 + ch * H::JC + jj] = kv[comp];
+          for (int c = 0; c < 6; c++)
+            tc::store_split3(sK, H::SZ_K, tc::umma_off((t * 6 + c) * 32 + lat, jj, H::JC), (float)kv[c]);
         }
       }
       tc::fence_async_smem();
@@ -830,10 +827,20 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
       i_k++;
     }
     if (!ok) break;
+    // ---- the last latitude's kernel (warps 12-15, one (point, target) each) while the
+    // last GEMM 2 runs; then the transposed-DFT result -> shared (FP32) ------------------
+    if (warp >= 12) {
+      const int item = tid - 384, j = item >> 1, t = item & 1;
+      const float* xs = sX32 + j;
+      const double area = area_of(xs[3 * N1], xs[4 * N1], xs[5 * N1], xs[6 * N1], xs[7 * N1], xs[8 * N1]);
+      double kv[6];
+      ring_kernel_sl(xs[0], xs[N1], xs[2 * N1], area, trg, cen, 1, t, sSw[t ? 32 : H::P1 - 32], kv);
+#pragma unroll
+      for (int c = 0; c < 6; c++) sK32[(t * 6 + c) * N1 + j] = kv[c];
+    }
     wait(bar_k, n_k);  // the last chunk's GEMM 2 before TMEM is read and the region reused
     if (!(ok = sync_ok())) break;
     tc::tc_after_sync();
-    // ---- transposed-DFT result -> shared (FP32); the last latitude in FP64 ----------------
     if (warp < 12) {
       const int q = warp & 3, tt = warp >> 2;
       const int comp = 4 * tt + q, lat = lane;  // row comp * 32 + lat of tile tt
@@ -841,57 +848,49 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
 #pragma unroll
       for (int half = 0; half < 2; half++) {
         tc::tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + H::COL_T + tt * F0 + half * 16, v);
-        float* o = sC + (lat * 12 + comp) * H::LDC + half * 16;
+        float* o = sC + (lat * 12 + comp) * LDC + half * 16;
 #pragma unroll
         for (int x = 0; x < 16; x++) o[x] = v[x];
-      }
-    } else {
-      for (int o = tid - 12 * 32; o < 12 * F0; o += NTHR - 12 * 32) {
-        const int comp = o / F0, jf = o - comp * F0;
-        const double* kr = sK32 + comp * N1;
-        const double* mf = T.syn1_four + jf * N1;
-        double s = 0.0;
-        for (int j = 0; j < N1; j++) s = fma(kr[j], __ldg(mf + j), s);
-        sC[(32 * 12 + comp) * H::LDC + jf] = (float)s;
       }
     }
     tc::tc_before_sync();
     __syncthreads();
-    // ---- pass 2: transposed Legendre sums (FP64 tensor cores), no barrier inside ---------
-    double acc[H::QMAX][2];
-#pragma unroll
-    for (int q = 0; q < H::QMAX; q++) acc[q][0] = acc[q][1] = 0.0;
-    for (int g = 0; g < H::NGRP; g++) {
-      const int lat0 = g * LG, nlat = min(LG, L1 - lat0);
-      const int l = gcol, lat = lat0 + (l < nlat ? l : 0);
-#pragma unroll
-      for (int q = 0; q < H::QMAX; q++) {
-        const int tile = warp + NWARP * q;
-        if (tile < 2 * G::NTT) {
-          const int mt = tile / G::NTT;
-          const uchar2 kt = sTl[tile - mt * G::NTT];
-          const int k = kt.x, c0 = sBo[k], c1 = sBo[k + 1];
-          const int comp = mt * 8 + grow, c = c0 + kt.y * 8 + grow;
-          const double a = (comp < 12 && l < nlat) ? (double)sC[(lat * 12 + comp) * H::LDC + k] : 0.0;
-          double bb = 0.0;
-          if (l < nlat && c < c1) bb = k == 0 ? sT0[lat * LD0 + c] : (double)sTF[lat * LDF + c];
-          dmma(acc[q][0], acc[q][1], a, bb);
-        }
+    // the last latitude's transposed DFT in FP64 (its row of C)
+    if (tid < 12 * F0) {
+      const int comp = tid / F0, jf = tid - comp * F0;
+      const double* kr = sK32 + comp * N1;
+      const double* mf = T.syn1_four + jf * N1;
+      double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+      for (int j = 0; j < N1; j += 4) {
+        s0 = fma(kr[j], __ldg(mf + j), s0);
+        s1 = fma(kr[j + 1], __ldg(mf + j + 1), s1);
+        s2 = fma(kr[j + 2], __ldg(mf + j + 2), s2);
+        s3 = fma(kr[j + 3], __ldg(mf + j + 3), s3);
       }
+      sC[(32 * 12 + comp) * LDC + jf] = (float)((s0 + s1) + (s2 + s3));
     }
-#pragma unroll
-    for (int q = 0; q < H::QMAX; q++) {
-      const int tile = warp + NWARP * q;
-      if (tile < 2 * G::NTT) {
-        const int mt = tile / G::NTT;
-        const uchar2 kt = sTl[tile - mt * G::NTT];
-        const int c0 = sBo[kt.x], c1 = sBo[kt.x + 1];
-        const int comp = mt * 8 + grow, c = c0 + kt.y * 8 + 2 * gcol;
-        if (comp < 12) {
-          if (c < c1) C[rot * G::NOUT + comp * NC + c] = acc[q][0];
-          if (c + 1 < c1) C[rot * G::NOUT + comp * NC + c + 1] = acc[q][1];
+    __syncthreads();
+    // ---- pass 2: transposed Legendre sums (FP64 FMA), one output coefficient per item ----
+    for (int o = tid; o < 12 * NC; o += NTHR) {
+      const int comp = o / NC, c = o - comp * NC;
+      const float* a = sC + comp * LDC + sJf[c];
+      double s0 = 0.0, s1 = 0.0;
+      if (c < M0) {
+        const double* b = sT0 + c;
+        for (int lat = 0; lat + 1 < L1; lat += 2) {
+          s0 = fma((double)a[lat * 12 * LDC], b[lat * LD0], s0);
+          s1 = fma((double)a[(lat + 1) * 12 * LDC], b[(lat + 1) * LD0], s1);
         }
+        s0 = fma((double)a[(L1 - 1) * 12 * LDC], b[(L1 - 1) * LD0], s0);
+      } else {
+        const float* b = sTF + c;
+        for (int lat = 0; lat + 1 < L1; lat += 2) {
+          s0 = fma((double)a[lat * 12 * LDC], (double)b[lat * LDF], s0);
+          s1 = fma((double)a[(lat + 1) * 12 * LDC], (double)b[(lat + 1) * LDF], s1);
+        }
+        s0 = fma((double)a[(L1 - 1) * 12 * LDC], (double)b[(L1 - 1) * LDF], s0);
       }
+      C[rot * G::NOUT + o] = s0 + s1;
     }
     __syncthreads();  // pass 2's reads of C before the next rotation's pass 1 overwrites it
   }
