@@ -369,6 +369,15 @@ int ves3d_sht_backward_d2(const double* S, long n_fun, int p, double* X_uu, doub
  * (device, [n_vec][p+1][p][3][p(p+2)]). MovePole::operator()(t, j, ...) for j < p is the
  * (t, j) slice. Builds the order-p rotation tables for the call. */
 int ves3d_sht_rotate_all(const double* S, long n_vec, int p, double* R, void* stream);
+/* MovePole<Container, Operators>::operator()(trg_i, trg_j, results) (include/MovePole.h:16-23,
+ * src/MovePole.cc:159-195): n_fun grid functions X [n_fun][(p+1) 2p] (device) rotated so
+ * that grid point (latitude trg_i, longitude trg_j), trg_j in [0, 2p), sits at the x = -1
+ * pole, as the reference's precomputed rotations place it; Y [n_fun][(p+1) 2p] on the same
+ * grid. Computed through the coefficients (Grid2SHC, the rotation of RotateAll for that
+ * point, SHC2Grid): it equals the reference's Direct scheme on functions of degree < p and
+ * differs from it on the degree-p (Nyquist) band, which a grid of 2p longitudes cannot
+ * rotate exactly. Returns when the work is done. */
+int ves3d_move_pole(const double* X, long n_fun, int p, int trg_i, int trg_j, double* Y, void* stream);
 /* SHTrans's frequency filters (constructor, src/SHTrans.cc:8-45) written to a host array of
  * p(p+2) values in the per-function coefficient order (Fourier blocks, degrees ascending):
  * exponent <= 0 gives lowPassFilter's hard cut (1 for degree n <= filter_freq, else 0),
@@ -409,6 +418,20 @@ int ves3d_dev_reduce(const double* x, int x_dim, const double* w, const double* 
  * (trans 'N', 'T' or 'C'), through cuBLAS. */
 int ves3d_dev_gemm(char trans_a, char trans_b, int m, int n, int k, double alpha, const double* A, int lda,
                    const double* B, int ldb, double beta, double* C, int ldc, void* stream);
+/* Device::AggregateRotation(sh_order, nlat, nlong, n_vec, n_sub, mat, vec, wrk, res, n_stream)
+ * (include/Device.h:234-237; the argument order of the declaration and of Device<CPU>,
+ * src/DeviceCPU.cc:646-680, which MovePole::updateEagerResults calls): for every longitude
+ * jj < nlong and operand ii < n_vec, res[n_vec jj + ii] = Permute(mat, jj) . vec[ii], where
+ * mat is an np x np rotation (np = nlat nlong, column-major) whose columns are shifted by
+ * jj within every latitude block (CircShift / PermuteGpu), vec[ii] holds n_sub[ii] grid
+ * functions of np values. vec and res are HOST arrays of DEVICE pointers, as in the
+ * reference; wrk and n_stream are accepted and unused (the permuted matrix is never
+ * formed). Returns when the work is done. (src/DeviceGPU.cc:314 defines the GPU version
+ * with n_vec second, a different order from its declaration; this follows the
+ * declaration.) */
+int ves3d_dev_aggregate_rotation(int sh_order, int nlat, int nlong, int n_vec, const int* n_sub, const double* mat,
+                                 const double* const* vec, double* const* wrk, double* const* res, int n_stream,
+                                 void* stream);
 
 /* ---------------------------------------------------------------------------
  * Direct Stokes sums on device pointers.
@@ -430,6 +453,12 @@ int ves3d_cuda_stokes_double_layer_f64(int src_m, int trg_m, int n, int t_head, 
                                        void* stream);
 int ves3d_cuda_stokes_f64(int src_m, int trg_m, int n, int t_head, int t_tail, const double* T,
                           const double* S, const double* D, double* U, const double* Q, void* stream);
+/* The single-precision overload cuda_stokes(..., const float* T, ...) (src/CudaKernels.cu:
+ * 751-761, used by SINGLE_PREC builds of the reference): float arrays, FP32 pair
+ * arithmetic, FP64 sums across 128-source tiles. Q may be NULL (unit weights) here and in
+ * the double version. Both are asynchronous on the given stream. */
+int ves3d_cuda_stokes_f32(int src_m, int trg_m, int n, int t_head, int t_tail, const float* T,
+                          const float* S, const float* D, float* U, const float* Q, void* stream);
 
 /* All-pairs interaction with the reference's VesInteraction handle signature
  * (include/VesInteraction.h:21, matched by StokesAlltoAll, include/CPUKernels.h:46-49):

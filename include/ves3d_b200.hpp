@@ -5,7 +5,10 @@
  *   reference (lu1and10/ves3d)                              here
  *   StokesVelocity<Real> (include/StokesVelocity.h:9-44)     ves3d_b200::StokesVelocity<double>
  *   SHTrans<Container, Mats> (include/SHTrans.h:21-63)       ves3d_b200::SHTrans<double>
- *   Device<GPU>::DirectStokes (include/Device.h:205-209)     ves3d_b200::DirectStokes
+ *   Device<GPU>::DirectStokes (include/Device.h:205-209)     ves3d_b200::DirectStokes (double, float)
+ *   Device<GPU>::AggregateRotation (include/Device.h:234-237) ves3d_b200::Device::AggregateRotation
+ *   MovePole<Container, Operators> (include/MovePole.h:16-23) ves3d_b200::MovePole
+ *   Surface<Sca, Vec> (include/Surface.h:38-77)              ves3d_b200::Surface<double>
  *   InterfacialVelocity implicit solve (src/InterfacialVelocity.cc:203-1172)
  *                                                            StokesVelocity::ImplicitSolve
  *
@@ -243,6 +246,14 @@ class Device {
           "Device::gemm");
     return C;
   }
+  /* AggregateRotation(sh_order, nlat, nlong, n_vec, n_sub, mat, vec, wrk, res, n_stream):
+   * res[n_vec jj + ii] = (mat with columns shifted by jj per latitude) . vec[ii], for every
+   * longitude jj; vec, wrk, res are host arrays of device pointers (wrk is not used). */
+  void AggregateRotation(int sh_order, int nlat, int nlong, int n_vec, const int* n_sub, const double* mat,
+                         const double** vec, double** wrk, double** res, int n_stream = 1) const {
+    check(ves3d_dev_aggregate_rotation(sh_order, nlat, nlong, n_vec, n_sub, mat, vec, wrk, res, n_stream, stream_),
+          "Device::AggregateRotation");
+  }
 
  private:
   void* stream_;
@@ -290,6 +301,114 @@ inline void DirectStokesDoubleLayer(const double* src, const double* norm, const
                                            (int)trg_idx_tail, trg, src, norm, den, pot, qw, stream),
         "DirectStokesDoubleLayer");
 }
+
+/* Device<GPU>::DirectStokes for float (cuda_stokes's single-precision overload,
+ * src/CudaKernels.cu:751-761): float device arrays; qw may be NULL. */
+inline void DirectStokes(const float* src, const float* den, const float* qw, size_t src_stride, size_t trg_stride,
+                         size_t n_surfs, const float* trg, size_t trg_idx_head, size_t trg_idx_tail, float* pot,
+                         void* stream = 0) {
+  check(ves3d_cuda_stokes_f32((int)src_stride, (int)trg_stride, (int)n_surfs, (int)trg_idx_head, (int)trg_idx_tail,
+                              trg, src, den, pot, qw, stream),
+        "DirectStokes");
+}
+
+/* MovePole<Container, Operators> (include/MovePole.h:16-23): setOperands(arr, num) takes
+ * num device arrays of grid functions of order p (n_funs[i] functions each, [n][(p+1) 2p]);
+ * operator()(trg_i, trg_j, results) writes into results[i] those functions rotated so that
+ * grid point (trg_i, trg_j) sits at the x = -1 pole (the reference's Direct scheme; through
+ * the coefficients, exact on degrees < p). Only the Direct scheme is offered. */
+class MovePole {
+ public:
+  enum Scheme { Direct = 0 };
+  explicit MovePole(int sh_order, void* stream = 0) : p_(sh_order), stream_(stream), arr_(0), n_funs_(0), num_(0) {}
+  void setOperands(const double* const* arr, const long* n_funs, int num, Scheme rot_scheme = Direct) {
+    (void)rot_scheme;
+    arr_ = arr;
+    n_funs_ = n_funs;
+    num_ = num;
+  }
+  void operator()(int trg_i, int trg_j, double* const* results) const {
+    for (int i = 0; i < num_; i++)
+      check(ves3d_move_pole(arr_[i], n_funs_[i], p_, trg_i, trg_j, results[i], stream_), "MovePole");
+  }
+
+ private:
+  int p_;
+  void* stream_;
+  const double* const* arr_;
+  const long* n_funs_;
+  int num_;
+};
+
+/* Surface (include/Surface.h:38-77) of n_ves vesicles of order p on host arrays (positions
+ * and fields AxisMajor [n_ves][3][(p+1) 2p], scalars [n_ves][(p+1) 2p]): geometry
+ * (normal, area element, mean and Gaussian curvature), grad, div, linearizedMeanCurv,
+ * area, volume, getCenters. diff_filter_freq: the low-pass filter of the differential
+ * operators (0 none, -1 2p/3, > 0 the highest degree kept). */
+template <class Real>
+class Surface {
+ public:
+  Surface(int sh_order, const Real* x_in, size_t n, int diff_filter_freq = 0, int device = -1)
+      : sv_(0), p_(sh_order), nv_(0) {
+    check(ves3d_sv_create(sh_order, 2 * sh_order, VES3D_PREC_FP64, device, &sv_), "Surface");
+    if (diff_filter_freq) check(ves3d_sv_set_surface_filter(sv_, diff_filter_freq), "Surface");
+    setPosition(x_in, n);
+  }
+  ~Surface() { ves3d_sv_destroy(sv_); }
+  void setPosition(const Real* x, size_t n) {
+    const size_t per = 3 * ngrid();
+    if (n == 0 || n % per) throw Error(VES3D_ERR_ARG, "Surface: size is not a multiple of 3 (p+1) 2p");
+    nv_ = (long)(n / per);
+    check(ves3d_sv_set_src_coord(sv_, x, nv_, 0), "Surface::setPosition");
+  }
+  int getNumberOfSurfaces() const { return (int)nv_; }
+  int getShOrder() const { return p_; }
+  /* unit outward normal [n_ves][3][Ngrid], area element W, mean curvature H (sphere of
+   * radius R: -1/R), Gaussian curvature K, each [n_ves][Ngrid] */
+  void getNormal(std::vector<Real>& n) const { geometry_part(4, 3, n); }
+  void getAreaElement(std::vector<Real>& w) const { geometry_part(3, 1, w); }
+  void getMeanCurv(std::vector<Real>& h) const { geometry_part(13, 1, h); }
+  void getGaussianCurv(std::vector<Real>& k) const { geometry_part(14, 1, k); }
+  void grad(const Real* f_in, Real* grad_f_out) const {
+    check(ves3d_sv_surface_op(sv_, VES3D_OP_GRAD, f_in, grad_f_out, 0), "Surface::grad");
+  }
+  void div(const Real* f_in, Real* div_f_out) const {
+    check(ves3d_sv_surface_op(sv_, VES3D_OP_DIV, f_in, div_f_out, 0), "Surface::div");
+  }
+  void linearizedMeanCurv(const Real* x_new, Real* h_lin) const {
+    check(ves3d_sv_surface_op(sv_, VES3D_OP_LIN_MEANCURV, x_new, h_lin, 0), "Surface::linearizedMeanCurv");
+  }
+  void area(std::vector<Real>& a) const {
+    a.resize(nv_);
+    check(ves3d_sv_integrals(sv_, &a[0], 0, 0, 0), "Surface::area");
+  }
+  void volume(std::vector<Real>& v) const {
+    v.resize(nv_);
+    check(ves3d_sv_integrals(sv_, 0, &v[0], 0, 0), "Surface::volume");
+  }
+  void getCenters(std::vector<Real>& c) const {
+    c.resize(3 * nv_);
+    check(ves3d_sv_integrals(sv_, 0, 0, &c[0], 0), "Surface::getCenters");
+  }
+
+ private:
+  size_t ngrid() const { return (size_t)2 * p_ * (p_ + 1); }
+  // components [c0, c0 + nc) of the geometry record [n_ves][15][Ngrid]
+  void geometry_part(int c0, int nc, std::vector<Real>& out) const {
+    const size_t ng = ngrid();
+    std::vector<Real> geo((size_t)nv_ * 15 * ng);
+    check(ves3d_sv_surface_op(sv_, VES3D_OP_GEOMETRY, 0, &geo[0], 0), "Surface geometry");
+    out.resize((size_t)nv_ * nc * ng);
+    for (long v = 0; v < nv_; v++)
+      for (int c = 0; c < nc; c++)
+        for (size_t i = 0; i < ng; i++) out[((size_t)v * nc + c) * ng + i] = geo[((size_t)v * 15 + c0 + c) * ng + i];
+  }
+  Surface(const Surface&);
+  Surface& operator=(const Surface&);
+  ves3d_sv* sv_;
+  int p_;
+  long nv_;
+};
 
 }  // namespace ves3d_b200
 

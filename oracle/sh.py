@@ -419,6 +419,30 @@ def rotate_all(S, p0, dof, stable=True):
     return out.reshape(-1)
 
 
+def move_pole(X, p0, trg_i, trg_j, stable=True):
+    """MovePole(trg_i, trg_j) on grid functions X [n][(p0+1) 2p0] (src/MovePole.cc:159-195):
+    the rotation of rotate_all for latitude trg_i and longitude trg_j, trg_j in [0, 2p0)
+    (grid point (trg_i, trg_j) to the x = -1 pole), through the coefficients."""
+    nc = ncoef(p0)
+    S = grid2shc(X, p0, p0).reshape(-1, nc)
+    B0 = _phase(S, p0, trg_j, -1.0)
+    R = _apply_blocks(B0, mat_rotate(p0, stable), p0, trg_i)
+    return shc2grid(R.reshape(-1), p0, p0)
+
+
+def aggregate_rotation(mat, nlat, nlong, vec):
+    """Device<CPU>::AggregateRotation for one operand (src/DeviceCPU.cc:646-680): for every
+    longitude jj, CircShift the columns of the column-major np x np matrix mat within each
+    latitude block by jj and apply it to the nsub grid functions vec [nsub][np]. Returns
+    [nlong][nsub][np]."""
+    npt = nlat * nlong
+    A = np.asarray(mat, np.float64).reshape(npt, npt).T  # A[row][col]
+    lat = np.arange(npt) // nlong
+    lon = np.arange(npt) % nlong
+    vec = np.asarray(vec, np.float64).reshape(-1, npt)
+    return np.stack([vec @ A[:, lat * nlong + (lon - jj) % nlong].T for jj in range(nlong)])
+
+
 def rotate_transpose(S_, p0, dof, stable=True):
     """Adjoint of rotate_all (src/SphericalHarmonics.cc:452-541); same layout in and out."""
     nc = ncoef(p0)

@@ -128,15 +128,49 @@ def noise_floor():
     np.savez_compressed(os.path.join(HERE, "ref_noise_floor_p12_p24.npz"), **out)
 
 
+def move_pole():
+    """The reference's MovePole in its Direct scheme at p = 6 (src/MovePole.cc:166-180:
+    rot_mat = CircShift(all_rot_mats[trg_i], trg_j np), results = rot_mat . arr, the gemm in
+    column-major BLAS terms) on its own precomputed rotations
+    (precomputed/all_rot_mats_6_double.txt), applied to grid functions of degree < p: the
+    coordinate functions of a perturbed ellipsoid and three functions of random
+    coefficients up to degree p - 1. Also the matrix of latitude 2, for AggregateRotation."""
+    from oracle import sh
+    p = 6
+    npt = 2 * p * (p + 1)
+    path = os.path.join(_reference_root(), "precomputed", "all_rot_mats_6_double.txt")
+    M = np.loadtxt(path).ravel()[: (p + 1) * npt * npt].reshape(p + 1, npt, npt)  # [lat][col][row]
+    X, _ = workloads.suspension(1, p, 3.0, semi_axes=(1.0, 1.0, 0.6), deg=4, amp=0.05, seed=66)
+    rng = np.random.default_rng(67)
+    S = rng.standard_normal((3, sh.ncoef(p)))
+    deg = np.concatenate([np.arange((jf + 1) // 2, p + 1) for jf in range(2 * p)])
+    S[:, deg >= p] = 0.0  # degree < p
+    F = np.concatenate([X.reshape(3, npt), sh.shc2grid(S.reshape(-1), p, p).reshape(3, npt)])
+    lat = np.arange(npt) // (2 * p)
+    lon = np.arange(npt) % (2 * p)
+    targets = np.array([(0, 0), (2, 3), (2, 9), (5, 5), (3, 11), (6, 2), (1, 7)])
+    out = []
+    for i, j in targets:
+        A = M[i].T  # A[row][col]
+        Aj = A[:, lat * 2 * p + (lon - j) % (2 * p)]  # CircShift of the columns per latitude block
+        out.append(F @ Aj.T)
+    np.savez_compressed(os.path.join(HERE, "ref_movepole_p6.npz"), p=p, F=F, targets=targets,
+                        rotated=np.array(out), mat_lat2=M[2].ravel())
+
+
 def main():
     import sys
-    if "--noise-floor" in sys.argv:  # the newest fixture alone
+    if "--noise-floor" in sys.argv:  # the newest fixtures alone
         noise_floor()
+        return
+    if "--move-pole" in sys.argv:
+        move_pole()
         return
     dumbbell()
     streamable()
     double_layer()
     noise_floor()
+    move_pole()
     assert reflib.available(), "build oracle/_ref first (make -C oracle/ref)"
     reflib.set_threads(os.cpu_count() or 1)
     # p = 6: two ellipsoids; quadrature rules, transforms, the self matrix of vesicle 0

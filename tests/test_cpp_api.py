@@ -62,3 +62,10 @@ def test_cpp_api_matches_oracle(tmp_path):
     b = step.to_coef(step.rhs())
     r = b - step.matvec_sh(step.to_coef(x))
     assert np.linalg.norm(r) / np.linalg.norm(b) < 3e-9
+
+
+def test_cpp_device_api_builds_as_cpp03_and_links(tmp_path):
+    """The device-pointer callers (MovePole, AggregateRotation, float DirectStokes, Surface)
+    compile as C++03 against the mirror header and link (no GPU needed)."""
+    from tests.test_gpu_boundary import build_device_api_test
+    assert os.path.exists(build_device_api_test(tmp_path))

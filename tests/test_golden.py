@@ -96,3 +96,27 @@ def test_reference_noise_floor_bounds_the_oracle(gnf, case):
     o = sh.self_apply(sh.stokes_singular_matrix(X, p, 2 * p), f, p)
     for r in (a, b):
         assert rel_err(o, r) < 3 * floor
+
+
+def test_move_pole_oracle_matches_reference_direct_scheme():
+    """MovePole through the coefficients (the oracle) against the reference's Direct scheme
+    on its own precomputed rotations (tests/golden/ref_movepole_p6.npz) for functions of
+    degree < p, every target including longitudes >= p; the target point ends at x = -1."""
+    g = dict(np.load(os.path.join(HERE, "ref_movepole_p6.npz")))
+    p, F = int(g["p"]), g["F"]
+    for (i, j), ref in zip(g["targets"], g["rotated"]):
+        got = sh.move_pole(F, p, int(i), int(j)).reshape(ref.shape)
+        assert rel_err(got, ref) < 1e-13
+        poles = sh.shc2pole(sh.grid2shc(got[:3].reshape(-1), p, p), p).reshape(3, 2)
+        assert np.abs(poles[:, 0] - F[:3, i * 2 * p + j]).max() < 1e-13
+
+
+def test_aggregate_rotation_oracle_is_move_pole_for_every_longitude():
+    """AggregateRotation with the reference's latitude-2 rotation reproduces its Direct
+    MovePole at every longitude of that latitude (the eager scheme of MovePole.cc:272-305)."""
+    g = dict(np.load(os.path.join(HERE, "ref_movepole_p6.npz")))
+    p, F = int(g["p"]), g["F"]
+    res = sh.aggregate_rotation(g["mat_lat2"], p + 1, 2 * p, F)
+    for (i, j), ref in zip(g["targets"], g["rotated"]):
+        if i == 2:
+            assert rel_err(res[j], ref) < 1e-13

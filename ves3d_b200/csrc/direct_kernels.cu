@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(kFarBS) k_direct_stokes_f64(int src_m, int trg
     __syncthreads();
     for (int i = threadIdx.x; i < ns; i += kFarBS) {
       const int s = s0 + i;
-      const double q = Q[s];
+      const double q = Q ? Q[s] : 1.0;
       sp[3 * i] = Sv[s];
       sp[3 * i + 1] = Sv[src_m + s];
       sp[3 * i + 2] = Sv[2 * src_m + s];
@@ -123,6 +123,76 @@ int launch_direct_stokes_f64(int src_m, int trg_m, int n, int t_head, int t_tail
   if (n <= 0 || t_tail <= t_head) return VES3D_OK;
   dim3 grid((t_tail - t_head + kFarBS - 1) / kFarBS, n);
   k_direct_stokes_f64<<<grid, kFarBS, 0, st>>>(src_m, trg_m, t_head, t_tail, T, S, D, U, Q);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
+// The single-precision overload of cuda_stokes (src/CudaKernels.cu:594-761, the kernel
+// `stokes` on float arrays, used by SINGLE_PREC builds of the reference): FP32 inputs and
+// outputs and FP32 pair arithmetic (hardware reciprocal square root, a coincident pair
+// contributes nothing), each thread's FP32 sum over a tile of 128 sources added into an
+// FP64 accumulator. Q may be NULL (unit weights), as in the reference's second kernel.
+__global__ void __launch_bounds__(kFarBS) k_direct_stokes_f32(int src_m, int trg_m, int t_head, int t_tail,
+                                                              const float* __restrict__ T,
+                                                              const float* __restrict__ S,
+                                                              const float* __restrict__ D, float* __restrict__ U,
+                                                              const float* __restrict__ Q) {
+  __shared__ float sp[kFarBS * 3];
+  __shared__ float sd[kFarBS * 3];
+  const long v = blockIdx.y;
+  const int t = t_head + blockIdx.x * kFarBS + threadIdx.x;
+  const bool active = t < t_tail;
+  const float* Tv = T + v * 3 * (long)trg_m;
+  const float* Sv = S + v * 3 * (long)src_m;
+  const float* Dv = D + v * 3 * (long)src_m;
+  float tx = 0.f, ty = 0.f, tz = 0.f;
+  if (active) {
+    tx = Tv[t];
+    ty = Tv[trg_m + t];
+    tz = Tv[2 * trg_m + t];
+  }
+  double ax = 0.0, ay = 0.0, az = 0.0;
+  for (int s0 = 0; s0 < src_m; s0 += kFarBS) {
+    const int ns = min(kFarBS, src_m - s0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < ns; i += kFarBS) {
+      const int s = s0 + i;
+      const float q = Q ? Q[s] : 1.f;
+      sp[3 * i] = Sv[s];
+      sp[3 * i + 1] = Sv[src_m + s];
+      sp[3 * i + 2] = Sv[2 * src_m + s];
+      sd[3 * i] = Dv[s] * q;
+      sd[3 * i + 1] = Dv[src_m + s] * q;
+      sd[3 * i + 2] = Dv[2 * src_m + s] * q;
+    }
+    __syncthreads();
+    if (!active) continue;
+    float ux = 0.f, uy = 0.f, uz = 0.f;
+    for (int k = 0; k < ns; k++) {
+      const float dx = sp[3 * k] - tx, dy = sp[3 * k + 1] - ty, dz = sp[3 * k + 2] - tz;
+      const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+      const float rinv = r2 > 0.f ? rsqrtf(r2) : 0.f;
+      const float cc = fmaf(dz, sd[3 * k + 2], fmaf(dy, sd[3 * k + 1], dx * sd[3 * k])) * rinv * rinv;
+      ux = fmaf(fmaf(cc, dx, sd[3 * k]), rinv, ux);
+      uy = fmaf(fmaf(cc, dy, sd[3 * k + 1]), rinv, uy);
+      uz = fmaf(fmaf(cc, dz, sd[3 * k + 2]), rinv, uz);
+    }
+    ax += ux;
+    ay += uy;
+    az += uz;
+  }
+  if (!active) return;
+  float* Uv = U + v * 3 * (long)trg_m;
+  Uv[t] = (float)(ax * kInv8Pi);
+  Uv[trg_m + t] = (float)(ay * kInv8Pi);
+  Uv[2 * trg_m + t] = (float)(az * kInv8Pi);
+}
+
+int launch_direct_stokes_f32(int src_m, int trg_m, int n, int t_head, int t_tail, const float* T, const float* S,
+                             const float* D, float* U, const float* Q, cudaStream_t st) {
+  if (n <= 0 || t_tail <= t_head) return VES3D_OK;
+  dim3 grid((t_tail - t_head + kFarBS - 1) / kFarBS, n);
+  k_direct_stokes_f32<<<grid, kFarBS, 0, st>>>(src_m, trg_m, t_head, t_tail, T, S, D, U, Q);
   VES3D_LAUNCHED();
   return VES3D_OK;
 }

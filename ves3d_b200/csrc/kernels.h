@@ -50,6 +50,15 @@ int launch_synthesis(const double* S, long nfun, int p0, int q, const double* le
 // RotateAll with dof = 3 (src/SphericalHarmonics.cc:363-449):
 // S [nv][3][Ncoef] -> R [nv][p0+1][p0][3][Ncoef].
 int launch_rotate_all(const double* S, long nv, const DevTables& T, double* R, cudaStream_t st);
+// One rotation (MovePole): S [n_fun][Ncoef] -> R [n_fun][Ncoef] with grid point (t, j),
+// j in [0, 2 p0), moved to the x = -1 pole.
+int launch_rotate_one(const double* S, long n_fun, int t, int j, const DevTables& T, double* R, cudaStream_t st);
+// Device::AggregateRotation: res = mat . (vec with longitudes shifted by jj), see device_prims.cu
+int launch_aggregate_rotation(const double* mat, int nlat, int nlong, int jj, const double* vec, int nsub,
+                              double* res, cudaStream_t st);
+// the single-precision cuda_stokes
+int launch_direct_stokes_f32(int src_m, int trg_m, int n, int t_head, int t_tail, const float* T, const float* S,
+                             const float* D, float* U, const float* Q, cudaStream_t st);
 // Singular kernel (src/SphericalHarmonics.cc:971-1068) for nrot rotated surfaces:
 // X, Xt, Xp [nrot][3][M1], R [nrot][3][Ncoef] -> K [nrot][2][6][M1].
 int launch_singular_sl(const double* X, const double* Xt, const double* Xp, const double* R, long nrot,

@@ -83,6 +83,45 @@ __global__ void __launch_bounds__(256) k_rotate_all(const double* __restrict__ S
 
 static int mr_per_t(const DevTables& T) { return T.mr_total / (T.p0 + 1); }
 
+// One rotation of n_fun coefficient vectors: the grid point (latitude t, longitude j) of
+// order p0 moved to the x = -1 pole, j in [0, 2 p0) (the step of RotateAll for one (t, j),
+// src/SphericalHarmonics.cc:363-449: longitude phase P_j, then the per-degree blocks of
+// MatRotate for latitude t). One CTA per function.
+__global__ void __launch_bounds__(256) k_rotate_one(const double* __restrict__ S, int p0, int t, int j, DevTables T,
+                                                    double* __restrict__ R) {
+  extern __shared__ double sB[];  // phase-shifted coefficients [nc]
+  const int nc = p0 * (p0 + 2);
+  const long f = blockIdx.x;
+  const double* s = S + f * nc;
+  for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+    const int pc = __ldg(T.partner + c);
+    if (pc < 0) {
+      sB[c] = s[c];
+    } else {
+      const int q = (__ldg(T.m_of_coef + c) * j) % (2 * p0);
+      const double cs = __ldg(T.cos_tab + q), sn = __ldg(T.sin_tab + q);
+      sB[c] = __ldg(T.is_sin + c) ? -s[pc] * sn + s[c] * cs : s[c] * cs + s[pc] * sn;
+    }
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+    const int n = __ldg(T.n_of_coef + c), bp = __ldg(T.pos_in_block + c);
+    const int po = __ldg(T.perm_off + n), bn = __ldg(T.perm_off + n + 1) - po;
+    const double* M = T.mr + __ldg(T.mr_off + t * (p0 + 1) + n);
+    double acc = 0.0;
+    for (int k = 0; k < bn; k++) acc = fma(sB[__ldg(T.perm + po + k)], __ldg(M + k * bn + bp), acc);
+    R[f * nc + c] = acc;
+  }
+}
+
+int launch_rotate_one(const double* S, long n_fun, int t, int j, const DevTables& T, double* R, cudaStream_t st) {
+  if (n_fun <= 0) return VES3D_OK;
+  const int nc = ncoef_(T.p0);
+  k_rotate_one<<<(unsigned)n_fun, 256, nc * sizeof(double), st>>>(S, T.p0, t, j, T, R);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
 int launch_rotate_all(const double* S, long nv, const DevTables& T, double* R, cudaStream_t st) {
   if (nv <= 0) return VES3D_OK;
   const int p0 = T.p0;

@@ -1148,6 +1148,41 @@ int ves3d_sht_rotate_all(const double* S, long n_vec, int p, double* R, void* st
   return VES3D_OK;
 }
 
+int ves3d_move_pole(const double* X, long n_fun, int p, int trg_i, int trg_j, double* Y, void* stream) {
+  VES3D_ARG(X && Y, "null pointer");
+  VES3D_ARG(p >= 1 && p <= 127, "order must be in [1, 127]");
+  VES3D_ARG(n_fun >= 0, "n_fun < 0");
+  VES3D_ARG(trg_i >= 0 && trg_i <= p && trg_j >= 0 && trg_j < 2 * p, "target outside the (p + 1) x 2p grid");
+  if (n_fun == 0) return VES3D_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  TablesOwner tab;  // transforms and rotation tables of order p (freed on return)
+  build_tables(p, p, tab.h);
+  int s = tab.upload(st);
+  const DevTables& T = tab.d;
+  const size_t nc = ncoef_(p);
+  double* work = nullptr;  // coefficients, then rotated coefficients
+  if (!s) s = cuda_status(cudaMallocAsync((void**)&work, 2 * n_fun * nc * sizeof(double), st), "cudaMallocAsync",
+                          __FILE__, __LINE__);
+  if (!s) s = launch_grid2shc(X, n_fun, p, T.ana_four, T.ana_leg, T.jf_of_coef, work, st);
+  if (!s) s = launch_rotate_one(work, n_fun, trg_i, trg_j, T, work + n_fun * nc, st);
+  if (!s)
+    s = launch_synthesis(work + n_fun * nc, n_fun, p, p, T.syn0_leg, T.syn0_dleg, T.syn0_four, T.syn0_dfour,
+                         T.blk_off, Y, nullptr, nullptr, st);
+  if (work) cudaFreeAsync(work, st);
+  const cudaError_t e = cudaStreamSynchronize(st);
+  if (s) return s;
+  VES3D_CK(e);
+  return VES3D_OK;
+}
+
+int ves3d_cuda_stokes_f32(int src_m, int trg_m, int n, int t_head, int t_tail, const float* T, const float* S,
+                          const float* D, float* U, const float* Q, void* stream) {
+  VES3D_ARG(T && S && D && U, "null pointer");
+  VES3D_ARG(src_m >= 0 && trg_m >= 0 && n >= 0, "negative size");
+  VES3D_ARG(t_head >= 0 && t_tail <= trg_m && t_head <= t_tail, "target range outside [0, trg_m]");
+  return launch_direct_stokes_f32(src_m, trg_m, n, t_head, t_tail, T, S, D, U, Q, (cudaStream_t)stream);
+}
+
 int ves3d_sht_backward_d2(const double* S, long n_fun, int p, double* X_uu, double* X_vv, double* X_uv,
                           void* stream) {
   VES3D_ARG(S && (X_uu || X_vv || X_uv), "null pointer");
@@ -1282,7 +1317,7 @@ int ves3d_tables_export(int p0, int p1, const char* name, double* out, size_t ca
 
 int ves3d_cuda_stokes_f64(int src_m, int trg_m, int n, int t_head, int t_tail, const double* T, const double* S,
                           const double* D, double* U, const double* Q, void* stream) {
-  VES3D_ARG(T && S && D && U && Q, "null pointer");
+  VES3D_ARG(T && S && D && U, "null pointer");
   VES3D_ARG(src_m >= 0 && trg_m >= 0 && n >= 0, "negative size");
   VES3D_ARG(t_head >= 0 && t_tail <= trg_m && t_head <= t_tail, "target range outside [0, trg_m]");
   return launch_direct_stokes_f64(src_m, trg_m, n, t_head, t_tail, T, S, D, U, Q, (cudaStream_t)stream);
