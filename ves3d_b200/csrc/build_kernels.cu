@@ -554,18 +554,23 @@ struct RingTcCfg {
   static constexpr int OFF_K = OFF_U;
   static constexpr int OFF_XS = OFF_K + 3 * SZ_K;
   static constexpr int U_SZ = std::max(std::max(6 * SZ_A, 3 * SZ_K + SZ_XS), SZ_C);
-  static constexpr int OFF_R = (OFF_U + U_SZ + 127) / 128 * 128;  // 2 x [3][LDR] FP64
-  static constexpr int OFF_T0 = OFF_R + 2 * 3 * LDR * 8;          // FP64 m = 0 tables: leg, dleg [L1][LD0]
-  static constexpr int OFF_TF = OFF_T0 + 2 * L1 * LD0 * 8;        // FP32 tables: leg, dleg [L1][LDF]
-  static constexpr int OFF_X32 = OFF_TF + (2 * L1 * LDF * 4 + 7) / 8 * 8;  // last latitude: [9][N1] FP32
-  static constexpr int OFF_K32 = OFF_X32 + 9 * N1 * 4;            // its kernel values [12][N1] FP64
-  static constexpr int OFF_R4 = OFF_K32 + 12 * N1 * 8;             // R as float4 (x, y, z, 0) [NC]
-  static constexpr int OFF_TRG = OFF_R4 + NC * 16;
+  // every region starts on a 16-byte boundary (float4 and bulk-copy destinations need it)
+  static constexpr int al16(int x) { return (x + 15) / 16 * 16; }
+  static constexpr int OFF_R = (OFF_U + U_SZ + 127) / 128 * 128;      // 2 x [3][LDR] FP64
+  static constexpr int OFF_T0 = al16(OFF_R + 2 * 3 * LDR * 8);        // FP64 m = 0 tables: leg, dleg [L1][LD0]
+  static constexpr int OFF_TF = al16(OFF_T0 + 2 * L1 * LD0 * 8);      // FP32 tables: leg, dleg [L1][LDF]
+  static constexpr int OFF_X32 = al16(OFF_TF + 2 * L1 * LDF * 4);     // last latitude: [9][N1] FP32
+  static constexpr int OFF_K32 = al16(OFF_X32 + 9 * N1 * 4);          // its kernel values [12][N1] FP64
+  static constexpr int OFF_R4 = al16(OFF_K32 + 12 * N1 * 8);          // R as float4 (x, y, z, 0) [NC]
+  static constexpr int OFF_TRG = al16(OFF_R4 + NC * 16);
   static constexpr int OFF_CEN = OFF_TRG + 6 * 8;
   static constexpr int OFF_SW = OFF_CEN + 6 * 8;
   static constexpr int OFF_BO = OFF_SW + L1 * 8;
   static constexpr int OFF_JF = OFF_BO + ((F0 + 1) * 4 + 7) / 8 * 8;   // Fourier block of each coefficient
   static constexpr int OFF_BAR = OFF_JF + (NC + 7) / 8 * 8;
+  static_assert(OFF_U % 16 == 0 && OFF_R % 16 == 0 && OFF_T0 % 16 == 0 && OFF_TF % 16 == 0 && OFF_X32 % 16 == 0 &&
+                    OFF_K32 % 16 == 0 && OFF_R4 % 16 == 0 && OFF_BAR % 8 == 0 && (LDCL * 4) % 16 == 0,
+                "alignment of the shared-memory regions");
   static constexpr int NBAR = 4;  // GEMM 1, GEMM 2, R buffers 0 and 1
   static constexpr int OFF_TMEM = OFF_BAR + NBAR * 8;
   static constexpr int SMEM = OFF_TMEM + 16;
