@@ -94,6 +94,22 @@ int ves3d_sv_set_trg_coord(ves3d_sv* sv, const double* T, long n_trg, int is_dev
  * targets near a surface with its NearSingular module, which this build does not have:
  * the result is accurate only away from the surfaces (a few grid spacings). */
 int ves3d_sv_eval_trg(ves3d_sv* sv, double* vel, int is_device);
+/* Near-singular correction of the off-surface targets (NearSingular, src/NearSingular.cc,
+ * as StokesVelocity composes it for SetTrgCoord targets, src/StokesVelocity.cc:475-500),
+ * off by default. With it on, ves3d_sv_eval_trg sums every vesicle's smooth quadrature at
+ * the far upsampling order p_up, and for a target closer than r_near = r_ves 2 / sqrt(p_up)
+ * to a vesicle (r_ves: the largest distance of a surface point from its vesicle's
+ * centroid) replaces that vesicle's contribution by the reference's interpolation: 8
+ * Lagrange nodes along the line from the target's projection P on the surface (the
+ * on-surface singular-quadrature velocity at P, plus +-g(P)/2 for the double layer
+ * outside / inside, and the smooth quadrature at P + r_near (1 + (l - 1)/6) d, l = 1..7).
+ * The projection is Gauss-Newton on the spherical-harmonic surface (the reference uses
+ * quadratic patches); at most 4 near vesicles per target (more is an error). FP64; orders
+ * up to 31. */
+int ves3d_sv_set_near_singular(ves3d_sv* sv, int on);
+/* r_near of the last corrected target evaluation and the number of (target, vesicle) pairs
+ * it corrected. */
+int ves3d_sv_near_info(ves3d_sv* sv, double* r_near, long* n_near);
 /* The self part's upsampling order (sh_order_up_self, src/StokesVelocity.cc:26-57): new
  * operator tables, the self matrices rebuilt on next use. */
 int ves3d_sv_set_order_up(ves3d_sv* sv, int sh_order_up);

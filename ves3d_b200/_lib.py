@@ -45,6 +45,8 @@ SIGNATURES = [
     ("ves3d_sv_get_parts", _i, [_vp, _vp, _vp, _i]),
     ("ves3d_sv_stage_times", _i, [_vp, ctypes.POINTER(ctypes.c_float)]),
     ("ves3d_sv_far_dl_time", _i, [_vp, ctypes.POINTER(ctypes.c_float)]),
+    ("ves3d_sv_set_near_singular", _i, [_vp, _i]),
+    ("ves3d_sv_near_info", _i, [_vp, ctypes.POINTER(_d), ctypes.POINTER(ctypes.c_long)]),
     ("ves3d_sv_device_buffer", _i, [_vp, _i, ctypes.POINTER(_vp), ctypes.POINTER(_sz)]),
     ("ves3d_sv_eval_resident", _i, [_vp]),
     ("ves3d_sv_capture_eval", _i, [_vp]),

@@ -11,7 +11,7 @@ PEAK_LIB = os.path.join(HERE, "libves3d_peak.so")
 PEAK_SOURCE = "peak_probe.cu"
 SOURCES = ["sh_tables.cc", "sht_kernels.cu", "singular_kernels.cu", "direct_kernels.cu", "far_kernels.cu", "build_kernels.cu", "stokes_velocity.cu",
            "noalloc.cu", "geometry_kernels.cu", "bicgstab.cu", "mlp.cu", "device_prims.cu",
-           "vtk_output.cu"]
+           "vtk_output.cu", "near_kernels.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared", "-Wno-deprecated-gpu-targets"]
 

@@ -56,6 +56,17 @@ int launch_rotate_one(const double* S, long n_fun, int t, int j, const DevTables
 // Device::AggregateRotation: res = mat . (vec with longitudes shifted by jj), see device_prims.cu
 int launch_aggregate_rotation(const double* mat, int nlat, int nlong, int jj, const double* vec, int nsub,
                               double* res, cudaStream_t st);
+// Near-singular correction at off-surface targets (near_kernels.cu)
+constexpr int kNearMax = 4;  // near vesicles per target
+int launch_centroid_radius(const double* X, long nv, int p, double* cen_r, unsigned long long* rmax_bits,
+                           cudaStream_t st);
+int launch_near_find(const double* trg, long M, const double* cen_r, long nv, const double* pos_up, int p_up,
+                     double r_near, int* count, int* near_v, int* near_k, cudaStream_t st);
+int launch_near_correct(const double* trg, long M, const int* count, const int* near_v, const int* near_k,
+                        const double* Sx, const double* Vc, const double* Gc, const double* pos_up,
+                        const double* den_up, const double* nrm_up, const double* dden_up, const double* theta_up,
+                        const int* blk_off, int p, int p_up, double r_near, double* corr, double* vel,
+                        cudaStream_t st);
 // the single-precision cuda_stokes
 int launch_direct_stokes_f32(int src_m, int trg_m, int n, int t_head, int t_tail, const float* T, const float* S,
                              const float* D, float* U, const float* Q, cudaStream_t st);

@@ -167,6 +167,33 @@ struct ves3d_sv {
   // off-surface targets (SetTrgCoord): point-major [trg_n][3] and their velocities
   double *trg = nullptr, *vtrg = nullptr;
   long trg_n = 0, trg_cap = 0;
+  // near-singular correction of the targets (NearSingular): the upsampled sources of every
+  // vesicle (surface, tangents, density, double-layer density at p_up, AxisMajor; area;
+  // point-major positions, weighted densities, normals), vesicle centroids and radii,
+  // near lists and per-slot corrections of the targets, the upsampled grid's latitudes
+  // and smooth weights
+  bool near_on = false;
+  double *nu_X = nullptr, *nu_Xt = nullptr, *nu_Xp = nullptr, *nu_F = nullptr, *nu_G = nullptr, *nu_area = nullptr;
+  double *nu_pos = nullptr, *nu_den = nullptr, *nu_nrm = nullptr, *nu_dden = nullptr, *nu_cen = nullptr;
+  double *nu_theta = nullptr, *nu_w = nullptr, *nu_corr = nullptr;
+  unsigned long long* nu_rmax = nullptr;
+  int *nu_count = nullptr, *nu_v = nullptr, *nu_k = nullptr;
+  long nu_ves_cap = 0, nu_trg_cap = 0;
+  double near_r = 0.0;  // r_near of the last corrected evaluation
+  void free_near() {
+    double* ps[] = {nu_X, nu_Xt, nu_Xp, nu_F, nu_G, nu_area, nu_pos, nu_den, nu_nrm, nu_dden, nu_cen, nu_theta, nu_w,
+                    nu_corr};
+    for (double* q : ps) dfree(q);
+    nu_X = nu_Xt = nu_Xp = nu_F = nu_G = nu_area = nu_pos = nu_den = nu_nrm = nu_dden = nu_cen = nullptr;
+    nu_theta = nu_w = nu_corr = nullptr;
+    dfree(nu_rmax);
+    dfree(nu_count);
+    dfree(nu_v);
+    dfree(nu_k);
+    nu_rmax = nullptr;
+    nu_count = nu_v = nu_k = nullptr;
+    nu_ves_cap = nu_trg_cap = 0;
+  }
   double *velc = nullptr, *dlc = nullptr;
   long contrast_nves = -1;  // vesicle count the device coefficients were made for
   long* off = nullptr;  // [nves+1] point offsets of the vesicles
@@ -216,6 +243,7 @@ struct ves3d_sv {
   float far_dl_ms = 0;  // the far double layer's segment kernels in the last evaluation
 
   ~ves3d_sv() {
+    free_near();
     dfree(filt);
     dfree(velc);
     dfree(dlc);
@@ -631,6 +659,122 @@ int run_eval(ves3d_sv* sv, bool dl) {
 
 }  // namespace
 
+namespace {
+
+// Targets with the near-singular correction (near_kernels.cu): the self part of the
+// current densities (its coefficients are the on-surface values), the upsampled sources of
+// every vesicle, the smooth quadrature of all of them at the targets, then the correction
+// of the targets near a vesicle.
+int eval_trg_near(ves3d_sv* sv) {
+  const DevTables& T = sv->tab->d;
+  cudaStream_t st = sv->stream;
+  const int p = sv->p, q = sv->pup, nc = ncoef_(p);
+  const long nv = sv->nves, M = sv->trg_n, ng1 = ngrid_(q);
+  const bool dl = sv->have_dl;
+  int s;
+  if (!sv->sl_valid && (s = run_setup(sv))) return s;
+  if (dl && !sv->dl_valid && (s = run_setup(sv, true))) return s;
+  if ((s = run_self_apply(sv, dl))) return s;  // Fc (Gc) and the self coefficients Vc
+  if (sv->nu_ves_cap < nv || (dl && !sv->nu_G)) {
+    double* ps[] = {sv->nu_X, sv->nu_Xt, sv->nu_Xp, sv->nu_F, sv->nu_G, sv->nu_area, sv->nu_pos, sv->nu_den,
+                    sv->nu_nrm, sv->nu_dden, sv->nu_cen, sv->nu_theta, sv->nu_w};
+    for (double* x : ps) dfree(x);
+    const size_t f = (size_t)nv * 3 * ng1;
+    s = 0;
+    s |= dalloc(&sv->nu_X, f);
+    s |= dalloc(&sv->nu_Xt, f);
+    s |= dalloc(&sv->nu_Xp, f);
+    s |= dalloc(&sv->nu_F, f);
+    s |= dalloc(&sv->nu_G, f);
+    s |= dalloc(&sv->nu_area, (size_t)nv * ng1);
+    s |= dalloc(&sv->nu_pos, f);
+    s |= dalloc(&sv->nu_den, f);
+    s |= dalloc(&sv->nu_nrm, f);
+    s |= dalloc(&sv->nu_dden, f);
+    s |= dalloc(&sv->nu_cen, 4 * (size_t)nv);
+    if (!sv->nu_rmax) s |= dalloc(&sv->nu_rmax, 1);
+    // the upsampled grid's latitudes and smooth weights (LegendreWeights(p_up))
+    std::vector<double> x, w, th(q + 1), sw(q + 1);
+    gauss_legendre(q + 1, x, w);
+    for (int i = 0; i <= q; i++) {
+      th[i] = std::acos(x[i]);
+      sw[i] = w[i] * M_PI / q / std::sqrt(1.0 - x[i] * x[i]);
+    }
+    if (!s) s = dupload(&sv->nu_theta, th, st);
+    if (!s) s = dupload(&sv->nu_w, sw, st);
+    if (s) {
+      sv->free_near();
+      return s;
+    }
+    sv->nu_ves_cap = nv;
+  }
+  if (sv->nu_trg_cap < M) {
+    dfree(sv->nu_count);
+    dfree(sv->nu_v);
+    dfree(sv->nu_k);
+    dfree(sv->nu_corr);
+    sv->nu_count = sv->nu_v = sv->nu_k = nullptr;
+    sv->nu_corr = nullptr;
+    s = 0;
+    s |= dalloc(&sv->nu_count, (size_t)M);
+    s |= dalloc(&sv->nu_v, (size_t)M * kNearMax);
+    s |= dalloc(&sv->nu_k, (size_t)M * kNearMax);
+    s |= dalloc(&sv->nu_corr, (size_t)M * kNearMax * 3);
+    if (s) {
+      sv->free_near();
+      return s;
+    }
+    sv->nu_trg_cap = M;
+  }
+  // upsampled sources
+  if ((s = launch_synthesis(sv->Sx, nv * 3, p, q, T.syn1_leg, T.syn1_dleg, T.syn1_four, T.syn1_dfour, T.blk_off,
+                            sv->nu_X, sv->nu_Xt, sv->nu_Xp, st)))
+    return s;
+  if ((s = launch_synthesis(sv->Fc, nv * 3, p, q, T.syn1_leg, T.syn1_dleg, T.syn1_four, T.syn1_dfour, T.blk_off,
+                            sv->nu_F, nullptr, nullptr, st)))
+    return s;
+  if ((s = launch_far_sources(sv->nu_X, sv->nu_F, sv->nu_Xt, sv->nu_Xp, nv, q, sv->nu_w, sv->nu_area, sv->nu_pos,
+                              sv->nu_den, st)))
+    return s;
+  if (dl) {
+    if ((s = launch_synthesis(sv->Gc, nv * 3, p, q, T.syn1_leg, T.syn1_dleg, T.syn1_four, T.syn1_dfour, T.blk_off,
+                              sv->nu_G, nullptr, nullptr, st)))
+      return s;
+    if ((s = launch_unit_normals(sv->nu_Xt, sv->nu_Xp, nv, q, sv->nu_nrm, st))) return s;
+    if ((s = launch_far_density(sv->nu_G, sv->nu_area, nv, q, sv->nu_w, sv->nu_dden, st))) return s;
+  }
+  // the smooth quadrature of every vesicle at every target
+  if ((s = launch_targets_f64(sv->nu_pos, sv->nu_den, dl ? sv->nu_nrm : nullptr, dl ? sv->nu_dden : nullptr,
+                              nv * ng1, sv->trg, M, sv->vtrg, st)))
+    return s;
+  // r_near = r_ves 2 / sqrt(p_up) (src/NearSingular.cc:160, :119-158)
+  if ((s = launch_centroid_radius(sv->X, nv, p, sv->nu_cen, sv->nu_rmax, st))) return s;
+  unsigned long long bits = 0;
+  VES3D_CK(cudaMemcpyAsync(&bits, sv->nu_rmax, sizeof(bits), cudaMemcpyDeviceToHost, st));
+  VES3D_CK(cudaStreamSynchronize(st));
+  double r_ves;
+  std::memcpy(&r_ves, &bits, sizeof(double));
+  sv->near_r = r_ves * 2.0 / std::sqrt((double)q);
+  if ((s = launch_near_find(sv->trg, M, sv->nu_cen, nv, sv->nu_pos, q, sv->near_r, sv->nu_count, sv->nu_v, sv->nu_k,
+                            st)))
+    return s;
+  {  // more near vesicles than slots for some target: an error, not a silent truncation
+    std::vector<int> c(M);
+    VES3D_CK(cudaMemcpyAsync(c.data(), sv->nu_count, M * sizeof(int), cudaMemcpyDeviceToHost, st));
+    VES3D_CK(cudaStreamSynchronize(st));
+    for (long t = 0; t < M; t++)
+      if (c[t] > kNearMax) {
+        set_error("target %ld is near more than %d vesicles (the near-singular correction's limit)", t, kNearMax);
+        return VES3D_ERR_ARG;
+      }
+  }
+  return launch_near_correct(sv->trg, M, sv->nu_count, sv->nu_v, sv->nu_k, sv->Sx, sv->Vc, dl ? sv->Gc : nullptr,
+                             sv->nu_pos, sv->nu_den, dl ? sv->nu_nrm : nullptr, dl ? sv->nu_dden : nullptr,
+                             sv->nu_theta, T.blk_off, p, q, sv->near_r, sv->nu_corr, sv->vtrg, st);
+}
+
+}  // namespace
+
 extern "C" {
 
 int ves3d_version(void) { return 100; }
@@ -838,8 +982,37 @@ int ves3d_sv_eval_trg(ves3d_sv* sv, double* vel, int is_device) {
     nrm = sv->nrm;
     dden = sv->dden;
   }
-  if ((s = launch_targets_f64(sv->pos, sv->den, nrm, dden, sv->npts(), sv->trg, sv->trg_n, sv->vtrg, st))) return s;
+  if (sv->near_on) {
+    if ((s = eval_trg_near(sv))) return s;
+  } else if ((s = launch_targets_f64(sv->pos, sv->den, nrm, dden, sv->npts(), sv->trg, sv->trg_n, sv->vtrg, st))) {
+    return s;
+  }
   return copy_out(vel, sv->vtrg, 3 * (size_t)sv->trg_n, is_device, st);
+}
+
+int ves3d_sv_set_near_singular(ves3d_sv* sv, int on) {
+  int s = check_sv(sv);
+  if (s) return s;
+  VES3D_ARG(sv->p + 1 <= 32, "the near-singular correction supports orders up to 31");
+  sv->near_on = on != 0;
+  return VES3D_OK;
+}
+
+int ves3d_sv_near_info(ves3d_sv* sv, double* r_near, long* n_near) {
+  int s = check_sv(sv);
+  if (s) return s;
+  if (r_near) *r_near = sv->near_r;
+  if (n_near) {
+    long n = 0;
+    if (sv->near_on && sv->nu_count && sv->trg_n > 0) {
+      std::vector<int> c(sv->trg_n);
+      VES3D_CK(cudaMemcpyAsync(c.data(), sv->nu_count, c.size() * sizeof(int), cudaMemcpyDeviceToHost, sv->stream));
+      VES3D_CK(cudaStreamSynchronize(sv->stream));
+      for (int x : c) n += x;
+    }
+    *n_near = n;
+  }
+  return VES3D_OK;
 }
 
 int ves3d_sv_set_order_up(ves3d_sv* sv, int sh_order_up) {

@@ -183,6 +183,18 @@ class StokesVelocity:
         check(lib().ves3d_sv_stage_times(self._h, ms), "stage_times")
         return {"setup_ms": ms[0], "self_apply_ms": ms[1], "far_ms": ms[2], "eval_ms": ms[3]}
 
+    def set_near_singular(self, on=True):
+        """Near-singular correction of the off-surface targets (NearSingular): with it on,
+        eval_targets() is accurate up to the surfaces."""
+        check(lib().ves3d_sv_set_near_singular(self._h, 1 if on else 0), "set_near_singular")
+
+    def near_info(self):
+        """(r_near, number of corrected (target, vesicle) pairs) of the last evaluation."""
+        r = ctypes.c_double()
+        n = ctypes.c_long()
+        check(lib().ves3d_sv_near_info(self._h, ctypes.byref(r), ctypes.byref(n)), "near_info")
+        return r.value, n.value
+
     def far_dl_ms(self):
         """Device ms of the far double layer's kernels in the last evaluation (0 without
         a double-layer density)."""
