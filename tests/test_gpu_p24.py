@@ -1,7 +1,8 @@
 """Order p = 24 (a quarter of the polydisperse 4,096-vesicle suspension) and the full
-512-vesicle p = 16 suspension against the oracle. At p = 24 the self-matrix build takes
-the stage-by-stage path (the fused ring kernel is instantiated up to p = 16) and the
-CUDA-core form of the rotate-transpose, neither of which the smaller orders reach.
+512-vesicle p = 16 suspension against the oracle. At p = 24 the self-matrix build runs the
+fused ring with one CTA per SM (its tables fill the shared memory) and the CUDA-core form
+of the rotate-transpose, which the smaller orders do not reach; the stage-by-stage build
+(VES3D_FUSED_BUILD=0) is checked at p = 24 too.
 Tolerances: 1e-12 relative max-norm for FP64 against the oracle, 1e-6 for the mixed
 form, 5e-9 against the reference's own output (its self-part noise floor)."""
 import os
@@ -24,6 +25,16 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref
 def test_p24_self_matrix_matches_oracle():
     p = 24
     X = ellipsoid_pair(p)
+    with StokesVelocity(p, 2 * p) as sv:
+        sv.SetSrcCoord(X)
+        SL = sv.self_matrix()
+    assert rel_err(SL, sh.stokes_singular_matrix(X, p, 2 * p)) < TOL
+
+
+def test_p24_stage_by_stage_build_matches_oracle(monkeypatch):
+    monkeypatch.setenv("VES3D_FUSED_BUILD", "0")
+    p = 24
+    X = ellipsoid_pair(p)[: 3 * sh.ngrid(p)]
     with StokesVelocity(p, 2 * p) as sv:
         sv.SetSrcCoord(X)
         SL = sv.self_matrix()

@@ -93,8 +93,10 @@ struct RingCfg {
 
 // Persistent: each CTA stages the DFT tables and the small index tables once, then walks
 // rotations blockIdx.x, blockIdx.x + gridDim.x, ...
+// Two CTAs per SM up to p = 16; at p = 24 the tables and stage buffers take ~208 KB of
+// shared memory and one CTA fills the SM.
 template <int P0>
-__global__ void __launch_bounds__(256, 2) k_build_ring(const double* __restrict__ R, DevTables T,
+__global__ void __launch_bounds__(256, (P0 <= 16 ? 2 : 1)) k_build_ring(const double* __restrict__ R, DevTables T,
                                                        double* __restrict__ C, long nrot) {
   using G = RingCfg<P0>;
   extern __shared__ __align__(16) double sm[];
@@ -337,7 +339,7 @@ static int launch_ring(const double* R, long nrot, const DevTables& T, double* C
   int dev = 0, nsm = 148;
   VES3D_CK(cudaGetDevice(&dev));
   VES3D_CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  const long grid = std::min(nrot, (long)nsm * ring_ctas_per_sm());
+  const long grid = std::min(nrot, (long)nsm * (P0 <= 16 ? ring_ctas_per_sm() : 1));
   k_build_ring<P0><<<(unsigned)grid, 256, G::SMEM, st>>>(R, T, C, nrot);
   VES3D_LAUNCHED();
   return VES3D_OK;
@@ -997,7 +999,7 @@ bool fused_build_supported(int p0, int p1) {
   if (p1 != 2 * p0) return false;
   // the tensor-core tiling needs 2 p0 % 8 == 0 and 4 p0 % 16 == 0
   switch (p0) {
-    case 4: case 8: case 12: case 16: return true;
+    case 4: case 8: case 12: case 16: case 24: return true;
     default: return false;
   }
 }
@@ -1009,6 +1011,7 @@ int launch_build_ring(const double* R, long nrot, const DevTables& T, double* C,
     case 8: return launch_ring<8>(R, nrot, T, C, st);
     case 12: return launch_ring<12>(R, nrot, T, C, st);
     case 16: return launch_ring<16>(R, nrot, T, C, st);
+    case 24: return launch_ring<24>(R, nrot, T, C, st);
     default:
       set_error("fused build not instantiated for p = %d", T.p0);
       return VES3D_ERR_ARG;
