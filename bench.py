@@ -374,6 +374,9 @@ def implicit_step_measurement(local, stream, steps=2, forms=None):
                 rec["guess_relres"] = info["relres"]
                 rec["start_relres"] = info["relres_combined"]
                 rec["guess_weights"] = info["weights"]
+                # host wall time of the network's prediction and of the combination (its
+                # FP64 right-hand side and operator applications), inside the step's time
+                rec["guess_s"] = {"predict": info.get("predict_s"), "combine": info.get("combine_s")}
             if pc == "self_block":
                 pi = sv.precond_info()
                 if pi["age"] == 0:

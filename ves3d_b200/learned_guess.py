@@ -242,9 +242,10 @@ def initial_guess(sv, learned=None, previous=None):
         names.append("previous")
     if not cands:
         return None, {}
+    t0 = time.perf_counter()
     x0, w, r = sv.implicit_combine(cands)
     info = {"candidates": names, "weights": w.tolist(), "relres": dict(zip(names, r[:-1].tolist())),
-            "relres_combined": float(r[-1])}
+            "relres_combined": float(r[-1]), "combine_s": time.perf_counter() - t0}
     if learned is not None:
         info["predict_s"] = t_pred
     return x0, info
