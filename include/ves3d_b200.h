@@ -180,6 +180,17 @@ int ves3d_svp_create(int precision, int device, ves3d_svp** out);
 int ves3d_svp_destroy(ves3d_svp* g);
 int ves3d_svp_set_src_coord(ves3d_svp* g, const double* S, const int* orders, long n_ves, int is_device);
 int ves3d_svp_set_density_sl(ves3d_svp* g, const double* f, int is_device);
+/* SetDensityDL over the suspension (src/StokesVelocity.cc:107-142): the double layer of g
+ * (same layout as f; NULL: off) is added to ves3d_svp_eval's velocity, each vesicle's self
+ * part at its own order and the far double layer (FP64) over every point of the other
+ * vesicles. Invalidated by ves3d_svp_set_src_coord and by an implicit solve under a
+ * viscosity contrast (which takes the double-layer buffers for its operator). */
+int ves3d_svp_set_density_dl(ves3d_svp* g, const double* gdl, int is_device);
+/* Viscosity contrast of the suspension's implicit step (VesicleProps::viscosity_contrast,
+ * as ves3d_sv_set_viscosity_contrast): lambda[n], n = 1 (every vesicle) or n_ves in vesicle
+ * order; NULL or n = 0 removes it. The operator becomes (1 + lambda)/2 u - S[f] -
+ * D[(1 - lambda) u] with the double layer over the whole suspension. */
+int ves3d_svp_set_viscosity_contrast(ves3d_svp* g, const double* lambda, long n);
 int ves3d_svp_setup(ves3d_svp* g);
 int ves3d_svp_eval(ves3d_svp* g, double* vel, int is_device);
 /* ms[0] self-matrix builds, ms[1] self parts, ms[2] far field, ms[3] whole last eval. */

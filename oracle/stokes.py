@@ -148,15 +148,24 @@ def unit_normal(X, p):
     return (n / np.sqrt((n * n).sum(axis=1))[:, None, :]).reshape(-1)
 
 
+def far_dl(X, nrm, D, pt_off):
+    """Far double layer at every point over the points of the other vesicles: positions,
+    unit normals and weighted densities as per-vesicle AxisMajor blocks at offsets pt_off.
+    Returns [N][3] point-major."""
+    pt_off = np.ascontiguousarray(pt_off, np.int64)
+    out = np.empty(3 * int(pt_off[-1]))
+    direct_lib().oracle_far_dl(_p(np.ascontiguousarray(X, np.float64)), _p(np.ascontiguousarray(nrm, np.float64)),
+                               _p(np.ascontiguousarray(D, np.float64)), ctypes.c_long(pt_off.size - 1),
+                               pt_off.ctypes.data_as(_lp), _p(out))
+    return out.reshape(-1, 3)
+
+
 def far_dl_velocity(X, g, p):
     """Far double layer at every point, AxisMajor: the points of the other vesicles with unit
     normals and densities g * area * qw (the single layer's composition)."""
     ng = sh.ngrid(p)
     nves = np.asarray(X).size // (3 * ng)
-    D = far_density(X, g, p)
-    out = np.empty(3 * nves * ng)
-    direct_lib().oracle_far_dl(_p(np.ascontiguousarray(X, np.float64)), _p(unit_normal(X, p)), _p(D),
-                               ctypes.c_long(nves), uniform_offsets(nves, p).ctypes.data_as(_lp), _p(out))
+    out = far_dl(X, unit_normal(X, p), far_density(X, g, p), uniform_offsets(nves, p))
     return out.reshape(nves, ng, 3).transpose(0, 2, 1).reshape(-1)
 
 
@@ -193,9 +202,11 @@ def target_velocity(X, f, p, T, g=None):
     return u.reshape(3, M).T.reshape(-1)
 
 
-def stokes_velocity_poly(X, f, orders):
+def stokes_velocity_poly(X, f, orders, g=None):
     """FP64 velocity of a polydisperse suspension (per-vesicle AxisMajor blocks concatenated;
-    each vesicle's self part at its own order, p_up = 2p)."""
+    each vesicle's self part at its own order, p_up = 2p). With g, the double layer of g as
+    well: each vesicle's DL matrix at its own order and the far double layer over the points
+    of the other vesicles (SetDensityDL, src/StokesVelocity.cc:107-142, 418-436)."""
     X = np.asarray(X, np.float64)
     f = np.asarray(f, np.float64)
     orders = np.asarray(orders)
@@ -203,13 +214,24 @@ def stokes_velocity_poly(X, f, orders):
     off = np.concatenate([[0], np.cumsum(ng)]).astype(np.int64)
     D = np.empty_like(f)
     vel = np.empty_like(f)
+    if g is not None:
+        g = np.asarray(g, np.float64)
+        Dg = np.empty_like(g)
+        nrm = np.empty_like(g)
     for v, p in enumerate(orders):
         p = int(p)
         a, b = 3 * off[v], 3 * off[v + 1]
         D[a:b] = far_density(X[a:b], f[a:b], p)
         SL = sh.stokes_singular_matrix(X[a:b], p, 2 * p)
         vel[a:b] = sh.self_apply(SL, f[a:b], p)
+        if g is not None:
+            DL = sh.stokes_singular_matrix(X[a:b], p, 2 * p, single=False)
+            vel[a:b] += sh.self_apply(DL, g[a:b], p)
+            Dg[a:b] = far_density(X[a:b], g[a:b], p)
+            nrm[a:b] = unit_normal(X[a:b], p)
     farv = far(X, D, off)
+    if g is not None:
+        farv = farv + far_dl(X, nrm, Dg, off)
     for v in range(orders.size):
         a = off[v]
         n = ng[v]

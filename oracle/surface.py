@@ -312,7 +312,8 @@ class PolyImplicitStep:
     coefficient vectors are, run after run, [u coefficients; sigma coefficients] of the run
     (the layout of ImplicitStep.to_coef for each run)."""
 
-    def __init__(self, X, orders, kappa, dt, shear_rate, excess_density=0.0, gravity=(0.0, 0.0, -1.0)):
+    def __init__(self, X, orders, kappa, dt, shear_rate, excess_density=0.0, gravity=(0.0, 0.0, -1.0),
+                 viscosity_contrast=None):
         X = np.asarray(X, dtype=np.float64).reshape(-1)
         orders = [int(q) for q in orders]
         self.runs = []  # (p, first vesicle, vesicles, first point)
@@ -323,10 +324,29 @@ class PolyImplicitStep:
             self.runs[-1][2] += 1
             pt += sh.ngrid(q)
         self.N = pt
+        lam = np.broadcast_to(np.asarray(1.0 if viscosity_contrast is None else viscosity_contrast, np.float64),
+                              (len(orders),)).copy()
+        self.contrast = bool(np.any(np.abs(lam - 1.0) > 1e-12))
         self.steps = [ImplicitStep(X[3 * r[3]:3 * (r[3] + r[2] * sh.ngrid(r[0]))], r[0], kappa, dt, shear_rate,
-                                   excess_density=excess_density, gravity=gravity) for r in self.runs]
+                                   excess_density=excess_density, gravity=gravity,
+                                   viscosity_contrast=lam[r[1]:r[1] + r[2]]) for r in self.runs]
         self.X = X
         self.off = np.concatenate([[0], np.cumsum([sh.ngrid(q) for q in orders])]).astype(np.int64)
+
+    def stokes_dl(self, gs):
+        """Double layer of per-run densities gs[r] ([nv][3][ng]) -> per-run velocities: each
+        run's DL matrices plus the far double layer over every point of the other vesicles."""
+        D = np.concatenate([stokes.far_density(st.X, g.reshape(-1), st.p) for st, g in zip(self.steps, gs)])
+        nrm = np.concatenate([stokes.unit_normal(st.X, st.p) for st in self.steps])
+        farv = stokes.far_dl(self.X, nrm, D, self.off)
+        out = []
+        for r, st, g in zip(self.runs, self.steps, gs):
+            ng = sh.ngrid(r[0])
+            if st._DL is None:
+                st._DL = sh.stokes_singular_matrix(st.X, st.p, 2 * st.p, single=False)
+            fv = farv[r[3]:r[3] + r[2] * ng].reshape(r[2], ng, 3).transpose(0, 2, 1)
+            out.append(sh.self_apply(st._DL, g.reshape(-1), st.p).reshape(r[2], 3, ng) + fv)
+        return out
 
     def stokes(self, fs):
         """Single layer of per-run tractions fs[r] ([nv][3][ng]) -> per-run velocities."""
@@ -359,6 +379,11 @@ class PolyImplicitStep:
                 f = f + gravity_force(st.dt * u, st.geo, st.drho, st.g)
             fs.append(f)
         Sf = self.stokes(fs)
+        if self.contrast:  # (1 + lambda)/2 u - S[f] - D[(1 - lambda) u] over the suspension
+            Df = self.stokes_dl([st.dl_coeff * u for st, u in zip(self.steps, us)])
+            Sf = [v + w for v, w in zip(Sf, Df)]
+            return self.join([st.vel_coeff * u - v for st, u, v in zip(self.steps, us, Sf)],
+                             [-div(v, st.geo) for st, v in zip(self.steps, Sf)])
         return self.join([u - v for u, v in zip(us, Sf)], [-div(v, st.geo) for st, v in zip(self.steps, Sf)])
 
     def rhs(self):

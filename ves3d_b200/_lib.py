@@ -88,6 +88,8 @@ SIGNATURES = [
     ("ves3d_svp_destroy", _i, [_vp]),
     ("ves3d_svp_set_src_coord", _i, [_vp, _vp, _vp, _l, _i]),
     ("ves3d_svp_set_density_sl", _i, [_vp, _vp, _i]),
+    ("ves3d_svp_set_density_dl", _i, [_vp, _vp, _i]),
+    ("ves3d_svp_set_viscosity_contrast", _i, [_vp, _vp, _l]),
     ("ves3d_svp_setup", _i, [_vp]),
     ("ves3d_svp_eval", _i, [_vp, _vp, _i]),
     ("ves3d_svp_stage_times", _i, [_vp, ctypes.POINTER(ctypes.c_float)]),

@@ -153,9 +153,9 @@ __device__ __forceinline__ void pair_dl64(const double* s, double tx, double ty,
 // point-major [N][3]; part [seg][N][3].
 __global__ void __launch_bounds__(512) k_far_dl_f64_seg(const double* __restrict__ pos, const double* __restrict__ nrm,
                                                         const double* __restrict__ dden, const long* __restrict__ off,
-                                                        long N, int seg_tiles, double* __restrict__ part) {
+                                                        long N, int seg_tiles, int v0, double* __restrict__ part) {
   __shared__ __align__(16) double sm[kTileF64 * 9];
-  const int v = blockIdx.y, seg = blockIdx.x;
+  const int v = v0 + blockIdx.y, seg = blockIdx.x;
   const long t0 = off[v], nt = off[v + 1] - t0;
   const int nthr = blockDim.x;
   const long c0 = (long)blockIdx.z * 2 * nthr;
@@ -704,24 +704,43 @@ std::string autotune_report() {
   return r;
 }
 
-int launch_far_dl(const double* pos, const double* nrm, const double* dden, const long* off, long nves, long N,
-                  int max_nt, double* part, long part_cap_segments, cudaStream_t st, int* nseg_out) {
+// The far double layer of a suspension in order groups: one launch per group (its own
+// target chunking and block shape), one segment layout for all, as launch_far_shape.
+int launch_far_dl_groups(const double* pos, const double* nrm, const double* dden, const long* off, long nves, long N,
+                         const FarGroup* groups, int ngroups, double* part, long part_cap_segments, cudaStream_t st,
+                         int* nseg_out) {
   *nseg_out = 0;
   if (N <= 0 || nves <= 0) return VES3D_OK;
-  int nchunk, nthr;
-  chunking(max_nt, 1024, 2, &nchunk, &nthr);
+  long nthr_sum = 0, nchunk_tot = 0;
+  for (int g = 0; g < ngroups; g++) {
+    int nc, nt;
+    chunking(groups[g].nt, 1024, 2, &nc, &nt);
+    nthr_sum += (long)nt * groups[g].nv;
+    nchunk_tot += (long)nc * groups[g].nv;
+  }
   int seg_tiles = 1;
-  int nseg = far_segments((long)nchunk * nves, N, kTileF64, nthr, 8, &seg_tiles);
+  int nseg = far_segments(nchunk_tot, N, kTileF64, (int)(nthr_sum / nves), 8, &seg_tiles);
   if (nseg > part_cap_segments) {
     const long ntiles = (N + kTileF64 - 1) / kTileF64;
     seg_tiles = (int)((ntiles + part_cap_segments - 1) / part_cap_segments);
     nseg = (int)((ntiles + seg_tiles - 1) / seg_tiles);
   }
-  dim3 grid(nseg, (unsigned)nves, nchunk);
-  k_far_dl_f64_seg<<<grid, nthr, 0, st>>>(pos, nrm, dden, off, N, seg_tiles, part);
-  VES3D_LAUNCHED();
+  for (int g = 0; g < ngroups; g++) {
+    if (groups[g].nv <= 0) continue;
+    int nchunk, nthr;
+    chunking(groups[g].nt, 1024, 2, &nchunk, &nthr);
+    dim3 grid(nseg, (unsigned)groups[g].nv, nchunk);
+    k_far_dl_f64_seg<<<grid, nthr, 0, st>>>(pos, nrm, dden, off, N, seg_tiles, (int)groups[g].v0, part);
+    VES3D_LAUNCHED();
+  }
   *nseg_out = nseg;
   return VES3D_OK;
+}
+
+int launch_far_dl(const double* pos, const double* nrm, const double* dden, const long* off, long nves, long N,
+                  int max_nt, double* part, long part_cap_segments, cudaStream_t st, int* nseg_out) {
+  FarGroup g{0, nves, max_nt};
+  return launch_far_dl_groups(pos, nrm, dden, off, nves, N, &g, 1, part, part_cap_segments, st, nseg_out);
 }
 
 int launch_far(bool mixed, const double* pos, const double* den, const long* off, long nves, long N, int max_nt,

@@ -151,6 +151,11 @@ std::string autotune_report();
 int launch_far_groups(bool mixed, const double* pos, const double* den, const long* off, long nves, long N,
                       const FarGroup* groups, int ngroups, const double* add, double* out, double* far_out,
                       double* part, long part_cap_segments, cudaStream_t st, int* nseg_out = nullptr);
+// launch_far_dl over order groups (a polydisperse suspension): per-group block shapes, one
+// segment layout.
+int launch_far_dl_groups(const double* pos, const double* nrm, const double* dden, const long* off, long nves, long N,
+                         const FarGroup* groups, int ngroups, double* part, long part_cap_segments, cudaStream_t st,
+                         int* nseg_out);
 // out = a + b elementwise.
 int launch_add(const double* a, const double* b, long n, double* out, cudaStream_t st);
 // All pairs, point-major in/out (StokesAlltoAll semantics).

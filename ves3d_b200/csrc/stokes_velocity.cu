@@ -528,18 +528,27 @@ int run_setup(ves3d_sv* sv, bool dl) {
 
 // Self part of an evaluation: Vself = SHC2Grid(Grid2SHC(F) . SL) and the weighted far-field
 // density den = F * area * qw, written to the given buffers (the context's own, or slices
-// of a polydisperse suspension's global arrays).
-int run_self(ves3d_sv* sv, double* vself, double* den) {
+// of a polydisperse suspension's global arrays). With nrm given, the double layer of the
+// density in G as well: Grid2SHC(G) . DL added in coefficients, and the far double layer's
+// unit normals (nrm) and weighted density dden = G * area * qw.
+int run_self(ves3d_sv* sv, double* vself, double* den, double* nrm = nullptr, double* dden = nullptr) {
   const DevTables& T = sv->tab->d;
   const int p0 = sv->p, n = 3 * ncoef_(p0);
   cudaStream_t st = sv->stream;
   int s;
   if ((s = launch_grid2shc(sv->F, sv->nves * 3, p0, T.ana_four, T.ana_leg, T.jf_of_coef, sv->Fc, st))) return s;
   if ((s = launch_self_gemv(sv->Fc, sv->SL, sv->nves, n, sv->Vc, st))) return s;
+  if (nrm) {
+    if ((s = launch_grid2shc(sv->G, sv->nves * 3, p0, T.ana_four, T.ana_leg, T.jf_of_coef, sv->Gc, st))) return s;
+    if ((s = launch_self_gemv(sv->Gc, sv->DL, sv->nves, n, sv->Vc, st, /*accumulate=*/true))) return s;
+  }
   if ((s = launch_synthesis(sv->Vc, sv->nves * 3, p0, p0, T.syn0_leg, T.syn0_dleg, T.syn0_four, T.syn0_dfour,
                             T.blk_off, vself, nullptr, nullptr, st)))
     return s;
-  return launch_far_density(sv->F, sv->area, sv->nves, p0, T.smooth_w0, den, st);
+  if ((s = launch_far_density(sv->F, sv->area, sv->nves, p0, T.smooth_w0, den, st))) return s;
+  if (!nrm) return VES3D_OK;
+  if ((s = launch_unit_normals(sv->Xt, sv->Xp, sv->nves, p0, nrm, st))) return s;
+  return launch_far_density(sv->G, sv->area, sv->nves, p0, T.smooth_w0, dden, st);
 }
 
 // Self part alone: Vself = SHC2Grid(Grid2SHC(F) . SL [+ Grid2SHC(G) . DL]) on the
@@ -2988,6 +2997,13 @@ struct ves3d_svp {
   long* off = nullptr;
   long capN = 0, capV = 0;
   bool have_den = false;
+  // double layer: a density set by ves3d_svp_set_density_dl (in the groups' G buffers), or
+  // the implicit step's (1 - lambda) u under a viscosity contrast; unit normals, weighted
+  // densities and far partials over all points
+  bool have_dl = false;
+  double *nrm = nullptr, *dden = nullptr, *part_dl = nullptr;
+  std::vector<double> lam;  // viscosity contrast: one value, or one per vesicle
+  bool contrast = false;
   cudaEvent_t ev[4] = {};
   float ms[4] = {0, 0, 0, 0};
   cudaGraph_t graph = nullptr;  // captured evaluation (self parts of every group + far field)
@@ -3011,10 +3027,10 @@ struct ves3d_svp {
     graph = nullptr;
   }
   void free_global() {
-    double* ps[] = {pos, den, vself, V, Vfar, part};
+    double* ps[] = {pos, den, vself, V, Vfar, part, nrm, dden, part_dl};
     for (double* q : ps) dfree(q);
     dfree(off);
-    pos = den = vself = V = Vfar = part = nullptr;
+    pos = den = vself = V = Vfar = part = nrm = dden = part_dl = nullptr;
     off = nullptr;
     capN = capV = 0;
   }
@@ -3139,6 +3155,7 @@ int ves3d_svp_set_src_coord(ves3d_svp* g, const double* S, const int* orders, lo
   }
   VES3D_CK(cudaStreamSynchronize(g->stream));
   g->have_den = false;
+  g->have_dl = false;
   return VES3D_OK;
 }
 
@@ -3153,28 +3170,87 @@ int ves3d_svp_set_density_sl(ves3d_svp* g, const double* f, int is_device) {
   return VES3D_OK;
 }
 
+// Double-layer buffers of the suspension (normals, weighted densities, far partials) and of
+// every group (density, coefficients, self matrices).
+static int svp_alloc_dl(ves3d_svp* g) {
+  int s = 0;
+  for (ves3d_sv* sv : g->grp)
+    if ((s = alloc_dl(sv))) return s;
+  if (g->nrm) return VES3D_OK;
+  s |= dalloc(&g->nrm, 3 * (size_t)g->capN);
+  s |= dalloc(&g->dden, 3 * (size_t)g->capN);
+  s |= dalloc(&g->part_dl, (size_t)kFarMaxSegments * 3 * g->capN);
+  if (s) {
+    dfree(g->nrm);
+    dfree(g->dden);
+    dfree(g->part_dl);
+    g->nrm = g->dden = g->part_dl = nullptr;
+  }
+  return s;
+}
+
+int ves3d_svp_set_density_dl(ves3d_svp* g, const double* gdl, int is_device) {
+  VES3D_ARG(g != nullptr, "null context");
+  VES3D_ARG(!g->grp.empty(), "set_src_coord first");
+  if (!gdl) {  // SetDensityDL(NULL): the double layer off
+    if (g->have_dl) g->drop_graph();
+    g->have_dl = false;
+    return VES3D_OK;
+  }
+  int s;
+  if ((s = svp_alloc_dl(g))) return s;
+  for (size_t r = 0; r < g->grp.size(); r++)
+    if ((s = copy_in(g->grp[r]->G, gdl + 3 * g->gpt0[r], 3 * (size_t)g->grp[r]->npts(), is_device, g->stream)))
+      return s;
+  if (!g->have_dl) g->drop_graph();  // a captured evaluation without the double layer
+  g->have_dl = true;
+  return VES3D_OK;
+}
+
+int ves3d_svp_set_viscosity_contrast(ves3d_svp* g, const double* lambda, long n) {
+  VES3D_ARG(g != nullptr, "null context");
+  g->rhs_valid = false;
+  if (!lambda || n == 0) {
+    g->lam.clear();
+    g->contrast = false;
+    return VES3D_OK;
+  }
+  VES3D_ARG(n == 1 || (!g->grp.empty() && n == g->nves), "n must be 1 or the number of vesicles");
+  for (long i = 0; i < n; i++) VES3D_ARG(std::isfinite(lambda[i]) && lambda[i] > 0.0, "contrast must be positive");
+  g->lam.assign(lambda, lambda + n);
+  bool any = false;
+  for (double l : g->lam) any |= std::fabs(l - 1.0) > 1e-12;  // has_contrast, VesicleProps.cc:45-49
+  g->contrast = any;
+  return VES3D_OK;
+}
+
 int ves3d_svp_setup(ves3d_svp* g) {
   VES3D_ARG(g != nullptr, "null context");
   VES3D_ARG(!g->grp.empty(), "set_src_coord first");
   for (ves3d_sv* sv : g->grp) {
-    if (!sv->sl_valid) {
-      int s = run_setup(sv);
-      if (s) return s;
-    }
+    int s;
+    if (!sv->sl_valid && (s = run_setup(sv))) return s;
+    if (g->have_dl && !sv->dl_valid && (s = run_setup(sv, true))) return s;
   }
   return VES3D_OK;
 }
 
-static int svp_self_parts(ves3d_svp* g) {
+// every group's self part (with dl, of both layers: the DL matrices are built on first use)
+static int svp_self_parts(ves3d_svp* g, bool dl) {
   for (size_t r = 0; r < g->grp.size(); r++) {
-    const int s = run_self(g->grp[r], g->vself + 3 * g->gpt0[r], g->den + 3 * g->gpt0[r]);
-    if (s) return s;
+    ves3d_sv* sv = g->grp[r];
+    int s;
+    if (dl && !sv->dl_valid && (s = run_setup(sv, true))) return s;
+    const long o = 3 * g->gpt0[r];
+    if ((s = run_self(sv, g->vself + o, g->den + o, dl ? g->nrm + o : nullptr, dl ? g->dden + o : nullptr)))
+      return s;
   }
   return VES3D_OK;
 }
 
-// one far-field pass over every point, launched per order group (block shape per group)
-static int svp_far(ves3d_svp* g) {
+// one far-field pass over every point, launched per order group (block shape per group);
+// with dl the far double layer (FP64) as a second set of partials of the same reduce
+static int svp_far(ves3d_svp* g, bool dl) {
   NvtxRange nvtx("ves3d far");
   const bool mixed = g->prec == VES3D_PREC_MIXED && !g->far_force_fp64;
   std::vector<FarGroup> fg;
@@ -3183,8 +3259,18 @@ static int svp_far(ves3d_svp* g) {
     fg.push_back(FarGroup{v0, g->gnv[r], ngrid_(g->gp[r])});
     v0 += g->gnv[r];
   }
-  return launch_far_groups(mixed, g->pos, g->den, g->off, g->nves, g->N, fg.data(), (int)fg.size(), g->vself, g->V,
-                           g->Vfar, g->part, kFarMaxSegments, g->stream);
+  if (!dl)
+    return launch_far_groups(mixed, g->pos, g->den, g->off, g->nves, g->N, fg.data(), (int)fg.size(), g->vself, g->V,
+                             g->Vfar, g->part, kFarMaxSegments, g->stream);
+  int s, nseg = 0, nseg_dl = 0;
+  if ((s = launch_far_groups(mixed, g->pos, g->den, g->off, g->nves, g->N, fg.data(), (int)fg.size(), nullptr,
+                             nullptr, nullptr, g->part, kFarMaxSegments, g->stream, &nseg)))
+    return s;
+  if ((s = launch_far_dl_groups(g->pos, g->nrm, g->dden, g->off, g->nves, g->N, fg.data(), (int)fg.size(),
+                                g->part_dl, kFarMaxSegments, g->stream, &nseg_dl)))
+    return s;
+  return launch_far_reduce(g->part, nseg, g->off, g->nves, g->N, g->vself, g->V, g->Vfar, g->stream, g->part_dl,
+                           nseg_dl, kDl);
 }
 
 int ves3d_svp_capture_eval(ves3d_svp* g) {
@@ -3198,11 +3284,11 @@ int ves3d_svp_capture_eval(ves3d_svp* g) {
   int s;
   if ((s = ves3d_svp_setup(g))) return s;
   // one eager pass first: kernel attributes are set outside the capture
-  if ((s = svp_self_parts(g)) || (s = svp_far(g))) return s;
+  if ((s = svp_self_parts(g, g->have_dl)) || (s = svp_far(g, g->have_dl))) return s;
   VES3D_CK(cudaStreamSynchronize(g->stream));
   VES3D_CK(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal));
-  s = svp_self_parts(g);
-  if (!s) s = svp_far(g);
+  s = svp_self_parts(g, g->have_dl);
+  if (!s) s = svp_far(g, g->have_dl);
   cudaGraph_t gr = nullptr;
   const cudaError_t e = cudaStreamEndCapture(g->stream, &gr);
   if (!s && e != cudaSuccess) s = cuda_status(e, "cudaStreamEndCapture", __FILE__, __LINE__);
@@ -3242,9 +3328,9 @@ int ves3d_svp_eval(ves3d_svp* g, double* vel, int is_device) {
   VES3D_CK(cudaEventRecord(g->ev[0], g->stream));
   if ((s = ves3d_svp_setup(g))) return s;
   VES3D_CK(cudaEventRecord(g->ev[1], g->stream));
-  if ((s = svp_self_parts(g))) return s;
+  if ((s = svp_self_parts(g, g->have_dl))) return s;
   VES3D_CK(cudaEventRecord(g->ev[2], g->stream));
-  if ((s = svp_far(g))) return s;
+  if ((s = svp_far(g, g->have_dl))) return s;
   VES3D_CK(cudaEventRecord(g->ev[3], g->stream));
   VES3D_CK(cudaEventSynchronize(g->ev[3]));
   VES3D_CK(cudaEventElapsedTime(&g->ms[0], g->ev[0], g->ev[1]));
@@ -3273,6 +3359,10 @@ namespace {
 
 int svp_prepare_implicit(ves3d_svp* g) {
   int s;
+  if (g->contrast && g->lam.size() != 1 && (long)g->lam.size() != g->nves) {
+    set_error("viscosity contrast was set for %ld vesicles, the surfaces have %ld", (long)g->lam.size(), g->nves);
+    return VES3D_ERR_STATE;
+  }
   for (ves3d_sv* sv : g->grp) mark_implicit(sv);  // FP64 self matrices before the setup
   if ((s = ves3d_svp_setup(g))) return s;
   g->coff.assign(g->grp.size() + 1, 0);
@@ -3283,6 +3373,19 @@ int svp_prepare_implicit(ves3d_svp* g) {
     if ((s = ves3d_sv_set_precond(sv, g->precond))) return s;
     if ((s = ves3d_sv_set_precond_refresh(sv, g->pc_refresh))) return s;
     if ((s = ves3d_sv_set_surface_filter(sv, g->filter_freq))) return s;
+    // the suspension's viscosity contrast for this group's vesicles (one value: all of
+    // them), pushed only when it changed (a change rebuilds the group's preconditioner)
+    std::vector<double> want;
+    if (g->contrast && g->lam.size() == 1) {
+      want = g->lam;
+    } else if (g->contrast) {
+      long first = 0;
+      for (size_t q = 0; q < r; q++) first += g->gnv[q];
+      want.assign(g->lam.begin() + first, g->lam.begin() + first + g->gnv[r]);
+    }
+    if (want != sv->lam &&
+        (s = ves3d_sv_set_viscosity_contrast(sv, want.empty() ? nullptr : want.data(), (long)want.size())))
+      return s;
     if ((s = ensure_geometry(sv))) return s;
     ImplicitWork iw;
     if ((s = implicit_work(sv, iw))) return s;
@@ -3291,8 +3394,9 @@ int svp_prepare_implicit(ves3d_svp* g) {
   return VES3D_OK;
 }
 
-// g->V = S[f] over the whole suspension, f = every group's iw.f
-int svp_stokes(ves3d_svp* g) {
+// g->V = S[f] over the whole suspension, f = every group's iw.f; with dl plus D[G], G the
+// density in every group's G buffer
+int svp_stokes(ves3d_svp* g, bool dl = false) {
   int s;
   for (ves3d_sv* sv : g->grp) {
     ImplicitWork iw;
@@ -3301,25 +3405,48 @@ int svp_stokes(ves3d_svp* g) {
                              g->stream));
     sv->have_den = true;
   }
-  if ((s = svp_self_parts(g))) return s;
-  return svp_far(g);
+  if ((s = svp_self_parts(g, dl))) return s;
+  return svp_far(g, dl);
 }
 
+// The suspension's implicit operator on SH coefficients c (ImplicitApply,
+// src/InterfacialVelocity.cc:878-966): every group's forces, one evaluation over all points,
+// every group's finish. Under a viscosity contrast the evaluation adds the double layer of
+// (1 - lambda) u and the finish takes (1 + lambda)/2 u - Sf (the groups' own contrast
+// coefficients); the groups' G buffers then belong to the operator.
 int svp_matvec_sh(ves3d_svp* g, const double* c, double* y) {
   int s;
+  const bool con = g->contrast;
+  if (con) {
+    if ((s = svp_alloc_dl(g))) return s;
+    g->have_dl = false;  // the G buffers hold the operator's densities from here on
+    g->drop_graph();
+  }
   for (size_t r = 0; r < g->grp.size(); r++) {
     ves3d_sv* sv = g->grp[r];
     ImplicitWork iw;
     if ((s = implicit_work(sv, iw))) return s;
     if ((s = coef_to_grid(sv, c + g->coff[r], iw.g1))) return s;
     if ((s = implicit_forces(sv, base_space(sv), iw, iw.g1))) return s;
+    if (con) {
+      const long N = sv->npts(), per = 3L * ngrid_(sv->p);
+      if ((s = ensure_contrast(sv))) return s;
+      if ((s = launch_scale_vesicles(iw.g1, 3 * N, per, sv->dlc, sv->nves, nullptr, 0.0, sv->G, g->stream))) return s;
+    }
   }
-  if ((s = svp_stokes(g))) return s;
+  if ((s = svp_stokes(g, con))) return s;
   for (size_t r = 0; r < g->grp.size(); r++) {
     ves3d_sv* sv = g->grp[r];
     ImplicitWork iw;
     if ((s = implicit_work(sv, iw))) return s;
-    if ((s = implicit_finish(sv, base_space(sv), iw.g1, g->V + 3 * g->gpt0[r], iw.g2))) return s;
+    const double* Sf = g->V + 3 * g->gpt0[r];
+    if (!con) {
+      if ((s = implicit_finish(sv, base_space(sv), iw.g1, Sf, iw.g2))) return s;
+    } else {
+      const long N = sv->npts(), per = 3L * ngrid_(sv->p);
+      if ((s = launch_scale_vesicles(iw.g1, 3 * N, per, sv->velc, sv->nves, Sf, -1.0, iw.g2, g->stream))) return s;
+      if ((s = op_div(sv, base_space(sv), Sf, iw.g2 + 3 * N, -1.0))) return s;
+    }
     if ((s = grid_to_coef(sv, iw.g2, y + g->coff[r]))) return s;
   }
   return VES3D_OK;

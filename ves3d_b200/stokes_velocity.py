@@ -461,6 +461,24 @@ class PolydisperseStokesVelocity:
             raise ValueError("density size does not match the surfaces")
         check(lib().ves3d_svp_set_density_sl(self._h, p, dev), "SetDensitySL")
 
+    def SetDensityDL(self, g):
+        """Double-layer density (same layout as SetDensitySL), or None to switch it off."""
+        if g is None:
+            check(lib().ves3d_svp_set_density_dl(self._h, None, 0), "SetDensityDL")
+            return
+        p, dev, n = _ptr(g)
+        if n != 3 * self.npoints():
+            raise ValueError("density size does not match the surfaces")
+        check(lib().ves3d_svp_set_density_dl(self._h, p, dev), "SetDensityDL")
+
+    def set_viscosity_contrast(self, lam):
+        """Viscosity contrast of the implicit step: one value, one per vesicle, or None."""
+        if lam is None:
+            check(lib().ves3d_svp_set_viscosity_contrast(self._h, None, 0), "set_viscosity_contrast")
+            return
+        a = np.ascontiguousarray(np.atleast_1d(np.asarray(lam, dtype=np.float64)))
+        check(lib().ves3d_svp_set_viscosity_contrast(self._h, a.ctypes.data, a.size), "set_viscosity_contrast")
+
     def setup(self):
         check(lib().ves3d_svp_setup(self._h), "setup")
 
