@@ -684,7 +684,7 @@ def double_layer_measurement(X, f, p, local, stream, steps=3):
     return {"what": "512-vesicle p=16 evaluation with single- and double-layer densities, FP64; surfaces and "
                     "self matrices built before the timed evaluations",
             "eval_ms": statistics.mean(evals), "far_dl_ms": ms, "first_eval_with_dl_build_s": first_s,
-            "far_dl_roofline": {"kernel": "k_far_dl_f64_seg", "bound": "fp64_pipe", "achieved": achieved,
+            "far_dl_roofline": {"kernel": "k_far_dl_f64_flat", "bound": "fp64_pipe", "achieved": achieved,
                                 "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                                 "work": f"{DL_FLOPS_PER_PAIR} flops per (target, source) pair x {pairs} pairs"}}
 

@@ -155,15 +155,14 @@ int ves3d_sv_launch_eval_graph(ves3d_sv* sv);
 /* Far-field launch-shape autotuner (no reference counterpart), process-wide, off by
  * default (or VES3D_AUTOTUNE=1): on the first far-field launch of a configuration
  * (precision, points, vesicles and their sizes) every candidate shape -- waves of CTAs
- * per SM in {4, 8, 16} x targets per CTA in {512, 1024} x (FP64 form) targets per thread
- * in {2, 4} -- is timed once with CUDA events and the fastest is kept. Never tunes during
- * stream capture. */
+ * per SM in {4, 8, 16} x threads per CTA in {256, 384} (two targets each; the mixed form
+ * 256 only, for its accuracy) -- is timed once with CUDA events and the fastest is kept.
+ * Never tunes during stream capture. */
 int ves3d_set_autotune(int on);
-/* Fix the far-field launch shape instead (waves in {4, 8, 16}, targets per CTA in
- * {512, 1024}, targets per thread in {2, 4}, the last for the FP64 form); waves = 0
- * returns to the default / autotuned shape. */
-int ves3d_set_far_shape(int waves, int chunk_max, int targets_per_thread);
-/* Text report of the tuned configurations, one line each ("key waves=W chunk=C ms=T");
+/* Fix the far-field launch shape instead (waves in {4, 8, 16}, threads per CTA in
+ * {256, 384}, targets per thread 2); waves = 0 returns to the default / autotuned shape. */
+int ves3d_set_far_shape(int waves, int threads, int targets_per_thread);
+/* Text report of the tuned configurations, one line each ("key waves=W threads=T ms=M");
  * *len receives its length (buf may be NULL). */
 int ves3d_autotune_report(char* buf, size_t cap, size_t* len);
 

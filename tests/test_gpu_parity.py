@@ -259,16 +259,15 @@ def test_far_field_autotuner():
             _lib.set_autotune(False)
     assert any(k.startswith("f64:N=%d:" % (X.size // 3)) for k in rep), rep
     for e in rep.values():
-        assert e["waves"] in (4, 8, 16) and e["chunk"] in (512, 1024) and e["ms"] > 0
+        assert e["waves"] in (4, 8, 16) and e["threads"] in (256, 384) and e["ms"] > 0
     assert rel_err(v1, v_default) < 1e-13
     assert np.array_equal(v1, v2)
 
 
-@pytest.mark.parametrize("shape", [(4, 512, 4), (16, 1024, 4), (8, 512, 2)])
+@pytest.mark.parametrize("shape", [(4, 256, 2), (16, 384, 2), (8, 256, 2)])
 def test_far_field_launch_shapes_agree(shape):
-    """Every launch shape the autotuner may pick (segments, targets per CTA, targets per
-    thread) computes the same far field as the default one to rounding, and matches the
-    oracle to 1e-12."""
+    """Every launch shape the autotuner may pick (segments, threads per CTA) computes the
+    same far field as the default one to rounding, and matches the oracle to 1e-12."""
     p = 8
     X, f = small_suspension(2, p, 73, spacing=2.7)
     with StokesVelocity(p) as sv:

@@ -180,13 +180,13 @@ def set_autotune(on):
     check(lib().ves3d_set_autotune(1 if on else 0), "set_autotune")
 
 
-def set_far_shape(waves=0, chunk=0, targets_per_thread=0):
+def set_far_shape(waves=0, threads=0, targets_per_thread=0):
     """Fix the far-field launch shape (waves=0: back to the default / autotuned one)."""
-    check(lib().ves3d_set_far_shape(int(waves), int(chunk), int(targets_per_thread)), "set_far_shape")
+    check(lib().ves3d_set_far_shape(int(waves), int(threads), int(targets_per_thread)), "set_far_shape")
 
 
 def autotune_report():
-    """{configuration key: {"waves", "chunk", "ms"}} of the tuned far-field launches."""
+    """{configuration key: {"waves", "threads", "ms"}} of the tuned far-field launches."""
     n = ctypes.c_size_t(0)
     check(lib().ves3d_autotune_report(None, 0, ctypes.byref(n)), "autotune_report")
     buf = ctypes.create_string_buffer(n.value + 1)

@@ -70,6 +70,25 @@ __device__ __forceinline__ float rsqrt_ftz(float x) {
 // error (~2^-23) becomes O(2^-66), i.e. the result is within rounding of 1/sqrt(r2).
 // Valid for FLT_MIN < r2 < FLT_MAX. (The flush-to-zero seed gives the same bits here and
 // measured no faster in the FP64 far field, which is bound by its FP64 pipe.)
+// The same refinement from a seed formed without FP64 conversions: the FP32 operand is
+// cut from the double's bits (exponent rebased, significand truncated to 23 bits) and the
+// hardware result put back into a double by integer operations, so the FP64 pipe only
+// sees the refinement (two conversions fewer per call; the seed's relative error stays
+// ~2^-22, within the refinement's reach). Valid for FLT_MIN <= r2 < FLT_MAX; a caller
+// treats smaller r2 (below 2^-126) as a coincident pair.
+__device__ __forceinline__ double rsqrt_f64_int_seed(double r2) {
+  constexpr int kRebias = (1023 - 127) << 20;  // exponent bias difference, in the high word
+  const unsigned fb = __funnelshift_l((unsigned)__double2loint(r2), (unsigned)(__double2hiint(r2) - kRebias), 3);
+  const unsigned yb = __float_as_uint(rsqrt_ftz(__uint_as_float(fb)));
+  const double y = __hiloint2double((int)((yb >> 3) + kRebias), (int)(yb << 29));
+  const double e = fma(-r2 * y, y, 1.0);
+  const double c = fma(e, 0.375, 0.5);
+  return fma(y * e, c, y);
+}
+
+// Coincidence test on the high word of a squared distance: true for r2 >= 2^-126.
+__device__ __forceinline__ bool r2_normal(double r2) { return __double2hiint(r2) >= 0x38100000; }
+
 __device__ __forceinline__ double rsqrt_f64(double r2) {
   double y = (double)rsqrtf((float)r2);
   double e = fma(-r2 * y, y, 1.0);

@@ -146,7 +146,7 @@ struct FarGroup {
 };
 // far-field launch-shape autotuner (far_kernels.cu)
 int set_autotune(int on);
-int set_far_shape(int waves, int chunk_max, int tpt);
+int set_far_shape(int waves, int nthr, int tpt);
 std::string autotune_report();
 int launch_far_groups(bool mixed, const double* pos, const double* den, const long* off, long nves, long N,
                       const FarGroup* groups, int ngroups, const double* add, double* out, double* far_out,

@@ -1141,8 +1141,8 @@ int ves3d_sv_eval_resident(ves3d_sv* sv) {
 
 int ves3d_set_autotune(int on) { return set_autotune(on); }
 
-int ves3d_set_far_shape(int waves, int chunk_max, int targets_per_thread) {
-  return set_far_shape(waves, chunk_max, targets_per_thread);
+int ves3d_set_far_shape(int waves, int threads, int targets_per_thread) {
+  return set_far_shape(waves, threads, targets_per_thread);
 }
 
 int ves3d_autotune_report(char* buf, size_t cap, size_t* len) {
@@ -3192,16 +3192,18 @@ static int svp_alloc_dl(ves3d_svp* g) {
 int ves3d_svp_set_density_dl(ves3d_svp* g, const double* gdl, int is_device) {
   VES3D_ARG(g != nullptr, "null context");
   VES3D_ARG(!g->grp.empty(), "set_src_coord first");
+  int s;
   if (!gdl) {  // SetDensityDL(NULL): the double layer off
+    for (ves3d_sv* sv : g->grp)
+      if ((s = ves3d_sv_set_density_dl(sv, nullptr, 0))) return s;
     if (g->have_dl) g->drop_graph();
     g->have_dl = false;
     return VES3D_OK;
   }
-  int s;
   if ((s = svp_alloc_dl(g))) return s;
+  // each group's own SetDensityDL: its G buffer, and the stage buffers its DL build needs
   for (size_t r = 0; r < g->grp.size(); r++)
-    if ((s = copy_in(g->grp[r]->G, gdl + 3 * g->gpt0[r], 3 * (size_t)g->grp[r]->npts(), is_device, g->stream)))
-      return s;
+    if ((s = ves3d_sv_set_density_dl(g->grp[r], gdl + 3 * g->gpt0[r], is_device))) return s;
   if (!g->have_dl) g->drop_graph();  // a captured evaluation without the double layer
   g->have_dl = true;
   return VES3D_OK;
