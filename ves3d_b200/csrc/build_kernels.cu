@@ -544,7 +544,9 @@ struct RingTcCfg {
   static constexpr int SZ_B12 = 128 * F0 * 2;     // [Mf | dMf]^T: N = 2 N1 = 128 rows x K = F0
   static constexpr int SZ_BT = F0 * N1 * 2;       // Mf: N = F0 rows x K = N1
   static constexpr int SZ_K = KROWS * JC * 2;     // one chunk of kernel values
-  static constexpr int SXS_LD = JC + 1;           // FP32 surface values [9][32 lat][SXS_LD]
+  // FP32 surface values [9][32 lat][SXS_LD]: rows of 80 bytes take the TMEM rows as
+  // conflict-free float4 stores, and 8 latitudes x 4 longitudes of a warp read distinct banks
+  static constexpr int SXS_LD = 20;
   static constexpr int SZ_XS = 9 * 32 * SXS_LD * 4;
   static constexpr int SZ_C = L1 * LDCL * 4;      // FP32 transposed-DFT result [lat][jf][comp]
   // byte offsets; the union region U holds A/dA (pass 1 -> GEMM 1), then the chunk buffer
@@ -562,15 +564,16 @@ struct RingTcCfg {
   static constexpr int OFF_T0 = al16(OFF_R + 2 * 3 * LDR * 8);        // FP64 m = 0 tables: leg, dleg [L1][LD0]
   static constexpr int OFF_TF = al16(OFF_T0 + 2 * L1 * LD0 * 8);      // FP32 tables: leg, dleg [L1][LDF]
   static constexpr int OFF_X32 = al16(OFF_TF + 2 * L1 * LDF * 4);     // last latitude: [9][N1] FP32
-  static constexpr int OFF_K32 = al16(OFF_X32 + 9 * N1 * 4);          // its kernel values [12][N1] FP64
-  static constexpr int OFF_R4 = al16(OFF_K32 + 12 * N1 * 8);          // R as float4 (x, y, z, 0) [NC]
-  static constexpr int OFF_TRG = al16(OFF_R4 + NC * 16);
+  static constexpr int OFF_K32 = al16(OFF_X32 + 9 * N1 * 4);          // its kernel values [12][N1] FP32
+  static constexpr int OFF_R4 = al16(OFF_K32 + 12 * N1 * 4);          // R as float4 (x, y, z, 0) [NC]
+  static constexpr int OFF_MFT = al16(OFF_R4 + NC * 16);              // Mf^T [N1][F0] FP32 (the last latitude's DFT)
+  static constexpr int OFF_TRG = al16(OFF_MFT + N1 * F0 * 4);
   static constexpr int OFF_CEN = OFF_TRG + 6 * 8;
   static constexpr int OFF_SW = OFF_CEN + 6 * 8;
   static constexpr int OFF_BO = OFF_SW + L1 * 8;
   static constexpr int OFF_JF = OFF_BO + ((F0 + 1) * 4 + 7) / 8 * 8;   // Fourier block of each coefficient
   static constexpr int OFF_BAR = OFF_JF + (NC + 7) / 8 * 8;
-  static_assert(OFF_U % 16 == 0 && OFF_R % 16 == 0 && OFF_T0 % 16 == 0 && OFF_TF % 16 == 0 && OFF_X32 % 16 == 0 &&
+  static_assert(OFF_U % 16 == 0 && OFF_XS % 16 == 0 && OFF_R % 16 == 0 && OFF_T0 % 16 == 0 && OFF_TF % 16 == 0 && OFF_X32 % 16 == 0 &&
                     OFF_K32 % 16 == 0 && OFF_R4 % 16 == 0 && OFF_BAR % 8 == 0 && (LDCL * 4) % 16 == 0,
                 "alignment of the shared-memory regions");
   static constexpr int NBAR = 4;  // GEMM 1, GEMM 2, R buffers 0 and 1
@@ -626,8 +629,9 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
   double* sT0 = reinterpret_cast<double*>(smem + H::OFF_T0);  // leg, then dleg: [L1][LD0]
   float* sTF = reinterpret_cast<float*>(smem + H::OFF_TF);    // leg, then dleg: [L1][LDF]
   float* sX32 = reinterpret_cast<float*>(smem + H::OFF_X32);
-  double* sK32 = reinterpret_cast<double*>(smem + H::OFF_K32);
+  float* sK32 = reinterpret_cast<float*>(smem + H::OFF_K32);
   float4* sR4 = reinterpret_cast<float4*>(smem + H::OFF_R4);
+  float* sMfT = reinterpret_cast<float*>(smem + H::OFF_MFT);
   double* trg = reinterpret_cast<double*>(smem + H::OFF_TRG);
   double* cen = reinterpret_cast<double*>(smem + H::OFF_CEN);
   double* sSw = reinterpret_cast<double*>(smem + H::OFF_SW);
@@ -665,7 +669,9 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
   }
   for (int i = tid; i < F0 * N1; i += NTHR) {
     const int n = i / N1, k = i - n * N1;  // BT[jf][j] = Mf[jf][j]
-    tc::store_split3(sBT, H::SZ_BT, tc::umma_off(n, k, N1), (float)__ldg(T.syn1_four + i));
+    const float v = (float)__ldg(T.syn1_four + i);
+    tc::store_split3(sBT, H::SZ_BT, tc::umma_off(n, k, N1), v);
+    sMfT[k * F0 + n] = v;  // the same FP32 values (the split covers them exactly), transposed
   }
   // Legendre tables resident for the CTA's life: the m = 0 block in FP64 (it carries the
   // vesicle's position), the other blocks in FP32 (their values multiply shape-sized
@@ -811,9 +817,10 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
         const int col = (var == 0 ? H::COL_X : var == 1 ? H::COL_XT : H::COL_XP) + ch * H::JC;
         tc::tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + col, v);
         if (q < 3) {
-          float* o = sXs + ((var * 3 + q) * 32 + lane) * H::SXS_LD;
+          float4* o = reinterpret_cast<float4*>(sXs + ((var * 3 + q) * 32 + lane) * H::SXS_LD);
 #pragma unroll
-          for (int jj = 0; jj < H::JC; jj++) o[jj] = v[jj];
+          for (int jj = 0; jj < H::JC / 4; jj++)
+            o[jj] = make_float4(v[4 * jj], v[4 * jj + 1], v[4 * jj + 2], v[4 * jj + 3]);
         } else if (lane < 3) {
           float* o = sX32 + (var * 3 + lane) * N1 + ch * H::JC;
 #pragma unroll
@@ -824,9 +831,10 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
       if (ch > 0) wait(bar_k, n_k);  // GEMM 2 of the previous chunk has read the chunk buffer
       if (!(ok = sync_ok())) break;
       // (b) singular kernel (FP64) at the chunk's 32 x 16 points (one per thread) -> split
-      // BF16 chunk operand
+      // BF16 chunk operand; a warp takes 8 latitudes x 4 longitudes (its split stores then
+      // fall on 16 banks twice, against four times for 2 latitudes x 16 longitudes)
       {
-        const int lat = tid >> 4, jj = tid & 15;
+        const int lat = (warp >> 2) * 8 + (lane >> 2), jj = (warp & 3) * 4 + (lane & 3);
         const int h = 2 * lat > H::P1 ? 1 : 0;
         const float* xs = sXs + lat * H::SXS_LD + jj;
         constexpr int VS = 32 * H::SXS_LD;
@@ -881,7 +889,7 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
       double kv[6];
       ring_kernel_sl(xs[0], xs[N1], xs[2 * N1], area, trg, cen, 1, t, sSw[t ? 32 : H::P1 - 32], kv);
 #pragma unroll
-      for (int c = 0; c < 6; c++) sK32[(t * 6 + c) * N1 + j] = kv[c];
+      for (int c = 0; c < 6; c++) sK32[(t * 6 + c) * N1 + j] = (float)kv[c];
     }
     wait(bar_k, n_k);  // the last chunk's GEMM 2 before TMEM is read and the region reused
     if (!(ok = sync_ok())) break;
@@ -900,19 +908,23 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
     }
     tc::tc_before_sync();
     __syncthreads();
-    // the last latitude's transposed DFT in FP64 (its row of C)
+    // the last latitude's transposed DFT (its row of C), FP32 like the BF16-split GEMM of
+    // the other rows (the same FP32 values of Mf): a warp takes one component, its lanes the
+    // 32 Fourier columns (broadcast kernel values, conflict-free Mf^T rows). It read Mf from
+    // global memory in FP64 before, 32 cache lines per load: 42% of a rotation's time.
     if (tid < 12 * F0) {
       const int comp = tid / F0, jf = tid - comp * F0;
-      const double* kr = sK32 + comp * N1;
-      const double* mf = T.syn1_four + jf * N1;
-      double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+      const float* kr = sK32 + comp * N1;
+      const float* mf = sMfT + jf;
+      float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+#pragma unroll 4
       for (int j = 0; j < N1; j += 4) {
-        s0 = fma(kr[j], __ldg(mf + j), s0);
-        s1 = fma(kr[j + 1], __ldg(mf + j + 1), s1);
-        s2 = fma(kr[j + 2], __ldg(mf + j + 2), s2);
-        s3 = fma(kr[j + 3], __ldg(mf + j + 3), s3);
+        s0 = fmaf(kr[j], mf[j * F0], s0);
+        s1 = fmaf(kr[j + 1], mf[(j + 1) * F0], s1);
+        s2 = fmaf(kr[j + 2], mf[(j + 2) * F0], s2);
+        s3 = fmaf(kr[j + 3], mf[(j + 3) * F0], s3);
       }
-      sC[32 * LDCL + jf * 12 + comp] = (float)((s0 + s1) + (s2 + s3));
+      sC[32 * LDCL + jf * 12 + comp] = (s0 + s1) + (s2 + s3);
     }
     __syncthreads();
     // ---- pass 2: transposed Legendre sums (FP32 FMA over the 33 latitudes), one output
