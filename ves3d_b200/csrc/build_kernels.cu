@@ -245,12 +245,12 @@ __global__ void __launch_bounds__(256, (P0 <= 16 ? 2 : 1)) k_build_ring(const do
       const double bx = xp[0], by = xp[G::LDX], bz = xp[2 * G::LDX];
       const double nx = ay * bz - az * by, ny = az * bx - ax * bz, nz = ax * by - ay * bx;
       const double n2 = nx * nx + ny * ny + nz * nz;
-      const double area = n2 * rsqrt_f64(n2);  // |X_theta x X_phi| > 0 on the upsampled grid
+      const double area = n2 * rsqrt_f64_int_seed(n2);  // |X_theta x X_phi| > 0 on the upsampled grid
 #pragma unroll
       for (int t = 0; t < 2; t++) {
         const double dx = trg[t] - px, dy = trg[2 + t] - py, dz = trg[4 + t] - pz;
         const double r2 = dx * dx + dy * dy + dz * dz;
-        double rinv = rsqrt_f64(r2);
+        double rinv = rsqrt_f64_int_seed(r2);  // (r2 below 2^-126 is cut off here too)
         if (r2 <= 2.220446049250313e-16) rinv = 0.0;
         const double a1 = kInv8Pi * sSw[t ? lat : G::P1 - lat] * area * rinv;
         const double a2 = a1 * rinv * rinv;
@@ -518,9 +518,14 @@ __device__ __forceinline__ void store_split3x2(unsigned char* base, uint32_t str
   *reinterpret_cast<__nv_bfloat162*>(base + 2 * stride + off) = h2;
 }
 
-// Split products (i, j), i + j <= 2, smallest first.
-__constant__ int kSplitI[6] = {2, 1, 0, 1, 0, 0};
-__constant__ int kSplitJ[6] = {0, 1, 2, 0, 1, 0};
+// Split products (i, j), i + j <= 2, smallest first (compile-time in the unrolled issue loops).
+__host__ __device__ constexpr int split_i(int pr) { return pr == 0 ? 2 : (pr == 1 || pr == 3) ? 1 : 0; }
+__host__ __device__ constexpr int split_j(int pr) { return pr == 2 ? 2 : (pr == 1 || pr == 4) ? 1 : 0; }
+
+// Descriptor of an operand at a byte offset from the one described by d: the start address
+// field holds address >> 4 in 14 bits, so a 16-byte multiple is added there directly (no
+// carry out of the field below 256 KB of shared memory).
+__device__ __forceinline__ uint64_t desc_at(uint64_t d, uint32_t byte_off) { return d + (byte_off >> 4); }
 
 }  // namespace tc
 
@@ -549,25 +554,30 @@ struct RingTcCfg {
   static constexpr int SXS_LD = 20;
   static constexpr int SZ_XS = 9 * 32 * SXS_LD * 4;
   static constexpr int SZ_C = L1 * LDCL * 4;      // FP32 transposed-DFT result [lat][jf][comp]
-  // byte offsets; the union region U holds A/dA (pass 1 -> GEMM 1), then the chunk buffer
-  // and the chunk's surface values (-> GEMM 2), then C (-> pass 2)
+  // byte offsets; the union region U holds A/dA (pass 1 -> GEMM 1), then two chunk buffers
+  // (chunk ch in buffer ch % 2: GEMM 2 of one chunk runs while the next is formed) and the
+  // chunk's surface values (-> GEMM 2), then C (-> pass 2)
   static constexpr int OFF_B12 = 0;
   static constexpr int OFF_BT = OFF_B12 + 3 * SZ_B12;
   static constexpr int OFF_U = OFF_BT + 3 * SZ_BT;
   static constexpr int OFF_A = OFF_U;
   static constexpr int OFF_K = OFF_U;
-  static constexpr int OFF_XS = OFF_K + 3 * SZ_K;
-  static constexpr int U_SZ = std::max(std::max(6 * SZ_A, 3 * SZ_K + SZ_XS), SZ_C);
+  static constexpr int OFF_XS = OFF_K + 6 * SZ_K;
+  static constexpr int U_SZ = std::max(std::max(6 * SZ_A, 6 * SZ_K + SZ_XS), SZ_C);
   // every region starts on a 16-byte boundary (float4 and bulk-copy destinations need it)
   static constexpr int al16(int x) { return (x + 15) / 16 * 16; }
   static constexpr int OFF_R = (OFF_U + U_SZ + 127) / 128 * 128;      // 2 x [3][LDR] FP64
-  static constexpr int OFF_T0 = al16(OFF_R + 2 * 3 * LDR * 8);        // FP64 m = 0 tables: leg, dleg [L1][LD0]
-  static constexpr int OFF_TF = al16(OFF_T0 + 2 * L1 * LD0 * 8);      // FP32 tables: leg, dleg [L1][LDF]
-  static constexpr int OFF_X32 = al16(OFF_TF + 2 * L1 * LDF * 4);     // last latitude: [9][N1] FP32
+  // Legendre tables of latitudes 0..LH - 1 only: the Gauss nodes are symmetric and
+  // P_n^m(-x) = (-1)^(n+m) P_n^m(x), so latitude 32 - l follows from latitude l
+  static constexpr int LH = P1 / 2 + 1;
+  static constexpr int OFF_T0 = al16(OFF_R + 2 * 3 * LDR * 8);        // FP64 m = 0 tables: leg, dleg [LH][LD0]
+  static constexpr int OFF_TF = al16(OFF_T0 + 2 * LH * LD0 * 8);      // FP32 tables: leg, dleg [LH][LDF]
+  static constexpr int OFF_X32 = al16(OFF_TF + 2 * LH * LDF * 4);     // last latitude: [9][N1] FP32
   static constexpr int OFF_K32 = al16(OFF_X32 + 9 * N1 * 4);          // its kernel values [12][N1] FP32
   static constexpr int OFF_R4 = al16(OFF_K32 + 12 * N1 * 4);          // R as float4 (x, y, z, 0) [NC]
   static constexpr int OFF_MFT = al16(OFF_R4 + NC * 16);              // Mf^T [N1][F0] FP32 (the last latitude's DFT)
-  static constexpr int OFF_TRG = al16(OFF_MFT + N1 * F0 * 4);
+  static constexpr int OFF_C32 = al16(OFF_MFT + N1 * F0 * 4);         // row 32 of C [F0][12], outside U
+  static constexpr int OFF_TRG = al16(OFF_C32 + F0 * 12 * 4);
   static constexpr int OFF_CEN = OFF_TRG + 6 * 8;
   static constexpr int OFF_SW = OFF_CEN + 6 * 8;
   static constexpr int OFF_BO = OFF_SW + L1 * 8;
@@ -576,7 +586,7 @@ struct RingTcCfg {
   static_assert(OFF_U % 16 == 0 && OFF_XS % 16 == 0 && OFF_R % 16 == 0 && OFF_T0 % 16 == 0 && OFF_TF % 16 == 0 && OFF_X32 % 16 == 0 &&
                     OFF_K32 % 16 == 0 && OFF_R4 % 16 == 0 && OFF_BAR % 8 == 0 && (LDCL * 4) % 16 == 0,
                 "alignment of the shared-memory regions");
-  static constexpr int NBAR = 4;  // GEMM 1, GEMM 2, R buffers 0 and 1
+  static constexpr int NBAR = 5;  // GEMM 1, GEMM 2 of chunk buffers 0 and 1, R buffers 0 and 1
   static constexpr int OFF_TMEM = OFF_BAR + NBAR * 8;
   static constexpr int SMEM = OFF_TMEM + 16;
   static constexpr uint32_t TMEM_COLS = 512;
@@ -594,7 +604,7 @@ __device__ __forceinline__ void ring_kernel_sl(double px, double py, double pz, 
   const double dx = (trg[t] - cen[h * 3]) - px, dy = (trg[2 + t] - cen[h * 3 + 1]) - py,
                dz = (trg[4 + t] - cen[h * 3 + 2]) - pz;
   const double r2 = dx * dx + dy * dy + dz * dz;
-  double rinv = rsqrt_f64(r2);
+  double rinv = rsqrt_f64_int_seed(r2);  // (r2 below 2^-126 is cut off here too)
   if (r2 <= 2.220446049250313e-16) rinv = 0.0;
   const double a1 = kInv8Pi * w * area * rinv;
   const double a2 = a1 * rinv * rinv;
@@ -609,7 +619,7 @@ __device__ __forceinline__ void ring_kernel_sl(double px, double py, double pz, 
 __device__ __forceinline__ double area_of(double ax, double ay, double az, double bx, double by, double bz) {
   const double nx = ay * bz - az * by, ny = az * bx - ax * bz, nz = ax * by - ay * bx;
   const double n2 = nx * nx + ny * ny + nz * nz;
-  return n2 * rsqrt_f64(n2);  // |X_theta x X_phi| > 0 on the upsampled grid
+  return n2 * rsqrt_f64_int_seed(n2);  // |X_theta x X_phi| > 0 on the upsampled grid
 }
 
 template <int P0>
@@ -626,12 +636,13 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
   float* sXs = reinterpret_cast<float*>(smem + H::OFF_XS);
   float* sC = reinterpret_cast<float*>(smem + H::OFF_U);
   double* sRb = reinterpret_cast<double*>(smem + H::OFF_R);
-  double* sT0 = reinterpret_cast<double*>(smem + H::OFF_T0);  // leg, then dleg: [L1][LD0]
-  float* sTF = reinterpret_cast<float*>(smem + H::OFF_TF);    // leg, then dleg: [L1][LDF]
+  double* sT0 = reinterpret_cast<double*>(smem + H::OFF_T0);  // leg, then dleg: [LH][LD0]
+  float* sTF = reinterpret_cast<float*>(smem + H::OFF_TF);    // leg, then dleg: [LH][LDF]
   float* sX32 = reinterpret_cast<float*>(smem + H::OFF_X32);
   float* sK32 = reinterpret_cast<float*>(smem + H::OFF_K32);
   float4* sR4 = reinterpret_cast<float4*>(smem + H::OFF_R4);
   float* sMfT = reinterpret_cast<float*>(smem + H::OFF_MFT);
+  float* sC32 = reinterpret_cast<float*>(smem + H::OFF_C32);
   double* trg = reinterpret_cast<double*>(smem + H::OFF_TRG);
   double* cen = reinterpret_cast<double*>(smem + H::OFF_CEN);
   double* sSw = reinterpret_cast<double*>(smem + H::OFF_SW);
@@ -639,15 +650,15 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
   unsigned char* sJf = smem + H::OFF_JF;
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + H::OFF_BAR);
   uint64_t* bar_mma1 = bars;     // GEMM 1 done
-  uint64_t* bar_k = bars + 1;    // GEMM 2 of the last chunk done (the chunk buffer is free)
-  uint64_t* bar_r = bars + 2;    // [2] R buffers loaded
+  uint64_t* bar_k = bars + 1;    // [2] GEMM 2 of the chunk in buffer 0 / 1 done (the buffer is free)
+  uint64_t* bar_r = bars + 3;    // [2] R buffers loaded
   uint32_t* s_tmem = reinterpret_cast<uint32_t*>(smem + H::OFF_TMEM);
   int* s_abort = reinterpret_cast<int*>(smem + H::OFF_TMEM + 4);
 
   constexpr int NTHR = H::NTHR;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int NC = H::NC, LDR = H::LDR, F0 = H::F0, N1 = H::N1, L1 = H::L1, M0 = H::M0;
-  constexpr int LD0 = H::LD0, LDF = H::LDF, LDCL = H::LDCL;
+  constexpr int LD0 = H::LD0, LDF = H::LDF, LDCL = H::LDCL, LH = H::LH;
 
   // ---- set-up: TMEM, barriers, constant operands and tables ---------------------------
   if (warp == 0) {
@@ -676,12 +687,12 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
   // Legendre tables resident for the CTA's life: the m = 0 block in FP64 (it carries the
   // vesicle's position), the other blocks in FP32 (their values multiply shape-sized
   // coefficients; no change in the self velocity's error measured)
-  for (int i = tid; i < 2 * L1 * LD0; i += NTHR) {
-    const int tb = i / (L1 * LD0), r = i - tb * L1 * LD0, lat = r / LD0, c = r - lat * LD0;
+  for (int i = tid; i < 2 * LH * LD0; i += NTHR) {
+    const int tb = i / (LH * LD0), r = i - tb * LH * LD0, lat = r / LD0, c = r - lat * LD0;
     sT0[i] = __ldg((tb ? T.syn1_dleg_t : T.syn1_leg_t) + (long)lat * NC + c);
   }
-  for (int i = tid; i < 2 * L1 * LDF; i += NTHR) {
-    const int tb = i / (L1 * LDF), r = i - tb * L1 * LDF, lat = r / LDF, c = r - lat * LDF;
+  for (int i = tid; i < 2 * LH * LDF; i += NTHR) {
+    const int tb = i / (LH * LDF), r = i - tb * LH * LDF, lat = r / LDF, c = r - lat * LDF;
     sTF[i] = c < NC ? (float)__ldg((tb ? T.syn1_dleg_t : T.syn1_leg_t) + (long)lat * NC + c) : 0.f;
   }
   for (int i = tid; i < L1; i += NTHR) sSw[i] = __ldg(T.sing_w + i);
@@ -693,6 +704,12 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
   tc::tc_after_sync();
   const uint32_t tmem = *s_tmem;
   const double mf00 = __ldg(T.syn1_four);  // the constant m = 0 Fourier row
+  // operand descriptors of split 0 (K-major, no swizzle; LBO 128 B, SBO one 8-row group)
+  const uint64_t dA = tc::umma_desc(tc::saddr(sA), 128, F0 * 16), ddA = tc::umma_desc(tc::saddr(sdA), 128, F0 * 16);
+  const uint64_t dB12 = tc::umma_desc(tc::saddr(sB12), 128, F0 * 16);
+  const uint64_t dBT = tc::umma_desc(tc::saddr(sBT), 128, N1 * 16);
+  const uint64_t dK0 = tc::umma_desc(tc::saddr(sK), 128, H::JC * 16);
+  const uint64_t dK1 = tc::umma_desc(tc::saddr(sK + 3 * H::SZ_K), 128, H::JC * 16);
 
   auto issue_r = [&](long rot, int b) {
     double* dst = sRb + b * 3 * LDR;
@@ -701,8 +718,8 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
   };
   // phases waited for per barrier and issued (uniform over the CTA: every issue decision
   // depends only on loop indices)
-  uint32_t n_r[2] = {0, 0}, n_k = 0, n_mma1 = 0;
-  uint32_t i_r[2] = {0, 0}, i_k = 0, i_mma1 = 0;
+  uint32_t n_r[2] = {0, 0}, n_k[2] = {0, 0}, n_mma1 = 0;
+  uint32_t i_r[2] = {0, 0}, i_k[2] = {0, 0}, i_mma1 = 0;
   bool ok = true;
   auto wait = [&](uint64_t* bar, uint32_t& cnt) {
     if (!tc::mbar_wait(bar, cnt & 1)) {
@@ -743,46 +760,94 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
     // the m = 0 block in FP64 (it carries the vesicle's position, shifted by the pole target
     // here), the others in FP32 (shape-sized terms; their sums are rounded to FP32 for the
     // split anyway)
-    // item (Fourier block k, latitude): a warp takes 32 latitudes of one block (the same
-    // trip count; conflict-free table columns), the last latitude of every block follows
-    for (int itm = tid; itm < F0 * L1; itm += NTHR) {
-      const int k = itm < F0 * 32 ? itm >> 5 : itm - F0 * 32;
-      const int lat = itm < F0 * 32 ? itm & 31 : 32;
-      double e0 = 0.0, e1 = 0.0, e2 = 0.0, f0 = 0.0, f1 = 0.0, f2 = 0.0;
-      if (k == 0) {
-        const double* L = sT0 + lat * LD0;
-        const double* dL = sT0 + (L1 + lat) * LD0;
-        for (int c = 0; c < M0; c++) {
-          const double l = L[c], dl = dL[c], r0 = sR[c], r1 = sR[LDR + c], r2 = sR[2 * LDR + c];
-          e0 = fma(l, r0, e0); e1 = fma(l, r1, e1); e2 = fma(l, r2, e2);
-          f0 = fma(dl, r0, f0); f1 = fma(dl, r1, f1); f2 = fma(dl, r2, f2);
+    // item (pair of Fourier blocks k0, k0 + 1; latitude pair l): sums over each block split by
+    // the parity of n + m give latitude l (even + odd) and its mirror 32 - l (even - odd; the
+    // theta derivative odd - even) from one pass over the coefficients (P_n^m(-x) =
+    // (-1)^(n+m) P_n^m(x) on the symmetric Gauss nodes); l = 16 is the equator. A warp holds
+    // 8 latitude pairs x 4 block pairs, so each of its bf16x2 stores fills whole core
+    // matrices of the K-major operands (conflict-free); warps 0-7 take l < 16, warp 8 the
+    // equator.
+    static_assert(H::P1 == 32 && LH == 17 && F0 == 32 && NTHR >= 9 * 32, "latitude and block pairs");
+    if (warp < 9) {
+      const int l = warp < 8 ? 8 * (warp & 1) + (lane >> 2) : 16;
+      const int kp = warp < 8 ? 4 * (warp >> 1) + (lane & 3) : lane;
+      if (warp < 8 || lane < 16) {
+        const int lb = H::P1 - l;
+        float ev[2][3], od[2][3], dev[2][3], dod[2][3];  // [block][coordinate]
+#pragma unroll
+        for (int b = 0; b < 2; b++) {
+          const int k = 2 * kp + b;
+          if (k == 0) {  // block m = 0 (n = c) in FP64, centred on the pole targets below
+            const double* L = sT0 + l * LD0;
+            const double* dL = sT0 + (LH + l) * LD0;
+            double e0 = 0, e1 = 0, e2 = 0, f0 = 0, f1 = 0, f2 = 0;  // n even
+            double o0 = 0, o1 = 0, o2 = 0, g0 = 0, g1 = 0, g2 = 0;  // n odd
+            for (int c = 0; c < M0; c += 2) {
+              const double lv = L[c], dl = dL[c], r0 = sR[c], r1 = sR[LDR + c], r2 = sR[2 * LDR + c];
+              e0 = fma(lv, r0, e0); e1 = fma(lv, r1, e1); e2 = fma(lv, r2, e2);
+              f0 = fma(dl, r0, f0); f1 = fma(dl, r1, f1); f2 = fma(dl, r2, f2);
+              if (c + 1 < M0) {
+                const double lw = L[c + 1], dw = dL[c + 1], q0 = sR[c + 1], q1 = sR[LDR + c + 1],
+                             q2 = sR[2 * LDR + c + 1];
+                o0 = fma(lw, q0, o0); o1 = fma(lw, q1, o1); o2 = fma(lw, q2, o2);
+                g0 = fma(dw, q0, g0); g1 = fma(dw, q1, g1); g2 = fma(dw, q2, g2);
+              }
+            }
+            // the centring by the pole targets is applied to each side in FP64
+            const int hl = 0, hb = 1;
+            const double c0 = cen[hl * 3] / mf00, c1 = cen[hl * 3 + 1] / mf00, c2 = cen[hl * 3 + 2] / mf00;
+            const double d0 = cen[hb * 3] / mf00, d1 = cen[hb * 3 + 1] / mf00, d2 = cen[hb * 3 + 2] / mf00;
+            // side values formed here: ev = value at l, od = value at lb (mirror)
+            ev[b][0] = (float)(e0 + o0 - c0); ev[b][1] = (float)(e1 + o1 - c1); ev[b][2] = (float)(e2 + o2 - c2);
+            od[b][0] = (float)(e0 - o0 - d0); od[b][1] = (float)(e1 - o1 - d1); od[b][2] = (float)(e2 - o2 - d2);
+            dev[b][0] = (float)(f0 + g0); dev[b][1] = (float)(f1 + g1); dev[b][2] = (float)(f2 + g2);
+            dod[b][0] = (float)(g0 - f0); dod[b][1] = (float)(g1 - f1); dod[b][2] = (float)(g2 - f2);
+          } else {
+            const float* L = sTF + l * LDF;
+            const float* dL = sTF + (LH + l) * LDF;
+            const int c0 = sBo[k], c1 = sBo[k + 1];
+            float ge[6] = {}, go[6] = {};
+            int c = c0;
+            for (; c + 1 < c1; c += 2) {  // n - m = c - c0: even, then odd
+              const float l0 = L[c], d0 = dL[c], l1 = L[c + 1], d1 = dL[c + 1];
+              const float4 r = sR4[c], q = sR4[c + 1];
+              ge[0] = fmaf(l0, r.x, ge[0]); ge[1] = fmaf(l0, r.y, ge[1]); ge[2] = fmaf(l0, r.z, ge[2]);
+              ge[3] = fmaf(d0, r.x, ge[3]); ge[4] = fmaf(d0, r.y, ge[4]); ge[5] = fmaf(d0, r.z, ge[5]);
+              go[0] = fmaf(l1, q.x, go[0]); go[1] = fmaf(l1, q.y, go[1]); go[2] = fmaf(l1, q.z, go[2]);
+              go[3] = fmaf(d1, q.x, go[3]); go[4] = fmaf(d1, q.y, go[4]); go[5] = fmaf(d1, q.z, go[5]);
+            }
+            if (c < c1) {
+              const float l0 = L[c], d0 = dL[c];
+              const float4 r = sR4[c];
+              ge[0] = fmaf(l0, r.x, ge[0]); ge[1] = fmaf(l0, r.y, ge[1]); ge[2] = fmaf(l0, r.z, ge[2]);
+              ge[3] = fmaf(d0, r.x, ge[3]); ge[4] = fmaf(d0, r.y, ge[4]); ge[5] = fmaf(d0, r.z, ge[5]);
+            }
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+              ev[b][d] = ge[d] + go[d];
+              od[b][d] = ge[d] - go[d];
+              dev[b][d] = ge[3 + d] + go[3 + d];
+              dod[b][d] = go[3 + d] - ge[3 + d];
+            }
+          }
         }
-        // centred on the hemisphere's pole target: X - c enters through the m = 0 column
-        const int h = 2 * lat > H::P1 ? 1 : 0;
-        e0 -= cen[h * 3] / mf00;
-        e1 -= cen[h * 3 + 1] / mf00;
-        e2 -= cen[h * 3 + 2] / mf00;
-      } else {
-        const float* L = sTF + lat * LDF;
-        const float* dL = sTF + (L1 + lat) * LDF;
-        const int c1 = sBo[k + 1];
-        float g0 = 0.f, g1 = 0.f, g2 = 0.f, q0 = 0.f, q1 = 0.f, q2 = 0.f;
-        for (int c = sBo[k]; c < c1; c++) {
-          const float l = L[c], dl = dL[c];
-          const float4 r = sR4[c];
-          g0 = fmaf(l, r.x, g0); g1 = fmaf(l, r.y, g1); g2 = fmaf(l, r.z, g2);
-          q0 = fmaf(dl, r.x, q0); q1 = fmaf(dl, r.y, q1); q2 = fmaf(dl, r.z, q2);
+        // latitude l (hemisphere 0; rows l + 32 d), then its mirror (hemisphere 1: rows
+        // 32 - l + 32 d, or 96 + d for latitude 32) unless l is the equator
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          const uint32_t o = tc::umma_off(l + 32 * d, 2 * kp, F0);
+          tc::store_split3x2(sA, H::SZ_A, o, ev[0][d], ev[1][d]);
+          tc::store_split3x2(sdA, H::SZ_A, o, dev[0][d], dev[1][d]);
         }
-        e0 = g0; e1 = g1; e2 = g2; f0 = q0; f1 = q1; f2 = q2;
+        if (l < 16) {
+#pragma unroll
+          for (int d = 0; d < 3; d++) {
+            const uint32_t o = tc::umma_off(lb < 32 ? lb + 32 * d : 96 + d, 2 * kp, F0);
+            tc::store_split3x2(sA, H::SZ_A, o, od[0][d], od[1][d]);
+            tc::store_split3x2(sdA, H::SZ_A, o, dod[0][d], dod[1][d]);
+          }
+        }
       }
-      const int rb0 = lat < 32 ? lat : 96;  // row of d = 0; d adds 32 (lat < 32) or 1 (lat 32)
-      const int rs = lat < 32 ? 32 : 1;
-      tc::store_split3(sA, H::SZ_A, tc::umma_off(rb0, k, F0), (float)e0);
-      tc::store_split3(sA, H::SZ_A, tc::umma_off(rb0 + rs, k, F0), (float)e1);
-      tc::store_split3(sA, H::SZ_A, tc::umma_off(rb0 + 2 * rs, k, F0), (float)e2);
-      tc::store_split3(sdA, H::SZ_A, tc::umma_off(rb0, k, F0), (float)f0);
-      tc::store_split3(sdA, H::SZ_A, tc::umma_off(rb0 + rs, k, F0), (float)f1);
-      tc::store_split3(sdA, H::SZ_A, tc::umma_off(rb0 + 2 * rs, k, F0), (float)f2);
     }
     // ---- GEMM 1 on the tensor cores ------------------------------------------------------
     tc::fence_async_smem();
@@ -790,15 +855,15 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
     if (tid == 0) {
       tc::tc_after_sync();
       constexpr uint32_t id128 = tc::idesc_bf16(128, 2 * N1), id64 = tc::idesc_bf16(128, N1);
-      constexpr uint32_t SBO = F0 * 16;
+#pragma unroll
       for (int pr = 0; pr < 6; pr++) {
-        const int i = tc::kSplitI[pr], j = tc::kSplitJ[pr];
+#pragma unroll
         for (int s = 0; s < F0 / 16; s++) {
-          const uint64_t db = tc::umma_desc(tc::saddr(sB12 + j * H::SZ_B12) + s * 256, 128, SBO);
-          const uint64_t da = tc::umma_desc(tc::saddr(sA + i * H::SZ_A) + s * 256, 128, SBO);
-          tc::mma_bf16(tmem + H::COL_X, da, db, id128, (pr | s) ? 1u : 0u);
-          const uint64_t dd = tc::umma_desc(tc::saddr(sdA + i * H::SZ_A) + s * 256, 128, SBO);
-          tc::mma_bf16(tmem + H::COL_XP, dd, db, id64, (pr | s) ? 1u : 0u);
+          const uint64_t db = tc::desc_at(dB12, tc::split_j(pr) * H::SZ_B12 + s * 256);
+          tc::mma_bf16(tmem + H::COL_X, tc::desc_at(dA, tc::split_i(pr) * H::SZ_A + s * 256), db, id128,
+                       (pr | s) ? 1u : 0u);
+          tc::mma_bf16(tmem + H::COL_XP, tc::desc_at(ddA, tc::split_i(pr) * H::SZ_A + s * 256), db, id64,
+                       (pr | s) ? 1u : 0u);
         }
       }
       tc::mma_commit(bar_mma1);
@@ -828,7 +893,9 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
         }
       }
       tc::tc_before_sync();
-      if (ch > 0) wait(bar_k, n_k);  // GEMM 2 of the previous chunk has read the chunk buffer
+      const int kb = ch & 1;
+      unsigned char* sKb = sK + kb * 3 * H::SZ_K;
+      if (ch >= 2) wait(bar_k + kb, n_k[kb]);  // GEMM 2 of chunk ch - 2 has read this buffer
       if (!(ok = sync_ok())) break;
       // (b) singular kernel (FP64) at the chunk's 32 x 16 points (one per thread) -> split
       // BF16 chunk operand; a warp takes 8 latitudes x 4 longitudes (its split stores then
@@ -859,29 +926,33 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
           const float recv = __shfl_xor_sync(0xffffffffu, send, 1);
           const float lo = odd ? recv : kv[c], hi = odd ? kv[6 + c] : recv;
           const int comp = odd ? 6 + c : c;
-          tc::store_split3x2(sK, H::SZ_K, off + tc::umma_off(comp * 32 + lat, 0, H::JC), lo, hi);
+          tc::store_split3x2(sKb, H::SZ_K, off + tc::umma_off(comp * 32 + lat, 0, H::JC), lo, hi);
         }
       }
       tc::fence_async_smem();
       __syncthreads();
-      if (tid == 0) {
+      // GEMM 2 issued by warp 12, which has no surface values to move: warps 0-11 start the
+      // next chunk's TMEM reads meanwhile
+      if (tid == 12 * 32) {
         tc::tc_after_sync();
         constexpr uint32_t id32 = tc::idesc_bf16(128, F0);
+        const uint64_t dBc = tc::desc_at(dBT, ch * (H::JC / 8) * 128), dKc = kb ? dK1 : dK0;
+#pragma unroll
         for (int pr = 0; pr < 6; pr++) {
-          const int i = tc::kSplitI[pr], j = tc::kSplitJ[pr];
-          const uint64_t db = tc::umma_desc(tc::saddr(sBT + j * H::SZ_BT) + ch * (H::JC / 8) * 128, 128, N1 * 16);
-          for (int tt = 0; tt < 3; tt++) {
-            const uint64_t da = tc::umma_desc(tc::saddr(sK + i * H::SZ_K) + tt * 128 * H::JC * 2, 128, H::JC * 16);
-            tc::mma_bf16(tmem + H::COL_T + tt * F0, da, db, id32, (ch | pr) ? 1u : 0u);
-          }
+          const uint64_t db = tc::desc_at(dBc, tc::split_j(pr) * H::SZ_BT);
+#pragma unroll
+          for (int tt = 0; tt < 3; tt++)
+            tc::mma_bf16(tmem + H::COL_T + tt * F0, tc::desc_at(dKc, tc::split_i(pr) * H::SZ_K + tt * 128 * H::JC * 2),
+                         db, id32, (ch | pr) ? 1u : 0u);
         }
-        tc::mma_commit(bar_k);
+        tc::mma_commit(bar_k + kb);
       }
-      i_k++;
+      i_k[kb]++;
     }
     if (!ok) break;
-    // ---- the last latitude's kernel (warps 12-15, one (point, target) each) while the
-    // last GEMM 2 runs; then the transposed-DFT result -> shared (FP32) ------------------
+    // ---- the last latitude's kernel (warps 12-15, one (point, target) each) and its
+    // transposed DFT (its row of C, into a buffer outside U) while the last GEMMs 2 run;
+    // then the transposed-DFT result -> shared (FP32) ----------------------------------
     if (warp >= 12) {
       const int item = tid - 384, j = item >> 1, t = item & 1;
       const float* xs = sX32 + j;
@@ -891,7 +962,28 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
 #pragma unroll
       for (int c = 0; c < 6; c++) sK32[(t * 6 + c) * N1 + j] = (float)kv[c];
     }
-    wait(bar_k, n_k);  // the last chunk's GEMM 2 before TMEM is read and the region reused
+    __syncthreads();
+    // FP32 like the BF16-split GEMM of the other rows (the same FP32 values of Mf): a warp
+    // takes one component, its lanes the 32 Fourier columns (broadcast kernel values,
+    // conflict-free Mf^T rows). It read Mf from global memory in FP64 before, 32 cache lines
+    // per load: 42% of a rotation's time.
+    if (tid < 12 * F0) {
+      const int comp = tid / F0, jf = tid - comp * F0;
+      const float* kr = sK32 + comp * N1;
+      const float* mf = sMfT + jf;
+      float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+#pragma unroll 4
+      for (int j = 0; j < N1; j += 4) {
+        s0 = fmaf(kr[j], mf[j * F0], s0);
+        s1 = fmaf(kr[j + 1], mf[(j + 1) * F0], s1);
+        s2 = fmaf(kr[j + 2], mf[(j + 2) * F0], s2);
+        s3 = fmaf(kr[j + 3], mf[(j + 3) * F0], s3);
+      }
+      sC32[jf * 12 + comp] = (s0 + s1) + (s2 + s3);
+    }
+    // the last two chunks' GEMMs 2 before TMEM is read and U reused
+    wait(bar_k + 0, n_k[0]);
+    wait(bar_k + 1, n_k[1]);
     if (!(ok = sync_ok())) break;
     tc::tc_after_sync();
     if (warp < 12) {
@@ -908,38 +1000,36 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
     }
     tc::tc_before_sync();
     __syncthreads();
-    // the last latitude's transposed DFT (its row of C), FP32 like the BF16-split GEMM of
-    // the other rows (the same FP32 values of Mf): a warp takes one component, its lanes the
-    // 32 Fourier columns (broadcast kernel values, conflict-free Mf^T rows). It read Mf from
-    // global memory in FP64 before, 32 cache lines per load: 42% of a rotation's time.
-    if (tid < 12 * F0) {
-      const int comp = tid / F0, jf = tid - comp * F0;
-      const float* kr = sK32 + comp * N1;
-      const float* mf = sMfT + jf;
-      float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
-#pragma unroll 4
-      for (int j = 0; j < N1; j += 4) {
-        s0 = fmaf(kr[j], mf[j * F0], s0);
-        s1 = fmaf(kr[j + 1], mf[(j + 1) * F0], s1);
-        s2 = fmaf(kr[j + 2], mf[(j + 2) * F0], s2);
-        s3 = fmaf(kr[j + 3], mf[(j + 3) * F0], s3);
+    // ---- pass 2: transposed Legendre sums (FP32 FMA), one output coefficient and its 12
+    // components per thread; measured 1.1e-7 on the self velocity (emulation against the
+    // FP64 oracle). Latitude pairs first: row l <- C[l] + C[32 - l], row 32 - l <- C[l] -
+    // C[32 - l] (l < 16), so that a coefficient of parity n + m sums 17 rows with the
+    // tables of latitudes 0..16 (P_n^m at latitude 32 - l is (-1)^(n+m) that at l). -------
+    {
+      constexpr int RQ = F0 * 12 / 4;  // float4 per row of C
+      for (int i = tid; i < (H::P1 / 2) * RQ; i += NTHR) {
+        const int l = i / RQ, f = i - l * RQ;
+        float4* pa = reinterpret_cast<float4*>(sC + l * LDCL) + f;
+        float4* pb = reinterpret_cast<float4*>(l ? sC + (H::P1 - l) * LDCL : sC32) + f;  // row 32 in sC32
+        const float4 x = *pa, y = *pb;
+        *pa = make_float4(x.x + y.x, x.y + y.y, x.z + y.z, x.w + y.w);
+        *pb = make_float4(x.x - y.x, x.y - y.y, x.z - y.z, x.w - y.w);
       }
-      sC[32 * LDCL + jf * 12 + comp] = (s0 + s1) + (s2 + s3);
     }
     __syncthreads();
-    // ---- pass 2: transposed Legendre sums (FP32 FMA over the 33 latitudes), one output
-    // coefficient and its 12 components per thread; measured 1.1e-7 on the self velocity
-    // (emulation against the FP64 oracle) ----------------------------------------------
     if (tid < NC) {
-      const int c = tid;
-      const float4* a = reinterpret_cast<const float4*>(sC + sJf[c] * 12);
+      const int c = tid, jf = sJf[c];
+      const bool odd = (c - sBo[jf]) & 1;  // parity of n + m
+      const float4* a = reinterpret_cast<const float4*>(sC + jf * 12);
       const float* b = sTF + c;
       float acc[12];
 #pragma unroll
       for (int q = 0; q < 12; q++) acc[q] = 0.f;
-      for (int lat = 0; lat < L1; lat++) {
-        const float w = b[lat * LDF];
-        const float4* al = a + lat * (LDCL / 4);
+#pragma unroll 4
+      for (int l = 0; l < LH; l++) {
+        const float w = b[l * LDF];
+        const int row = (odd && l < H::P1 / 2) ? H::P1 - l : l;  // C- for odd parity; the equator alone
+        const float4* al = row == H::P1 ? reinterpret_cast<const float4*>(sC32 + jf * 12) : a + row * (LDCL / 4);
         const float4 a0 = al[0], a1 = al[1], a2 = al[2];
         acc[0] = fmaf(a0.x, w, acc[0]); acc[1] = fmaf(a0.y, w, acc[1]);
         acc[2] = fmaf(a0.z, w, acc[2]); acc[3] = fmaf(a0.w, w, acc[3]);
@@ -967,7 +1057,7 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
       }
     };
     for (int b = 0; b < 2; b++) drain(bar_r + b, n_r[b], i_r[b]);
-    drain(bar_k, n_k, i_k);
+    for (int b = 0; b < 2; b++) drain(bar_k + b, n_k[b], i_k[b]);
     drain(bar_mma1, n_mma1, i_mma1);
   }
   tc::tc_before_sync();
