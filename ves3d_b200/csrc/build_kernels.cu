@@ -624,7 +624,7 @@ __device__ __forceinline__ double area_of(double ax, double ay, double az, doubl
 
 template <int P0>
 __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restrict__ R, DevTables T,
-                                                          double* __restrict__ C, long nrot) {
+                                                          float* __restrict__ C, long nrot) {
   using G = RingCfg<P0>;
   using H = RingTcCfg<P0>;
   extern __shared__ __align__(1024) unsigned char smem[];
@@ -1070,7 +1070,7 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
 
 bool tc_build_supported(int p0, int p1) { return p0 == 16 && p1 == 32; }
 
-int launch_build_ring_tc(const double* R, long nrot, const DevTables& T, double* C, cudaStream_t st) {
+int launch_build_ring_tc(const double* R, long nrot, const DevTables& T, float* C, cudaStream_t st) {
   if (nrot <= 0) return VES3D_OK;
   if (!tc_build_supported(T.p0, T.p1)) {
     set_error("tensor-core build not laid out for p = %d, p_up = %d", T.p0, T.p1);

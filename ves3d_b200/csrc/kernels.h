@@ -38,6 +38,9 @@ int launch_analysis(const double* in, long nfun, int pin, int pout, const double
 // VES3D_TC_ANALYSIS=0 forces the generic kernel.
 int launch_grid2shc(const double* in, long nfun, int p, const double* four, const double* leg, const int* jf,
                     double* out, cudaStream_t st);
+// The same for FP32 grid values (FP64 arithmetic and output), p in {4, 8, 12, 16}.
+int launch_grid2shc_f32(const float* in, long nfun, int p, const double* four, const double* leg, const int* jf,
+                        double* out, cudaStream_t st);
 // shc_out[f][c] = shc_in[f][c] * scale[c] for nfun functions of nc coefficients
 int launch_scale_freq(const double* in, long nfun, int nc, const double* scale, double* out, cudaStream_t st);
 // SHC2Pole: P[2 f + t] = values of function f at x = -1 (t = 0) and x = +1 (t = 1) from its
@@ -80,6 +83,9 @@ int launch_singular_dl(const double* X, const double* Xt, const double* Xp, cons
 // RotateTranspose with dof = 12 (:452-541) fused with the Rearrange (:1090-1172):
 // C [nv][p0+1][p0][2][6][Ncoef] -> SL3 [nv][3][Ncoef][3][Ngrid].
 int launch_rotate_transpose_scatter(const double* C, long nv, const DevTables& T, double* SL3, cudaStream_t st);
+// The same from FP32 transposed-DFT results (the tensor-core build's), rotated back in FP32,
+// into an FP32 grid.
+int launch_rotate_transpose_f32(const float* C, long nv, const DevTables& T, float* SL3, cudaStream_t st);
 // Fused per-rotation build (FP64 tensor cores): R [nrot][3][Nc] -> C [nrot][2][6][Nc],
 // i.e. upsampled synthesis + singular kernel + transposed synthesis in one kernel.
 bool fused_build_supported(int p0, int p1);
@@ -87,7 +93,7 @@ int launch_build_ring(const double* R, long nrot, const DevTables& T, double* C,
 // Mixed form of the fused build: the DFT GEMMs on tcgen05 tensor cores as split-BF16
 // products with FP32 accumulation (Legendre sums, kernel and targets FP64); same layouts.
 bool tc_build_supported(int p0, int p1);
-int launch_build_ring_tc(const double* R, long nrot, const DevTables& T, double* C, cudaStream_t st);
+int launch_build_ring_tc(const double* R, long nrot, const DevTables& T, float* C, cudaStream_t st);
 // Error flag of the tensor-core build (a bounded wait ran out), optionally reset.
 int tc_build_error(bool reset);
 // V[v] = F[v] . SL[v] (src/StokesVelocity.cc:397-416), n = 3 Ncoef.

@@ -178,8 +178,8 @@ struct AnaTcCfg {
 // Persistent CTAs: the DFT and Legendre tables are staged once per CTA, which then walks
 // groups of FB functions (grid-stride). Per group: rows (function, latitude) x 2p DFT on
 // the tensor cores, then per-frequency Legendre sums on the CUDA cores.
-template <int P>
-__global__ void __launch_bounds__(256, 2) k_analysis_tc(const double* __restrict__ in, long nfun,
+template <int P, typename InT>
+__global__ void __launch_bounds__(256, 2) k_analysis_tc(const InT* __restrict__ in, long nfun,
                                                         const double* __restrict__ four, const double* __restrict__ leg,
                                                         const int* __restrict__ jf, double* __restrict__ out) {
   using G = AnaTcCfg<P>;
@@ -207,11 +207,11 @@ __global__ void __launch_bounds__(256, 2) k_analysis_tc(const double* __restrict
   auto load_group = [&](long g) {
     const long f0 = g * G::FB;
     const int nf = g < ngroups ? (int)min((long)G::FB, nfun - f0) : 0;
-    const double* src = in + (nf ? f0 : 0) * G::NLAT * G::NLON;  // no loads past the last group
+    const InT* src = in + (nf ? f0 : 0) * G::NLAT * G::NLON;  // no loads past the last group
 #pragma unroll
     for (int u = 0; u < U; u++) {
       const int i = tid + u * 256;
-      pre[u] = (i < G::ROWS * G::NLON && i / G::NLON < nf * G::NLAT) ? src[i] : 0.0;
+      pre[u] = (i < G::ROWS * G::NLON && i / G::NLON < nf * G::NLAT) ? (double)src[i] : 0.0;
     }
   };
   load_group(blockIdx.x);
@@ -311,14 +311,14 @@ static int sm_count() {
   return n;
 }
 
-template <int P>
-static int launch_ana_tc(const double* in, long nfun, const double* four, const double* leg, const int* jf,
+template <int P, typename InT>
+static int launch_ana_tc(const InT* in, long nfun, const double* four, const double* leg, const int* jf,
                          double* out, cudaStream_t st) {
   using G = AnaTcCfg<P>;
-  VES3D_CK(cudaFuncSetAttribute(k_analysis_tc<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM));
+  VES3D_CK(cudaFuncSetAttribute(k_analysis_tc<P, InT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM));
   const long ngroups = (nfun + G::FB - 1) / G::FB;
   const long grid = std::min(ngroups, 2L * sm_count());
-  k_analysis_tc<P><<<(unsigned)grid, 256, G::SMEM, st>>>(in, nfun, four, leg, jf, out);
+  k_analysis_tc<P, InT><<<(unsigned)grid, 256, G::SMEM, st>>>(in, nfun, four, leg, jf, out);
   VES3D_LAUNCHED();
   return VES3D_OK;
 }
@@ -339,6 +339,21 @@ int launch_grid2shc(const double* in, long nfun, int p, const double* four, cons
     }
   }
   return launch_analysis(in, nfun, p, p, four, leg, jf, out, st);
+}
+
+// Grid2SHC(p, p) of FP32 grid values (FP64 arithmetic and output), p in {4, 8, 12, 16}.
+int launch_grid2shc_f32(const float* in, long nfun, int p, const double* four, const double* leg, const int* jf,
+                        double* out, cudaStream_t st) {
+  if (nfun <= 0) return VES3D_OK;
+  switch (p) {
+    case 4: return launch_ana_tc<4>(in, nfun, four, leg, jf, out, st);
+    case 8: return launch_ana_tc<8>(in, nfun, four, leg, jf, out, st);
+    case 12: return launch_ana_tc<12>(in, nfun, four, leg, jf, out, st);
+    case 16: return launch_ana_tc<16>(in, nfun, four, leg, jf, out, st);
+    default: break;
+  }
+  set_error("Grid2SHC of FP32 values is instantiated for p in {4, 8, 12, 16}, not %d", p);
+  return VES3D_ERR_ARG;
 }
 
 }  // namespace ves3d

@@ -10,16 +10,22 @@
 
 namespace ves3d {
 
-// One CTA per (vesicle v, latitude rotation t); loops over the p0 longitude phases j.
+// One CTA per (vesicle v, latitude rotation t); loops over the p0 longitude phases j, JB
+// of them at a time (4, or fewer where the staging would not fit: p = 24).
 // out[c'] = sum_b (P_j s)[perm_n[b]] * Mr[t][n][b][pos(c')],   n = degree(c').
 // The blocks Mr[t][.] (mr_per_t doubles, contiguous for one t) are staged in shared memory.
+// Outputs are formed in degree-major order (a warp's lanes share a degree: one loop length,
+// broadcast inputs, consecutive block columns) and each thread forms its coefficient for
+// JB longitudes at once, reusing every block element.
+template <int JB>
 __global__ void __launch_bounds__(256) k_rotate_all(const double* __restrict__ S, int p0, int mr_per_t, DevTables T,
                                                     double* __restrict__ R) {
+  constexpr int kRaJ = JB;
   extern __shared__ double sm[];
   const int nc = p0 * (p0 + 2);
   double* sS = sm;
-  double* sB = sm + 3 * nc;
-  double* sM = sm + 6 * nc;
+  double* sB = sm + 3 * nc;                                        // [kRaJ][3 nc]
+  double* sM = sB + kRaJ * 3 * nc;
   double* sCs = sM + mr_per_t;                                     // cos_tab [2 p0]
   double* sSn = sCs + 2 * p0;                                      // sin_tab [2 p0]
   int* sMo = reinterpret_cast<int*>(sSn + 2 * p0);                 // mr_off of (t, n) - base [p0 + 1]
@@ -27,8 +33,7 @@ __global__ void __launch_bounds__(256) k_rotate_all(const double* __restrict__ S
   short* sPc = reinterpret_cast<short*>(sPo + (p0 + 2));           // partner [nc]
   unsigned short* sPerm = reinterpret_cast<unsigned short*>(sPc + nc);  // perm [nc]
   unsigned char* sMs = reinterpret_cast<unsigned char*>(sPerm + nc);    // m | (is_sin << 7) [nc]
-  unsigned char* sN = sMs + nc;                                    // degree [nc]
-  unsigned char* sBp = sN + nc;                                    // position in block [nc]
+  unsigned char* sNd = sMs + nc;                                   // degree of degree-major position [nc]
   const int t = blockIdx.x;
   const long v = blockIdx.y;
   const int mbase = __ldg(T.mr_off + t * (p0 + 1));
@@ -44,38 +49,47 @@ __global__ void __launch_bounds__(256) k_rotate_all(const double* __restrict__ S
     sPc[c] = (short)__ldg(T.partner + c);
     sPerm[c] = (unsigned short)__ldg(T.perm + c);
     sMs[c] = (unsigned char)(__ldg(T.m_of_coef + c) | (__ldg(T.is_sin + c) ? 0x80 : 0));
-    sN[c] = (unsigned char)__ldg(T.n_of_coef + c);
-    sBp[c] = (unsigned char)__ldg(T.pos_in_block + c);
+    const int n = __ldg(T.n_of_coef + c);
+    sNd[__ldg(T.perm_off + n) + __ldg(T.pos_in_block + c)] = (unsigned char)n;
   }
   __syncthreads();
-  for (int j = 0; j < p0; j++) {
-    for (int i = threadIdx.x; i < 3 * nc; i += blockDim.x) {
-      const int d = i / nc, c = i % nc;
+  for (int j0 = 0; j0 < p0; j0 += kRaJ) {
+    const int nj = min(kRaJ, p0 - j0);
+    for (int i = threadIdx.x; i < nj * 3 * nc; i += blockDim.x) {
+      const int jj = i / (3 * nc), r = i - jj * 3 * nc;
+      const int d = r / nc, c = r - d * nc;
       const int pc = sPc[c];
+      double val;
       if (pc < 0) {
-        sB[i] = sS[i];
+        val = sS[r];
       } else {
         const int ms = sMs[c];
-        const int q = ((ms & 0x7f) * j) % (2 * p0);
+        const int q = ((ms & 0x7f) * (j0 + jj)) % (2 * p0);
         const double cs = sCs[q], sn = sSn[q];
-        if (!(ms & 0x80)) {
-          sB[i] = sS[i] * cs + sS[d * nc + pc] * sn;
-        } else {
-          sB[i] = -sS[d * nc + pc] * sn + sS[i] * cs;
-        }
+        val = (ms & 0x80) ? -sS[d * nc + pc] * sn + sS[r] * cs : sS[r] * cs + sS[d * nc + pc] * sn;
       }
+      sB[jj * 3 * nc + r] = val;
     }
     __syncthreads();
-    double* out = R + (((v * (p0 + 1) + t) * p0 + j) * 3) * (long)nc;
     for (int i = threadIdx.x; i < 3 * nc; i += blockDim.x) {
-      const int d = i / nc, c = i % nc;
-      const int n = sN[c], bp = sBp[c];
-      const int po = sPo[n], bn = sPo[n + 1] - po;
-      const double* M = sM + sMo[n];
+      const int d = i / nc, e = i - d * nc;  // e: degree-major position of the output
+      const int n = sNd[e];
+      const int po = sPo[n], bn = sPo[n + 1] - po, bp = e - po;
+      const double* M = sM + sMo[n] + bp;
       const double* b = sB + d * nc;
-      double s = 0.0;
-      for (int k = 0; k < bn; k++) s = fma(b[sPerm[po + k]], M[k * bn + bp], s);
-      out[i] = s;
+      double acc[kRaJ];
+#pragma unroll
+      for (int q = 0; q < kRaJ; q++) acc[q] = 0.0;
+      for (int k = 0; k < bn; k++) {
+        const double m = M[k * bn];
+        const int src = sPerm[po + k];
+#pragma unroll
+        for (int q = 0; q < kRaJ; q++) acc[q] = fma(b[q * 3 * nc + src], m, acc[q]);
+      }
+      const int c = sPerm[e];
+#pragma unroll
+      for (int q = 0; q < kRaJ; q++)
+        if (q < nj) R[(((v * (p0 + 1) + t) * p0 + j0 + q) * 3 + d) * (long)nc + c] = acc[q];
     }
     __syncthreads();
   }
@@ -131,11 +145,25 @@ int launch_rotate_all(const double* S, long nv, const DevTables& T, double* R, c
     set_error("rotation kernels support SH orders up to 127");
     return VES3D_ERR_ARG;
   }
-  const size_t smem = ((6 * nc + mpt + 4 * p0) * sizeof(double) + (2 * p0 + 3) * sizeof(int) + nc * 4 + nc * 3 + 15) /
-                      16 * 16;
-  if (smem > 48 * 1024) VES3D_CK(cudaFuncSetAttribute(k_rotate_all, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  auto smem_of = [&](int jb) {
+    return (((3 + 3 * (size_t)jb) * nc + mpt + 4 * p0) * sizeof(double) + (2 * p0 + 3) * sizeof(int) + nc * 4 + nc * 2 +
+            15) / 16 * 16;
+  };
   dim3 grid(p0 + 1, (unsigned)nv);
-  k_rotate_all<<<grid, 256, smem, st>>>(S, p0, mpt, T, R);
+  const size_t cap = 227 * 1024;
+  if (smem_of(4) <= cap) {
+    VES3D_CK(cudaFuncSetAttribute(k_rotate_all<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_of(4)));
+    k_rotate_all<4><<<grid, 256, smem_of(4), st>>>(S, p0, mpt, T, R);
+  } else if (smem_of(2) <= cap) {
+    VES3D_CK(cudaFuncSetAttribute(k_rotate_all<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_of(2)));
+    k_rotate_all<2><<<grid, 256, smem_of(2), st>>>(S, p0, mpt, T, R);
+  } else if (smem_of(1) <= cap) {
+    VES3D_CK(cudaFuncSetAttribute(k_rotate_all<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_of(1)));
+    k_rotate_all<1><<<grid, 256, smem_of(1), st>>>(S, p0, mpt, T, R);
+  } else {
+    set_error("RotateAll: the rotation blocks of p = %d do not fit in shared memory", p0);
+    return VES3D_ERR_ARG;
+  }
   VES3D_LAUNCHED();
   return VES3D_OK;
 }
@@ -243,8 +271,6 @@ __global__ void __launch_bounds__(256) k_rotate_transpose_scatter(const double* 
   const long v = blockIdx.y;
   const int mbase = __ldg(T.mr_off + t * (p0 + 1));
   for (int i = threadIdx.x; i < mr_per_t; i += blockDim.x) sM[i] = __ldg(T.mr + mbase + i);
-  // symmetric component -> (c_in, c_out) pairs
-  const int ci0[6] = {0, 0, 0, 1, 1, 2}, co0[6] = {0, 1, 2, 1, 2, 2};
   for (int pole = 0; pole < 2; pole++) {
     for (int comp = 0; comp < 6; comp++) {
       for (int j0 = 0; j0 < p0; j0 += jb) {
@@ -295,13 +321,154 @@ __global__ void __launch_bounds__(256) k_rotate_transpose_scatter(const double* 
             }
           }
           const int grid = pole == 0 ? t * 2 * p0 + j : (p0 - t) * 2 * p0 + p0 + j;
-          const int cin = ci0[comp], cout = co0[comp];
+          const int cin = comp < 3 ? 0 : (comp < 5 ? 1 : 2), cout = comp < 3 ? comp : (comp < 5 ? comp - 2 : 2);  // (0,0) (0,1) (0,2) (1,1) (1,2) (2,2)
           SL3[(((v * 3 + cin) * nc + c) * 3 + cout) * (long)ng + grid] = val;
           if (cin != cout) SL3[(((v * 3 + cout) * nc + c) * 3 + cin) * (long)ng + grid] = val;
         }
       }
     }
   }
+}
+
+// Mixed form of the rotate-transpose (after the tensor-core build, whose transposed-DFT
+// results C are FP32): one CTA per (latitude rotation t, vesicle v), rows (component,
+// longitude j) in groups of CB components. Per degree n the rotation back
+//     B[row][po + b] = sum_k A[row][po + k] Mr_{t,n}[b][k]
+// runs in FP32 on the CUDA cores (the values carry FP32 precision already; the FP64 form
+// uses the DMMA kernel below), reading the degree-major staged inputs and the rotation
+// blocks of this t held in shared memory with an odd row stride (bn | 1: consecutive b of a
+// warp fall on distinct banks); then the inverse longitude phase and the scatter into the
+// self-matrix grid SL3 (FP32: the Grid2SHC that follows reads it into FP64), laid out as the
+// FP64 forms'. Compared with the DMMA form on FP64 C it moves half the bytes and keeps no
+// per-degree barriers.
+template <int CB>
+__global__ void __launch_bounds__(256, 3) k_rotate_transpose_f32(const float* __restrict__ C, int p0, int mr_per_t,
+                                                              DevTables T, float* __restrict__ SL3) {
+  extern __shared__ __align__(16) float smf[];
+  const int nc = p0 * (p0 + 2), ng = 2 * p0 * (p0 + 1);
+  const int lda = nc + 1;  // odd row stride
+  const int rows = CB * p0;
+  float* sA = smf;                         // [rows][lda], degree-major
+  float* sB = sA + rows * lda;             // [rows][lda], coefficient order
+  float* sM = sB + rows * lda;             // blocks of degree n at sMo[n], rows of bn | 1
+  const int msz = mr_per_t + (p0 + 1) * 2 * p0;  // (upper bound of the padded size)
+  float* sCs = sM + msz;                   // cos_tab [2 p0]
+  float* sSn = sCs + 2 * p0;               // sin_tab [2 p0]
+  int* sMo = reinterpret_cast<int*>(sSn + 2 * p0);           // [p0 + 2] padded block offsets
+  unsigned short* sDm = reinterpret_cast<unsigned short*>(sMo + p0 + 2);  // degree-major position [nc]
+  short* sPc = reinterpret_cast<short*>(sDm + nc);                       // partner (or -1) [nc]
+  unsigned char* sMs = reinterpret_cast<unsigned char*>(sPc + nc);       // m | (is_sin << 7) [nc]
+  unsigned char* sN = sMs + nc;                                           // degree of position d [nc]
+  unsigned short* sP = reinterpret_cast<unsigned short*>(sN + ((nc + 1) & ~1));  // coefficient at d [nc]
+  const int t = blockIdx.x;
+  const long v = blockIdx.y;
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    int o = 0;
+    for (int n = 0; n <= p0; n++) {
+      sMo[n] = o;
+      const int bn = __ldg(T.perm_off + n + 1) - __ldg(T.perm_off + n);
+      o += bn * (bn | 1);
+    }
+    sMo[p0 + 1] = o;
+  }
+  for (int c = tid; c < nc; c += 256) {
+    const int n = __ldg(T.n_of_coef + c);
+    const int d = __ldg(T.perm_off + n) + __ldg(T.pos_in_block + c);
+    sDm[c] = (unsigned short)d;
+    sPc[c] = (short)__ldg(T.partner + c);
+    sMs[c] = (unsigned char)(__ldg(T.m_of_coef + c) | (__ldg(T.is_sin + c) ? 0x80 : 0));
+    sN[d] = (unsigned char)n;
+    sP[d] = (unsigned short)c;
+  }
+  for (int i = tid; i < 2 * p0; i += 256) {
+    sCs[i] = (float)__ldg(T.cos_tab + i);
+    sSn[i] = (float)__ldg(T.sin_tab + i);
+  }
+  __syncthreads();
+  // the rotation blocks of this t, FP32, rows padded to bn + 1
+  for (int n = 0; n <= p0; n++) {
+    const int bn = __ldg(T.perm_off + n + 1) - __ldg(T.perm_off + n);
+    const double* M = T.mr + __ldg(T.mr_off + t * (p0 + 1) + n);
+    for (int i = tid; i < bn * bn; i += 256) {
+      const int b = i / bn, k = i - b * bn;
+      sM[sMo[n] + b * (bn | 1) + k] = (float)__ldg(M + i);
+    }
+  }
+  for (int pole = 0; pole < 2; pole++) {
+    for (int comp0 = 0; comp0 < 6; comp0 += CB) {
+      __syncthreads();
+      // stage: A[(cc, j)][dm(c)] = C[v][t][j][pole][comp0 + cc][c]
+      for (int i = tid; i < rows * nc; i += 256) {
+        const int r = i / nc, c = i - r * nc;
+        const int cc = r / p0, j = r - cc * p0;
+        sA[r * lda + sDm[c]] = C[((((v * (p0 + 1) + t) * p0 + j) * 2 + pole) * 6 + comp0 + cc) * (long)nc + c];
+      }
+      __syncthreads();
+      // rotation back: thread (degree-major position d, 4 rows), so that a warp's lanes
+      // share a degree (the same loop length, broadcast inputs, consecutive block rows)
+      const int nrq = (rows + 3) / 4;
+      for (int i = tid; i < nrq * nc; i += 256) {
+        const int d = i % nc, rq = i / nc;
+        const int n = sN[d], c = sP[d];
+        const int po = __ldg(T.perm_off + n), bn = __ldg(T.perm_off + n + 1) - po;
+        const int b = d - po;
+        const float* M = sM + sMo[n] + b * (bn | 1);
+        const float* a = sA + rq * 4 * lda + po;
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int k = 0; k < bn; k++) {
+          const float m = M[k];
+#pragma unroll
+          for (int q = 0; q < 4; q++) acc[q] = fmaf(a[q * lda + k], m, acc[q]);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          if (rq * 4 + q < rows) sB[(rq * 4 + q) * lda + c] = acc[q];
+      }
+      __syncthreads();
+      // inverse phase and scatter; consecutive threads take consecutive j
+      for (int i = tid; i < rows * nc; i += 256) {
+        const int j = i % p0, rest = i / p0;
+        const int c = rest % nc, cc = rest / nc;
+        const float* in = sB + (cc * p0 + j) * lda;
+        const int pc = sPc[c];
+        float val;
+        if (pc < 0) {
+          val = in[c];
+        } else {
+          const int ms = sMs[c];
+          const int q = ((ms & 0x7f) * j) % (2 * p0);
+          const float cs = sCs[q], sn = sSn[q];
+          val = (ms & 0x80) ? fmaf(in[pc], sn, in[c] * cs) : fmaf(-in[pc], sn, in[c] * cs);
+        }
+        const int grid = pole == 0 ? t * 2 * p0 + j : (p0 - t) * 2 * p0 + p0 + j;
+        // symmetric component -> (c_in, c_out): (0,0) (0,1) (0,2) (1,1) (1,2) (2,2)
+        const int comp = comp0 + cc;
+        const int cin = comp < 3 ? 0 : (comp < 5 ? 1 : 2), cout = comp < 3 ? comp : (comp < 5 ? comp - 2 : 2);
+        SL3[(((v * 3 + cin) * nc + c) * 3 + cout) * (long)ng + grid] = val;
+        if (cin != cout) SL3[(((v * 3 + cout) * nc + c) * 3 + cin) * (long)ng + grid] = val;
+      }
+    }
+  }
+}
+
+static size_t rt_f32_smem(int p0, int cb, int mpt) {
+  const int nc = p0 * (p0 + 2), lda = nc + 1;
+  const size_t fl = (size_t)2 * cb * p0 * lda + mpt + (size_t)(p0 + 1) * 2 * p0 + 4 * p0;
+  return fl * sizeof(float) + (size_t)(p0 + 2) * sizeof(int) + (size_t)nc * 8 + 16;
+}
+
+int launch_rotate_transpose_f32(const float* C, long nv, const DevTables& T, float* SL3, cudaStream_t st) {
+  if (nv <= 0) return VES3D_OK;
+  const int p0 = T.p0, mpt = mr_per_t(T);
+  dim3 grid(p0 + 1, (unsigned)nv);
+  // one component per group: 68 KB of shared memory at p = 16, three CTAs per SM (two
+  // components per group, two CTAs: 9.1 ms at 512 vesicles)
+  const size_t smem = rt_f32_smem(p0, 1, mpt);
+  VES3D_CK(cudaFuncSetAttribute(k_rotate_transpose_f32<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_rotate_transpose_f32<1><<<grid, 256, smem, st>>>(C, p0, mpt, T, SL3);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
 }
 
 // VES3D_TC_ROTATE=0 selects the CUDA-core form of the rotate-transpose (for comparison).
@@ -365,7 +532,6 @@ __global__ void __launch_bounds__(256, 2) k_rotate_transpose_tc(const double* __
     const int r = i / ldi, col = i - r * ldi;
     if (r >= rows || col >= nc) sIn[i] = 0.0;
   }
-  const int ci0[6] = {0, 0, 0, 1, 1, 2}, co0[6] = {0, 1, 2, 1, 2, 2};
   const int mtiles = rows8 / 8;
   for (int pole = 0; pole < 2; pole++) {
     for (int comp0 = 0; comp0 < 6; comp0 += cb) {
@@ -458,7 +624,7 @@ __global__ void __launch_bounds__(256, 2) k_rotate_transpose_tc(const double* __
         }
         const int grid = pole == 0 ? t * 2 * p0 + j : (p0 - t) * 2 * p0 + p0 + j;
         const int comp = comp0 + cc;
-        const int cin = ci0[comp], cout = co0[comp];
+        const int cin = comp < 3 ? 0 : (comp < 5 ? 1 : 2), cout = comp < 3 ? comp : (comp < 5 ? comp - 2 : 2);  // (0,0) (0,1) (0,2) (1,1) (1,2) (2,2)
         SL3[(((v * 3 + cin) * nc + c) * 3 + cout) * (long)ng + grid] = val;
         if (cin != cout) SL3[(((v * 3 + cout) * nc + c) * 3 + cin) * (long)ng + grid] = val;
       }

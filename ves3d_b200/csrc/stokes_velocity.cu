@@ -490,8 +490,11 @@ int run_setup(ves3d_sv* sv, bool dl) {
     const long nb = std::min(sv->chunk, sv->nves - v0);
     const long nrot = nb * npr;
     if ((s = launch_rotate_all(sv->Sx + v0 * 3 * nc, nb, T, sv->R, st))) return s;
+    // the tensor-core build leaves FP32 transposed-DFT results (in the first half of C),
+    // rotated back in FP32; the FP64 builds leave FP64 ones
+    float* Cf = reinterpret_cast<float*>(sv->C);
     if (fused && tc) {
-      if ((s = launch_build_ring_tc(sv->R, nrot, T, sv->C, st))) return s;
+      if ((s = launch_build_ring_tc(sv->R, nrot, T, Cf, st))) return s;
     } else if (fused) {
       if ((s = launch_build_ring(sv->R, nrot, T, sv->C, st))) return s;
     } else {
@@ -503,10 +506,15 @@ int run_setup(ves3d_sv* sv, bool dl) {
       if ((s = launch_analysis(sv->K, nrot * 12, p1, p0, T.synT_four, T.syn1_leg, T.jf_of_coef, sv->C, st)))
         return s;
     }
-    if ((s = launch_rotate_transpose_scatter(sv->C, nb, T, sv->SL3, st))) return s;
-    if ((s = launch_grid2shc(sv->SL3, nb * 3 * nc * 3, p0, T.ana_four, T.ana_leg, T.jf_of_coef,
-                             M + v0 * (long)(3 * nc) * (3 * nc), st)))
-      return s;
+    double* Mv = M + v0 * (long)(3 * nc) * (3 * nc);
+    if (fused && tc) {  // FP32 grid between the rotation back and Grid2SHC
+      float* SLf = reinterpret_cast<float*>(sv->SL3);
+      if ((s = launch_rotate_transpose_f32(Cf, nb, T, SLf, st))) return s;
+      if ((s = launch_grid2shc_f32(SLf, nb * 3 * nc * 3, p0, T.ana_four, T.ana_leg, T.jf_of_coef, Mv, st))) return s;
+    } else {
+      if ((s = launch_rotate_transpose_scatter(sv->C, nb, T, sv->SL3, st))) return s;
+      if ((s = launch_grid2shc(sv->SL3, nb * 3 * nc * 3, p0, T.ana_four, T.ana_leg, T.jf_of_coef, Mv, st))) return s;
+    }
     (void)ng;
     (void)M1;
   }
