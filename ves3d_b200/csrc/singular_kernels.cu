@@ -398,11 +398,29 @@ __global__ void __launch_bounds__(256, 3) k_rotate_transpose_f32(const float* __
   for (int pole = 0; pole < 2; pole++) {
     for (int comp0 = 0; comp0 < 6; comp0 += CB) {
       __syncthreads();
-      // stage: A[(cc, j)][dm(c)] = C[v][t][j][pole][comp0 + cc][c]
-      for (int i = tid; i < rows * nc; i += 256) {
-        const int r = i / nc, c = i - r * nc;
-        const int cc = r / p0, j = r - cc * p0;
-        sA[r * lda + sDm[c]] = C[((((v * (p0 + 1) + t) * p0 + j) * 2 + pole) * 6 + comp0 + cc) * (long)nc + c];
+      // stage: A[(cc, j)][dm(c)] = C[v][t][j][pole][comp0 + cc][c], eight loads in flight
+      // per thread before the shared-memory stores (degree-major: the rotation below reads
+      // a degree's inputs contiguously; gathering them through the permutation there cost
+      // more issue slots than the scattered stores here)
+      for (int i0 = tid; i0 < rows * nc; i0 += 256 * 8) {
+        float val[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          const int i = i0 + u * 256;
+          if (i < rows * nc) {
+            const int r = i / nc, c = i - r * nc;
+            const int cc = r / p0, j = r - cc * p0;
+            val[u] = C[((((v * (p0 + 1) + t) * p0 + j) * 2 + pole) * 6 + comp0 + cc) * (long)nc + c];
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          const int i = i0 + u * 256;
+          if (i < rows * nc) {
+            const int r = i / nc, c = i - r * nc;
+            sA[r * lda + sDm[c]] = val[u];
+          }
+        }
       }
       __syncthreads();
       // rotation back: thread (degree-major position d, 4 rows), so that a warp's lanes
