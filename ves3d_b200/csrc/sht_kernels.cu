@@ -311,6 +311,129 @@ static int sm_count() {
   return n;
 }
 
+// Grid2SHC(p, p) of FP32 grid values in FP32 on the CUDA cores (the mixed form's
+// self-matrix grid, whose values carry FP32 precision): persistent CTAs stage the DFT and
+// Legendre tables (FP32) once and walk groups of FB functions. Per group the length-2p DFT of
+// every (function, latitude) row, one thread per 4 rows x 4 frequencies (16 accumulators:
+// row values broadcast across a warp's frequency quads, conflict-free table rows), then the
+// per-frequency Legendre sums, one thread per (function, coefficient); the next group's grid
+// values are loaded into registers meanwhile. Output FP64 like the FP64 forms'.
+template <int P>
+struct AnaF32Cfg {
+  static constexpr int FB = 8;
+  static constexpr int NLAT = P + 1, NLON = 2 * P, NC = P * (P + 2);
+  static constexpr int ROWS = FB * NLAT, RQ = (ROWS + 3) / 4, KQ = NLON / 4;
+  static constexpr int LDG = NLON + 1;  // grid rows (odd: a warp's 4 row quads on distinct banks)
+  static constexpr int LDF = NLON + 1;  // DFT result rows
+  static constexpr int SZ_G = RQ * 4 * LDG, SZ_F = ROWS * LDF;
+  static constexpr int OFF_G = 0, OFF_F = OFF_G + SZ_G, OFF_M = OFF_F + SZ_F, OFF_L = OFF_M + NLON * NLON;
+  static constexpr int OFF_JF = OFF_L + NC * NLAT;
+  static constexpr size_t SMEM = (size_t)(OFF_JF + NC) * sizeof(float);
+  static constexpr int U = (ROWS * NLON + 255) / 256;  // grid values per thread per group
+  static_assert(NLON % 4 == 0, "frequency quads");
+};
+
+template <int P>
+__global__ void __launch_bounds__(256, 3) k_analysis_f32(const float* __restrict__ in, long nfun,
+                                                         const double* __restrict__ four,
+                                                         const double* __restrict__ leg, const int* __restrict__ jf,
+                                                         double* __restrict__ out) {
+  using G = AnaF32Cfg<P>;
+  extern __shared__ __align__(16) float smf[];
+  float* sG = smf + G::OFF_G;
+  float* sF = smf + G::OFF_F;
+  float* sM = smf + G::OFF_M;  // four [j][k], row stride NLON (float4 reads of 4 frequencies)
+  float* sL = smf + G::OFF_L;  // leg [c][lat]
+  int* sJf = reinterpret_cast<int*>(smf + G::OFF_JF);
+  const int tid = threadIdx.x;
+  for (int i = tid; i < G::NLON * G::NLON; i += 256) sM[i] = (float)__ldg(four + i);
+  for (int i = tid; i < G::NC * G::NLAT; i += 256) sL[i] = (float)__ldg(leg + i);
+  for (int i = tid; i < G::NC; i += 256) sJf[i] = __ldg(jf + i);
+  // rows past the group's last function stay zero (their outputs are never written)
+  for (int i = tid; i < G::SZ_G; i += 256) sG[i] = 0.f;
+  const long ngroups = (nfun + G::FB - 1) / G::FB;
+  float pre[G::U];
+  auto load_group = [&](long g) {
+    const long f0 = g * G::FB;
+    const int nf = g < ngroups ? (int)min((long)G::FB, nfun - f0) : 0;
+    const float* src = in + (nf ? f0 : 0) * G::NLAT * G::NLON;
+#pragma unroll
+    for (int u = 0; u < G::U; u++) {
+      const int i = tid + u * 256;
+      pre[u] = (i < nf * G::NLAT * G::NLON) ? src[i] : 0.f;
+    }
+  };
+  load_group(blockIdx.x);
+  for (long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+    const long f0 = grp * G::FB;
+    const int nf = (int)min((long)G::FB, nfun - f0);
+    __syncthreads();  // the previous group's sG / sF reads are done
+#pragma unroll
+    for (int u = 0; u < G::U; u++) {
+      const int i = tid + u * 256;
+      if (i < G::ROWS * G::NLON) {
+        const int r = i / G::NLON, j = i - r * G::NLON;
+        sG[r * G::LDG + j] = pre[u];
+      }
+    }
+    __syncthreads();
+    load_group(grp + gridDim.x);
+    // DFT: F[r][k] = sum_j G[r][j] four[j][k]
+    for (int it = tid; it < G::RQ * G::KQ; it += 256) {
+      const int kq = it % G::KQ, rq = it / G::KQ;
+      const float* g = sG + rq * 4 * G::LDG;
+      const float4* m = reinterpret_cast<const float4*>(sM) + kq;
+      float acc[4][4] = {};
+#pragma unroll 8
+      for (int j = 0; j < G::NLON; j++) {
+        const float4 b = m[j * G::KQ];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const float a = g[q * G::LDG + j];
+          acc[q][0] = fmaf(a, b.x, acc[q][0]);
+          acc[q][1] = fmaf(a, b.y, acc[q][1]);
+          acc[q][2] = fmaf(a, b.z, acc[q][2]);
+          acc[q][3] = fmaf(a, b.w, acc[q][3]);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int r = rq * 4 + q;
+        if (r < G::ROWS) {
+          float* o = sF + r * G::LDF + kq * 4;
+          o[0] = acc[q][0];
+          o[1] = acc[q][1];
+          o[2] = acc[q][2];
+          o[3] = acc[q][3];
+        }
+      }
+    }
+    __syncthreads();
+    // Legendre: out[f][c] = sum_lat F[f][lat][jf(c)] leg[c][lat]
+    for (int i = tid; i < nf * G::NC; i += 256) {
+      const int f = i / G::NC, c = i - f * G::NC;
+      const float* fr = sF + (f * G::NLAT) * G::LDF + sJf[c];
+      const float* lr = sL + c * G::NLAT;
+      float s = 0.f;
+#pragma unroll
+      for (int lat = 0; lat < G::NLAT; lat++) s = fmaf(fr[lat * G::LDF], lr[lat], s);
+      out[(f0 + f) * G::NC + c] = (double)s;
+    }
+  }
+}
+
+template <int P>
+static int launch_ana_f32(const float* in, long nfun, const double* four, const double* leg, const int* jf,
+                          double* out, cudaStream_t st) {
+  using G = AnaF32Cfg<P>;
+  VES3D_CK(cudaFuncSetAttribute(k_analysis_f32<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM));
+  const long ngroups = (nfun + G::FB - 1) / G::FB;
+  const long grid = std::min(ngroups, 3L * sm_count());
+  k_analysis_f32<P><<<(unsigned)grid, 256, G::SMEM, st>>>(in, nfun, four, leg, jf, out);
+  VES3D_LAUNCHED();
+  return VES3D_OK;
+}
+
 template <int P, typename InT>
 static int launch_ana_tc(const InT* in, long nfun, const double* four, const double* leg, const int* jf,
                          double* out, cudaStream_t st) {
@@ -341,7 +464,9 @@ int launch_grid2shc(const double* in, long nfun, int p, const double* four, cons
   return launch_analysis(in, nfun, p, p, four, leg, jf, out, st);
 }
 
-// Grid2SHC(p, p) of FP32 grid values (FP64 arithmetic and output), p in {4, 8, 12, 16}.
+// Grid2SHC(p, p) of FP32 grid values, p in {4, 8, 12, 16}: FP32 arithmetic on the CUDA
+// cores at p = 16 (the mixed self-matrix grid), FP64 DMMA from the FP32 values otherwise;
+// FP64 output.
 int launch_grid2shc_f32(const float* in, long nfun, int p, const double* four, const double* leg, const int* jf,
                         double* out, cudaStream_t st) {
   if (nfun <= 0) return VES3D_OK;
@@ -349,7 +474,7 @@ int launch_grid2shc_f32(const float* in, long nfun, int p, const double* four, c
     case 4: return launch_ana_tc<4>(in, nfun, four, leg, jf, out, st);
     case 8: return launch_ana_tc<8>(in, nfun, four, leg, jf, out, st);
     case 12: return launch_ana_tc<12>(in, nfun, four, leg, jf, out, st);
-    case 16: return launch_ana_tc<16>(in, nfun, four, leg, jf, out, st);
+    case 16: return launch_ana_f32<16>(in, nfun, four, leg, jf, out, st);
     default: break;
   }
   set_error("Grid2SHC of FP32 values is instantiated for p in {4, 8, 12, 16}, not %d", p);
