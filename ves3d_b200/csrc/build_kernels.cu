@@ -579,7 +579,8 @@ struct RingTcCfg {
   static constexpr int OFF_C32 = al16(OFF_MFT + N1 * F0 * 4);         // row 32 of C [F0][12], outside U
   static constexpr int OFF_TRG = al16(OFF_C32 + F0 * 12 * 4);
   static constexpr int OFF_CEN = OFF_TRG + 6 * 8;
-  static constexpr int OFF_SW = OFF_CEN + 6 * 8;
+  static constexpr int OFF_CQ = OFF_CEN + 6 * 8;  // the centres over the m = 0 Fourier row
+  static constexpr int OFF_SW = OFF_CQ + 6 * 8;
   static constexpr int OFF_BO = OFF_SW + L1 * 8;
   static constexpr int OFF_JF = OFF_BO + ((F0 + 1) * 4 + 7) / 8 * 8;   // Fourier block of each coefficient
   static constexpr int OFF_BAR = OFF_JF + (NC + 7) / 8 * 8;
@@ -645,6 +646,7 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
   float* sC32 = reinterpret_cast<float*>(smem + H::OFF_C32);
   double* trg = reinterpret_cast<double*>(smem + H::OFF_TRG);
   double* cen = reinterpret_cast<double*>(smem + H::OFF_CEN);
+  double* cq = reinterpret_cast<double*>(smem + H::OFF_CQ);
   double* sSw = reinterpret_cast<double*>(smem + H::OFF_SW);
   int* sBo = reinterpret_cast<int*>(smem + H::OFF_BO);
   unsigned char* sJf = smem + H::OFF_JF;
@@ -753,99 +755,116 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
       trg[c * 2 + t] = s;
     }
     __syncthreads();
-    if (tid < 6) cen[tid] = trg[(tid % 3) * 2 + tid / 3];  // cen[h * 3 + d]: target of hemisphere h
+    if (tid < 6) {  // cen[h * 3 + d]: target of hemisphere h; cq the same over the m = 0 row
+      const double c = trg[(tid % 3) * 2 + tid / 3];
+      cen[tid] = c;
+      cq[tid] = c / mf00;
+    }
     for (int c = tid; c < NC; c += NTHR) sR4[c] = make_float4((float)sR[c], (float)sR[LDR + c], (float)sR[2 * LDR + c], 0.f);
     __syncthreads();
     // ---- pass 1: Legendre synthesis -> split BF16 A, dA -----------------------------------
     // the m = 0 block in FP64 (it carries the vesicle's position, shifted by the pole target
     // here), the others in FP32 (shape-sized terms; their sums are rounded to FP32 for the
     // split anyway)
-    // item (pair of Fourier blocks k0, k0 + 1; latitude pair l): sums over each block split by
-    // the parity of n + m give latitude l (even + odd) and its mirror 32 - l (even - odd; the
-    // theta derivative odd - even) from one pass over the coefficients (P_n^m(-x) =
-    // (-1)^(n+m) P_n^m(x) on the symmetric Gauss nodes); l = 16 is the equator. A warp holds
-    // 8 latitude pairs x 4 block pairs, so each of its bf16x2 stores fills whole core
-    // matrices of the K-major operands (conflict-free); warps 0-7 take l < 16, warp 8 the
-    // equator.
-    static_assert(H::P1 == 32 && LH == 17 && F0 == 32 && NTHR >= 9 * 32, "latitude and block pairs");
+    // Sums over Fourier block k at latitude pair l, split by the parity of n + m: latitude l
+    // is even + odd, its mirror 32 - l even - odd (the theta derivative odd - even), from
+    // one pass over the coefficients (P_n^m(-x) = (-1)^(n+m) P_n^m(x) on the symmetric Gauss
+    // nodes); l = 16 is the equator. The m = 0 block in FP64, centred on the pole targets
+    // (its values carry the vesicle's position), the others in FP32.
+    auto block_sums = [&](int k, int l, float* ev, float* od, float* dev, float* dod) {
+      if (k == 0) {
+        const double* L = sT0 + l * LD0;
+        const double* dL = sT0 + (LH + l) * LD0;
+        double e0 = 0, e1 = 0, e2 = 0, f0 = 0, f1 = 0, f2 = 0;  // n even
+        double o0 = 0, o1 = 0, o2 = 0, g0 = 0, g1 = 0, g2 = 0;  // n odd
+#pragma unroll
+        for (int c = 0; c < M0; c += 2) {
+          const double lv = L[c], dl = dL[c], r0 = sR[c], r1 = sR[LDR + c], r2 = sR[2 * LDR + c];
+          e0 = fma(lv, r0, e0); e1 = fma(lv, r1, e1); e2 = fma(lv, r2, e2);
+          f0 = fma(dl, r0, f0); f1 = fma(dl, r1, f1); f2 = fma(dl, r2, f2);
+          if (c + 1 < M0) {
+            const double lw = L[c + 1], dw = dL[c + 1], q0 = sR[c + 1], q1 = sR[LDR + c + 1], q2 = sR[2 * LDR + c + 1];
+            o0 = fma(lw, q0, o0); o1 = fma(lw, q1, o1); o2 = fma(lw, q2, o2);
+            g0 = fma(dw, q0, g0); g1 = fma(dw, q1, g1); g2 = fma(dw, q2, g2);
+          }
+        }
+        ev[0] = (float)(e0 + o0 - cq[0]); ev[1] = (float)(e1 + o1 - cq[1]); ev[2] = (float)(e2 + o2 - cq[2]);
+        od[0] = (float)(e0 - o0 - cq[3]); od[1] = (float)(e1 - o1 - cq[4]); od[2] = (float)(e2 - o2 - cq[5]);
+        dev[0] = (float)(f0 + g0); dev[1] = (float)(f1 + g1); dev[2] = (float)(f2 + g2);
+        dod[0] = (float)(g0 - f0); dod[1] = (float)(g1 - f1); dod[2] = (float)(g2 - f2);
+      } else {
+        const float* L = sTF + l * LDF;
+        const float* dL = sTF + (LH + l) * LDF;
+        const int c0 = sBo[k], c1 = sBo[k + 1];
+        float ge[6] = {}, go[6] = {};
+        int c = c0;
+        for (; c + 1 < c1; c += 2) {  // n - m = c - c0: even, then odd
+          const float l0 = L[c], d0 = dL[c], l1 = L[c + 1], d1 = dL[c + 1];
+          const float4 r = sR4[c], q = sR4[c + 1];
+          ge[0] = fmaf(l0, r.x, ge[0]); ge[1] = fmaf(l0, r.y, ge[1]); ge[2] = fmaf(l0, r.z, ge[2]);
+          ge[3] = fmaf(d0, r.x, ge[3]); ge[4] = fmaf(d0, r.y, ge[4]); ge[5] = fmaf(d0, r.z, ge[5]);
+          go[0] = fmaf(l1, q.x, go[0]); go[1] = fmaf(l1, q.y, go[1]); go[2] = fmaf(l1, q.z, go[2]);
+          go[3] = fmaf(d1, q.x, go[3]); go[4] = fmaf(d1, q.y, go[4]); go[5] = fmaf(d1, q.z, go[5]);
+        }
+        if (c < c1) {
+          const float l0 = L[c], d0 = dL[c];
+          const float4 r = sR4[c];
+          ge[0] = fmaf(l0, r.x, ge[0]); ge[1] = fmaf(l0, r.y, ge[1]); ge[2] = fmaf(l0, r.z, ge[2]);
+          ge[3] = fmaf(d0, r.x, ge[3]); ge[4] = fmaf(d0, r.y, ge[4]); ge[5] = fmaf(d0, r.z, ge[5]);
+        }
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          ev[d] = ge[d] + go[d];
+          od[d] = ge[d] - go[d];
+          dev[d] = ge[3 + d] + go[3 + d];
+          dod[d] = go[3 + d] - ge[3 + d];
+        }
+      }
+    };
+    // rows of latitude l (hemisphere 0: l + 32 d) and of its mirror (hemisphere 1: 32 - l +
+    // 32 d, or 96 + d for latitude 32)
+    auto row_of = [&](int lat, int d) { return lat < 32 ? lat + 32 * d : 96 + d; };
+    // Items (pair of blocks kp = (2 kp, 2 kp + 1) >= 1, latitude pair l): a warp holds 8
+    // latitude pairs x 4 block pairs, so each of its bf16x2 stores fills whole core matrices
+    // of the K-major operands (conflict-free); warps 0-7 take l < 16, warp 8 the equator.
+    // The pair of blocks 0 and 1 goes to warps 9 (block 0, FP64) and 10 (block 1), one lane
+    // per latitude pair with 16-bit stores, so that the FP64 sums run beside the others
+    // instead of after them (they were the pass's critical path).
+    static_assert(H::P1 == 32 && LH == 17 && F0 == 32 && NTHR >= 11 * 32, "latitude and block pairs");
     if (warp < 9) {
       const int l = warp < 8 ? 8 * (warp & 1) + (lane >> 2) : 16;
       const int kp = warp < 8 ? 4 * (warp >> 1) + (lane & 3) : lane;
-      if (warp < 8 || lane < 16) {
+      if (kp > 0 && (warp < 8 || lane < 16)) {
         const int lb = H::P1 - l;
         float ev[2][3], od[2][3], dev[2][3], dod[2][3];  // [block][coordinate]
-#pragma unroll
-        for (int b = 0; b < 2; b++) {
-          const int k = 2 * kp + b;
-          if (k == 0) {  // block m = 0 (n = c) in FP64, centred on the pole targets below
-            const double* L = sT0 + l * LD0;
-            const double* dL = sT0 + (LH + l) * LD0;
-            double e0 = 0, e1 = 0, e2 = 0, f0 = 0, f1 = 0, f2 = 0;  // n even
-            double o0 = 0, o1 = 0, o2 = 0, g0 = 0, g1 = 0, g2 = 0;  // n odd
-            for (int c = 0; c < M0; c += 2) {
-              const double lv = L[c], dl = dL[c], r0 = sR[c], r1 = sR[LDR + c], r2 = sR[2 * LDR + c];
-              e0 = fma(lv, r0, e0); e1 = fma(lv, r1, e1); e2 = fma(lv, r2, e2);
-              f0 = fma(dl, r0, f0); f1 = fma(dl, r1, f1); f2 = fma(dl, r2, f2);
-              if (c + 1 < M0) {
-                const double lw = L[c + 1], dw = dL[c + 1], q0 = sR[c + 1], q1 = sR[LDR + c + 1],
-                             q2 = sR[2 * LDR + c + 1];
-                o0 = fma(lw, q0, o0); o1 = fma(lw, q1, o1); o2 = fma(lw, q2, o2);
-                g0 = fma(dw, q0, g0); g1 = fma(dw, q1, g1); g2 = fma(dw, q2, g2);
-              }
-            }
-            // the centring by the pole targets is applied to each side in FP64
-            const int hl = 0, hb = 1;
-            const double c0 = cen[hl * 3] / mf00, c1 = cen[hl * 3 + 1] / mf00, c2 = cen[hl * 3 + 2] / mf00;
-            const double d0 = cen[hb * 3] / mf00, d1 = cen[hb * 3 + 1] / mf00, d2 = cen[hb * 3 + 2] / mf00;
-            // side values formed here: ev = value at l, od = value at lb (mirror)
-            ev[b][0] = (float)(e0 + o0 - c0); ev[b][1] = (float)(e1 + o1 - c1); ev[b][2] = (float)(e2 + o2 - c2);
-            od[b][0] = (float)(e0 - o0 - d0); od[b][1] = (float)(e1 - o1 - d1); od[b][2] = (float)(e2 - o2 - d2);
-            dev[b][0] = (float)(f0 + g0); dev[b][1] = (float)(f1 + g1); dev[b][2] = (float)(f2 + g2);
-            dod[b][0] = (float)(g0 - f0); dod[b][1] = (float)(g1 - f1); dod[b][2] = (float)(g2 - f2);
-          } else {
-            const float* L = sTF + l * LDF;
-            const float* dL = sTF + (LH + l) * LDF;
-            const int c0 = sBo[k], c1 = sBo[k + 1];
-            float ge[6] = {}, go[6] = {};
-            int c = c0;
-            for (; c + 1 < c1; c += 2) {  // n - m = c - c0: even, then odd
-              const float l0 = L[c], d0 = dL[c], l1 = L[c + 1], d1 = dL[c + 1];
-              const float4 r = sR4[c], q = sR4[c + 1];
-              ge[0] = fmaf(l0, r.x, ge[0]); ge[1] = fmaf(l0, r.y, ge[1]); ge[2] = fmaf(l0, r.z, ge[2]);
-              ge[3] = fmaf(d0, r.x, ge[3]); ge[4] = fmaf(d0, r.y, ge[4]); ge[5] = fmaf(d0, r.z, ge[5]);
-              go[0] = fmaf(l1, q.x, go[0]); go[1] = fmaf(l1, q.y, go[1]); go[2] = fmaf(l1, q.z, go[2]);
-              go[3] = fmaf(d1, q.x, go[3]); go[4] = fmaf(d1, q.y, go[4]); go[5] = fmaf(d1, q.z, go[5]);
-            }
-            if (c < c1) {
-              const float l0 = L[c], d0 = dL[c];
-              const float4 r = sR4[c];
-              ge[0] = fmaf(l0, r.x, ge[0]); ge[1] = fmaf(l0, r.y, ge[1]); ge[2] = fmaf(l0, r.z, ge[2]);
-              ge[3] = fmaf(d0, r.x, ge[3]); ge[4] = fmaf(d0, r.y, ge[4]); ge[5] = fmaf(d0, r.z, ge[5]);
-            }
-#pragma unroll
-            for (int d = 0; d < 3; d++) {
-              ev[b][d] = ge[d] + go[d];
-              od[b][d] = ge[d] - go[d];
-              dev[b][d] = ge[3 + d] + go[3 + d];
-              dod[b][d] = go[3 + d] - ge[3 + d];
-            }
-          }
-        }
-        // latitude l (hemisphere 0; rows l + 32 d), then its mirror (hemisphere 1: rows
-        // 32 - l + 32 d, or 96 + d for latitude 32) unless l is the equator
+        block_sums(2 * kp, l, ev[0], od[0], dev[0], dod[0]);
+        block_sums(2 * kp + 1, l, ev[1], od[1], dev[1], dod[1]);
 #pragma unroll
         for (int d = 0; d < 3; d++) {
-          const uint32_t o = tc::umma_off(l + 32 * d, 2 * kp, F0);
+          const uint32_t o = tc::umma_off(row_of(l, d), 2 * kp, F0);
           tc::store_split3x2(sA, H::SZ_A, o, ev[0][d], ev[1][d]);
           tc::store_split3x2(sdA, H::SZ_A, o, dev[0][d], dev[1][d]);
         }
         if (l < 16) {
 #pragma unroll
           for (int d = 0; d < 3; d++) {
-            const uint32_t o = tc::umma_off(lb < 32 ? lb + 32 * d : 96 + d, 2 * kp, F0);
+            const uint32_t o = tc::umma_off(row_of(lb, d), 2 * kp, F0);
             tc::store_split3x2(sA, H::SZ_A, o, od[0][d], od[1][d]);
             tc::store_split3x2(sdA, H::SZ_A, o, dod[0][d], dod[1][d]);
           }
+        }
+      }
+    } else if (warp < 11 && lane < LH) {
+      const int k = warp - 9, l = lane, lb = H::P1 - l;
+      float ev[3], od[3], dev[3], dod[3];
+      block_sums(k, l, ev, od, dev, dod);
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        tc::store_split3(sA, H::SZ_A, tc::umma_off(row_of(l, d), k, F0), ev[d]);
+        tc::store_split3(sdA, H::SZ_A, tc::umma_off(row_of(l, d), k, F0), dev[d]);
+        if (l < 16) {
+          tc::store_split3(sA, H::SZ_A, tc::umma_off(row_of(lb, d), k, F0), od[d]);
+          tc::store_split3(sdA, H::SZ_A, tc::umma_off(row_of(lb, d), k, F0), dod[d]);
         }
       }
     }
