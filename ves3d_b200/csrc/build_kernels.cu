@@ -578,10 +578,10 @@ struct RingTcCfg {
   static constexpr int OFF_MFT = al16(OFF_R4 + NC * 16);              // Mf^T [N1][F0] FP32 (the last latitude's DFT)
   static constexpr int OFF_C32 = al16(OFF_MFT + N1 * F0 * 4);         // row 32 of C [F0][12], outside U
   static constexpr int OFF_TRG = al16(OFF_C32 + F0 * 12 * 4);
-  static constexpr int OFF_CEN = OFF_TRG + 6 * 8;
-  static constexpr int OFF_CQ = OFF_CEN + 6 * 8;  // the centres over the m = 0 Fourier row
-  static constexpr int OFF_SW = OFF_CQ + 6 * 8;
-  static constexpr int OFF_BO = OFF_SW + L1 * 8;
+  static constexpr int OFF_CQ = OFF_TRG + 6 * 8;  // the pole targets over the m = 0 Fourier row
+  static constexpr int OFF_DF = OFF_CQ + 6 * 8;   // target t - centre h as FP32 pairs: hi [2][2][3], lo [2][2][3]
+  static constexpr int OFF_SWF = OFF_DF + 24 * 4;  // singular weights x 1/(8 pi), FP32
+  static constexpr int OFF_BO = OFF_SWF + (L1 * 4 + 7) / 8 * 8;
   static constexpr int OFF_JF = OFF_BO + ((F0 + 1) * 4 + 7) / 8 * 8;   // Fourier block of each coefficient
   static constexpr int OFF_BAR = OFF_JF + (NC + 7) / 8 * 8;
   static_assert(OFF_U % 16 == 0 && OFF_XS % 16 == 0 && OFF_R % 16 == 0 && OFF_T0 % 16 == 0 && OFF_TF % 16 == 0 && OFF_X32 % 16 == 0 &&
@@ -623,6 +623,40 @@ __device__ __forceinline__ double area_of(double ax, double ay, double az, doubl
   return n2 * rsqrt_f64_int_seed(n2);  // |X_theta x X_phi| > 0 on the upsampled grid
 }
 
+// 1/sqrt(x) in FP32: the hardware estimate and one Newton step (about one ulp).
+__device__ __forceinline__ float rsqrt_f32_nr(float x) {
+  const float y = rsqrt_ftz(x);
+  const float e = fmaf(-x * y, y, 1.f);
+  return fmaf(0.5f * y, e, y);
+}
+
+// FP32 forms of the two above for the tensor-core build, whose surface values are FP32
+// and whose kernel values are rounded to FP32 for the split. The offset of the pole target
+// t from the point's hemisphere centre h arrives as an FP32 pair (hi + lo: the FP64
+// difference to FP32 rounding); it is 0 for t == h, so the near-pole differences, where
+// the kernel is large, are exact, and for t != h the point is a vesicle size away. w holds
+// the latitude's singular weight times 1/(8 pi).
+__device__ __forceinline__ float area_of_f32(float ax, float ay, float az, float bx, float by, float bz) {
+  const float nx = fmaf(ay, bz, -az * by), ny = fmaf(az, bx, -ax * bz), nz = fmaf(ax, by, -ay * bx);
+  const float n2 = fmaf(nx, nx, fmaf(ny, ny, nz * nz));
+  return n2 * rsqrt_f32_nr(n2);
+}
+
+__device__ __forceinline__ void ring_kernel_sl_f32(float px, float py, float pz, float area, const float* dhi,
+                                                   const float* dlo, float w, float* out) {
+  const float dx = (dhi[0] - px) + dlo[0], dy = (dhi[1] - py) + dlo[1], dz = (dhi[2] - pz) + dlo[2];
+  const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  const float rinv = r2 > 2.220446049250313e-16f ? rsqrt_f32_nr(r2) : 0.f;
+  const float a1 = w * area * rinv;
+  const float a2 = a1 * rinv * rinv;
+  out[0] = fmaf(dx * dx, a2, a1);
+  out[1] = dx * dy * a2;
+  out[2] = dx * dz * a2;
+  out[3] = fmaf(dy * dy, a2, a1);
+  out[4] = dy * dz * a2;
+  out[5] = fmaf(dz * dz, a2, a1);
+}
+
 template <int P0>
 __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restrict__ R, DevTables T,
                                                           float* __restrict__ C, long nrot) {
@@ -645,9 +679,9 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
   float* sMfT = reinterpret_cast<float*>(smem + H::OFF_MFT);
   float* sC32 = reinterpret_cast<float*>(smem + H::OFF_C32);
   double* trg = reinterpret_cast<double*>(smem + H::OFF_TRG);
-  double* cen = reinterpret_cast<double*>(smem + H::OFF_CEN);
   double* cq = reinterpret_cast<double*>(smem + H::OFF_CQ);
-  double* sSw = reinterpret_cast<double*>(smem + H::OFF_SW);
+  float* sSwf = reinterpret_cast<float*>(smem + H::OFF_SWF);
+  float* sDf = reinterpret_cast<float*>(smem + H::OFF_DF);  // hi at [(h * 2 + t) * 3 + d], lo 12 on
   int* sBo = reinterpret_cast<int*>(smem + H::OFF_BO);
   unsigned char* sJf = smem + H::OFF_JF;
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + H::OFF_BAR);
@@ -697,7 +731,7 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
     const int tb = i / (LH * LDF), r = i - tb * LH * LDF, lat = r / LDF, c = r - lat * LDF;
     sTF[i] = c < NC ? (float)__ldg((tb ? T.syn1_dleg_t : T.syn1_leg_t) + (long)lat * NC + c) : 0.f;
   }
-  for (int i = tid; i < L1; i += NTHR) sSw[i] = __ldg(T.sing_w + i);
+  for (int i = tid; i < L1; i += NTHR) sSwf[i] = (float)(kInv8Pi * __ldg(T.sing_w + i));
   for (int i = tid; i <= F0; i += NTHR) sBo[i] = __ldg(T.blk_off + i);
   for (int i = tid; i < NC; i += NTHR) sJf[i] = (unsigned char)__ldg(T.jf_of_coef + i);
   tc::fence_async_smem();
@@ -755,10 +789,14 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
       trg[c * 2 + t] = s;
     }
     __syncthreads();
-    if (tid < 6) {  // cen[h * 3 + d]: target of hemisphere h; cq the same over the m = 0 row
-      const double c = trg[(tid % 3) * 2 + tid / 3];
-      cen[tid] = c;
-      cq[tid] = c / mf00;
+    if (tid < 6) {  // cq[h * 3 + d]: the target of hemisphere h (its centre) over the m = 0 row
+      cq[tid] = trg[(tid % 3) * 2 + tid / 3] / mf00;
+    } else if (tid >= 32 && tid < 44) {  // target t - centre h (the target of hemisphere h) as FP32 pairs
+      const int i = tid - 32, h = i / 6, t = (i / 3) & 1, d = i % 3;
+      const double dd = trg[d * 2 + t] - trg[d * 2 + h];
+      const float hi = (float)dd;
+      sDf[i] = hi;
+      sDf[12 + i] = (float)(dd - (double)hi);
     }
     for (int c = tid; c < NC; c += NTHR) sR4[c] = make_float4((float)sR[c], (float)sR[LDR + c], (float)sR[2 * LDR + c], 0.f);
     __syncthreads();
@@ -924,16 +962,13 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
         const int h = 2 * lat > H::P1 ? 1 : 0;
         const float* xs = sXs + lat * H::SXS_LD + jj;
         constexpr int VS = 32 * H::SXS_LD;
-        const double area = area_of(xs[3 * VS], xs[4 * VS], xs[5 * VS], xs[6 * VS], xs[7 * VS], xs[8 * VS]);
-        const double px = xs[0], py = xs[VS], pz = xs[2 * VS];
+        const float area = area_of_f32(xs[3 * VS], xs[4 * VS], xs[5 * VS], xs[6 * VS], xs[7 * VS], xs[8 * VS]);
+        const float px = xs[0], py = xs[VS], pz = xs[2 * VS];
         float kv[12];
 #pragma unroll
-        for (int t = 0; t < 2; t++) {
-          double k6[6];
-          ring_kernel_sl(px, py, pz, area, trg, cen, h, t, sSw[t ? lat : H::P1 - lat], k6);
-#pragma unroll
-          for (int c = 0; c < 6; c++) kv[t * 6 + c] = (float)k6[c];
-        }
+        for (int t = 0; t < 2; t++)
+          ring_kernel_sl_f32(px, py, pz, area, sDf + (h * 2 + t) * 3, sDf + 12 + (h * 2 + t) * 3,
+                             sSwf[t ? lat : H::P1 - lat], kv + t * 6);
         // lanes 2i, 2i + 1 hold longitudes jj, jj + 1 of one latitude: the even lane splits
         // components 0..5 of both, the odd lane 6..11, as BF16 pairs (one 32-bit word per
         // split and component)
@@ -975,11 +1010,12 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
     if (warp >= 12) {
       const int item = tid - 384, j = item >> 1, t = item & 1;
       const float* xs = sX32 + j;
-      const double area = area_of(xs[3 * N1], xs[4 * N1], xs[5 * N1], xs[6 * N1], xs[7 * N1], xs[8 * N1]);
-      double kv[6];
-      ring_kernel_sl(xs[0], xs[N1], xs[2 * N1], area, trg, cen, 1, t, sSw[t ? 32 : H::P1 - 32], kv);
+      const float area = area_of_f32(xs[3 * N1], xs[4 * N1], xs[5 * N1], xs[6 * N1], xs[7 * N1], xs[8 * N1]);
+      float kv[6];
+      ring_kernel_sl_f32(xs[0], xs[N1], xs[2 * N1], area, sDf + (2 + t) * 3, sDf + 12 + (2 + t) * 3,
+                         sSwf[t ? 32 : H::P1 - 32], kv);
 #pragma unroll
-      for (int c = 0; c < 6; c++) sK32[(t * 6 + c) * N1 + j] = (float)kv[c];
+      for (int c = 0; c < 6; c++) sK32[(t * 6 + c) * N1 + j] = kv[c];
     }
     __syncthreads();
     // FP32 like the BF16-split GEMM of the other rows (the same FP32 values of Mf): a warp

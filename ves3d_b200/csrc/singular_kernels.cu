@@ -341,17 +341,18 @@ __global__ void __launch_bounds__(256) k_rotate_transpose_scatter(const double* 
 // self-matrix grid SL3 (FP32: the Grid2SHC that follows reads it into FP64), laid out as the
 // FP64 forms'. Compared with the DMMA form on FP64 C it moves half the bytes and keeps no
 // per-degree barriers.
-template <int CB>
-__global__ void __launch_bounds__(256, 3) k_rotate_transpose_f32(const float* __restrict__ C, int p0, int mr_per_t,
+template <int P, int CB>
+__global__ void __launch_bounds__(256, 3) k_rotate_transpose_f32(const float* __restrict__ C, int mr_per_t,
                                                               DevTables T, float* __restrict__ SL3) {
   extern __shared__ __align__(16) float smf[];
-  const int nc = p0 * (p0 + 2), ng = 2 * p0 * (p0 + 1);
-  const int lda = nc + 1;  // odd row stride
-  const int rows = CB * p0;
+  // compile-time order: every index division below becomes a multiply and shift
+  constexpr int p0 = P, nc = P * (P + 2), ng = 2 * P * (P + 1);
+  constexpr int lda = nc + 1;  // odd row stride
+  constexpr int rows = CB * P;
   float* sA = smf;                         // [rows][lda], degree-major
   float* sB = sA + rows * lda;             // [rows][lda], coefficient order
   float* sM = sB + rows * lda;             // blocks of degree n at sMo[n], rows of bn | 1
-  const int msz = mr_per_t + (p0 + 1) * 2 * p0;  // (upper bound of the padded size)
+  const int msz = mr_per_t + (P + 1) * 2 * P;  // (upper bound of the padded size)
   float* sCs = sM + msz;                   // cos_tab [2 p0]
   float* sSn = sCs + 2 * p0;               // sin_tab [2 p0]
   int* sMo = reinterpret_cast<int*>(sSn + 2 * p0);           // [p0 + 2] padded block offsets
@@ -425,7 +426,7 @@ __global__ void __launch_bounds__(256, 3) k_rotate_transpose_f32(const float* __
       __syncthreads();
       // rotation back: thread (degree-major position d, 4 rows), so that a warp's lanes
       // share a degree (the same loop length, broadcast inputs, consecutive block rows)
-      const int nrq = (rows + 3) / 4;
+      constexpr int nrq = (rows + 3) / 4;
       for (int i = tid; i < nrq * nc; i += 256) {
         const int d = i % nc, rq = i / nc;
         const int n = sN[d], c = sP[d];
@@ -479,12 +480,17 @@ static size_t rt_f32_smem(int p0, int cb, int mpt) {
 int launch_rotate_transpose_f32(const float* C, long nv, const DevTables& T, float* SL3, cudaStream_t st) {
   if (nv <= 0) return VES3D_OK;
   const int p0 = T.p0, mpt = mr_per_t(T);
+  // the FP32 results come from the tensor-core build, which is laid out for p = 16 only
+  if (p0 != 16) {
+    set_error("internal: FP32 rotate-transpose at p = %d (built for p = 16)", p0);
+    return VES3D_ERR_ARG;
+  }
   dim3 grid(p0 + 1, (unsigned)nv);
   // one component per group: 68 KB of shared memory at p = 16, three CTAs per SM (two
   // components per group, two CTAs: 9.1 ms at 512 vesicles)
   const size_t smem = rt_f32_smem(p0, 1, mpt);
-  VES3D_CK(cudaFuncSetAttribute(k_rotate_transpose_f32<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_rotate_transpose_f32<1><<<grid, 256, smem, st>>>(C, p0, mpt, T, SL3);
+  VES3D_CK(cudaFuncSetAttribute(k_rotate_transpose_f32<16, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_rotate_transpose_f32<16, 1><<<grid, 256, smem, st>>>(C, mpt, T, SL3);
   VES3D_LAUNCHED();
   return VES3D_OK;
 }
