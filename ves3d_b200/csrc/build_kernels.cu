@@ -486,6 +486,30 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
+// The same for three column ranges, one wait for the three loads.
+__device__ __forceinline__ void tmem_ld16x3(uint32_t ta, uint32_t tb, uint32_t tc_, float* a, float* b, float* c) {
+  uint32_t r[48];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%48];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%49];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47}, [%50];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]),
+        "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]),
+        "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47])
+      : "r"(ta), "r"(tb), "r"(tc_)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 16; i++) {
+    a[i] = __uint_as_float(r[i]);
+    b[i] = __uint_as_float(r[16 + i]);
+    c[i] = __uint_as_float(r[32 + i]);
+  }
+}
+
 // Byte offset of element (row, k) of a K-major no-swizzle operand with kcols columns
 // (core matrices K-adjacent at 128 B, 8-row groups at kcols * 16 B).
 __host__ __device__ constexpr uint32_t umma_off(int row, int k, int kcols) {
@@ -591,8 +615,10 @@ struct RingTcCfg {
   static constexpr int OFF_TMEM = OFF_BAR + NBAR * 8;
   static constexpr int SMEM = OFF_TMEM + 16;
   static constexpr uint32_t TMEM_COLS = 512;
+  // GEMM 2 accumulates per M tile and per split j of Mf: columns COL_T + (tile * 3 + j) * F0
   static constexpr int COL_X = 0, COL_XT = N1, COL_XP = 2 * N1, COL_T = 3 * N1;
-  static_assert(COL_T + 3 * F0 <= (int)TMEM_COLS, "TMEM columns");
+  static_assert(COL_T + 9 * F0 <= (int)TMEM_COLS, "TMEM columns");
+  static_assert(SZ_BT == (F0 / 8) * (N1 * 16), "the three Mf splits continue one K-major operand of N = 3 F0");
   static_assert(SMEM <= 227 * 1024, "shared memory");
 };
 
@@ -989,15 +1015,18 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
       // next chunk's TMEM reads meanwhile
       if (tid == 12 * 32) {
         tc::tc_after_sync();
-        constexpr uint32_t id32 = tc::idesc_bf16(128, F0);
+        // split i of the kernel values against the Mf splits j <= 2 - i stacked along N (the
+        // three split buffers continue one operand): one MMA of N = (3 - i) F0 per M tile puts
+        // K_i Mf_j^T into column block j; nine MMAs per chunk instead of eighteen of N = F0.
+        // Split 0 comes first: it writes all three blocks (the first chunk's initial values).
         const uint64_t dBc = tc::desc_at(dBT, ch * (H::JC / 8) * 128), dKc = kb ? dK1 : dK0;
 #pragma unroll
-        for (int pr = 0; pr < 6; pr++) {
-          const uint64_t db = tc::desc_at(dBc, tc::split_j(pr) * H::SZ_BT);
+        for (int i = 0; i < 3; i++) {
+          const uint32_t idn = tc::idesc_bf16(128, (3 - i) * F0);
 #pragma unroll
           for (int tt = 0; tt < 3; tt++)
-            tc::mma_bf16(tmem + H::COL_T + tt * F0, tc::desc_at(dKc, tc::split_i(pr) * H::SZ_K + tt * 128 * H::JC * 2),
-                         db, id32, (ch | pr) ? 1u : 0u);
+            tc::mma_bf16(tmem + H::COL_T + tt * 3 * F0, tc::desc_at(dKc, i * H::SZ_K + tt * 128 * H::JC * 2), dBc, idn,
+                         (ch | i) ? 1u : 0u);
         }
         tc::mma_commit(bar_k + kb);
       }
@@ -1044,13 +1073,14 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
     if (warp < 12) {
       const int q = warp & 3, tt = warp >> 2;
       const int comp = 4 * tt + q, lat = lane;  // row comp * 32 + lat of tile tt
-      float v[16];
+      float v[16], w1[16], w2[16];
 #pragma unroll
-      for (int half = 0; half < 2; half++) {
-        tc::tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + H::COL_T + tt * F0 + half * 16, v);
+      for (int half = 0; half < 2; half++) {  // the split blocks summed smallest first
+        const uint32_t ta = tmem + ((uint32_t)(32 * q) << 16) + H::COL_T + tt * 3 * F0 + half * 16;
+        tc::tmem_ld16x3(ta, ta + F0, ta + 2 * F0, v, w1, w2);
         float* o = sC + lat * LDCL + half * 16 * 12 + comp;
 #pragma unroll
-        for (int x = 0; x < 16; x++) o[x * 12] = v[x];
+        for (int x = 0; x < 16; x++) o[x * 12] = v[x] + (w1[x] + w2[x]);
       }
     }
     tc::tc_before_sync();
