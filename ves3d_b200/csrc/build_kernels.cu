@@ -443,6 +443,17 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                : "memory");
 }
 
+// 1-D bulk copy shared -> global through the TMA engine (bulk-group completion, tracked
+// per issuing thread; addresses 16-byte aligned, size a multiple of 16).
+__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(saddr(src)), "r"(bytes)
+               : "memory");
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+// this thread's bulk stores have read their shared-memory sources / are complete
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void tc_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -588,6 +599,12 @@ struct RingTcCfg {
   static constexpr int OFF_K = OFF_U;
   static constexpr int OFF_XS = OFF_K + 6 * SZ_K;
   static constexpr int U_SZ = std::max(std::max(6 * SZ_A, 6 * SZ_K + SZ_XS), SZ_C);
+  // a rotation's output C [12][NC] FP32, staged in U by pass 2 beside the C tile and above
+  // A/dA, stored by a bulk copy during the next rotation's pass 1 (before the chunk buffers
+  // reuse it)
+  static constexpr int SZ_CST = 12 * NC * 4;
+  static constexpr int OFF_CST = OFF_U + (std::max(SZ_C, 6 * SZ_A) + 15) / 16 * 16;
+  static_assert(OFF_CST + SZ_CST <= OFF_U + U_SZ && SZ_CST % 16 == 0, "output staging inside U");
   // every region starts on a 16-byte boundary (float4 and bulk-copy destinations need it)
   static constexpr int al16(int x) { return (x + 15) / 16 * 16; }
   static constexpr int OFF_R = (OFF_U + U_SZ + 127) / 128 * 128;      // 2 x [3][LDR] FP64
@@ -794,38 +811,44 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
     __syncthreads();
     return *s_abort == 0;
   };
+  // Per-rotation values from R, formed by the 224 threads i = 0..223 of seven whole warps
+  // (named barrier 1) before the rotation begins: the pole targets (trg), their values over
+  // the m = 0 Fourier row (cq), target t - centre h as FP32 pairs (sDf), R as float4 (sR4).
+  // Inside the loop the warps idle in pass 2 (threads NC..511) form the next rotation's.
+  static_assert(NTHR - NC == 224 && NC >= 224, "seven warps idle in pass 2");
+  auto prep = [&](const double* sRn, int i) {
+    for (int c = i; c < NC; c += 224) sR4[c] = make_float4((float)sRn[c], (float)sRn[LDR + c], (float)sRn[2 * LDR + c], 0.f);
+    if (i < 6) {
+      const int c = i >> 1, t = i & 1;
+      double s = 0.0;
+      for (int n = 0; n <= P0; n++) s += sRn[c * LDR + n] * __ldg(T.qp + t * (P0 + 1) + n);
+      trg[c * 2 + t] = s;
+    }
+    asm volatile("bar.sync 1, 224;" ::: "memory");
+    if (i < 6) {  // cq[h * 3 + d]: the target of hemisphere h (its centre) over the m = 0 row
+      cq[i] = trg[(i % 3) * 2 + i / 3] / mf00;
+    } else if (i < 18) {  // target t - centre h (the target of hemisphere h) as FP32 pairs
+      const int j = i - 6, h = j / 6, t = (j / 3) & 1, d = j % 3;
+      const double dd = trg[d * 2 + t] - trg[d * 2 + h];
+      const float hi = (float)dd;
+      sDf[j] = hi;
+      sDf[12 + j] = (float)(dd - (double)hi);
+    }
+  };
   if (blockIdx.x < nrot) {
     if (tid == 0) issue_r(blockIdx.x, 0);
     i_r[0]++;
+    wait(bar_r, n_r[0]);
+    if (tid < 224) prep(sRb, tid);
+    ok = sync_ok();
   }
-  long it = 0;
+  float* sCst = reinterpret_cast<float*>(smem + H::OFF_CST);
+  constexpr int kIssuer = 12 * 32;  // a thread of a warp idle in pass 1: bulk copies in and out
+  long it = 0, staged = -1;         // staged: the rotation whose C waits in sCst
   for (long rot = blockIdx.x; rot < nrot && ok; rot += gridDim.x, it++) {
     const int rb = (int)(it & 1);
     const double* sR = sRb + rb * 3 * LDR;
-    wait(bar_r + rb, n_r[rb]);
-    if (rot + gridDim.x < nrot) {
-      if (tid == 0) issue_r(rot + gridDim.x, rb ^ 1);
-      i_r[rb ^ 1]++;
-    }
-    if (!(ok = sync_ok())) break;
-    if (tid < 6) {
-      const int c = tid >> 1, t = tid & 1;
-      double s = 0.0;
-      for (int n = 0; n <= P0; n++) s += sR[c * LDR + n] * __ldg(T.qp + t * (P0 + 1) + n);
-      trg[c * 2 + t] = s;
-    }
-    __syncthreads();
-    if (tid < 6) {  // cq[h * 3 + d]: the target of hemisphere h (its centre) over the m = 0 row
-      cq[tid] = trg[(tid % 3) * 2 + tid / 3] / mf00;
-    } else if (tid >= 32 && tid < 44) {  // target t - centre h (the target of hemisphere h) as FP32 pairs
-      const int i = tid - 32, h = i / 6, t = (i / 3) & 1, d = i % 3;
-      const double dd = trg[d * 2 + t] - trg[d * 2 + h];
-      const float hi = (float)dd;
-      sDf[i] = hi;
-      sDf[12 + i] = (float)(dd - (double)hi);
-    }
-    for (int c = tid; c < NC; c += NTHR) sR4[c] = make_float4((float)sR[c], (float)sR[LDR + c], (float)sR[2 * LDR + c], 0.f);
-    __syncthreads();
+    const bool has_next = rot + gridDim.x < nrot;
     // ---- pass 1: Legendre synthesis -> split BF16 A, dA -----------------------------------
     // the m = 0 block in FP64 (it carries the vesicle's position, shifted by the pole target
     // here), the others in FP32 (shape-sized terms; their sums are rounded to FP32 for the
@@ -918,6 +941,11 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
           }
         }
       }
+    } else if (tid == kIssuer) {
+      // the previous rotation's C out, the next rotation's R in (buffer rb ^ 1 held the R of
+      // rotation it - 1, whose readers are done)
+      if (staged >= 0) tc::bulk_s2g(C + staged * G::NOUT, sCst, H::SZ_CST);
+      if (has_next) issue_r(rot + gridDim.x, rb ^ 1);
     } else if (warp < 11 && lane < LH) {
       const int k = warp - 9, l = lane, lb = H::P1 - l;
       float ev[3], od[3], dev[3], dod[3];
@@ -932,6 +960,9 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
         }
       }
     }
+    if (has_next) i_r[rb ^ 1]++;
+    if (tid == kIssuer && staged >= 0) tc::bulk_wait_read();  // sCst free for the chunk buffers
+    staged = -1;
     // ---- GEMM 1 on the tensor cores ------------------------------------------------------
     tc::fence_async_smem();
     __syncthreads();
@@ -1102,7 +1133,15 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
       }
     }
     __syncthreads();
-    if (tid < NC) {
+    if (has_next) {  // the next rotation's R (issued during pass 1)
+      if (tid >= NC)
+        wait(bar_r + (rb ^ 1), n_r[rb ^ 1]);
+      else
+        n_r[rb ^ 1]++;
+    }
+    if (tid >= NC) {
+      if (has_next) prep(sRb + (rb ^ 1) * 3 * LDR, tid - NC);
+    } else {
       const int c = tid, jf = sJf[c];
       const bool odd = (c - sBo[jf]) & 1;  // parity of n + m
       const float4* a = reinterpret_cast<const float4*>(sC + jf * 12);
@@ -1124,9 +1163,16 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
         acc[10] = fmaf(a2.z, w, acc[10]); acc[11] = fmaf(a2.w, w, acc[11]);
       }
 #pragma unroll
-      for (int q = 0; q < 12; q++) C[rot * G::NOUT + q * NC + c] = acc[q];
+      for (int q = 0; q < 12; q++) sCst[q * NC + c] = acc[q];  // conflict-free: consecutive c
     }
-    __syncthreads();  // pass 2's reads of C before the next rotation's pass 1 overwrites it
+    staged = rot;
+    tc::fence_async_smem();  // the staged C is read by the bulk copy (async proxy)
+    // pass 2's reads of C before the next rotation's pass 1 overwrites it
+    if (!(ok = sync_ok())) break;
+  }
+  if (tid == kIssuer) {  // the last rotation's C, then every bulk store complete
+    if (ok && staged >= 0) tc::bulk_s2g(C + staged * G::NOUT, sCst, H::SZ_CST);
+    tc::bulk_wait_all();
   }
   // ---- drain: copies and MMAs issued but not waited for (after an abort, whatever was in
   // flight), each wait bounded; then TMEM is freed -------------------------------------
@@ -1159,6 +1205,10 @@ int launch_build_ring_tc(const double* R, long nrot, const DevTables& T, float* 
   if (nrot <= 0) return VES3D_OK;
   if (!tc_build_supported(T.p0, T.p1)) {
     set_error("tensor-core build not laid out for p = %d, p_up = %d", T.p0, T.p1);
+    return VES3D_ERR_ARG;
+  }
+  if (((uintptr_t)R | (uintptr_t)C) & 15) {  // the bulk copies in and out need 16-byte alignment
+    set_error("internal: tensor-core build buffers not 16-byte aligned");
     return VES3D_ERR_ARG;
   }
   using H = RingTcCfg<16>;
