@@ -578,6 +578,14 @@ struct RingTcCfg {
   static constexpr int JC = 16;          // longitudes per kernel chunk (K of one GEMM-2 step)
   static constexpr int NCH = N1 / JC;    // chunks per rotation
   static constexpr int KROWS = 12 * 32;  // GEMM-2 rows (component, latitude < 32): 3 M-tiles
+  // Row of (component, latitude) in the GEMM-2 operand, hence TMEM lane of its result: tile
+  // comp / 4; lane quarter lat / 8; within the quarter, lane bits (lat & 3, comp bit 1) low and
+  // (lat bit 2, comp bit 0) high. A quarter then holds 8 latitudes x 4 components, whose FP32
+  // stores into C (latitude stride LDCL = 4 mod 32 words) fall on 32 distinct banks; the
+  // chunk operand's stores stay two-way.
+  __host__ __device__ static constexpr int krow(int comp, int lat) {
+    return (comp >> 2) * 128 + (lat >> 3) * 32 + (((lat >> 2) & 1) * 2 + (comp & 1)) * 8 + (lat & 3) * 2 + ((comp >> 1) & 1);
+  }
   static_assert(32 * JC == NTHR, "one chunk point per thread");
   // operand sizes (bytes, one split)
   static constexpr int SZ_A = 128 * F0 * 2;       // A or dA: 128 rows x K = F0
@@ -1037,7 +1045,7 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
           const float recv = __shfl_xor_sync(0xffffffffu, send, 1);
           const float lo = odd ? recv : kv[c], hi = odd ? kv[6 + c] : recv;
           const int comp = odd ? 6 + c : c;
-          tc::store_split3x2(sKb, H::SZ_K, off + tc::umma_off(comp * 32 + lat, 0, H::JC), lo, hi);
+          tc::store_split3x2(sKb, H::SZ_K, off + tc::umma_off(H::krow(comp, lat), 0, H::JC), lo, hi);
         }
       }
       tc::fence_async_smem();
@@ -1064,11 +1072,12 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
       i_k[kb]++;
     }
     if (!ok) break;
-    // ---- the last latitude's kernel (warps 12-15, one (point, target) each) and its
-    // transposed DFT (its row of C, into a buffer outside U) while the last GEMMs 2 run;
+    // ---- the last latitude's kernel (warps 8-11, one (point, target) each) and its
+    // transposed DFT (its row of C, into a buffer outside U) by warps 0-11 while warp 12
+    // issues the last GEMM 2 and the GEMMs run (named barrier 2: warp 12 is not waited for);
     // then the transposed-DFT result -> shared (FP32) ----------------------------------
-    if (warp >= 12) {
-      const int item = tid - 384, j = item >> 1, t = item & 1;
+    if (warp >= 8 && warp < 12) {
+      const int item = tid - 256, j = item >> 1, t = item & 1;
       const float* xs = sX32 + j;
       const float area = area_of_f32(xs[3 * N1], xs[4 * N1], xs[5 * N1], xs[6 * N1], xs[7 * N1], xs[8 * N1]);
       float kv[6];
@@ -1077,7 +1086,8 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
 #pragma unroll
       for (int c = 0; c < 6; c++) sK32[(t * 6 + c) * N1 + j] = kv[c];
     }
-    __syncthreads();
+    static_assert(12 * F0 == 384 && 2 * N1 == 128, "warps 0-11: the DFT; warps 8-11: the 128 kernel items");
+    if (warp < 12) asm volatile("bar.sync 2, 384;" ::: "memory");
     // FP32 like the BF16-split GEMM of the other rows (the same FP32 values of Mf): a warp
     // takes one component, its lanes the 32 Fourier columns (broadcast kernel values,
     // conflict-free Mf^T rows). It read Mf from global memory in FP64 before, 32 cache lines
@@ -1103,7 +1113,9 @@ __global__ void __launch_bounds__(512, 1) k_build_ring_tc(const double* __restri
     tc::tc_after_sync();
     if (warp < 12) {
       const int q = warp & 3, tt = warp >> 2;
-      const int comp = 4 * tt + q, lat = lane;  // row comp * 32 + lat of tile tt
+      // TMEM lane 32 q + lane of tile tt holds row krow(comp, lat)
+      const int lat = 8 * q + ((lane >> 4) & 1) * 4 + ((lane >> 1) & 3);
+      const int comp = 4 * tt + (((lane & 1) << 1) | ((lane >> 3) & 1));
       float v[16], w1[16], w2[16];
 #pragma unroll
       for (int half = 0; half < 2; half++) {  // the split blocks summed smallest first
