@@ -331,150 +331,151 @@ __global__ void __launch_bounds__(256) k_rotate_transpose_scatter(const double* 
 }
 
 // Mixed form of the rotate-transpose (after the tensor-core build, whose transposed-DFT
-// results C are FP32): one CTA per (latitude rotation t, vesicle v), rows (component,
-// longitude j) in groups of CB components. Per degree n the rotation back
+// results C are FP32): one CTA per (latitude rotation t, vesicle v); for each pole and
+// symmetric component the P longitude rows of C are staged in degree-major order, then
+// each thread takes one item (degree n, order m): the coefficient of cos(m phi) and its
+// sin(m phi) partner (one coefficient for m = 0 and m = P), and forms for all P rows the
+// rotation back
 //     B[row][po + b] = sum_k A[row][po + k] Mr_{t,n}[b][k]
-// runs in FP32 on the CUDA cores (the values carry FP32 precision already; the FP64 form
-// uses the DMMA kernel below), reading the degree-major staged inputs and the rotation
-// blocks of this t held in shared memory with an odd row stride (bn | 1: consecutive b of a
-// warp fall on distinct banks); then the inverse longitude phase and the scatter into the
-// self-matrix grid SL3 (FP32: the Grid2SHC that follows reads it into FP64), laid out as the
-// FP64 forms'. Compared with the DMMA form on FP64 C it moves half the bytes and keeps no
-// per-degree barriers.
-template <int P, int CB>
-__global__ void __launch_bounds__(256, 3) k_rotate_transpose_f32(const float* __restrict__ C, int mr_per_t,
+// at its two positions b in FP32 (the values carry FP32 precision already; the FP64 form
+// uses the DMMA kernel below), then the inverse longitude phase of the pair in registers
+// and the P consecutive grid values of each coefficient as float4 stores into the
+// self-matrix grid SL3 (FP32: the Grid2SHC that follows reads it into FP64), laid out as
+// the FP64 forms'. A thread's rows share the staged inputs (broadcast to the lanes of its
+// degree) and its two rotation rows: 18 shared loads per 32 FMAs.
+template <int P>
+__global__ void __launch_bounds__(160, 4) k_rotate_transpose_f32(const float* __restrict__ C, int mr_per_t,
                                                               DevTables T, float* __restrict__ SL3) {
+  constexpr int nc = P * (P + 2), ng = 2 * P * (P + 1), lda = nc + 1, NT = 160;
+  constexpr int NI = (P + 1) * (P + 2) / 2;  // items (n, m <= n), degree-major: n (n + 1) / 2 + m
+  static_assert(NI <= NT && (P & (P - 1)) == 0, "one item per thread; 2P a power of two");
   extern __shared__ __align__(16) float smf[];
-  // compile-time order: every index division below becomes a multiply and shift
-  constexpr int p0 = P, nc = P * (P + 2), ng = 2 * P * (P + 1);
-  constexpr int lda = nc + 1;  // odd row stride
-  constexpr int rows = CB * P;
-  float* sA = smf;                         // [rows][lda], degree-major
-  float* sB = sA + rows * lda;             // [rows][lda], coefficient order
-  float* sM = sB + rows * lda;             // blocks of degree n at sMo[n], rows of bn | 1
+  float* sA = smf;                         // [P rows][lda], degree-major
+  float* sM = sA + P * lda;                // blocks of degree n at sMo[n], rows of bn | 1
   const int msz = mr_per_t + (P + 1) * 2 * P;  // (upper bound of the padded size)
-  float* sCs = sM + msz;                   // cos_tab [2 p0]
-  float* sSn = sCs + 2 * p0;               // sin_tab [2 p0]
-  int* sMo = reinterpret_cast<int*>(sSn + 2 * p0);           // [p0 + 2] padded block offsets
-  unsigned short* sDm = reinterpret_cast<unsigned short*>(sMo + p0 + 2);  // degree-major position [nc]
-  short* sPc = reinterpret_cast<short*>(sDm + nc);                       // partner (or -1) [nc]
-  unsigned char* sMs = reinterpret_cast<unsigned char*>(sPc + nc);       // m | (is_sin << 7) [nc]
-  unsigned char* sN = sMs + nc;                                           // degree of position d [nc]
-  unsigned short* sP = reinterpret_cast<unsigned short*>(sN + ((nc + 1) & ~1));  // coefficient at d [nc]
+  float* sCs = sM + msz;                   // cos_tab [2P]
+  float* sSn = sCs + 2 * P;                // sin_tab [2P]
+  int* sMo = reinterpret_cast<int*>(sSn + 2 * P);                        // [P + 2] padded block offsets
+  unsigned short* sDm = reinterpret_cast<unsigned short*>(sMo + P + 2);  // degree-major position [nc]
+  short* sI0 = reinterpret_cast<short*>(sDm + nc);                       // cos (or single) coefficient [NI]
+  short* sI1 = sI0 + NI;                                                 // its sin partner or -1 [NI]
   const int t = blockIdx.x;
   const long v = blockIdx.y;
   const int tid = threadIdx.x;
   if (tid == 0) {
     int o = 0;
-    for (int n = 0; n <= p0; n++) {
+    for (int n = 0; n <= P; n++) {
       sMo[n] = o;
       const int bn = __ldg(T.perm_off + n + 1) - __ldg(T.perm_off + n);
       o += bn * (bn | 1);
     }
-    sMo[p0 + 1] = o;
+    sMo[P + 1] = o;
   }
-  for (int c = tid; c < nc; c += 256) {
-    const int n = __ldg(T.n_of_coef + c);
-    const int d = __ldg(T.perm_off + n) + __ldg(T.pos_in_block + c);
-    sDm[c] = (unsigned short)d;
-    sPc[c] = (short)__ldg(T.partner + c);
-    sMs[c] = (unsigned char)(__ldg(T.m_of_coef + c) | (__ldg(T.is_sin + c) ? 0x80 : 0));
-    sN[d] = (unsigned char)n;
-    sP[d] = (unsigned short)c;
-  }
-  for (int i = tid; i < 2 * p0; i += 256) {
+  for (int i = tid; i < NI; i += NT) sI0[i] = sI1[i] = -1;
+  for (int i = tid; i < 2 * P; i += NT) {
     sCs[i] = (float)__ldg(T.cos_tab + i);
     sSn[i] = (float)__ldg(T.sin_tab + i);
   }
   __syncthreads();
-  // the rotation blocks of this t, FP32, rows padded to bn + 1
-  for (int n = 0; n <= p0; n++) {
+  for (int c = tid; c < nc; c += NT) {
+    const int n = __ldg(T.n_of_coef + c), item = n * (n + 1) / 2 + __ldg(T.m_of_coef + c);
+    sDm[c] = (unsigned short)(__ldg(T.perm_off + n) + __ldg(T.pos_in_block + c));
+    if (__ldg(T.is_sin + c))
+      sI1[item] = (short)c;
+    else
+      sI0[item] = (short)c;
+  }
+  // the rotation blocks of this t, FP32, rows padded to bn | 1
+  for (int n = 0; n <= P; n++) {
     const int bn = __ldg(T.perm_off + n + 1) - __ldg(T.perm_off + n);
-    const double* M = T.mr + __ldg(T.mr_off + t * (p0 + 1) + n);
-    for (int i = tid; i < bn * bn; i += 256) {
+    const double* M = T.mr + __ldg(T.mr_off + t * (P + 1) + n);
+    for (int i = tid; i < bn * bn; i += NT) {
       const int b = i / bn, k = i - b * bn;
       sM[sMo[n] + b * (bn | 1) + k] = (float)__ldg(M + i);
     }
   }
+  __syncthreads();
+  // this thread's item
+  int n = 0;
+  while ((n + 1) * (n + 2) / 2 <= tid && n < P) n++;
+  const bool active = tid < NI && sI0[tid] >= 0;  // (every (n, m <= n) has its cos coefficient)
+  const int m = active ? tid - n * (n + 1) / 2 : 0;
+  const int c0 = active ? sI0[tid] : 0, c1 = active ? sI1[tid] : -1;
+  const int po = __ldg(T.perm_off + n), bn = __ldg(T.perm_off + n + 1) - po;
+  const float* M0 = active ? sM + sMo[n] + (sDm[c0] - po) * (bn | 1) : sM;
+  const float* M1 = c1 >= 0 ? sM + sMo[n] + (sDm[c1] - po) * (bn | 1) : M0;
   for (int pole = 0; pole < 2; pole++) {
-    for (int comp0 = 0; comp0 < 6; comp0 += CB) {
+    const int grid0 = pole == 0 ? t * 2 * P : (P - t) * 2 * P + P;
+    for (int comp = 0; comp < 6; comp++) {
       __syncthreads();
-      // stage: A[(cc, j)][dm(c)] = C[v][t][j][pole][comp0 + cc][c], eight loads in flight
-      // per thread before the shared-memory stores (degree-major: the rotation below reads
-      // a degree's inputs contiguously; gathering them through the permutation there cost
-      // more issue slots than the scattered stores here)
-      for (int i0 = tid; i0 < rows * nc; i0 += 256 * 8) {
+      // stage: A[j][dm(c)] = C[v][t][j][pole][comp][c], eight loads in flight per thread
+      for (int i0 = tid; i0 < P * nc; i0 += NT * 8) {
         float val[8];
 #pragma unroll
         for (int u = 0; u < 8; u++) {
-          const int i = i0 + u * 256;
-          if (i < rows * nc) {
-            const int r = i / nc, c = i - r * nc;
-            const int cc = r / p0, j = r - cc * p0;
-            val[u] = C[((((v * (p0 + 1) + t) * p0 + j) * 2 + pole) * 6 + comp0 + cc) * (long)nc + c];
+          const int i = i0 + u * NT;
+          if (i < P * nc) {
+            const int j = i / nc, c = i - j * nc;
+            val[u] = C[((((v * (P + 1) + t) * P + j) * 2 + pole) * 6 + comp) * (long)nc + c];
           }
         }
 #pragma unroll
         for (int u = 0; u < 8; u++) {
-          const int i = i0 + u * 256;
-          if (i < rows * nc) {
-            const int r = i / nc, c = i - r * nc;
-            sA[r * lda + sDm[c]] = val[u];
+          const int i = i0 + u * NT;
+          if (i < P * nc) {
+            const int j = i / nc, c = i - j * nc;
+            sA[j * lda + sDm[c]] = val[u];
           }
         }
       }
       __syncthreads();
-      // rotation back: thread (degree-major position d, 4 rows), so that a warp's lanes
-      // share a degree (the same loop length, broadcast inputs, consecutive block rows)
-      constexpr int nrq = (rows + 3) / 4;
-      for (int i = tid; i < nrq * nc; i += 256) {
-        const int d = i % nc, rq = i / nc;
-        const int n = sN[d], c = sP[d];
-        const int po = __ldg(T.perm_off + n), bn = __ldg(T.perm_off + n + 1) - po;
-        const int b = d - po;
-        const float* M = sM + sMo[n] + b * (bn | 1);
-        const float* a = sA + rq * 4 * lda + po;
-        float acc[4] = {0.f, 0.f, 0.f, 0.f};
-        for (int k = 0; k < bn; k++) {
-          const float m = M[k];
+      if (!active) continue;
+      float acc0[P], acc1[P];
 #pragma unroll
-          for (int q = 0; q < 4; q++) acc[q] = fmaf(a[q * lda + k], m, acc[q]);
+      for (int j = 0; j < P; j++) acc0[j] = acc1[j] = 0.f;
+      const float* a = sA + po;
+      for (int k = 0; k < bn; k++) {
+        const float m0 = M0[k], m1 = M1[k];
+#pragma unroll
+        for (int j = 0; j < P; j++) {
+          const float x = a[j * lda + k];
+          acc0[j] = fmaf(x, m0, acc0[j]);
+          acc1[j] = fmaf(x, m1, acc1[j]);
         }
-#pragma unroll
-        for (int q = 0; q < 4; q++)
-          if (rq * 4 + q < rows) sB[(rq * 4 + q) * lda + c] = acc[q];
       }
-      __syncthreads();
-      // inverse phase and scatter; consecutive threads take consecutive j
-      for (int i = tid; i < rows * nc; i += 256) {
-        const int j = i % p0, rest = i / p0;
-        const int c = rest % nc, cc = rest / nc;
-        const float* in = sB + (cc * p0 + j) * lda;
-        const int pc = sPc[c];
-        float val;
-        if (pc < 0) {
-          val = in[c];
-        } else {
-          const int ms = sMs[c];
-          const int q = ((ms & 0x7f) * j) % (2 * p0);
+      // inverse longitude phase of the pair: cos row c0, sin row c1
+      if (c1 >= 0) {
+#pragma unroll
+        for (int j = 0; j < P; j++) {
+          const int q = (m * j) & (2 * P - 1);
           const float cs = sCs[q], sn = sSn[q];
-          val = (ms & 0x80) ? fmaf(in[pc], sn, in[c] * cs) : fmaf(-in[pc], sn, in[c] * cs);
+          const float x0 = acc0[j], x1 = acc1[j];
+          acc0[j] = fmaf(-x1, sn, x0 * cs);
+          acc1[j] = fmaf(x0, sn, x1 * cs);
         }
-        const int grid = pole == 0 ? t * 2 * p0 + j : (p0 - t) * 2 * p0 + p0 + j;
-        // symmetric component -> (c_in, c_out): (0,0) (0,1) (0,2) (1,1) (1,2) (2,2)
-        const int comp = comp0 + cc;
-        const int cin = comp < 3 ? 0 : (comp < 5 ? 1 : 2), cout = comp < 3 ? comp : (comp < 5 ? comp - 2 : 2);
-        SL3[(((v * 3 + cin) * nc + c) * 3 + cout) * (long)ng + grid] = val;
-        if (cin != cout) SL3[(((v * 3 + cout) * nc + c) * 3 + cin) * (long)ng + grid] = val;
       }
+      // symmetric component -> (c_in, c_out): (0,0) (0,1) (0,2) (1,1) (1,2) (2,2)
+      const int cin = comp < 3 ? 0 : (comp < 5 ? 1 : 2), cout = comp < 3 ? comp : (comp < 5 ? comp - 2 : 2);
+      auto put = [&](int c, const float* o) {
+        float4* d0 = reinterpret_cast<float4*>(SL3 + (((v * 3 + cin) * nc + c) * 3 + cout) * (long)ng + grid0);
+        float4* d1 = reinterpret_cast<float4*>(SL3 + (((v * 3 + cout) * nc + c) * 3 + cin) * (long)ng + grid0);
+#pragma unroll
+        for (int q = 0; q < P / 4; q++) {
+          const float4 w = make_float4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
+          d0[q] = w;
+          if (cin != cout) d1[q] = w;
+        }
+      };
+      put(c0, acc0);
+      if (c1 >= 0) put(c1, acc1);
     }
   }
 }
 
-static size_t rt_f32_smem(int p0, int cb, int mpt) {
-  const int nc = p0 * (p0 + 2), lda = nc + 1;
-  const size_t fl = (size_t)2 * cb * p0 * lda + mpt + (size_t)(p0 + 1) * 2 * p0 + 4 * p0;
-  return fl * sizeof(float) + (size_t)(p0 + 2) * sizeof(int) + (size_t)nc * 8 + 16;
+static size_t rt_f32_smem(int p0, int mpt) {
+  const int nc = p0 * (p0 + 2), lda = nc + 1, ni = (p0 + 1) * (p0 + 2) / 2;
+  const size_t fl = (size_t)p0 * lda + mpt + (size_t)(p0 + 1) * 2 * p0 + 4 * p0;
+  return fl * sizeof(float) + (size_t)(p0 + 2) * sizeof(int) + (size_t)nc * 2 + (size_t)ni * 4 + 16;
 }
 
 int launch_rotate_transpose_f32(const float* C, long nv, const DevTables& T, float* SL3, cudaStream_t st) {
@@ -486,11 +487,10 @@ int launch_rotate_transpose_f32(const float* C, long nv, const DevTables& T, flo
     return VES3D_ERR_ARG;
   }
   dim3 grid(p0 + 1, (unsigned)nv);
-  // one component per group: 68 KB of shared memory at p = 16, three CTAs per SM (two
-  // components per group, two CTAs: 9.1 ms at 512 vesicles)
-  const size_t smem = rt_f32_smem(p0, 1, mpt);
-  VES3D_CK(cudaFuncSetAttribute(k_rotate_transpose_f32<16, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_rotate_transpose_f32<16, 1><<<grid, 256, smem, st>>>(C, mpt, T, SL3);
+  // about 48 KB of shared memory at p = 16: four CTAs of 160 threads per SM
+  const size_t smem = rt_f32_smem(p0, mpt);
+  VES3D_CK(cudaFuncSetAttribute(k_rotate_transpose_f32<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_rotate_transpose_f32<16><<<grid, 160, smem, st>>>(C, mpt, T, SL3);
   VES3D_LAUNCHED();
   return VES3D_OK;
 }
