@@ -312,45 +312,50 @@ static int sm_count() {
 }
 
 // Grid2SHC(p, p) of FP32 grid values in FP32 on the CUDA cores (the mixed form's
-// self-matrix grid, whose values carry FP32 precision): persistent CTAs stage the DFT and
-// Legendre tables (FP32) once and walk groups of FB functions. Per group the length-2p DFT of
-// every (function, latitude) row, one thread per 4 rows x 4 frequencies (16 accumulators:
-// row values broadcast across a warp's frequency quads, conflict-free table rows), then the
-// per-frequency Legendre sums, one thread per (function, coefficient); the next group's grid
-// values are loaded into registers meanwhile. Output FP64 like the FP64 forms'.
+// self-matrix grid, whose values carry FP32 precision): persistent CTAs of NC = p (p + 2)
+// threads stage the DFT table (FP32) once, each thread keeps the Legendre row of its
+// coefficient in registers, and the CTA walks groups of FB functions. Per group the
+// length-2p DFT of every (function, latitude) row, one thread per 4 rows x 4 frequencies
+// (16 accumulators: row values broadcast across a warp's frequency quads, conflict-free
+// table rows; one pass: RQ x KQ <= NC), then the Legendre sums of every function of the
+// group at the thread's coefficient (the DFT rows of its Fourier block, broadcast to the
+// block's coefficients); the next group's grid values are loaded into registers meanwhile.
+// Output FP64 like the FP64 forms'.
 template <int P>
 struct AnaF32Cfg {
   static constexpr int FB = 8;
-  static constexpr int NLAT = P + 1, NLON = 2 * P, NC = P * (P + 2);
+  static constexpr int NLAT = P + 1, NLON = 2 * P, NC = P * (P + 2), NT = NC;
   static constexpr int ROWS = FB * NLAT, RQ = (ROWS + 3) / 4, KQ = NLON / 4;
   static constexpr int LDG = NLON + 1;  // grid rows (odd: a warp's 4 row quads on distinct banks)
   static constexpr int LDF = NLON + 1;  // DFT result rows
   static constexpr int SZ_G = RQ * 4 * LDG, SZ_F = ROWS * LDF;
-  static constexpr int OFF_G = 0, OFF_F = OFF_G + SZ_G, OFF_M = OFF_F + SZ_F, OFF_L = OFF_M + NLON * NLON;
-  static constexpr int OFF_JF = OFF_L + NC * NLAT;
-  static constexpr size_t SMEM = (size_t)(OFF_JF + NC) * sizeof(float);
-  static constexpr int U = (ROWS * NLON + 255) / 256;  // grid values per thread per group
-  static_assert(NLON % 4 == 0, "frequency quads");
+  static constexpr int OFF_G = 0, OFF_F = OFF_G + SZ_G, OFF_M = OFF_F + SZ_F;
+  static constexpr size_t SMEM = (size_t)(OFF_M + NLON * NLON) * sizeof(float);
+  static constexpr int U = (ROWS * NLON + NT - 1) / NT;  // grid values per thread per group
+  static_assert(NLON % 4 == 0 && NT % 32 == 0 && RQ * KQ <= NT, "frequency quads; whole warps; one DFT pass");
 };
 
 template <int P>
-__global__ void __launch_bounds__(256, 3) k_analysis_f32(const float* __restrict__ in, long nfun,
-                                                         const double* __restrict__ four,
-                                                         const double* __restrict__ leg, const int* __restrict__ jf,
-                                                         double* __restrict__ out) {
+__global__ void __launch_bounds__(AnaF32Cfg<P>::NT, 2) k_analysis_f32(const float* __restrict__ in, long nfun,
+                                                                       const double* __restrict__ four,
+                                                                       const double* __restrict__ leg,
+                                                                       const int* __restrict__ jf,
+                                                                       double* __restrict__ out) {
   using G = AnaF32Cfg<P>;
+  constexpr int NT = G::NT;
   extern __shared__ __align__(16) float smf[];
   float* sG = smf + G::OFF_G;
   float* sF = smf + G::OFF_F;
   float* sM = smf + G::OFF_M;  // four [j][k], row stride NLON (float4 reads of 4 frequencies)
-  float* sL = smf + G::OFF_L;  // leg [c][lat]
-  int* sJf = reinterpret_cast<int*>(smf + G::OFF_JF);
   const int tid = threadIdx.x;
-  for (int i = tid; i < G::NLON * G::NLON; i += 256) sM[i] = (float)__ldg(four + i);
-  for (int i = tid; i < G::NC * G::NLAT; i += 256) sL[i] = (float)__ldg(leg + i);
-  for (int i = tid; i < G::NC; i += 256) sJf[i] = __ldg(jf + i);
+  for (int i = tid; i < G::NLON * G::NLON; i += NT) sM[i] = (float)__ldg(four + i);
   // rows past the group's last function stay zero (their outputs are never written)
-  for (int i = tid; i < G::SZ_G; i += 256) sG[i] = 0.f;
+  for (int i = tid; i < G::SZ_G; i += NT) sG[i] = 0.f;
+  // this thread's coefficient c = tid: its Fourier block and Legendre row
+  const int jfc = __ldg(jf + tid);
+  float lr[G::NLAT];
+#pragma unroll
+  for (int lat = 0; lat < G::NLAT; lat++) lr[lat] = (float)__ldg(leg + tid * G::NLAT + lat);
   const long ngroups = (nfun + G::FB - 1) / G::FB;
   float pre[G::U];
   auto load_group = [&](long g) {
@@ -359,7 +364,7 @@ __global__ void __launch_bounds__(256, 3) k_analysis_f32(const float* __restrict
     const float* src = in + (nf ? f0 : 0) * G::NLAT * G::NLON;
 #pragma unroll
     for (int u = 0; u < G::U; u++) {
-      const int i = tid + u * 256;
+      const int i = tid + u * NT;
       pre[u] = (i < nf * G::NLAT * G::NLON) ? src[i] : 0.f;
     }
   };
@@ -370,7 +375,7 @@ __global__ void __launch_bounds__(256, 3) k_analysis_f32(const float* __restrict
     __syncthreads();  // the previous group's sG / sF reads are done
 #pragma unroll
     for (int u = 0; u < G::U; u++) {
-      const int i = tid + u * 256;
+      const int i = tid + u * NT;
       if (i < G::ROWS * G::NLON) {
         const int r = i / G::NLON, j = i - r * G::NLON;
         sG[r * G::LDG + j] = pre[u];
@@ -379,8 +384,8 @@ __global__ void __launch_bounds__(256, 3) k_analysis_f32(const float* __restrict
     __syncthreads();
     load_group(grp + gridDim.x);
     // DFT: F[r][k] = sum_j G[r][j] four[j][k]
-    for (int it = tid; it < G::RQ * G::KQ; it += 256) {
-      const int kq = it % G::KQ, rq = it / G::KQ;
+    if (tid < G::RQ * G::KQ) {
+      const int kq = tid % G::KQ, rq = tid / G::KQ;
       const float* g = sG + rq * 4 * G::LDG;
       const float4* m = reinterpret_cast<const float4*>(sM) + kq;
       float acc[4][4] = {};
@@ -409,15 +414,13 @@ __global__ void __launch_bounds__(256, 3) k_analysis_f32(const float* __restrict
       }
     }
     __syncthreads();
-    // Legendre: out[f][c] = sum_lat F[f][lat][jf(c)] leg[c][lat]
-    for (int i = tid; i < nf * G::NC; i += 256) {
-      const int f = i / G::NC, c = i - f * G::NC;
-      const float* fr = sF + (f * G::NLAT) * G::LDF + sJf[c];
-      const float* lr = sL + c * G::NLAT;
+    // Legendre: out[f][c] = sum_lat F[f][lat][jf(c)] leg[c][lat], c = tid
+    for (int f = 0; f < nf; f++) {
+      const float* fr = sF + (f * G::NLAT) * G::LDF + jfc;
       float s = 0.f;
 #pragma unroll
       for (int lat = 0; lat < G::NLAT; lat++) s = fmaf(fr[lat * G::LDF], lr[lat], s);
-      out[(f0 + f) * G::NC + c] = (double)s;
+      out[(f0 + f) * G::NC + tid] = (double)s;
     }
   }
 }
@@ -427,9 +430,11 @@ static int launch_ana_f32(const float* in, long nfun, const double* four, const 
                           double* out, cudaStream_t st) {
   using G = AnaF32Cfg<P>;
   VES3D_CK(cudaFuncSetAttribute(k_analysis_f32<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM));
+  int per_sm = 0;
+  VES3D_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_analysis_f32<P>, G::NT, G::SMEM));
   const long ngroups = (nfun + G::FB - 1) / G::FB;
-  const long grid = std::min(ngroups, 3L * sm_count());
-  k_analysis_f32<P><<<(unsigned)grid, 256, G::SMEM, st>>>(in, nfun, four, leg, jf, out);
+  const long grid = std::min(ngroups, (long)std::max(per_sm, 1) * sm_count());
+  k_analysis_f32<P><<<(unsigned)grid, G::NT, G::SMEM, st>>>(in, nfun, four, leg, jf, out);
   VES3D_LAUNCHED();
   return VES3D_OK;
 }
