@@ -336,7 +336,7 @@ struct AnaF32Cfg {
 };
 
 template <int P>
-__global__ void __launch_bounds__(AnaF32Cfg<P>::NT, 2) k_analysis_f32(const float* __restrict__ in, long nfun,
+__global__ void __launch_bounds__(AnaF32Cfg<P>::NT, 3) k_analysis_f32(const float* __restrict__ in, long nfun,
                                                                        const double* __restrict__ four,
                                                                        const double* __restrict__ leg,
                                                                        const int* __restrict__ jf,
