@@ -644,49 +644,64 @@ DL_FLOPS_PER_PAIR = 30  # r, |r|^2, 1/|r|, |r|^-5, two dots, their product, thre
 
 
 def double_layer_measurement(X, f, p, local, stream, steps=3):
-    """The 512-vesicle evaluation with a double-layer density set as well (SetDensityDL):
-    device time of the far double layer's kernels (FP64 in both forms) against the FP64
-    FMA peak, and of the whole evaluation (single + double layer) in the FP64 form."""
+    """The 512-vesicle evaluation with a double-layer density set as well (SetDensityDL), in
+    the FP64 form and in the mixed form with its opt-in FP32 far double layer
+    (VES3D_FAR_DL_F32=1; by default the mixed form keeps the far double layer in FP64):
+    device time of the far double layer's kernel against the FMA peak of its precision and
+    of the whole evaluation (single + double layer); the mixed velocity's error against the
+    FP64 form's (which is parity-pinned to the oracle)."""
     import torch
     from ves3d_b200.stokes_velocity import StokesVelocity
     ng = 2 * p * (p + 1)
     nves = X.size // (3 * ng)
-    N = nves * ng
     g = np.random.default_rng(4242).standard_normal(X.size)
     dev = torch.device("cuda", local)
-    sv = StokesVelocity(p, 2 * p, precision="fp64", device=local)
-    sv.set_stream(stream.cuda_stream)
-    out = torch.empty(X.size, dtype=torch.float64, device=dev)
-    sv.SetSrcCoord(X)
-    sv.SetDensitySL(f)
-    sv.SetDensityDL(g)
-    torch.cuda.synchronize()
-    b0 = time.perf_counter()
-    sv(out)  # builds the DL self matrices (stage by stage) on first use
-    torch.cuda.synchronize()
-    first_s = time.perf_counter() - b0
-    evals, far_dl = [], []
-    for _ in range(steps):
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        sv(out)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        evals.append(e0.elapsed_time(e1))
-        far_dl.append(sv.far_dl_ms())
-    sv.close()
     pairs = far_pairs(nves, ng)
-    ms = statistics.mean(far_dl)
-    achieved = DL_FLOPS_PER_PAIR * pairs / (ms * 1e-3) / 1e12
-    peak = fma_peak(True)
-    return {"what": "512-vesicle p=16 evaluation with single- and double-layer densities, FP64; surfaces and "
-                    "self matrices built before the timed evaluations",
-            "eval_ms": statistics.mean(evals), "far_dl_ms": ms, "first_eval_with_dl_build_s": first_s,
-            "far_dl_roofline": {"kernel": "k_far_dl_f64_flat", "bound": "fp64_pipe", "achieved": achieved,
-                                "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                                "work": f"{DL_FLOPS_PER_PAIR} flops per (target, source) pair x {pairs} pairs"}}
+    res, vel = {}, {}
+    for prec in ("fp64", "mixed"):
+        saved = os.environ.get("VES3D_FAR_DL_F32")
+        os.environ["VES3D_FAR_DL_F32"] = "1" if prec == "mixed" else "0"
+        sv = StokesVelocity(p, 2 * p, precision=prec, device=local)  # reads the switch
+        if saved is None:
+            del os.environ["VES3D_FAR_DL_F32"]
+        else:
+            os.environ["VES3D_FAR_DL_F32"] = saved
+        sv.set_stream(stream.cuda_stream)
+        out = torch.empty(X.size, dtype=torch.float64, device=dev)
+        sv.SetSrcCoord(X)
+        sv.SetDensitySL(f)
+        sv.SetDensityDL(g)
+        torch.cuda.synchronize()
+        b0 = time.perf_counter()
+        sv(out)  # builds the DL self matrices (stage by stage) on first use
+        torch.cuda.synchronize()
+        first_s = time.perf_counter() - b0
+        evals, far_dl = [], []
+        for _ in range(steps):
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            sv(out)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            evals.append(e0.elapsed_time(e1))
+            far_dl.append(sv.far_dl_ms())
+        vel[prec] = out.cpu().numpy()
+        sv.close()
+        ms = statistics.mean(far_dl)
+        achieved = DL_FLOPS_PER_PAIR * pairs / (ms * 1e-3) / 1e12
+        peak = fma_peak(prec == "fp64")
+        kernel = "k_far_dl_f64_flat" if prec == "fp64" else "k_far_dl_f32_flat"
+        res[prec] = {"eval_ms": statistics.mean(evals), "far_dl_ms": ms, "first_eval_with_dl_build_s": first_s,
+                     "far_dl_roofline": {"kernel": kernel, "bound": "fp64_pipe" if prec == "fp64" else "fp32_pipe",
+                                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                                         "work": f"{DL_FLOPS_PER_PAIR} flops per (target, source) pair x {pairs} pairs"}}
+    d = np.abs(vel["mixed"] - vel["fp64"]).max() / np.abs(vel["fp64"]).max()
+    res["mixed"]["error_vs_fp64_form"] = {"max_rel": float(d), "sample": "all points, single + double layer"}
+    return {"what": "512-vesicle p=16 evaluation with single- and double-layer densities; surfaces and "
+                    "self matrices built before the timed evaluations; top level: FP64 form",
+            **res["fp64"], "mixed": res["mixed"]}
 
 
 def run_ours(args, world, rank, local):

@@ -43,6 +43,29 @@ def test_single_and_double_layer_match_oracle(nside, p, seed):
         assert rel_err(vself + vfar, vel) < 1e-14
 
 
+@pytest.mark.parametrize("nside,p,seed", [(2, 8, 5), (2, 16, 3)])
+def test_mixed_double_layer_matches_oracle(nside, p, seed, monkeypatch):
+    """Mixed form with the far double layer in FP32 pair arithmetic (k_far_dl_f32_flat,
+    opt-in: VES3D_FAR_DL_F32=1, read when the context is created). The double layer alone,
+    then single + double layer, the evaluation and its far part within 1e-6 (relative,
+    max-norm) of the FP64 oracle."""
+    monkeypatch.setenv("VES3D_FAR_DL_F32", "1")
+    X, f = small_suspension(nside, p, seed)
+    g = np.random.default_rng(seed + 100).standard_normal(X.size)
+    with StokesVelocity(p, precision="mixed") as sv:
+        sv.SetSrcCoord(X)
+        sv.SetDensitySL(np.zeros_like(X))
+        sv.SetDensityDL(g)
+        sv()
+        _, vfar_dl = sv.parts()
+        sv.SetDensitySL(f)
+        vel = sv()
+        _, vfar = sv.parts()
+    assert rel_err(vfar_dl, stokes.far_dl_velocity(X, g, p)) < 1e-6
+    assert rel_err(vel, stokes.stokes_velocity_sl(X, f, p) + stokes.stokes_velocity_dl(X, g, p)) < 1e-6
+    assert rel_err(vfar, stokes.far_velocity(X, f, p) + stokes.far_dl_velocity(X, g, p)) < 1e-6
+
+
 def test_double_layer_on_and_off():
     """Turning the double layer off returns the single-layer evaluation; the difference
     while it is on is the double-layer velocity; new surfaces clear the density."""
@@ -92,7 +115,8 @@ def test_double_layer_in_the_captured_evaluation(precision):
 def test_double_layer_of_constant_densities_at_size(precision):
     """Gauss's identity on 64 vesicles of p = 12: a constant double-layer density c_v on each
     vesicle gives -c_v / 2 on its surface and nothing on the others (the oracle measures
-    4.2e-6 on this suspension); the double layer is FP64 in both forms."""
+    4.2e-6 on this suspension); the far double layer is FP64 in both forms (FP32 pairs only
+    on request)."""
     p = 12
     X, _ = workloads.suspension(4, p, 3.0, semi_axes=(1.0, 1.0, 0.6), deg=4, amp=0.05, seed=8)
     ng = sh.ngrid(p)

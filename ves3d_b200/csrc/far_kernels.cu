@@ -533,6 +533,179 @@ __global__ void __launch_bounds__(NT, 1152 / NT) k_far_f32_flat(const double* __
   }
 }
 
+// ---- the far double layer in the mixed form --------------------------------------------
+// Pair arithmetic of k_far_dl_f64_flat (u += (t - s) (r.n)(r.g) / |r|^5, r = t - s) in
+// packed FP32 pairs: coordinates relative to the centroid of the chunk's targets (FP64
+// difference rounded once per source per CTA), the hardware 1/sqrt with one Newton step
+// (the kernel takes its fifth power), coincident pairs dropped by a select, FP32 sums per
+// sub-tile of kSubDL32 sources added in FP64.
+constexpr int kTileDL32 = 640;  // 9 float2 per source: 46 KB staged per barrier pair
+constexpr int kSubDL32 = 128;
+
+template <int NT>
+__device__ __forceinline__ void stage_dl32(float2* sm, const double* __restrict__ pos, const double* __restrict__ nrm,
+                                           const double* __restrict__ dden, long s0, int ns, const double* cen) {
+  const double cx = cen[0], cy = cen[1], cz = cen[2];
+#pragma unroll 1
+  for (int i = threadIdx.x; i < ns; i += NT) {
+    const long s = s0 + i;
+    float2* d = sm + 9 * i;
+    d[0] = f2((float)(pos[3 * s] - cx));
+    d[1] = f2((float)(pos[3 * s + 1] - cy));
+    d[2] = f2((float)(pos[3 * s + 2] - cz));
+    d[3] = f2((float)nrm[3 * s]);
+    d[4] = f2((float)nrm[3 * s + 1]);
+    d[5] = f2((float)nrm[3 * s + 2]);
+    d[6] = f2((float)dden[3 * s]);
+    d[7] = f2((float)dden[3 * s + 1]);
+    d[8] = f2((float)dden[3 * s + 2]);
+  }
+}
+
+// One staged source against the thread's two targets (negated, packed); own: the lanes
+// whose target belongs to this source's vesicle (their pair is dropped).
+__device__ __forceinline__ void pair_dl32(const float2* __restrict__ q, float2 ntx, float2 nty, float2 ntz,
+                                          bool own_a, bool own_b, float2& ux, float2& uy, float2& uz) {
+  // s - t (the sign of t - s cancels in (r.n)(r.g); the sum takes -(s - t))
+  const float2 rx = make_float2(__fadd_rn(q[0].x, ntx.x), __fadd_rn(q[0].y, ntx.y));
+  const float2 ry = make_float2(__fadd_rn(q[1].x, nty.x), __fadd_rn(q[1].y, nty.y));
+  const float2 rz = make_float2(__fadd_rn(q[2].x, ntz.x), __fadd_rn(q[2].y, ntz.y));
+  float2 r2 = __fmul2_rn(rx, rx);
+  r2 = __ffma2_rn(ry, ry, r2);
+  r2 = __ffma2_rn(rz, rz, r2);
+  float2 y = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
+  const float2 e = __ffma2_rn(__fmul2_rn(make_float2(-r2.x, -r2.y), y), y, f2(1.f));
+  y = __ffma2_rn(__fmul2_rn(f2(0.5f), y), e, y);
+  // coincident pairs (|r|^2 below 2^-126) and the target's own vesicle contribute nothing
+  y.x = (own_a || !(r2.x >= 1.17549435e-38f)) ? 0.f : y.x;
+  y.y = (own_b || !(r2.y >= 1.17549435e-38f)) ? 0.f : y.y;
+  float2 rn = __fmul2_rn(rx, q[3]);
+  rn = __ffma2_rn(ry, q[4], rn);
+  rn = __ffma2_rn(rz, q[5], rn);
+  float2 rg = __fmul2_rn(rx, q[6]);
+  rg = __ffma2_rn(ry, q[7], rg);
+  rg = __ffma2_rn(rz, q[8], rg);
+  const float2 y2 = __fmul2_rn(y, y);
+  const float2 y5 = __fmul2_rn(__fmul2_rn(y2, y2), y);
+  const float2 nq = __fmul2_rn(__fmul2_rn(rn, rg), make_float2(-y5.x, -y5.y));
+  ux = __ffma2_rn(rx, nq, ux);
+  uy = __ffma2_rn(ry, nq, uy);
+  uz = __ffma2_rn(rz, nq, uz);
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT, 1024 / NT) k_far_dl_f32_flat(const double* __restrict__ pos,
+                                                                    const double* __restrict__ nrm,
+                                                                    const double* __restrict__ dden,
+                                                                    const long* __restrict__ off, long nves, long N,
+                                                                    int seg_tiles, double* __restrict__ part) {
+  __shared__ __align__(16) float2 sm[kTileDL32 * 9];
+  __shared__ ChunkRange cr;
+  __shared__ double cen[3];
+  __shared__ double red[3][NT / 32];
+  chunk_range<NT>(off, nves, N, &cr);
+  const int seg = blockIdx.x;
+  {  // centroid of the chunk's targets (FP64), the origin of this CTA's FP32 coordinates
+    const long c0 = cr.c0, nt = cr.c1 - cr.c0;
+    double cx = 0, cy = 0, cz = 0;
+#pragma unroll 1
+    for (long i = threadIdx.x; i < nt; i += NT) {
+      cx += pos[3 * (c0 + i)];
+      cy += pos[3 * (c0 + i) + 1];
+      cz += pos[3 * (c0 + i) + 2];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      cx += __shfl_down_sync(0xffffffffu, cx, o);
+      cy += __shfl_down_sync(0xffffffffu, cy, o);
+      cz += __shfl_down_sync(0xffffffffu, cz, o);
+    }
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+      red[0][w] = cx;
+      red[1][w] = cy;
+      red[2][w] = cz;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+      double sum = 0;
+      for (int i = 0; i < NT / 32; i++) sum += red[threadIdx.x][i];
+      cen[threadIdx.x] = sum / (double)nt;
+    }
+    __syncthreads();
+  }
+  const long ja = cr.c0 + threadIdx.x, jb = ja + NT;
+  const long la = ja < cr.c1 ? ja : cr.c0, lb = jb < cr.c1 ? jb : cr.c0;
+  float2 ntx, nty, ntz;  // negated targets, packed (lane x = target a, lane y = target b)
+  {
+    const double cx = cen[0], cy = cen[1], cz = cen[2];
+    ntx = make_float2((float)(cx - pos[3 * la]), (float)(cx - pos[3 * lb]));
+    nty = make_float2((float)(cy - pos[3 * la + 1]), (float)(cy - pos[3 * lb + 1]));
+    ntz = make_float2((float)(cz - pos[3 * la + 2]), (float)(cz - pos[3 * lb + 2]));
+  }
+  double A[2][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+  auto flush = [&](float2 ux, float2 uy, float2 uz) {
+    A[0][0] += ux.x;
+    A[0][1] += uy.x;
+    A[0][2] += uz.x;
+    A[1][0] += ux.y;
+    A[1][1] += uy.y;
+    A[1][2] += uz.y;
+  };
+  const long ntiles = (N + kTileDL32 - 1) / kTileDL32;
+  const long tb = (long)seg * seg_tiles, te = min(tb + seg_tiles, ntiles);
+  for (long tile = tb; tile < te; tile++) {
+    const long s0 = tile * kTileDL32;
+    const int ns = (int)min((long)kTileDL32, N - s0);
+    __syncthreads();
+    stage_dl32<NT>(sm, pos, nrm, dden, s0, ns, cen);
+    __syncthreads();
+    int r0[2], r1[2];
+    split_tile(s0, ns, cr.u0, cr.u1, r0[0], r1[0], r0[1], r1[1]);
+    for (int sb = 0; sb < ns; sb += kSubDL32) {
+      const int se = min(sb + kSubDL32, ns);
+      float2 ux = f2(0.f), uy = f2(0.f), uz = f2(0.f);
+#pragma unroll
+      for (int part_i = 0; part_i < 2; part_i++) {
+        const int k1 = min(r1[part_i], se);
+#pragma unroll 2
+        for (int k = max(r0[part_i], sb); k < k1; k++) pair_dl32(sm + 9 * k, ntx, nty, ntz, false, false, ux, uy, uz);
+      }
+      flush(ux, uy, uz);
+    }
+  }
+  // the chunk's own vesicles within this segment: each target skips its own vesicle
+  const long g0 = max(cr.u0, tb * kTileDL32), g1 = min(cr.u1, min(te * kTileDL32, N));
+  if (g0 < g1) {
+    const long va = vesicle_of(off, nves, la), vb = vesicle_of(off, nves, lb);
+    const long ea0 = off[va], ea1 = off[va + 1], eb0 = off[vb], eb1 = off[vb + 1];
+    for (long s0 = g0; s0 < g1; s0 += kTileDL32) {
+      const int ns = (int)min((long)kTileDL32, g1 - s0);
+      __syncthreads();
+      stage_dl32<NT>(sm, pos, nrm, dden, s0, ns, cen);
+      __syncthreads();
+      for (int sb = 0; sb < ns; sb += kSubDL32) {
+        const int se = min(sb + kSubDL32, ns);
+        float2 ux = f2(0.f), uy = f2(0.f), uz = f2(0.f);
+        for (int k = sb; k < se; k++) {
+          const long sg = s0 + k;
+          pair_dl32(sm + 9 * k, ntx, nty, ntz, sg >= ea0 && sg < ea1, sg >= eb0 && sg < eb1, ux, uy, uz);
+        }
+        flush(ux, uy, uz);
+      }
+    }
+  }
+  double* P = part + (long)seg * 3 * N;
+#pragma unroll
+  for (int j = 0; j < 2; j++) {
+    const long g = cr.c0 + threadIdx.x + (long)j * NT;
+    if (g < cr.c1) {
+      P[3 * g] = A[j][0];
+      P[3 * g + 1] = A[j][1];
+      P[3 * g + 2] = A[j][2];
+    }
+  }
+}
+
 // out (AxisMajor per vesicle) = add + (1/8pi) sum over segments in order. One CTA per
 // vesicle; vesicle v holds points [off[v], off[v+1]) as [3][n_v] from 3*off[v].
 __global__ void k_far_reduce(const double* __restrict__ part, int nseg, const long* __restrict__ off, long N,
@@ -757,14 +930,30 @@ std::string autotune_report() {
   return r;
 }
 
-// The far double layer (FP64) over every point, one launch whatever the vesicle sizes.
-int launch_far_dl_groups(const double* pos, const double* nrm, const double* dden, const long* off, long nves, long N,
-                         const FarGroup* groups, int ngroups, double* part, long part_cap_segments, cudaStream_t st,
-                         int* nseg_out) {
+// The far double layer over every point, one launch whatever the vesicle sizes: FP64, or
+// packed FP32 pairs with FP64 sub-tile sums in the mixed form.
+int launch_far_dl_groups(bool mixed, const double* pos, const double* nrm, const double* dden, const long* off,
+                         long nves, long N, const FarGroup* groups, int ngroups, double* part, long part_cap_segments,
+                         cudaStream_t st, int* nseg_out) {
   (void)groups;
   (void)ngroups;
   *nseg_out = 0;
   if (N <= 0 || nves <= 0) return VES3D_OK;
+  if (mixed) {
+    constexpr int NT = 256;
+    const long nchunk = (N + 2L * NT - 1) / (2L * NT);
+    if (nchunk > 65535) {
+      set_error("far double layer: %ld points exceed the launch's %ld target chunks", N, 65535L * 2 * NT);
+      return VES3D_ERR_ARG;
+    }
+    int seg_tiles = 1;
+    const int nseg = far_segments(nchunk, N, kTileDL32, NT, 16, part_cap_segments, &seg_tiles);
+    k_far_dl_f32_flat<NT><<<dim3((unsigned)nseg, (unsigned)nchunk), NT, 0, st>>>(pos, nrm, dden, off, nves, N,
+                                                                                 seg_tiles, part);
+    VES3D_LAUNCHED();
+    *nseg_out = nseg;
+    return VES3D_OK;
+  }
   constexpr int NT = 384;
   const long nchunk = (N + 2L * NT - 1) / (2L * NT);
   if (nchunk > 65535) {
@@ -780,10 +969,10 @@ int launch_far_dl_groups(const double* pos, const double* nrm, const double* dde
   return VES3D_OK;
 }
 
-int launch_far_dl(const double* pos, const double* nrm, const double* dden, const long* off, long nves, long N,
-                  int max_nt, double* part, long part_cap_segments, cudaStream_t st, int* nseg_out) {
+int launch_far_dl(bool mixed, const double* pos, const double* nrm, const double* dden, const long* off, long nves,
+                  long N, int max_nt, double* part, long part_cap_segments, cudaStream_t st, int* nseg_out) {
   FarGroup g{0, nves, max_nt};
-  return launch_far_dl_groups(pos, nrm, dden, off, nves, N, &g, 1, part, part_cap_segments, st, nseg_out);
+  return launch_far_dl_groups(mixed, pos, nrm, dden, off, nves, N, &g, 1, part, part_cap_segments, st, nseg_out);
 }
 
 int launch_far(bool mixed, const double* pos, const double* den, const long* off, long nves, long N, int max_nt,

@@ -125,12 +125,13 @@ int launch_far(bool mixed, const double* pos, const double* den, const long* off
 int launch_far_reduce(const double* part, int nseg, const long* off, long nves, long N, const double* add, double* out,
                       double* far_out, cudaStream_t st, const double* part2 = nullptr, int nseg2 = 0,
                       double scale2 = 0.0);
-// Far double layer over the points of the other vesicles (FP64): pos, unit normals nrm and
-// densities dden (times area and weights) point-major; the segments' unscaled partials go to
-// part (at most part_cap_segments), their count to *nseg_out, for launch_far_reduce's second
-// set with scale kDl.
-int launch_far_dl(const double* pos, const double* nrm, const double* dden, const long* off, long nves, long N,
-                  int max_nt, double* part, long part_cap_segments, cudaStream_t st, int* nseg_out);
+// Far double layer over the points of the other vesicles (FP64, or packed FP32 pairs with
+// FP64 sub-tile sums when mixed): pos, unit normals nrm and densities dden (times area and
+// weights) point-major; the segments' unscaled partials go to part (at most
+// part_cap_segments), their count to *nseg_out, for launch_far_reduce's second set with
+// scale kDl.
+int launch_far_dl(bool mixed, const double* pos, const double* nrm, const double* dden, const long* off, long nves,
+                  long N, int max_nt, double* part, long part_cap_segments, cudaStream_t st, int* nseg_out);
 // Velocity at M off-surface targets (point-major [M][3]) from N surface points: single
 // layer of den, plus with nrm non-null the double layer of nrm and dden (all point-major,
 // densities times area and weights).
@@ -159,9 +160,9 @@ int launch_far_groups(bool mixed, const double* pos, const double* den, const lo
                       double* part, long part_cap_segments, cudaStream_t st, int* nseg_out = nullptr);
 // launch_far_dl over order groups (a polydisperse suspension): per-group block shapes, one
 // segment layout.
-int launch_far_dl_groups(const double* pos, const double* nrm, const double* dden, const long* off, long nves, long N,
-                         const FarGroup* groups, int ngroups, double* part, long part_cap_segments, cudaStream_t st,
-                         int* nseg_out);
+int launch_far_dl_groups(bool mixed, const double* pos, const double* nrm, const double* dden, const long* off,
+                         long nves, long N, const FarGroup* groups, int ngroups, double* part, long part_cap_segments,
+                         cudaStream_t st, int* nseg_out);
 // out = a + b elementwise.
 int launch_add(const double* a, const double* b, long n, double* out, cudaStream_t st);
 // All pairs, point-major in/out (StokesAlltoAll semantics).

@@ -146,6 +146,7 @@ struct ves3d_sv {
   // because both kernels already fill the SMs, and each kernel's own duration (the
   // roofline denominator) then includes the sharing
   bool overlap = false;
+  bool far_dl_f32 = false;  // the mixed form's far double layer in FP32 pairs (opt-in, VES3D_FAR_DL_F32=1)
   std::unique_ptr<TablesOwner> tab;
   long nves = 0, cap_ves = 0;
   // resident buffers
@@ -594,12 +595,13 @@ int fork_far(ves3d_sv* sv, int* nseg, cudaEvent_t ev_far0, cudaEvent_t ev_far1, 
     return s;
   if (ev_far1) VES3D_CK(cudaEventRecord(ev_far1, fs));
   sv->nseg_dl = 0;
-  if (dl) {  // the far double layer (FP64) after the single layer's segments
+  if (dl) {  // the far double layer after the single layer's segments: FP64 (FP32 pairs on request)
     if ((s = launch_unit_normals(sv->Xt, sv->Xp, sv->nves, sv->p, sv->nrm, fs))) return s;
     if ((s = launch_far_density(sv->G, sv->area, sv->nves, sv->p, T.smooth_w0, sv->dden, fs))) return s;
     if (ev_far0) VES3D_CK(cudaEventRecord(sv->ev[8], fs));
-    if ((s = launch_far_dl(sv->pos, sv->nrm, sv->dden, sv->off, sv->nves, sv->npts(), ngrid_(sv->p), sv->part_dl,
-                           kFarMaxSegments, fs, &sv->nseg_dl)))
+    const bool dl32 = sv->prec == VES3D_PREC_MIXED && !sv->far_force_fp64 && sv->far_dl_f32;
+    if ((s = launch_far_dl(dl32, sv->pos, sv->nrm, sv->dden, sv->off, sv->nves, sv->npts(), ngrid_(sv->p),
+                           sv->part_dl, kFarMaxSegments, fs, &sv->nseg_dl)))
       return s;
     if (ev_far0) VES3D_CK(cudaEventRecord(sv->ev[9], fs));
   }
@@ -838,6 +840,8 @@ int ves3d_sv_create(int sh_order, int sh_order_up, int precision, int device, ve
     VES3D_CK(cudaStreamCreateWithPriority(&sv->hi, cudaStreamNonBlocking, greatest));
     const char* e = getenv("VES3D_FAR_OVERLAP");
     sv->overlap = e && e[0] == '1';
+    const char* d = getenv("VES3D_FAR_DL_F32");
+    sv->far_dl_f32 = d && d[0] == '1';
   }
   VES3D_CK(cudaEventCreateWithFlags(&sv->ev_fork, cudaEventDisableTiming));
   VES3D_CK(cudaEventCreateWithFlags(&sv->ev_join, cudaEventDisableTiming));
@@ -2995,6 +2999,7 @@ int ves3d_sv_implicit_combine(ves3d_sv* sv, int n_cand, const double* const* can
 // ======================================================================================
 struct ves3d_svp {
   int prec = 0, device = 0;
+  bool far_dl_f32 = false;  // the mixed form's far double layer in FP32 pairs (opt-in, VES3D_FAR_DL_F32=1)
   cudaStream_t stream = nullptr;
   std::vector<ves3d_sv*> grp;          // one operator per run of equal order
   std::vector<int> gp;                 // order of each run
@@ -3076,6 +3081,10 @@ int ves3d_svp_create(int precision, int device, ves3d_svp** out) {
   std::unique_ptr<ves3d_svp> g(new ves3d_svp());
   g->prec = precision;
   g->device = device;
+  {
+    const char* d = getenv("VES3D_FAR_DL_F32");
+    g->far_dl_f32 = d && d[0] == '1';
+  }
   VES3D_CK(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
   for (auto& e : g->ev) VES3D_CK(cudaEventCreate(&e));
   *out = g.release();
@@ -3276,8 +3285,8 @@ static int svp_far(ves3d_svp* g, bool dl) {
   if ((s = launch_far_groups(mixed, g->pos, g->den, g->off, g->nves, g->N, fg.data(), (int)fg.size(), nullptr,
                              nullptr, nullptr, g->part, kFarMaxSegments, g->stream, &nseg)))
     return s;
-  if ((s = launch_far_dl_groups(g->pos, g->nrm, g->dden, g->off, g->nves, g->N, fg.data(), (int)fg.size(),
-                                g->part_dl, kFarMaxSegments, g->stream, &nseg_dl)))
+  if ((s = launch_far_dl_groups(mixed && g->far_dl_f32, g->pos, g->nrm, g->dden, g->off, g->nves, g->N, fg.data(),
+                                (int)fg.size(), g->part_dl, kFarMaxSegments, g->stream, &nseg_dl)))
     return s;
   return launch_far_reduce(g->part, nseg, g->off, g->nves, g->N, g->vself, g->V, g->Vfar, g->stream, g->part_dl,
                            nseg_dl, kDl);
