@@ -86,6 +86,10 @@ int launch_rotate_transpose_scatter(const double* C, long nv, const DevTables& T
 // The same from FP32 transposed-DFT results (the tensor-core build's), rotated back in FP32,
 // into an FP32 grid.
 int launch_rotate_transpose_f32(const float* C, long nv, const DevTables& T, float* SL3, cudaStream_t st);
+// The same from the FP64 ring's results (rounded to FP32 when staged), at the orders it is
+// instantiated for (the mixed form's self matrices at p = 12 and 24).
+bool rotate_transpose_f32_from_f64_supported(int p0);
+int launch_rotate_transpose_f32(const double* C, long nv, const DevTables& T, float* SL3, cudaStream_t st);
 // Fused per-rotation build (FP64 tensor cores): R [nrot][3][Nc] -> C [nrot][2][6][Nc],
 // i.e. upsampled synthesis + singular kernel + transposed synthesis in one kernel.
 bool fused_build_supported(int p0, int p1);

@@ -324,7 +324,8 @@ static int sm_count() {
 template <int P>
 struct AnaF32Cfg {
   static constexpr int FB = 8;
-  static constexpr int NLAT = P + 1, NLON = 2 * P, NC = P * (P + 2), NT = NC;
+  static constexpr int NLAT = P + 1, NLON = 2 * P, NC = P * (P + 2), NT = (NC + 31) / 32 * 32;
+  static constexpr int MINB = P == 16 ? 3 : 1;  // CTAs per SM the registers are sized for
   static constexpr int ROWS = FB * NLAT, RQ = (ROWS + 3) / 4, KQ = NLON / 4;
   static constexpr int LDG = NLON + 1;  // grid rows (odd: a warp's 4 row quads on distinct banks)
   static constexpr int LDF = NLON + 1;  // DFT result rows
@@ -336,7 +337,7 @@ struct AnaF32Cfg {
 };
 
 template <int P>
-__global__ void __launch_bounds__(AnaF32Cfg<P>::NT, 3) k_analysis_f32(const float* __restrict__ in, long nfun,
+__global__ void __launch_bounds__(AnaF32Cfg<P>::NT, AnaF32Cfg<P>::MINB) k_analysis_f32(const float* __restrict__ in, long nfun,
                                                                        const double* __restrict__ four,
                                                                        const double* __restrict__ leg,
                                                                        const int* __restrict__ jf,
@@ -351,11 +352,13 @@ __global__ void __launch_bounds__(AnaF32Cfg<P>::NT, 3) k_analysis_f32(const floa
   for (int i = tid; i < G::NLON * G::NLON; i += NT) sM[i] = (float)__ldg(four + i);
   // rows past the group's last function stay zero (their outputs are never written)
   for (int i = tid; i < G::SZ_G; i += NT) sG[i] = 0.f;
-  // this thread's coefficient c = tid: its Fourier block and Legendre row
-  const int jfc = __ldg(jf + tid);
+  // this thread's coefficient c = tid (threads past NC have none): its Fourier block and
+  // Legendre row
+  const bool has_c = tid < G::NC;
+  const int jfc = has_c ? __ldg(jf + tid) : 0;
   float lr[G::NLAT];
 #pragma unroll
-  for (int lat = 0; lat < G::NLAT; lat++) lr[lat] = (float)__ldg(leg + tid * G::NLAT + lat);
+  for (int lat = 0; lat < G::NLAT; lat++) lr[lat] = has_c ? (float)__ldg(leg + tid * G::NLAT + lat) : 0.f;
   const long ngroups = (nfun + G::FB - 1) / G::FB;
   float pre[G::U];
   auto load_group = [&](long g) {
@@ -415,7 +418,7 @@ __global__ void __launch_bounds__(AnaF32Cfg<P>::NT, 3) k_analysis_f32(const floa
     }
     __syncthreads();
     // Legendre: out[f][c] = sum_lat F[f][lat][jf(c)] leg[c][lat], c = tid
-    for (int f = 0; f < nf; f++) {
+    for (int f = 0; f < (has_c ? nf : 0); f++) {
       const float* fr = sF + (f * G::NLAT) * G::LDF + jfc;
       float s = 0.f;
 #pragma unroll
@@ -478,11 +481,12 @@ int launch_grid2shc_f32(const float* in, long nfun, int p, const double* four, c
   switch (p) {
     case 4: return launch_ana_tc<4>(in, nfun, four, leg, jf, out, st);
     case 8: return launch_ana_tc<8>(in, nfun, four, leg, jf, out, st);
-    case 12: return launch_ana_tc<12>(in, nfun, four, leg, jf, out, st);
+    case 12: return launch_ana_f32<12>(in, nfun, four, leg, jf, out, st);
     case 16: return launch_ana_f32<16>(in, nfun, four, leg, jf, out, st);
+    case 24: return launch_ana_f32<24>(in, nfun, four, leg, jf, out, st);
     default: break;
   }
-  set_error("Grid2SHC of FP32 values is instantiated for p in {4, 8, 12, 16}, not %d", p);
+  set_error("Grid2SHC of FP32 values is instantiated for p in {4, 8, 12, 16, 24}, not %d", p);
   return VES3D_ERR_ARG;
 }
 

@@ -342,13 +342,20 @@ __global__ void __launch_bounds__(256) k_rotate_transpose_scatter(const double* 
 // and the P consecutive grid values of each coefficient as float4 stores into the
 // self-matrix grid SL3 (FP32: the Grid2SHC that follows reads it into FP64), laid out as
 // the FP64 forms'. A thread's rows share the staged inputs (broadcast to the lanes of its
-// degree) and its two rotation rows: 18 shared loads per 32 FMAs.
+// degree) and its two rotation rows: 18 shared loads per 32 FMAs at p = 16. The input C is
+// FP32 (after the tensor-core build) or FP64 (after the FP64 ring, rounded when staged).
 template <int P>
-__global__ void __launch_bounds__(160, 4) k_rotate_transpose_f32(const float* __restrict__ C, int mr_per_t,
-                                                              DevTables T, float* __restrict__ SL3) {
-  constexpr int nc = P * (P + 2), ng = 2 * P * (P + 1), lda = nc + 1, NT = 160;
-  constexpr int NI = (P + 1) * (P + 2) / 2;  // items (n, m <= n), degree-major: n (n + 1) / 2 + m
-  static_assert(NI <= NT && (P & (P - 1)) == 0, "one item per thread; 2P a power of two");
+struct RtF32Cfg {
+  static constexpr int NI = (P + 1) * (P + 2) / 2;  // items (n, m <= n), degree-major: n (n + 1) / 2 + m
+  static constexpr int NT = (NI + 31) / 32 * 32;   // one item per thread
+  static constexpr int MINB = P == 16 ? 4 : 1;     // CTAs per SM the registers are sized for
+};
+
+template <int P, typename TC>
+__global__ void __launch_bounds__(RtF32Cfg<P>::NT, RtF32Cfg<P>::MINB)
+    k_rotate_transpose_f32(const TC* __restrict__ C, int mr_per_t, DevTables T, float* __restrict__ SL3) {
+  constexpr int nc = P * (P + 2), ng = 2 * P * (P + 1), lda = nc + 1;
+  constexpr int NI = RtF32Cfg<P>::NI, NT = RtF32Cfg<P>::NT;
   extern __shared__ __align__(16) float smf[];
   float* sA = smf;                         // [P rows][lda], degree-major
   float* sM = sA + P * lda;                // blocks of degree n at sMo[n], rows of bn | 1
@@ -416,7 +423,7 @@ __global__ void __launch_bounds__(160, 4) k_rotate_transpose_f32(const float* __
           const int i = i0 + u * NT;
           if (i < P * nc) {
             const int j = i / nc, c = i - j * nc;
-            val[u] = C[((((v * (P + 1) + t) * P + j) * 2 + pole) * 6 + comp) * (long)nc + c];
+            val[u] = (float)C[((((v * (P + 1) + t) * P + j) * 2 + pole) * 6 + comp) * (long)nc + c];
           }
         }
 #pragma unroll
@@ -447,7 +454,7 @@ __global__ void __launch_bounds__(160, 4) k_rotate_transpose_f32(const float* __
       if (c1 >= 0) {
 #pragma unroll
         for (int j = 0; j < P; j++) {
-          const int q = (m * j) & (2 * P - 1);
+          const int q = (m * j) % (2 * P);
           const float cs = sCs[q], sn = sSn[q];
           const float x0 = acc0[j], x1 = acc1[j];
           acc0[j] = fmaf(-x1, sn, x0 * cs);
@@ -478,21 +485,38 @@ static size_t rt_f32_smem(int p0, int mpt) {
   return fl * sizeof(float) + (size_t)(p0 + 2) * sizeof(int) + (size_t)nc * 2 + (size_t)ni * 4 + 16;
 }
 
-int launch_rotate_transpose_f32(const float* C, long nv, const DevTables& T, float* SL3, cudaStream_t st) {
-  if (nv <= 0) return VES3D_OK;
-  const int p0 = T.p0, mpt = mr_per_t(T);
-  // the FP32 results come from the tensor-core build, which is laid out for p = 16 only
-  if (p0 != 16) {
-    set_error("internal: FP32 rotate-transpose at p = %d (built for p = 16)", p0);
-    return VES3D_ERR_ARG;
-  }
-  dim3 grid(p0 + 1, (unsigned)nv);
-  // about 48 KB of shared memory at p = 16: four CTAs of 160 threads per SM
-  const size_t smem = rt_f32_smem(p0, mpt);
-  VES3D_CK(cudaFuncSetAttribute(k_rotate_transpose_f32<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_rotate_transpose_f32<16><<<grid, 160, smem, st>>>(C, mpt, T, SL3);
+template <int P, typename TC>
+static int launch_rt_f32(const TC* C, long nv, const DevTables& T, float* SL3, cudaStream_t st) {
+  const int mpt = mr_per_t(T);
+  dim3 grid(P + 1, (unsigned)nv);
+  const size_t smem = rt_f32_smem(P, mpt);  // about 48 KB at p = 16 (four CTAs per SM), 149 KB at p = 24
+  VES3D_CK(cudaFuncSetAttribute(k_rotate_transpose_f32<P, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_rotate_transpose_f32<P, TC><<<grid, RtF32Cfg<P>::NT, smem, st>>>(C, mpt, T, SL3);
   VES3D_LAUNCHED();
   return VES3D_OK;
+}
+
+int launch_rotate_transpose_f32(const float* C, long nv, const DevTables& T, float* SL3, cudaStream_t st) {
+  if (nv <= 0) return VES3D_OK;
+  // the FP32 results come from the tensor-core build, which is laid out for p = 16 only
+  if (T.p0 != 16) {
+    set_error("internal: FP32 rotate-transpose at p = %d (built for p = 16)", T.p0);
+    return VES3D_ERR_ARG;
+  }
+  return launch_rt_f32<16>(C, nv, T, SL3, st);
+}
+
+bool rotate_transpose_f32_from_f64_supported(int p0) { return p0 == 12 || p0 == 24; }
+
+int launch_rotate_transpose_f32(const double* C, long nv, const DevTables& T, float* SL3, cudaStream_t st) {
+  if (nv <= 0) return VES3D_OK;
+  switch (T.p0) {
+    case 12: return launch_rt_f32<12>(C, nv, T, SL3, st);
+    case 24: return launch_rt_f32<24>(C, nv, T, SL3, st);
+    default: break;
+  }
+  set_error("internal: FP32 rotate-transpose of FP64 results at p = %d (built for p in {12, 24})", T.p0);
+  return VES3D_ERR_ARG;
 }
 
 // VES3D_TC_ROTATE=0 selects the CUDA-core form of the rotate-transpose (for comparison).

@@ -203,7 +203,8 @@ struct ves3d_sv {
   long chunk = 0;
   double *R = nullptr, *Xu = nullptr, *Xut = nullptr, *Xup = nullptr, *K = nullptr, *C = nullptr, *SL3 = nullptr;
   bool have_src = false, have_den = false, sl_valid = false, parts_valid = false;
-  // sl_tc: the current self matrices come from the tensor-core build of the mixed form;
+  // sl_tc: the current self matrices come from the mixed form's FP32 build stages (the
+  // tensor-core build at p = 16, the FP32 rotate-transpose and Grid2SHC at p = 12, 24);
   // implicit_on: implicit parameters were set, whose FP64 residuals need FP64 self matrices
   bool sl_tc = false, implicit_on = false;
   // implicit step: geometry record and work fields (allocated on first use)
@@ -390,6 +391,15 @@ bool use_tc_build(const ves3d_sv* sv) {
   return !(env && env[0] == '0');
 }
 
+// The mixed form's other fused orders (p = 12, 24): the FP64 ring's results rotated back and
+// taken to coefficients in FP32 (as after the tensor-core build); the same conditions and
+// switch as the tensor-core build.
+bool use_f32_post(const ves3d_sv* sv) {
+  if (sv->prec != VES3D_PREC_MIXED || sv->implicit_on || !rotate_transpose_f32_from_f64_supported(sv->p)) return false;
+  const char* env = getenv("VES3D_TC_BUILD");
+  return !(env && env[0] == '0');
+}
+
 // A context that takes implicit steps keeps FP64 self matrices: the mixed refinement's
 // outer residuals are those of the FP64 system. Self matrices from the tensor-core build
 // are rebuilt on next use.
@@ -481,6 +491,7 @@ int run_setup(ves3d_sv* sv, bool dl) {
   if (s) return s;
   const bool fused = !dl && use_fused(sv);
   const bool tc = fused && use_tc_build(sv);
+  const bool f32post = fused && !tc && use_f32_post(sv);
   double* M = dl ? sv->DL : sv->SL;
   if ((!fused && !sv->K) || !M) {
     set_error("internal: self-matrix build without its buffers");
@@ -508,9 +519,11 @@ int run_setup(ves3d_sv* sv, bool dl) {
         return s;
     }
     double* Mv = M + v0 * (long)(3 * nc) * (3 * nc);
-    if (fused && tc) {  // FP32 grid between the rotation back and Grid2SHC
+    if (tc || f32post) {  // FP32 grid between the rotation back and Grid2SHC
       float* SLf = reinterpret_cast<float*>(sv->SL3);
-      if ((s = launch_rotate_transpose_f32(Cf, nb, T, SLf, st))) return s;
+      if ((s = tc ? launch_rotate_transpose_f32(Cf, nb, T, SLf, st)
+                  : launch_rotate_transpose_f32(sv->C, nb, T, SLf, st)))
+        return s;
       if ((s = launch_grid2shc_f32(SLf, nb * 3 * nc * 3, p0, T.ana_four, T.ana_leg, T.jf_of_coef, Mv, st))) return s;
     } else {
       if ((s = launch_rotate_transpose_scatter(sv->C, nb, T, sv->SL3, st))) return s;
@@ -530,7 +543,7 @@ int run_setup(ves3d_sv* sv, bool dl) {
     sv->dl_valid = true;
   } else {
     sv->sl_valid = true;
-    sv->sl_tc = tc;
+    sv->sl_tc = tc || f32post;
   }
   return VES3D_OK;
 }
