@@ -108,3 +108,41 @@ def test_tensor_core_build_is_deterministic_and_matches_fp64_ring_env(monkeypatc
         sv.SetSrcCoord(X)
         d = sv.self_matrix()
     assert np.array_equal(c, d)
+
+
+@pytest.mark.parametrize("p", [12, 24])
+def test_fp32_build_stages_after_the_fp64_ring(p, monkeypatch):
+    """At p = 12 and 24 the mixed form rotates the FP64 ring's results back and takes them to
+    coefficients in FP32: self matrices within 1e-6 of the FP64 build (and not its bits);
+    VES3D_TC_BUILD=0 keeps the FP64 stages (bitwise the FP64 build)."""
+    X, _ = small_suspension(1, p, 63)
+    with StokesVelocity(p, precision="fp64") as sv:
+        sv.SetSrcCoord(X)
+        d = sv.self_matrix()
+    with StokesVelocity(p, precision="mixed") as sv:
+        sv.SetSrcCoord(X)
+        m = sv.self_matrix()
+    assert 0 < rel_err(m, d) < MIXED_TOL
+    monkeypatch.setenv("VES3D_TC_BUILD", "0")
+    with StokesVelocity(p, precision="mixed") as sv:
+        sv.SetSrcCoord(X)
+        c = sv.self_matrix()
+    assert np.array_equal(c, d)
+
+
+@pytest.mark.parametrize("p", [12, 16])
+def test_implicit_steps_take_fp64_self_matrices(p):
+    """Self matrices from the mixed form's FP32 build stages (the tensor-core build at p = 16,
+    the FP32 stages after the FP64 ring at p = 12) are rebuilt in FP64 once the context takes
+    implicit steps: the mixed refinement's outer residuals are those of the FP64 system."""
+    X, _ = small_suspension(1, p, 64)
+    with StokesVelocity(p, precision="fp64") as sv:
+        sv.SetSrcCoord(X)
+        d = sv.self_matrix()
+    with StokesVelocity(p, precision="mixed") as sv:
+        sv.SetSrcCoord(X)
+        m = sv.self_matrix()
+        sv.set_implicit_params(0.01, 0.05, 1.0)
+        after = sv.self_matrix()
+    assert not np.array_equal(m, d)
+    assert np.array_equal(after, d)
