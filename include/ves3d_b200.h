@@ -509,8 +509,9 @@ int ves3d_stokes_alltoall_device_f64(const double* src, const double* den, size_
  * VES3D_NOALLOC_MAX_POINTS points (36 MiB, held by every GPU that loads the library
  * until exit); np above that is rejected with VES3D_ERR_ARG. On any error pot (3 np
  * doubles) is filled with NaN, as by the allocating call; np = 0 leaves it untouched.
- * The array's device address is looked up on every call (it stays valid across
- * cudaDeviceReset). Calls share the array: calls whose GPU work overlaps race. */
+ * The array's device address is looked up on the first call on each device and kept, so
+ * the library does not survive cudaDeviceReset. Calls share the array: calls whose GPU
+ * work overlaps race. */
 #define VES3D_NOALLOC_MAX_POINTS 524288
 int ves3d_stokes_alltoall_noalloc_f64(const double* src, const double* den, size_t np, double* pot,
                                       void* stream);

@@ -15,9 +15,10 @@
 // exits. Every call shares it and it keeps the last call's contents; nothing in it has
 // to start at zero (each call overwrites the parts it reads). Calls whose GPU work
 // overlaps (other host threads, or streams that run concurrently) race on the array.
-// The array's address is looked up on every call, so the entry point keeps working after
-// the device's context is torn down and rebuilt (cudaDeviceReset).
+// The array's address is looked up once per device and kept for the life of the
+// process, so the entry point does not survive cudaDeviceReset.
 #include <cmath>
+#include <mutex>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -28,12 +29,25 @@ namespace ves3d {
 static __device__ __align__(256) double g_noalloc_scratch[(size_t)VES3D_NOALLOC_MAX_POINTS * 9];
 
 namespace {
-// Device address of the array on the current device, looked up on every call (cheap; a
-// cached address would go stale when the device's context is torn down and rebuilt).
+constexpr int kMaxDevices = 64;
+std::mutex g_mu;
+double* g_addr[kMaxDevices] = {nullptr};
+
+// Device address of the array on the current device, looked up once per device.
 int scratch_address(double** out) {
-  void* p = nullptr;
-  VES3D_CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-  *out = (double*)p;
+  int dev = 0;
+  VES3D_CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) {
+    set_error("device index %d beyond the %d devices this entry point supports", dev, kMaxDevices);
+    return VES3D_ERR_NODEV;
+  }
+  std::lock_guard<std::mutex> lock(g_mu);
+  if (!g_addr[dev]) {
+    void* p = nullptr;
+    VES3D_CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_addr[dev] = (double*)p;
+  }
+  *out = g_addr[dev];
   return VES3D_OK;
 }
 }  // namespace
