@@ -504,14 +504,14 @@ int ves3d_stokes_alltoall_device_f64(const double* src, const double* den, size_
  * cudaMalloc/cudaFree between time steps), which cannot let the library allocate. Same
  * HOST-pointer arguments and result as ves3d_stokes_alltoall_f64, plus an optional
  * stream (NULL = legacy default stream); returns an int status. The call is synchronous:
- * it waits for its result on that stream before returning, so it cannot be recorded
- * into a CUDA graph. Inputs are staged through one fixed device array of
+ * it waits for its result on that stream before returning. Inputs are staged through one
+ * fixed device array of
  * VES3D_NOALLOC_MAX_POINTS points (36 MiB, held by every GPU that loads the library
  * until exit); np above that is rejected with VES3D_ERR_ARG. On any error pot (3 np
  * doubles) is filled with NaN, as by the allocating call; np = 0 leaves it untouched.
- * The array's device address is looked up on the first call on each device and kept, so
- * the library does not survive cudaDeviceReset. Calls share the array: calls whose GPU
- * work overlaps race. */
+ * The first call on each device does the set-up (looks up the array's device address and
+ * keeps it): make it before any stream capture. The kept address does not survive
+ * cudaDeviceReset. Calls share the array: calls whose GPU work overlaps race. */
 #define VES3D_NOALLOC_MAX_POINTS 524288
 int ves3d_stokes_alltoall_noalloc_f64(const double* src, const double* den, size_t np, double* pot,
                                       void* stream);

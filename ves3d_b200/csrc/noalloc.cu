@@ -7,16 +7,17 @@
 // use; this variant stages them through a fixed, file-scope device array instead.
 //
 // The call is synchronous: it copies host arrays in, runs the sum and waits for the
-// result on the caller's stream before it returns, so it cannot be recorded into a
-// CUDA graph.
+// result on the caller's stream before it returns.
 //
 // The array holds VES3D_NOALLOC_MAX_POINTS points (source, density and result, three
 // doubles each: 36 MiB). Every GPU that loads the library holds it until the process
 // exits. Every call shares it and it keeps the last call's contents; nothing in it has
 // to start at zero (each call overwrites the parts it reads). Calls whose GPU work
 // overlaps (other host threads, or streams that run concurrently) race on the array.
-// The array's address is looked up once per device and kept for the life of the
-// process, so the entry point does not survive cudaDeviceReset.
+// The first call on each device does the set-up: with that device current it looks up
+// the array's device address (cudaGetSymbolAddress; host code may not use the array's
+// name as a device pointer) and keeps it for the life of the process. Make that first
+// call before any stream capture. The kept address does not survive cudaDeviceReset.
 #include <cmath>
 #include <mutex>
 
