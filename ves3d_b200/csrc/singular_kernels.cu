@@ -330,38 +330,43 @@ __global__ void __launch_bounds__(256) k_rotate_transpose_scatter(const double* 
   }
 }
 
-// Mixed form of the rotate-transpose (after the tensor-core build, whose transposed-DFT
-// results C are FP32): one CTA per (latitude rotation t, vesicle v); for each pole and
-// symmetric component the P longitude rows of C are staged in degree-major order, then
-// each thread takes one item (degree n, order m): the coefficient of cos(m phi) and its
-// sin(m phi) partner (one coefficient for m = 0 and m = P), and forms for all P rows the
-// rotation back
+// The rotate-transpose per (degree, order) item, in the arithmetic type TV: one CTA per
+// (latitude rotation t, vesicle v); for each pole and symmetric component the P longitude
+// rows of C are staged in degree-major order, then each thread takes one item (degree n,
+// order m): the coefficient of cos(m phi) and its sin(m phi) partner (one coefficient for
+// m = 0 and m = P), and forms for all P rows the rotation back
 //     B[row][po + b] = sum_k A[row][po + k] Mr_{t,n}[b][k]
-// at its two positions b in FP32 (the values carry FP32 precision already; the FP64 form
-// uses the DMMA kernel below), then the inverse longitude phase of the pair in registers
-// and the P consecutive grid values of each coefficient as float4 stores into the
-// self-matrix grid SL3 (FP32: the Grid2SHC that follows reads it into FP64), laid out as
-// the FP64 forms'. A thread's rows share the staged inputs (broadcast to the lanes of its
-// degree) and its two rotation rows: 18 shared loads per 32 FMAs at p = 16. The input C is
-// FP32 (after the tensor-core build) or FP64 (after the FP64 ring, rounded when staged).
-template <int P>
-struct RtF32Cfg {
+// at its two positions b, then the inverse longitude phase of the pair in registers and
+// the P consecutive grid values of each coefficient as 16-byte vector stores into the
+// self-matrix grid SL3, laid out as the other forms'. A thread's rows share the staged
+// inputs (broadcast to the lanes of its degree) and its two rotation rows: 18 shared loads
+// per 32 FMAs at p = 16. TV = float in the mixed form (C is FP32 after the tensor-core
+// build, FP64 after the FP64 ring and rounded when staged; the FP32 grid goes to the FP32
+// Grid2SHC); TV = double in the FP64 form at p = 16 (the DMMA kernel below keeps the
+// other orders up to 16).
+// The 16-byte vector of 16 / sizeof(T) values starting at o[i] (destinations 16-byte aligned).
+__device__ __forceinline__ float4 vec16(const float* o, int i) { return make_float4(o[i], o[i + 1], o[i + 2], o[i + 3]); }
+__device__ __forceinline__ double2 vec16(const double* o, int i) { return make_double2(o[i], o[i + 1]); }
+
+template <int P, typename TV>
+struct RtItemCfg {
   static constexpr int NI = (P + 1) * (P + 2) / 2;  // items (n, m <= n), degree-major: n (n + 1) / 2 + m
   static constexpr int NT = (NI + 31) / 32 * 32;   // one item per thread
-  static constexpr int MINB = P == 16 ? 4 : 1;     // CTAs per SM the registers are sized for
+  // CTAs per SM the registers are sized for (shared memory allows 4 in FP32, 2 in FP64 at p = 16)
+  static constexpr int MINB = P == 16 ? (sizeof(TV) == 4 ? 4 : 2) : 1;
 };
 
-template <int P, typename TC>
-__global__ void __launch_bounds__(RtF32Cfg<P>::NT, RtF32Cfg<P>::MINB)
-    k_rotate_transpose_f32(const TC* __restrict__ C, int mr_per_t, DevTables T, float* __restrict__ SL3) {
+template <int P, typename TC, typename TV>
+__global__ void __launch_bounds__(RtItemCfg<P, TV>::NT, RtItemCfg<P, TV>::MINB)
+    k_rotate_transpose_item(const TC* __restrict__ C, int mr_per_t, DevTables T, TV* __restrict__ SL3) {
   constexpr int nc = P * (P + 2), ng = 2 * P * (P + 1), lda = nc + 1;
-  constexpr int NI = RtF32Cfg<P>::NI, NT = RtF32Cfg<P>::NT;
-  extern __shared__ __align__(16) float smf[];
-  float* sA = smf;                         // [P rows][lda], degree-major
-  float* sM = sA + P * lda;                // blocks of degree n at sMo[n], rows of bn | 1
+  constexpr int NI = RtItemCfg<P, TV>::NI, NT = RtItemCfg<P, TV>::NT;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  TV* sA = reinterpret_cast<TV*>(smraw);  // [P rows][lda], degree-major
+  TV* sM = sA + P * lda;                  // blocks of degree n at sMo[n], rows of bn | 1
   const int msz = mr_per_t + (P + 1) * 2 * P;  // (upper bound of the padded size)
-  float* sCs = sM + msz;                   // cos_tab [2P]
-  float* sSn = sCs + 2 * P;                // sin_tab [2P]
+  TV* sCs = sM + msz;                     // cos_tab [2P]
+  TV* sSn = sCs + 2 * P;                  // sin_tab [2P]
   int* sMo = reinterpret_cast<int*>(sSn + 2 * P);                        // [P + 2] padded block offsets
   unsigned short* sDm = reinterpret_cast<unsigned short*>(sMo + P + 2);  // degree-major position [nc]
   short* sI0 = reinterpret_cast<short*>(sDm + nc);                       // cos (or single) coefficient [NI]
@@ -380,8 +385,8 @@ __global__ void __launch_bounds__(RtF32Cfg<P>::NT, RtF32Cfg<P>::MINB)
   }
   for (int i = tid; i < NI; i += NT) sI0[i] = sI1[i] = -1;
   for (int i = tid; i < 2 * P; i += NT) {
-    sCs[i] = (float)__ldg(T.cos_tab + i);
-    sSn[i] = (float)__ldg(T.sin_tab + i);
+    sCs[i] = (TV)__ldg(T.cos_tab + i);
+    sSn[i] = (TV)__ldg(T.sin_tab + i);
   }
   __syncthreads();
   for (int c = tid; c < nc; c += NT) {
@@ -398,7 +403,7 @@ __global__ void __launch_bounds__(RtF32Cfg<P>::NT, RtF32Cfg<P>::MINB)
     const double* M = T.mr + __ldg(T.mr_off + t * (P + 1) + n);
     for (int i = tid; i < bn * bn; i += NT) {
       const int b = i / bn, k = i - b * bn;
-      sM[sMo[n] + b * (bn | 1) + k] = (float)__ldg(M + i);
+      sM[sMo[n] + b * (bn | 1) + k] = (TV)__ldg(M + i);
     }
   }
   __syncthreads();
@@ -409,21 +414,21 @@ __global__ void __launch_bounds__(RtF32Cfg<P>::NT, RtF32Cfg<P>::MINB)
   const int m = active ? tid - n * (n + 1) / 2 : 0;
   const int c0 = active ? sI0[tid] : 0, c1 = active ? sI1[tid] : -1;
   const int po = __ldg(T.perm_off + n), bn = __ldg(T.perm_off + n + 1) - po;
-  const float* M0 = active ? sM + sMo[n] + (sDm[c0] - po) * (bn | 1) : sM;
-  const float* M1 = c1 >= 0 ? sM + sMo[n] + (sDm[c1] - po) * (bn | 1) : M0;
+  const TV* M0 = active ? sM + sMo[n] + (sDm[c0] - po) * (bn | 1) : sM;
+  const TV* M1 = c1 >= 0 ? sM + sMo[n] + (sDm[c1] - po) * (bn | 1) : M0;
   for (int pole = 0; pole < 2; pole++) {
     const int grid0 = pole == 0 ? t * 2 * P : (P - t) * 2 * P + P;
     for (int comp = 0; comp < 6; comp++) {
       __syncthreads();
       // stage: A[j][dm(c)] = C[v][t][j][pole][comp][c], eight loads in flight per thread
       for (int i0 = tid; i0 < P * nc; i0 += NT * 8) {
-        float val[8];
+        TV val[8];
 #pragma unroll
         for (int u = 0; u < 8; u++) {
           const int i = i0 + u * NT;
           if (i < P * nc) {
             const int j = i / nc, c = i - j * nc;
-            val[u] = (float)C[((((v * (P + 1) + t) * P + j) * 2 + pole) * 6 + comp) * (long)nc + c];
+            val[u] = (TV)C[((((v * (P + 1) + t) * P + j) * 2 + pole) * 6 + comp) * (long)nc + c];
           }
         }
 #pragma unroll
@@ -437,17 +442,17 @@ __global__ void __launch_bounds__(RtF32Cfg<P>::NT, RtF32Cfg<P>::MINB)
       }
       __syncthreads();
       if (!active) continue;
-      float acc0[P], acc1[P];
+      TV acc0[P], acc1[P];
 #pragma unroll
-      for (int j = 0; j < P; j++) acc0[j] = acc1[j] = 0.f;
-      const float* a = sA + po;
+      for (int j = 0; j < P; j++) acc0[j] = acc1[j] = TV(0);
+      const TV* a = sA + po;
       for (int k = 0; k < bn; k++) {
-        const float m0 = M0[k], m1 = M1[k];
+        const TV m0 = M0[k], m1 = M1[k];
 #pragma unroll
         for (int j = 0; j < P; j++) {
-          const float x = a[j * lda + k];
-          acc0[j] = fmaf(x, m0, acc0[j]);
-          acc1[j] = fmaf(x, m1, acc1[j]);
+          const TV x = a[j * lda + k];
+          acc0[j] = fma(x, m0, acc0[j]);
+          acc1[j] = fma(x, m1, acc1[j]);
         }
       }
       // inverse longitude phase of the pair: cos row c0, sin row c1
@@ -455,22 +460,24 @@ __global__ void __launch_bounds__(RtF32Cfg<P>::NT, RtF32Cfg<P>::MINB)
 #pragma unroll
         for (int j = 0; j < P; j++) {
           const int q = (m * j) % (2 * P);
-          const float cs = sCs[q], sn = sSn[q];
-          const float x0 = acc0[j], x1 = acc1[j];
-          acc0[j] = fmaf(-x1, sn, x0 * cs);
-          acc1[j] = fmaf(x0, sn, x1 * cs);
+          const TV cs = sCs[q], sn = sSn[q];
+          const TV x0 = acc0[j], x1 = acc1[j];
+          acc0[j] = fma(-x1, sn, x0 * cs);
+          acc1[j] = fma(x0, sn, x1 * cs);
         }
       }
       // symmetric component -> (c_in, c_out): (0,0) (0,1) (0,2) (1,1) (1,2) (2,2)
       const int cin = comp < 3 ? 0 : (comp < 5 ? 1 : 2), cout = comp < 3 ? comp : (comp < 5 ? comp - 2 : 2);
-      auto put = [&](int c, const float* o) {
-        float4* d0 = reinterpret_cast<float4*>(SL3 + (((v * 3 + cin) * nc + c) * 3 + cout) * (long)ng + grid0);
-        float4* d1 = reinterpret_cast<float4*>(SL3 + (((v * 3 + cout) * nc + c) * 3 + cin) * (long)ng + grid0);
+      auto put = [&](int c, const TV* o) {
+        TV* d0 = SL3 + (((v * 3 + cin) * nc + c) * 3 + cout) * (long)ng + grid0;
+        TV* d1 = SL3 + (((v * 3 + cout) * nc + c) * 3 + cin) * (long)ng + grid0;
+        using V = decltype(vec16(o, 0));
+        constexpr int W = 16 / sizeof(TV);
 #pragma unroll
-        for (int q = 0; q < P / 4; q++) {
-          const float4 w = make_float4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
-          d0[q] = w;
-          if (cin != cout) d1[q] = w;
+        for (int q = 0; q < P / W; q++) {
+          const V w = vec16(o, W * q);
+          reinterpret_cast<V*>(d0)[q] = w;
+          if (cin != cout) reinterpret_cast<V*>(d1)[q] = w;
         }
       };
       put(c0, acc0);
@@ -479,19 +486,21 @@ __global__ void __launch_bounds__(RtF32Cfg<P>::NT, RtF32Cfg<P>::MINB)
   }
 }
 
-static size_t rt_f32_smem(int p0, int mpt) {
+template <typename TV>
+static size_t rt_item_smem(int p0, int mpt) {
   const int nc = p0 * (p0 + 2), lda = nc + 1, ni = (p0 + 1) * (p0 + 2) / 2;
   const size_t fl = (size_t)p0 * lda + mpt + (size_t)(p0 + 1) * 2 * p0 + 4 * p0;
-  return fl * sizeof(float) + (size_t)(p0 + 2) * sizeof(int) + (size_t)nc * 2 + (size_t)ni * 4 + 16;
+  return fl * sizeof(TV) + (size_t)(p0 + 2) * sizeof(int) + (size_t)nc * 2 + (size_t)ni * 4 + 16;
 }
 
-template <int P, typename TC>
-static int launch_rt_f32(const TC* C, long nv, const DevTables& T, float* SL3, cudaStream_t st) {
+template <int P, typename TC, typename TV = float>
+static int launch_rt_item(const TC* C, long nv, const DevTables& T, TV* SL3, cudaStream_t st) {
   const int mpt = mr_per_t(T);
   dim3 grid(P + 1, (unsigned)nv);
-  const size_t smem = rt_f32_smem(P, mpt);  // about 48 KB at p = 16 (four CTAs per SM), 149 KB at p = 24
-  VES3D_CK(cudaFuncSetAttribute(k_rotate_transpose_f32<P, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_rotate_transpose_f32<P, TC><<<grid, RtF32Cfg<P>::NT, smem, st>>>(C, mpt, T, SL3);
+  const size_t smem = rt_item_smem<TV>(P, mpt);  // about 48 KB at p = 16 (four CTAs per SM), 149 KB at p = 24
+  VES3D_CK(cudaFuncSetAttribute(k_rotate_transpose_item<P, TC, TV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem));
+  k_rotate_transpose_item<P, TC, TV><<<grid, RtItemCfg<P, TV>::NT, smem, st>>>(C, mpt, T, SL3);
   VES3D_LAUNCHED();
   return VES3D_OK;
 }
@@ -503,7 +512,7 @@ int launch_rotate_transpose_f32(const float* C, long nv, const DevTables& T, flo
     set_error("internal: FP32 rotate-transpose at p = %d (built for p = 16)", T.p0);
     return VES3D_ERR_ARG;
   }
-  return launch_rt_f32<16>(C, nv, T, SL3, st);
+  return launch_rt_item<16>(C, nv, T, SL3, st);
 }
 
 bool rotate_transpose_f32_from_f64_supported(int p0) { return p0 == 12 || p0 == 24; }
@@ -511,8 +520,8 @@ bool rotate_transpose_f32_from_f64_supported(int p0) { return p0 == 12 || p0 == 
 int launch_rotate_transpose_f32(const double* C, long nv, const DevTables& T, float* SL3, cudaStream_t st) {
   if (nv <= 0) return VES3D_OK;
   switch (T.p0) {
-    case 12: return launch_rt_f32<12>(C, nv, T, SL3, st);
-    case 24: return launch_rt_f32<24>(C, nv, T, SL3, st);
+    case 12: return launch_rt_item<12>(C, nv, T, SL3, st);
+    case 24: return launch_rt_item<24>(C, nv, T, SL3, st);
     default: break;
   }
   set_error("internal: FP32 rotate-transpose of FP64 results at p = %d (built for p in {12, 24})", T.p0);
@@ -683,6 +692,9 @@ __global__ void __launch_bounds__(256, 2) k_rotate_transpose_tc(const double* __
 int launch_rotate_transpose_scatter(const double* C, long nv, const DevTables& T, double* SL3, cudaStream_t st) {
   if (nv <= 0) return VES3D_OK;
   const int p0 = T.p0, nc = ncoef_(p0);
+  // p = 16: the per-item kernel in FP64 (5.8 ms per 512-vesicle build against 9.5 ms for the
+  // DMMA form below, which keeps the other orders up to 16)
+  if (p0 == 16 && !tc_rotate_disabled()) return launch_rt_item<16, double, double>(C, nv, T, SL3, st);
   {
     // tensor-core form: the largest component block (3, 2 or 1 components x p0 rows)
     // whose staging fits two CTAs per SM; 6 must be a multiple of the block
